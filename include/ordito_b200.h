@@ -1,0 +1,185 @@
+/*
+ * ordito_b200 -- C ABI of the B200 heat-method geodesic path.
+ *
+ * Every entry point is extern "C", takes plain device pointers and sizes, returns an int status
+ * (OB_OK = 0) and never throws across the boundary. A failed call leaves a one-line message in
+ * ob_last_error() (per thread). Device buffers are caller-owned unless a function says otherwise;
+ * all work is enqueued on the given stream (NULL = the legacy default stream) and is asynchronous
+ * unless a function documents a host read-back.
+ *
+ * Each declaration names the reference interface it replaces (paths within the ordito project,
+ * ordito 0.5.2). A Python binding of this header is ordito_b200/_lib.py (ctypes).
+ */
+#ifndef ORDITO_B200_H
+#define ORDITO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* ob_stream_t; /* a cudaStream_t */
+
+/* Status codes. */
+#define OB_OK 0
+#define OB_ERR_INVALID 1         /* bad argument (shape, size, null pointer)            */
+#define OB_ERR_CUDA 2            /* a CUDA runtime call failed                           */
+#define OB_ERR_NOMEM 3           /* device allocation refused                            */
+#define OB_ERR_INDEX 4           /* a vertex index out of [0, n_vertices)                */
+#define OB_ERR_NOT_CONVERGED 5   /* iteration cap reached outside tolerance              */
+#define OB_ERR_NONFINITE 6       /* a non-finite residual stopped the iteration          */
+#define OB_ERR_INDEFINITE 7      /* a factorisation met a non-positive pivot             */
+#define OB_ERR_TIMEOUT 8         /* a bounded device wait gave up                        */
+#define OB_ERR_BUDGET 9          /* over the memory budget                               */
+
+/* Solver status words written by the device loops (never a trap). */
+#define OB_STATUS_CONVERGED 0
+#define OB_STATUS_CAPPED 1
+#define OB_STATUS_NONFINITE 2
+#define OB_STATUS_SETTLED 3
+#define OB_STATUS_SETTLE_BOUND 4
+
+const char* ob_last_error(void);
+int ob_version(void);
+
+/* ---- runtime plumbing (device memory, copies, streams, events) ---------------------------- */
+int ob_device_count(int* count);
+int ob_set_device(int device);
+int ob_get_device(int* device);
+/* Stream-ordered pool allocation: usable on `stream` (and after a sync, anywhere); ob_free
+ * releases it in `stream` order, so pass the stream of the buffer's last use. */
+int ob_malloc(size_t bytes, void** ptr, ob_stream_t stream);
+int ob_free(void* ptr, ob_stream_t stream);
+int ob_host_alloc(size_t bytes, void** ptr);             /* pinned host memory              */
+int ob_host_free(void* ptr);
+/* kind: 0 host->device, 1 device->host, 2 device->device, 3 host->host (cudaMemcpyKind order
+ * 1, 2, 3, 0); the copy is enqueued on stream and, with sync != 0, waited for. */
+int ob_memcpy(void* dst, const void* src, size_t bytes, int kind, ob_stream_t stream, int sync);
+int ob_memset(void* dst, int value, size_t bytes, ob_stream_t stream);
+int ob_stream_create(ob_stream_t* stream);
+int ob_stream_destroy(ob_stream_t stream);
+int ob_stream_synchronize(ob_stream_t stream);
+int ob_device_synchronize(void);
+int ob_event_create(void** event);
+int ob_event_destroy(void* event);
+int ob_event_record(void* event, ob_stream_t stream);
+int ob_event_elapsed_ms(void* start, void* end, float* ms); /* synchronizes on end           */
+/* Number of this library's kernel launches so far in this process (a counter the launches bump). */
+int ob_launch_count(uint64_t* count);
+
+/* ---- a1: mesh operator pattern --------------------------------------------------------------
+ * Replaces ordito.laplacian.mesh_operator_pattern(faces, n_vertices) for the "cotmatrix"
+ * operator (ordito/laplacian.py:1071, _mesh_operator_pattern :1212, kernels store_operator_keys
+ * ordito/kernels/laplacian.py:707, csr_from_keys ordito/array.py:1688). Writes count = 6 F + V
+ * keys (row * V + col for both directions of each face edge, payload = corner slot 3 f + e; the
+ * diagonal of every referenced vertex; the sentinel V * V otherwise), sorts them stably and
+ * places the runs: offsets[V + 1], columns[count] (offsets[V] used), run_start[count], and the
+ * sorted keys[count] / order[count]. The diagonal slots' payload is -1. */
+int ob_pattern_workspace(int n_vertices, int n_faces, size_t* bytes);
+int ob_pattern_build(const int32_t* faces, int n_faces, int n_vertices, int32_t* offsets,
+                     int32_t* columns, int32_t* run_start, uint64_t* keys, int32_t* order,
+                     void* workspace, size_t workspace_bytes, ob_stream_t stream);
+
+/* ---- a2/a3: per-face terms -------------------------------------------------------------------
+ * Replaces kernels/heat.py:92 heat_face_terms (and laplacian.cotmatrix_entries,
+ * ordito/laplacian.py:189): the float32 half-cotangent table cot[F, 3] (skipped when cot is NULL),
+ * unit normals[F, 3], areas[F] and the exact float64 corner sums of the areas area_sums[V]
+ * (zeroed here first). xyz is float32[V, 3], faces int32[F, 3]. */
+int ob_face_terms(const float* xyz, const int32_t* faces, int n_faces, int n_vertices, float* cot,
+                  float* normals, float* areas, double* area_sums, ob_stream_t stream);
+
+/* ---- a4: edge-length sums for the default time step -----------------------------------------
+ * Replaces kernels/heat.py:173 upper_edge_length_sum_and_count (heat.py:2248 _edge_length_sums):
+ * out[0] = sum of weight * |v_col - v_row| over the strict upper triangle, out[1] = sum of
+ * weights; weight = run length (faces holding the edge) with face_edges != 0, else 1. Summed in a
+ * fixed order (bit-reproducible). */
+int ob_edge_sums(const int32_t* offsets, const int32_t* columns, const int32_t* run_start,
+                 const uint64_t* keys, int count, int n_vertices, const float* xyz,
+                 int face_edges, double* out, ob_stream_t stream);
+
+/* ---- a5: operator rows ------------------------------------------------------------------------
+ * Replaces kernels/heat.py:361 heat_system_rows: over the pattern, L (cotangent Laplacian,
+ * off-diagonal = run sum of f64(cot) in sorted order, diagonal = -row sum), H = factor L + M and
+ * P = -L, with factor = scale (from_edges == 0) or scale * (out[0] / out[1])^2 from ob_edge_sums
+ * (from_edges != 0); mass[V] = area_sums / mass_divisor. L/H/P have offsets[V] entries. */
+int ob_heat_rows(const int32_t* offsets, const int32_t* columns, const int32_t* run_start,
+                 const uint64_t* keys, int count, const int32_t* order, int n_vertices,
+                 const float* cot, double scale, const double* edge_sums, int from_edges,
+                 const double* area_sums, double mass_divisor, double* L, double* H, double* P,
+                 double* mass, ob_stream_t stream);
+
+/* ---- a6: source indicator -------------------------------------------------------------------
+ * Replaces kernels/heat.py:614 seed_source_indicator: u0[V] zeroed then u0[s] = 1 for each source;
+ * an index outside [0, V) writes nothing and sets invalid[0] = 1 (invalid is zeroed here). */
+int ob_seed(const int32_t* sources, int n_sources, int n_vertices, double* u0, int32_t* invalid,
+            ob_stream_t stream);
+
+/* ---- a8: unit gradient and divergence ---------------------------------------------------------
+ * Replaces kernels/heat.py:658 unit_gradient_divergence: neg_div[V] (zeroed here) accumulates
+ * -div(X) of the per-face normalised gradient of u (float64). With n_columns > 1, u and neg_div
+ * hold n_columns fields laid out [V][n_columns] (one vertex's columns contiguous). */
+int ob_grad_div(const float* xyz, const int32_t* faces, int n_faces, int n_vertices,
+                const float* normals, const float* areas, const double* u, const float* cot,
+                int n_columns, double* neg_div, ob_stream_t stream);
+
+/* ---- a13: shift to the sources ------------------------------------------------------------
+ * Replaces heat.py:3134 _shift_to_sources (kernels source_and_global_sums :3384 and
+ * shift_and_orient :3410): phi -= mean(phi[sources]); with orient != 0 the field is flipped when
+ * its mean falls below that offset. With n_columns > 1 phi is [V][n_columns] and column c uses
+ * sources[source_offsets[c] .. source_offsets[c + 1]) (a device array; NULL for one column, which
+ * then uses the n_sources entries of sources). Every column needs at least one source. The sums
+ * are folded in a fixed order. */
+int ob_shift(double* phi, int n_vertices, const int32_t* sources, int n_sources,
+             const int32_t* source_offsets, int n_columns, int orient, ob_stream_t stream);
+
+/* ---- a7/a9: preconditioned conjugate gradient ---------------------------------------------
+ * Replaces ordito/linalg.py:3619 _BatchedCg with the kernels of
+ * kernels/algorithms/conjugate_gradient.py (cg_matvec_dots :453, cg_update :797, settle
+ * :1509/:1564) and the Jacobi-Chebyshev preconditioner (linalg.py:5135, multigrid.py:988).
+ * A solver borrows the CSR arrays (they must outlive it) and owns its work vectors.
+ * precond: 0 Jacobi, 1 Jacobi-Chebyshev (degree 12, interval [max(min(80/n, .5), 1-r), 1+r]).
+ * narrow != 0 iterates on float32 copies of the values (vectors, dots, scalars stay float64).
+ * n_columns right-hand sides are solved together; rhs/x are laid out [n][n_columns]. */
+int ob_pcg_create(int n, const int32_t* offsets, const int32_t* columns, const double* values,
+                  int n_columns, int precond, int narrow, void** solver, ob_stream_t stream);
+int ob_pcg_destroy(void* solver);
+/* solve_spd (linalg.py:1356): stops a column at |r| <= tol |b| (2-norm), or at maxiter rounds.
+ * Host read-back of iterations[n_columns] and residual[n_columns] (|r| / |b|) when non-NULL. */
+int ob_pcg_solve(void* solver, const double* rhs, double* x, double tol, int maxiter,
+                 int* iterations, double* relative_residual, ob_stream_t stream);
+/* solve_spd_settled (linalg.py:2490): tolerance 0; every check_rounds rounds stop once no entry
+ * is newly non-zero and none moved by change_tolerance of itself, or settle_rounds rounds after
+ * the non-zero count last changed, or at maxiter. Host read-back of *rounds and *status. */
+int ob_pcg_settle(void* solver, const double* rhs, double* x, int check_rounds,
+                  double change_tolerance, int settle_rounds, int maxiter, int* rounds,
+                  int* status, ob_stream_t stream);
+/* Measurement hooks (no counterpart in the reference): the average duration of `reps` standalone
+ * launches of the solver's round mat-vec-with-dots kernel on its current vectors (CUDA events on
+ * `stream`), and the solver's shape: info[0..4] = n, padded columns, nnz, narrow, blocks. */
+int ob_pcg_time_matvec(void* solver, int reps, float* ms, ob_stream_t stream);
+int ob_pcg_info(void* solver, long long* info);
+/* backward_error_exceeds (kernels/linalg.py:1167): flag[0] = 1 when some row has
+ * |b - A x|_i > tol (|A| |x| + |b|)_i (or is NaN). flag is zeroed here. */
+int ob_backward_error(int n, const int32_t* offsets, const int32_t* columns, const double* values,
+                      const double* x, const double* rhs, int n_columns, double tol,
+                      int32_t* flag, ob_stream_t stream);
+/* Element-wise out[i] = in[i] * scale with a type conversion; types 0 = float32, 1 = float64.
+ * A utility of the host layer (no counterpart in the reference's path; it keeps every value the
+ * host layer returns formed on the device). */
+int ob_cast_scale(const void* in, int in_type, void* out, int out_type, long long n, double scale,
+                  ob_stream_t stream);
+/* Axis-aligned bounds of float32 points xyz[n, 3]: out[6] = (min xyz, max xyz), as float64 of the
+ * float32 extremes. Replaces the mesh bounds the time-step floor reads (ordito/mesh.py:1045,
+ * heat.py:5228 _diffusion_floor). */
+int ob_bounds(const float* xyz, int n, double* out, ob_stream_t stream);
+/* y = A x (float64), n_columns columns [n][n_columns]. */
+int ob_spmv(int n, const int32_t* offsets, const int32_t* columns, const double* values,
+            const double* x, double* y, int n_columns, ob_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ORDITO_B200_H */

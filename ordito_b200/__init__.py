@@ -1,0 +1,13 @@
+"""ordito_b200: a B200 (sm_100a) build of ordito's heat-method geodesic path.
+
+Drop-in modules for the path: ``laplacian`` (pattern, cotangent weights, Laplacian, mass),
+``heat`` (``heat_operators``, ``heat_geodesic``, ``HeatSolver``), ``linalg`` (``solve_spd``,
+``solve_spd_settled``, the Jacobi and Chebyshev preconditioners), ``cholesky`` and ``mesh``
+(``Trimesh``). The compute runs in hand-written CUDA kernels behind the C ABI of
+``include/ordito_b200.h`` (``libordito_b200.so``, built by ``python -m ordito_b200.build``).
+"""
+
+from ordito_b200 import creation  # noqa: F401  (host-only mesh generators)
+
+__all__ = ["array", "cholesky", "creation", "device", "heat", "laplacian", "linalg", "mesh"]
+__version__ = "0.1.0"

@@ -1,0 +1,140 @@
+"""ctypes binding of ``include/ordito_b200.h`` (``libordito_b200.so``, built in-tree).
+
+The product path has no CPU fallback: importing a function of this module on a machine without
+the built library raises ``ImportError``, and a CUDA error in any call raises ``RuntimeError``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_size_t, c_uint64, c_void_p
+from pathlib import Path
+
+LIBRARY_PATH = Path(__file__).resolve().parent / "libordito_b200.so"
+
+OB_OK = 0
+OB_ERR_INVALID = 1
+OB_ERR_CUDA = 2
+OB_ERR_NOMEM = 3
+OB_ERR_INDEX = 4
+OB_ERR_NOT_CONVERGED = 5
+OB_ERR_NONFINITE = 6
+OB_ERR_INDEFINITE = 7
+OB_ERR_TIMEOUT = 8
+OB_ERR_BUDGET = 9
+
+STATUS_CONVERGED = 0
+STATUS_CAPPED = 1
+STATUS_NONFINITE = 2
+STATUS_SETTLED = 3
+STATUS_SETTLE_BOUND = 4
+
+P = c_void_p
+I = c_int
+D = c_double
+
+# name -> argument types (every function returns int status unless listed in _RESTYPES).
+SIGNATURES: dict[str, list] = {
+    "ob_last_error": [],
+    "ob_version": [],
+    "ob_device_count": [POINTER(c_int)],
+    "ob_set_device": [I],
+    "ob_get_device": [POINTER(c_int)],
+    "ob_malloc": [c_size_t, POINTER(c_void_p), P],
+    "ob_free": [P, P],
+    "ob_host_alloc": [c_size_t, POINTER(c_void_p)],
+    "ob_host_free": [P],
+    "ob_memcpy": [P, P, c_size_t, I, P, I],
+    "ob_memset": [P, I, c_size_t, P],
+    "ob_stream_create": [POINTER(c_void_p)],
+    "ob_stream_destroy": [P],
+    "ob_stream_synchronize": [P],
+    "ob_device_synchronize": [],
+    "ob_event_create": [POINTER(c_void_p)],
+    "ob_event_destroy": [P],
+    "ob_event_record": [P, P],
+    "ob_event_elapsed_ms": [P, P, POINTER(c_float)],
+    "ob_launch_count": [POINTER(c_uint64)],
+    "ob_pattern_workspace": [I, I, POINTER(c_size_t)],
+    "ob_pattern_build": [P, I, I, P, P, P, P, P, P, c_size_t, P],
+    "ob_face_terms": [P, P, I, I, P, P, P, P, P],
+    "ob_edge_sums": [P, P, P, P, I, I, P, I, P, P],
+    "ob_heat_rows": [P, P, P, P, I, P, I, P, D, P, I, P, D, P, P, P, P, P],
+    "ob_seed": [P, I, I, P, P, P],
+    "ob_grad_div": [P, P, I, I, P, P, P, P, I, P, P],
+    "ob_shift": [P, I, P, I, P, I, I, P],
+    "ob_pcg_create": [I, P, P, P, I, I, I, POINTER(c_void_p), P],
+    "ob_pcg_destroy": [P],
+    "ob_pcg_solve": [P, P, P, D, I, POINTER(c_int), POINTER(c_double), P],
+    "ob_pcg_settle": [P, P, P, I, D, I, I, POINTER(c_int), POINTER(c_int), P],
+    "ob_pcg_time_matvec": [P, I, POINTER(c_float), P],
+    "ob_pcg_info": [P, POINTER(ctypes.c_longlong)],
+    "ob_backward_error": [I, P, P, P, P, P, I, D, P, P],
+    "ob_spmv": [I, P, P, P, P, P, I, P],
+    "ob_cast_scale": [P, I, P, I, ctypes.c_longlong, D, P],
+    "ob_bounds": [P, I, P, P],
+}
+_RESTYPES = {"ob_last_error": c_char_p}
+
+
+class _Library:
+    """The loaded library with typed functions; missing library -> ImportError on first use."""
+
+    def __init__(self) -> None:
+        self._lib: ctypes.CDLL | None = None
+
+    def load(self) -> ctypes.CDLL:
+        if self._lib is None:
+            if not LIBRARY_PATH.exists():
+                raise ImportError(
+                    f"{LIBRARY_PATH.name} is not built: run `python -m ordito_b200.build` "
+                    "(nvcc, sm_100a); ordito_b200 has no CPU fallback"
+                )
+            lib = ctypes.CDLL(str(LIBRARY_PATH))
+            for name, argtypes in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.argtypes = argtypes
+                fn.restype = _RESTYPES.get(name, c_int)
+            self._lib = lib
+        return self._lib
+
+    def __getattr__(self, name: str):
+        return getattr(self.load(), name)
+
+
+lib = _Library()
+
+
+class CudaError(RuntimeError):
+    """A CUDA runtime failure inside the library."""
+
+
+def check(status: int, what: str = "") -> None:
+    """Raise the Python exception an ``OB_ERR_*`` status maps to."""
+    if status == OB_OK:
+        return
+    message = (lib.ob_last_error() or b"").decode(errors="replace")
+    text = f"{what}: {message}" if what else message
+    if status == OB_ERR_INVALID or status == OB_ERR_INDEX:
+        raise ValueError(text)
+    if status == OB_ERR_NOMEM:
+        raise MemoryError(text)
+    raise CudaError(f"[status {status}] {text}")
+
+
+def call(name: str, *args) -> None:
+    """Call ``name`` and raise on a non-zero status."""
+    check(getattr(lib, name)(*args), name)
+
+
+def launch_count() -> int:
+    """Kernel launches this library made so far in the process."""
+    value = c_uint64(0)
+    check(lib.ob_launch_count(ctypes.byref(value)))
+    return int(value.value)
+
+
+def device_count() -> int:
+    value = c_int(0)
+    check(lib.ob_device_count(ctypes.byref(value)))
+    return int(value.value)

@@ -1,0 +1,64 @@
+"""Builds libordito_b200.so in-tree: every .cu under csrc/ for sm_100a, linked with static cudart.
+
+Run as ``python -m ordito_b200.build`` (or through ``__graft_entry__.build()``). Objects are
+rebuilt only when a source or header is newer than them.
+"""
+
+from __future__ import annotations
+
+import concurrent.futures
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+BUILD = HERE / "_build"
+LIBRARY = HERE / "libordito_b200.so"
+INCLUDE = HERE.parent / "include"
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+         f"-I{INCLUDE}"]
+
+
+def _headers() -> list[Path]:
+    return sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
+
+
+def _compile(source: Path, verbose: bool) -> Path:
+    obj = BUILD / (source.stem + ".o")
+    newest = max([source.stat().st_mtime] + [h.stat().st_mtime for h in _headers()])
+    if obj.exists() and obj.stat().st_mtime >= newest:
+        return obj
+    cmd = [NVCC, *ARCH, *FLAGS, "-c", str(source), "-o", str(obj)]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    result = subprocess.run(cmd, capture_output=True, text=True)
+    if result.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {source.name}:\n{result.stdout}\n{result.stderr}")
+    if verbose:
+        sys.stderr.write(result.stderr)
+    return obj
+
+
+def build(verbose: bool = False) -> Path:
+    """Compile and link the library; returns its path."""
+    BUILD.mkdir(exist_ok=True)
+    sources = sorted(CSRC.glob("*.cu"))
+    with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as pool:
+        objects = list(pool.map(lambda s: _compile(s, verbose), sources))
+    newest = max(o.stat().st_mtime for o in objects)
+    if not LIBRARY.exists() or LIBRARY.stat().st_mtime < newest:
+        cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(LIBRARY),
+               *map(str, objects), "-lcuda"]
+        result = subprocess.run(cmd, capture_output=True, text=True)
+        if result.returncode != 0:
+            raise RuntimeError(f"link failed:\n{result.stdout}\n{result.stderr}")
+    return LIBRARY
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

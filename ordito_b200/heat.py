@@ -1,0 +1,347 @@
+"""The heat-method geodesic distance (Crane et al.), ``ordito.heat``'s path subset.
+
+``heat_geodesic`` (ordito/heat.py:391), ``heat_operators`` (:200) and ``HeatSolver`` (:3491) with
+the reference's signatures, defaults and errors. A query is: seed the source indicator, diffuse it
+by the heat system ``M - t L`` (Jacobi CG to settled entries, or the held Cholesky factor),
+integrate the face-wise unit gradient's divergence, solve the Poisson system ``-L`` (Chebyshev-
+preconditioned CG to relative residual 1e-8, or the held factor), and shift to the sources. Every
+step is a CUDA kernel of ``libordito_b200.so``; the host only reads back the documented scalars
+(an invalid-source flag, solver counts, and -- once per solver -- the mean edge length and bounds).
+"""
+
+from __future__ import annotations
+
+import logging
+import math
+from typing import Any, NamedTuple
+
+import numpy as np
+
+from ordito_b200 import _lib
+from ordito_b200 import linalg as twl
+from ordito_b200.array import CsrMatrix
+from ordito_b200.device import DEFAULT_STREAM, DeviceArray, as_device, device_pointer
+from ordito_b200.laplacian import (
+    MeshOperatorPattern,
+    assemble_rows,
+    face_terms,
+    mesh_arrays,
+    mesh_operator_pattern,
+)
+from ordito_b200.mesh import Trimesh, mesh_arguments
+
+_LOGGER = logging.getLogger(__name__)
+
+_CG_TOLERANCE = 1e-8  # ordito/heat.py:108
+_HEAT_CHECK_ROUNDS = 16  # :142
+_HEAT_CHANGE_TOLERANCE = 1e-6  # :146
+_HEAT_SETTLE_ROUNDS = 192  # :147
+_DIFFUSION_DECAY = 400.0  # :158
+
+
+class HeatOperators(NamedTuple):
+    """What ``heat_operators`` returns (ordito/heat.py:169-178)."""
+
+    heat_system: CsrMatrix
+    heat_preconditioner: twl.Preconditioner
+    laplacian: CsrMatrix
+    poisson_system: CsrMatrix
+    poisson_preconditioner: twl.Preconditioner
+    cot_entries: DeviceArray
+    face_normals: DeviceArray
+    face_areas: DeviceArray
+
+
+def _heat_method_choices(method: str) -> tuple[str, str]:
+    """``(mass, timestep)`` of a discretization (ordito/heat.py:2002-2012)."""
+    if method == "potpourri3d":
+        return "barycentric", "unique_edges"
+    if method == "meshlab":
+        return "barycentric", "face_edges"
+    if method == "igl":
+        return "voronoi", "unique_edges"
+    raise ValueError(f"method must be 'potpourri3d', 'meshlab' or 'igl', got {method!r}")
+
+
+def _supported(method: str, use_robust: bool) -> None:
+    mass, _ = _heat_method_choices(method)
+    if mass == "voronoi":
+        raise NotImplementedError("method='igl' (Voronoi mass, rim-pinned heat) is not built yet")
+    if use_robust:
+        raise NotImplementedError("use_robust (mollified / intrinsic operators) is not built yet")
+
+
+def _assemble(mesh: Trimesh, t: float | None, method: str, cot_entries: Any = None,
+              pattern: MeshOperatorPattern | None = None) -> tuple[HeatOperators, Any]:
+    _, timestep = _heat_method_choices(method)
+    if pattern is None:
+        pattern = mesh.mesh_operator_pattern
+    elif pattern.n_vertices != mesh.n_vertices or pattern.operator != "cotmatrix":
+        raise ValueError("pattern was built for another operator or vertex count")
+    if cot_entries is None:
+        terms = mesh.face_terms
+    else:
+        terms = face_terms(mesh.vertices, mesh.faces, mesh.n_vertices, mesh.n_faces, cot_entries)
+    built = assemble_rows(
+        pattern, mesh.vertices, terms.cot, terms.area_sums, t=t, face_edges=timestep == "face_edges"
+    )
+    operators = HeatOperators(
+        built.heat,
+        twl.jacobi_preconditioner(built.heat),
+        built.laplacian,
+        built.poisson,
+        twl.chebyshev_preconditioner(built.poisson),
+        terms.cot,
+        terms.normals,
+        terms.areas,
+    )
+    return operators, built
+
+
+def heat_operators(
+    vertices: Any,
+    faces: Any,
+    t: float | None = None,
+    *,
+    use_robust: bool = False,
+    cot_entries: Any = None,
+    pattern: MeshOperatorPattern | None = None,
+    method: str = "potpourri3d",
+) -> HeatOperators:
+    """Assemble the source-independent operators the heat method solves against.
+
+    ``t`` None takes ``h ** 2`` formed on the device, ``h`` the mean edge length ``method`` names
+    (unique edges for ``"potpourri3d"``, every face's three edges for ``"meshlab"``).
+    """
+    if cot_entries is not None and use_robust:
+        raise ValueError(
+            "cot_entries and use_robust are mutually exclusive: use_robust rebuilds the "
+            "half-cotangent table from mollified edge lengths."
+        )
+    _supported(method, use_robust)
+    mesh = Trimesh(vertices, faces)
+    return _assemble(mesh, t, method, cot_entries, pattern)[0]
+
+
+def _diffusion_floor(mesh: Trimesh) -> float:
+    """``(|bounding-box diagonal| / 400) ** 2`` (ordito/heat.py:5228)."""
+    low, high = mesh.bounds
+    return (math.dist(low, high) / _DIFFUSION_DECAY) ** 2
+
+
+def _settle_window(t: float | None, default: float) -> int:
+    """ordito/heat.py:5234: the settle window grows like ``sqrt(t / h^2)``."""
+    if t is None or not t > default > 0.0:
+        return _HEAT_SETTLE_ROUNDS
+    return math.ceil(_HEAT_SETTLE_ROUNDS * math.sqrt(t / default))
+
+
+class HeatSolver:
+    """A mesh's heat-method state for one ``(t, use_robust, method)`` (ordito/heat.py:3491).
+
+    Holds the operators, the native solver states, and -- on a system's second solve (rent or
+    buy, ordito/heat.py:4394) or when a settled iterate fails its check -- its sparse Cholesky
+    factorization, which later solves go through directly.
+    """
+
+    def __init__(self, mesh: Trimesh, t: float | None = None, *, use_robust: bool = False,
+                 method: str = "potpourri3d") -> None:
+        _supported(method, use_robust)
+        self._mesh = mesh
+        self.t = t
+        self.use_robust = use_robust
+        self.method = method
+        self._operators: HeatOperators | None = None
+        self._resolved: tuple[float | None, int] | None = None
+        self._systems: dict[str, Any] = {}
+        self._ill_conditioned = False
+        self._unfactorable = False
+        self.factor_on_second_solve = True
+
+    # -- time and operators ------------------------------------------------------------------
+    def _vertex_time(self) -> tuple[float | None, int]:
+        """The time the systems are built at (``None``: the device's ``h ** 2``) and the settle
+        window (ordito/heat.py:3714-3736)."""
+        if self._resolved is None:
+            t = self.t
+            mesh = self._mesh
+            if self.method == "meshlab":
+                mean = mesh.mean_edge_length
+            else:
+                mean = self._unique_mean_edge_length()
+            default = mean**2
+            if t is None:
+                floor = _diffusion_floor(mesh)
+                t = floor if floor > default else None
+            self._resolved = (t, _settle_window(t, default))
+        return self._resolved
+
+    def _unique_mean_edge_length(self) -> float:
+        mesh = self._mesh
+        pattern = mesh.mesh_operator_pattern
+        sums = DeviceArray.empty(2, np.float64)
+        _lib.call(
+            "ob_edge_sums", pattern.offsets.ptr, pattern.columns.ptr, pattern.run_start.ptr,
+            pattern.keys.ptr, pattern.n_keys, mesh.n_vertices, mesh.vertices.ptr, 0, sums.ptr,
+            DEFAULT_STREAM,
+        )  # fmt: skip
+        total, count = sums.numpy()
+        return float(total / count) if count > 0 else 0.0
+
+    @property
+    def operators(self) -> HeatOperators:
+        if self._operators is None:
+            t, _ = self._vertex_time()
+            self._operators = _assemble(self._mesh, t, self.method)[0]
+        return self._operators
+
+    # -- solves --------------------------------------------------------------------------------
+    def _system(self, role: str) -> Any:
+        from ordito_b200.cholesky import OperatorFactorization  # noqa: PLC0415
+
+        kept = self._systems.get(role)
+        if kept is None:
+            matrix = self.operators.heat_system if role == "heat" else self.operators.poisson_system
+            kept = self._systems[role] = {
+                "factorization": OperatorFactorization(matrix, self._mesh.vertices),
+                "solves": 0,
+            }
+        return kept
+
+    def _kept(self, role: str) -> Any:
+        """Count a solve of ``role``'s system, factoring it on its second (rent or buy)."""
+        kept = self._system(role)
+        kept["solves"] += 1
+        factorization = kept["factorization"]
+        if (self.factor_on_second_solve and kept["solves"] >= 2
+                and factorization.factorization is None and not factorization.refused):
+            if factorization.factor(self._sharing(role)):
+                _LOGGER.debug("HeatSolver: factored the %s system on its second solve", role)
+        return kept
+
+    def _sharing(self, role: str) -> Any:
+        heat = self._systems.get("heat")
+        return heat["factorization"] if role == "poisson" and heat is not None else None
+
+    def factor(self) -> bool:
+        """Factor both systems now (ordito/heat.py:3863); False if either could not be."""
+        ok = True
+        for role in ("heat", "poisson"):
+            kept = self._system(role)
+            if kept["factorization"].factorization is None:
+                ok = kept["factorization"].factor(self._sharing(role)) and ok
+        return ok
+
+    def diffuse(self, rhs: Any, solution: Any) -> None:
+        """Solve the heat system ``(M - t L) u = rhs`` to settled entries, in place."""
+        operators = self.operators
+        kept = self._kept("heat")
+        held = kept["factorization"].factorization is not None
+        twl.solve_spd_settled(
+            operators.heat_system,
+            rhs,
+            solution,
+            check_rounds=_HEAT_CHECK_ROUNDS,
+            change_tolerance=_HEAT_CHANGE_TOLERANCE,
+            settle_rounds=self._vertex_time()[1],
+            factorization=kept["factorization"],
+            narrow_values=True,
+        )
+        if not held and kept["factorization"].factorization is not None:
+            self._ill_conditioned = True
+
+    def solve_poisson(self, rhs: Any, solution: Any) -> None:
+        """Solve ``(-L) phi = rhs`` (consistent), warm-started from ``solution``, in place."""
+        operators = self.operators
+        kept = self._kept("poisson")
+        factorization = kept["factorization"]
+        if factorization.factorization is None and self._ill_conditioned:
+            factorization.factor(self._sharing("poisson"))
+        if factorization.factorization is not None:
+            factorization.solve(rhs, solution, tol=twl.SETTLE_DIRECT_TOLERANCE)
+            return
+        twl.solve_spd(
+            operators.poisson_system,
+            rhs,
+            solution,
+            tol=_CG_TOLERANCE,
+            preconditioner=operators.poisson_preconditioner,
+            name="heat_geodesic",
+        )
+
+    def release_factorizations(self) -> None:
+        for kept in self._systems.values():
+            kept["factorization"].release()
+
+    @property
+    def nbytes(self) -> int:
+        total = 0
+        for kept in self._systems.values():
+            total += kept["factorization"].nbytes
+        return total
+
+
+def _require_sources(sources: Any, n_vertices: int) -> DeviceArray:
+    src = as_device(sources, np.int32)
+    return src.reshape(src.size)
+
+
+def _distance_from_heat(mesh: Trimesh, solver: HeatSolver, sources: DeviceArray,
+                        heat: DeviceArray, n_columns: int = 1,
+                        source_offsets: DeviceArray | None = None) -> DeviceArray:
+    """Divergence, Poisson solve and shift (ordito/heat.py:3052-3131)."""
+    operators = solver.operators
+    n = mesh.n_vertices
+    neg_div = DeviceArray.empty(n * n_columns, np.float64)
+    _lib.call(
+        "ob_grad_div", mesh.vertices.ptr, mesh.faces.ptr, mesh.n_faces, n,
+        operators.face_normals.ptr, operators.face_areas.ptr, heat.ptr, operators.cot_entries.ptr,
+        n_columns, neg_div.ptr, DEFAULT_STREAM,
+    )  # fmt: skip
+    phi = DeviceArray.zeros(n * n_columns, np.float64)
+    solver.solve_poisson(neg_div, phi)
+    _lib.call(
+        "ob_shift", phi.ptr, n, sources.ptr, sources.size,
+        source_offsets.ptr if source_offsets is not None else None, n_columns, 1, DEFAULT_STREAM,
+    )  # fmt: skip
+    return phi
+
+
+def heat_geodesic(
+    mesh: Any = None,
+    faces: Any = None,
+    sources: Any = None,
+    t: float | None = None,
+    *,
+    vertices: Any = None,
+    use_robust: bool = False,
+    method: str = "meshlab",
+) -> DeviceArray:
+    """Approximate geodesic distance to the nearest source vertex (heat method).
+
+    ``heat_geodesic(trimesh, sources)`` keeps the operators, solver states and factorizations on
+    the mesh; ``heat_geodesic(vertices, faces, sources, t=None)`` builds them for the call. Returns
+    the ``(n_vertices,)`` float64 distance on the device. Raises ``ValueError`` for a source index
+    outside ``[0, n_vertices)`` or an unknown ``method``.
+    """
+    if method not in ("meshlab", "igl", "potpourri3d"):
+        raise ValueError(f"method must be 'meshlab', 'igl' or 'potpourri3d', got {method!r}")
+    bound, _owned, src_arg = mesh_arguments("heat_geodesic", mesh, vertices, faces, sources)
+    if src_arg is None:
+        raise TypeError("heat_geodesic: sources are required")
+    n = bound.n_vertices
+    src = _require_sources(src_arg, n)
+    if n == 0 or bound.n_faces == 0 or src.size == 0:
+        return DeviceArray.zeros(n, np.float64)
+    _supported(method, use_robust)
+    solver = bound.heat_solver(t, use_robust=use_robust, method=method)
+    u0 = DeviceArray.empty(n, np.float64)
+    invalid = DeviceArray.empty(1, np.int32)
+    _lib.call("ob_seed", src.ptr, src.size, n, u0.ptr, invalid.ptr, DEFAULT_STREAM)
+    if int(invalid.numpy()[0]) != 0:
+        raise ValueError(
+            "heat_geodesic: every entry of sources must be a vertex index in [0, n_vertices)"
+        )
+    heat = DeviceArray.zeros(n, np.float64)
+    solver.diffuse(u0, heat)
+    return _distance_from_heat(bound, solver, src, heat)

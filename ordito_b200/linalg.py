@@ -1,0 +1,212 @@
+"""Conjugate-gradient solves of the heat path (``ordito.linalg``'s path subset).
+
+``solve_spd`` (ordito/linalg.py:1356), ``solve_spd_settled`` (:2490), ``jacobi_preconditioner``
+(:1591) and ``chebyshev_preconditioner`` (:5135) with the reference's signatures and contracts:
+``solution`` is the initial guess and is overwritten in place; a solver state is kept per operator
+for its lifetime, so a later solve replays its recorded device loop. The iteration runs in
+``libordito_b200.so`` (ob_pcg_*): Chronopoulos-Gear CG, loop and stopping tests on the device.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import warnings
+from typing import Any
+
+import numpy as np
+
+from ordito_b200 import _lib
+from ordito_b200.array import CsrMatrix
+from ordito_b200.device import DEFAULT_STREAM, DeviceArray, device_pointer, element_count
+
+CG_TOLERANCE = 1e-8
+CG_MAXITER_FACTOR = 10  # ordito/linalg.py:172
+SETTLE_BACKWARD_ERROR = 1e-6  # :178
+SETTLE_DIRECT_TOLERANCE = 1e-12  # :181
+
+_KINDS = {"diag": 0, "chebyshev": 1}
+
+
+class Preconditioner:
+    """A preconditioner this module builds for one operator: Jacobi or Jacobi-Chebyshev.
+
+    Stands in for the ``warp.optim.linear.LinearOperator`` ordito returns; ``solve_spd`` accepts
+    it only for the matrix it was built for, as the reference does (linalg.py:1500-1530).
+    """
+
+    def __init__(self, matrix: CsrMatrix, kind: str, n_columns: int = 1) -> None:
+        self.matrix = matrix
+        self.kind = kind
+        self.n_columns = n_columns
+        self.shape = (matrix.nrow * n_columns, matrix.nrow * n_columns)
+
+
+def jacobi_preconditioner(matrix: CsrMatrix) -> Preconditioner:
+    return Preconditioner(matrix, "diag")
+
+
+def chebyshev_preconditioner(matrix: CsrMatrix, n_columns: int = 1) -> Preconditioner:
+    """Degree-12 Jacobi-Chebyshev polynomial on ``[max(min(80/n, .5), 1-r), 1+r]``, ``r`` the
+    rows' largest Gershgorin ratio (built on the device at the first solve)."""
+    return Preconditioner(matrix, "chebyshev", n_columns)
+
+
+class NativeSolver:
+    """One ``ob_pcg_*`` solver state (owned work vectors and recorded loop graphs)."""
+
+    def __init__(self, matrix: CsrMatrix, kind: str, narrow: bool, n_columns: int) -> None:
+        handle = ctypes.c_void_p(0)
+        _lib.call(
+            "ob_pcg_create", matrix.nrow, matrix.offsets.ptr, matrix.columns.ptr,
+            matrix.values.ptr, int(n_columns), _KINDS[kind], int(narrow), ctypes.byref(handle),
+            DEFAULT_STREAM,
+        )  # fmt: skip
+        self.handle = handle
+        self.n = matrix.nrow
+        self.n_columns = n_columns
+        self._matrix = matrix  # keep the borrowed CSR arrays alive
+
+    def close(self) -> None:
+        if self.handle and self.handle.value:
+            _lib.lib.ob_pcg_destroy(self.handle)
+            self.handle = ctypes.c_void_p(0)
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, rhs: int, x: int, tol: float, maxiter: int) -> tuple[np.ndarray, np.ndarray]:
+        iters = (ctypes.c_int * self.n_columns)()
+        residual = (ctypes.c_double * self.n_columns)()
+        _lib.call("ob_pcg_solve", self.handle, rhs, x, float(tol), int(maxiter), iters, residual,
+                  DEFAULT_STREAM)
+        return np.frombuffer(iters, dtype=np.int32).copy(), np.frombuffer(residual).copy()
+
+    def settle(self, rhs: int, x: int, check_rounds: int, change_tolerance: float,
+               settle_rounds: int, maxiter: int) -> tuple[int, int]:
+        rounds, status = ctypes.c_int(0), ctypes.c_int(0)
+        _lib.call(
+            "ob_pcg_settle", self.handle, rhs, x, int(check_rounds), float(change_tolerance),
+            int(settle_rounds), int(maxiter), ctypes.byref(rounds), ctypes.byref(status),
+            DEFAULT_STREAM,
+        )  # fmt: skip
+        return rounds.value, status.value
+
+
+def _solver(matrix: CsrMatrix, kind: str, narrow: bool, n_columns: int) -> NativeSolver:
+    key = (kind, bool(narrow), int(n_columns))
+    solver = matrix._solvers.get(key)
+    if solver is None:
+        solver = matrix._solvers[key] = NativeSolver(matrix, kind, narrow, n_columns)
+    return solver
+
+
+def _kind(matrix: CsrMatrix, preconditioner: Preconditioner | None) -> str:
+    if preconditioner is None:
+        return "diag"
+    if not isinstance(preconditioner, Preconditioner) or preconditioner.matrix is not matrix:
+        raise ValueError("preconditioner must be one this module built for matrix")
+    return preconditioner.kind
+
+
+def _columns(matrix: CsrMatrix, rhs: Any, solution: Any) -> int:
+    n_rhs = element_count(rhs)
+    if matrix.nrow == 0 or n_rhs % matrix.nrow or element_count(solution) != n_rhs:
+        raise ValueError(
+            f"rhs and solution must hold n_columns * {matrix.nrow} entries of one shape"
+        )
+    return n_rhs // matrix.nrow
+
+
+def solve_spd(
+    matrix: CsrMatrix,
+    rhs: Any,
+    solution: Any,
+    *,
+    tol: float = CG_TOLERANCE,
+    maxiter: int | None = None,
+    check_every: int = 10,
+    preconditioner: Preconditioner | None = None,
+    name: str = "solve_spd",
+    narrow_values: bool = False,
+) -> tuple[int, float, float]:
+    """Solve one SPD (or consistent semi-definite) system by preconditioned CG, in place.
+
+    Returns ``(iterations, residual, tol)`` with ``residual`` the relative residual |r|/|b|;
+    warns (``UserWarning``) when the solve stops outside ``tol``, as ordito/linalg.py:7610 does.
+    ``narrow_values`` iterates on float32 copies of the values (float64 vectors and dots).
+    """
+    n_columns = _columns(matrix, rhs, solution)
+    kind = _kind(matrix, preconditioner)
+    cap = CG_MAXITER_FACTOR * matrix.nrow if maxiter is None else int(maxiter)
+    rhs_ptr, keep_rhs = device_pointer(rhs, np.float64)
+    x_ptr, keep_x = device_pointer(solution, np.float64)
+    solver = _solver(matrix, kind, narrow_values, n_columns)
+    iters, residual = solver.solve(rhs_ptr, x_ptr, tol, cap)
+    if isinstance(keep_x, DeviceArray) and keep_x is not solution and not hasattr(solution, "__cuda_array_interface__"):
+        np.copyto(solution, keep_x.numpy().reshape(np.shape(solution)))
+    worst = float(np.max(residual)) if residual.size else 0.0
+    if check_every > 0 and not worst <= tol:
+        warnings.warn(
+            f"{name}: conjugate gradient stopped at relative residual {worst:.3g} "
+            f"(tolerance {tol:.3g}) after {int(iters.max())} iterations",
+            UserWarning,
+            stacklevel=2,
+        )
+    del keep_rhs
+    return int(iters.max()), worst, float(tol)
+
+
+def solve_spd_settled(
+    matrix: CsrMatrix,
+    rhs: Any,
+    solution: Any,
+    *,
+    check_rounds: int,
+    change_tolerance: float,
+    settle_rounds: int,
+    maxiter: int | None = None,
+    preconditioner: Preconditioner | None = None,
+    factorization: Any = None,
+    narrow_values: bool = True,
+) -> DeviceArray:
+    """Jacobi CG at zero tolerance until every entry has settled relative to itself.
+
+    ordito/linalg.py:2490: a check every ``check_rounds`` rounds stops once no entry is newly
+    non-zero and none moved by ``change_tolerance`` of itself, or ``settle_rounds`` rounds after the
+    non-zero count last changed, or at ``maxiter``. The settled iterate is then verified by its
+    componentwise backward error (``SETTLE_BACKWARD_ERROR``); where it fails and a
+    ``factorization`` (``OperatorFactorization``) is given or can be built, the system is solved by
+    the sparse Cholesky factorization instead. Returns the ``(1,)`` int32 device array of rounds.
+    """
+    n_columns = _columns(matrix, rhs, solution)
+    if _kind(matrix, preconditioner) != "diag":
+        raise ValueError("solve_spd_settled runs under its own Jacobi preconditioner")
+    rhs_ptr, keep_rhs = device_pointer(rhs, np.float64)
+    x_ptr, keep_x = device_pointer(solution, np.float64)
+    if factorization is not None and getattr(factorization, "factorization", None) is not None:
+        factorization.solve(rhs, solution, tol=SETTLE_DIRECT_TOLERANCE, componentwise=True)
+        return DeviceArray.from_host(np.zeros(1, dtype=np.int32))
+    cap = CG_MAXITER_FACTOR * matrix.nrow if maxiter is None else int(maxiter)
+    solver = _solver(matrix, "diag", narrow_values, n_columns)
+    rounds, status = solver.settle(rhs_ptr, x_ptr, check_rounds, change_tolerance, settle_rounds, cap)
+    flag = DeviceArray.empty(1, np.int32)
+    _lib.call(
+        "ob_backward_error", matrix.nrow, matrix.offsets.ptr, matrix.columns.ptr, matrix.values.ptr,
+        x_ptr, rhs_ptr, n_columns, SETTLE_BACKWARD_ERROR, flag.ptr, DEFAULT_STREAM,
+    )  # fmt: skip
+    verified = int(flag.numpy()[0]) == 0
+    if not verified:
+        fallback = factorization
+        if fallback is None:
+            from ordito_b200.cholesky import OperatorFactorization  # noqa: PLC0415
+
+            fallback = OperatorFactorization(matrix)
+        fallback.iterate_rejected = True
+        if fallback.factor():
+            DeviceArray(x_ptr, (matrix.nrow * n_columns,), np.float64, owned=False).fill_zero()
+            fallback.solve(rhs, solution, tol=SETTLE_DIRECT_TOLERANCE, componentwise=True)
+    del keep_rhs, keep_x
+    return DeviceArray.from_host(np.array([rounds], dtype=np.int32))

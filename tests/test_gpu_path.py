@@ -1,0 +1,153 @@
+"""Parity of the CUDA path with the oracle (GPU): pattern bit-exact, values to 1e-6 relative,
+distances to 1e-5 of their range (relative L-infinity), errors and edge cases."""
+
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from oracle import heat_path as hp
+from ordito_b200 import _lib, creation
+from ordito_b200 import heat as gheat
+from ordito_b200 import laplacian as glap
+from ordito_b200 import linalg as glinalg
+from ordito_b200.mesh import Trimesh
+from tests import meshes
+
+pytestmark = pytest.mark.gpu
+
+VALUE_RTOL = 1e-6  # Laplacian / mass values against the float64 oracle (relative)
+DISTANCE_TOL = 1e-5  # distance: max |d - d_oracle| / max |d_oracle|
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def rel_err(a: np.ndarray, b: np.ndarray) -> float:
+    scale = max(np.max(np.abs(b)), 1e-300)
+    return float(np.max(np.abs(a - b)) / scale)
+
+
+@pytest.mark.parametrize("name", sorted(meshes.ALL))
+def test_pattern_is_bit_exact(gpu, name: str) -> None:
+    v, f = meshes.ALL[name]()
+    n = v.shape[0]
+    ref = hp.mesh_operator_pattern(f, n)
+    got = glap.mesh_operator_pattern(f.reshape(-1), n)
+    nnz = int(ref["offsets"][-1])
+    assert np.array_equal(got.offsets.numpy(), ref["offsets"])
+    assert np.array_equal(got.columns.numpy()[:nnz], ref["columns"])
+    assert np.array_equal(got.run_start.numpy()[:nnz], ref["run_start"])
+    assert np.array_equal(got.keys.numpy(), ref["keys"])
+    order = got.order.numpy()
+    in_face = ref["order"] >= 0
+    assert np.array_equal(order[in_face], ref["order"][in_face])
+
+
+@pytest.mark.parametrize("name", sorted(meshes.ALL))
+def test_face_terms_and_operators(gpu, name: str) -> None:
+    v, f = meshes.ALL[name]()
+    ref = hp.heat_operators(v, f)
+    mesh = Trimesh(v, f.reshape(-1))
+    terms = mesh.face_terms
+    assert np.allclose(terms.cot.numpy(), ref["cot"], rtol=VALUE_RTOL, atol=1e-6 * np.abs(ref["cot"]).max())
+    assert np.allclose(terms.normals.numpy(), ref["normals"], atol=1e-6)
+    assert np.allclose(terms.areas.numpy(), ref["areas"], rtol=VALUE_RTOL)
+    assert np.allclose(terms.area_sums.numpy(), ref["area_sums"], rtol=1e-12)
+    built = glap.assemble_rows(
+        mesh.mesh_operator_pattern, mesh.vertices, terms.cot, terms.area_sums, t=None, face_edges=True
+    )
+    nnz = int(ref["pattern"]["offsets"][-1])
+    scale = np.abs(ref["L"]).max()
+    for key, matrix in (("L", built.laplacian), ("H", built.heat), ("P", built.poisson)):
+        got = matrix.values.numpy()[:nnz]
+        assert np.allclose(got, ref[key], rtol=VALUE_RTOL, atol=VALUE_RTOL * scale), key
+    assert np.allclose(built.mass.numpy(), ref["mass"], rtol=1e-12)
+    total, count = built.edge_sums.numpy()
+    assert total / count == pytest.approx(np.sqrt(ref["t"]), rel=1e-9)
+
+
+def test_golden_ico3_fixture(gpu) -> None:
+    g = np.load(os.path.join(GOLDEN, "oracle_ico3.npz"))
+    d = gheat.heat_geodesic(g["vertices"], g["faces"].reshape(-1), np.array([0], dtype=np.int32))
+    assert rel_err(d.numpy(), g["distance"]) <= DISTANCE_TOL
+
+
+@pytest.mark.parametrize(
+    ("name", "sources"),
+    [("ico3", [0]), ("saddle_graded", [17]), ("bumpy_sphere", [5]), ("small_torus", [0, 400, 900]),
+     ("grid", [3]), ("unreferenced", [1])],
+)
+def test_heat_geodesic_matches_the_oracle(gpu, name: str, sources: list[int]) -> None:
+    v, f = meshes.ALL[name]()
+    ref = hp.heat_geodesic(v, f, np.array(sources))
+    got = gheat.heat_geodesic(v, f.reshape(-1), np.array(sources, dtype=np.int32)).numpy()
+    assert rel_err(got, ref) <= DISTANCE_TOL
+
+
+def test_icosphere5_single_source(gpu) -> None:
+    v, f = creation.icosphere(5)
+    ref = hp.heat_geodesic(v, f, np.array([0]))
+    got = gheat.heat_geodesic(v, f.reshape(-1), np.array([0], dtype=np.int32)).numpy()
+    assert got[0] == 0.0
+    assert rel_err(got, ref) <= DISTANCE_TOL
+
+
+def test_trimesh_reuses_its_solver(gpu) -> None:
+    v, f = meshes.small_torus()
+    mesh = Trimesh(v, f.reshape(-1))
+    for src in ([0], [123], [5, 600]):
+        ref = hp.heat_geodesic(v, f, np.array(src))
+        got = gheat.heat_geodesic(mesh, np.array(src, dtype=np.int32)).numpy()
+        assert rel_err(got, ref) <= DISTANCE_TOL
+    assert len(mesh._solvers) == 1
+
+
+def test_out_of_range_sources_raise(gpu) -> None:
+    v, f = creation.icosphere(1)
+    with pytest.raises(ValueError):
+        gheat.heat_geodesic(v, f.reshape(-1), np.array([0, v.shape[0]], dtype=np.int32))
+    with pytest.raises(ValueError):
+        gheat.heat_geodesic(v, f.reshape(-1), np.array([-1], dtype=np.int32))
+
+
+def test_empty_inputs_return_zero_fields(gpu) -> None:
+    v, f = creation.icosphere(1)
+    out = gheat.heat_geodesic(v, f.reshape(-1), np.zeros(0, dtype=np.int32))
+    assert out.shape == (v.shape[0],) and not out.numpy().any()
+    empty = gheat.heat_geodesic(v, np.zeros(0, dtype=np.int32), np.array([0], dtype=np.int32))
+    assert not empty.numpy().any()
+
+
+def test_solve_spd_recovers_the_constant(gpu) -> None:
+    v, f = creation.icosphere(2)
+    ops = gheat.heat_operators(v, f.reshape(-1))
+    mass = glap.mass_matrix_entries(v, f.reshape(-1), dtype=np.float64)
+    x = glap.DeviceArray.zeros(v.shape[0], np.float64)
+    iters, residual, tol = glinalg.solve_spd(ops.heat_system, mass, x)
+    assert residual <= tol
+    assert np.allclose(x.numpy(), 1.0, atol=1e-6)
+
+
+def test_poisson_solve_matches_a_direct_solve(gpu) -> None:
+    v, f = meshes.bumpy_sphere()
+    ref = hp.heat_operators(v, f)
+    P = hp.csr_matrix(ref["pattern"], ref["P"])
+    rng = np.random.default_rng(0)
+    b = rng.normal(size=v.shape[0])
+    b -= b.mean()
+    direct = hp.PoissonFactor(P).solve(b)
+    ops = gheat.heat_operators(v, f.reshape(-1))
+    x = glap.DeviceArray.zeros(v.shape[0], np.float64)
+    glinalg.solve_spd(ops.poisson_system, b, x, tol=1e-10, preconditioner=ops.poisson_preconditioner)
+    got = x.numpy()
+    got -= got.mean()
+    direct -= direct.mean()
+    assert rel_err(got, direct) <= 1e-6
+
+
+def test_launches_are_counted(gpu) -> None:
+    before = _lib.launch_count()
+    v, f = creation.icosphere(2)
+    gheat.heat_geodesic(v, f.reshape(-1), np.array([0], dtype=np.int32))
+    assert _lib.launch_count() - before >= 10
