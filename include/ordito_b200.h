@@ -170,6 +170,17 @@ int ob_backward_error(int n, const int32_t* offsets, const int32_t* columns, con
  * host layer returns formed on the device). */
 int ob_cast_scale(const void* in, int in_type, void* out, int out_type, long long n, double scale,
                   ob_stream_t stream);
+/* Host-layer utilities (no counterpart in the reference's path; they keep every value the host
+ * layer returns formed on the device): out = a x + b y elementwise (y may alias out); the
+ * transpose of a rows x cols row-major float64 matrix; and the source indicators of n_columns
+ * source sets at once -- column c's sources are sources[source_offsets[c] .. [c + 1]) (device
+ * array), u0 is [V][n_columns] and zeroed first, an index outside [0, V) sets invalid[0] = 1
+ * (replaces kernels/heat.py:614 seed_source_indicator for several columns). */
+int ob_axpby(long long n, double a, const double* x, double b, const double* y, double* out,
+             ob_stream_t stream);
+int ob_transpose(int rows, int cols, const double* in, double* out, ob_stream_t stream);
+int ob_seed_columns(const int32_t* sources, const int32_t* source_offsets, int n_columns,
+                    int n_vertices, double* u0, int32_t* invalid, ob_stream_t stream);
 /* Axis-aligned bounds of float32 points xyz[n, 3]: out[6] = (min xyz, max xyz), as float64 of the
  * float32 extremes. Replaces the mesh bounds the time-step floor reads (ordito/mesh.py:1045,
  * heat.py:5228 _diffusion_floor). */
@@ -177,6 +188,36 @@ int ob_bounds(const float* xyz, int n, double* out, ob_stream_t stream);
 /* y = A x (float64), n_columns columns [n][n_columns]. */
 int ob_spmv(int n, const int32_t* offsets, const int32_t* columns, const double* values,
             const double* x, double* y, int n_columns, ob_stream_t stream);
+
+/* ---- a11: sparse Cholesky ----------------------------------------------------------------
+ * Replaces ordito.cholesky (SparseCholesky :121, sparse_cholesky :538, _analyse :881, _factor
+ * :1399, _Solve :1606) behind linalg.OperatorFactorization (ordito/linalg.py:2191).
+ * ob_chol_analyse: nested-dissection ordering of the pattern (geometric from xyz[n, 3] when not
+ * NULL) and the supernodal structure; host work, reads the pattern back. info[0..4] = n,
+ * supernodes, tree levels, factor entries, widest front.
+ * ob_chol_factor: numeric factorisation of `values` over the analysed pattern; singular != 0 pins
+ * the last vertex of each connected component (the Poisson system). OB_ERR_INDEFINITE on a
+ * non-positive pivot. The factor (partitioned inverse) is uploaded to the device.
+ * ob_chol_solve: x = A^-1 rhs for n_columns interleaved columns ([n][n_columns]), then `refine`
+ * float64 refinement steps x += A^-1 (rhs - A x) with the operator's CSR arrays (may be NULL when
+ * refine == 0); level-scheduled batched dense products on the device, no host read-back. */
+int ob_chol_analyse(int n, const int32_t* offsets, const int32_t* columns, const float* xyz,
+                    void** analysis, ob_stream_t stream);
+int ob_chol_analysis_info(void* analysis, long long* info);
+int ob_chol_analysis_destroy(void* analysis);
+int ob_chol_factor(void* analysis, const double* values, int singular, void** factor,
+                   ob_stream_t stream);
+int ob_chol_nbytes(void* factor, size_t* bytes);
+/* Host check of the same analysis, factorisation and solve algorithm on host arrays (no device;
+ * a test hook, no counterpart in the reference): x = A^-1 rhs for one column; info[0..3] as
+ * ob_chol_analysis_info's first four (may be NULL). */
+int ob_chol_host_solve(int n, const int32_t* offsets, const int32_t* columns,
+                       const double* values, const float* xyz, int singular, const double* rhs,
+                       double* x, long long* info);
+int ob_chol_destroy(void* factor);
+int ob_chol_solve(void* factor, const double* rhs, double* x, int n_columns, int refine,
+                  const int32_t* offsets, const int32_t* columns, const double* values,
+                  ob_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -73,6 +73,17 @@ SIGNATURES: dict[str, list] = {
     "ob_spmv": [I, P, P, P, P, P, I, P],
     "ob_cast_scale": [P, I, P, I, ctypes.c_longlong, D, P],
     "ob_bounds": [P, I, P, P],
+    "ob_axpby": [ctypes.c_longlong, D, P, D, P, P, P],
+    "ob_transpose": [I, I, P, P, P],
+    "ob_seed_columns": [P, P, I, I, P, P, P],
+    "ob_chol_analyse": [I, P, P, P, POINTER(c_void_p), P],
+    "ob_chol_analysis_info": [P, POINTER(ctypes.c_longlong)],
+    "ob_chol_analysis_destroy": [P],
+    "ob_chol_factor": [P, P, I, POINTER(c_void_p), P],
+    "ob_chol_nbytes": [P, POINTER(c_size_t)],
+    "ob_chol_host_solve": [I, P, P, P, P, I, P, P, POINTER(ctypes.c_longlong)],
+    "ob_chol_destroy": [P],
+    "ob_chol_solve": [P, P, P, I, I, P, P, P, P],
 }
 _RESTYPES = {"ob_last_error": c_char_p}
 

@@ -1,47 +1,227 @@
 """Sparse Cholesky of the heat path's systems (``ordito.cholesky`` / ``linalg.OperatorFactorization``).
 
-``OperatorFactorization(matrix, coordinates)`` is the caller-owned slot a ``HeatSolver`` keeps per
-system (ordito/linalg.py:2191): ``factor()`` builds the factorization (False when it cannot:
-over the memory budget, or not positive definite), ``solve(rhs, solution)`` solves by it.
+``sparse_cholesky(matrix, coordinates)`` (ordito/cholesky.py:538) returns a ``SparseCholesky`` whose
+``solve(rhs, solution, *, tol, componentwise, refine)`` (:427) solves by the factor on the device;
+``OperatorFactorization(matrix, coordinates)`` (ordito/linalg.py:2191) is the caller-owned slot a
+``HeatSolver`` keeps per system: ``factor()`` builds the factorization (``False`` when it cannot --
+over ``CHOLESKY_MEMORY_BUDGET``, or not positive definite), ``solve(rhs, solution)`` solves by it.
+
+The ordering is a nested dissection of the operator's graph (geometric, from the vertex positions
+when given) and the supernodes are the dissection tree's nodes; the analysis and the numeric
+factorisation run on the host (``ob_chol_analyse`` / ``ob_chol_factor``), the triangular solves on
+the device, level by level, as batched dense products over all right-hand sides at once
+(``ob_chol_solve``). A singular operator (the Poisson system ``-L``) has one vertex per connected
+component pinned, so its solution is the consistent system's up to a constant per component
+(ordito/cholesky.py:17-20).
 """
 
 from __future__ import annotations
 
+import ctypes
 from typing import Any
 
+import numpy as np
+
+from ordito_b200 import _lib
 from ordito_b200.array import CsrMatrix
+from ordito_b200.device import DEFAULT_STREAM, DeviceArray, device_pointer, element_count
 
 CHOLESKY_MEMORY_BUDGET = 4 << 30  # ordito/cholesky.py:74
+CHOLESKY_REFINE_ROUNDS = 12  # :72
 
 
 class NotPositiveDefiniteError(ValueError):
     """A factorization met a non-positive pivot (ordito/cholesky.py:90)."""
 
 
-class OperatorFactorization:
-    """The factorization slot of one operator."""
+class CholeskyAnalysis:
+    """The ordering and symbolic structure of one pattern, shareable by every operator on it."""
 
     def __init__(self, matrix: CsrMatrix, coordinates: Any = None) -> None:
+        handle = ctypes.c_void_p(0)
+        xyz = 0
+        keep = None
+        if coordinates is not None:
+            xyz, keep = device_pointer(coordinates, np.float32, 3 * matrix.nrow)
+        _lib.call("ob_chol_analyse", matrix.nrow, matrix.offsets.ptr, matrix.columns.ptr, xyz,
+                  ctypes.byref(handle), DEFAULT_STREAM)
+        del keep
+        self.handle = handle
+        info = (ctypes.c_longlong * 5)()
+        _lib.call("ob_chol_analysis_info", handle, info)
+        self.n, self.supernodes, self.levels, self.factor_entries, self.widest_front = map(int, info)
+        self.offsets = matrix.offsets
+        self.columns = matrix.columns
+
+    @property
+    def factor_bytes(self) -> int:
+        return 8 * self.factor_entries
+
+    def close(self) -> None:
+        if self.handle and self.handle.value:
+            _lib.lib.ob_chol_analysis_destroy(self.handle)
+            self.handle = ctypes.c_void_p(0)
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SparseCholesky:
+    """A device-resident factor of one operator (ordito/cholesky.py:121)."""
+
+    def __init__(self, matrix: CsrMatrix, analysis: CholeskyAnalysis, *, singular: bool) -> None:
+        if analysis.n != matrix.nrow:
+            raise ValueError("analysis was built for another operator size")
+        handle = ctypes.c_void_p(0)
+        status = _lib.lib.ob_chol_factor(analysis.handle, matrix.values.ptr, int(singular),
+                                         ctypes.byref(handle), DEFAULT_STREAM)
+        if status == _lib.OB_ERR_INDEFINITE:
+            raise NotPositiveDefiniteError("sparse_cholesky: the operator is not positive definite")
+        _lib.check(status, "ob_chol_factor")
+        self.handle = handle
+        self.matrix = matrix
+        self.analysis = analysis
+        self.singular = singular
+
+    @property
+    def nbytes(self) -> int:
+        size = ctypes.c_size_t(0)
+        _lib.call("ob_chol_nbytes", self.handle, ctypes.byref(size))
+        return int(size.value)
+
+    def solve_pointers(self, rhs: int, x: int, n_columns: int, refine: int, stream: Any = None) -> None:
+        """``x = A^-1 rhs`` for ``n_columns`` interleaved columns ([n][n_columns]) plus ``refine``
+        float64 refinement steps, all enqueued on the device (no read-back)."""
+        m = self.matrix
+        _lib.call("ob_chol_solve", self.handle, rhs, x, int(n_columns), int(refine), m.offsets.ptr,
+                  m.columns.ptr, m.values.ptr, stream if stream is not None else DEFAULT_STREAM)
+
+    def solve(self, rhs: Any, solution: Any, *, tol: float = 1e-12, componentwise: bool = False,
+              refine: bool = True) -> None:
+        """Solve into ``solution``; with ``refine`` iterate ``x += A^-1 (b - A x)`` until the
+        componentwise backward error is within ``tol`` (at most ``CHOLESKY_REFINE_ROUNDS``), or
+        one step when ``componentwise`` is off (ordito/cholesky.py:427)."""
+        n = self.matrix.nrow
+        count = element_count(rhs)
+        if count % n or element_count(solution) != count:
+            raise ValueError("rhs and solution must hold n_columns * n entries of one shape")
+        k = count // n
+        rhs_ptr, keep_rhs = device_pointer(rhs, np.float64)
+        x_ptr, keep_x = device_pointer(solution, np.float64)
+        self.solve_pointers(rhs_ptr, x_ptr, k, 1 if refine else 0)
+        if refine and componentwise and not self.singular:
+            flag = DeviceArray.empty(1, np.int32)
+            m = self.matrix
+            for _ in range(CHOLESKY_REFINE_ROUNDS):
+                _lib.call("ob_backward_error", n, m.offsets.ptr, m.columns.ptr, m.values.ptr,
+                          x_ptr, rhs_ptr, k, float(tol), flag.ptr, DEFAULT_STREAM)
+                if int(flag.numpy()[0]) == 0:
+                    break
+                # One more correction: x += A^-1 (b - A x) (the refinement kernel's own form).
+                self._refine_once(rhs_ptr, x_ptr, k)
+        if isinstance(keep_x, DeviceArray) and not hasattr(solution, "__cuda_array_interface__"):
+            np.copyto(solution, keep_x.numpy().reshape(np.shape(solution)))
+        del keep_rhs
+
+    def _refine_once(self, rhs_ptr: int, x_ptr: int, k: int) -> None:
+        m = self.matrix
+        n = m.nrow
+        residual = DeviceArray.empty(n * k, np.float64)
+        correction = DeviceArray.empty(n * k, np.float64)
+        _lib.call("ob_spmv", n, m.offsets.ptr, m.columns.ptr, m.values.ptr, x_ptr, residual.ptr, k,
+                  DEFAULT_STREAM)
+        _lib.call("ob_axpby", n * k, 1.0, rhs_ptr, -1.0, residual.ptr, residual.ptr, DEFAULT_STREAM)
+        self.solve_pointers(residual.ptr, correction.ptr, k, 0)
+        _lib.call("ob_axpby", n * k, 1.0, x_ptr, 1.0, correction.ptr, x_ptr, DEFAULT_STREAM)
+
+    def close(self) -> None:
+        if self.handle and self.handle.value:
+            _lib.lib.ob_chol_destroy(self.handle)
+            self.handle = ctypes.c_void_p(0)
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def sparse_cholesky(matrix: CsrMatrix, coordinates: Any = None, *, negated: bool | None = False,
+                    singular: bool | None = None) -> SparseCholesky:
+    """Factor ``matrix`` (ordito/cholesky.py:538). ``singular`` None tries the operator as it is
+    and, on a non-positive pivot, again with one vertex per connected component pinned."""
+    if negated:
+        raise NotImplementedError("negated operators are not on the heat-geodesic path")
+    analysis = CholeskyAnalysis(matrix, coordinates)
+    if singular is None:
+        try:
+            return SparseCholesky(matrix, analysis, singular=False)
+        except NotPositiveDefiniteError:
+            return SparseCholesky(matrix, analysis, singular=True)
+    return SparseCholesky(matrix, analysis, singular=singular)
+
+
+class OperatorFactorization:
+    """The factorization slot of one operator (ordito/linalg.py:2191)."""
+
+    def __init__(self, matrix: CsrMatrix, coordinates: Any = None, *, singular: bool | None = None) -> None:
         self.matrix = matrix
         self.coordinates = coordinates
-        self.factorization: Any = None
-        self.refused = True
+        self.singular = singular
+        self.factorization: SparseCholesky | None = None
+        self.analysis: CholeskyAnalysis | None = None
+        self.refused = False
+        self.indefinite = False
         self.iterate_rejected = False
 
-    def factor(self, sharing: "OperatorFactorization | None" = None) -> bool:
-        """Build the factorization; returns whether one is held."""
-        return False
+    def exceeds_budget(self) -> bool:
+        """Whether the factor would exceed ``CHOLESKY_MEMORY_BUDGET`` (asks the analysis)."""
+        if self.analysis is None:
+            self.analysis = CholeskyAnalysis(self.matrix, self.coordinates)
+        return self.analysis.factor_bytes > CHOLESKY_MEMORY_BUDGET
 
-    def solve(self, rhs: Any, solution: Any, *, tol: float = 1e-12,
-              componentwise: bool = False) -> None:
-        raise RuntimeError("OperatorFactorization.solve: no factorization is held")
+    def factor(self, sharing: "OperatorFactorization | None" = None) -> bool:
+        """Build the factorization (reusing ``sharing``'s analysis when it has one)."""
+        if self.factorization is not None:
+            return True
+        if self.refused:
+            return False
+        if self.analysis is None and sharing is not None and sharing.analysis is not None:
+            self.analysis = sharing.analysis
+        if self.exceeds_budget():
+            self.refused = True
+            return False
+        singular = self.singular
+        try:
+            if singular is None:
+                try:
+                    self.factorization = SparseCholesky(self.matrix, self.analysis, singular=False)
+                except NotPositiveDefiniteError:
+                    self.factorization = SparseCholesky(self.matrix, self.analysis, singular=True)
+            else:
+                self.factorization = SparseCholesky(self.matrix, self.analysis, singular=singular)
+        except NotPositiveDefiniteError:
+            self.indefinite = True
+            self.refused = True
+            return False
+        return True
+
+    def solve(self, rhs: Any, solution: Any, *, tol: float = 1e-12, componentwise: bool = False) -> None:
+        if self.factorization is None:
+            raise RuntimeError("OperatorFactorization.solve: no factorization is held")
+        self.factorization.solve(rhs, solution, tol=tol, componentwise=componentwise)
 
     def release(self) -> None:
-        self.factorization = None
+        if self.factorization is not None:
+            self.factorization.close()
+            self.factorization = None
 
     def close(self) -> None:
         self.release()
 
     @property
     def nbytes(self) -> int:
-        return 0
+        return 0 if self.factorization is None else self.factorization.nbytes

@@ -1,0 +1,865 @@
+// a11: sparse Cholesky of the heat path's systems, solved on the GPU.
+//
+// Follows the structure of ordito/cholesky.py (SparseCholesky :121, _analyse :881, _factor :1399,
+// _Solve :1606, _nested_dissection :2227): a nested-dissection ordering (geometric when vertex
+// positions are given), a supernodal factor whose supernodes are the dissection tree's nodes
+// (each leaf domain and each separator one dense front), the diagonal blocks stored as their
+// inverses (a partitioned inverse, so both triangular solves are products), and a singular
+// operator's components pinned at one vertex each (kernels/cholesky.py:196). The analysis and the
+// numeric factorisation run on the host (multifrontal, dense fronts); the solves run on the device,
+// level by level of the tree, as batched dense products over many right-hand sides at once.
+//
+// Device layout of a factor: per supernode s with own columns [c0, c0 + nc) (in the factor's
+// numbering) and m rows R_s (the nc own rows first, then the off-diagonal rows, ascending):
+//   inv[s]  nc x nc row-major, the inverse of the diagonal block L11 (lower triangular);
+//   off[s]  (m - nc) x nc row-major, the off-diagonal panel L21;
+//   rows[s] the m - nc off-diagonal row indices.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <numeric>
+#include <thread>
+#include <vector>
+
+#include "ob_internal.cuh"
+
+namespace ob {
+namespace {
+
+constexpr int kLeafSize = 96;
+
+struct Node {
+    int start = 0, count = 0;          // own columns [start, start + count) in the new numbering
+    int parent = -1;
+    std::vector<int> children;
+    std::vector<int> off_rows;         // ascending, > start + count - 1
+    int level = 0;                     // height from the leaves (leaf = 0)
+};
+
+struct Analysis {
+    int n = 0;
+    std::vector<int> perm;   // new -> old
+    std::vector<int> iperm;  // old -> new
+    std::vector<int> offsets, columns;  // the operator's pattern (old numbering)
+    std::vector<Node> nodes;            // postorder: children before parents
+    std::vector<int> component_last;    // per vertex (old): is it its component's pin (1/0)
+    long long factor_entries = 0;       // sum of nc * nc + (m - nc) * nc
+    int levels = 0;
+};
+
+// ------------------------------------------------------------------------------------------
+// Ordering: recursive coordinate bisection with one-sided vertex separators.
+// ------------------------------------------------------------------------------------------
+
+struct Dissector {
+    const std::vector<int>& off;
+    const std::vector<int>& col;
+    const float* xyz;  // may be null: breadth-first level bisection instead
+    std::vector<int> side;  // scratch marks per vertex
+    std::vector<Node> tree;  // built in postorder
+    std::vector<int> order;  // new -> old, filled in postorder
+
+    Dissector(const std::vector<int>& o, const std::vector<int>& c, const float* p, int n)
+        : off(o), col(c), xyz(p), side(n, 0) {}
+
+    // Splits `verts` into (a, b) halves: by the median of the widest coordinate, or by BFS levels.
+    void bisect(std::vector<int>& verts, std::vector<int>& a, std::vector<int>& b) {
+        const size_t half = verts.size() / 2;
+        if (xyz != nullptr) {
+            float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+            for (int v : verts)
+                for (int d = 0; d < 3; ++d) {
+                    lo[d] = std::min(lo[d], xyz[3 * v + d]);
+                    hi[d] = std::max(hi[d], xyz[3 * v + d]);
+                }
+            int axis = 0;
+            for (int d = 1; d < 3; ++d)
+                if (hi[d] - lo[d] > hi[axis] - lo[axis]) axis = d;
+            auto key = [&](int v) { return std::make_pair(xyz[3 * v + axis], v); };
+            std::nth_element(verts.begin(), verts.begin() + half, verts.end(),
+                             [&](int x, int y) { return key(x) < key(y); });
+        } else {
+            // Breadth-first order from the first vertex; the first half of the visit is `a`.
+            for (int v : verts) side[v] = 1;
+            std::vector<int> queue;
+            queue.reserve(verts.size());
+            std::vector<int> visited;
+            for (int seed : verts) {
+                if (side[seed] != 1) continue;
+                side[seed] = 2;
+                queue.push_back(seed);
+                for (size_t h = visited.size(); h < queue.size(); ++h) {
+                    const int v = queue[h];
+                    for (int e = off[v]; e < off[v + 1]; ++e)
+                        if (side[col[e]] == 1) {
+                            side[col[e]] = 2;
+                            queue.push_back(col[e]);
+                        }
+                }
+                visited = queue;
+            }
+            for (int v : verts) side[v] = 0;
+            verts = queue;
+        }
+        a.assign(verts.begin(), verts.begin() + half);
+        b.assign(verts.begin() + half, verts.end());
+    }
+
+    // Returns the index of the node built for `verts` (postorder append).
+    int dissect(std::vector<int> verts) {
+        if ((int)verts.size() <= kLeafSize) {
+            std::sort(verts.begin(), verts.end());
+            Node leaf;
+            leaf.start = (int)order.size();
+            leaf.count = (int)verts.size();
+            order.insert(order.end(), verts.begin(), verts.end());
+            tree.push_back(leaf);
+            return (int)tree.size() - 1;
+        }
+        std::vector<int> a, b;
+        bisect(verts, a, b);
+        // One-sided separator: the vertices of the smaller-boundary side adjacent to the other.
+        for (int v : b) side[v] = 2;
+        std::vector<int> sep, rest_a;
+        for (int v : a) {
+            bool cut = false;
+            for (int e = off[v]; e < off[v + 1] && !cut; ++e) cut = side[col[e]] == 2;
+            (cut ? sep : rest_a).push_back(v);
+        }
+        for (int v : b) side[v] = 0;
+        std::vector<int> children;
+        if (!rest_a.empty()) children.push_back(dissect(std::move(rest_a)));
+        if (!b.empty()) children.push_back(dissect(std::move(b)));
+        std::sort(sep.begin(), sep.end());
+        Node node;
+        node.start = (int)order.size();
+        node.count = (int)sep.size();
+        node.children = children;
+        order.insert(order.end(), sep.begin(), sep.end());
+        tree.push_back(node);
+        const int id = (int)tree.size() - 1;
+        for (int c : children) tree[c].parent = id;
+        return id;
+    }
+};
+
+int analyse(int n, std::vector<int> offsets, std::vector<int> columns, const float* xyz,
+            Analysis* out) {
+    Analysis& A = *out;
+    A.n = n;
+    A.offsets = std::move(offsets);
+    A.columns = std::move(columns);
+    // Adjacency without the diagonal, for the separators and the components.
+    std::vector<int> adj_off(n + 1, 0), adj;
+    adj.reserve(A.columns.size());
+    for (int i = 0; i < n; ++i) {
+        for (int e = A.offsets[i]; e < A.offsets[i + 1]; ++e)
+            if (A.columns[e] != i) adj.push_back(A.columns[e]);
+        adj_off[i + 1] = (int)adj.size();
+    }
+    Dissector D(adj_off, adj, xyz, n);
+    std::vector<int> all(n);
+    std::iota(all.begin(), all.end(), 0);
+    D.dissect(std::move(all));
+    A.perm = std::move(D.order);
+    A.nodes = std::move(D.tree);
+    A.iperm.assign(n, 0);
+    for (int i = 0; i < n; ++i) A.iperm[A.perm[i]] = i;
+    // Symbolic: each node's off-diagonal rows are its columns' later neighbours plus its
+    // children's off-diagonal rows past its own columns.
+    std::vector<int> mark(n, -1);
+    A.factor_entries = 0;
+    A.levels = 0;
+    for (int s = 0; s < (int)A.nodes.size(); ++s) {
+        Node& node = A.nodes[s];
+        const int end = node.start + node.count;
+        std::vector<int> rows;
+        for (int j = node.start; j < end; ++j) {
+            const int old = A.perm[j];
+            for (int e = adj_off[old]; e < adj_off[old + 1]; ++e) {
+                const int r = A.iperm[adj[e]];
+                if (r >= end && mark[r] != s) {
+                    mark[r] = s;
+                    rows.push_back(r);
+                }
+            }
+        }
+        int level = 0;
+        for (int c : node.children) {
+            level = std::max(level, A.nodes[c].level + 1);
+            for (int r : A.nodes[c].off_rows)
+                if (r >= end && mark[r] != s) {
+                    mark[r] = s;
+                    rows.push_back(r);
+                }
+        }
+        std::sort(rows.begin(), rows.end());
+        node.off_rows = std::move(rows);
+        node.level = level;
+        A.levels = std::max(A.levels, level + 1);
+        A.factor_entries += (long long)node.count * node.count +
+                            (long long)node.off_rows.size() * node.count;
+    }
+    // Components (for pinning a singular operator): the last vertex of each in the new order.
+    A.component_last.assign(n, 0);
+    std::vector<int> comp(n, -1);
+    std::vector<int> queue;
+    for (int seed = 0; seed < n; ++seed) {
+        if (comp[seed] >= 0) continue;
+        comp[seed] = seed;
+        queue.assign(1, seed);
+        int last = seed;
+        for (size_t h = 0; h < queue.size(); ++h) {
+            const int v = queue[h];
+            if (A.iperm[v] > A.iperm[last]) last = v;
+            for (int e = adj_off[v]; e < adj_off[v + 1]; ++e)
+                if (comp[adj[e]] < 0) {
+                    comp[adj[e]] = seed;
+                    queue.push_back(adj[e]);
+                }
+        }
+        A.component_last[last] = 1;
+    }
+    return OB_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Numeric factorisation (host, multifrontal over the dissection tree).
+// ------------------------------------------------------------------------------------------
+
+struct HostFactor {
+    std::vector<std::vector<double>> inv;     // per node: nc x nc row-major inverse of L11
+    std::vector<std::vector<double>> off;     // per node: (m - nc) x nc row-major L21
+    std::vector<std::vector<double>> update;  // per node: (m - nc)^2 column-major, for the parent
+    std::vector<char> pinned;                 // per new index: identity row (pinned / empty)
+};
+
+// Dense partial Cholesky of the m x m column-major front F (lower part used): the first nc
+// columns are factored in place (L11, L21) and F22 becomes the Schur complement.
+bool partial_cholesky(double* F, int m, int nc) {
+    constexpr int kBlock = 48;
+    for (int j0 = 0; j0 < nc; j0 += kBlock) {
+        const int j1 = std::min(nc, j0 + kBlock);
+        // Factor the panel columns [j0, j1) (already updated by earlier panels).
+        for (int j = j0; j < j1; ++j) {
+            double* cj = F + (size_t)j * m;
+            const double d = cj[j];
+            if (!(d > 0.0)) return false;
+            const double r = std::sqrt(d);
+            cj[j] = r;
+            const double inv = 1.0 / r;
+            for (int i = j + 1; i < m; ++i) cj[i] *= inv;
+            for (int k = j + 1; k < j1; ++k) {
+                double* ck = F + (size_t)k * m;
+                const double f = cj[k];
+                if (f != 0.0)
+                    for (int i = k; i < m; ++i) ck[i] -= cj[i] * f;
+            }
+        }
+        // Update every later column with the panel: F[k:, k] -= L[k:, j0:j1] L[k, j0:j1]^T.
+        for (int k = j1; k < m; ++k) {
+            double* ck = F + (size_t)k * m;
+            for (int j = j0; j < j1; ++j) {
+                const double* cj = F + (size_t)j * m;
+                const double f = cj[k];
+                if (f != 0.0)
+                    for (int i = k; i < m; ++i) ck[i] -= cj[i] * f;
+            }
+        }
+    }
+    return true;
+}
+
+int factor_node(const Analysis& A, const double* values, int s, bool singular, HostFactor& H,
+                std::vector<int>& local) {
+    const Node& node = A.nodes[s];
+    const int nc = node.count, noff = (int)node.off_rows.size(), m = nc + noff;
+    const int end = node.start + nc;
+    std::vector<double> F((size_t)m * m, 0.0);
+    for (int j = 0; j < nc; ++j) local[node.start + j] = j;
+    for (int r = 0; r < noff; ++r) local[node.off_rows[r]] = nc + r;
+    // Assemble the operator's entries of the own columns (lower part, rows in R_s).
+    for (int j = node.start; j < end; ++j) {
+        const int old = A.perm[j];
+        const bool pin = H.pinned[j];
+        const int lj = j - node.start;
+        if (pin) {
+            F[(size_t)lj * m + lj] = 1.0;
+            continue;
+        }
+        for (int e = A.offsets[old]; e < A.offsets[old + 1]; ++e) {
+            const int r = A.iperm[A.columns[e]];
+            if (r < j || H.pinned[r]) continue;
+            F[(size_t)lj * m + local[r]] += values[e];
+        }
+    }
+    // Extend-add the children's update matrices.
+    for (int c : node.children) {
+        const Node& ch = A.nodes[c];
+        const int cm = (int)ch.off_rows.size();
+        const std::vector<double>& U = H.update[c];
+        for (int b = 0; b < cm; ++b) {
+            const int lb = local[ch.off_rows[b]];
+            for (int a = b; a < cm; ++a) {
+                const int la = local[ch.off_rows[a]];
+                const int row = std::max(la, lb), colm = std::min(la, lb);
+                F[(size_t)colm * m + row] += U[(size_t)b * cm + a];
+            }
+        }
+        H.update[c].clear();
+        H.update[c].shrink_to_fit();
+    }
+    if (!partial_cholesky(F.data(), m, nc)) return OB_ERR_INDEFINITE;
+    // Inverse of L11 (lower triangular), row-major: solve L X = I column by column.
+    std::vector<double> inv((size_t)nc * nc, 0.0);
+    for (int c = 0; c < nc; ++c) {
+        // Column c of X: x_i = (delta_ic - sum_{k<i} L_ik x_k) / L_ii, for i >= c.
+        for (int i = c; i < nc; ++i) {
+            double acc = (i == c) ? 1.0 : 0.0;
+            for (int k = c; k < i; ++k) acc -= F[(size_t)k * m + i] * inv[(size_t)k * nc + c];
+            inv[(size_t)i * nc + c] = acc / F[(size_t)i * m + i];
+        }
+    }
+    H.inv[s] = std::move(inv);
+    std::vector<double> L21((size_t)noff * nc);
+    for (int r = 0; r < noff; ++r)
+        for (int j = 0; j < nc; ++j) L21[(size_t)r * nc + j] = F[(size_t)j * m + nc + r];
+    H.off[s] = std::move(L21);
+    std::vector<double> U((size_t)noff * noff);
+    for (int b = 0; b < noff; ++b)
+        for (int a = b; a < noff; ++a) U[(size_t)b * noff + a] = F[(size_t)(nc + b) * m + nc + a];
+    H.update[s] = std::move(U);
+    (void)singular;
+    return OB_OK;
+}
+
+int numeric(const Analysis& A, const double* values, bool singular, HostFactor* out) {
+    HostFactor& H = *out;
+    const int ns = (int)A.nodes.size();
+    H.inv.assign(ns, {});
+    H.off.assign(ns, {});
+    H.update.assign(ns, {});
+    H.pinned.assign(A.n, 0);
+    for (int i = 0; i < A.n; ++i) {
+        const int old = A.perm[i];
+        bool empty = true;
+        for (int e = A.offsets[old]; e < A.offsets[old + 1]; ++e)
+            if (A.columns[e] == old && values[e] != 0.0) empty = false;
+        if (empty || (singular && A.component_last[old])) H.pinned[i] = 1;
+    }
+    // Subtrees below a cut level are factored in parallel, the rest in postorder.
+    const unsigned threads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    int cut = A.levels - 1;
+    while (cut > 0) {
+        int count = 0;
+        for (const Node& nd : A.nodes)
+            if (nd.level == cut - 1 && (nd.parent < 0 || A.nodes[nd.parent].level >= cut)) ++count;
+        if (count >= (int)threads * 2) break;
+        --cut;
+    }
+    // Roots of the parallel subtrees: nodes below `cut` whose parent is at or above it.
+    std::vector<int> roots;
+    for (int s = 0; s < ns; ++s)
+        if (A.nodes[s].level < cut && (A.nodes[s].parent < 0 || A.nodes[A.nodes[s].parent].level >= cut))
+            roots.push_back(s);
+    std::vector<int> status(roots.size(), OB_OK);
+    std::atomic<size_t> next{0};
+    auto worker = [&]() {
+        std::vector<int> local(A.n, -1);
+        for (;;) {
+            const size_t i = next.fetch_add(1);
+            if (i >= roots.size()) break;
+            // Postorder of the subtree rooted at roots[i]: its nodes are a contiguous index range
+            // ending at the root (the tree was appended in postorder).
+            const int root = roots[i];
+            int first = root;
+            std::function<void(int)> lowest = [&](int v) {
+                first = std::min(first, v);
+                for (int c : A.nodes[v].children) lowest(c);
+            };
+            lowest(root);
+            for (int s = first; s <= root && status[i] == OB_OK; ++s)
+                status[i] = factor_node(A, values, s, singular, H, local);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (unsigned t = 0; t < threads; ++t) pool.emplace_back(worker);
+    for (auto& th : pool) th.join();
+    for (int st : status)
+        if (st) return st;
+    std::vector<int> local(A.n, -1);
+    for (int s = 0; s < ns; ++s) {
+        if (A.nodes[s].level < cut) continue;
+        int st = factor_node(A, values, s, singular, H, local);
+        if (st) return st;
+    }
+    return OB_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Device factor and the level-scheduled solve.
+// ------------------------------------------------------------------------------------------
+
+// One output tile of a batched dense product: out rows [r0, r0 + rows) of a block whose matrix
+// is M (row-major, leading dimension ld, or its transpose when trans), times the K input rows.
+struct Tile {
+    long long m;       // offset of the matrix in the value buffer
+    int ld, trans;     // leading dimension; 1 when the matrix is read transposed
+    int r0, rows, K;   // output rows of the tile and the inner dimension
+    int in_base;       // input row index: in_rows == -1 -> in_base + kk, else idx[in_rows + kk]
+    int in_rows;
+    int out_base;      // output row index: out_rows == -1 -> out_base + i, else idx[out_rows + i]
+    int out_rows;
+};
+
+constexpr int kTileRows = 32;
+constexpr int kTileCols = 32;
+constexpr int kTileK = 32;
+
+// mode 0: out = M in; mode 1: out -= M in (atomic, scattered rows); mode 2: out -= M in (plain).
+template <int MODE>
+__global__ void tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
+                                    const int* __restrict__ idx, const double* __restrict__ in,
+                                    double* __restrict__ out, int k) {
+    __shared__ double sm[kTileRows][kTileK + 1];
+    __shared__ double sx[kTileK][kTileCols + 1];
+    const Tile t = tiles[blockIdx.x];
+    const int c0 = blockIdx.y * kTileCols;
+    const int tx = threadIdx.x % kTileCols;  // column within the tile
+    const int ty = threadIdx.x / kTileCols;  // 8 row groups
+    double acc[kTileRows / 8];
+#pragma unroll
+    for (int q = 0; q < kTileRows / 8; ++q) acc[q] = 0.0;
+    const double* M = vals + t.m;
+    for (int k0 = 0; k0 < t.K; k0 += kTileK) {
+        for (int e = threadIdx.x; e < kTileRows * kTileK; e += blockDim.x) {
+            const int i = e / kTileK, kk = e % kTileK;
+            const int row = t.r0 + i, col = k0 + kk;
+            double v = 0.0;
+            if (i < t.rows && col < t.K)
+                v = t.trans ? M[(size_t)col * t.ld + row] : M[(size_t)row * t.ld + col];
+            sm[i][kk] = v;
+        }
+        for (int e = threadIdx.x; e < kTileK * kTileCols; e += blockDim.x) {
+            const int kk = e / kTileCols, c = e % kTileCols;
+            const int col = k0 + kk;
+            double v = 0.0;
+            if (col < t.K && c0 + c < k) {
+                const int r = t.in_rows < 0 ? t.in_base + col : idx[t.in_rows + col];
+                v = in[(size_t)r * k + c0 + c];
+            }
+            sx[kk][c] = v;
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < kTileK; ++kk) {
+            const double x = sx[kk][tx];
+#pragma unroll
+            for (int q = 0; q < kTileRows / 8; ++q) acc[q] = fma(sm[ty + 8 * q][kk], x, acc[q]);
+        }
+        __syncthreads();
+    }
+    if (c0 + tx >= k) return;
+#pragma unroll
+    for (int q = 0; q < kTileRows / 8; ++q) {
+        const int i = ty + 8 * q;
+        if (i >= t.rows) continue;
+        const int r = t.out_rows < 0 ? t.out_base + t.r0 + i : idx[t.out_rows + t.r0 + i];
+        double* o = out + (size_t)r * k + c0 + tx;
+        if (MODE == 0)
+            *o = acc[q];
+        else if (MODE == 1)
+            atomicAdd(o, -acc[q]);
+        else
+            *o -= acc[q];
+    }
+}
+
+// Gathers rows of x (old numbering) into the factor's numbering, zeroing pinned rows; or
+// scatters back.
+__global__ void permute_in_kernel(int n, int k, const int* __restrict__ perm,
+                                  const char* __restrict__ pinned, const double* __restrict__ src,
+                                  double* __restrict__ dst) {
+    const long long total = (long long)n * k;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / k), c = (int)(t % k);
+        dst[t] = pinned[i] ? 0.0 : src[(size_t)perm[i] * k + c];
+    }
+}
+
+__global__ void permute_out_kernel(int n, int k, const int* __restrict__ perm,
+                                   const double* __restrict__ src, double* __restrict__ dst,
+                                   int accumulate) {
+    const long long total = (long long)n * k;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / k), c = (int)(t % k);
+        double* d = dst + (size_t)perm[i] * k + c;
+        *d = accumulate ? *d + src[t] : src[t];
+    }
+}
+
+// r = b - A x over n_columns interleaved columns (float64).
+__global__ void residual_kernel(int n, int k, const int* __restrict__ offsets,
+                                const int* __restrict__ columns, const double* __restrict__ values,
+                                const double* __restrict__ b, const double* __restrict__ x,
+                                double* __restrict__ r) {
+    const long long total = (long long)n * k;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int row = (int)(t / k), c = (int)(t % k);
+        double acc = 0.0;
+        for (int j = offsets[row]; j < offsets[row + 1]; ++j)
+            acc = fma(values[j], x[(size_t)columns[j] * k + c], acc);
+        r[t] = b[t] - acc;
+    }
+}
+
+struct Factor {
+    const Analysis* analysis = nullptr;
+    int n = 0;
+    bool singular = false;
+    double* vals = nullptr;  // device: all inverses and panels
+    int* idx = nullptr;      // device: off-diagonal row lists
+    int* perm = nullptr;     // device: new -> old
+    char* pinned = nullptr;  // device
+    long long n_vals = 0;
+    // Tile lists per (direction, level, phase); host copies of counts, device tile arrays.
+    std::vector<Tile*> fwd_diag, fwd_off, bwd_off, bwd_diag;
+    std::vector<int> n_fwd_diag, n_fwd_off, n_bwd_off, n_bwd_diag;
+    std::vector<void*> owned;
+    // Work buffers sized for `cap_k` columns.
+    int cap_k = 0;
+    double *B = nullptr, *Y = nullptr, *X = nullptr, *R = nullptr, *D = nullptr;
+    size_t bytes = 0;
+};
+
+int dev_alloc(Factor* F, void** p, size_t bytes, cudaStream_t stream) {
+    OB_CUDA(cudaMallocAsync(p, std::max<size_t>(bytes, 8), stream));
+    F->owned.push_back(*p);
+    F->bytes += bytes;
+    return OB_OK;
+}
+
+void factor_release(Factor* F) {
+    if (F == nullptr) return;
+    cudaDeviceSynchronize();
+    for (void* p : F->owned) cudaFree(p);
+    delete F;
+}
+
+int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
+    const Analysis& A = *F->analysis;
+    const int ns = (int)A.nodes.size();
+    std::vector<long long> inv_at(ns), off_at(ns);
+    std::vector<int> rows_at(ns);
+    long long total = 0;
+    int total_rows = 0;
+    for (int s = 0; s < ns; ++s) {
+        inv_at[s] = total;
+        total += (long long)H.inv[s].size();
+        off_at[s] = total;
+        total += (long long)H.off[s].size();
+        rows_at[s] = total_rows;
+        total_rows += (int)A.nodes[s].off_rows.size();
+    }
+    std::vector<double> vals(std::max<long long>(total, 1));
+    std::vector<int> idx(std::max(total_rows, 1));
+    for (int s = 0; s < ns; ++s) {
+        std::copy(H.inv[s].begin(), H.inv[s].end(), vals.begin() + inv_at[s]);
+        std::copy(H.off[s].begin(), H.off[s].end(), vals.begin() + off_at[s]);
+        std::copy(A.nodes[s].off_rows.begin(), A.nodes[s].off_rows.end(), idx.begin() + rows_at[s]);
+    }
+    F->n_vals = total;
+    int st = dev_alloc(F, (void**)&F->vals, sizeof(double) * vals.size(), stream);
+    if (!st) st = dev_alloc(F, (void**)&F->idx, sizeof(int) * idx.size(), stream);
+    if (!st) st = dev_alloc(F, (void**)&F->perm, sizeof(int) * A.n, stream);
+    if (!st) st = dev_alloc(F, (void**)&F->pinned, std::max(A.n, 1), stream);
+    if (st) return st;
+    OB_CUDA(cudaMemcpyAsync(F->vals, vals.data(), sizeof(double) * vals.size(),
+                            cudaMemcpyHostToDevice, stream));
+    OB_CUDA(cudaMemcpyAsync(F->idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice,
+                            stream));
+    OB_CUDA(cudaMemcpyAsync(F->perm, A.perm.data(), sizeof(int) * A.n, cudaMemcpyHostToDevice,
+                            stream));
+    OB_CUDA(cudaMemcpyAsync(F->pinned, H.pinned.data(), A.n, cudaMemcpyHostToDevice, stream));
+    // Tiles per level and phase.
+    const int L = A.levels;
+    std::vector<std::vector<Tile>> fd(L), fo(L), bo(L), bd(L);
+    for (int s = 0; s < ns; ++s) {
+        const Node& nd = A.nodes[s];
+        const int nc = nd.count, noff = (int)nd.off_rows.size();
+        if (nc == 0) continue;
+        for (int r0 = 0; r0 < nc; r0 += kTileRows) {
+            const int rows = std::min(kTileRows, nc - r0);
+            // Forward diagonal: Y[own] = inv B[own].
+            fd[nd.level].push_back(Tile{inv_at[s], nc, 0, r0, rows, nc, nd.start, -1, nd.start, -1});
+            // Backward diagonal: X[own] = inv^T Z[own].
+            bd[nd.level].push_back(Tile{inv_at[s], nc, 1, r0, rows, nc, nd.start, -1, nd.start, -1});
+            // Backward off-diagonal: Z[own] -= L21^T X[off rows].
+            if (noff > 0)
+                bo[nd.level].push_back(
+                    Tile{off_at[s], nc, 1, r0, rows, noff, 0, rows_at[s], nd.start, -1});
+        }
+        for (int r0 = 0; r0 < noff; r0 += kTileRows) {
+            const int rows = std::min(kTileRows, noff - r0);
+            // Forward off-diagonal: B[off rows] -= L21 Y[own].
+            fo[nd.level].push_back(Tile{off_at[s], nc, 0, r0, rows, nc, nd.start, -1, 0, rows_at[s]});
+        }
+    }
+    auto push = [&](std::vector<std::vector<Tile>>& lists, std::vector<Tile*>& dst,
+                    std::vector<int>& counts) -> int {
+        dst.assign(L, nullptr);
+        counts.assign(L, 0);
+        for (int l = 0; l < L; ++l) {
+            counts[l] = (int)lists[l].size();
+            if (lists[l].empty()) continue;
+            int st2 = dev_alloc(F, (void**)&dst[l], sizeof(Tile) * lists[l].size(), stream);
+            if (st2) return st2;
+            OB_CUDA(cudaMemcpyAsync(dst[l], lists[l].data(), sizeof(Tile) * lists[l].size(),
+                                    cudaMemcpyHostToDevice, stream));
+        }
+        return OB_OK;
+    };
+    st = push(fd, F->fwd_diag, F->n_fwd_diag);
+    if (!st) st = push(fo, F->fwd_off, F->n_fwd_off);
+    if (!st) st = push(bo, F->bwd_off, F->n_bwd_off);
+    if (!st) st = push(bd, F->bwd_diag, F->n_bwd_diag);
+    if (st) return st;
+    OB_CUDA(cudaStreamSynchronize(stream));  // host staging buffers go out of scope
+    return OB_OK;
+}
+
+int ensure_work(Factor* F, int k, cudaStream_t stream) {
+    if (k <= F->cap_k) return OB_OK;
+    const size_t vec = sizeof(double) * (size_t)F->n * k;
+    for (double** p : {&F->B, &F->Y, &F->X, &F->R, &F->D}) {
+        int st = dev_alloc(F, (void**)p, vec, stream);
+        if (st) return st;
+    }
+    F->cap_k = k;
+    return OB_OK;
+}
+
+// x_new = A^-1 b_new in the factor's numbering (B is consumed).
+int triangular_solves(Factor* F, int k, cudaStream_t stream) {
+    const int L = F->analysis->levels;
+    const dim3 threads(256);
+    const int ct = (k + kTileCols - 1) / kTileCols;
+    for (int l = 0; l < L; ++l) {
+        if (F->n_fwd_diag[l]) {
+            tile_product_kernel<0><<<dim3(F->n_fwd_diag[l], ct), threads, 0, stream>>>(
+                F->fwd_diag[l], F->vals, F->idx, F->B, F->Y, k);
+            OB_CHECK_LAUNCH("chol forward diagonal");
+        }
+        if (F->n_fwd_off[l]) {
+            tile_product_kernel<1><<<dim3(F->n_fwd_off[l], ct), threads, 0, stream>>>(
+                F->fwd_off[l], F->vals, F->idx, F->Y, F->B, k);
+            OB_CHECK_LAUNCH("chol forward update");
+        }
+    }
+    for (int l = L - 1; l >= 0; --l) {
+        if (F->n_bwd_off[l]) {
+            tile_product_kernel<2><<<dim3(F->n_bwd_off[l], ct), threads, 0, stream>>>(
+                F->bwd_off[l], F->vals, F->idx, F->X, F->Y, k);
+            OB_CHECK_LAUNCH("chol backward gather");
+        }
+        if (F->n_bwd_diag[l]) {
+            tile_product_kernel<0><<<dim3(F->n_bwd_diag[l], ct), threads, 0, stream>>>(
+                F->bwd_diag[l], F->vals, F->idx, F->Y, F->X, k);
+            OB_CHECK_LAUNCH("chol backward diagonal");
+        }
+    }
+    return OB_OK;
+}
+
+int grid_for(long long total) {
+    return (int)std::max(1LL, std::min((total + 255) / 256, (long long)8 * sm_count()));
+}
+
+}  // namespace
+}  // namespace ob
+
+using namespace ob;
+
+extern "C" {
+
+int ob_chol_analyse(int n, const int32_t* offsets, const int32_t* columns, const float* xyz,
+                    void** analysis, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(analysis != nullptr, "ob_chol_analyse: null output");
+    *analysis = nullptr;
+    OB_REQUIRE(n >= 1 && offsets && columns, "ob_chol_analyse: bad argument");
+    std::vector<int> off(n + 1);
+    OB_CUDA(cudaMemcpyAsync(off.data(), offsets, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost,
+                            stream));
+    OB_CUDA(cudaStreamSynchronize(stream));
+    std::vector<int> col(std::max(off[n], 1));
+    std::vector<float> pts;
+    OB_CUDA(cudaMemcpyAsync(col.data(), columns, sizeof(int) * off[n], cudaMemcpyDeviceToHost,
+                            stream));
+    if (xyz != nullptr) {
+        pts.resize(3 * (size_t)n);
+        OB_CUDA(cudaMemcpyAsync(pts.data(), xyz, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost,
+                                stream));
+    }
+    OB_CUDA(cudaStreamSynchronize(stream));
+    col.resize(off[n]);
+    Analysis* A = new Analysis();
+    int st = analyse(n, std::move(off), std::move(col), xyz ? pts.data() : nullptr, A);
+    if (st) {
+        delete A;
+        return st;
+    }
+    *analysis = A;
+    return OB_OK;
+}
+
+int ob_chol_analysis_info(void* analysis, long long* info) {
+    OB_REQUIRE(analysis && info, "ob_chol_analysis_info: bad argument");
+    const Analysis* A = static_cast<Analysis*>(analysis);
+    info[0] = A->n;
+    info[1] = (long long)A->nodes.size();
+    info[2] = A->levels;
+    info[3] = A->factor_entries;
+    long long widest = 0;
+    for (const Node& nd : A->nodes) widest = std::max<long long>(widest, nd.count + nd.off_rows.size());
+    info[4] = widest;
+    return OB_OK;
+}
+
+int ob_chol_analysis_destroy(void* analysis) {
+    delete static_cast<Analysis*>(analysis);
+    return OB_OK;
+}
+
+int ob_chol_factor(void* analysis, const double* values, int singular, void** factor,
+                   ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(analysis && values && factor, "ob_chol_factor: bad argument");
+    *factor = nullptr;
+    const Analysis* A = static_cast<Analysis*>(analysis);
+    std::vector<double> host(std::max(A->offsets[A->n], 1));
+    OB_CUDA(cudaMemcpyAsync(host.data(), values, sizeof(double) * A->offsets[A->n],
+                            cudaMemcpyDeviceToHost, stream));
+    OB_CUDA(cudaStreamSynchronize(stream));
+    HostFactor H;
+    int st = numeric(*A, host.data(), singular != 0, &H);
+    if (st == OB_ERR_INDEFINITE) return fail(OB_ERR_INDEFINITE, "ob_chol_factor: not positive definite");
+    if (st) return st;
+    Factor* F = new Factor();
+    F->analysis = A;
+    F->n = A->n;
+    F->singular = singular != 0;
+    st = upload_factor(F, H, stream);
+    if (st) {
+        factor_release(F);
+        return st;
+    }
+    *factor = F;
+    return OB_OK;
+}
+
+int ob_chol_host_solve(int n, const int32_t* offsets, const int32_t* columns,
+                       const double* values, const float* xyz, int singular, const double* rhs,
+                       double* x, long long* info) {
+    OB_REQUIRE(n >= 1 && offsets && columns && values && rhs && x, "ob_chol_host_solve: bad argument");
+    std::vector<int> off(offsets, offsets + n + 1), col(columns, columns + offsets[n]);
+    Analysis A;
+    int st = analyse(n, std::move(off), std::move(col), xyz, &A);
+    if (st) return st;
+    HostFactor H;
+    st = numeric(A, values, singular != 0, &H);
+    if (st == OB_ERR_INDEFINITE) return fail(OB_ERR_INDEFINITE, "ob_chol_host_solve: not positive definite");
+    if (st) return st;
+    if (info) {
+        info[0] = A.n;
+        info[1] = (long long)A.nodes.size();
+        info[2] = A.levels;
+        info[3] = A.factor_entries;
+    }
+    // The device algorithm, run on the host: forward by levels' postorder, backward reversed.
+    std::vector<double> b(n), y(n, 0.0), xs(n, 0.0);
+    for (int i = 0; i < n; ++i) b[i] = H.pinned[i] ? 0.0 : rhs[A.perm[i]];
+    for (int s = 0; s < (int)A.nodes.size(); ++s) {
+        const Node& nd = A.nodes[s];
+        const int nc = nd.count, noff = (int)nd.off_rows.size();
+        for (int i = 0; i < nc; ++i) {
+            double acc = 0.0;
+            for (int j = 0; j < nc; ++j) acc += H.inv[s][(size_t)i * nc + j] * b[nd.start + j];
+            y[nd.start + i] = acc;
+        }
+        for (int r = 0; r < noff; ++r) {
+            double acc = 0.0;
+            for (int j = 0; j < nc; ++j) acc += H.off[s][(size_t)r * nc + j] * y[nd.start + j];
+            b[nd.off_rows[r]] -= acc;
+        }
+    }
+    for (int s = (int)A.nodes.size() - 1; s >= 0; --s) {
+        const Node& nd = A.nodes[s];
+        const int nc = nd.count, noff = (int)nd.off_rows.size();
+        std::vector<double> z(nc);
+        for (int j = 0; j < nc; ++j) {
+            double acc = y[nd.start + j];
+            for (int r = 0; r < noff; ++r) acc -= H.off[s][(size_t)r * nc + j] * xs[nd.off_rows[r]];
+            z[j] = acc;
+        }
+        for (int i = 0; i < nc; ++i) {
+            double acc = 0.0;
+            for (int j = 0; j < nc; ++j) acc += H.inv[s][(size_t)j * nc + i] * z[j];
+            xs[nd.start + i] = acc;
+        }
+    }
+    for (int i = 0; i < n; ++i) x[A.perm[i]] = xs[i];
+    return OB_OK;
+}
+
+int ob_chol_nbytes(void* factor, size_t* bytes) {
+    OB_REQUIRE(factor && bytes, "ob_chol_nbytes: bad argument");
+    *bytes = static_cast<Factor*>(factor)->bytes;
+    return OB_OK;
+}
+
+int ob_chol_destroy(void* factor) {
+    factor_release(static_cast<Factor*>(factor));
+    return OB_OK;
+}
+
+int ob_chol_solve(void* factor, const double* rhs, double* x, int n_columns, int refine,
+                  const int32_t* offsets, const int32_t* columns, const double* values,
+                  ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(factor && rhs && x && n_columns >= 1, "ob_chol_solve: bad argument");
+    OB_REQUIRE(refine == 0 || (offsets && columns && values),
+               "ob_chol_solve: refinement needs the operator");
+    Factor* F = static_cast<Factor*>(factor);
+    int st = ensure_work(F, n_columns, stream);
+    if (st) return st;
+    const int n = F->n, k = n_columns;
+    const long long total = (long long)n * k;
+    const int grid = grid_for(total);
+    // x = A^-1 b.
+    permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->pinned, rhs, F->B);
+    OB_CHECK_LAUNCH("chol permute in");
+    st = triangular_solves(F, k, stream);
+    if (st) return st;
+    permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->X, x, 0);
+    OB_CHECK_LAUNCH("chol permute out");
+    // Iterative refinement in float64: x += A^-1 (b - A x).
+    for (int it = 0; it < refine; ++it) {
+        residual_kernel<<<grid, 256, 0, stream>>>(n, k, offsets, columns, values, rhs, x, F->R);
+        OB_CHECK_LAUNCH("chol residual");
+        permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->pinned, F->R, F->B);
+        OB_CHECK_LAUNCH("chol permute in");
+        st = triangular_solves(F, k, stream);
+        if (st) return st;
+        permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->X, x, 1);
+        OB_CHECK_LAUNCH("chol permute out");
+    }
+    return OB_OK;
+}
+
+}  // extern "C"

@@ -13,6 +13,46 @@ __global__ void cast_scale_kernel(long long n, const S* __restrict__ in, T* __re
         out[i] = (T)((double)in[i] * scale);
 }
 
+__global__ void axpby_kernel(long long n, double a, const double* __restrict__ x, double b,
+                             const double* y, double* out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = a * x[i] + b * y[i];
+}
+
+// out[c][r] = in[r][c] for a rows x cols row-major float64 matrix.
+__global__ void transpose_kernel(int rows, int cols, const double* __restrict__ in,
+                                 double* __restrict__ out) {
+    __shared__ double tile[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int r = r0 + i, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) tile[i][threadIdx.x] = in[(size_t)r * cols + c];
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int c = c0 + i, r = r0 + threadIdx.x;
+        if (r < rows && c < cols) out[(size_t)c * rows + r] = tile[threadIdx.x][i];
+    }
+}
+
+// Source indicators of several columns: u0[v][c] = 1 for v in column c's sources.
+__global__ void seed_columns_kernel(const int* __restrict__ sources,
+                                    const int* __restrict__ source_offsets, int n_columns, int n,
+                                    double* __restrict__ u0, int* __restrict__ invalid) {
+    const int c = blockIdx.y;
+    const int begin = source_offsets[c], end = source_offsets[c + 1];
+    for (int i = begin + blockIdx.x * blockDim.x + threadIdx.x; i < end;
+         i += gridDim.x * blockDim.x) {
+        const int v = sources[i];
+        if (v < 0 || v >= n) {
+            invalid[0] = 1;
+            continue;
+        }
+        u0[(size_t)v * n_columns + c] = 1.0;
+    }
+}
+
 // Axis-aligned bounds of float32 points: out = (min x, min y, min z, max x, max y, max z).
 __global__ void bounds_kernel(const float* __restrict__ xyz, int n, float* __restrict__ partials,
                               unsigned int* counter, double* __restrict__ out) {
@@ -52,6 +92,42 @@ __global__ void bounds_kernel(const float* __restrict__ xyz, int n, float* __res
 using namespace ob;
 
 extern "C" {
+
+int ob_axpby(long long n, double a, const double* x, double b, const double* y, double* out,
+             ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    if (n <= 0) return OB_OK;
+    OB_REQUIRE(x && y && out, "ob_axpby: null pointer");
+    const int blocks = (int)std::min((n + 255) / 256, (long long)8 * sm_count());
+    axpby_kernel<<<blocks, 256, 0, stream>>>(n, a, x, b, y, out);
+    OB_CHECK_LAUNCH("axpby");
+    return OB_OK;
+}
+
+int ob_transpose(int rows, int cols, const double* in, double* out, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    if (rows <= 0 || cols <= 0) return OB_OK;
+    OB_REQUIRE(in && out && in != out, "ob_transpose: bad argument");
+    transpose_kernel<<<dim3(ceil_div(cols, 32), ceil_div(rows, 32)), dim3(32, 8), 0, stream>>>(
+        rows, cols, in, out);
+    OB_CHECK_LAUNCH("transpose");
+    return OB_OK;
+}
+
+int ob_seed_columns(const int32_t* sources, const int32_t* source_offsets, int n_columns,
+                    int n_vertices, double* u0, int32_t* invalid, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_columns >= 1 && n_vertices >= 0 && invalid && source_offsets,
+               "ob_seed_columns: bad argument");
+    OB_CUDA(cudaMemsetAsync(invalid, 0, sizeof(int32_t), stream));
+    if (n_vertices == 0) return OB_OK;
+    OB_REQUIRE(u0 && sources, "ob_seed_columns: null pointer");
+    OB_CUDA(cudaMemsetAsync(u0, 0, sizeof(double) * (size_t)n_vertices * n_columns, stream));
+    seed_columns_kernel<<<dim3(1, n_columns), 128, 0, stream>>>(sources, source_offsets, n_columns,
+                                                              n_vertices, u0, invalid);
+    OB_CHECK_LAUNCH("seed_columns");
+    return OB_OK;
+}
 
 int ob_bounds(const float* xyz, int n, double* out, ob_stream_t stream_) {
     cudaStream_t stream = as_stream(stream_);

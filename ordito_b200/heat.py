@@ -203,7 +203,9 @@ class HeatSolver:
         if kept is None:
             matrix = self.operators.heat_system if role == "heat" else self.operators.poisson_system
             kept = self._systems[role] = {
-                "factorization": OperatorFactorization(matrix, self._mesh.vertices),
+                "factorization": OperatorFactorization(
+                    matrix, self._mesh.vertices, singular=role == "poisson"
+                ),
                 "solves": 0,
             }
         return kept
@@ -231,6 +233,16 @@ class HeatSolver:
             if kept["factorization"].factorization is None:
                 ok = kept["factorization"].factor(self._sharing(role)) and ok
         return ok
+
+    @property
+    def heat_factor(self):
+        """The heat system's held ``SparseCholesky`` (``None`` before ``factor``)."""
+        return self._system("heat")["factorization"].factorization
+
+    @property
+    def poisson_factor(self):
+        """The Poisson system's held ``SparseCholesky`` (``None`` before ``factor``)."""
+        return self._system("poisson")["factorization"].factorization
 
     def diffuse(self, rhs: Any, solution: Any) -> None:
         """Solve the heat system ``(M - t L) u = rhs`` to settled entries, in place."""
@@ -305,6 +317,73 @@ def _distance_from_heat(mesh: Trimesh, solver: HeatSolver, sources: DeviceArray,
         source_offsets.ptr if source_offsets is not None else None, n_columns, 1, DEFAULT_STREAM,
     )  # fmt: skip
     return phi
+
+
+def _source_columns(source_sets: Any, n: int) -> tuple[DeviceArray, DeviceArray, int]:
+    """Concatenated int32 sources and their column offsets (device), from a list of sets."""
+    sets = [np.asarray(s, dtype=np.int64).reshape(-1) for s in source_sets]
+    if not sets:
+        raise ValueError("heat_geodesic_batch: no source sets")
+    if any(s.size == 0 for s in sets):
+        raise ValueError("heat_geodesic_batch: every source set needs at least one vertex")
+    offsets = np.zeros(len(sets) + 1, dtype=np.int32)
+    offsets[1:] = np.cumsum([s.size for s in sets])
+    flat = np.concatenate(sets).astype(np.int32)
+    return DeviceArray.from_host(flat), DeviceArray.from_host(offsets), len(sets)
+
+
+def heat_geodesic_batch(
+    mesh: Trimesh,
+    source_sets: Any,
+    *,
+    t: float | None = None,
+    method: str = "meshlab",
+    refine: int = 1,
+    transpose: bool = True,
+) -> DeviceArray:
+    """Distances for many source sets on one resident mesh, solved together.
+
+    The served form of ``heat_geodesic(trimesh, sources)``: both systems are factored once and
+    kept on the mesh's solver, and each batch of ``k`` source sets (ragged) is one pass of the
+    path over ``k`` right-hand sides -- seeding, the two factored solves (``refine`` float64
+    refinement steps each), the divergence and the shift all run as batched kernels over the
+    interleaved ``[V][k]`` columns. Returns ``(k, V)`` (or ``(V, k)`` with ``transpose=False``).
+    Each column equals ``heat_geodesic(mesh, source_sets[c])`` up to the solves' rounding.
+    """
+    if not isinstance(mesh, Trimesh):
+        raise TypeError("heat_geodesic_batch: serves a resident Trimesh")
+    n = mesh.n_vertices
+    _supported(method, False)
+    src, offsets, k = _source_columns(source_sets, n)
+    if n == 0 or mesh.n_faces == 0:
+        return DeviceArray.zeros((k, n) if transpose else (n, k), np.float64)
+    solver = mesh.heat_solver(t, method=method)
+    if not solver.factor():
+        raise RuntimeError("heat_geodesic_batch: the systems could not be factored (over budget)")
+    u0 = DeviceArray.empty(n * k, np.float64)
+    invalid = DeviceArray.empty(1, np.int32)
+    _lib.call("ob_seed_columns", src.ptr, offsets.ptr, k, n, u0.ptr, invalid.ptr, DEFAULT_STREAM)
+    if int(invalid.numpy()[0]) != 0:
+        raise ValueError(
+            "heat_geodesic_batch: every source must be a vertex index in [0, n_vertices)"
+        )
+    heat = DeviceArray.empty(n * k, np.float64)
+    solver.heat_factor.solve_pointers(u0.ptr, heat.ptr, k, refine)
+    operators = solver.operators
+    neg_div = DeviceArray.empty(n * k, np.float64)
+    _lib.call(
+        "ob_grad_div", mesh.vertices.ptr, mesh.faces.ptr, mesh.n_faces, n,
+        operators.face_normals.ptr, operators.face_areas.ptr, heat.ptr, operators.cot_entries.ptr,
+        k, neg_div.ptr, DEFAULT_STREAM,
+    )  # fmt: skip
+    phi = DeviceArray.empty(n * k, np.float64)
+    solver.poisson_factor.solve_pointers(neg_div.ptr, phi.ptr, k, refine)
+    _lib.call("ob_shift", phi.ptr, n, src.ptr, src.size, offsets.ptr, k, 1, DEFAULT_STREAM)
+    if not transpose:
+        return phi.reshape(n, k)
+    out = DeviceArray.empty((k, n), np.float64)
+    _lib.call("ob_transpose", n, k, phi.ptr, out.ptr, DEFAULT_STREAM)
+    return out
 
 
 def heat_geodesic(

@@ -1,0 +1,94 @@
+"""Device Cholesky solves and the batched served path against the oracle (GPU)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import heat_path as hp
+from ordito_b200 import creation
+from ordito_b200 import heat as gheat
+from ordito_b200.cholesky import OperatorFactorization, sparse_cholesky
+from ordito_b200.device import DeviceArray
+from ordito_b200.mesh import Trimesh
+from tests import meshes
+
+pytestmark = pytest.mark.gpu
+
+DISTANCE_TOL = 1e-5
+
+
+@pytest.mark.parametrize("name", ["ico3", "saddle_graded", "bumpy_sphere", "small_torus", "unreferenced"])
+@pytest.mark.parametrize("k", [1, 5, 64])
+def test_heat_system_factor_solves_many_columns(gpu, name: str, k: int) -> None:
+    v, f = meshes.ALL[name]()
+    ref_ops = hp.heat_operators(v, f)
+    n = v.shape[0]
+    ops = gheat.heat_operators(v, f.reshape(-1), method="meshlab")
+    chol = sparse_cholesky(ops.heat_system, v, singular=False)
+    rng = np.random.default_rng(k)
+    B = np.zeros((n, k))
+    for c in range(k):
+        B[rng.integers(0, n), c] = 1.0
+    X = DeviceArray.zeros(n * k, np.float64)
+    chol.solve(B.reshape(-1), X, componentwise=True)
+    got = X.numpy().reshape(n, k)
+    H = hp.csr_matrix(ref_ops["pattern"], ref_ops["H"])
+    ref = hp.solve_heat(H, B)
+    mask = ref > 1e-250
+    assert np.max(np.abs(got - ref)[mask] / ref[mask]) <= 1e-8
+
+
+def test_poisson_factor_is_the_consistent_solution(gpu) -> None:
+    v, f = meshes.bumpy_sphere()
+    ref_ops = hp.heat_operators(v, f)
+    ops = gheat.heat_operators(v, f.reshape(-1), method="meshlab")
+    slot = OperatorFactorization(ops.poisson_system, v, singular=True)
+    assert slot.factor()
+    rng = np.random.default_rng(3)
+    b = rng.normal(size=v.shape[0])
+    b -= b.mean()
+    x = DeviceArray.zeros(v.shape[0], np.float64)
+    slot.solve(b, x)
+    got = x.numpy()
+    ref = hp.PoissonFactor(hp.csr_matrix(ref_ops["pattern"], ref_ops["P"])).solve(b)
+    assert hp.relative_linf(got - got.mean(), ref - ref.mean()) <= 1e-9
+
+
+@pytest.mark.parametrize("name", ["ico3", "small_torus", "bumpy_sphere", "saddle_graded"])
+def test_batched_queries_match_the_oracle_and_single_queries(gpu, name: str) -> None:
+    v, f = meshes.ALL[name]()
+    n = v.shape[0]
+    rng = np.random.default_rng(7)
+    sets = [rng.choice(n, size=int(s), replace=False) for s in rng.integers(1, 6, size=9)]
+    mesh = Trimesh(v, f.reshape(-1))
+    batch = gheat.heat_geodesic_batch(mesh, sets).numpy()
+    assert batch.shape == (len(sets), n)
+    t_eff, _ = hp.vertex_time(v, f, None)
+    ops = hp.heat_operators(v, f, t_eff)
+    factors = (hp.HeatFactor(hp.csr_matrix(ops["pattern"], ops["H"])),
+               hp.PoissonFactor(hp.csr_matrix(ops["pattern"], ops["P"])))
+    for c, s in enumerate(sets):
+        ref = hp.heat_geodesic(v, f, s, operators=ops, factors=factors)
+        assert hp.relative_linf(batch[c], ref) <= DISTANCE_TOL
+        alone = gheat.heat_geodesic_batch(mesh, [s]).numpy()[0]
+        assert hp.relative_linf(alone, batch[c]) <= 1e-9
+
+
+def test_batched_sources_are_validated(gpu) -> None:
+    v, f = creation.icosphere(2)
+    mesh = Trimesh(v, f.reshape(-1))
+    with pytest.raises(ValueError):
+        gheat.heat_geodesic_batch(mesh, [[0], [v.shape[0]]])
+    with pytest.raises(ValueError):
+        gheat.heat_geodesic_batch(mesh, [[0], []])
+
+
+def test_full_size_torus_single_query(gpu) -> None:
+    """The 131 072-vertex jittered torus: the settled iterate fails its backward-error check
+    (the idle bound stops it before the far field settles), and the factored fallback answers."""
+    v, f = creation.jittered_torus(512, 256, seed=0)
+    src = np.array([5], dtype=np.int32)
+    got = gheat.heat_geodesic(v, f.reshape(-1), src).numpy()
+    ref = hp.heat_geodesic(v, f, src)
+    assert hp.relative_linf(got, ref) <= DISTANCE_TOL
