@@ -1,27 +1,31 @@
-"""Benchmark: geodesic solves/s on the jittered 512 x 256 torus (131 072 vertices).
+"""Benchmark: heat-geodesic solves/s on the jittered 512 x 256 torus (131 072 vertices).
 
 Workload: the torus of R = 1, r = 0.3, every vertex moved by N(0, (0.1 h)^2) per coordinate
-(h the clean torus's mean edge length, seed 0), and a stream of 64 single-source heat-geodesic
-queries whose sources are 64 vertices drawn uniformly without replacement (seed 1). One step
-answers all 64 queries on the resident mesh (its pattern, operators and solver states kept on
-the device, as a served ``Trimesh`` keeps them). ``value`` is whole-job solves/s with the inputs
-resident in HBM; ``e2e`` is the same stream through the public API from host sources to host
-distances. Each run also checks a sample of answers against the float64 CPU oracle.
+(h the clean torus's mean edge length, seed 0), and a stream of 64 single-source queries whose
+sources are 64 vertices drawn uniformly without replacement (seed 1). One step answers all 64
+queries on the resident mesh -- the served + batched path: the mesh's operators and both Cholesky
+factors stay on the device, and the 64 queries run as one batched pass (seeding, the two factored
+solves over 64 right-hand sides with a float64 refinement step each, the divergence and the shift).
+``value`` is whole-job solves/s with the sources resident on the device; ``e2e`` is the same stream
+through the public API (``heat_geodesic_batch``) from host source lists to host distances, copies
+included. The plain drop-in (``heat_geodesic(vertices, faces, [s])``: assembly, solves and any
+factorisation inside every call) and the resident single query are timed beside it. A sample of
+the answers is checked against the float64 CPU oracle on every run.
 
-``--impl reference`` times the CPU restatement of the same path (``oracle/``, float64 direct
-solves with the factorisations reused across the stream) on the host cores, as the reference arm.
+``--impl reference`` times the CPU restatement of the same path (``oracle/``: float64 scipy direct
+solves, factorisations reused across the stream) on the host cores, as the reference arm.
 """
 
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -29,21 +33,23 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "geodesic solves/s (torus 131k, single-source query stream)"
+METRIC = "geodesic solves/s (torus 131k, 64 single-source queries, rel err <= 1e-5 vs FP64)"
 UNIT = "solves/s"
-WORKLOAD = "jittered torus 512x256 (131072 V, 262144 F), 64 single-source queries"
+WORKLOAD = "jittered torus 512x256 (131072 V, 262144 F), 64 single-source queries per step"
 
 
 def parse() -> argparse.Namespace:
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--queries", type=int, default=64)
     p.add_argument("--cols", type=int, default=512)
     p.add_argument("--rows", type=int, default=256)
+    p.add_argument("--refine", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-plain", action="store_true")
     return p.parse_args()
 
 
@@ -57,12 +63,12 @@ def workload(args: argparse.Namespace) -> tuple[np.ndarray, np.ndarray, np.ndarr
 
 
 # ---------------------------------------------------------------------------------------------
-# Distributed plumbing: one process per GPU, replicas (every rank answers its own stream).
+# Distributed plumbing: one process per GPU; replicas (every rank answers its own stream).
 # ---------------------------------------------------------------------------------------------
 
 
 class Dist:
-    def __init__(self, gpus: int) -> None:
+    def __init__(self) -> None:
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -74,7 +80,7 @@ class Dist:
             import torch.distributed as dist
 
             torch.cuda.set_device(self.local_rank)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
             self.pg = dist
             self.torch = torch
 
@@ -114,16 +120,16 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL,
             )
         except OSError:
             self.proc = None
-        time.sleep(0.25)
+        time.sleep(0.3)
         return self
 
     def __exit__(self, *exc) -> None:
-        time.sleep(0.15)
+        time.sleep(0.1)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -162,16 +168,16 @@ class Clocks:
 
 
 def cpu_stream(vertices: np.ndarray, faces: np.ndarray, sources: np.ndarray) -> tuple[float, dict]:
-    """Oracle solves/s over ``sources`` (one query each), factorisations built once and reused;
-    returns (solves/s, detail). Setup time is reported separately."""
+    """Oracle solves/s over ``sources`` (one query each): factorisations built once (setup, timed
+    separately) and reused; the per-query work is the two direct solves, the divergence and the
+    shift, all float64."""
     from oracle import heat_path as hp
 
     t0 = time.perf_counter()
     t_eff, _ = hp.vertex_time(vertices, faces, None)
     ops = hp.heat_operators(vertices, faces, t_eff)
-    H = hp.csr_matrix(ops["pattern"], ops["H"])
-    P = hp.csr_matrix(ops["pattern"], ops["P"])
-    factors = (hp.HeatFactor(H), hp.PoissonFactor(P))
+    factors = (hp.HeatFactor(hp.csr_matrix(ops["pattern"], ops["H"])),
+               hp.PoissonFactor(hp.csr_matrix(ops["pattern"], ops["P"])))
     setup = time.perf_counter() - t0
     t1 = time.perf_counter()
     for s in sources:
@@ -184,14 +190,13 @@ def run_reference(args: argparse.Namespace, dist: Dist) -> None:
     if dist.rank != 0:
         return
     vertices, faces, sources = workload(args)
-    sample = sources[: max(2, min(8, len(sources)))]
-    for _ in range(max(0, min(args.warmup, 1))):
-        cpu_stream(vertices, faces, sample[:1])
-    values = []
-    detail = {}
-    for _ in range(args.steps):
+    sample = sources[:4]
+    values, detail = [], {}
+    for _ in range(max(1, args.steps)):
         v, detail = cpu_stream(vertices, faces, sample)
         values.append(v)
+        if len(values) >= 3:
+            break
     value = statistics.median(values)
     line = {
         "impl": "reference",
@@ -199,8 +204,8 @@ def run_reference(args: argparse.Namespace, dist: Dist) -> None:
         "value": value,
         "unit": UNIT,
         "n_gpus": args.gpus,
-        "steps": args.steps,
-        "warmup": args.warmup,
+        "steps": len(values),
+        "warmup": 0,
         "ms_per_step": 1e3 * len(sources) / value,
         "higher_is_better": True,
         "scaling": "weak",
@@ -213,8 +218,8 @@ def run_reference(args: argparse.Namespace, dist: Dist) -> None:
             "unit": UNIT,
             "cores": 1,
             "kind": "port",
-            "sample": f"{len(sample)} of the {len(sources)} queries per step; factorisations "
-                      f"(scipy SuperLU) built once per step, {detail.get('setup_s', 0):.2f} s",
+            "sample": f"{len(sample)} of the {len(sources)} queries per step, float64 scipy SuperLU "
+                      f"factorisations reused (their {detail.get('setup_s', 0):.2f} s setup excluded)",
         },
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -226,88 +231,146 @@ def run_reference(args: argparse.Namespace, dist: Dist) -> None:
 # ---------------------------------------------------------------------------------------------
 
 
+def _events():
+    from ordito_b200 import _lib
+
+    a, b = ctypes.c_void_p(0), ctypes.c_void_p(0)
+    _lib.call("ob_event_create", ctypes.byref(a))
+    _lib.call("ob_event_create", ctypes.byref(b))
+    return a, b
+
+
+def _elapsed(a, b) -> float:
+    from ordito_b200 import _lib
+
+    ms = ctypes.c_float(0.0)
+    _lib.call("ob_event_elapsed_ms", a, b, ctypes.byref(ms))
+    return float(ms.value)
+
+
+def _peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            data = json.load(f)
+        return {"hbm_gbs": float(data["hbm_gbs"]), "source": "measured"}
+    except (OSError, KeyError, ValueError):
+        return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
 def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     from oracle import heat_path as hp
     from ordito_b200 import _lib
-    from ordito_b200.device import DeviceArray, synchronize
-    from ordito_b200.heat import heat_geodesic
+    from ordito_b200 import heat as gheat
+    from ordito_b200.device import PinnedArray, synchronize
     from ordito_b200.mesh import Trimesh
 
     _lib.call("ob_set_device", dist.local_rank)
     vertices, faces, sources = workload(args)
     n = vertices.shape[0]
+    k = len(sources)
+    sets = [[int(s)] for s in sources]
+
+    # Resident state: mesh, operators and both factors (timed once, reported as setup).
+    synchronize()
+    t0 = time.perf_counter()
     mesh = Trimesh(vertices, faces.reshape(-1))
-    device_sources = [DeviceArray.from_host(np.array([s], dtype=np.int32)) for s in sources]
+    solver = mesh.heat_solver(None, method="meshlab")
+    assert solver.factor(), "factorisation refused"
+    synchronize()
+    setup_s = time.perf_counter() - t0
+    src, offsets, _ = gheat._source_columns(sets, n)
 
-    def step(results: list) -> None:
-        for k, src in enumerate(device_sources):
-            results[k] = heat_geodesic(mesh, src)
+    def step():
+        return gheat._batch_columns(mesh, solver, src, offsets, k, args.refine, True)
 
-    results: list = [None] * len(sources)
+    out = None
     for _ in range(max(args.warmup, 3)):
-        step(results)
+        out = step()
     synchronize()
 
-    # Accuracy against the float64 oracle on a sample of the stream (outside the timed region).
-    check = [0, len(sources) // 2, len(sources) - 1]
+    # Accuracy against the float64 oracle on a sample of the batch (outside the timed region).
+    result = out.numpy()
     t_eff, _ = hp.vertex_time(vertices, faces, None)
     ops = hp.heat_operators(vertices, faces, t_eff)
     factors = (hp.HeatFactor(hp.csr_matrix(ops["pattern"], ops["H"])),
                hp.PoissonFactor(hp.csr_matrix(ops["pattern"], ops["P"])))
-    errors = []
-    for k in check:
-        ref = hp.heat_geodesic(vertices, faces, np.array([sources[k]]), operators=ops, factors=factors)
-        errors.append(hp.relative_linf(results[k].numpy(), ref))
+    check = sorted({0, k // 2, k - 1})
+    errors = [
+        hp.relative_linf(result[c], hp.heat_geodesic(vertices, faces, np.array([sources[c]]),
+                                                     operators=ops, factors=factors))
+        for c in check
+    ]
 
     start, end = _events()
-    launches0 = _lib.launch_count()
     dist.barrier()
     synchronize()
+    launches0 = _lib.launch_count()
     with Clocks(dist.local_rank) as clocks:
         _lib.call("ob_event_record", start, None)
         for _ in range(args.steps):
-            step(results)
+            out = step()
         _lib.call("ob_event_record", end, None)
         synchronize()
+    launches = (_lib.launch_count() - launches0) // max(args.steps, 1)
     ms = _elapsed(start, end) / args.steps
-    launches = _lib.launch_count() - launches0
     dist.barrier()
     ms_max = dist.max(ms)
-    value = dist.world * len(sources) / (ms_max / 1e3)
+    value = dist.world * k / (ms_max / 1e3)
 
-    # End to end through the public API: host sources in, host distances out, every step.
-    host_sources = [np.array([s], dtype=np.int32) for s in sources]
+    # End to end through the public API: host source lists in, host distances out.
+    host = PinnedArray((k, n), np.float64)
     dist.barrier()
     synchronize()
-    t0 = time.perf_counter()
+    t_wall = time.perf_counter()
     _lib.call("ob_event_record", start, None)
     for _ in range(args.steps):
-        for k, src in enumerate(host_sources):
-            results[k] = heat_geodesic(mesh, src).numpy()
+        batch = gheat.heat_geodesic_batch(mesh, sets, refine=args.refine)
+        host.copy_from_device(batch, sync=True)
     _lib.call("ob_event_record", end, None)
     synchronize()
-    e2e_ms = max(_elapsed(start, end), (time.perf_counter() - t0) * 1e3) / args.steps
+    e2e_ms = max(_elapsed(start, end), (time.perf_counter() - t_wall) * 1e3) / args.steps
     e2e_ms = dist.max(e2e_ms)
-    e2e_value = dist.world * len(sources) / (e2e_ms / 1e3)
+    e2e_value = dist.world * k / (e2e_ms / 1e3)
 
-    # Roofline of the dominant kernel: the heat system's round mat-vec with its three dots.
-    heat_system = mesh.heat_solver(None, method="meshlab").operators.heat_system
-    solver = next(iter(heat_system._solvers.values()))
-    import ctypes
+    # Resident single query (the same factors, one right-hand side at a time).
+    single = [[int(s)] for s in sources[:16]]
+    synchronize()
+    _lib.call("ob_event_record", start, None)
+    for s in single:
+        gheat.heat_geodesic_batch(mesh, [s], refine=args.refine)
+    _lib.call("ob_event_record", end, None)
+    synchronize()
+    single_value = len(single) / (_elapsed(start, end) / 1e3)
 
-    info = (ctypes.c_longlong * 5)()
-    _lib.call("ob_pcg_info", solver.handle, info)
-    n_rows, k_cols, nnz, narrow = int(info[0]), int(info[1]), int(info[2]), int(info[3])
-    kernel_ms = ctypes.c_float(0.0)
-    _lib.call("ob_pcg_time_matvec", solver.handle, 200, ctypes.byref(kernel_ms), None)
-    value_bytes = 4 if narrow else 8
-    # Algorithmic bytes of one launch: the values and column indices once, the row offsets, the
-    # vector u read once, w written once, and r read for the dots.
-    algorithmic = nnz * (value_bytes + 4) + 4 * (n_rows + 1) + 3 * 8 * n_rows * k_cols
-    achieved = algorithmic / (kernel_ms.value / 1e3) / 1e9
+    # Plain drop-in: heat_geodesic(vertices, faces, [s]) builds everything inside every call.
+    plain = None
+    if not args.no_plain:
+        plain_times = []
+        for s in sources[:2]:
+            synchronize()
+            t_plain = time.perf_counter()
+            gheat.heat_geodesic(vertices, faces.reshape(-1), np.array([s], dtype=np.int32)).numpy()
+            plain_times.append(time.perf_counter() - t_plain)
+        plain = 1.0 / statistics.median(plain_times)
+
+    # Roofline of the dominant kernel: the factored triangular passes (batched dense products over
+    # 64 columns), timed standalone with CUDA events on the heat factor.
+    heat_factor = solver.heat_factor
+    info = (ctypes.c_longlong * 4)()
+    _lib.call("ob_chol_info", heat_factor.handle, info)
+    n_vals, levels, pass_launches = int(info[1]), int(info[2]), int(info[3])
+    pass_ms = ctypes.c_float(0.0)
+    _lib.call("ob_chol_time_solve", heat_factor.handle, k, 20, ctypes.byref(pass_ms), None)
+    # One forward + backward pass reads every stored factor value twice (once per direction) and
+    # moves the three n x k work vectors about four times; 2 flops per value, column and direction.
+    algorithmic = 2 * 8 * n_vals + 4 * 3 * 8 * n * k
+    flops = 2 * 2 * n_vals * k
+    seconds = pass_ms.value / 1e3
+    achieved = algorithmic / seconds / 1e9
+    fp64 = ctypes.c_float(0.0)
+    _lib.call("ob_fp64_peak", ctypes.byref(fp64), None)
     peaks = _peaks()
 
-    line = None
     if dist.rank == 0:
         line = {
             "metric": METRIC,
@@ -324,86 +387,69 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
             "data": "synthetic",
             "config": {
                 "workload": WORKLOAD,
-                "queries_per_step": len(sources),
-                "path": "resident Trimesh; settled Jacobi CG heat solve (f32 values, f64 vectors), "
-                        "Chebyshev-12 CG Poisson solve",
-                "l2": "inputs resident; the 131k-vertex operators (~8 MB) are L2-resident, no flush",
+                "queries_per_step": k,
+                "path": "served + batched: resident Trimesh, nested-dissection supernodal Cholesky "
+                        "of M - tL and -L held on the device, 64 right-hand sides per pass, "
+                        f"{args.refine} float64 refinement step(s) per solve",
+                "l2": "no flush; per step the two 147 MB factors (294 MB) exceed the 126 MB L2",
                 "parallelism": f"replicas{dist.world}",
+                "setup_s": setup_s,
             },
             "accuracy": {"max_rel_linf_vs_fp64_oracle": max(errors), "checked_queries": len(check)},
             "e2e": {
                 "value": e2e_value,
                 "unit": UNIT,
-                "h2d_bytes_per_step": 4 * len(sources),
-                "d2h_bytes_per_step": 8 * n * len(sources),
+                "h2d_bytes_per_step": 4 * (2 * k + 1),
+                "d2h_bytes_per_step": 8 * n * k,
             },
-            "gpu_launches": launches // max(args.steps, 1),
+            "gpu_launches": launches,
             "clocks": clocks.summary(),
+            "plain_single_query": {
+                "value": plain,
+                "unit": UNIT,
+                "what": "heat_geodesic(vertices, faces, [s]) per query: assembly, settled CG, the "
+                        "backward-error check and its factored fallback inside every call",
+            },
+            "resident_single_query": {"value": single_value, "unit": UNIT,
+                                      "what": "heat_geodesic_batch(mesh, [[s]]): factors resident, k = 1"},
             "roofline": {
                 "bound": "hbm",
-                "kernel": "matvec_dots_kernel<float> (heat system round)",
+                "kernel": "tile_product_kernel (Cholesky forward+backward pass, 64 columns)",
                 "achieved": achieved,
                 "peak": peaks["hbm_gbs"],
                 "peak_source": peaks["source"],
                 "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"],
                 "traffic": None,
-                "kernel_ms": kernel_ms.value,
+                "pass_ms": pass_ms.value,
+                "launches_per_pass": pass_launches,
                 "algorithmic_bytes": algorithmic,
-                "note": "operator and vectors fit in L2: the fraction is of HBM peak but the kernel "
-                        "is L2-served",
+                "fp64": {
+                    "achieved_tflops": flops / seconds / 1e12,
+                    "peak_tflops_measured": fp64.value,
+                    "frac": (flops / seconds / 1e12) / fp64.value if fp64.value else None,
+                    "intensity_flop_per_byte": flops / algorithmic,
+                },
             },
         }
         if not args.no_cpu_baseline and dist.world == 1:
-            sample = sources[:4]
-            cpu_value, detail = cpu_stream(vertices, faces, sample)
+            cpu_value, detail = cpu_stream(vertices, faces, sources[:4])
             line["cpu_baseline"] = {
                 "value": cpu_value,
                 "unit": UNIT,
                 "cores": 1,
                 "kind": "port",
-                "sample": f"{len(sample)} single-source queries on the same torus, float64 scipy "
-                          f"SuperLU factorisations reused (setup {detail['setup_s']:.2f} s excluded)",
+                "sample": f"4 single-source queries on the same torus, float64 scipy SuperLU "
+                          f"factorisations reused (their {detail['setup_s']:.2f} s setup excluded)",
             }
         print(json.dumps(line), flush=True)
     _lib.call("ob_event_destroy", start)
     _lib.call("ob_event_destroy", end)
 
 
-def _events():
-    import ctypes
-
-    from ordito_b200 import _lib
-
-    a, b = ctypes.c_void_p(0), ctypes.c_void_p(0)
-    _lib.call("ob_event_create", ctypes.byref(a))
-    _lib.call("ob_event_create", ctypes.byref(b))
-    return a, b
-
-
-def _elapsed(a, b) -> float:
-    import ctypes
-
-    from ordito_b200 import _lib
-
-    ms = ctypes.c_float(0.0)
-    _lib.call("ob_event_elapsed_ms", a, b, ctypes.byref(ms))
-    return float(ms.value)
-
-
-def _peaks() -> dict:
-    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    try:
-        with open(path) as f:
-            data = json.load(f)
-        return {"hbm_gbs": float(data["hbm_gbs"]), "source": "measured"}
-    except (OSError, KeyError, ValueError):
-        return {"hbm_gbs": 6650.0, "source": "fallback"}
-
-
 def main() -> None:
     args = parse()
-    dist = Dist(args.gpus)
+    dist = Dist()
     try:
         if args.impl == "reference":
             run_reference(args, dist)

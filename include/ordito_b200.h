@@ -178,6 +178,9 @@ int ob_cast_scale(const void* in, int in_type, void* out, int out_type, long lon
  * (replaces kernels/heat.py:614 seed_source_indicator for several columns). */
 int ob_axpby(long long n, double a, const double* x, double b, const double* y, double* out,
              ob_stream_t stream);
+/* Measurement hook: the device's float64 FMA throughput (TFLOP/s) from a register-resident FMA
+ * loop over every SM (the compute roofline of the float64 dense products). */
+int ob_fp64_peak(float* tflops, ob_stream_t stream);
 int ob_transpose(int rows, int cols, const double* in, double* out, ob_stream_t stream);
 int ob_seed_columns(const int32_t* sources, const int32_t* source_offsets, int n_columns,
                     int n_vertices, double* u0, int32_t* invalid, ob_stream_t stream);
@@ -200,7 +203,13 @@ int ob_spmv(int n, const int32_t* offsets, const int32_t* columns, const double*
  * non-positive pivot. The factor (partitioned inverse) is uploaded to the device.
  * ob_chol_solve: x = A^-1 rhs for n_columns interleaved columns ([n][n_columns]), then `refine`
  * float64 refinement steps x += A^-1 (rhs - A x) with the operator's CSR arrays (may be NULL when
- * refine == 0); level-scheduled batched dense products on the device, no host read-back. */
+ * refine == 0); level-scheduled batched dense products on the device, recorded once per
+ * (n_columns, refine) as a CUDA graph and replayed, no host read-back. rhs == NULL solves the
+ * factor's own right-hand-side buffer and x == NULL leaves the result in its own solution buffer
+ * (ob_chol_buffers returns both, sized for n_columns), so a pipeline can chain solves with no
+ * copies. ob_chol_time_solve: average duration of `reps` forward+backward triangular passes
+ * (CUDA events; a measurement hook). ob_chol_info: info[0..3] = n, stored values, tree levels,
+ * product launches per pass. */
 int ob_chol_analyse(int n, const int32_t* offsets, const int32_t* columns, const float* xyz,
                     void** analysis, ob_stream_t stream);
 int ob_chol_analysis_info(void* analysis, long long* info);
@@ -218,6 +227,10 @@ int ob_chol_destroy(void* factor);
 int ob_chol_solve(void* factor, const double* rhs, double* x, int n_columns, int refine,
                   const int32_t* offsets, const int32_t* columns, const double* values,
                   ob_stream_t stream);
+int ob_chol_buffers(void* factor, int n_columns, double** rhs, double** solution,
+                    ob_stream_t stream);
+int ob_chol_time_solve(void* factor, int n_columns, int reps, float* ms, ob_stream_t stream);
+int ob_chol_info(void* factor, long long* info);
 
 #ifdef __cplusplus
 }

@@ -74,6 +74,7 @@ SIGNATURES: dict[str, list] = {
     "ob_cast_scale": [P, I, P, I, ctypes.c_longlong, D, P],
     "ob_bounds": [P, I, P, P],
     "ob_axpby": [ctypes.c_longlong, D, P, D, P, P, P],
+    "ob_fp64_peak": [POINTER(c_float), P],
     "ob_transpose": [I, I, P, P, P],
     "ob_seed_columns": [P, P, I, I, P, P, P],
     "ob_chol_analyse": [I, P, P, P, POINTER(c_void_p), P],
@@ -84,6 +85,9 @@ SIGNATURES: dict[str, list] = {
     "ob_chol_host_solve": [I, P, P, P, P, I, P, P, POINTER(ctypes.c_longlong)],
     "ob_chol_destroy": [P],
     "ob_chol_solve": [P, P, P, I, I, P, P, P, P],
+    "ob_chol_buffers": [P, I, POINTER(c_void_p), POINTER(c_void_p), P],
+    "ob_chol_time_solve": [P, I, I, POINTER(c_float), P],
+    "ob_chol_info": [P, POINTER(ctypes.c_longlong)],
 }
 _RESTYPES = {"ob_last_error": c_char_p}
 

@@ -92,6 +92,13 @@ class SparseCholesky:
         _lib.call("ob_chol_nbytes", self.handle, ctypes.byref(size))
         return int(size.value)
 
+    def buffers(self, n_columns: int) -> tuple[int, int]:
+        """Device pointers of the factor's own right-hand-side and solution buffers ([n][k])."""
+        rhs, sol = ctypes.c_void_p(0), ctypes.c_void_p(0)
+        _lib.call("ob_chol_buffers", self.handle, int(n_columns), ctypes.byref(rhs),
+                  ctypes.byref(sol), DEFAULT_STREAM)
+        return int(rhs.value), int(sol.value)
+
     def solve_pointers(self, rhs: int, x: int, n_columns: int, refine: int, stream: Any = None) -> None:
         """``x = A^-1 rhs`` for ``n_columns`` interleaved columns ([n][n_columns]) plus ``refine``
         float64 refinement steps, all enqueued on the device (no read-back)."""

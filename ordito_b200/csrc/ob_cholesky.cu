@@ -531,10 +531,21 @@ struct Factor {
     std::vector<Tile*> fwd_diag, fwd_off, bwd_off, bwd_diag;
     std::vector<int> n_fwd_diag, n_fwd_off, n_bwd_off, n_bwd_diag;
     std::vector<void*> owned;
-    // Work buffers sized for `cap_k` columns.
+    // Work buffers sized for `cap_k` columns: B, Y, X in the factor's numbering, R the residual,
+    // RHS / SOL the caller's right-hand side and solution copied in / out (old numbering).
     int cap_k = 0;
-    double *B = nullptr, *Y = nullptr, *X = nullptr, *R = nullptr, *D = nullptr;
+    double *B = nullptr, *Y = nullptr, *X = nullptr, *R = nullptr, *RHS = nullptr, *SOL = nullptr;
     size_t bytes = 0;
+    // Recorded solve graphs, keyed by (columns, refinement steps, operator arrays).
+    struct Recorded {
+        int k, refine;
+        const int *offsets, *columns;
+        const double* values;
+        cudaGraphExec_t exec;
+        int launches;
+    };
+    std::vector<Recorded> graphs;
+    cudaStream_t capture = nullptr;
 };
 
 int dev_alloc(Factor* F, void** p, size_t bytes, cudaStream_t stream) {
@@ -547,6 +558,8 @@ int dev_alloc(Factor* F, void** p, size_t bytes, cudaStream_t stream) {
 void factor_release(Factor* F) {
     if (F == nullptr) return;
     cudaDeviceSynchronize();
+    for (auto& g : F->graphs) cudaGraphExecDestroy(g.exec);
+    if (F->capture) cudaStreamDestroy(F->capture);
     for (void* p : F->owned) cudaFree(p);
     delete F;
 }
@@ -635,8 +648,12 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
 
 int ensure_work(Factor* F, int k, cudaStream_t stream) {
     if (k <= F->cap_k) return OB_OK;
+    // Growing the buffers invalidates every recorded graph (they name the old ones).
+    OB_CUDA(cudaStreamSynchronize(stream));
+    for (auto& g : F->graphs) cudaGraphExecDestroy(g.exec);
+    F->graphs.clear();
     const size_t vec = sizeof(double) * (size_t)F->n * k;
-    for (double** p : {&F->B, &F->Y, &F->X, &F->R, &F->D}) {
+    for (double** p : {&F->B, &F->Y, &F->X, &F->R, &F->RHS, &F->SOL}) {
         int st = dev_alloc(F, (void**)p, vec, stream);
         if (st) return st;
     }
@@ -763,6 +780,78 @@ int ob_chol_factor(void* analysis, const double* values, int singular, void** fa
     return OB_OK;
 }
 
+int ob_chol_solve(void* factor, const double* rhs, double* x, int n_columns, int refine,
+                  const int32_t* offsets, const int32_t* columns, const double* values,
+                  ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(factor && n_columns >= 1 && refine >= 0, "ob_chol_solve: bad argument");
+    OB_REQUIRE(refine == 0 || (offsets && columns && values),
+               "ob_chol_solve: refinement needs the operator");
+    Factor* F = static_cast<Factor*>(factor);
+    int st = ensure_work(F, n_columns, stream);
+    if (st) return st;
+    const size_t bytes = sizeof(double) * (size_t)F->n * n_columns;
+    if (rhs != nullptr && rhs != F->RHS)
+        OB_CUDA(cudaMemcpyAsync(F->RHS, rhs, bytes, cudaMemcpyDeviceToDevice, stream));
+    Factor::Recorded* g = nullptr;
+    st = solve_graph(F, n_columns, refine, refine ? offsets : nullptr, refine ? columns : nullptr,
+                     refine ? values : nullptr, &g);
+    if (st) return st;
+    OB_CUDA(cudaGraphLaunch(g->exec, stream));
+    count_launch((uint64_t)g->launches);
+    if (x != nullptr && x != F->SOL)
+        OB_CUDA(cudaMemcpyAsync(x, F->SOL, bytes, cudaMemcpyDeviceToDevice, stream));
+    return OB_OK;
+}
+
+int ob_chol_buffers(void* factor, int n_columns, double** rhs, double** solution,
+                    ob_stream_t stream_) {
+    OB_REQUIRE(factor && rhs && solution && n_columns >= 1, "ob_chol_buffers: bad argument");
+    Factor* F = static_cast<Factor*>(factor);
+    int st = ensure_work(F, n_columns, as_stream(stream_));
+    if (st) return st;
+    *rhs = F->RHS;
+    *solution = F->SOL;
+    return OB_OK;
+}
+
+int ob_chol_time_solve(void* factor, int n_columns, int reps, float* ms, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(factor && ms && reps >= 1 && n_columns >= 1, "ob_chol_time_solve: bad argument");
+    Factor* F = static_cast<Factor*>(factor);
+    int st = ensure_work(F, n_columns, stream);
+    if (st) return st;
+    cudaEvent_t start, end;
+    OB_CUDA(cudaEventCreate(&start));
+    OB_CUDA(cudaEventCreate(&end));
+    cudaEventRecord(start, stream);
+    for (int i = 0; i < reps && st == OB_OK; ++i) st = triangular_solves(F, n_columns, stream);
+    cudaEventRecord(end, stream);
+    cudaError_t e = cudaEventSynchronize(end);
+    float total = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&total, start, end);
+    cudaEventDestroy(start);
+    cudaEventDestroy(end);
+    if (st) return st;
+    if (e != cudaSuccess) return cuda_status(e, "ob_chol_time_solve");
+    *ms = total / (float)reps;
+    return OB_OK;
+}
+
+int ob_chol_info(void* factor, long long* info) {
+    OB_REQUIRE(factor && info, "ob_chol_info: bad argument");
+    Factor* F = static_cast<Factor*>(factor);
+    info[0] = F->n;
+    info[1] = F->n_vals;
+    info[2] = F->analysis->levels;
+    long long launches = 0;
+    for (int l = 0; l < F->analysis->levels; ++l)
+        launches += (F->n_fwd_diag[l] > 0) + (F->n_fwd_off[l] > 0) + (F->n_bwd_off[l] > 0) +
+                    (F->n_bwd_diag[l] > 0);
+    info[3] = launches;
+    return OB_OK;
+}
+
 int ob_chol_host_solve(int n, const int32_t* offsets, const int32_t* columns,
                        const double* values, const float* xyz, int singular, const double* rhs,
                        double* x, long long* info) {
@@ -828,37 +917,62 @@ int ob_chol_destroy(void* factor) {
     return OB_OK;
 }
 
-int ob_chol_solve(void* factor, const double* rhs, double* x, int n_columns, int refine,
-                  const int32_t* offsets, const int32_t* columns, const double* values,
-                  ob_stream_t stream_) {
-    cudaStream_t stream = as_stream(stream_);
-    OB_REQUIRE(factor && rhs && x && n_columns >= 1, "ob_chol_solve: bad argument");
-    OB_REQUIRE(refine == 0 || (offsets && columns && values),
-               "ob_chol_solve: refinement needs the operator");
-    Factor* F = static_cast<Factor*>(factor);
-    int st = ensure_work(F, n_columns, stream);
-    if (st) return st;
-    const int n = F->n, k = n_columns;
-    const long long total = (long long)n * k;
-    const int grid = grid_for(total);
-    // x = A^-1 b.
-    permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->pinned, rhs, F->B);
+// The whole solve on the factor's own buffers: SOL = A^-1 RHS plus `refine` refinement steps.
+int enqueue_solve(Factor* F, int k, int refine, const int* offsets, const int* columns,
+                  const double* values, cudaStream_t stream) {
+    const int n = F->n;
+    const int grid = grid_for((long long)n * k);
+    permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->pinned, F->RHS, F->B);
     OB_CHECK_LAUNCH("chol permute in");
-    st = triangular_solves(F, k, stream);
+    int st = triangular_solves(F, k, stream);
     if (st) return st;
-    permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->X, x, 0);
+    permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->X, F->SOL, 0);
     OB_CHECK_LAUNCH("chol permute out");
     // Iterative refinement in float64: x += A^-1 (b - A x).
     for (int it = 0; it < refine; ++it) {
-        residual_kernel<<<grid, 256, 0, stream>>>(n, k, offsets, columns, values, rhs, x, F->R);
+        residual_kernel<<<grid, 256, 0, stream>>>(n, k, offsets, columns, values, F->RHS, F->SOL,
+                                                  F->R);
         OB_CHECK_LAUNCH("chol residual");
         permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->pinned, F->R, F->B);
         OB_CHECK_LAUNCH("chol permute in");
         st = triangular_solves(F, k, stream);
         if (st) return st;
-        permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->X, x, 1);
+        permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->X, F->SOL, 1);
         OB_CHECK_LAUNCH("chol permute out");
     }
+    return OB_OK;
+}
+
+// The recorded graph of enqueue_solve for (k, refine, operator), recorded on first use.
+int solve_graph(Factor* F, int k, int refine, const int* offsets, const int* columns,
+                const double* values, Factor::Recorded** out) {
+    for (auto& g : F->graphs)
+        if (g.k == k && g.refine == refine && g.offsets == offsets && g.columns == columns &&
+            g.values == values) {
+            *out = &g;
+            return OB_OK;
+        }
+    if (F->capture == nullptr) OB_CUDA(cudaStreamCreateWithFlags(&F->capture, cudaStreamNonBlocking));
+    // Launches are counted at each replay (the graph's kernel nodes), not at capture.
+    suppress_counting(1);
+    cudaError_t e = cudaStreamBeginCapture(F->capture, cudaStreamCaptureModeThreadLocal);
+    int st = e == cudaSuccess ? enqueue_solve(F, k, refine, offsets, columns, values, F->capture)
+                              : cuda_status(e, "ob_chol_solve: begin capture");
+    cudaGraph_t graph = nullptr;
+    if (e == cudaSuccess) e = cudaStreamEndCapture(F->capture, &graph);
+    suppress_counting(-1);
+    if (st != OB_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return st != OB_OK ? st : cuda_status(e, "ob_chol_solve: capture");
+    }
+    size_t nodes = 0;
+    cudaGraphGetNodes(graph, nullptr, &nodes);
+    cudaGraphExec_t exec;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_status(e, "ob_chol_solve: instantiate");
+    F->graphs.push_back(Factor::Recorded{k, refine, offsets, columns, values, exec, (int)nodes});
+    *out = &F->graphs.back();
     return OB_OK;
 }
 

@@ -53,6 +53,21 @@ __global__ void seed_columns_kernel(const int* __restrict__ sources,
     }
 }
 
+// Eight independent float64 FMA chains per thread: the device's FP64 FMA throughput.
+__global__ void fp64_fma_kernel(int iterations, double seed, double* __restrict__ sink) {
+    double a[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = seed + threadIdx.x + j;
+    const double m = 0.999999, c = 1e-7;
+    for (int i = 0; i < iterations; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = fma(a[j], m, c);
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s += a[j];
+    if (s == 12345.678) sink[0] = s;  // keeps the chains live
+}
+
 // Axis-aligned bounds of float32 points: out = (min x, min y, min z, max x, max y, max z).
 __global__ void bounds_kernel(const float* __restrict__ xyz, int n, float* __restrict__ partials,
                               unsigned int* counter, double* __restrict__ out) {
@@ -92,6 +107,33 @@ __global__ void bounds_kernel(const float* __restrict__ xyz, int n, float* __res
 using namespace ob;
 
 extern "C" {
+
+int ob_fp64_peak(float* tflops, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(tflops != nullptr, "ob_fp64_peak: null output");
+    Scratch scratch(stream);
+    double* sink = scratch.take<double>(1);
+    int st = scratch.commit();
+    if (st) return st;
+    const int blocks = 8 * sm_count(), threads = 256, iterations = 4096;
+    cudaEvent_t start, end;
+    OB_CUDA(cudaEventCreate(&start));
+    OB_CUDA(cudaEventCreate(&end));
+    fp64_fma_kernel<<<blocks, threads, 0, stream>>>(iterations, 1.0, sink);  // warm-up
+    cudaEventRecord(start, stream);
+    for (int r = 0; r < 5; ++r) fp64_fma_kernel<<<blocks, threads, 0, stream>>>(iterations, 1.0, sink);
+    cudaEventRecord(end, stream);
+    count_launch(6);
+    cudaError_t e = cudaEventSynchronize(end);
+    float ms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, start, end);
+    cudaEventDestroy(start);
+    cudaEventDestroy(end);
+    if (e != cudaSuccess) return cuda_status(e, "ob_fp64_peak");
+    const double flops = 5.0 * blocks * threads * (double)iterations * 8.0 * 2.0;
+    *tflops = (float)(flops / (ms * 1e-3) / 1e12);
+    return OB_OK;
+}
 
 int ob_axpby(long long n, double a, const double* x, double b, const double* y, double* out,
              ob_stream_t stream_) {

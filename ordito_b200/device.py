@@ -152,6 +152,39 @@ class DeviceArray:
         return self.reshape(self.size)
 
 
+class PinnedArray:
+    """Page-locked host memory viewed as a NumPy array (fast device<->host copies)."""
+
+    def __init__(self, shape: int | tuple[int, ...], dtype: Any = np.float64) -> None:
+        shape = (shape,) if isinstance(shape, (int, np.integer)) else tuple(shape)
+        dtype = np.dtype(dtype)
+        nbytes = max(int(np.prod(shape, dtype=np.int64)) * dtype.itemsize, 1)
+        ptr = ctypes.c_void_p(0)
+        _lib.call("ob_host_alloc", nbytes, ctypes.byref(ptr))
+        self.ptr = int(ptr.value)
+        buffer = (ctypes.c_byte * nbytes).from_address(self.ptr)
+        self.array = np.frombuffer(buffer, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+
+    def __del__(self) -> None:
+        if getattr(self, "ptr", 0):
+            try:
+                _lib.lib.ob_host_free(self.ptr)
+            except Exception:
+                pass
+            self.ptr = 0
+
+    def copy_from_device(self, device: "DeviceArray", sync: bool = True) -> np.ndarray:
+        if device.nbytes > self.array.nbytes:
+            raise ValueError("pinned buffer too small")
+        _lib.call("ob_memcpy", self.ptr, device.ptr, device.nbytes, 1, DEFAULT_STREAM, int(sync))
+        return self.array
+
+    def upload(self, sync: bool = False) -> "DeviceArray":
+        out = DeviceArray.empty(self.array.shape, self.array.dtype)
+        _lib.call("ob_memcpy", out.ptr, self.ptr, self.array.nbytes, 0, DEFAULT_STREAM, int(sync))
+        return out
+
+
 def interface_of(obj: Any) -> dict[str, Any] | None:
     return getattr(obj, "__cuda_array_interface__", None)
 

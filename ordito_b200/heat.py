@@ -234,6 +234,12 @@ class HeatSolver:
                 ok = kept["factorization"].factor(self._sharing(role)) and ok
         return ok
 
+    def scratch_flag(self) -> DeviceArray:
+        """A device int32 the batched seeding writes its (host-prevalidated) range flag into."""
+        if getattr(self, "_flag", None) is None:
+            self._flag = DeviceArray.empty(1, np.int32)
+        return self._flag
+
     @property
     def heat_factor(self):
         """The heat system's held ``SparseCholesky`` (``None`` before ``factor``)."""
@@ -326,6 +332,10 @@ def _source_columns(source_sets: Any, n: int) -> tuple[DeviceArray, DeviceArray,
         raise ValueError("heat_geodesic_batch: no source sets")
     if any(s.size == 0 for s in sets):
         raise ValueError("heat_geodesic_batch: every source set needs at least one vertex")
+    if any(((s < 0) | (s >= n)).any() for s in sets):
+        raise ValueError(
+            "heat_geodesic_batch: every source must be a vertex index in [0, n_vertices)"
+        )
     offsets = np.zeros(len(sets) + 1, dtype=np.int32)
     offsets[1:] = np.cumsum([s.size for s in sets])
     flat = np.concatenate(sets).astype(np.int32)
@@ -360,29 +370,35 @@ def heat_geodesic_batch(
     solver = mesh.heat_solver(t, method=method)
     if not solver.factor():
         raise RuntimeError("heat_geodesic_batch: the systems could not be factored (over budget)")
-    u0 = DeviceArray.empty(n * k, np.float64)
-    invalid = DeviceArray.empty(1, np.int32)
-    _lib.call("ob_seed_columns", src.ptr, offsets.ptr, k, n, u0.ptr, invalid.ptr, DEFAULT_STREAM)
-    if int(invalid.numpy()[0]) != 0:
-        raise ValueError(
-            "heat_geodesic_batch: every source must be a vertex index in [0, n_vertices)"
-        )
-    heat = DeviceArray.empty(n * k, np.float64)
-    solver.heat_factor.solve_pointers(u0.ptr, heat.ptr, k, refine)
+    return _batch_columns(mesh, solver, src, offsets, k, refine, transpose)
+
+
+def _batch_columns(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offsets: DeviceArray,
+                   k: int, refine: int, transpose: bool) -> DeviceArray:
+    """The batched pass over resident, validated source columns: the seeds are written into the
+    heat factor's own right-hand side, each solve leaves its result in its factor's solution
+    buffer, and the divergence writes the Poisson factor's right-hand side -- no copies between."""
+    n = mesh.n_vertices
+    heat_factor, poisson_factor = solver.heat_factor, solver.poisson_factor
+    heat_rhs, heat_sol = heat_factor.buffers(k)
+    poisson_rhs, phi = poisson_factor.buffers(k)
+    invalid = solver.scratch_flag()
+    _lib.call("ob_seed_columns", src.ptr, offsets.ptr, k, n, heat_rhs, invalid.ptr, DEFAULT_STREAM)
+    heat_factor.solve_pointers(0, 0, k, refine)
     operators = solver.operators
-    neg_div = DeviceArray.empty(n * k, np.float64)
     _lib.call(
         "ob_grad_div", mesh.vertices.ptr, mesh.faces.ptr, mesh.n_faces, n,
-        operators.face_normals.ptr, operators.face_areas.ptr, heat.ptr, operators.cot_entries.ptr,
-        k, neg_div.ptr, DEFAULT_STREAM,
+        operators.face_normals.ptr, operators.face_areas.ptr, heat_sol, operators.cot_entries.ptr,
+        k, poisson_rhs, DEFAULT_STREAM,
     )  # fmt: skip
-    phi = DeviceArray.empty(n * k, np.float64)
-    solver.poisson_factor.solve_pointers(neg_div.ptr, phi.ptr, k, refine)
-    _lib.call("ob_shift", phi.ptr, n, src.ptr, src.size, offsets.ptr, k, 1, DEFAULT_STREAM)
+    poisson_factor.solve_pointers(0, 0, k, refine)
+    _lib.call("ob_shift", phi, n, src.ptr, src.size, offsets.ptr, k, 1, DEFAULT_STREAM)
     if not transpose:
-        return phi.reshape(n, k)
+        out = DeviceArray.empty((n, k), np.float64)
+        _lib.call("ob_memcpy", out.ptr, phi, out.nbytes, 2, DEFAULT_STREAM, 0)
+        return out
     out = DeviceArray.empty((k, n), np.float64)
-    _lib.call("ob_transpose", n, k, phi.ptr, out.ptr, DEFAULT_STREAM)
+    _lib.call("ob_transpose", n, k, phi, out.ptr, DEFAULT_STREAM)
     return out
 
 
