@@ -697,6 +697,66 @@ int grid_for(long long total) {
     return (int)std::max(1LL, std::min((total + 255) / 256, (long long)8 * sm_count()));
 }
 
+// The whole solve on the factor's own buffers: SOL = A^-1 RHS plus `refine` refinement steps.
+int enqueue_solve(Factor* F, int k, int refine, const int* offsets, const int* columns,
+                  const double* values, cudaStream_t stream) {
+    const int n = F->n;
+    const int grid = grid_for((long long)n * k);
+    permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->pinned, F->RHS, F->B);
+    OB_CHECK_LAUNCH("chol permute in");
+    int st = triangular_solves(F, k, stream);
+    if (st) return st;
+    permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->X, F->SOL, 0);
+    OB_CHECK_LAUNCH("chol permute out");
+    // Iterative refinement in float64: x += A^-1 (b - A x).
+    for (int it = 0; it < refine; ++it) {
+        residual_kernel<<<grid, 256, 0, stream>>>(n, k, offsets, columns, values, F->RHS, F->SOL,
+                                                  F->R);
+        OB_CHECK_LAUNCH("chol residual");
+        permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->pinned, F->R, F->B);
+        OB_CHECK_LAUNCH("chol permute in");
+        st = triangular_solves(F, k, stream);
+        if (st) return st;
+        permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->X, F->SOL, 1);
+        OB_CHECK_LAUNCH("chol permute out");
+    }
+    return OB_OK;
+}
+
+// The recorded graph of enqueue_solve for (k, refine, operator), recorded on first use.
+int solve_graph(Factor* F, int k, int refine, const int* offsets, const int* columns,
+                const double* values, Factor::Recorded** out) {
+    for (auto& g : F->graphs)
+        if (g.k == k && g.refine == refine && g.offsets == offsets && g.columns == columns &&
+            g.values == values) {
+            *out = &g;
+            return OB_OK;
+        }
+    if (F->capture == nullptr) OB_CUDA(cudaStreamCreateWithFlags(&F->capture, cudaStreamNonBlocking));
+    // Launches are counted at each replay (the graph's kernel nodes), not at capture.
+    suppress_counting(1);
+    cudaError_t e = cudaStreamBeginCapture(F->capture, cudaStreamCaptureModeThreadLocal);
+    int st = e == cudaSuccess ? enqueue_solve(F, k, refine, offsets, columns, values, F->capture)
+                              : cuda_status(e, "ob_chol_solve: begin capture");
+    cudaGraph_t graph = nullptr;
+    if (e == cudaSuccess) e = cudaStreamEndCapture(F->capture, &graph);
+    suppress_counting(-1);
+    if (st != OB_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return st != OB_OK ? st : cuda_status(e, "ob_chol_solve: capture");
+    }
+    size_t nodes = 0;
+    cudaGraphGetNodes(graph, nullptr, &nodes);
+    cudaGraphExec_t exec;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_status(e, "ob_chol_solve: instantiate");
+    F->graphs.push_back(Factor::Recorded{k, refine, offsets, columns, values, exec, (int)nodes});
+    *out = &F->graphs.back();
+    return OB_OK;
+}
+
+
 }  // namespace
 }  // namespace ob
 
@@ -914,65 +974,6 @@ int ob_chol_nbytes(void* factor, size_t* bytes) {
 
 int ob_chol_destroy(void* factor) {
     factor_release(static_cast<Factor*>(factor));
-    return OB_OK;
-}
-
-// The whole solve on the factor's own buffers: SOL = A^-1 RHS plus `refine` refinement steps.
-int enqueue_solve(Factor* F, int k, int refine, const int* offsets, const int* columns,
-                  const double* values, cudaStream_t stream) {
-    const int n = F->n;
-    const int grid = grid_for((long long)n * k);
-    permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->pinned, F->RHS, F->B);
-    OB_CHECK_LAUNCH("chol permute in");
-    int st = triangular_solves(F, k, stream);
-    if (st) return st;
-    permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->X, F->SOL, 0);
-    OB_CHECK_LAUNCH("chol permute out");
-    // Iterative refinement in float64: x += A^-1 (b - A x).
-    for (int it = 0; it < refine; ++it) {
-        residual_kernel<<<grid, 256, 0, stream>>>(n, k, offsets, columns, values, F->RHS, F->SOL,
-                                                  F->R);
-        OB_CHECK_LAUNCH("chol residual");
-        permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->pinned, F->R, F->B);
-        OB_CHECK_LAUNCH("chol permute in");
-        st = triangular_solves(F, k, stream);
-        if (st) return st;
-        permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, F->perm, F->X, F->SOL, 1);
-        OB_CHECK_LAUNCH("chol permute out");
-    }
-    return OB_OK;
-}
-
-// The recorded graph of enqueue_solve for (k, refine, operator), recorded on first use.
-int solve_graph(Factor* F, int k, int refine, const int* offsets, const int* columns,
-                const double* values, Factor::Recorded** out) {
-    for (auto& g : F->graphs)
-        if (g.k == k && g.refine == refine && g.offsets == offsets && g.columns == columns &&
-            g.values == values) {
-            *out = &g;
-            return OB_OK;
-        }
-    if (F->capture == nullptr) OB_CUDA(cudaStreamCreateWithFlags(&F->capture, cudaStreamNonBlocking));
-    // Launches are counted at each replay (the graph's kernel nodes), not at capture.
-    suppress_counting(1);
-    cudaError_t e = cudaStreamBeginCapture(F->capture, cudaStreamCaptureModeThreadLocal);
-    int st = e == cudaSuccess ? enqueue_solve(F, k, refine, offsets, columns, values, F->capture)
-                              : cuda_status(e, "ob_chol_solve: begin capture");
-    cudaGraph_t graph = nullptr;
-    if (e == cudaSuccess) e = cudaStreamEndCapture(F->capture, &graph);
-    suppress_counting(-1);
-    if (st != OB_OK || e != cudaSuccess) {
-        if (graph) cudaGraphDestroy(graph);
-        return st != OB_OK ? st : cuda_status(e, "ob_chol_solve: capture");
-    }
-    size_t nodes = 0;
-    cudaGraphGetNodes(graph, nullptr, &nodes);
-    cudaGraphExec_t exec;
-    e = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) return cuda_status(e, "ob_chol_solve: instantiate");
-    F->graphs.push_back(Factor::Recorded{k, refine, offsets, columns, values, exec, (int)nodes});
-    *out = &F->graphs.back();
     return OB_OK;
 }
 
