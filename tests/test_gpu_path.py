@@ -68,7 +68,9 @@ def test_face_terms_and_operators(gpu, name: str) -> None:
         assert np.allclose(got, ref[key], rtol=VALUE_RTOL, atol=VALUE_RTOL * scale), key
     assert np.allclose(built.mass.numpy(), ref["mass"], rtol=1e-12)
     total, count = built.edge_sums.numpy()
-    assert total / count == pytest.approx(np.sqrt(ref["t"]), rel=1e-9)
+    # Each length is a float32 sqrt of a float32 dot (fused on the device): h agrees to a few
+    # float32 ulps averaged over the edges.
+    assert total / count == pytest.approx(np.sqrt(ref["t"]), rel=VALUE_RTOL)
 
 
 def test_golden_ico3_fixture(gpu) -> None:
