@@ -134,6 +134,17 @@ int ob_grad_div(const float* xyz, const int32_t* faces, int n_faces, int n_verti
 int ob_shift(double* phi, int n_vertices, const int32_t* sources, int n_sources,
              const int32_t* source_offsets, int n_columns, int orient, ob_stream_t stream);
 
+/* ob_shift with no device allocation (no counterpart in the reference: this is an entry point for
+ * callers that cannot let a library allocate device memory, e.g. a host runtime that owns and
+ * accounts all device memory, or a latency-critical loop that may not risk an allocation's
+ * driver call). Same arguments and result as ob_shift, at most 64 columns (more are rejected with
+ * OB_ERR_INVALID). Its scratch is a static device array of about 129 KiB that every device
+ * loading the library holds until exit, shared by every call on that device: calls whose work
+ * overlaps on the device race on it and must be ordered by the caller. The first call on each
+ * device looks the array's address up (make it before any stream capture). */
+int ob_shift_noalloc(double* phi, int n_vertices, const int32_t* sources, int n_sources,
+                     const int32_t* source_offsets, int n_columns, int orient, ob_stream_t stream);
+
 /* ---- a7/a9: preconditioned conjugate gradient ---------------------------------------------
  * Replaces ordito/linalg.py:3619 _BatchedCg with the kernels of
  * kernels/algorithms/conjugate_gradient.py (cg_matvec_dots :453, cg_update :797, settle

@@ -63,6 +63,7 @@ SIGNATURES: dict[str, list] = {
     "ob_seed": [P, I, I, P, P, P],
     "ob_grad_div": [P, P, I, I, P, P, P, P, I, P, P],
     "ob_shift": [P, I, P, I, P, I, I, P],
+    "ob_shift_noalloc": [P, I, P, I, P, I, I, P],
     "ob_pcg_create": [I, P, P, P, I, I, I, POINTER(c_void_p), P],
     "ob_pcg_destroy": [P],
     "ob_pcg_solve": [P, P, P, D, I, POINTER(c_int), POINTER(c_double), P],
