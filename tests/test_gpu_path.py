@@ -88,7 +88,11 @@ def test_heat_geodesic_matches_the_oracle(gpu, name: str, sources: list[int]) ->
     v, f = meshes.ALL[name]()
     ref = hp.heat_geodesic(v, f, np.array(sources))
     got = gheat.heat_geodesic(v, f.reshape(-1), np.array(sources, dtype=np.int32)).numpy()
-    assert rel_err(got, ref) <= DISTANCE_TOL
+    # A vertex no face references has no equation: its value is the Poisson solution's arbitrary
+    # constant (each solver picks its own) less the shift, not a distance. Compare the rest.
+    referenced = np.zeros(v.shape[0], dtype=bool)
+    referenced[f.reshape(-1)] = True
+    assert rel_err(got[referenced], ref[referenced]) <= DISTANCE_TOL
 
 
 def test_icosphere5_single_source(gpu) -> None:
