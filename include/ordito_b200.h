@@ -207,7 +207,8 @@ int ob_spmv(int n, const int32_t* offsets, const int32_t* columns, const double*
  * Replaces ordito.cholesky (SparseCholesky :121, sparse_cholesky :538, _analyse :881, _factor
  * :1399, _Solve :1606) behind linalg.OperatorFactorization (ordito/linalg.py:2191).
  * ob_chol_analyse: nested-dissection ordering of the pattern (geometric from xyz[n, 3] when not
- * NULL) and the supernodal structure; host work, reads the pattern back. info[0..4] = n,
+ * NULL; dissection leaves of at most leaf_size vertices, <= 0 for the default) and the supernodal
+ * structure; host work, reads the pattern back. info[0..4] = n,
  * supernodes, tree levels, factor entries, widest front.
  * ob_chol_factor: numeric factorisation of `values` over the analysed pattern; singular != 0 pins
  * the last vertex of each connected component (the Poisson system). OB_ERR_INDEFINITE on a
@@ -222,7 +223,7 @@ int ob_spmv(int n, const int32_t* offsets, const int32_t* columns, const double*
  * (CUDA events; a measurement hook). ob_chol_info: info[0..3] = n, stored values, tree levels,
  * product launches per pass. */
 int ob_chol_analyse(int n, const int32_t* offsets, const int32_t* columns, const float* xyz,
-                    void** analysis, ob_stream_t stream);
+                    int leaf_size, void** analysis, ob_stream_t stream);
 int ob_chol_analysis_info(void* analysis, long long* info);
 int ob_chol_analysis_destroy(void* analysis);
 int ob_chol_factor(void* analysis, const double* values, int singular, void** factor,
@@ -232,8 +233,8 @@ int ob_chol_nbytes(void* factor, size_t* bytes);
  * a test hook, no counterpart in the reference): x = A^-1 rhs for one column; info[0..3] as
  * ob_chol_analysis_info's first four (may be NULL). */
 int ob_chol_host_solve(int n, const int32_t* offsets, const int32_t* columns,
-                       const double* values, const float* xyz, int singular, const double* rhs,
-                       double* x, long long* info);
+                       const double* values, const float* xyz, int leaf_size, int singular,
+                       const double* rhs, double* x, long long* info);
 int ob_chol_destroy(void* factor);
 int ob_chol_solve(void* factor, const double* rhs, double* x, int n_columns, int refine,
                   const int32_t* offsets, const int32_t* columns, const double* values,

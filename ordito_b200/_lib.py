@@ -78,12 +78,12 @@ SIGNATURES: dict[str, list] = {
     "ob_fp64_peak": [POINTER(c_float), P],
     "ob_transpose": [I, I, P, P, P],
     "ob_seed_columns": [P, P, I, I, P, P, P],
-    "ob_chol_analyse": [I, P, P, P, POINTER(c_void_p), P],
+    "ob_chol_analyse": [I, P, P, P, I, POINTER(c_void_p), P],
     "ob_chol_analysis_info": [P, POINTER(ctypes.c_longlong)],
     "ob_chol_analysis_destroy": [P],
     "ob_chol_factor": [P, P, I, POINTER(c_void_p), P],
     "ob_chol_nbytes": [P, POINTER(c_size_t)],
-    "ob_chol_host_solve": [I, P, P, P, P, I, P, P, POINTER(ctypes.c_longlong)],
+    "ob_chol_host_solve": [I, P, P, P, P, I, I, P, P, POINTER(ctypes.c_longlong)],
     "ob_chol_destroy": [P],
     "ob_chol_solve": [P, P, P, I, I, P, P, P, P],
     "ob_chol_buffers": [P, I, POINTER(c_void_p), POINTER(c_void_p), P],

@@ -28,6 +28,9 @@ from ordito_b200.device import DEFAULT_STREAM, DeviceArray, device_pointer, elem
 
 CHOLESKY_MEMORY_BUDGET = 4 << 30  # ordito/cholesky.py:74
 CHOLESKY_REFINE_ROUNDS = 12  # :72
+# Vertices a nested-dissection leaf holds (ordito's CHOLESKY_LEAF_ROWS, :65, is 32 for its own
+# supernodes); each leaf is one dense front of the factor.
+CHOLESKY_LEAF_ROWS = 96
 
 
 class NotPositiveDefiniteError(ValueError):
@@ -37,14 +40,16 @@ class NotPositiveDefiniteError(ValueError):
 class CholeskyAnalysis:
     """The ordering and symbolic structure of one pattern, shareable by every operator on it."""
 
-    def __init__(self, matrix: CsrMatrix, coordinates: Any = None) -> None:
+    def __init__(self, matrix: CsrMatrix, coordinates: Any = None, leaf_size: int | None = None) -> None:
+        if leaf_size is None:
+            leaf_size = CHOLESKY_LEAF_ROWS
         handle = ctypes.c_void_p(0)
         xyz = 0
         keep = None
         if coordinates is not None:
             xyz, keep = device_pointer(coordinates, np.float32, 3 * matrix.nrow)
         _lib.call("ob_chol_analyse", matrix.nrow, matrix.offsets.ptr, matrix.columns.ptr, xyz,
-                  ctypes.byref(handle), DEFAULT_STREAM)
+                  int(leaf_size), ctypes.byref(handle), DEFAULT_STREAM)
         del keep
         self.handle = handle
         info = (ctypes.c_longlong * 5)()

@@ -28,7 +28,8 @@
 namespace ob {
 namespace {
 
-constexpr int kLeafSize = 96;
+// Vertices a dissection leaf holds when the caller asks for the default (leaf_size <= 0).
+constexpr int kDefaultLeafSize = 96;
 
 struct Node {
     int start = 0, count = 0;          // own columns [start, start + count) in the new numbering
@@ -57,12 +58,13 @@ struct Dissector {
     const std::vector<int>& off;
     const std::vector<int>& col;
     const float* xyz;  // may be null: breadth-first level bisection instead
+    int leaf_size;
     std::vector<int> side;  // scratch marks per vertex
     std::vector<Node> tree;  // built in postorder
     std::vector<int> order;  // new -> old, filled in postorder
 
-    Dissector(const std::vector<int>& o, const std::vector<int>& c, const float* p, int n)
-        : off(o), col(c), xyz(p), side(n, 0) {}
+    Dissector(const std::vector<int>& o, const std::vector<int>& c, const float* p, int n, int leaf)
+        : off(o), col(c), xyz(p), leaf_size(leaf), side(n, 0) {}
 
     // Splits `verts` into (a, b) halves: by the median of the widest coordinate, or by BFS levels.
     void bisect(std::vector<int>& verts, std::vector<int>& a, std::vector<int>& b) {
@@ -109,7 +111,7 @@ struct Dissector {
 
     // Returns the index of the node built for `verts` (postorder append).
     int dissect(std::vector<int> verts) {
-        if ((int)verts.size() <= kLeafSize) {
+        if ((int)verts.size() <= leaf_size) {
             std::sort(verts.begin(), verts.end());
             Node leaf;
             leaf.start = (int)order.size();
@@ -146,7 +148,7 @@ struct Dissector {
 };
 
 int analyse(int n, std::vector<int> offsets, std::vector<int> columns, const float* xyz,
-            Analysis* out) {
+            int leaf_size, Analysis* out) {
     Analysis& A = *out;
     A.n = n;
     A.offsets = std::move(offsets);
@@ -159,7 +161,7 @@ int analyse(int n, std::vector<int> offsets, std::vector<int> columns, const flo
             if (A.columns[e] != i) adj.push_back(A.columns[e]);
         adj_off[i + 1] = (int)adj.size();
     }
-    Dissector D(adj_off, adj, xyz, n);
+    Dissector D(adj_off, adj, xyz, n, leaf_size > 0 ? leaf_size : kDefaultLeafSize);
     std::vector<int> all(n);
     std::iota(all.begin(), all.end(), 0);
     D.dissect(std::move(all));
@@ -403,78 +405,123 @@ int numeric(const Analysis& A, const double* values, bool singular, HostFactor* 
 // ------------------------------------------------------------------------------------------
 
 // One output tile of a batched dense product: out rows [r0, r0 + rows) of a block whose matrix
-// is M (row-major, leading dimension ld, or its transpose when trans), times the K input rows.
+// is M (row-major, leading dimension ld, or its transpose when trans), times input rows
+// [k0, k1) of the inner dimension (a long inner dimension is split over several tiles).
+enum TileOp : int { kAssign = 0, kAtomicSub = 1, kSub = 2, kAtomicAdd = 3 };
+
 struct Tile {
-    long long m;       // offset of the matrix in the value buffer
-    int ld, trans;     // leading dimension; 1 when the matrix is read transposed
-    int r0, rows, K;   // output rows of the tile and the inner dimension
-    int in_base;       // input row index: in_rows == -1 -> in_base + kk, else idx[in_rows + kk]
+    long long m;     // offset of the matrix in the value buffer
+    int ld, trans;   // leading dimension; 1 when the matrix is read transposed
+    int r0, rows;    // output rows [r0, r0 + rows) of the block
+    int k0, k1;      // inner-dimension range of this tile
+    int in_base;     // input row index: in_rows == -1 -> in_base + kk, else idx[in_rows + kk]
     int in_rows;
-    int out_base;      // output row index: out_rows == -1 -> out_base + i, else idx[out_rows + i]
+    int out_base;    // output row index: out_rows == -1 -> out_base + i, else idx[out_rows + i]
     int out_rows;
+    int op;          // TileOp
 };
 
-constexpr int kTileRows = 32;
-constexpr int kTileCols = 32;
-constexpr int kTileK = 32;
+constexpr int kTileRows = 64;   // output rows per tile
+constexpr int kTileCols = 64;   // right-hand-side columns per tile
+constexpr int kTileK = 16;      // inner-dimension step staged in shared memory
+constexpr int kSplitK = 128;    // a tile's inner-dimension range at most (split beyond)
 
-// mode 0: out = M in; mode 1: out -= M in (atomic, scattered rows); mode 2: out -= M in (plain).
-template <int MODE>
-__global__ void tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
-                                    const int* __restrict__ idx, const double* __restrict__ in,
-                                    double* __restrict__ out, int k) {
-    __shared__ double sm[kTileRows][kTileK + 1];
-    __shared__ double sx[kTileK][kTileCols + 1];
+// 256 threads as a 16 x 16 grid, each accumulating a 4 x 4 register block of the 64 x 64 output
+// tile: per inner step four matrix and four input values (two 16-byte shared loads each) feed
+// sixteen FMAs. Both operands are staged with coalesced global loads (row-major and transposed
+// matrices alike), and the output is assigned, subtracted, or added atomically per the tile's op.
+__global__ void __launch_bounds__(256)
+tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
+                    const int* __restrict__ idx, const double* __restrict__ in,
+                    double* __restrict__ out, int k) {
+    __shared__ __align__(16) double sa[kTileK][kTileRows + 2];
+    __shared__ __align__(16) double sb[kTileK][kTileCols + 2];
     const Tile t = tiles[blockIdx.x];
     const int c0 = blockIdx.y * kTileCols;
-    const int tx = threadIdx.x % kTileCols;  // column within the tile
-    const int ty = threadIdx.x / kTileCols;  // 8 row groups
-    double acc[kTileRows / 8];
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    double acc[4][4];
 #pragma unroll
-    for (int q = 0; q < kTileRows / 8; ++q) acc[q] = 0.0;
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
     const double* M = vals + t.m;
-    for (int k0 = 0; k0 < t.K; k0 += kTileK) {
-        for (int e = threadIdx.x; e < kTileRows * kTileK; e += blockDim.x) {
-            const int i = e / kTileK, kk = e % kTileK;
-            const int row = t.r0 + i, col = k0 + kk;
+    for (int kb = t.k0; kb < t.k1; kb += kTileK) {
+#pragma unroll
+        for (int q = 0; q < (kTileRows * kTileK) / 256; ++q) {
+            const int e = threadIdx.x + q * 256;
+            int i, kk;
+            if (t.trans) {
+                i = e % kTileRows;
+                kk = e / kTileRows;
+            } else {
+                i = e / kTileK;
+                kk = e % kTileK;
+            }
+            const int row = t.r0 + i, col = kb + kk;
             double v = 0.0;
-            if (i < t.rows && col < t.K)
+            if (i < t.rows && col < t.k1)
                 v = t.trans ? M[(size_t)col * t.ld + row] : M[(size_t)row * t.ld + col];
-            sm[i][kk] = v;
+            sa[kk][i] = v;
         }
-        for (int e = threadIdx.x; e < kTileK * kTileCols; e += blockDim.x) {
+#pragma unroll
+        for (int q = 0; q < (kTileK * kTileCols) / 256; ++q) {
+            const int e = threadIdx.x + q * 256;
             const int kk = e / kTileCols, c = e % kTileCols;
-            const int col = k0 + kk;
+            const int col = kb + kk;
             double v = 0.0;
-            if (col < t.K && c0 + c < k) {
+            if (col < t.k1 && c0 + c < k) {
                 const int r = t.in_rows < 0 ? t.in_base + col : idx[t.in_rows + col];
                 v = in[(size_t)r * k + c0 + c];
             }
-            sx[kk][c] = v;
+            sb[kk][c] = v;
         }
         __syncthreads();
-#pragma unroll 8
+#pragma unroll
         for (int kk = 0; kk < kTileK; ++kk) {
-            const double x = sx[kk][tx];
+            const double2 a01 = *reinterpret_cast<const double2*>(&sa[kk][4 * ty]);
+            const double2 a23 = *reinterpret_cast<const double2*>(&sa[kk][4 * ty + 2]);
+            const double2 b01 = *reinterpret_cast<const double2*>(&sb[kk][4 * tx]);
+            const double2 b23 = *reinterpret_cast<const double2*>(&sb[kk][4 * tx + 2]);
+            const double a[4] = {a01.x, a01.y, a23.x, a23.y};
+            const double b[4] = {b01.x, b01.y, b23.x, b23.y};
 #pragma unroll
-            for (int q = 0; q < kTileRows / 8; ++q) acc[q] = fma(sm[ty + 8 * q][kk], x, acc[q]);
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
         }
         __syncthreads();
     }
-    if (c0 + tx >= k) return;
 #pragma unroll
-    for (int q = 0; q < kTileRows / 8; ++q) {
-        const int i = ty + 8 * q;
-        if (i >= t.rows) continue;
-        const int r = t.out_rows < 0 ? t.out_base + t.r0 + i : idx[t.out_rows + t.r0 + i];
-        double* o = out + (size_t)r * k + c0 + tx;
-        if (MODE == 0)
-            *o = acc[q];
-        else if (MODE == 1)
-            atomicAdd(o, -acc[q]);
-        else
-            *o -= acc[q];
+    for (int i = 0; i < 4; ++i) {
+        const int local = 4 * ty + i;
+        if (local >= t.rows) continue;
+        const int r = t.out_rows < 0 ? t.out_base + t.r0 + local : idx[t.out_rows + t.r0 + local];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int c = c0 + 4 * tx + j;
+            if (c >= k) continue;
+            double* o = out + (size_t)r * k + c;
+            switch (t.op) {
+                case kAssign: *o = acc[i][j]; break;
+                case kAtomicSub: atomicAdd(o, -acc[i][j]); break;
+                case kSub: *o -= acc[i][j]; break;
+                default: atomicAdd(o, acc[i][j]); break;
+            }
+        }
     }
+}
+
+// Zeroes rows [start, start + count) of y and x for every listed range (the outputs that split
+// tiles accumulate into atomically).
+__global__ void zero_rows_kernel(const int2* __restrict__ ranges, int n_ranges, int k,
+                                 double* __restrict__ y, double* __restrict__ x) {
+    const int2 range = ranges[blockIdx.x];
+    const long long begin = (long long)range.x * k, end = (long long)(range.x + range.y) * k;
+    for (long long t = begin + threadIdx.x; t < end; t += blockDim.x) {
+        y[t] = 0.0;
+        x[t] = 0.0;
+    }
+    (void)n_ranges;
 }
 
 // Gathers rows of x (old numbering) into the factor's numbering, zeroing pinned rows; or
@@ -531,6 +578,8 @@ struct Factor {
     std::vector<Tile*> fwd_diag, fwd_off, bwd_off, bwd_diag;
     std::vector<int> n_fwd_diag, n_fwd_off, n_bwd_off, n_bwd_diag;
     std::vector<void*> owned;
+    int2* zero = nullptr;  // row ranges split tiles accumulate into (zeroed each pass)
+    int n_zero = 0;
     // Work buffers sized for `cap_k` columns: B, Y, X in the factor's numbering, R the residual,
     // RHS / SOL the caller's right-hand side and solution copied in / out (old numbering).
     int cap_k = 0;
@@ -599,29 +648,53 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
     OB_CUDA(cudaMemcpyAsync(F->perm, A.perm.data(), sizeof(int) * A.n, cudaMemcpyHostToDevice,
                             stream));
     OB_CUDA(cudaMemcpyAsync(F->pinned, H.pinned.data(), A.n, cudaMemcpyHostToDevice, stream));
-    // Tiles per level and phase.
+    // Tiles per level and phase; an inner dimension beyond kSplitK is split over several tiles,
+    // which then accumulate atomically (into rows zeroed at the start of each pass).
     const int L = A.levels;
     std::vector<std::vector<Tile>> fd(L), fo(L), bo(L), bd(L);
+    std::vector<int2> zero_ranges;
+    auto emit = [](std::vector<Tile>& list, Tile t, int K, int whole_op, int split_op) {
+        const bool split = K > kSplitK + kSplitK / 2;
+        for (int k0 = 0; k0 < K; k0 += split ? kSplitK : K) {
+            t.k0 = k0;
+            t.k1 = split ? std::min(K, k0 + kSplitK) : K;
+            t.op = split ? split_op : whole_op;
+            list.push_back(t);
+        }
+        return split;
+    };
     for (int s = 0; s < ns; ++s) {
         const Node& nd = A.nodes[s];
         const int nc = nd.count, noff = (int)nd.off_rows.size();
         if (nc == 0) continue;
+        bool zero = false;
         for (int r0 = 0; r0 < nc; r0 += kTileRows) {
             const int rows = std::min(kTileRows, nc - r0);
             // Forward diagonal: Y[own] = inv B[own].
-            fd[nd.level].push_back(Tile{inv_at[s], nc, 0, r0, rows, nc, nd.start, -1, nd.start, -1});
+            zero |= emit(fd[nd.level], Tile{inv_at[s], nc, 0, r0, rows, 0, 0, nd.start, -1, nd.start, -1, 0},
+                         nc, kAssign, kAtomicAdd);
             // Backward diagonal: X[own] = inv^T Z[own].
-            bd[nd.level].push_back(Tile{inv_at[s], nc, 1, r0, rows, nc, nd.start, -1, nd.start, -1});
+            emit(bd[nd.level], Tile{inv_at[s], nc, 1, r0, rows, 0, 0, nd.start, -1, nd.start, -1, 0},
+                 nc, kAssign, kAtomicAdd);
             // Backward off-diagonal: Z[own] -= L21^T X[off rows].
             if (noff > 0)
-                bo[nd.level].push_back(
-                    Tile{off_at[s], nc, 1, r0, rows, noff, 0, rows_at[s], nd.start, -1});
+                emit(bo[nd.level], Tile{off_at[s], nc, 1, r0, rows, 0, 0, 0, rows_at[s], nd.start, -1, 0},
+                     noff, kSub, kAtomicSub);
         }
+        if (zero) zero_ranges.push_back(make_int2(nd.start, nc));
         for (int r0 = 0; r0 < noff; r0 += kTileRows) {
             const int rows = std::min(kTileRows, noff - r0);
             // Forward off-diagonal: B[off rows] -= L21 Y[own].
-            fo[nd.level].push_back(Tile{off_at[s], nc, 0, r0, rows, nc, nd.start, -1, 0, rows_at[s]});
+            emit(fo[nd.level], Tile{off_at[s], nc, 0, r0, rows, 0, 0, nd.start, -1, 0, rows_at[s], 0},
+                 nc, kAtomicSub, kAtomicSub);
         }
+    }
+    F->n_zero = (int)zero_ranges.size();
+    if (F->n_zero > 0) {
+        st = dev_alloc(F, (void**)&F->zero, sizeof(int2) * zero_ranges.size(), stream);
+        if (st) return st;
+        OB_CUDA(cudaMemcpyAsync(F->zero, zero_ranges.data(), sizeof(int2) * zero_ranges.size(),
+                                cudaMemcpyHostToDevice, stream));
     }
     auto push = [&](std::vector<std::vector<Tile>>& lists, std::vector<Tile*>& dst,
                     std::vector<int>& counts) -> int {
@@ -666,26 +739,30 @@ int triangular_solves(Factor* F, int k, cudaStream_t stream) {
     const int L = F->analysis->levels;
     const dim3 threads(256);
     const int ct = (k + kTileCols - 1) / kTileCols;
+    if (F->n_zero > 0) {
+        zero_rows_kernel<<<F->n_zero, 256, 0, stream>>>(F->zero, F->n_zero, k, F->Y, F->X);
+        OB_CHECK_LAUNCH("chol zero split rows");
+    }
     for (int l = 0; l < L; ++l) {
         if (F->n_fwd_diag[l]) {
-            tile_product_kernel<0><<<dim3(F->n_fwd_diag[l], ct), threads, 0, stream>>>(
+            tile_product_kernel<<<dim3(F->n_fwd_diag[l], ct), threads, 0, stream>>>(
                 F->fwd_diag[l], F->vals, F->idx, F->B, F->Y, k);
             OB_CHECK_LAUNCH("chol forward diagonal");
         }
         if (F->n_fwd_off[l]) {
-            tile_product_kernel<1><<<dim3(F->n_fwd_off[l], ct), threads, 0, stream>>>(
+            tile_product_kernel<<<dim3(F->n_fwd_off[l], ct), threads, 0, stream>>>(
                 F->fwd_off[l], F->vals, F->idx, F->Y, F->B, k);
             OB_CHECK_LAUNCH("chol forward update");
         }
     }
     for (int l = L - 1; l >= 0; --l) {
         if (F->n_bwd_off[l]) {
-            tile_product_kernel<2><<<dim3(F->n_bwd_off[l], ct), threads, 0, stream>>>(
+            tile_product_kernel<<<dim3(F->n_bwd_off[l], ct), threads, 0, stream>>>(
                 F->bwd_off[l], F->vals, F->idx, F->X, F->Y, k);
             OB_CHECK_LAUNCH("chol backward gather");
         }
         if (F->n_bwd_diag[l]) {
-            tile_product_kernel<0><<<dim3(F->n_bwd_diag[l], ct), threads, 0, stream>>>(
+            tile_product_kernel<<<dim3(F->n_bwd_diag[l], ct), threads, 0, stream>>>(
                 F->bwd_diag[l], F->vals, F->idx, F->Y, F->X, k);
             OB_CHECK_LAUNCH("chol backward diagonal");
         }
@@ -765,7 +842,7 @@ using namespace ob;
 extern "C" {
 
 int ob_chol_analyse(int n, const int32_t* offsets, const int32_t* columns, const float* xyz,
-                    void** analysis, ob_stream_t stream_) {
+                    int leaf_size, void** analysis, ob_stream_t stream_) {
     cudaStream_t stream = as_stream(stream_);
     OB_REQUIRE(analysis != nullptr, "ob_chol_analyse: null output");
     *analysis = nullptr;
@@ -786,7 +863,7 @@ int ob_chol_analyse(int n, const int32_t* offsets, const int32_t* columns, const
     OB_CUDA(cudaStreamSynchronize(stream));
     col.resize(off[n]);
     Analysis* A = new Analysis();
-    int st = analyse(n, std::move(off), std::move(col), xyz ? pts.data() : nullptr, A);
+    int st = analyse(n, std::move(off), std::move(col), xyz ? pts.data() : nullptr, leaf_size, A);
     if (st) {
         delete A;
         return st;
@@ -913,12 +990,13 @@ int ob_chol_info(void* factor, long long* info) {
 }
 
 int ob_chol_host_solve(int n, const int32_t* offsets, const int32_t* columns,
-                       const double* values, const float* xyz, int singular, const double* rhs,
+                       const double* values, const float* xyz, int leaf_size, int singular,
+                       const double* rhs,
                        double* x, long long* info) {
     OB_REQUIRE(n >= 1 && offsets && columns && values && rhs && x, "ob_chol_host_solve: bad argument");
     std::vector<int> off(offsets, offsets + n + 1), col(columns, columns + offsets[n]);
     Analysis A;
-    int st = analyse(n, std::move(off), std::move(col), xyz, &A);
+    int st = analyse(n, std::move(off), std::move(col), xyz, leaf_size, &A);
     if (st) return st;
     HostFactor H;
     st = numeric(A, values, singular != 0, &H);

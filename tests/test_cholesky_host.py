@@ -13,7 +13,7 @@ from ordito_b200 import _lib, creation
 from tests import meshes
 
 
-def host_solve(pattern, values, vertices, singular, rhs, coordinates=True):
+def host_solve(pattern, values, vertices, singular, rhs, coordinates=True, leaf_size=0):
     n = pattern["offsets"].size - 1
     off = np.ascontiguousarray(pattern["offsets"], dtype=np.int32)
     col = np.ascontiguousarray(pattern["columns"], dtype=np.int32)
@@ -23,8 +23,8 @@ def host_solve(pattern, values, vertices, singular, rhs, coordinates=True):
     x = np.zeros(n)
     info = (ctypes.c_longlong * 4)()
     _lib.call("ob_chol_host_solve", n, off.ctypes.data, col.ctypes.data, val.ctypes.data,
-              xyz.ctypes.data if coordinates else None, int(singular), b.ctypes.data,
-              x.ctypes.data, info)
+              xyz.ctypes.data if coordinates else None, int(leaf_size), int(singular),
+              b.ctypes.data, x.ctypes.data, info)
     return x, [int(i) for i in info]
 
 
