@@ -225,6 +225,12 @@ int ob_spmv(int n, const int32_t* offsets, const int32_t* columns, const double*
 int ob_chol_analyse(int n, const int32_t* offsets, const int32_t* columns, const float* xyz,
                     int leaf_size, void** analysis, ob_stream_t stream);
 int ob_chol_analysis_info(void* analysis, long long* info);
+/* The same analysis from host arrays (no device), and the supernodes of an analysis as
+ * out[4 s .. 4 s + 3] = (tree level, own columns, off-diagonal rows, parent or -1), postorder.
+ * Inspection hooks (no counterpart in the reference). */
+int ob_chol_host_analyse(int n, const int32_t* offsets, const int32_t* columns, const float* xyz,
+                         int leaf_size, void** analysis);
+int ob_chol_analysis_nodes(void* analysis, int32_t* out);
 int ob_chol_analysis_destroy(void* analysis);
 int ob_chol_factor(void* analysis, const double* values, int singular, void** factor,
                    ob_stream_t stream);

@@ -80,6 +80,8 @@ SIGNATURES: dict[str, list] = {
     "ob_seed_columns": [P, P, I, I, P, P, P],
     "ob_chol_analyse": [I, P, P, P, I, POINTER(c_void_p), P],
     "ob_chol_analysis_info": [P, POINTER(ctypes.c_longlong)],
+    "ob_chol_host_analyse": [I, P, P, P, I, POINTER(c_void_p)],
+    "ob_chol_analysis_nodes": [P, P],
     "ob_chol_analysis_destroy": [P],
     "ob_chol_factor": [P, P, I, POINTER(c_void_p), P],
     "ob_chol_nbytes": [P, POINTER(c_size_t)],

@@ -424,31 +424,49 @@ struct Tile {
 constexpr int kTileRows = 64;   // output rows per tile
 constexpr int kTileCols = 64;   // right-hand-side columns per tile
 constexpr int kTileK = 16;      // inner-dimension step staged in shared memory
-constexpr int kSplitK = 128;    // a tile's inner-dimension range at most (split beyond)
+constexpr int kSplitK = 64;     // a tile's inner-dimension range at most (split beyond)
+constexpr int kTileThreads = 128;
+// Shared rows of 72 doubles: the 8 x 4 fragment loads of a warp then touch every 8-byte bank
+// pair exactly twice (the minimum for 256 bytes).
+constexpr int kLd = kTileCols + 8;
 
-// 256 threads as a 16 x 16 grid, each accumulating a 4 x 4 register block of the 64 x 64 output
-// tile: per inner step four matrix and four input values (two 16-byte shared loads each) feed
-// sixteen FMAs. Both operands are staged with coalesced global loads (row-major and transposed
-// matrices alike), and the output is assigned, subtracted, or added atomically per the tile's op.
-__global__ void __launch_bounds__(256)
+// D (8 x 8) += A (8 x 4) B (4 x 8) in float64 on the tensor cores (mma.sync m8n8k4 .f64, the
+// float64 matrix instruction sm_100 offers). Fragments: a = A[lane / 4][lane % 4],
+// b = B[lane % 4][lane / 4], d = D[lane / 4][2 (lane % 4) + {0, 1}].
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// One 64 x 64 output tile per CTA of four warps, each warp a 32 x 32 quadrant as 4 x 4 float64
+// MMA tiles. The tile's matrix rows and gathered input rows are staged 16 inner steps at a time
+// in shared memory (coalesced global loads for row-major and transposed matrices alike), the next
+// stage prefetched into registers while the current one is multiplied. The output is assigned,
+// subtracted, or added atomically per the tile's op.
+__global__ void __launch_bounds__(kTileThreads)
 tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
                     const int* __restrict__ idx, const double* __restrict__ in,
                     double* __restrict__ out, int k) {
-    __shared__ __align__(16) double sa[kTileK][kTileRows + 2];
-    __shared__ __align__(16) double sb[kTileK][kTileCols + 2];
+    __shared__ __align__(16) double sa[kTileK][kLd];
+    __shared__ __align__(16) double sb[kTileK][kLd];
     const Tile t = tiles[blockIdx.x];
     const int c0 = blockIdx.y * kTileCols;
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    double acc[4][4];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;  // the warp's quadrant
+    const int fr = lane >> 2, fk = lane & 3;                 // fragment coordinates
+    double acc[4][4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     const double* M = vals + t.m;
-    for (int kb = t.k0; kb < t.k1; kb += kTileK) {
+    constexpr int kPer = kTileRows * kTileK / kTileThreads;  // 8 values of each operand a thread
+    double ra[kPer], rb[kPer];
+    auto load = [&](int kb) {
 #pragma unroll
-        for (int q = 0; q < (kTileRows * kTileK) / 256; ++q) {
-            const int e = threadIdx.x + q * 256;
+        for (int q = 0; q < kPer; ++q) {
+            const int e = threadIdx.x + q * kTileThreads;
             int i, kk;
             if (t.trans) {
                 i = e % kTileRows;
@@ -461,53 +479,67 @@ tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ v
             double v = 0.0;
             if (i < t.rows && col < t.k1)
                 v = t.trans ? M[(size_t)col * t.ld + row] : M[(size_t)row * t.ld + col];
-            sa[kk][i] = v;
-        }
-#pragma unroll
-        for (int q = 0; q < (kTileK * kTileCols) / 256; ++q) {
-            const int e = threadIdx.x + q * 256;
-            const int kk = e / kTileCols, c = e % kTileCols;
-            const int col = kb + kk;
-            double v = 0.0;
-            if (col < t.k1 && c0 + c < k) {
-                const int r = t.in_rows < 0 ? t.in_base + col : idx[t.in_rows + col];
-                v = in[(size_t)r * k + c0 + c];
+            ra[q] = v;
+            const int kb2 = e / kTileCols, c = e % kTileCols;
+            const int col2 = kb + kb2;
+            double x = 0.0;
+            if (col2 < t.k1 && c0 + c < k) {
+                const int r = t.in_rows < 0 ? t.in_base + col2 : idx[t.in_rows + col2];
+                x = in[(size_t)r * k + c0 + c];
             }
-            sb[kk][c] = v;
+            rb[q] = x;
         }
-        __syncthreads();
+    };
+    auto store = [&]() {
 #pragma unroll
-        for (int kk = 0; kk < kTileK; ++kk) {
-            const double2 a01 = *reinterpret_cast<const double2*>(&sa[kk][4 * ty]);
-            const double2 a23 = *reinterpret_cast<const double2*>(&sa[kk][4 * ty + 2]);
-            const double2 b01 = *reinterpret_cast<const double2*>(&sb[kk][4 * tx]);
-            const double2 b23 = *reinterpret_cast<const double2*>(&sb[kk][4 * tx + 2]);
-            const double a[4] = {a01.x, a01.y, a23.x, a23.y};
-            const double b[4] = {b01.x, b01.y, b23.x, b23.y};
+        for (int q = 0; q < kPer; ++q) {
+            const int e = threadIdx.x + q * kTileThreads;
+            if (t.trans)
+                sa[e / kTileRows][e % kTileRows] = ra[q];
+            else
+                sa[e % kTileK][e / kTileK] = ra[q];
+            sb[e / kTileCols][e % kTileCols] = rb[q];
+        }
+    };
+    load(t.k0);
+    for (int kb = t.k0; kb < t.k1; kb += kTileK) {
+        store();
+        __syncthreads();
+        if (kb + kTileK < t.k1) load(kb + kTileK);
+#pragma unroll
+        for (int k4 = 0; k4 < kTileK; k4 += 4) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = sa[k4 + fk][wr + 8 * i + fr];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = sb[k4 + fk][wc + 8 * j + fr];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+                for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
         }
         __syncthreads();
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const int local = 4 * ty + i;
+        const int local = wr + 8 * i + fr;
         if (local >= t.rows) continue;
         const int r = t.out_rows < 0 ? t.out_base + t.r0 + local : idx[t.out_rows + t.r0 + local];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int c = c0 + 4 * tx + j;
-            if (c >= k) continue;
-            double* o = out + (size_t)r * k + c;
-            switch (t.op) {
-                case kAssign: *o = acc[i][j]; break;
-                case kAtomicSub: atomicAdd(o, -acc[i][j]); break;
-                case kSub: *o -= acc[i][j]; break;
-                default: atomicAdd(o, acc[i][j]); break;
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int c = c0 + wc + 8 * j + 2 * fk + h;
+                if (c >= k) continue;
+                double* o = out + (size_t)r * k + c;
+                const double v = acc[i][j][h];
+                switch (t.op) {
+                    case kAssign: *o = v; break;
+                    case kAtomicSub: atomicAdd(o, -v); break;
+                    case kSub: *o -= v; break;
+                    default: atomicAdd(o, v); break;
+                }
             }
-        }
     }
 }
 
@@ -737,7 +769,7 @@ int ensure_work(Factor* F, int k, cudaStream_t stream) {
 // x_new = A^-1 b_new in the factor's numbering (B is consumed).
 int triangular_solves(Factor* F, int k, cudaStream_t stream) {
     const int L = F->analysis->levels;
-    const dim3 threads(256);
+    const dim3 threads(kTileThreads);
     const int ct = (k + kTileCols - 1) / kTileCols;
     if (F->n_zero > 0) {
         zero_rows_kernel<<<F->n_zero, 256, 0, stream>>>(F->zero, F->n_zero, k, F->Y, F->X);
@@ -869,6 +901,33 @@ int ob_chol_analyse(int n, const int32_t* offsets, const int32_t* columns, const
         return st;
     }
     *analysis = A;
+    return OB_OK;
+}
+
+int ob_chol_host_analyse(int n, const int32_t* offsets, const int32_t* columns, const float* xyz,
+                         int leaf_size, void** analysis) {
+    OB_REQUIRE(analysis != nullptr && n >= 1 && offsets && columns, "ob_chol_host_analyse: bad argument");
+    *analysis = nullptr;
+    std::vector<int> off(offsets, offsets + n + 1), col(columns, columns + offsets[n]);
+    Analysis* A = new Analysis();
+    int st = analyse(n, std::move(off), std::move(col), xyz, leaf_size, A);
+    if (st) {
+        delete A;
+        return st;
+    }
+    *analysis = A;
+    return OB_OK;
+}
+
+int ob_chol_analysis_nodes(void* analysis, int32_t* out) {
+    OB_REQUIRE(analysis && out, "ob_chol_analysis_nodes: bad argument");
+    const Analysis* A = static_cast<Analysis*>(analysis);
+    for (size_t s = 0; s < A->nodes.size(); ++s) {
+        out[4 * s] = A->nodes[s].level;
+        out[4 * s + 1] = A->nodes[s].count;
+        out[4 * s + 2] = (int)A->nodes[s].off_rows.size();
+        out[4 * s + 3] = A->nodes[s].parent;
+    }
     return OB_OK;
 }
 
