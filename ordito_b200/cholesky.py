@@ -30,7 +30,7 @@ CHOLESKY_MEMORY_BUDGET = 4 << 30  # ordito/cholesky.py:74
 CHOLESKY_REFINE_ROUNDS = 12  # :72
 # Vertices a nested-dissection leaf holds (ordito's CHOLESKY_LEAF_ROWS, :65, is 32 for its own
 # supernodes); each leaf is one dense front of the factor.
-CHOLESKY_LEAF_ROWS = 96
+CHOLESKY_LEAF_ROWS = 64
 
 
 class NotPositiveDefiniteError(ValueError):
