@@ -247,6 +247,44 @@ int ob_chol_solve(void* factor, const double* rhs, double* x, int n_columns, int
                   ob_stream_t stream);
 int ob_chol_buffers(void* factor, int n_columns, double** rhs, double** solution,
                     ob_stream_t stream);
+/* The factor's internal buffers in its own numbering, for pipelines that stay in it: rhs (B) and
+ * solution (X) hold row i of the factor's ordering at i * stride (stride = n_columns rounded up
+ * to even; a pad column must be zero), iperm maps a vertex to its row, pinned marks the rows
+ * whose right-hand side must be zero. ob_chol_solve_in_place: X = A^-1 B in that numbering (no
+ * permutation, no refinement), recorded once per n_columns as a CUDA graph. B is consumed. */
+int ob_chol_work(void* factor, int n_columns, double** rhs, double** solution, int* stride,
+                 const int32_t** iperm, const char** pinned, ob_stream_t stream);
+int ob_chol_solve_in_place(void* factor, int n_columns, ob_stream_t stream);
+
+/* ---- the served batch's per-query kernels (ordito_b200/csrc/ob_served.cu) ------------------
+ * ob_corner_index: each vertex's corner slots (3 f + e) in ascending order -- a stable sort of
+ * the face buffer by vertex (ordito/heat.py:3198 _corner_order) -- as corner_offsets[V + 1] and
+ * corner_slots[3 F]; workspace from ob_corner_index_workspace.
+ * ob_grad_div_gather: kernels/heat.py:658 unit_gradient_divergence gathered per vertex instead of
+ * scattered per face: out[row(v) * out_stride + c] = -div of column c's unit gradient at v,
+ * summed over v's corners in ascending slot order (no atomics; bit-reproducible), where
+ * row(v) = out_iperm[v] (or v when NULL) and u is read at u_iperm rows with stride u_stride;
+ * rows marked in out_pinned (in out's numbering, may be NULL) are written as 0, and so are the
+ * pad columns n_columns .. out_stride - 1.
+ * ob_seed_permuted: the source indicators of n_columns source sets written into a factor's
+ * right-hand side in its numbering (zeroed first; pinned rows stay 0).
+ * ob_shift_permuted: heat.py:3134 _shift_to_sources for n_columns columns of phi held in a
+ * factor's numbering (stride, iperm), written out transposed as out[c * V + v]. */
+int ob_corner_index_workspace(int n_vertices, int n_faces, size_t* bytes);
+int ob_corner_index(const int32_t* faces, int n_faces, int n_vertices, int32_t* corner_offsets,
+                    int32_t* corner_slots, void* workspace, size_t workspace_bytes,
+                    ob_stream_t stream);
+int ob_grad_div_gather(const float* xyz, const int32_t* faces, const float* normals,
+                       const float* areas, const float* cot, const int32_t* corner_offsets,
+                       const int32_t* corner_slots, int n_vertices, int n_columns, const double* u,
+                       int u_stride, const int32_t* u_iperm, double* out, int out_stride,
+                       const int32_t* out_iperm, const char* out_pinned, ob_stream_t stream);
+int ob_seed_permuted(const int32_t* sources, const int32_t* source_offsets, int n_columns,
+                     int n_vertices, const int32_t* iperm, const char* pinned, int stride,
+                     double* rhs, ob_stream_t stream);
+int ob_shift_permuted(const double* phi, int n_vertices, int stride, const int32_t* iperm,
+                      const int32_t* sources, const int32_t* source_offsets, int n_columns,
+                      int orient, double* out, ob_stream_t stream);
 int ob_chol_time_solve(void* factor, int n_columns, int reps, float* ms, ob_stream_t stream);
 int ob_chol_info(void* factor, long long* info);
 

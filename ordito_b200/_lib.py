@@ -89,6 +89,14 @@ SIGNATURES: dict[str, list] = {
     "ob_chol_destroy": [P],
     "ob_chol_solve": [P, P, P, I, I, P, P, P, P],
     "ob_chol_buffers": [P, I, POINTER(c_void_p), POINTER(c_void_p), P],
+    "ob_chol_work": [P, I, POINTER(c_void_p), POINTER(c_void_p), POINTER(c_int), POINTER(c_void_p),
+                     POINTER(c_void_p), P],
+    "ob_chol_solve_in_place": [P, I, P],
+    "ob_corner_index_workspace": [I, I, POINTER(c_size_t)],
+    "ob_corner_index": [P, I, I, P, P, P, c_size_t, P],
+    "ob_grad_div_gather": [P, P, P, P, P, P, P, I, I, P, I, P, P, I, P, P, P],
+    "ob_seed_permuted": [P, P, I, I, P, P, I, P, P],
+    "ob_shift_permuted": [P, I, I, P, P, P, I, I, P, P],
     "ob_chol_time_solve": [P, I, I, POINTER(c_float), P],
     "ob_chol_info": [P, POINTER(ctypes.c_longlong)],
 }

@@ -104,6 +104,20 @@ class SparseCholesky:
                   ctypes.byref(sol), DEFAULT_STREAM)
         return int(rhs.value), int(sol.value)
 
+    def work(self, n_columns: int) -> tuple[int, int, int, int, int]:
+        """``(B, X, stride, iperm, pinned)`` device pointers of the factor's own buffers in its
+        numbering (``ob_chol_work``), for pipelines that stay in it."""
+        b, x, iperm, pinned = (ctypes.c_void_p(0) for _ in range(4))
+        stride = ctypes.c_int(0)
+        _lib.call("ob_chol_work", self.handle, int(n_columns), ctypes.byref(b), ctypes.byref(x),
+                  ctypes.byref(stride), ctypes.byref(iperm), ctypes.byref(pinned), DEFAULT_STREAM)
+        return int(b.value), int(x.value), int(stride.value), int(iperm.value), int(pinned.value)
+
+    def solve_in_place(self, n_columns: int, stream: Any = None) -> None:
+        """``X = A^-1 B`` on the factor's own buffers, in its numbering (no read-back)."""
+        _lib.call("ob_chol_solve_in_place", self.handle, int(n_columns),
+                  stream if stream is not None else DEFAULT_STREAM)
+
     def solve_pointers(self, rhs: int, x: int, n_columns: int, refine: int, stream: Any = None) -> None:
         """``x = A^-1 rhs`` for ``n_columns`` interleaved columns ([n][n_columns]) plus ``refine``
         float64 refinement steps, all enqueued on the device (no read-back)."""

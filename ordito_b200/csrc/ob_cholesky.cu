@@ -628,6 +628,7 @@ struct Factor {
     double* vals = nullptr;  // device: all inverses and panels
     int* idx = nullptr;      // device: off-diagonal row lists
     int* perm = nullptr;     // device: new -> old
+    int* iperm = nullptr;    // device: old -> new
     char* pinned = nullptr;  // device
     long long n_vals = 0;
     // Tile lists per (direction, level, phase); host copies of counts, device tile arrays.
@@ -705,11 +706,14 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
     int st = dev_alloc(F, (void**)&F->vals, sizeof(double) * vals.size(), stream);
     if (!st) st = dev_alloc(F, (void**)&F->idx, sizeof(int) * idx.size(), stream);
     if (!st) st = dev_alloc(F, (void**)&F->perm, sizeof(int) * A.n, stream);
+    if (!st) st = dev_alloc(F, (void**)&F->iperm, sizeof(int) * A.n, stream);
     if (!st) st = dev_alloc(F, (void**)&F->pinned, std::max(A.n, 1), stream);
     if (st) return st;
     OB_CUDA(cudaMemcpyAsync(F->vals, vals.data(), sizeof(double) * vals.size(),
                             cudaMemcpyHostToDevice, stream));
     OB_CUDA(cudaMemcpyAsync(F->idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice,
+                            stream));
+    OB_CUDA(cudaMemcpyAsync(F->iperm, A.iperm.data(), sizeof(int) * A.n, cudaMemcpyHostToDevice,
                             stream));
     OB_CUDA(cudaMemcpyAsync(F->perm, A.perm.data(), sizeof(int) * A.n, cudaMemcpyHostToDevice,
                             stream));
@@ -882,8 +886,10 @@ int solve_graph(Factor* F, int k, int refine, const int* offsets, const int* col
     // Launches are counted at each replay (the graph's kernel nodes), not at capture.
     suppress_counting(1);
     cudaError_t e = cudaStreamBeginCapture(F->capture, cudaStreamCaptureModeThreadLocal);
-    int st = e == cudaSuccess ? enqueue_solve(F, k, refine, offsets, columns, values, F->capture)
-                              : cuda_status(e, "ob_chol_solve: begin capture");
+    // refine < 0 records the bare triangular passes B -> X in the factor's own numbering.
+    int st = e != cudaSuccess ? cuda_status(e, "ob_chol_solve: begin capture")
+             : refine < 0     ? triangular_solves(F, even_columns(k), F->capture)
+                              : enqueue_solve(F, k, refine, offsets, columns, values, F->capture);
     cudaGraph_t graph = nullptr;
     if (e == cudaSuccess) e = cudaStreamEndCapture(F->capture, &graph);
     suppress_counting(-1);
@@ -1034,6 +1040,35 @@ int ob_chol_solve(void* factor, const double* rhs, double* x, int n_columns, int
     count_launch((uint64_t)g->launches);
     if (x != nullptr && x != F->SOL)
         OB_CUDA(cudaMemcpyAsync(x, F->SOL, bytes, cudaMemcpyDeviceToDevice, stream));
+    return OB_OK;
+}
+
+int ob_chol_work(void* factor, int n_columns, double** rhs, double** solution, int* stride,
+                 const int32_t** iperm, const char** pinned, ob_stream_t stream_) {
+    OB_REQUIRE(factor && rhs && solution && stride && iperm && pinned && n_columns >= 1,
+               "ob_chol_work: bad argument");
+    Factor* F = static_cast<Factor*>(factor);
+    int st = ensure_work(F, n_columns, as_stream(stream_));
+    if (st) return st;
+    *rhs = F->B;
+    *solution = F->X;
+    *stride = even_columns(n_columns);
+    *iperm = F->iperm;
+    *pinned = F->pinned;
+    return OB_OK;
+}
+
+int ob_chol_solve_in_place(void* factor, int n_columns, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(factor && n_columns >= 1, "ob_chol_solve_in_place: bad argument");
+    Factor* F = static_cast<Factor*>(factor);
+    int st = ensure_work(F, n_columns, stream);
+    if (st) return st;
+    Factor::Recorded* g = nullptr;
+    st = solve_graph(F, n_columns, -1, nullptr, nullptr, nullptr, &g);
+    if (st) return st;
+    OB_CUDA(cudaGraphLaunch(g->exec, stream));
+    count_launch((uint64_t)g->launches);
     return OB_OK;
 }
 

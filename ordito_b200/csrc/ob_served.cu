@@ -1,0 +1,306 @@
+// The served batch's per-query kernels, atomic-free and in the factors' own numbering.
+//
+// A served batch solves k right-hand sides against two held Cholesky factors that share one
+// ordering (the Poisson factor reuses the heat factor's analysis). These kernels let the batch
+// stay in that ordering between the two solves: the seeds are written straight into the heat
+// factor's right-hand side, the divergence reads the heat solution and writes the Poisson
+// right-hand side through the ordering's inverse permutation, and the shift reads the Poisson
+// solution the same way while writing the (k, V) distances out -- no permutation or transpose
+// passes between them.
+//
+// The divergence is gathered per vertex rather than scattered per face (ordito/kernels/heat.py:
+// 626-687 accumulates with float64 atomics, or under its deterministic mode stores per corner
+// and sums each vertex's corners in ascending corner order, ordito/heat.py:3170-3232): each
+// (vertex, column) thread walks the vertex's corners in ascending slot order (a stable sort of
+// the face buffer by vertex, ordito/heat.py:3198 _corner_order) and recomputes each incident
+// face's unit gradient itself. No atomics, the same bits on every run, and no per-corner table.
+#include <cub/device/device_radix_sort.cuh>
+
+#include "ob_geometry.cuh"
+#include "ob_internal.cuh"
+#include "ob_scratch.cuh"
+
+namespace ob {
+namespace {
+
+constexpr int kThreads = 256;
+
+__global__ void corner_keys_kernel(const int* __restrict__ faces, int n_corners, int n,
+                                   int* __restrict__ keys, int* __restrict__ slots) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n_corners) return;
+    const int v = faces[q];
+    keys[q] = (v >= 0 && v < n) ? v : n;
+    slots[q] = q;
+}
+
+// offsets[v] = first sorted position of vertex v (every vertex, empty ones included).
+__global__ void corner_offsets_kernel(const int* __restrict__ sorted, int n_corners, int n,
+                                      int* __restrict__ offsets) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > n_corners) return;
+    const int here = p < n_corners ? sorted[p] : n;
+    const int before = p > 0 ? sorted[p - 1] : -1;
+    for (int v = before + 1; v <= here && v <= n; ++v) offsets[v] = p;
+}
+
+struct d3 {
+    double x, y, z;
+};
+__device__ __forceinline__ d3 widen(f3 a) { return d3{(double)a.x, (double)a.y, (double)a.z}; }
+__device__ __forceinline__ d3 dsub(d3 a, d3 b) { return d3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ double ddot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ d3 dcross(d3 a, d3 b) {
+    return d3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// Row of vertex v in a buffer: its own index, or its position in the factor's ordering.
+__device__ __forceinline__ int row_of(const int* __restrict__ iperm, int v) {
+    return iperm ? iperm[v] : v;
+}
+
+// -div of the unit gradient at (vertex, column), summed over the vertex's corners in ascending
+// slot order: the same arithmetic per face as ob_grad_div (kernels/triangles.py:834-894,
+// kernels/predicates.py:719-724, kernels/heat.py:626-687), the corner's own term kept.
+__global__ void grad_div_gather_kernel(const float* __restrict__ xyz, const int* __restrict__ faces,
+                                       const float* __restrict__ normals,
+                                       const float* __restrict__ areas,
+                                       const float* __restrict__ cot,
+                                       const int* __restrict__ corner_offsets,
+                                       const int* __restrict__ corner_slots, int n, int k,
+                                       const double* __restrict__ u, int u_stride,
+                                       const int* __restrict__ u_iperm, double* __restrict__ out,
+                                       int out_stride, const int* __restrict__ out_iperm,
+                                       const char* __restrict__ out_pinned) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)n * out_stride) return;
+    const int v = (int)(t / out_stride), c = (int)(t % out_stride);
+    if (c >= k) {
+        // A pad column of the output stays zero.
+        out[(size_t)row_of(out_iperm, v) * out_stride + c] = 0.0;
+        return;
+    }
+    double acc = 0.0;
+    for (int p = corner_offsets[v]; p < corner_offsets[v + 1]; ++p) {
+        const int q = corner_slots[p];
+        const int f = q / 3, e = q - 3 * f;
+        const int i0 = faces[3 * f], i1 = faces[3 * f + 1], i2 = faces[3 * f + 2];
+        const d3 v0 = widen(load_f3(xyz, i0)), v1 = widen(load_f3(xyz, i1)),
+                 v2 = widen(load_f3(xyz, i2));
+        const d3 nrm = widen(load_f3(normals, f));
+        const double area = (double)areas[f];
+        d3 g{0.0, 0.0, 0.0};
+        if (area > 0.0) {
+            const double u0 = u[(size_t)row_of(u_iperm, i0) * u_stride + c];
+            const double u1 = u[(size_t)row_of(u_iperm, i1) * u_stride + c];
+            const double u2 = u[(size_t)row_of(u_iperm, i2) * u_stride + c];
+            const d3 a = dcross(nrm, dsub(v2, v1)), b = dcross(nrm, dsub(v0, v2)),
+                     w = dcross(nrm, dsub(v1, v0));
+            const double twice = 2.0 * area;
+            g = d3{(u0 * a.x + u1 * b.x + u2 * w.x) / twice, (u0 * a.y + u1 * b.y + u2 * w.y) / twice,
+                   (u0 * a.z + u1 * b.z + u2 * w.z) / twice};
+        }
+        const double largest = fmax(fabs(g.x), fmax(fabs(g.y), fabs(g.z)));
+        d3 x{0.0, 0.0, 0.0};
+        if (largest != 0.0) {
+            const d3 s{g.x / largest, g.y / largest, g.z / largest};
+            const double len = sqrt(ddot(s, s));
+            if (len > 0.0) x = d3{s.x / len, s.y / len, s.z / len};
+        }
+        const double c0 = (double)cot[3 * f], c1 = (double)cot[3 * f + 1], c2 = (double)cot[3 * f + 2];
+        double d;
+        if (e == 0)
+            d = c2 * ddot(dsub(v1, v0), x) + c1 * ddot(dsub(v2, v0), x);
+        else if (e == 1)
+            d = c0 * ddot(dsub(v2, v1), x) + c2 * ddot(dsub(v0, v1), x);
+        else
+            d = c1 * ddot(dsub(v0, v2), x) + c0 * ddot(dsub(v1, v2), x);
+        acc += d;
+    }
+    const int row = row_of(out_iperm, v);
+    out[(size_t)row * out_stride + c] = (out_pinned && out_pinned[row]) ? 0.0 : acc;
+}
+
+// Seeds of k source sets in a factor's numbering: rhs (stride `stride`, zeroed first) gets 1 at
+// each source's row, 0 at pinned rows.
+__global__ void seed_permuted_kernel(const int* __restrict__ sources,
+                                     const int* __restrict__ source_offsets, int k,
+                                     const int* __restrict__ iperm, const char* __restrict__ pinned,
+                                     int stride, double* __restrict__ rhs) {
+    const int c = blockIdx.y;
+    for (int i = source_offsets[c] + threadIdx.x; i < source_offsets[c + 1]; i += blockDim.x) {
+        const int row = iperm[sources[i]];
+        if (!pinned[row]) rhs[(size_t)row * stride + c] = 1.0;
+    }
+}
+
+// Per column: sum of phi over the sources and over every row (block partials, last block folds).
+__global__ void shift_sums_kernel(const double* __restrict__ phi, int n, int stride,
+                                  const int* __restrict__ iperm, const int* __restrict__ sources,
+                                  const int* __restrict__ source_offsets, int k,
+                                  double2* __restrict__ partials, unsigned int* counter,
+                                  double2* __restrict__ sums) {
+    __shared__ double scratch[32];
+    __shared__ int last;
+    const int c = blockIdx.y;
+    const int s_begin = source_offsets[c], s_end = source_offsets[c + 1];
+    double at_sources = 0.0, everywhere = 0.0;
+    const int step = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < s_end - s_begin; i += step)
+        at_sources += phi[(size_t)iperm[sources[s_begin + i]] * stride + c];
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += step)
+        everywhere += phi[(size_t)r * stride + c];
+    const double a = block_sum(at_sources, scratch);
+    const double b = block_sum(everywhere, scratch);
+    if (threadIdx.x == 0) partials[(size_t)c * gridDim.x + blockIdx.x] = make_double2(a, b);
+    if (!last_block_arrived(counter, &last)) return;
+    for (int col = threadIdx.x; col < k; col += blockDim.x) {
+        double s = 0.0, g = 0.0;
+        for (int bx = 0; bx < (int)gridDim.x; ++bx) {
+            const double2 p = __ldcg(&partials[(size_t)col * gridDim.x + bx]);
+            s += p.x;
+            g += p.y;
+        }
+        sums[col] = make_double2(s, g);
+    }
+}
+
+// out[c][v] = the shifted, oriented phi of vertex v in column c (ordito/kernels/heat.py:3406).
+__global__ void shift_out_kernel(const double* __restrict__ phi, int n, int stride,
+                                 const int* __restrict__ iperm, const double2* __restrict__ sums,
+                                 const int* __restrict__ source_offsets, int k, int orient,
+                                 double* __restrict__ out) {
+    __shared__ double tile[32][33];
+    // Tile of 32 vertices x 32 columns: read along columns (a factor row), write along vertices.
+    const int v0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int v = v0 + i, c = c0 + threadIdx.x;
+        if (v < n && c < k) tile[i][threadIdx.x] = phi[(size_t)iperm[v] * stride + c];
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int c = c0 + i, v = v0 + threadIdx.x;
+        if (v >= n || c >= k) continue;
+        const int count = source_offsets[c + 1] - source_offsets[c];
+        const double2 s = sums[c];
+        const double offset = s.x / (double)count;
+        const double value = tile[threadIdx.x][i];
+        double shifted = value - offset;
+        if (orient != 0 && s.y / (double)n - offset < 0.0) shifted = offset - value;
+        out[(size_t)c * n + v] = shifted;
+    }
+}
+
+}  // namespace
+}  // namespace ob
+
+using namespace ob;
+
+extern "C" {
+
+int ob_corner_index_workspace(int n_vertices, int n_faces, size_t* bytes) {
+    OB_REQUIRE(bytes && n_vertices >= 0 && n_faces >= 0, "ob_corner_index_workspace: bad argument");
+    const int corners = 3 * n_faces;
+    size_t sort_bytes = 0;
+    if (corners > 0)
+        OB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const int*)nullptr, (int*)nullptr,
+                                                (const int*)nullptr, (int*)nullptr, corners));
+    *bytes = align_up(sort_bytes) + 3 * align_up(sizeof(int) * (size_t)std::max(corners, 1)) + 256;
+    return OB_OK;
+}
+
+int ob_corner_index(const int32_t* faces, int n_faces, int n_vertices, int32_t* corner_offsets,
+                    int32_t* corner_slots, void* workspace, size_t workspace_bytes,
+                    ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(corner_offsets && n_vertices >= 0 && n_faces >= 0, "ob_corner_index: bad argument");
+    const int corners = 3 * n_faces;
+    if (corners == 0) {
+        OB_CUDA(cudaMemsetAsync(corner_offsets, 0, sizeof(int) * (size_t)(n_vertices + 1), stream));
+        return OB_OK;
+    }
+    OB_REQUIRE(faces && corner_slots && workspace, "ob_corner_index: null pointer");
+    size_t needed = 0;
+    int st = ob_corner_index_workspace(n_vertices, n_faces, &needed);
+    if (st) return st;
+    OB_REQUIRE(workspace_bytes >= needed, "ob_corner_index: workspace of %zu bytes, %zu needed",
+               workspace_bytes, needed);
+    char* ws = reinterpret_cast<char*>(align_up(reinterpret_cast<size_t>(workspace)));
+    const size_t vec = align_up(sizeof(int) * (size_t)corners);
+    int* keys_in = reinterpret_cast<int*>(ws);
+    int* slots_in = reinterpret_cast<int*>(ws + vec);
+    int* keys_out = reinterpret_cast<int*>(ws + 2 * vec);
+    void* sort_temp = ws + 3 * vec;
+    size_t sort_bytes = workspace_bytes - 256 - 3 * vec;
+    corner_keys_kernel<<<ceil_div(corners, kThreads), kThreads, 0, stream>>>(faces, corners,
+                                                                             n_vertices, keys_in,
+                                                                             slots_in);
+    OB_CHECK_LAUNCH("corner_keys");
+    int bits = 1;
+    while ((1LL << bits) <= (long long)n_vertices) ++bits;
+    OB_CUDA(cub::DeviceRadixSort::SortPairs(sort_temp, sort_bytes, keys_in, keys_out, slots_in,
+                                            corner_slots, corners, 0, bits, stream));
+    count_launch();
+    corner_offsets_kernel<<<ceil_div(corners + 1, kThreads), kThreads, 0, stream>>>(
+        keys_out, corners, n_vertices, corner_offsets);
+    OB_CHECK_LAUNCH("corner_offsets");
+    return OB_OK;
+}
+
+int ob_grad_div_gather(const float* xyz, const int32_t* faces, const float* normals,
+                       const float* areas, const float* cot, const int32_t* corner_offsets,
+                       const int32_t* corner_slots, int n_vertices, int n_columns, const double* u,
+                       int u_stride, const int32_t* u_iperm, double* out, int out_stride,
+                       const int32_t* out_iperm, const char* out_pinned, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_vertices >= 0 && n_columns >= 1 && u_stride >= n_columns && out_stride >= n_columns,
+               "ob_grad_div_gather: bad size");
+    if (n_vertices == 0) return OB_OK;
+    OB_REQUIRE(xyz && faces && normals && areas && cot && corner_offsets && corner_slots && u && out,
+               "ob_grad_div_gather: null pointer");
+    const long long total = (long long)n_vertices * out_stride;
+    grad_div_gather_kernel<<<ceil_div(total, kThreads), kThreads, 0, stream>>>(
+        xyz, faces, normals, areas, cot, corner_offsets, corner_slots, n_vertices, n_columns, u,
+        u_stride, u_iperm, out, out_stride, out_iperm, out_pinned);
+    OB_CHECK_LAUNCH("grad_div_gather");
+    return OB_OK;
+}
+
+int ob_seed_permuted(const int32_t* sources, const int32_t* source_offsets, int n_columns,
+                     int n_vertices, const int32_t* iperm, const char* pinned, int stride,
+                     double* rhs, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_columns >= 1 && stride >= n_columns && n_vertices >= 0, "ob_seed_permuted: bad size");
+    OB_REQUIRE(sources && source_offsets && iperm && pinned && rhs, "ob_seed_permuted: null pointer");
+    OB_CUDA(cudaMemsetAsync(rhs, 0, sizeof(double) * (size_t)n_vertices * stride, stream));
+    seed_permuted_kernel<<<dim3(1, n_columns), 128, 0, stream>>>(sources, source_offsets, n_columns,
+                                                               iperm, pinned, stride, rhs);
+    OB_CHECK_LAUNCH("seed_permuted");
+    return OB_OK;
+}
+
+int ob_shift_permuted(const double* phi, int n_vertices, int stride, const int32_t* iperm,
+                      const int32_t* sources, const int32_t* source_offsets, int n_columns,
+                      int orient, double* out, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_vertices >= 1 && n_columns >= 1 && stride >= n_columns, "ob_shift_permuted: bad size");
+    OB_REQUIRE(phi && iperm && sources && source_offsets && out, "ob_shift_permuted: null pointer");
+    const int blocks = std::max(1, std::min(ceil_div(n_vertices, kThreads * 4), 2 * sm_count()));
+    Scratch scratch(stream);
+    double2* partials = scratch.take<double2>((size_t)blocks * n_columns);
+    double2* sums = scratch.take<double2>(n_columns);
+    unsigned int* counter = scratch.take<unsigned int>(1);
+    int st = scratch.commit();
+    if (st) return st;
+    OB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned int), stream));
+    shift_sums_kernel<<<dim3(blocks, n_columns), kThreads, 0, stream>>>(
+        phi, n_vertices, stride, iperm, sources, source_offsets, n_columns, partials, counter, sums);
+    OB_CHECK_LAUNCH("shift_sums");
+    shift_out_kernel<<<dim3(ceil_div(n_vertices, 32), ceil_div(n_columns, 32)), dim3(32, 8), 0,
+                       stream>>>(phi, n_vertices, stride, iperm, sums, source_offsets, n_columns,
+                                 orient, out);
+    OB_CHECK_LAUNCH("shift_out");
+    return OB_OK;
+}
+
+}  // extern "C"

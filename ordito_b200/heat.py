@@ -311,10 +311,14 @@ def _distance_from_heat(mesh: Trimesh, solver: HeatSolver, sources: DeviceArray,
     operators = solver.operators
     n = mesh.n_vertices
     neg_div = DeviceArray.empty(n * n_columns, np.float64)
+    # Gathered per vertex over its corners in ascending order: no atomics, the same bits on every
+    # run (the reference's deterministic mode, ordito/heat.py:3170-3232, as its only mode).
+    corner_offsets, corner_slots = mesh.corner_index
     _lib.call(
-        "ob_grad_div", mesh.vertices.ptr, mesh.faces.ptr, mesh.n_faces, n,
-        operators.face_normals.ptr, operators.face_areas.ptr, heat.ptr, operators.cot_entries.ptr,
-        n_columns, neg_div.ptr, DEFAULT_STREAM,
+        "ob_grad_div_gather", mesh.vertices.ptr, mesh.faces.ptr, operators.face_normals.ptr,
+        operators.face_areas.ptr, operators.cot_entries.ptr, corner_offsets.ptr, corner_slots.ptr,
+        n, n_columns, heat.ptr, n_columns, None, neg_div.ptr, n_columns, None, None,
+        DEFAULT_STREAM,
     )  # fmt: skip
     phi = DeviceArray.zeros(n * n_columns, np.float64)
     solver.solve_poisson(neg_div, phi)
@@ -375,21 +379,45 @@ def heat_geodesic_batch(
 
 def _batch_columns(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offsets: DeviceArray,
                    k: int, refine: int, transpose: bool) -> DeviceArray:
-    """The batched pass over resident, validated source columns: the seeds are written into the
-    heat factor's own right-hand side, each solve leaves its result in its factor's solution
-    buffer, and the divergence writes the Poisson factor's right-hand side -- no copies between."""
+    """The batched pass over resident, validated source columns.
+
+    Without refinement the pass stays in the factors' shared ordering from the seeds to the shift:
+    the seeds go straight into the heat factor's right-hand side, the divergence (gathered per
+    vertex, no atomics) reads the heat solution and writes the Poisson right-hand side through
+    the inverse permutation, and the shift reads the Poisson solution the same way and writes the
+    ``(k, V)`` distances -- no permutation, copy or transpose passes. With ``refine`` each solve
+    instead runs in the caller's numbering with that many float64 refinement steps.
+    """
     n = mesh.n_vertices
     heat_factor, poisson_factor = solver.heat_factor, solver.poisson_factor
+    operators = solver.operators
+    corner_offsets, corner_slots = mesh.corner_index
+    if refine == 0:
+        h_rhs, h_sol, h_stride, h_iperm, h_pinned = heat_factor.work(k)
+        p_rhs, p_sol, p_stride, p_iperm, p_pinned = poisson_factor.work(k)
+        _lib.call("ob_seed_permuted", src.ptr, offsets.ptr, k, n, h_iperm, h_pinned, h_stride,
+                  h_rhs, DEFAULT_STREAM)
+        heat_factor.solve_in_place(k)
+        _lib.call(
+            "ob_grad_div_gather", mesh.vertices.ptr, mesh.faces.ptr, operators.face_normals.ptr,
+            operators.face_areas.ptr, operators.cot_entries.ptr, corner_offsets.ptr,
+            corner_slots.ptr, n, k, h_sol, h_stride, h_iperm, p_rhs, p_stride, p_iperm, p_pinned,
+            DEFAULT_STREAM,
+        )  # fmt: skip
+        poisson_factor.solve_in_place(k)
+        out = DeviceArray.empty((k, n), np.float64)
+        _lib.call("ob_shift_permuted", p_sol, n, p_stride, p_iperm, src.ptr, offsets.ptr, k, 1,
+                  out.ptr, DEFAULT_STREAM)
+        return out if transpose else _transposed(out, k, n)
     heat_rhs, heat_sol = heat_factor.buffers(k)
     poisson_rhs, phi = poisson_factor.buffers(k)
     invalid = solver.scratch_flag()
     _lib.call("ob_seed_columns", src.ptr, offsets.ptr, k, n, heat_rhs, invalid.ptr, DEFAULT_STREAM)
     heat_factor.solve_pointers(0, 0, k, refine)
-    operators = solver.operators
     _lib.call(
-        "ob_grad_div", mesh.vertices.ptr, mesh.faces.ptr, mesh.n_faces, n,
-        operators.face_normals.ptr, operators.face_areas.ptr, heat_sol, operators.cot_entries.ptr,
-        k, poisson_rhs, DEFAULT_STREAM,
+        "ob_grad_div_gather", mesh.vertices.ptr, mesh.faces.ptr, operators.face_normals.ptr,
+        operators.face_areas.ptr, operators.cot_entries.ptr, corner_offsets.ptr, corner_slots.ptr,
+        n, k, heat_sol, k, None, poisson_rhs, k, None, None, DEFAULT_STREAM,
     )  # fmt: skip
     poisson_factor.solve_pointers(0, 0, k, refine)
     _lib.call("ob_shift", phi, n, src.ptr, src.size, offsets.ptr, k, 1, DEFAULT_STREAM)
@@ -399,6 +427,12 @@ def _batch_columns(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offset
         return out
     out = DeviceArray.empty((k, n), np.float64)
     _lib.call("ob_transpose", n, k, phi, out.ptr, DEFAULT_STREAM)
+    return out
+
+
+def _transposed(array: DeviceArray, rows: int, cols: int) -> DeviceArray:
+    out = DeviceArray.empty((cols, rows), np.float64)
+    _lib.call("ob_transpose", rows, cols, array.ptr, out.ptr, DEFAULT_STREAM)
     return out
 
 

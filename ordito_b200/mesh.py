@@ -49,6 +49,23 @@ class Trimesh:
         return self.face_terms.cot
 
     @property
+    def corner_index(self) -> tuple[DeviceArray, DeviceArray]:
+        """``(corner_offsets[V + 1], corner_slots[3 F])``: each vertex's corners in ascending slot
+        order (a stable sort of the face buffer; ordito/heat.py:3198 ``_corner_order``)."""
+        if getattr(self, "_corner_index", None) is None:
+            import ctypes
+
+            offsets = DeviceArray.empty(self.n_vertices + 1, np.int32)
+            slots = DeviceArray.empty(max(3 * self.n_faces, 1), np.int32)
+            size = ctypes.c_size_t(0)
+            _lib.call("ob_corner_index_workspace", self.n_vertices, self.n_faces, ctypes.byref(size))
+            workspace = DeviceArray.empty(int(size.value), np.uint8)
+            _lib.call("ob_corner_index", self.faces.ptr, self.n_faces, self.n_vertices, offsets.ptr,
+                      slots.ptr, workspace.ptr, int(size.value), DEFAULT_STREAM)
+            self._corner_index = (offsets, slots)
+        return self._corner_index
+
+    @property
     def mean_edge_length(self) -> float:
         """Mean over all ``3 n_faces`` per-face edges (ordito/mesh.py:1179), read back once."""
         if self._mean_edge_length is None:

@@ -91,3 +91,60 @@ def test_full_size_torus_single_query(gpu) -> None:
     got = gheat.heat_geodesic(v, f.reshape(-1), src).numpy()
     ref = hp.heat_geodesic(v, f, src)
     assert hp.relative_linf(got, ref) <= DISTANCE_TOL
+
+
+@pytest.mark.parametrize("name", ["ico3", "bumpy_sphere", "unreferenced", "degenerate"])
+def test_corner_index_is_the_stable_sort_of_the_faces(gpu, name: str) -> None:
+    v, f = meshes.ALL[name]()
+    mesh = Trimesh(v, f.reshape(-1))
+    offsets, slots = mesh.corner_index
+    flat = f.reshape(-1)
+    order = np.argsort(flat, kind="stable")
+    expected_offsets = np.searchsorted(flat[order], np.arange(v.shape[0] + 1))
+    assert np.array_equal(offsets.numpy(), expected_offsets)
+    assert np.array_equal(slots.numpy()[: flat.size], order)
+
+
+@pytest.mark.parametrize("k", [1, 3, 64])
+def test_gathered_divergence_matches_the_scattered_one_and_repeats_bit_for_bit(gpu, k: int) -> None:
+    from ordito_b200 import _lib
+
+    v, f = meshes.bumpy_sphere()
+    n = v.shape[0]
+    mesh = Trimesh(v, f.reshape(-1))
+    terms = mesh.face_terms
+    rng = np.random.default_rng(k)
+    u = DeviceArray.from_host(np.exp(-5.0 * rng.random((n, k))).reshape(-1))
+    scattered = DeviceArray.empty(n * k, np.float64)
+    _lib.call("ob_grad_div", mesh.vertices.ptr, mesh.faces.ptr, mesh.n_faces, n, terms.normals.ptr,
+              terms.areas.ptr, u.ptr, terms.cot.ptr, k, scattered.ptr, None)
+    offsets, slots = mesh.corner_index
+    gathered = [DeviceArray.empty(n * k, np.float64) for _ in range(2)]
+    for out in gathered:
+        _lib.call("ob_grad_div_gather", mesh.vertices.ptr, mesh.faces.ptr, terms.normals.ptr,
+                  terms.areas.ptr, terms.cot.ptr, offsets.ptr, slots.ptr, n, k, u.ptr, k, None,
+                  out.ptr, k, None, None, None)
+    a, b, c = scattered.numpy(), gathered[0].numpy(), gathered[1].numpy()
+    assert np.array_equal(b, c)
+    assert np.allclose(b, a, rtol=1e-12, atol=1e-12 * np.abs(a).max())
+
+
+@pytest.mark.parametrize("refine", [0, 1])
+def test_batched_modes_agree_and_repeat(gpu, refine: int) -> None:
+    v, f = meshes.small_torus()
+    n = v.shape[0]
+    rng = np.random.default_rng(3)
+    sets = [rng.choice(n, size=int(s), replace=False) for s in rng.integers(1, 4, size=7)]
+    mesh = Trimesh(v, f.reshape(-1))
+    first = gheat.heat_geodesic_batch(mesh, sets, refine=refine).numpy()
+    again = gheat.heat_geodesic_batch(mesh, sets, refine=refine).numpy()
+    assert np.array_equal(first, again) or hp.relative_linf(again, first) <= 1e-12
+    t_eff, _ = hp.vertex_time(v, f, None)
+    ops = hp.heat_operators(v, f, t_eff)
+    factors = (hp.HeatFactor(hp.csr_matrix(ops["pattern"], ops["H"])),
+               hp.PoissonFactor(hp.csr_matrix(ops["pattern"], ops["P"])))
+    for c, s in enumerate(sets):
+        ref = hp.heat_geodesic(v, f, s, operators=ops, factors=factors)
+        assert hp.relative_linf(first[c], ref) <= DISTANCE_TOL
+    untransposed = gheat.heat_geodesic_batch(mesh, sets, refine=refine, transpose=False).numpy()
+    assert np.allclose(untransposed.T, first, rtol=0, atol=1e-12 * np.abs(first).max())
