@@ -89,6 +89,8 @@ __global__ void grad_div_gather_kernel(const float* __restrict__ xyz, const int*
                  v2 = widen(load_f3(xyz, i2));
         const d3 nrm = widen(load_f3(normals, f));
         const double area = (double)areas[f];
+        // The unnormalised gradient sum_k u_k (n x e_k); its direction is the unit gradient's, and
+        // the positive factor 1 / (2 A) cancels in the normalisation, so it is never divided in.
         d3 g{0.0, 0.0, 0.0};
         if (area > 0.0) {
             const double u0 = u[(size_t)row_of(u_iperm, i0) * u_stride + c];
@@ -96,16 +98,24 @@ __global__ void grad_div_gather_kernel(const float* __restrict__ xyz, const int*
             const double u2 = u[(size_t)row_of(u_iperm, i2) * u_stride + c];
             const d3 a = dcross(nrm, dsub(v2, v1)), b = dcross(nrm, dsub(v0, v2)),
                      w = dcross(nrm, dsub(v1, v0));
-            const double twice = 2.0 * area;
-            g = d3{(u0 * a.x + u1 * b.x + u2 * w.x) / twice, (u0 * a.y + u1 * b.y + u2 * w.y) / twice,
-                   (u0 * a.z + u1 * b.z + u2 * w.z) / twice};
+            g = d3{u0 * a.x + u1 * b.x + u2 * w.x, u0 * a.y + u1 * b.y + u2 * w.y,
+                   u0 * a.z + u1 * b.z + u2 * w.z};
         }
+        // Scaled by its largest component first so a far-field gradient's square cannot underflow
+        // (kernels/predicates.py:719 stable_normalize), then one reciprocal square root.
         const double largest = fmax(fabs(g.x), fmax(fabs(g.y), fabs(g.z)));
         d3 x{0.0, 0.0, 0.0};
         if (largest != 0.0) {
-            const d3 s{g.x / largest, g.y / largest, g.z / largest};
-            const double len = sqrt(ddot(s, s));
-            if (len > 0.0) x = d3{s.x / len, s.y / len, s.z / len};
+            // A subnormal largest component would overflow its reciprocal: divide instead.
+            d3 s;
+            if (largest > 1e-300) {
+                const double scale = 1.0 / largest;
+                s = d3{g.x * scale, g.y * scale, g.z * scale};
+            } else {
+                s = d3{g.x / largest, g.y / largest, g.z / largest};
+            }
+            const double inv_len = rsqrt(ddot(s, s));
+            x = d3{s.x * inv_len, s.y * inv_len, s.z * inv_len};
         }
         const double c0 = (double)cot[3 * f], c1 = (double)cot[3 * f + 1], c2 = (double)cot[3 * f + 2];
         double d;
