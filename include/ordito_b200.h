@@ -255,6 +255,10 @@ int ob_chol_buffers(void* factor, int n_columns, double** rhs, double** solution
 int ob_chol_work(void* factor, int n_columns, double** rhs, double** solution, int* stride,
                  const int32_t** iperm, const char** pinned, ob_stream_t stream);
 int ob_chol_solve_in_place(void* factor, int n_columns, ob_stream_t stream);
+/* The device status word of the factor's persistent passes (0, or OB_ERR_TIMEOUT when a bounded
+ * grid-barrier wait gave up -- the pass's results are then invalid), read back and cleared;
+ * *persistent = the cooperative grid size the passes use (0: a launch per phase). */
+int ob_chol_check(void* factor, int* status, int* persistent, ob_stream_t stream);
 
 /* ---- the served batch's per-query kernels (ordito_b200/csrc/ob_served.cu) ------------------
  * ob_corner_index: each vertex's corner slots (3 f + e) in ascending order -- a stable sort of

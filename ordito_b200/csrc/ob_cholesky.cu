@@ -424,7 +424,8 @@ struct Tile {
 constexpr int kTileRows = 64;   // output rows per tile
 constexpr int kTileCols = 64;   // right-hand-side columns per tile
 constexpr int kTileK = 16;      // inner-dimension step staged in shared memory
-constexpr int kSplitK = 64;     // a tile's inner-dimension range at most (split beyond)
+constexpr int kSplitK = 64;       // a leaf tile's inner-dimension range at most (split beyond)
+constexpr int kSplitKUpper = 32;  // the same above the leaves
 constexpr int kTileThreads = 128;
 // Shared rows of 72 doubles: the 8 x 4 fragment loads of a warp then touch every 8-byte bank
 // pair exactly twice (the minimum for 256 bytes).
@@ -439,11 +440,16 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
                  : "d"(a), "d"(b));
 }
 
-// 16-byte asynchronous global -> shared copy; bytes < 16 zero-fills the rest (0: all zeros, and
-// the source is not read).
+// 16-byte asynchronous global -> shared copies; bytes < 16 zero-fills the rest (0: all zeros, and
+// the source is not read). copy16 may cache in L1 (read-only data: the factor); copy16_l2 reads
+// through L2 only, for data other CTAs of a persistent launch wrote in an earlier phase.
 __device__ __forceinline__ void copy16(void* smem, const void* gmem, int bytes) {
     const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void copy16_l2(void* smem, const void* gmem, int bytes) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(gmem), "r"(bytes));
 }
 __device__ __forceinline__ void copy_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
@@ -459,19 +465,17 @@ struct Stage {
     double b[kTileK * kLd];
 };
 
-// One 64 x 64 output tile per CTA of four warps, each warp a 32 x 32 quadrant as 4 x 4 float64
+// One 64 x 64 output tile for a CTA of four warps, each warp a 32 x 32 quadrant as 4 x 4 float64
 // MMA tiles. The tile's matrix block and its gathered input rows are copied 16 inner steps at a
 // time into shared memory with asynchronous 16-byte copies (zero-filled at the edges), two stages
 // in flight: the next step's copies overlap the current step's MMAs. The output is assigned,
 // subtracted, or added atomically per the tile's op. `k` (the column stride) is even and every
-// block row starts on 16 bytes, so every copy is aligned.
-__global__ void __launch_bounds__(kTileThreads)
-tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
-                    const int* __restrict__ idx, const double* __restrict__ in,
-                    double* __restrict__ out, int k) {
-    __shared__ __align__(16) Stage stage[2];
-    const Tile t = tiles[blockIdx.x];
-    const int c0 = blockIdx.y * kTileCols;
+// block row starts on 16 bytes, so every copy is aligned. Vectors are read through L2, so a
+// persistent launch sees what other CTAs wrote before its last grid barrier.
+__device__ __forceinline__ void tile_product(const Tile& t, int c0, const double* __restrict__ vals,
+                                             const int* __restrict__ idx,
+                                             const double* __restrict__ in, double* __restrict__ out,
+                                             int k, Stage* stage) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;  // the warp's quadrant
     const int fr = lane >> 2, fk = lane & 3;                 // fragment coordinates
@@ -509,7 +513,7 @@ tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ v
                 src = in + (size_t)r * k + c0 + c2;
                 valid = 16;
             }
-            copy16(&s.b[kk * kLd + c2], src, valid);
+            copy16_l2(&s.b[kk * kLd + c2], src, valid);
         }
         copy_commit();
     };
@@ -559,10 +563,88 @@ tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ v
                 switch (t.op) {
                     case kAssign: *o = v; break;
                     case kAtomicSub: atomicAdd(o, -v); break;
-                    case kSub: *o -= v; break;
+                    case kSub: *o = __ldcg(o) - v; break;
                     default: atomicAdd(o, v); break;
                 }
             }
+    }
+}
+
+// One launch per phase: a CTA per (tile, column block).
+__global__ void __launch_bounds__(kTileThreads)
+tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
+                    const int* __restrict__ idx, const double* __restrict__ in,
+                    double* __restrict__ out, int k) {
+    __shared__ __align__(16) Stage stage[2];
+    tile_product(tiles[blockIdx.x], blockIdx.y * kTileCols, vals, idx, in, out, k, stage);
+}
+
+// A phase of a triangular pass: its tiles and which work buffers (0 B, 1 Y, 2 X) it reads and
+// writes.
+struct Phase {
+    const Tile* tiles;
+    int count, in, out;
+};
+
+// Grid-wide barrier of a cooperative (co-resident) launch: bar[0] counts arrivals, bar[1] is the
+// generation. Every wait is bounded: after `limit` polls (or once another CTA has given up) the
+// CTA records OB_ERR_TIMEOUT in *status and returns false, and so do the rest at their next poll.
+__device__ bool grid_barrier(unsigned int* bar, int* status, unsigned int limit) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile unsigned int* generation = bar + 1;
+        const unsigned int seen = *generation;
+        __threadfence();
+        const unsigned int arrived = atomicAdd(bar, 1u) + 1u;
+        if (arrived == gridDim.x) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            unsigned int polls = 0;
+            while (*generation == seen) {
+                if (++polls > limit || *(volatile int*)status != 0) {
+                    atomicExch(status, OB_ERR_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// A whole triangular pass (forward then backward, every level) in one cooperative launch: the
+// listed rows are zeroed, then each phase's (tile, column block) pairs are spread over the
+// resident CTAs with a grid barrier between phases.
+__global__ void __launch_bounds__(kTileThreads)
+pass_kernel(const Phase* __restrict__ phases, int n_phases, const int2* __restrict__ zero,
+            int n_zero, const double* __restrict__ vals, const int* __restrict__ idx, double* B,
+            double* Y, double* X, int k, unsigned int* bar, int* status, unsigned int limit) {
+    __shared__ __align__(16) Stage stage[2];
+    double* buffers[3] = {B, Y, X};
+    for (int z = blockIdx.x; z < n_zero; z += gridDim.x) {
+        const int2 range = zero[z];
+        const long long begin = (long long)range.x * k, end = (long long)(range.x + range.y) * k;
+        for (long long t = begin + threadIdx.x; t < end; t += blockDim.x) {
+            Y[t] = 0.0;
+            X[t] = 0.0;
+        }
+    }
+    if (!grid_barrier(bar, status, limit)) return;
+    const int column_blocks = (k + kTileCols - 1) / kTileCols;
+    for (int p = 0; p < n_phases; ++p) {
+        const Phase ph = phases[p];
+        const int work = ph.count * column_blocks;
+        for (int w = blockIdx.x; w < work; w += gridDim.x)
+            tile_product(ph.tiles[w / column_blocks], (w % column_blocks) * kTileCols, vals, idx,
+                         buffers[ph.in], buffers[ph.out], k, stage);
+        if (!grid_barrier(bar, status, limit)) return;
     }
 }
 
@@ -637,6 +719,13 @@ struct Factor {
     std::vector<void*> owned;
     int2* zero = nullptr;  // row ranges split tiles accumulate into (zeroed each pass)
     int n_zero = 0;
+    // The persistent pass: the phase table, barrier words [count, generation], the status word a
+    // timed-out barrier writes, and the cooperative grid size (0: launch each phase instead).
+    Phase* phases = nullptr;
+    int n_phases = 0;
+    unsigned int* barrier = nullptr;
+    int* status = nullptr;
+    int pass_grid = 0;
     // Work buffers sized for `cap_k` columns: B, Y, X in the factor's numbering, R the residual,
     // RHS / SOL the caller's right-hand side and solution copied in / out (old numbering).
     int cap_k = 0;
@@ -723,11 +812,14 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
     const int L = A.levels;
     std::vector<std::vector<Tile>> fd(L), fo(L), bo(L), bd(L);
     std::vector<int2> zero_ranges;
-    auto emit = [](std::vector<Tile>& list, Tile t, int K, int whole_op, int split_op) {
-        const bool split = K > kSplitK + kSplitK / 2;
-        for (int k0 = 0; k0 < K; k0 += split ? kSplitK : K) {
+    // Above the leaves a phase has few tiles, each a latency-bound chain of inner steps: split
+    // those finer, so more CTAs each walk fewer steps.
+    int chunk = kSplitK;
+    auto emit = [&chunk](std::vector<Tile>& list, Tile t, int K, int whole_op, int split_op) {
+        const bool split = K > chunk + chunk / 2;
+        for (int k0 = 0; k0 < K; k0 += split ? chunk : K) {
             t.k0 = k0;
-            t.k1 = split ? std::min(K, k0 + kSplitK) : K;
+            t.k1 = split ? std::min(K, k0 + chunk) : K;
             t.op = split ? split_op : whole_op;
             list.push_back(t);
         }
@@ -737,6 +829,7 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
         const Node& nd = A.nodes[s];
         const int nc = nd.count, noff = (int)nd.off_rows.size(), ld = ld_at[s];
         if (nc == 0) continue;
+        chunk = nd.level == 0 ? kSplitK : kSplitKUpper;
         bool zero = false;
         for (int r0 = 0; r0 < nc; r0 += kTileRows) {
             const int rows = std::min(kTileRows, nc - r0);
@@ -785,6 +878,34 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
     if (!st) st = push(bo, F->bwd_off, F->n_bwd_off);
     if (!st) st = push(bd, F->bwd_diag, F->n_bwd_diag);
     if (st) return st;
+    // The persistent pass's phase table, in the order the per-phase launches run.
+    std::vector<Phase> phases;
+    for (int l = 0; l < L; ++l) {
+        if (F->n_fwd_diag[l]) phases.push_back(Phase{F->fwd_diag[l], F->n_fwd_diag[l], 0, 1});
+        if (F->n_fwd_off[l]) phases.push_back(Phase{F->fwd_off[l], F->n_fwd_off[l], 1, 0});
+    }
+    for (int l = L - 1; l >= 0; --l) {
+        if (F->n_bwd_off[l]) phases.push_back(Phase{F->bwd_off[l], F->n_bwd_off[l], 2, 1});
+        if (F->n_bwd_diag[l]) phases.push_back(Phase{F->bwd_diag[l], F->n_bwd_diag[l], 1, 2});
+    }
+    F->n_phases = (int)phases.size();
+    st = dev_alloc(F, (void**)&F->phases, sizeof(Phase) * std::max<size_t>(phases.size(), 1), stream);
+    if (!st) st = dev_alloc(F, (void**)&F->barrier, 4 * sizeof(unsigned int), stream);
+    if (st) return st;
+    F->status = reinterpret_cast<int*>(F->barrier + 2);
+    OB_CUDA(cudaMemcpyAsync(F->phases, phases.data(), sizeof(Phase) * phases.size(),
+                            cudaMemcpyHostToDevice, stream));
+    OB_CUDA(cudaMemsetAsync(F->barrier, 0, 4 * sizeof(unsigned int), stream));
+    int per_sm = 0;
+    int device = 0, cooperative = 0;
+    if (cudaGetDevice(&device) == cudaSuccess &&
+        cudaDeviceGetAttribute(&cooperative, cudaDevAttrCooperativeLaunch, device) == cudaSuccess &&
+        cooperative &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel, kTileThreads, 0) ==
+            cudaSuccess &&
+        per_sm > 0)
+        F->pass_grid = per_sm * sm_count();
+    cudaGetLastError();
     OB_CUDA(cudaStreamSynchronize(stream));  // host staging buffers go out of scope
     return OB_OK;
 }
@@ -812,6 +933,27 @@ int triangular_solves(Factor* F, int k, cudaStream_t stream) {
     const int L = F->analysis->levels;
     const dim3 threads(kTileThreads);
     const int ct = (k + kTileCols - 1) / kTileCols;
+    if (F->pass_grid > 0) {
+        // One cooperative launch for the whole pass (every CTA resident, so the grid barriers
+        // between phases cannot wait on a CTA that never runs).
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(F->pass_grid);
+        cfg.blockDim = threads;
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const unsigned int limit = 1u << 23;
+        OB_CUDA(cudaLaunchKernelEx(&cfg, pass_kernel, (const Phase*)F->phases, F->n_phases,
+                                   (const int2*)F->zero, F->n_zero, (const double*)F->vals,
+                                   (const int*)F->idx, F->B, F->Y, F->X, k, F->barrier, F->status,
+                                   limit));
+        count_launch();
+        return OB_OK;
+    }
     if (F->n_zero > 0) {
         zero_rows_kernel<<<F->n_zero, 256, 0, stream>>>(F->zero, F->n_zero, k, F->Y, F->X);
         OB_CHECK_LAUNCH("chol zero split rows");
@@ -893,16 +1035,22 @@ int solve_graph(Factor* F, int k, int refine, const int* offsets, const int* col
     cudaGraph_t graph = nullptr;
     if (e == cudaSuccess) e = cudaStreamEndCapture(F->capture, &graph);
     suppress_counting(-1);
+    cudaGraphExec_t exec = nullptr;
+    size_t nodes = 0;
+    if (st == OB_OK && e == cudaSuccess) {
+        cudaGraphGetNodes(graph, nullptr, &nodes);
+        e = cudaGraphInstantiate(&exec, graph, 0);
+    }
+    if (graph) cudaGraphDestroy(graph);
     if (st != OB_OK || e != cudaSuccess) {
-        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        if (F->pass_grid > 0) {
+            // A cooperative launch this runtime cannot record: fall back to a launch per phase.
+            F->pass_grid = 0;
+            return solve_graph(F, k, refine, offsets, columns, values, out);
+        }
         return st != OB_OK ? st : cuda_status(e, "ob_chol_solve: capture");
     }
-    size_t nodes = 0;
-    cudaGraphGetNodes(graph, nullptr, &nodes);
-    cudaGraphExec_t exec;
-    e = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) return cuda_status(e, "ob_chol_solve: instantiate");
     F->graphs.push_back(Factor::Recorded{k, refine, offsets, columns, values, exec, (int)nodes});
     *out = &F->graphs.back();
     return OB_OK;
@@ -1055,6 +1203,19 @@ int ob_chol_work(void* factor, int n_columns, double** rhs, double** solution, i
     *stride = even_columns(n_columns);
     *iperm = F->iperm;
     *pinned = F->pinned;
+    return OB_OK;
+}
+
+int ob_chol_check(void* factor, int* status, int* persistent, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(factor && status, "ob_chol_check: bad argument");
+    Factor* F = static_cast<Factor*>(factor);
+    int word = 0;
+    OB_CUDA(cudaMemcpyAsync(&word, F->status, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    OB_CUDA(cudaStreamSynchronize(stream));
+    if (word != 0) OB_CUDA(cudaMemsetAsync(F->barrier, 0, 4 * sizeof(unsigned int), stream));
+    *status = word;
+    if (persistent) *persistent = F->pass_grid;
     return OB_OK;
 }
 

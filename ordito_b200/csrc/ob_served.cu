@@ -144,35 +144,41 @@ __global__ void seed_permuted_kernel(const int* __restrict__ sources,
     }
 }
 
-// Per column: sum of phi over the sources and over every row (block partials, last block folds).
+// Per column: the sum of phi over every row and over the column's sources. The whole-field sums
+// read rows whole (a row's columns are contiguous): thread t of a block owns column t % stride
+// (blockDim a multiple of stride), a block's per-column partials are added in thread order, then
+// across blocks in block order by the last block to finish. The source sums are a handful of
+// rows, added by that last block.
 __global__ void shift_sums_kernel(const double* __restrict__ phi, int n, int stride,
                                   const int* __restrict__ iperm, const int* __restrict__ sources,
                                   const int* __restrict__ source_offsets, int k,
-                                  double2* __restrict__ partials, unsigned int* counter,
+                                  double* __restrict__ partials, unsigned int* counter,
                                   double2* __restrict__ sums) {
-    __shared__ double scratch[32];
+    __shared__ double tree[kThreads];
     __shared__ int last;
-    const int c = blockIdx.y;
-    const int s_begin = source_offsets[c], s_end = source_offsets[c + 1];
-    double at_sources = 0.0, everywhere = 0.0;
-    const int step = gridDim.x * blockDim.x;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < s_end - s_begin; i += step)
-        at_sources += phi[(size_t)iperm[sources[s_begin + i]] * stride + c];
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += step)
-        everywhere += phi[(size_t)r * stride + c];
-    const double a = block_sum(at_sources, scratch);
-    const double b = block_sum(everywhere, scratch);
-    if (threadIdx.x == 0) partials[(size_t)c * gridDim.x + blockIdx.x] = make_double2(a, b);
+    const int c = threadIdx.x % stride;
+    double everywhere = 0.0;
+    const long long total = (long long)n * stride;
+    const long long step = (long long)gridDim.x * blockDim.x;  // a multiple of stride
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += step)
+        everywhere += phi[t];
+    tree[threadIdx.x] = everywhere;
+    __syncthreads();
+    if ((int)threadIdx.x < stride) {
+        double column = 0.0;
+        for (int t = threadIdx.x; t < (int)blockDim.x; t += stride) column += tree[t];
+        partials[(size_t)blockIdx.x * stride + threadIdx.x] = column;
+    }
     if (!last_block_arrived(counter, &last)) return;
     for (int col = threadIdx.x; col < k; col += blockDim.x) {
-        double s = 0.0, g = 0.0;
-        for (int bx = 0; bx < (int)gridDim.x; ++bx) {
-            const double2 p = __ldcg(&partials[(size_t)col * gridDim.x + bx]);
-            s += p.x;
-            g += p.y;
-        }
+        double g = 0.0;
+        for (int bx = 0; bx < (int)gridDim.x; ++bx) g += __ldcg(&partials[(size_t)bx * stride + col]);
+        double s = 0.0;
+        for (int i = source_offsets[col]; i < source_offsets[col + 1]; ++i)
+            s += __ldcg(&phi[(size_t)iperm[sources[i]] * stride + col]);
         sums[col] = make_double2(s, g);
     }
+    (void)c;
 }
 
 // out[c][v] = the shifted, oriented phi of vertex v in column c (ordito/kernels/heat.py:3406).
@@ -295,16 +301,21 @@ int ob_shift_permuted(const double* phi, int n_vertices, int stride, const int32
     cudaStream_t stream = as_stream(stream_);
     OB_REQUIRE(n_vertices >= 1 && n_columns >= 1 && stride >= n_columns, "ob_shift_permuted: bad size");
     OB_REQUIRE(phi && iperm && sources && source_offsets && out, "ob_shift_permuted: null pointer");
-    const int blocks = std::max(1, std::min(ceil_div(n_vertices, kThreads * 4), 2 * sm_count()));
+    OB_REQUIRE(stride <= kThreads, "ob_shift_permuted: stride above %d", kThreads);
+    const int threads = (kThreads / stride) * stride;
+    const long long total = (long long)n_vertices * stride;
+    const int blocks = (int)std::max(1LL, std::min((total + threads * 4 - 1) / (threads * 4),
+                                                   (long long)2 * sm_count()));
     Scratch scratch(stream);
-    double2* partials = scratch.take<double2>((size_t)blocks * n_columns);
+    double* partials = scratch.take<double>((size_t)blocks * stride);
     double2* sums = scratch.take<double2>(n_columns);
     unsigned int* counter = scratch.take<unsigned int>(1);
     int st = scratch.commit();
     if (st) return st;
     OB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned int), stream));
-    shift_sums_kernel<<<dim3(blocks, n_columns), kThreads, 0, stream>>>(
-        phi, n_vertices, stride, iperm, sources, source_offsets, n_columns, partials, counter, sums);
+    shift_sums_kernel<<<blocks, threads, 0, stream>>>(phi, n_vertices, stride, iperm, sources,
+                                                       source_offsets, n_columns, partials,
+                                                       counter, sums);
     OB_CHECK_LAUNCH("shift_sums");
     shift_out_kernel<<<dim3(ceil_div(n_vertices, 32), ceil_div(n_columns, 32)), dim3(32, 8), 0,
                        stream>>>(phi, n_vertices, stride, iperm, sums, source_offsets, n_columns,
