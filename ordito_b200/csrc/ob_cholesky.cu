@@ -423,9 +423,9 @@ struct Tile {
 
 constexpr int kTileRows = 64;   // output rows per tile
 constexpr int kTileCols = 64;   // right-hand-side columns per tile
-constexpr int kTileK = 16;      // inner-dimension step staged in shared memory
+constexpr int kTileK = 32;      // inner-dimension step staged in shared memory
 constexpr int kSplitK = 64;       // a leaf tile's inner-dimension range at most (split beyond)
-constexpr int kSplitKUpper = 32;  // the same above the leaves
+constexpr int kSplitKUpper = 64;  // the same above the leaves (32 measured slower: more atomics)
 constexpr int kTileThreads = 128;
 // Shared rows of 72 doubles: the 8 x 4 fragment loads of a warp then touch every 8-byte bank
 // pair exactly twice (the minimum for 256 bytes).
@@ -485,10 +485,11 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     const double* M = vals + t.m;
-    // Each operand block is 64 x 16 doubles = 512 16-byte chunks: four per thread.
+    // Each operand block is 64 x kTileK doubles in 16-byte chunks, kChunks per thread.
+    constexpr int kChunks = kTileRows * kTileK / 2 / kTileThreads;
     auto issue = [&](int kb, Stage& s) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < kChunks; ++q) {
             const int chunk = threadIdx.x + q * kTileThreads;
             // Matrix block.
             if (t.trans) {
@@ -570,12 +571,16 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
     }
 }
 
+// The two stages live in dynamic shared memory (kStageBytes, above the 48 KB static limit).
+constexpr int kStageBytes = 2 * (int)sizeof(Stage);
+
 // One launch per phase: a CTA per (tile, column block).
 __global__ void __launch_bounds__(kTileThreads)
 tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
                     const int* __restrict__ idx, const double* __restrict__ in,
                     double* __restrict__ out, int k) {
-    __shared__ __align__(16) Stage stage[2];
+    extern __shared__ __align__(16) unsigned char shared_stages[];
+    Stage* stage = reinterpret_cast<Stage*>(shared_stages);
     tile_product(tiles[blockIdx.x], blockIdx.y * kTileCols, vals, idx, in, out, k, stage);
 }
 
@@ -626,7 +631,8 @@ __global__ void __launch_bounds__(kTileThreads)
 pass_kernel(const Phase* __restrict__ phases, int n_phases, const int2* __restrict__ zero,
             int n_zero, const double* __restrict__ vals, const int* __restrict__ idx, double* B,
             double* Y, double* X, int k, unsigned int* bar, int* status, unsigned int limit) {
-    __shared__ __align__(16) Stage stage[2];
+    extern __shared__ __align__(16) unsigned char shared_stages[];
+    Stage* stage = reinterpret_cast<Stage*>(shared_stages);
     double* buffers[3] = {B, Y, X};
     for (int z = blockIdx.x; z < n_zero; z += gridDim.x) {
         const int2 range = zero[z];
@@ -759,7 +765,22 @@ void factor_release(Factor* F) {
     delete F;
 }
 
+// Lets the product kernels take their kStageBytes of dynamic shared memory (once per device).
+int allow_stage_memory() {
+    static int allowed[64] = {};
+    int device = 0;
+    OB_CUDA(cudaGetDevice(&device));
+    if (device >= 0 && device < 64 && allowed[device]) return OB_OK;
+    OB_CUDA(cudaFuncSetAttribute(tile_product_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kStageBytes));
+    OB_CUDA(cudaFuncSetAttribute(pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kStageBytes));
+    if (device >= 0 && device < 64) allowed[device] = 1;
+    return OB_OK;
+}
+
 int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
+    if (int st0 = allow_stage_memory()) return st0;
     const Analysis& A = *F->analysis;
     const int ns = (int)A.nodes.size();
     // Every block row is padded to a multiple of 8 doubles (and every block starts on one), so
@@ -896,12 +917,17 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
     OB_CUDA(cudaMemcpyAsync(F->phases, phases.data(), sizeof(Phase) * phases.size(),
                             cudaMemcpyHostToDevice, stream));
     OB_CUDA(cudaMemsetAsync(F->barrier, 0, 4 * sizeof(unsigned int), stream));
+    // The persistent pass is opt-in (OB_CHOL_PERSISTENT=1): measured on the 131k-vertex torus its
+    // 46 grid barriers over 592 CTAs cost more (1.14 ms a pass) than the recorded per-phase
+    // launches (0.82 ms).
+    const char* knob = getenv("OB_CHOL_PERSISTENT");
     int per_sm = 0;
     int device = 0, cooperative = 0;
-    if (cudaGetDevice(&device) == cudaSuccess &&
+    if (knob != nullptr && knob[0] == '1' && cudaGetDevice(&device) == cudaSuccess &&
         cudaDeviceGetAttribute(&cooperative, cudaDevAttrCooperativeLaunch, device) == cudaSuccess &&
         cooperative &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel, kTileThreads, 0) ==
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel, kTileThreads,
+                                                      kStageBytes) ==
             cudaSuccess &&
         per_sm > 0)
         F->pass_grid = per_sm * sm_count();
@@ -939,7 +965,7 @@ int triangular_solves(Factor* F, int k, cudaStream_t stream) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(F->pass_grid);
         cfg.blockDim = threads;
-        cfg.dynamicSmemBytes = 0;
+        cfg.dynamicSmemBytes = kStageBytes;
         cfg.stream = stream;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeCooperative;
@@ -960,24 +986,24 @@ int triangular_solves(Factor* F, int k, cudaStream_t stream) {
     }
     for (int l = 0; l < L; ++l) {
         if (F->n_fwd_diag[l]) {
-            tile_product_kernel<<<dim3(F->n_fwd_diag[l], ct), threads, 0, stream>>>(
+            tile_product_kernel<<<dim3(F->n_fwd_diag[l], ct), threads, kStageBytes, stream>>>(
                 F->fwd_diag[l], F->vals, F->idx, F->B, F->Y, k);
             OB_CHECK_LAUNCH("chol forward diagonal");
         }
         if (F->n_fwd_off[l]) {
-            tile_product_kernel<<<dim3(F->n_fwd_off[l], ct), threads, 0, stream>>>(
+            tile_product_kernel<<<dim3(F->n_fwd_off[l], ct), threads, kStageBytes, stream>>>(
                 F->fwd_off[l], F->vals, F->idx, F->Y, F->B, k);
             OB_CHECK_LAUNCH("chol forward update");
         }
     }
     for (int l = L - 1; l >= 0; --l) {
         if (F->n_bwd_off[l]) {
-            tile_product_kernel<<<dim3(F->n_bwd_off[l], ct), threads, 0, stream>>>(
+            tile_product_kernel<<<dim3(F->n_bwd_off[l], ct), threads, kStageBytes, stream>>>(
                 F->bwd_off[l], F->vals, F->idx, F->X, F->Y, k);
             OB_CHECK_LAUNCH("chol backward gather");
         }
         if (F->n_bwd_diag[l]) {
-            tile_product_kernel<<<dim3(F->n_bwd_diag[l], ct), threads, 0, stream>>>(
+            tile_product_kernel<<<dim3(F->n_bwd_diag[l], ct), threads, kStageBytes, stream>>>(
                 F->bwd_diag[l], F->vals, F->idx, F->Y, F->X, k);
             OB_CHECK_LAUNCH("chol backward diagonal");
         }
