@@ -423,7 +423,9 @@ struct Tile {
 
 constexpr int kTileRows = 64;   // output rows per tile
 constexpr int kTileCols = 64;   // right-hand-side columns per tile
-constexpr int kTileK = 32;      // inner-dimension step staged in shared memory
+// Inner-dimension step staged in shared memory. 16 (two stages, 39 KB, 4 CTAs per SM) measured
+// 0.82 ms a pass on the 131k torus at 64 columns, against 1.11 ms for 32 (74 KB, 3 CTAs per SM).
+constexpr int kTileK = 16;
 constexpr int kSplitK = 64;       // a leaf tile's inner-dimension range at most (split beyond)
 constexpr int kSplitKUpper = 64;  // the same above the leaves (32 measured slower: more atomics)
 constexpr int kTileThreads = 128;
