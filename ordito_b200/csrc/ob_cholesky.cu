@@ -238,6 +238,26 @@ struct HostFactor {
     std::vector<char> pinned;                 // per new index: identity row (pinned / empty)
 };
 
+// Runs fn(begin, end) over [0, n) split across host threads when the work is large (the fronts
+// at the top of the tree, factored after the parallel subtrees); serially otherwise.
+template <typename Fn>
+void parallel_range(int n, bool large, Fn fn) {
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    if (!large || hw == 1 || n < 64) {
+        fn(0, n);
+        return;
+    }
+    const int parts = (int)std::min<unsigned>(hw, (unsigned)(n / 16));
+    std::vector<std::thread> pool;
+    for (int p = 1; p < parts; ++p)
+        pool.emplace_back([=]() { fn((int)((long long)n * p / parts), (int)((long long)n * (p + 1) / parts)); });
+    fn(0, (int)((long long)n / parts));
+    for (auto& th : pool) th.join();
+}
+
+// Fronts from this size up spread their dense work over host threads.
+constexpr int kThreadedFront = 384;
+
 // Dense partial Cholesky of the m x m column-major front F (lower part used): the first nc
 // columns are factored in place (L11, L21) and F22 becomes the Schur complement.
 bool partial_cholesky(double* F, int m, int nc) {
@@ -260,16 +280,19 @@ bool partial_cholesky(double* F, int m, int nc) {
                     for (int i = k; i < m; ++i) ck[i] -= cj[i] * f;
             }
         }
-        // Update every later column with the panel: F[k:, k] -= L[k:, j0:j1] L[k, j0:j1]^T.
-        for (int k = j1; k < m; ++k) {
-            double* ck = F + (size_t)k * m;
-            for (int j = j0; j < j1; ++j) {
-                const double* cj = F + (size_t)j * m;
-                const double f = cj[k];
-                if (f != 0.0)
-                    for (int i = k; i < m; ++i) ck[i] -= cj[i] * f;
+        // Update every later column with the panel: F[k:, k] -= L[k:, j0:j1] L[k, j0:j1]^T
+        // (independent columns: threaded on a large front).
+        parallel_range(m - j1, m >= kThreadedFront, [&](int begin, int end) {
+            for (int k = j1 + begin; k < j1 + end; ++k) {
+                double* ck = F + (size_t)k * m;
+                for (int j = j0; j < j1; ++j) {
+                    const double* cj = F + (size_t)j * m;
+                    const double f = cj[k];
+                    if (f != 0.0)
+                        for (int i = k; i < m; ++i) ck[i] -= cj[i] * f;
+                }
             }
-        }
+        });
     }
     return true;
 }
@@ -314,16 +337,26 @@ int factor_node(const Analysis& A, const double* values, int s, bool singular, H
         H.update[c].shrink_to_fit();
     }
     if (!partial_cholesky(F.data(), m, nc)) return OB_ERR_INDEFINITE;
-    // Inverse of L11 (lower triangular), row-major: solve L X = I column by column.
-    std::vector<double> inv((size_t)nc * nc, 0.0);
-    for (int c = 0; c < nc; ++c) {
-        // Column c of X: x_i = (delta_ic - sum_{k<i} L_ik x_k) / L_ii, for i >= c.
-        for (int i = c; i < nc; ++i) {
-            double acc = (i == c) ? 1.0 : 0.0;
-            for (int k = c; k < i; ++k) acc -= F[(size_t)k * m + i] * inv[(size_t)k * nc + c];
-            inv[(size_t)i * nc + c] = acc / F[(size_t)i * m + i];
+    // Inverse of L11 (lower triangular): column c of X = L^-1 by forward substitution, each step
+    // an axpy down a contiguous column of L (independent columns: threaded on a large front),
+    // then stored row-major.
+    std::vector<double> X((size_t)nc * nc, 0.0);
+    parallel_range(nc, m >= kThreadedFront, [&](int begin, int end) {
+        for (int c = begin; c < end; ++c) {
+            double* x = X.data() + (size_t)c * nc;
+            x[c] = 1.0;
+            for (int k = c; k < nc; ++k) {
+                const double* lk = F.data() + (size_t)k * m;
+                const double xk = x[k] / lk[k];
+                x[k] = xk;
+                if (xk != 0.0)
+                    for (int i = k + 1; i < nc; ++i) x[i] -= xk * lk[i];
+            }
         }
-    }
+    });
+    std::vector<double> inv((size_t)nc * nc);
+    for (int c = 0; c < nc; ++c)
+        for (int i = 0; i < nc; ++i) inv[(size_t)i * nc + c] = X[(size_t)c * nc + i];
     H.inv[s] = std::move(inv);
     std::vector<double> L21((size_t)noff * nc);
     for (int r = 0; r < noff; ++r)
