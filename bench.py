@@ -4,8 +4,9 @@ Workload: the torus of R = 1, r = 0.3, every vertex moved by N(0, (0.1 h)^2) per
 (h the clean torus's mean edge length, seed 0), and a stream of 64 single-source queries whose
 sources are 64 vertices drawn uniformly without replacement (seed 1). One step answers all 64
 queries on the resident mesh -- the served + batched path: the mesh's operators and both Cholesky
-factors stay on the device, and the 64 queries run as one batched pass (seeding, the two factored
-solves over 64 right-hand sides with a float64 refinement step each, the divergence and the shift).
+factors stay on the device, and the 64 queries run as one batched pass in the factors' ordering
+(seeding, the two float64 factored solves over 64 right-hand sides, the gathered divergence and the
+shift; ``--refine 1`` adds a float64 refinement step to each solve).
 ``value`` is whole-job solves/s with the sources resident on the device; ``e2e`` is the same stream
 through the public API (``heat_geodesic_batch``) from host source lists to host distances, copies
 included. The plain drop-in (``heat_geodesic(vertices, faces, [s])``: assembly, solves and any
@@ -47,7 +48,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--queries", type=int, default=64)
     p.add_argument("--cols", type=int, default=512)
     p.add_argument("--rows", type=int, default=256)
-    p.add_argument("--refine", type=int, default=1)
+    p.add_argument("--refine", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     return p.parse_args()
@@ -390,7 +391,8 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
                 "queries_per_step": k,
                 "path": "served + batched: resident Trimesh, nested-dissection supernodal Cholesky "
                         "of M - tL and -L held on the device, 64 right-hand sides per pass, "
-                        f"{args.refine} float64 refinement step(s) per solve",
+                        f"{args.refine} float64 refinement step(s) per solve"
+                        + (" (in-place passes in the factors' ordering)" if args.refine == 0 else ""),
                 "l2": "no flush; per step the two 147 MB factors (294 MB) exceed the 126 MB L2",
                 "parallelism": f"replicas{dist.world}",
                 "setup_s": setup_s,

@@ -23,6 +23,7 @@
 #include <thread>
 #include <vector>
 
+#include "ob_host.hpp"
 #include "ob_internal.cuh"
 
 namespace ob {
@@ -238,24 +239,8 @@ struct HostFactor {
     std::vector<char> pinned;                 // per new index: identity row (pinned / empty)
 };
 
-// Runs fn(begin, end) over [0, n) split across host threads when the work is large (the fronts
-// at the top of the tree, factored after the parallel subtrees); serially otherwise.
-template <typename Fn>
-void parallel_range(int n, bool large, Fn fn) {
-    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-    if (!large || hw == 1 || n < 64) {
-        fn(0, n);
-        return;
-    }
-    const int parts = (int)std::min<unsigned>(hw, (unsigned)(n / 16));
-    std::vector<std::thread> pool;
-    for (int p = 1; p < parts; ++p)
-        pool.emplace_back([=]() { fn((int)((long long)n * p / parts), (int)((long long)n * (p + 1) / parts)); });
-    fn(0, (int)((long long)n / parts));
-    for (auto& th : pool) th.join();
-}
-
-// Fronts from this size up spread their dense work over host threads.
+// Fronts from this size up (the ones at the top of the tree, factored after the parallel
+// subtrees) spread their dense work over host threads (parallel_range).
 constexpr int kThreadedFront = 384;
 
 // Dense partial Cholesky of the m x m column-major front F (lower part used): the first nc
@@ -282,8 +267,8 @@ bool partial_cholesky(double* F, int m, int nc) {
         }
         // Update every later column with the panel: F[k:, k] -= L[k:, j0:j1] L[k, j0:j1]^T
         // (independent columns: threaded on a large front).
-        parallel_range(m - j1, m >= kThreadedFront, [&](int begin, int end) {
-            for (int k = j1 + begin; k < j1 + end; ++k) {
+        parallel_range(m - j1, m >= kThreadedFront, [&](long long begin, long long end) {
+            for (int k = j1 + (int)begin; k < j1 + (int)end; ++k) {
                 double* ck = F + (size_t)k * m;
                 for (int j = j0; j < j1; ++j) {
                     const double* cj = F + (size_t)j * m;
@@ -341,8 +326,8 @@ int factor_node(const Analysis& A, const double* values, int s, bool singular, H
     // an axpy down a contiguous column of L (independent columns: threaded on a large front),
     // then stored row-major.
     std::vector<double> X((size_t)nc * nc, 0.0);
-    parallel_range(nc, m >= kThreadedFront, [&](int begin, int end) {
-        for (int c = begin; c < end; ++c) {
+    parallel_range(nc, m >= kThreadedFront, [&](long long begin, long long end) {
+        for (int c = (int)begin; c < (int)end; ++c) {
             double* x = X.data() + (size_t)c * nc;
             x[c] = 1.0;
             for (int k = c; k < nc; ++k) {
