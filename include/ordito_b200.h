@@ -292,6 +292,46 @@ int ob_shift_permuted(const double* phi, int n_vertices, int stride, const int32
 int ob_chol_time_solve(void* factor, int n_columns, int reps, float* ms, ob_stream_t stream);
 int ob_chol_info(void* factor, long long* info);
 
+/* ---- Smoothed-aggregation multigrid and the mixed-precision solve --------------------------
+ *
+ * ob_amg_setup replaces ordito.linalg.multigrid_preconditioner(matrix, n_columns, seed=seed)
+ * (ordito/linalg.py:5020) and the hierarchy build behind it (_multigrid_hierarchy, :6412): a
+ * smoothed-aggregation hierarchy of the n x n symmetric positive (semi-)definite CSR operator
+ * (device arrays; float64 values), built once on the host and held on the device in float32.
+ * The handle borrows offsets/columns/values (the solve reads them for its float64 residual):
+ * they must outlive it. A hierarchy that cannot coarsen (ordito/linalg.py:5118) leaves a Jacobi
+ * preconditioner in its place (ob_amg_info: info[0] = 0).
+ *
+ * ob_amg_info: info[0..3] = levels (0 = Jacobi), coarsest rows, coarsest active rows, stored
+ * entries over all levels. ob_amg_levels: rows and stored entries per level (up to capacity).
+ *
+ * ob_amg_apply: x = M b, one V-cycle on k columns, the ``matvec(x, y, z, 1, 0)`` of the
+ * reference's returned operator (ordito/linalg.py:5123). Multi-column arrays are [n][ld] rows
+ * (entry (row, c) at row * ld + c, ld >= k), as everywhere in this library.
+ *
+ * ob_amg_solve replaces ordito.linalg.solve_spd(matrix, rhs, solution, tol=..., preconditioner=
+ * multigrid_preconditioner(matrix)) (ordito/linalg.py:1356) for k columns: x is the initial
+ * guess and is overwritten. Float64 iterative refinement around a float32 CG preconditioned by
+ * the float32 V-cycle: each outer round forms r = b - A x in float64, solves A d = r / |r| in
+ * float32 to a relative residual of inner_tol (at most max_inner iterations), and adds |r| d to
+ * x in float64; it stops per column at |b - A x|_2 <= tol |b|_2 or after max_outer rounds.
+ * Per column: iterations (inner CG iterations, all rounds), residuals (final |r|_2 / |b|_2),
+ * statuses (OB_STATUS_CONVERGED, _CAPPED or _NONFINITE). Any pointer among the three may be NULL.
+ *
+ * ob_amg_host_setup builds the same hierarchy from host arrays and reports its level shape
+ * (no device needed). */
+int ob_amg_setup(int n, const int32_t* offsets, const int32_t* columns, const double* values,
+                 unsigned seed, void** amg, ob_stream_t stream);
+int ob_amg_destroy(void* amg);
+int ob_amg_info(void* amg, long long* info);
+int ob_amg_levels(void* amg, long long* rows, long long* nnz, int capacity);
+int ob_amg_apply(void* amg, const double* b, double* x, int k, int ld, ob_stream_t stream);
+int ob_amg_solve(void* amg, const double* b, double* x, int k, int ld, double tol, int max_outer,
+                 int max_inner, double inner_tol, int* iterations, double* residuals,
+                 int* statuses, ob_stream_t stream);
+int ob_amg_host_setup(int n, const int32_t* offsets, const int32_t* columns, const double* values,
+                      unsigned seed, long long* rows, long long* nnz, int capacity, int* levels);
+
 #ifdef __cplusplus
 }
 #endif

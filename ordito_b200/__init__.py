@@ -2,7 +2,7 @@
 
 Drop-in modules for the path: ``laplacian`` (pattern, cotangent weights, Laplacian, mass),
 ``heat`` (``heat_operators``, ``heat_geodesic``, ``HeatSolver``), ``linalg`` (``solve_spd``,
-``solve_spd_settled``, the Jacobi and Chebyshev preconditioners), ``cholesky`` and ``mesh``
+``solve_spd_settled``, the Jacobi, Chebyshev and multigrid preconditioners), ``cholesky`` and ``mesh``
 (``Trimesh``). The compute runs in hand-written CUDA kernels behind the C ABI of
 ``include/ordito_b200.h`` (``libordito_b200.so``, built by ``python -m ordito_b200.build``).
 """

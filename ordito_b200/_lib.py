@@ -100,6 +100,14 @@ SIGNATURES: dict[str, list] = {
     "ob_shift_permuted": [P, I, I, P, P, P, I, I, P, P],
     "ob_chol_time_solve": [P, I, I, POINTER(c_float), P],
     "ob_chol_info": [P, POINTER(ctypes.c_longlong)],
+    "ob_amg_setup": [I, P, P, P, ctypes.c_uint, POINTER(c_void_p), P],
+    "ob_amg_destroy": [P],
+    "ob_amg_info": [P, POINTER(ctypes.c_longlong)],
+    "ob_amg_levels": [P, POINTER(ctypes.c_longlong), POINTER(ctypes.c_longlong), I],
+    "ob_amg_apply": [P, P, P, I, I, P],
+    "ob_amg_solve": [P, P, P, I, I, D, I, I, D, P, P, P, P],
+    "ob_amg_host_setup": [I, P, P, P, ctypes.c_uint, POINTER(ctypes.c_longlong),
+                          POINTER(ctypes.c_longlong), I, POINTER(c_int)],
 }
 _RESTYPES = {"ob_last_error": c_char_p}
 

@@ -30,6 +30,15 @@ class CsrMatrix:
         self._solvers: dict[Any, Any] = {}
         self._factorization: Any = None
 
+    @classmethod
+    def from_host(cls, offsets: Any, columns: Any, values: Any, shape: tuple[int, int]) -> "CsrMatrix":
+        """Upload host CSR arrays (int32 offsets/columns, float64 values)."""
+        offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+        return cls(int(shape[0]), int(shape[1]), DeviceArray.from_host(offsets),
+                   DeviceArray.from_host(np.ascontiguousarray(columns, dtype=np.int32)),
+                   DeviceArray.from_host(np.ascontiguousarray(values, dtype=np.float64)),
+                   int(offsets[-1]) if offsets.size else 0)
+
     @property
     def nnz(self) -> int:
         """Stored entries (``offsets[nrow]``; read back once)."""

@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import logging
 import math
+import warnings
 from typing import Any, NamedTuple
 
 import numpy as np
@@ -33,6 +34,8 @@ from ordito_b200.mesh import Trimesh, mesh_arguments
 _LOGGER = logging.getLogger(__name__)
 
 _CG_TOLERANCE = 1e-8  # ordito/heat.py:108
+# The relative residual the mixed-precision multigrid Poisson solve of the batched path reaches.
+_MULTIGRID_POISSON_TOLERANCE = 1e-10
 _HEAT_CHECK_ROUNDS = 16  # :142
 _HEAT_CHANGE_TOLERANCE = 1e-6  # :146
 _HEAT_SETTLE_ROUNDS = 192  # :147
@@ -225,14 +228,21 @@ class HeatSolver:
         heat = self._systems.get("heat")
         return heat["factorization"] if role == "poisson" and heat is not None else None
 
-    def factor(self) -> bool:
+    def factor(self, roles: tuple[str, ...] = ("heat", "poisson")) -> bool:
         """Factor both systems now (ordito/heat.py:3863); False if either could not be."""
         ok = True
-        for role in ("heat", "poisson"):
+        for role in roles:
             kept = self._system(role)
             if kept["factorization"].factorization is None:
                 ok = kept["factorization"].factor(self._sharing(role)) and ok
         return ok
+
+    @property
+    def poisson_multigrid(self) -> Any:
+        """The Poisson system's smoothed-aggregation hierarchy, built on first use and kept."""
+        if getattr(self, "_poisson_multigrid", None) is None:
+            self._poisson_multigrid = twl.multigrid_preconditioner(self.operators.poisson_system)
+        return self._poisson_multigrid
 
     def scratch_flag(self) -> DeviceArray:
         """A device int32 the batched seeding writes its (host-prevalidated) range flag into."""
@@ -354,6 +364,7 @@ def heat_geodesic_batch(
     method: str = "meshlab",
     refine: int = 1,
     transpose: bool = True,
+    poisson: str = "factor",
 ) -> DeviceArray:
     """Distances for many source sets on one resident mesh, solved together.
 
@@ -363,18 +374,70 @@ def heat_geodesic_batch(
     refinement steps each), the divergence and the shift all run as batched kernels over the
     interleaved ``[V][k]`` columns. Returns ``(k, V)`` (or ``(V, k)`` with ``transpose=False``).
     Each column equals ``heat_geodesic(mesh, source_sets[c])`` up to the solves' rounding.
+
+    ``poisson="multigrid"`` solves the Poisson system by the mixed-precision multigrid solve
+    (float32 CG and V-cycle inside float64 refinement to a relative residual of 1e-10) instead of
+    its factorisation; the heat system stays factored, because its far-field entries (down to
+    ``exp(-d/h)``, below float32's range on a large mesh) need the float64 direct solve.
     """
     if not isinstance(mesh, Trimesh):
         raise TypeError("heat_geodesic_batch: serves a resident Trimesh")
     n = mesh.n_vertices
     _supported(method, False)
+    if poisson not in ("factor", "multigrid"):
+        raise ValueError(f"poisson must be 'factor' or 'multigrid', got {poisson!r}")
     src, offsets, k = _source_columns(source_sets, n)
     if n == 0 or mesh.n_faces == 0:
         return DeviceArray.zeros((k, n) if transpose else (n, k), np.float64)
     solver = mesh.heat_solver(t, method=method)
+    if poisson == "multigrid":
+        if not solver.factor(("heat",)):
+            raise RuntimeError("heat_geodesic_batch: the heat system could not be factored (over budget)")
+        return _batch_multigrid(mesh, solver, src, offsets, k, refine, transpose)
     if not solver.factor():
         raise RuntimeError("heat_geodesic_batch: the systems could not be factored (over budget)")
     return _batch_columns(mesh, solver, src, offsets, k, refine, transpose)
+
+
+def _batch_multigrid(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offsets: DeviceArray,
+                     k: int, refine: int, transpose: bool) -> DeviceArray:
+    """The batched pass with the Poisson system on the mixed-precision multigrid solve."""
+    n = mesh.n_vertices
+    heat_factor = solver.heat_factor
+    operators = solver.operators
+    corner_offsets, corner_slots = mesh.corner_index
+    neg_div = DeviceArray.empty(n * k, np.float64)
+    if refine == 0:
+        h_rhs, h_sol, h_stride, h_iperm, h_pinned = heat_factor.work(k)
+        _lib.call("ob_seed_permuted", src.ptr, offsets.ptr, k, n, h_iperm, h_pinned, h_stride,
+                  h_rhs, DEFAULT_STREAM)
+        heat_factor.solve_in_place(k)
+        heat_sol, heat_stride, heat_iperm = h_sol, h_stride, h_iperm
+    else:
+        heat_rhs, heat_sol = heat_factor.buffers(k)
+        invalid = solver.scratch_flag()
+        _lib.call("ob_seed_columns", src.ptr, offsets.ptr, k, n, heat_rhs, invalid.ptr, DEFAULT_STREAM)
+        heat_factor.solve_pointers(0, 0, k, refine)
+        heat_stride, heat_iperm = k, None
+    _lib.call(
+        "ob_grad_div_gather", mesh.vertices.ptr, mesh.faces.ptr, operators.face_normals.ptr,
+        operators.face_areas.ptr, operators.cot_entries.ptr, corner_offsets.ptr, corner_slots.ptr,
+        n, k, heat_sol, heat_stride, heat_iperm, neg_div.ptr, k, None, None, DEFAULT_STREAM,
+    )  # fmt: skip
+    phi = DeviceArray.zeros(n * k, np.float64)
+    cycle = solver.poisson_multigrid
+    iters, residual, status = cycle.solve(neg_div.ptr, phi.ptr, k, _MULTIGRID_POISSON_TOLERANCE,
+                                          twl.CG_MAXITER_FACTOR * n)
+    if np.any(residual > _MULTIGRID_POISSON_TOLERANCE):
+        warnings.warn(
+            f"heat_geodesic_batch: multigrid Poisson solve stopped at relative residual "
+            f"{float(residual.max()):.3g} (tolerance {_MULTIGRID_POISSON_TOLERANCE:.3g})",
+            UserWarning, stacklevel=3,
+        )
+    _lib.call("ob_shift", phi.ptr, n, src.ptr, src.size, offsets.ptr, k, 1, DEFAULT_STREAM)
+    if not transpose:
+        return phi.reshape((n, k))
+    return _transposed(phi, n, k)
 
 
 def _batch_columns(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offsets: DeviceArray,

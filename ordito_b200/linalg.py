@@ -1,10 +1,13 @@
 """Conjugate-gradient solves of the heat path (``ordito.linalg``'s path subset).
 
 ``solve_spd`` (ordito/linalg.py:1356), ``solve_spd_settled`` (:2490), ``jacobi_preconditioner``
-(:1591) and ``chebyshev_preconditioner`` (:5135) with the reference's signatures and contracts:
-``solution`` is the initial guess and is overwritten in place; a solver state is kept per operator
-for its lifetime, so a later solve replays its recorded device loop. The iteration runs in
-``libordito_b200.so`` (ob_pcg_*): Chronopoulos-Gear CG, loop and stopping tests on the device.
+(:1591), ``chebyshev_preconditioner`` (:5135) and ``multigrid_preconditioner`` (:5020) with the
+reference's signatures and contracts: ``solution`` is the initial guess and is overwritten in
+place; a solver state is kept per operator for its lifetime, so a later solve replays its recorded
+device loop. The iteration runs in ``libordito_b200.so``: ob_pcg_* (Chronopoulos-Gear CG, loop and
+stopping tests on the device) for the Jacobi and Chebyshev preconditioners, ob_amg_* (float32 CG
+with the float32 smoothed-aggregation V-cycle inside float64 iterative refinement) for multigrid.
+Several right-hand sides are laid out ``[n][n_columns]`` (one row's columns contiguous).
 """
 
 from __future__ import annotations
@@ -26,6 +29,12 @@ SETTLE_DIRECT_TOLERANCE = 1e-12  # :181
 
 _KINDS = {"diag": 0, "chebyshev": 1}
 
+# The mixed-precision multigrid solve: float64 refinement rounds at most, and the relative residual
+# each float32 inner CG solve reaches before the next float64 residual is formed.
+AMG_MAX_OUTER = 20
+AMG_INNER_TOLERANCE = 1e-4
+AMG_MAX_INNER = 500
+
 
 class Preconditioner:
     """A preconditioner this module builds for one operator: Jacobi or Jacobi-Chebyshev.
@@ -39,6 +48,92 @@ class Preconditioner:
         self.kind = kind
         self.n_columns = n_columns
         self.shape = (matrix.nrow * n_columns, matrix.nrow * n_columns)
+
+
+class MultigridPreconditioner(Preconditioner):
+    """Smoothed-aggregation V-cycle of one operator (ordito/linalg.py:5020).
+
+    The hierarchy (strength 0.05, distance-2 aggregation, l1-Jacobi smoothing with the damping from
+    a power iteration, smoothed prolongation, Galerkin coarse operators, a dense pseudo-inverse at
+    <= 384 rows) is built once on the host (``ob_amg_setup``) and held on the device in float32.
+    An operator that does not coarsen gets a Jacobi preconditioner in its place, as the reference
+    returns one (ordito/linalg.py:5118-5119); ``grid`` then has a single level. ``matvec(x, y, z,
+    1, 0)`` applies one cycle, ``z = M x``; other ``alpha``/``beta`` raise ``ValueError``.
+    The matrix's arrays are borrowed and must stay alive (the preconditioner keeps a reference).
+    """
+
+    def __init__(self, matrix: CsrMatrix, n_columns: int = 1, *, seed: int = 0) -> None:
+        super().__init__(matrix, "multigrid", n_columns)
+        handle = ctypes.c_void_p(0)
+        _lib.call(
+            "ob_amg_setup", matrix.nrow, matrix.offsets.ptr, matrix.columns.ptr,
+            matrix.values.ptr, int(seed) & 0xFFFFFFFF, ctypes.byref(handle), DEFAULT_STREAM,
+        )  # fmt: skip
+        self.handle = handle
+        self.seed = seed
+
+    @property
+    def grid(self) -> list[int]:
+        """Rows per level, coarsest last (one level: the Jacobi fallback)."""
+        info = (ctypes.c_longlong * 4)()
+        _lib.call("ob_amg_info", self.handle, info)
+        levels = max(1, int(info[0]))
+        rows = (ctypes.c_longlong * levels)()
+        nnz = (ctypes.c_longlong * levels)()
+        _lib.call("ob_amg_levels", self.handle, rows, nnz, levels)
+        return [int(r) for r in rows]
+
+    @property
+    def is_jacobi(self) -> bool:
+        info = (ctypes.c_longlong * 4)()
+        _lib.call("ob_amg_info", self.handle, info)
+        return int(info[0]) == 0
+
+    def matvec(self, x: Any, y: Any, z: Any, alpha: float, beta: float) -> None:
+        if alpha != 1.0 or beta != 0.0:
+            raise ValueError(
+                "multigrid_preconditioner's operator only implements z = M x "
+                f"(got alpha={alpha}, beta={beta})"
+            )
+        n_columns = _columns(self.matrix, x, z)
+        x_ptr, keep_x = device_pointer(x, np.float64)
+        z_ptr, keep_z = device_pointer(z, np.float64)
+        _lib.call("ob_amg_apply", self.handle, x_ptr, z_ptr, n_columns, n_columns, DEFAULT_STREAM)
+        if isinstance(keep_z, DeviceArray) and not hasattr(z, "__cuda_array_interface__"):
+            np.copyto(z, keep_z.numpy().reshape(np.shape(z)))
+        del keep_x
+
+    def solve(self, rhs: int, x: int, n_columns: int, tol: float, maxiter: int,
+              inner_tol: float = AMG_INNER_TOLERANCE,
+              max_outer: int = AMG_MAX_OUTER) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Mixed-precision solve of ``n_columns`` systems in place (``ob_amg_solve``)."""
+        iters = (ctypes.c_int * n_columns)()
+        residual = (ctypes.c_double * n_columns)()
+        status = (ctypes.c_int * n_columns)()
+        _lib.call(
+            "ob_amg_solve", self.handle, rhs, x, n_columns, n_columns, float(tol), int(max_outer),
+            int(max(1, min(maxiter, AMG_MAX_INNER))), float(inner_tol), iters, residual, status,
+            DEFAULT_STREAM,
+        )  # fmt: skip
+        return (np.frombuffer(iters, dtype=np.int32).copy(), np.frombuffer(residual).copy(),
+                np.frombuffer(status, dtype=np.int32).copy())
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            _lib.lib.ob_amg_destroy(self.handle)
+            self.handle = ctypes.c_void_p(0)
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def multigrid_preconditioner(matrix: CsrMatrix, n_columns: int = 1, *,
+                             seed: int = 0) -> MultigridPreconditioner:
+    """ordito/linalg.py:5020: the smoothed-aggregation V-cycle of ``matrix`` (see the class)."""
+    return MultigridPreconditioner(matrix, n_columns, seed=seed)
 
 
 def jacobi_preconditioner(matrix: CsrMatrix) -> Preconditioner:
@@ -136,15 +231,20 @@ def solve_spd(
 
     Returns ``(iterations, residual, tol)`` with ``residual`` the relative residual |r|/|b|;
     warns (``UserWarning``) when the solve stops outside ``tol``, as ordito/linalg.py:7610 does.
-    ``narrow_values`` iterates on float32 copies of the values (float64 vectors and dots).
+    ``narrow_values`` iterates on float32 copies of the values (float64 vectors and dots). A
+    ``multigrid_preconditioner`` runs the mixed-precision solve: float32 CG with the float32
+    V-cycle inside float64 iterative refinement to the same relative residual ``tol``.
     """
     n_columns = _columns(matrix, rhs, solution)
     kind = _kind(matrix, preconditioner)
     cap = CG_MAXITER_FACTOR * matrix.nrow if maxiter is None else int(maxiter)
     rhs_ptr, keep_rhs = device_pointer(rhs, np.float64)
     x_ptr, keep_x = device_pointer(solution, np.float64)
-    solver = _solver(matrix, kind, narrow_values, n_columns)
-    iters, residual = solver.solve(rhs_ptr, x_ptr, tol, cap)
+    if kind == "multigrid":
+        iters, residual, _ = preconditioner.solve(rhs_ptr, x_ptr, n_columns, tol, cap)
+    else:
+        solver = _solver(matrix, kind, narrow_values, n_columns)
+        iters, residual = solver.solve(rhs_ptr, x_ptr, tol, cap)
     if isinstance(keep_x, DeviceArray) and keep_x is not solution and not hasattr(solution, "__cuda_array_interface__"):
         np.copyto(solution, keep_x.numpy().reshape(np.shape(solution)))
     worst = float(np.max(residual)) if residual.size else 0.0
