@@ -51,6 +51,12 @@ def parse() -> argparse.Namespace:
     p.add_argument("--refine", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-precision", action="store_true")
+    p.add_argument("--no-serving", action="store_true")
+    p.add_argument("--serving-requests", type=int, default=300)
+    p.add_argument("--serving-warmup", type=int, default=150)
+    p.add_argument("--serving-rate", type=float, default=40.0)
+    p.add_argument("--serving-vmax", type=float, default=2e5)
     return p.parse_args()
 
 
@@ -69,30 +75,43 @@ def workload(args: argparse.Namespace) -> tuple[np.ndarray, np.ndarray, np.ndarr
 
 
 class Dist:
-    def __init__(self) -> None:
+    """Replicas: every rank runs the whole workload on its own GPU; only the timing is reduced
+    (max over ranks). NCCL on GPUs, gloo where no CUDA device is visible (CPU tests)."""
+
+    def __init__(self, backend: str | None = None) -> None:
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.backend = None
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local_rank)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+            if backend is None:
+                backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local_rank)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
             self.pg = dist
             self.torch = torch
+            self.backend = backend
 
     def barrier(self) -> None:
-        if self.pg is not None:
+        if self.pg is None:
+            return
+        if self.backend == "nccl":
             self.pg.barrier(device_ids=[self.local_rank])
+        else:
+            self.pg.barrier()
 
     def max(self, value: float) -> float:
         if self.pg is None:
             return value
-        t = self.torch.tensor([value], dtype=self.torch.float64, device=f"cuda:{self.local_rank}")
+        device = f"cuda:{self.local_rank}" if self.backend == "nccl" else "cpu"
+        t = self.torch.tensor([value], dtype=self.torch.float64, device=device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
@@ -258,11 +277,52 @@ def _peaks() -> dict:
         return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
+def run_serving(args: argparse.Namespace) -> dict:
+    """The serving stream: Poisson arrivals, meshes log-uniform in size (icospheres and jittered
+    tori), 70 % of requests on one of the last 50 meshes, 1-32 sources each, 150 GB HBM budget.
+    The first ``serving_warmup`` requests fill the cache untimed (the steady state the stream
+    describes); the next ``serving_requests`` are timed at their arrival times."""
+    from ordito_b200.serving import GeodesicServer, mesh_for, serving_workload
+
+    total = args.serving_warmup + args.serving_requests
+    stream = serving_workload(2, total, args.serving_rate, v_min=1e3, v_max=args.serving_vmax)
+    meshes = {spec: mesh_for(spec) for spec in {r.mesh for r in stream}}
+    server = GeodesicServer(hbm_budget=150 << 30, max_columns=64, slots=4)
+    try:
+        for r in stream[: args.serving_warmup]:
+            server.submit(*meshes[r.mesh], r.sources)
+        server.reset_stats()
+        timed = stream[args.serving_warmup:]
+        futures = []
+        origin = time.perf_counter() - timed[0].arrival
+        for r in timed:
+            delay = origin + r.arrival - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            futures.append(server.submit(*meshes[r.mesh], r.sources))
+        for f in futures:
+            f.result(timeout=1800)
+        stats = server.stats()
+    finally:
+        server.close()
+    stats.update({
+        "unit": "solves/s",
+        "offered_rate_per_s": args.serving_rate,
+        "mesh_vertices": [1e3, args.serving_vmax],
+        "reuse": 0.7,
+        "hbm_budget_gb": 150,
+        "warmup_requests": args.serving_warmup,
+        "what": "GeodesicServer: continuous batching on 4 CUDA streams, resident factors keyed by "
+                "mesh hash, LRU eviction under the budget; latency = arrival to host result",
+    })
+    return stats
+
+
 def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     from oracle import heat_path as hp
     from ordito_b200 import _lib
     from ordito_b200 import heat as gheat
-    from ordito_b200.device import PinnedArray, synchronize
+    from ordito_b200.device import DeviceArray, PinnedArray, synchronize
     from ordito_b200.mesh import Trimesh
 
     _lib.call("ob_set_device", dist.local_rank)
@@ -281,8 +341,21 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     setup_s = time.perf_counter() - t0
     src, offsets, _ = gheat._source_columns(sets, n)
 
-    def step():
-        return gheat._batch_columns(mesh, solver, src, offsets, k, args.refine, True)
+    # One step = the whole batched pass, recorded once as a CUDA graph (BatchStep) and replayed
+    # with one launch on its own stream; with refinement steps, the eager pass instead.
+    stream = ctypes.c_void_p(0)
+    _lib.call("ob_stream_create", ctypes.byref(stream))
+    if args.refine == 0:
+        graph_step = gheat.BatchStep(mesh, solver, src, offsets, k,
+                                     DeviceArray.empty((k, n), np.float64), stream)
+
+        def step():
+            return graph_step.launch(stream)
+    else:
+        stream = ctypes.c_void_p(0)  # the eager pass runs on the default stream
+
+        def step():
+            return gheat._batch_columns(mesh, solver, src, offsets, k, args.refine, True)
 
     out = None
     for _ in range(max(args.warmup, 3)):
@@ -307,10 +380,10 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     synchronize()
     launches0 = _lib.launch_count()
     with Clocks(dist.local_rank) as clocks:
-        _lib.call("ob_event_record", start, None)
+        _lib.call("ob_event_record", start, stream)
         for _ in range(args.steps):
             out = step()
-        _lib.call("ob_event_record", end, None)
+        _lib.call("ob_event_record", end, stream)
         synchronize()
     launches = (_lib.launch_count() - launches0) // max(args.steps, 1)
     ms = _elapsed(start, end) / args.steps
@@ -372,6 +445,41 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     _lib.call("ob_fp64_peak", ctypes.byref(fp64), None)
     peaks = _peaks()
 
+    # Precision form: the same batch with the Poisson system on the mixed-precision multigrid solve
+    # (float32 CG and V-cycle inside float64 refinement to 1e-10), the heat system factored.
+    precision = None
+    if not args.no_precision:
+        def precise():
+            return gheat.heat_geodesic_batch(mesh, sets, refine=0, poisson="multigrid")
+        batch = precise()
+        synchronize()
+        _lib.call("ob_event_record", start, None)
+        for _ in range(3):
+            batch = precise()
+        _lib.call("ob_event_record", end, None)
+        synchronize()
+        p_ms = _elapsed(start, end) / 3
+        result = batch.numpy()
+        p_errors = [
+            hp.relative_linf(result[c], hp.heat_geodesic(vertices, faces, np.array([sources[c]]),
+                                                         operators=ops, factors=factors))
+            for c in check
+        ]
+        precision = {
+            "value": k / (p_ms / 1e3),
+            "unit": UNIT,
+            "ms_per_step": p_ms,
+            "max_rel_linf_vs_fp64_oracle": max(p_errors),
+            "multigrid_levels": solver.poisson_multigrid.grid,
+            "what": "heat_geodesic_batch(..., poisson='multigrid'): Poisson by float32 CG with the "
+                    "float32 smoothed-aggregation V-cycle inside float64 refinement to a relative "
+                    "residual of 1e-10; heat by the float64 factor (its far field is below float32)",
+        }
+
+    serving = None
+    if not args.no_serving and dist.world == 1:
+        serving = run_serving(args)
+
     if dist.rank == 0:
         line = {
             "metric": METRIC,
@@ -390,7 +498,8 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
                 "workload": WORKLOAD,
                 "queries_per_step": k,
                 "path": "served + batched: resident Trimesh, nested-dissection supernodal Cholesky "
-                        "of M - tL and -L held on the device, 64 right-hand sides per pass, "
+                        "of M - tL and -L held on the device, 64 right-hand sides per pass, the "
+                        "whole pass recorded once as a CUDA graph (one launch a step), "
                         f"{args.refine} float64 refinement step(s) per solve"
                         + (" (in-place passes in the factors' ordering)" if args.refine == 0 else ""),
                 "l2": "no flush; per step the two 147 MB factors (294 MB) exceed the 126 MB L2",
@@ -414,6 +523,8 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
             },
             "resident_single_query": {"value": single_value, "unit": UNIT,
                                       "what": "heat_geodesic_batch(mesh, [[s]]): factors resident, k = 1"},
+            "precision": precision,
+            "serving": serving,
             "roofline": {
                 "bound": "hbm",
                 "kernel": "tile_product_kernel (Cholesky forward+backward pass, 64 columns)",

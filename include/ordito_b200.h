@@ -66,6 +66,17 @@ int ob_event_create(void** event);
 int ob_event_destroy(void* event);
 int ob_event_record(void* event, ob_stream_t stream);
 int ob_event_elapsed_ms(void* start, void* end, float* ms); /* synchronizes on end           */
+int ob_event_query(void* event, int* done);               /* done = 1 once the event has passed */
+int ob_mem_info(size_t* free_bytes, size_t* total_bytes); /* the device's free / total memory  */
+/* Recording a sequence of this library's calls as one CUDA graph: ob_capture_begin(stream)
+ * (a created stream), the calls on that stream, ob_capture_end -> a graph replayed by
+ * ob_graph_launch on any stream; *kernels = the kernel launches one replay makes (counted by
+ * ob_launch_count at each replay). The recorded calls must not allocate persistent buffers
+ * (run them once first) and their pointer arguments are fixed in the graph. */
+int ob_capture_begin(ob_stream_t stream);
+int ob_capture_end(ob_stream_t stream, void** graph, int* kernels);
+int ob_graph_launch(void* graph, ob_stream_t stream);
+int ob_graph_destroy(void* graph);
 /* Number of this library's kernel launches so far in this process (a counter the launches bump). */
 int ob_launch_count(uint64_t* count);
 
@@ -283,6 +294,19 @@ int ob_grad_div_gather(const float* xyz, const int32_t* faces, const float* norm
                        const int32_t* corner_slots, int n_vertices, int n_columns, const double* u,
                        int u_stride, const int32_t* u_iperm, double* out, int out_stride,
                        const int32_t* out_iperm, const char* out_pinned, ob_stream_t stream);
+/* ob_face_gradient_terms: once per mesh, the divergence's u-independent per-face terms,
+ * terms[F][18] float64: the gradient bases n x e_k (e_0 = v2 - v1, e_1 = v0 - v2, e_2 = v1 - v0;
+ * zero for a face of no area) and per corner e the cotangent-weighted edge sum W_e, with
+ * d_e = W_e . X (kernels/heat.py:626-687 forms the same d_e as two dot products).
+ * ob_grad_div_terms: ob_grad_div_gather's result (the same layouts, permutations and pinned rows)
+ * from those terms: per corner g = sum_k u_k (n x e_k), rescaled exactly by a power of two to
+ * s = g 2^-e (e the exponent of its largest component), d_e = (W_e . s) / |s|. */
+int ob_face_gradient_terms(const float* xyz, const int32_t* faces, int n_faces, const float* normals,
+                           const float* areas, const float* cot, double* terms, ob_stream_t stream);
+int ob_grad_div_terms(const double* terms, const int32_t* faces, const int32_t* corner_offsets,
+                      const int32_t* corner_slots, int n_vertices, int n_columns, const double* u,
+                      int u_stride, const int32_t* u_iperm, double* out, int out_stride,
+                      const int32_t* out_iperm, const char* out_pinned, ob_stream_t stream);
 int ob_seed_permuted(const int32_t* sources, const int32_t* source_offsets, int n_columns,
                      int n_vertices, const int32_t* iperm, const char* pinned, int stride,
                      double* rhs, ob_stream_t stream);

@@ -54,6 +54,12 @@ SIGNATURES: dict[str, list] = {
     "ob_event_destroy": [P],
     "ob_event_record": [P, P],
     "ob_event_elapsed_ms": [P, P, POINTER(c_float)],
+    "ob_event_query": [P, POINTER(c_int)],
+    "ob_mem_info": [POINTER(c_size_t), POINTER(c_size_t)],
+    "ob_capture_begin": [P],
+    "ob_capture_end": [P, POINTER(c_void_p), POINTER(c_int)],
+    "ob_graph_launch": [P, P],
+    "ob_graph_destroy": [P],
     "ob_launch_count": [POINTER(c_uint64)],
     "ob_pattern_workspace": [I, I, POINTER(c_size_t)],
     "ob_pattern_build": [P, I, I, P, P, P, P, P, P, c_size_t, P],
@@ -96,6 +102,8 @@ SIGNATURES: dict[str, list] = {
     "ob_corner_index_workspace": [I, I, POINTER(c_size_t)],
     "ob_corner_index": [P, I, I, P, P, P, c_size_t, P],
     "ob_grad_div_gather": [P, P, P, P, P, P, P, I, I, P, I, P, P, I, P, P, P],
+    "ob_face_gradient_terms": [P, P, I, P, P, P, P, P],
+    "ob_grad_div_terms": [P, P, P, P, I, I, P, I, P, P, I, P, P, P],
     "ob_seed_permuted": [P, P, I, I, P, P, I, P, P],
     "ob_shift_permuted": [P, I, I, P, P, P, I, I, P, P],
     "ob_chol_time_solve": [P, I, I, POINTER(c_float), P],

@@ -104,13 +104,14 @@ class SparseCholesky:
                   ctypes.byref(sol), DEFAULT_STREAM)
         return int(rhs.value), int(sol.value)
 
-    def work(self, n_columns: int) -> tuple[int, int, int, int, int]:
+    def work(self, n_columns: int, stream: Any = None) -> tuple[int, int, int, int, int]:
         """``(B, X, stride, iperm, pinned)`` device pointers of the factor's own buffers in its
         numbering (``ob_chol_work``), for pipelines that stay in it."""
         b, x, iperm, pinned = (ctypes.c_void_p(0) for _ in range(4))
         stride = ctypes.c_int(0)
         _lib.call("ob_chol_work", self.handle, int(n_columns), ctypes.byref(b), ctypes.byref(x),
-                  ctypes.byref(stride), ctypes.byref(iperm), ctypes.byref(pinned), DEFAULT_STREAM)
+                  ctypes.byref(stride), ctypes.byref(iperm), ctypes.byref(pinned),
+                  stream if stream is not None else DEFAULT_STREAM)
         return int(b.value), int(x.value), int(stride.value), int(iperm.value), int(pinned.value)
 
     def solve_in_place(self, n_columns: int, stream: Any = None) -> None:

@@ -1397,6 +1397,7 @@ int inner_graph(Amg* M, Work* W) {
         return cuda_status(e, "cudaGraphAddNode(conditional)");
     }
     cudaGraph_t body = params.conditional.phGraph_out[0];
+    std::lock_guard<std::recursive_mutex> guard(capture_mutex());
     e = cudaStreamBeginCaptureToGraph(M->capture, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) {
         cudaGraphDestroy(graph);

@@ -778,7 +778,10 @@ int dev_alloc(Factor* F, void** p, size_t bytes, cudaStream_t stream) {
 
 void factor_release(Factor* F) {
     if (F == nullptr) return;
-    cudaDeviceSynchronize();
+    {
+        std::lock_guard<std::recursive_mutex> guard(capture_mutex());
+        cudaDeviceSynchronize();
+    }
     for (auto& g : F->graphs) cudaGraphExecDestroy(g.exec);
     if (F->capture) cudaStreamDestroy(F->capture);
     for (void* p : F->owned) cudaFree(p);
@@ -965,6 +968,18 @@ int ensure_work(Factor* F, int k, cudaStream_t stream) {
     OB_CUDA(cudaStreamSynchronize(stream));
     for (auto& g : F->graphs) cudaGraphExecDestroy(g.exec);
     F->graphs.clear();
+    // The smaller buffers go (no graph names them any more): one set of six at the widest width.
+    const size_t old_vec = sizeof(double) * (size_t)F->n * (F->cap_k > 0 ? even_columns(F->cap_k) : 0);
+    for (double** p : {&F->B, &F->Y, &F->X, &F->R, &F->RHS, &F->SOL}) {
+        if (*p == nullptr) continue;
+        auto it = std::find(F->owned.begin(), F->owned.end(), (void*)*p);
+        if (it != F->owned.end()) {
+            F->owned.erase(it);
+            F->bytes -= old_vec;
+            OB_CUDA(cudaFreeAsync(*p, stream));
+        }
+        *p = nullptr;
+    }
     const size_t vec = sizeof(double) * (size_t)F->n * even_columns(k);
     for (double** p : {&F->B, &F->Y, &F->X, &F->R, &F->RHS, &F->SOL}) {
         int st = dev_alloc(F, (void**)p, vec, stream);
@@ -1072,6 +1087,7 @@ int solve_graph(Factor* F, int k, int refine, const int* offsets, const int* col
         }
     if (F->capture == nullptr) OB_CUDA(cudaStreamCreateWithFlags(&F->capture, cudaStreamNonBlocking));
     // Launches are counted at each replay (the graph's kernel nodes), not at capture.
+    std::lock_guard<std::recursive_mutex> guard(capture_mutex());
     suppress_counting(1);
     cudaError_t e = cudaStreamBeginCapture(F->capture, cudaStreamCaptureModeThreadLocal);
     // refine < 0 records the bare triangular passes B -> X in the factor's own numbering.
@@ -1269,6 +1285,15 @@ int ob_chol_solve_in_place(void* factor, int n_columns, ob_stream_t stream_) {
     cudaStream_t stream = as_stream(stream_);
     OB_REQUIRE(factor && n_columns >= 1, "ob_chol_solve_in_place: bad argument");
     Factor* F = static_cast<Factor*>(factor);
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    OB_CUDA(cudaStreamIsCapturing(stream, &capturing));
+    if (capturing == cudaStreamCaptureStatusActive) {
+        // Recorded into the caller's graph: the passes' kernels themselves (the buffers must
+        // already hold n_columns: a capture cannot allocate them).
+        OB_REQUIRE(n_columns <= F->cap_k, "ob_chol_solve_in_place: %d columns not prepared before "
+                   "capture (ob_chol_work first)", n_columns);
+        return triangular_solves(F, even_columns(n_columns), stream);
+    }
     int st = ensure_work(F, n_columns, stream);
     if (st) return st;
     Factor::Recorded* g = nullptr;

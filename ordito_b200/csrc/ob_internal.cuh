@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <cstdio>
+#include <mutex>
 #include <string>
 
 #include "../../include/ordito_b200.h"
@@ -50,6 +51,12 @@ inline int ceil_div(long long a, long long b) { return static_cast<int>((a + b -
 inline size_t align_up(size_t bytes, size_t alignment = 256) {
     return (bytes + alignment - 1) / alignment * alignment;
 }
+
+// Serialises graph captures against device-wide synchronisation across host threads: a
+// cudaDeviceSynchronize while any thread's stream is capturing fails (and invalidates nothing
+// only because it is refused). Every capture holds it from begin to end, every device-wide
+// synchronisation while it runs; recursive, so a capturing thread may take it again.
+std::recursive_mutex& capture_mutex();
 
 // Number of SMs of the current device (cached per process; the library targets one device model).
 int sm_count();

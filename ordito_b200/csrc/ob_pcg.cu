@@ -603,6 +603,7 @@ int loop_graph(Solver* S, int mode, int rounds, int maxiter, int check_rounds, d
         return cuda_status(e, "cudaGraphAddNode(conditional)");
     }
     cudaGraph_t body = params.conditional.phGraph_out[0];
+    std::lock_guard<std::recursive_mutex> guard(capture_mutex());
     e = cudaStreamBeginCaptureToGraph(S->capture, body, nullptr, nullptr, 0,
                                       cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) {
@@ -796,7 +797,10 @@ int ob_pcg_create(int n, const int32_t* offsets, const int32_t* columns, const d
 int ob_pcg_destroy(void* solver) {
     if (solver == nullptr) return OB_OK;
     Solver* S = static_cast<Solver*>(solver);
-    cudaDeviceSynchronize();
+    {
+        std::lock_guard<std::recursive_mutex> guard(capture_mutex());
+        cudaDeviceSynchronize();
+    }
     solver_release(S);
     return OB_OK;
 }

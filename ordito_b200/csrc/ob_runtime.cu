@@ -1,5 +1,6 @@
 // Runtime plumbing behind the C ABI: error strings, device memory, copies, streams and events.
 #include <atomic>
+#include <vector>
 #include <cstdarg>
 #include <cstdio>
 
@@ -25,6 +26,11 @@ void count_launch(uint64_t n) {
 }
 
 void suppress_counting(int delta) { g_suppress += delta; }
+
+std::recursive_mutex& capture_mutex() {
+    static std::recursive_mutex mutex;
+    return mutex;
+}
 
 int sm_count() {
     static int cached = 0;
@@ -148,6 +154,7 @@ int ob_stream_synchronize(ob_stream_t stream) {
 }
 
 int ob_device_synchronize(void) {
+    std::lock_guard<std::recursive_mutex> guard(capture_mutex());
     OB_CUDA(cudaDeviceSynchronize());
     return OB_OK;
 }
@@ -176,6 +183,108 @@ int ob_event_elapsed_ms(void* start, void* end, float* ms) {
     OB_CUDA(cudaEventSynchronize(reinterpret_cast<cudaEvent_t>(end)));
     OB_CUDA(cudaEventElapsedTime(ms, reinterpret_cast<cudaEvent_t>(start),
                                  reinterpret_cast<cudaEvent_t>(end)));
+    return OB_OK;
+}
+
+int ob_event_query(void* event, int* done) {
+    OB_REQUIRE(event != nullptr && done != nullptr, "ob_event_query: bad argument");
+    const cudaError_t e = cudaEventQuery(reinterpret_cast<cudaEvent_t>(event));
+    if (e == cudaErrorNotReady) {
+        cudaGetLastError();  // not an error: clear it
+        *done = 0;
+        return OB_OK;
+    }
+    OB_CUDA(e);
+    *done = 1;
+    return OB_OK;
+}
+
+int ob_mem_info(size_t* free_bytes, size_t* total_bytes) {
+    OB_REQUIRE(free_bytes != nullptr && total_bytes != nullptr, "ob_mem_info: bad argument");
+    OB_CUDA(cudaMemGetInfo(free_bytes, total_bytes));
+    return OB_OK;
+}
+
+namespace {
+
+// A recorded graph and the kernel launches one replay makes (child graphs included).
+struct RecordedGraph {
+    cudaGraphExec_t exec = nullptr;
+    int kernels = 0;
+};
+
+int count_kernels(cudaGraph_t graph, int depth = 0) {
+    size_t count = 0;
+    if (depth > 8 || cudaGraphGetNodes(graph, nullptr, &count) != cudaSuccess || count == 0) return 0;
+    std::vector<cudaGraphNode_t> nodes(count);
+    if (cudaGraphGetNodes(graph, nodes.data(), &count) != cudaSuccess) return 0;
+    int kernels = 0;
+    for (cudaGraphNode_t node : nodes) {
+        cudaGraphNodeType type;
+        if (cudaGraphNodeGetType(node, &type) != cudaSuccess) continue;
+        if (type == cudaGraphNodeTypeKernel) {
+            ++kernels;
+        } else if (type == cudaGraphNodeTypeGraph) {
+            cudaGraph_t child = nullptr;
+            if (cudaGraphChildGraphNodeGetGraph(node, &child) == cudaSuccess) kernels += count_kernels(child, depth + 1);
+        }
+    }
+    return kernels;
+}
+
+}  // namespace
+
+int ob_capture_begin(ob_stream_t stream) {
+    OB_REQUIRE(stream != nullptr, "ob_capture_begin: capture needs a created stream, not the default");
+    capture_mutex().lock();  // held until ob_capture_end on this thread
+    const cudaError_t e = cudaStreamBeginCapture(as_stream(stream), cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        capture_mutex().unlock();
+        return cuda_status(e, "ob_capture_begin");
+    }
+    suppress_counting(1);
+    return OB_OK;
+}
+
+int ob_capture_end(ob_stream_t stream, void** graph, int* kernels) {
+    OB_REQUIRE(stream != nullptr && graph != nullptr, "ob_capture_end: bad argument");
+    *graph = nullptr;
+    suppress_counting(-1);
+    cudaGraph_t captured = nullptr;
+    cudaError_t e = cudaStreamEndCapture(as_stream(stream), &captured);
+    capture_mutex().unlock();
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (captured) cudaGraphDestroy(captured);
+        return cuda_status(e, "ob_capture_end");
+    }
+    auto* recorded = new RecordedGraph;
+    recorded->kernels = count_kernels(captured);
+    e = cudaGraphInstantiate(&recorded->exec, captured, 0);
+    cudaGraphDestroy(captured);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        delete recorded;
+        return cuda_status(e, "ob_capture_end: instantiate");
+    }
+    if (kernels) *kernels = recorded->kernels;
+    *graph = recorded;
+    return OB_OK;
+}
+
+int ob_graph_launch(void* graph, ob_stream_t stream) {
+    OB_REQUIRE(graph != nullptr, "ob_graph_launch: null graph");
+    auto* recorded = static_cast<RecordedGraph*>(graph);
+    OB_CUDA(cudaGraphLaunch(recorded->exec, as_stream(stream)));
+    count_launch((uint64_t)recorded->kernels);
+    return OB_OK;
+}
+
+int ob_graph_destroy(void* graph) {
+    if (graph == nullptr) return OB_OK;
+    auto* recorded = static_cast<RecordedGraph*>(graph);
+    cudaGraphExecDestroy(recorded->exec);
+    delete recorded;
     return OB_OK;
 }
 

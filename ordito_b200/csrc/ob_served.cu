@@ -131,6 +131,93 @@ __global__ void grad_div_gather_kernel(const float* __restrict__ xyz, const int*
     out[(size_t)row * out_stride + c] = (out_pinned && out_pinned[row]) ? 0.0 : acc;
 }
 
+// Per-face terms of the divergence that do not depend on u (once per mesh), 18 doubles a face:
+// the gradient bases n x e_k (e_0 = v2 - v1, e_1 = v0 - v2, e_2 = v1 - v0; zero for a face of
+// no area, whose gradient is zero) and, per corner e, the cotangent-weighted edge sum W_e with
+// d_e = W_e . X: W_0 = c2 (v1 - v0) + c1 (v2 - v0), W_1 = c0 (v2 - v1) + c2 (v0 - v1),
+// W_2 = c1 (v0 - v2) + c0 (v1 - v2) (kernels/heat.py:626-687 forms the same d_e as two dots).
+constexpr int kFaceTerms = 18;
+
+__global__ void face_gradient_terms_kernel(const float* __restrict__ xyz, const int* __restrict__ faces,
+                                           int n_faces, const float* __restrict__ normals,
+                                           const float* __restrict__ areas, const float* __restrict__ cot,
+                                           double* __restrict__ terms) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n_faces) return;
+    const d3 v0 = widen(load_f3(xyz, faces[3 * f])), v1 = widen(load_f3(xyz, faces[3 * f + 1])),
+             v2 = widen(load_f3(xyz, faces[3 * f + 2]));
+    const d3 nrm = widen(load_f3(normals, f));
+    d3 a{0, 0, 0}, b{0, 0, 0}, w{0, 0, 0};
+    if ((double)areas[f] > 0.0) {
+        a = dcross(nrm, dsub(v2, v1));
+        b = dcross(nrm, dsub(v0, v2));
+        w = dcross(nrm, dsub(v1, v0));
+    }
+    const double c0 = (double)cot[3 * f], c1 = (double)cot[3 * f + 1], c2 = (double)cot[3 * f + 2];
+    const d3 e10 = dsub(v1, v0), e20 = dsub(v2, v0), e21 = dsub(v2, v1);
+    // W_1 = c0 (v2 - v1) + c2 (v0 - v1) = c0 e21 - c2 e10; W_2 = c1 (v0 - v2) + c0 (v1 - v2)
+    // = -c1 e20 - c0 e21.
+    const d3 W0{c2 * e10.x + c1 * e20.x, c2 * e10.y + c1 * e20.y, c2 * e10.z + c1 * e20.z};
+    const d3 W1{c0 * e21.x - c2 * e10.x, c0 * e21.y - c2 * e10.y, c0 * e21.z - c2 * e10.z};
+    const d3 W2{-c1 * e20.x - c0 * e21.x, -c1 * e20.y - c0 * e21.y, -c1 * e20.z - c0 * e21.z};
+    double* T = terms + (size_t)kFaceTerms * f;
+    const double values[kFaceTerms] = {a.x, a.y, a.z, b.x, b.y, b.z, w.x, w.y, w.z,
+                                       W0.x, W0.y, W0.z, W1.x, W1.y, W1.z, W2.x, W2.y, W2.z};
+#pragma unroll
+    for (int i = 0; i < kFaceTerms; ++i) T[i] = values[i];
+}
+
+// 2^-e for the binary exponent e of `largest` (> 0), built from its exponent field: scaling by
+// it is exact, so a far-field gradient is brought to O(1) without a division's rounding before
+// its squared length is formed (kernels/predicates.py:719 stable_normalize divides by the
+// largest component instead). Exponent fields are clamped to [1, 2045] so the scale is a normal
+// number; a subnormal `largest` is then scaled by 2^1022, which keeps its square representable.
+__device__ __forceinline__ double inverse_power_of_two(double largest) {
+    long long e = (__double_as_longlong(largest) >> 52) & 0x7ff;
+    e = e < 1 ? 1 : (e > 2045 ? 2045 : e);
+    return __longlong_as_double((2046 - e) << 52);
+}
+
+// -div of the unit gradient at (vertex, column) from the per-face terms, summed over the vertex's
+// corners in ascending slot order: d_e = (W_e . s) / |s| with s = g 2^-e the rescaled gradient.
+__global__ void grad_div_terms_kernel(const double* __restrict__ terms, const int* __restrict__ faces,
+                                      const int* __restrict__ corner_offsets,
+                                      const int* __restrict__ corner_slots, int n, int k,
+                                      const double* __restrict__ u, int u_stride,
+                                      const int* __restrict__ u_iperm, double* __restrict__ out,
+                                      int out_stride, const int* __restrict__ out_iperm,
+                                      const char* __restrict__ out_pinned) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)n * out_stride) return;
+    const int v = (int)(t / out_stride), c = (int)(t % out_stride);
+    const int row = row_of(out_iperm, v);
+    if (c >= k) {
+        out[(size_t)row * out_stride + c] = 0.0;  // a pad column stays zero
+        return;
+    }
+    double acc = 0.0;
+    const int end = corner_offsets[v + 1];
+    for (int p = corner_offsets[v]; p < end; ++p) {
+        const int q = corner_slots[p];
+        const int f = q / 3, e = q - 3 * f;
+        const double u0 = u[(size_t)row_of(u_iperm, faces[3 * f]) * u_stride + c];
+        const double u1 = u[(size_t)row_of(u_iperm, faces[3 * f + 1]) * u_stride + c];
+        const double u2 = u[(size_t)row_of(u_iperm, faces[3 * f + 2]) * u_stride + c];
+        const double* T = terms + (size_t)kFaceTerms * f;
+        const double gx = fma(u0, T[0], fma(u1, T[3], u2 * T[6]));
+        const double gy = fma(u0, T[1], fma(u1, T[4], u2 * T[7]));
+        const double gz = fma(u0, T[2], fma(u1, T[5], u2 * T[8]));
+        const double largest = fmax(fabs(gx), fmax(fabs(gy), fabs(gz)));
+        if (largest == 0.0) continue;  // no gradient: the unit gradient is zero
+        const double scale = inverse_power_of_two(largest);
+        const double sx = gx * scale, sy = gy * scale, sz = gz * scale;
+        const double* W = T + 9 + 3 * e;
+        const double along = fma(sx, W[0], fma(sy, W[1], sz * W[2]));
+        acc += along * rsqrt(fma(sx, sx, fma(sy, sy, sz * sz)));
+    }
+    out[(size_t)row * out_stride + c] = (out_pinned && out_pinned[row]) ? 0.0 : acc;
+}
+
 // Seeds of k source sets in a factor's numbering: rhs (stride `stride`, zeroed first) gets 1 at
 // each source's row, 0 at pinned rows.
 __global__ void seed_permuted_kernel(const int* __restrict__ sources,
@@ -279,6 +366,35 @@ int ob_grad_div_gather(const float* xyz, const int32_t* faces, const float* norm
         xyz, faces, normals, areas, cot, corner_offsets, corner_slots, n_vertices, n_columns, u,
         u_stride, u_iperm, out, out_stride, out_iperm, out_pinned);
     OB_CHECK_LAUNCH("grad_div_gather");
+    return OB_OK;
+}
+
+int ob_face_gradient_terms(const float* xyz, const int32_t* faces, int n_faces, const float* normals,
+                           const float* areas, const float* cot, double* terms, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_faces >= 0, "ob_face_gradient_terms: bad size");
+    if (n_faces == 0) return OB_OK;
+    OB_REQUIRE(xyz && faces && normals && areas && cot && terms, "ob_face_gradient_terms: null pointer");
+    face_gradient_terms_kernel<<<ceil_div(n_faces, kThreads), kThreads, 0, stream>>>(
+        xyz, faces, n_faces, normals, areas, cot, terms);
+    OB_CHECK_LAUNCH("face_gradient_terms");
+    return OB_OK;
+}
+
+int ob_grad_div_terms(const double* terms, const int32_t* faces, const int32_t* corner_offsets,
+                      const int32_t* corner_slots, int n_vertices, int n_columns, const double* u,
+                      int u_stride, const int32_t* u_iperm, double* out, int out_stride,
+                      const int32_t* out_iperm, const char* out_pinned, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_vertices >= 0 && n_columns >= 1 && u_stride >= n_columns && out_stride >= n_columns,
+               "ob_grad_div_terms: bad size");
+    if (n_vertices == 0) return OB_OK;
+    OB_REQUIRE(terms && faces && corner_offsets && corner_slots && u && out, "ob_grad_div_terms: null pointer");
+    const long long total = (long long)n_vertices * out_stride;
+    grad_div_terms_kernel<<<ceil_div(total, kThreads), kThreads, 0, stream>>>(
+        terms, faces, corner_offsets, corner_slots, n_vertices, n_columns, u, u_stride, u_iperm, out,
+        out_stride, out_iperm, out_pinned);
+    OB_CHECK_LAUNCH("grad_div_terms");
     return OB_OK;
 }
 

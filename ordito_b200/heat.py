@@ -238,6 +238,18 @@ class HeatSolver:
         return ok
 
     @property
+    def gradient_terms(self) -> DeviceArray:
+        """The divergence's per-face terms ``[F][18]`` (``ob_face_gradient_terms``), built once."""
+        if getattr(self, "_gradient_terms", None) is None:
+            mesh, ops = self._mesh, self.operators
+            terms = DeviceArray.empty((max(mesh.n_faces, 1), 18), np.float64)
+            _lib.call("ob_face_gradient_terms", mesh.vertices.ptr, mesh.faces.ptr, mesh.n_faces,
+                      ops.face_normals.ptr, ops.face_areas.ptr, ops.cot_entries.ptr, terms.ptr,
+                      DEFAULT_STREAM)
+            self._gradient_terms = terms
+        return self._gradient_terms
+
+    @property
     def poisson_multigrid(self) -> Any:
         """The Poisson system's smoothed-aggregation hierarchy, built on first use and kept."""
         if getattr(self, "_poisson_multigrid", None) is None:
@@ -314,22 +326,28 @@ def _require_sources(sources: Any, n_vertices: int) -> DeviceArray:
     return src.reshape(src.size)
 
 
+def _divergence(mesh: Trimesh, solver: "HeatSolver", k: int, u: int, u_stride: int, u_iperm: Any,
+                out: int, out_stride: int, out_iperm: Any, out_pinned: Any, stream: Any) -> None:
+    """``-div`` of the per-face unit gradients of ``k`` heat columns, gathered per vertex over its
+    corners in ascending slot order (no atomics: the same bits on every run, the reference's
+    deterministic mode, ordito/heat.py:3170-3232, as the only mode), from the solver's per-face
+    terms (``ob_grad_div_terms``)."""
+    corner_offsets, corner_slots = mesh.corner_index
+    _lib.call(
+        "ob_grad_div_terms", solver.gradient_terms.ptr, mesh.faces.ptr, corner_offsets.ptr,
+        corner_slots.ptr, mesh.n_vertices, k, u, u_stride, u_iperm, out, out_stride, out_iperm,
+        out_pinned, stream,
+    )  # fmt: skip
+
+
 def _distance_from_heat(mesh: Trimesh, solver: HeatSolver, sources: DeviceArray,
                         heat: DeviceArray, n_columns: int = 1,
                         source_offsets: DeviceArray | None = None) -> DeviceArray:
     """Divergence, Poisson solve and shift (ordito/heat.py:3052-3131)."""
-    operators = solver.operators
     n = mesh.n_vertices
     neg_div = DeviceArray.empty(n * n_columns, np.float64)
-    # Gathered per vertex over its corners in ascending order: no atomics, the same bits on every
-    # run (the reference's deterministic mode, ordito/heat.py:3170-3232, as its only mode).
-    corner_offsets, corner_slots = mesh.corner_index
-    _lib.call(
-        "ob_grad_div_gather", mesh.vertices.ptr, mesh.faces.ptr, operators.face_normals.ptr,
-        operators.face_areas.ptr, operators.cot_entries.ptr, corner_offsets.ptr, corner_slots.ptr,
-        n, n_columns, heat.ptr, n_columns, None, neg_div.ptr, n_columns, None, None,
-        DEFAULT_STREAM,
-    )  # fmt: skip
+    _divergence(mesh, solver, n_columns, heat.ptr, n_columns, None, neg_div.ptr, n_columns, None,
+                None, DEFAULT_STREAM)
     phi = DeviceArray.zeros(n * n_columns, np.float64)
     solver.solve_poisson(neg_div, phi)
     _lib.call(
@@ -404,8 +422,6 @@ def _batch_multigrid(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offs
     """The batched pass with the Poisson system on the mixed-precision multigrid solve."""
     n = mesh.n_vertices
     heat_factor = solver.heat_factor
-    operators = solver.operators
-    corner_offsets, corner_slots = mesh.corner_index
     neg_div = DeviceArray.empty(n * k, np.float64)
     if refine == 0:
         h_rhs, h_sol, h_stride, h_iperm, h_pinned = heat_factor.work(k)
@@ -419,11 +435,8 @@ def _batch_multigrid(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offs
         _lib.call("ob_seed_columns", src.ptr, offsets.ptr, k, n, heat_rhs, invalid.ptr, DEFAULT_STREAM)
         heat_factor.solve_pointers(0, 0, k, refine)
         heat_stride, heat_iperm = k, None
-    _lib.call(
-        "ob_grad_div_gather", mesh.vertices.ptr, mesh.faces.ptr, operators.face_normals.ptr,
-        operators.face_areas.ptr, operators.cot_entries.ptr, corner_offsets.ptr, corner_slots.ptr,
-        n, k, heat_sol, heat_stride, heat_iperm, neg_div.ptr, k, None, None, DEFAULT_STREAM,
-    )  # fmt: skip
+    _divergence(mesh, solver, k, heat_sol, heat_stride, heat_iperm, neg_div.ptr, k, None, None,
+                DEFAULT_STREAM)
     phi = DeviceArray.zeros(n * k, np.float64)
     cycle = solver.poisson_multigrid
     iters, residual, status = cycle.solve(neg_div.ptr, phi.ptr, k, _MULTIGRID_POISSON_TOLERANCE,
@@ -441,7 +454,8 @@ def _batch_multigrid(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offs
 
 
 def _batch_columns(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offsets: DeviceArray,
-                   k: int, refine: int, transpose: bool) -> DeviceArray:
+                   k: int, refine: int, transpose: bool, *, stream: Any = None,
+                   out: DeviceArray | None = None) -> DeviceArray:
     """The batched pass over resident, validated source columns.
 
     Without refinement the pass stays in the factors' shared ordering from the seeds to the shift:
@@ -450,38 +464,35 @@ def _batch_columns(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offset
     the inverse permutation, and the shift reads the Poisson solution the same way and writes the
     ``(k, V)`` distances -- no permutation, copy or transpose passes. With ``refine`` each solve
     instead runs in the caller's numbering with that many float64 refinement steps.
+
+    ``stream`` (refinement-free pass only) enqueues the whole pass on that stream, and ``out`` (a
+    ``(k, V)`` float64 device buffer) receives the distances instead of a new array: the served
+    loop runs each batch this way, on its slot's stream, without allocating.
     """
     n = mesh.n_vertices
     heat_factor, poisson_factor = solver.heat_factor, solver.poisson_factor
-    operators = solver.operators
-    corner_offsets, corner_slots = mesh.corner_index
     if refine == 0:
-        h_rhs, h_sol, h_stride, h_iperm, h_pinned = heat_factor.work(k)
-        p_rhs, p_sol, p_stride, p_iperm, p_pinned = poisson_factor.work(k)
+        st = stream if stream is not None else DEFAULT_STREAM
+        h_rhs, h_sol, h_stride, h_iperm, h_pinned = heat_factor.work(k, st)
+        p_rhs, p_sol, p_stride, p_iperm, p_pinned = poisson_factor.work(k, st)
         _lib.call("ob_seed_permuted", src.ptr, offsets.ptr, k, n, h_iperm, h_pinned, h_stride,
-                  h_rhs, DEFAULT_STREAM)
-        heat_factor.solve_in_place(k)
-        _lib.call(
-            "ob_grad_div_gather", mesh.vertices.ptr, mesh.faces.ptr, operators.face_normals.ptr,
-            operators.face_areas.ptr, operators.cot_entries.ptr, corner_offsets.ptr,
-            corner_slots.ptr, n, k, h_sol, h_stride, h_iperm, p_rhs, p_stride, p_iperm, p_pinned,
-            DEFAULT_STREAM,
-        )  # fmt: skip
-        poisson_factor.solve_in_place(k)
-        out = DeviceArray.empty((k, n), np.float64)
+                  h_rhs, st)
+        heat_factor.solve_in_place(k, st)
+        _divergence(mesh, solver, k, h_sol, h_stride, h_iperm, p_rhs, p_stride, p_iperm, p_pinned, st)
+        poisson_factor.solve_in_place(k, st)
+        if out is None:
+            out = DeviceArray.empty((k, n), np.float64)
         _lib.call("ob_shift_permuted", p_sol, n, p_stride, p_iperm, src.ptr, offsets.ptr, k, 1,
-                  out.ptr, DEFAULT_STREAM)
+                  out.ptr, st)
         return out if transpose else _transposed(out, k, n)
+    if stream is not None or out is not None:
+        raise ValueError("_batch_columns: stream/out serve the refinement-free pass only")
     heat_rhs, heat_sol = heat_factor.buffers(k)
     poisson_rhs, phi = poisson_factor.buffers(k)
     invalid = solver.scratch_flag()
     _lib.call("ob_seed_columns", src.ptr, offsets.ptr, k, n, heat_rhs, invalid.ptr, DEFAULT_STREAM)
     heat_factor.solve_pointers(0, 0, k, refine)
-    _lib.call(
-        "ob_grad_div_gather", mesh.vertices.ptr, mesh.faces.ptr, operators.face_normals.ptr,
-        operators.face_areas.ptr, operators.cot_entries.ptr, corner_offsets.ptr, corner_slots.ptr,
-        n, k, heat_sol, k, None, poisson_rhs, k, None, None, DEFAULT_STREAM,
-    )  # fmt: skip
+    _divergence(mesh, solver, k, heat_sol, k, None, poisson_rhs, k, None, None, DEFAULT_STREAM)
     poisson_factor.solve_pointers(0, 0, k, refine)
     _lib.call("ob_shift", phi, n, src.ptr, src.size, offsets.ptr, k, 1, DEFAULT_STREAM)
     if not transpose:
@@ -491,6 +502,60 @@ def _batch_columns(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offset
     out = DeviceArray.empty((k, n), np.float64)
     _lib.call("ob_transpose", n, k, phi, out.ptr, DEFAULT_STREAM)
     return out
+
+
+class BatchStep:
+    """One served batch pass recorded as a CUDA graph and replayed with a single launch.
+
+    The refinement-free batched pass of ``_batch_columns`` -- seeding, the two factored
+    triangular passes, the gathered divergence and the shift -- over ``k`` columns, bound to fixed
+    device buffers: ``sources`` / ``offsets`` (read at every replay, so a caller rewrites their
+    contents between batches) and ``out`` (``(k, V)`` float64, rewritten by every replay). Built by
+    running the pass once eagerly on ``stream`` (a created stream: that prepares the factors'
+    buffers, the per-face terms and the corner index) and recording it on the same stream; the
+    graph then launches on any stream with no host work per step.
+    """
+
+    def __init__(self, mesh: Trimesh, solver: "HeatSolver", sources: DeviceArray,
+                 offsets: DeviceArray, k: int, out: DeviceArray, stream: Any) -> None:
+        import ctypes  # noqa: PLC0415
+
+        self.stream = stream
+        self.k = k
+        self.out = out
+        self._keep = (mesh, solver, sources, offsets)
+        _lib.call("ob_device_synchronize")  # buffers allocated on other streams are ready
+        _batch_columns(mesh, solver, sources, offsets, k, 0, True, stream=stream, out=out)
+        _lib.call("ob_stream_synchronize", stream)
+        _lib.call("ob_capture_begin", stream)
+        error: BaseException | None = None
+        try:
+            _batch_columns(mesh, solver, sources, offsets, k, 0, True, stream=stream, out=out)
+        except BaseException as exc:  # noqa: BLE001 -- the capture must be closed first
+            error = exc
+        handle, kernels = ctypes.c_void_p(0), ctypes.c_int(0)
+        status = _lib.lib.ob_capture_end(stream, ctypes.byref(handle), ctypes.byref(kernels))
+        if error is not None:
+            raise error
+        _lib.check(status, "ob_capture_end")
+        self.handle = handle
+        self.kernels = int(kernels.value)
+
+    def launch(self, stream: Any = None) -> DeviceArray:
+        """Replay the pass on ``stream`` (default: the recording stream); returns ``out``."""
+        _lib.call("ob_graph_launch", self.handle, self.stream if stream is None else stream)
+        return self.out
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            _lib.lib.ob_graph_destroy(self.handle)
+            self.handle.value = None
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _transposed(array: DeviceArray, rows: int, cols: int) -> DeviceArray:

@@ -129,6 +129,78 @@ def test_gathered_divergence_matches_the_scattered_one_and_repeats_bit_for_bit(g
     assert np.allclose(b, a, rtol=1e-12, atol=1e-12 * np.abs(a).max())
 
 
+@pytest.mark.parametrize("k", [1, 3, 64])
+def test_divergence_from_face_terms(gpu, k: int) -> None:
+    # The per-face-terms divergence agrees with the gathered one, repeats bit for bit, and -- its
+    # gradient rescaled by an exact power of two -- is unchanged bit for bit when u is scaled by
+    # 2^-900, the far field's magnitude (the unit gradient is scale-free).
+    from ordito_b200 import _lib
+
+    v, f = meshes.bumpy_sphere()
+    n = v.shape[0]
+    mesh = Trimesh(v, f.reshape(-1))
+    terms = mesh.face_terms
+    rng = np.random.default_rng(k)
+    host_u = np.exp(-5.0 * rng.random((n, k))).reshape(-1)
+    u = DeviceArray.from_host(host_u)
+    tiny = DeviceArray.from_host(np.ldexp(host_u, -900))
+    offsets, slots = mesh.corner_index
+    gathered = DeviceArray.empty(n * k, np.float64)
+    _lib.call("ob_grad_div_gather", mesh.vertices.ptr, mesh.faces.ptr, terms.normals.ptr,
+              terms.areas.ptr, terms.cot.ptr, offsets.ptr, slots.ptr, n, k, u.ptr, k, None,
+              gathered.ptr, k, None, None, None)
+    table = DeviceArray.empty((mesh.n_faces, 18), np.float64)
+    _lib.call("ob_face_gradient_terms", mesh.vertices.ptr, mesh.faces.ptr, mesh.n_faces,
+              terms.normals.ptr, terms.areas.ptr, terms.cot.ptr, table.ptr, None)
+    outs = []
+    for field in (u, u, tiny):
+        out = DeviceArray.empty(n * k, np.float64)
+        _lib.call("ob_grad_div_terms", table.ptr, mesh.faces.ptr, offsets.ptr, slots.ptr, n, k,
+                  field.ptr, k, None, out.ptr, k, None, None, None)
+        outs.append(out.numpy())
+    reference = gathered.numpy()
+    assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(outs[0], outs[2])
+    assert np.allclose(outs[0], reference, rtol=1e-12, atol=1e-12 * np.abs(reference).max())
+
+
+def test_recorded_batch_step_matches_the_eager_pass(gpu) -> None:
+    import ctypes
+
+    from ordito_b200 import _lib
+
+    v, f = meshes.small_torus()
+    n = v.shape[0]
+    rng = np.random.default_rng(9)
+    sets = [rng.choice(n, size=int(s), replace=False).tolist() for s in rng.integers(1, 4, size=8)]
+    mesh = Trimesh(v, f.reshape(-1))
+    solver = mesh.heat_solver(None, method="meshlab")
+    assert solver.factor()
+    src, offsets, k = gheat._source_columns(sets, n)
+    eager = gheat._batch_columns(mesh, solver, src, offsets, k, 0, True).numpy()
+    stream = ctypes.c_void_p(0)
+    _lib.call("ob_stream_create", ctypes.byref(stream))
+    step = gheat.BatchStep(mesh, solver, src, offsets, k, DeviceArray.empty((k, n), np.float64), stream)
+    assert step.kernels > 0
+    before = _lib.launch_count()
+    out = step.launch()
+    _lib.call("ob_stream_synchronize", stream)
+    assert _lib.launch_count() - before == step.kernels
+    assert hp.relative_linf(out.numpy(), eager) <= 1e-12
+    # New sources written into the same buffers are read by the next replay.
+    other = [[int(s[0]) + 1] for s in sets]
+    src2, offsets2, _ = gheat._source_columns(other, n)
+    _lib.call("ob_memcpy", src.ptr, src2.ptr, src2.nbytes, 2, None, 1)
+    _lib.call("ob_memcpy", offsets.ptr, offsets2.ptr, offsets2.nbytes, 2, None, 1)
+    step.launch()
+    _lib.call("ob_stream_synchronize", stream)
+    replay = step.out.numpy()
+    expected = gheat._batch_columns(mesh, solver, src2, offsets2, k, 0, True).numpy()
+    assert hp.relative_linf(replay, expected) <= 1e-12
+    step.close()
+    _lib.call("ob_stream_destroy", stream)
+
+
 @pytest.mark.parametrize("refine", [0, 1])
 def test_batched_modes_agree_and_repeat(gpu, refine: int) -> None:
     v, f = meshes.small_torus()

@@ -1,0 +1,98 @@
+"""The continuous-batching server (GPU): a result served in a mix of concurrent requests on
+several meshes equals the same query run alone, meshes are evicted and rebuilt under a small HBM
+budget, and invalid requests fail their future."""
+
+from __future__ import annotations
+
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from oracle import heat_path as hp
+from ordito_b200 import heat as gheat
+from ordito_b200.mesh import Trimesh
+from ordito_b200.serving import ESTIMATED_BYTES_PER_VERTEX, GeodesicServer, mesh_for
+
+pytestmark = pytest.mark.gpu
+
+SAME_TOL = 1e-12  # in the mix vs alone: the same passes, up to split-K atomic ordering
+ORACLE_TOL = 1e-5  # against the float64 oracle
+
+SPECS = [("icosphere", 4, 11), ("torus", 64, 32, 3), ("icosphere", 3, 5)]
+
+
+def rel_err(a: np.ndarray, b: np.ndarray) -> float:
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _requests(rng, meshes, count):
+    out = []
+    for _ in range(count):
+        m = int(rng.integers(len(meshes)))
+        n = meshes[m][0].shape[0]
+        out.append((m, rng.choice(n, size=int(rng.integers(1, 9)), replace=False).astype(np.int32)))
+    return out
+
+
+def _alone(meshes, m, sources, cache):
+    if m not in cache:
+        cache[m] = Trimesh(*meshes[m])
+    return gheat.heat_geodesic_batch(cache[m], [sources.tolist()], refine=0).numpy()[0]
+
+
+def test_results_alone_equal_results_in_the_mix(gpu) -> None:
+    meshes = [mesh_for(spec) for spec in SPECS]
+    rng = np.random.default_rng(0)
+    work = _requests(rng, meshes, 90)
+    server = GeodesicServer(max_columns=16, slots=3)
+    futures = [None] * len(work)
+
+    def feed() -> None:
+        for i, (m, sources) in enumerate(work):
+            futures[i] = server.submit(*meshes[m], sources)
+            if i % 7 == 0:
+                time.sleep(0.002)  # later requests arrive while earlier ones are on the GPU
+
+    feeder = threading.Thread(target=feed)
+    feeder.start()
+    feeder.join()
+    results = [f.result(timeout=300) for f in futures]
+    stats = server.stats()
+    server.close()
+    assert stats["requests"] == len(work) and stats["cache_misses"] == len(SPECS)
+    assert stats["batches"] < len(work)  # requests were batched
+    assert stats["p50_ms"] is not None and stats["p99_ms"] >= stats["p50_ms"]
+    cache = {}
+    for (m, sources), got in zip(work, results):
+        assert rel_err(got, _alone(meshes, m, sources, cache)) <= SAME_TOL
+    for (m, sources), got in list(zip(work, results))[:3]:
+        v, f = meshes[m]
+        assert rel_err(got, hp.heat_geodesic(v, f, sources)) <= ORACLE_TOL
+
+
+def test_eviction_under_a_small_budget(gpu) -> None:
+    meshes = [mesh_for(spec) for spec in SPECS[:2]]
+    largest = max(v.shape[0] for v, _ in meshes)
+    server = GeodesicServer(hbm_budget=int(1.5 * ESTIMATED_BYTES_PER_VERTEX * largest), max_columns=4, slots=2)
+    rng = np.random.default_rng(1)
+    cache = {}
+    for m, sources in _requests(rng, meshes, 6):
+        got = server.submit(*meshes[m], sources).result(timeout=300)
+        assert rel_err(got, _alone(meshes, m, sources, cache)) <= SAME_TOL
+    stats = server.stats()
+    server.close()
+    assert stats["evictions"] >= 1 and stats["resident_meshes"] == 1
+
+
+def test_invalid_requests_fail_their_future(gpu) -> None:
+    v, f = mesh_for(SPECS[2])
+    server = GeodesicServer(max_columns=4, slots=1)
+    with pytest.raises(ValueError):
+        server.submit(v, f, [v.shape[0]]).result(timeout=60)
+    with pytest.raises(ValueError):
+        server.submit(v, f, np.arange(40)).result(timeout=60)
+    ok = server.submit(v, f, [0]).result(timeout=300)
+    server.close()
+    assert ok[0] == 0.0 and np.all(ok >= -1e-6)
