@@ -356,6 +356,18 @@ int ob_amg_solve(void* amg, const double* b, double* x, int k, int ld, double to
 int ob_amg_host_setup(int n, const int32_t* offsets, const int32_t* columns, const double* values,
                       unsigned seed, long long* rows, long long* nnz, int capacity, int* levels);
 
+/* ---- a12: the marched settled solve --------------------------------------------------------
+ * Replaces ordito/linalg.py:2765 _march_settled (kernels/linalg.py:1229-1545): x = A^-1 rhs for
+ * one column, band by band outward from rhs's support, every entry to its own relative
+ * precision -- the settled solve's fallback where the operator's factorisation is refused. Bands
+ * grow breadth first from the finished rows; each band system (Dirichlet data from the finished
+ * neighbours, zero beyond, scaled so its front is O(1)) is solved by float64 CG to a relative
+ * residual of 1e-14; rows within e^14 of the band's peak and e^16 above its outer layer are
+ * finished. x is overwritten (its input is ignored). info[0..2] (may be NULL) = bands, CG rounds,
+ * band rows solved. Synchronises the stream (the loop reads each band's size back). */
+int ob_march_solve(int n, const int32_t* offsets, const int32_t* columns, const double* values,
+                   const double* rhs, double* x, long long* info, ob_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -108,6 +108,7 @@ SIGNATURES: dict[str, list] = {
     "ob_shift_permuted": [P, I, I, P, P, P, I, I, P, P],
     "ob_chol_time_solve": [P, I, I, POINTER(c_float), P],
     "ob_chol_info": [P, POINTER(ctypes.c_longlong)],
+    "ob_march_solve": [I, P, P, P, P, P, POINTER(ctypes.c_longlong), P],
     "ob_amg_setup": [I, P, P, P, ctypes.c_uint, POINTER(c_void_p), P],
     "ob_amg_destroy": [P],
     "ob_amg_info": [P, POINTER(ctypes.c_longlong)],

@@ -287,7 +287,10 @@ class HeatSolver:
             factorization=kept["factorization"],
             narrow_values=True,
         )
-        if not held and kept["factorization"].factorization is not None:
+        # A rejected settled iterate (answered by the factor or, past the budget, the march)
+        # marks the mesh ill-conditioned for its Poisson solve (ordito/heat.py:4394-4404).
+        if not held and (kept["factorization"].factorization is not None
+                         or getattr(kept["factorization"], "iterate_rejected", False)):
             self._ill_conditioned = True
 
     def solve_poisson(self, rhs: Any, solution: Any) -> None:
@@ -300,12 +303,15 @@ class HeatSolver:
         if factorization.factorization is not None:
             factorization.solve(rhs, solution, tol=twl.SETTLE_DIRECT_TOLERANCE)
             return
+        # An unfactorable (over the budget) or ill-conditioned system takes the multigrid
+        # preconditioner, otherwise the Chebyshev polynomial (ordito/heat.py:4118-4150).
+        unfactorable = factorization.refused or self._ill_conditioned
         twl.solve_spd(
             operators.poisson_system,
             rhs,
             solution,
             tol=_CG_TOLERANCE,
-            preconditioner=operators.poisson_preconditioner,
+            preconditioner=self.poisson_multigrid if unfactorable else operators.poisson_preconditioner,
             name="heat_geodesic",
         )
 

@@ -259,6 +259,37 @@ def solve_spd(
     return int(iters.max()), worst, float(tol)
 
 
+def march_settled(matrix: CsrMatrix, rhs: Any, solution: Any) -> int:
+    """Solve ``matrix x = rhs`` band by band, every entry to its own precision (ordito/linalg.py:
+    2765 ``_march_settled``; ``ob_march_solve``), into ``solution``, column by column for an
+    ``[n][k]`` layout. Returns the band solves' CG rounds."""
+    n_columns = _columns(matrix, rhs, solution)
+    n = matrix.nrow
+    rhs_ptr, keep_rhs = device_pointer(rhs, np.float64)
+    x_ptr, keep_x = device_pointer(solution, np.float64)
+    info = (ctypes.c_longlong * 3)()
+    rounds = 0
+    if n_columns == 1:
+        _lib.call("ob_march_solve", n, matrix.offsets.ptr, matrix.columns.ptr, matrix.values.ptr,
+                  rhs_ptr, x_ptr, info, DEFAULT_STREAM)
+        rounds = int(info[1])
+    else:
+        # [n][k] -> [k][n]: each column contiguous for its march, then back.
+        columns_in = DeviceArray.empty((n_columns, n), np.float64)
+        columns_out = DeviceArray.empty((n_columns, n), np.float64)
+        _lib.call("ob_transpose", n, n_columns, rhs_ptr, columns_in.ptr, DEFAULT_STREAM)
+        for c in range(n_columns):
+            _lib.call("ob_march_solve", n, matrix.offsets.ptr, matrix.columns.ptr,
+                      matrix.values.ptr, columns_in.ptr + 8 * n * c,
+                      columns_out.ptr + 8 * n * c, info, DEFAULT_STREAM)
+            rounds += int(info[1])
+        _lib.call("ob_transpose", n_columns, n, columns_out.ptr, x_ptr, DEFAULT_STREAM)
+    if isinstance(keep_x, DeviceArray) and keep_x is not solution and not hasattr(solution, "__cuda_array_interface__"):
+        np.copyto(solution, keep_x.numpy().reshape(np.shape(solution)))
+    del keep_rhs
+    return rounds
+
+
 def solve_spd_settled(
     matrix: CsrMatrix,
     rhs: Any,
@@ -308,5 +339,9 @@ def solve_spd_settled(
         if fallback.factor():
             DeviceArray(x_ptr, (matrix.nrow * n_columns,), np.float64, owned=False).fill_zero()
             fallback.solve(rhs, solution, tol=SETTLE_DIRECT_TOLERANCE, componentwise=True)
+        else:
+            # The factorisation is refused (over the budget): the band march reaches every entry
+            # with its own precision (ordito/linalg.py:2574-2590).
+            march_settled(matrix, rhs, solution)
     del keep_rhs, keep_x
     return DeviceArray.from_host(np.array([rounds], dtype=np.int32))
