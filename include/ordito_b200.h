@@ -167,6 +167,13 @@ int ob_shift_noalloc(double* phi, int n_vertices, const int32_t* sources, int n_
 int ob_pcg_create(int n, const int32_t* offsets, const int32_t* columns, const double* values,
                   int n_columns, int precond, int narrow, void** solver, ob_stream_t stream);
 int ob_pcg_destroy(void* solver);
+/* A solver keeps its own copy of the operator it was created for. ob_pcg_rebind copies another
+ * operator of the same shape (n, nnz) into it and redoes the value-dependent setup (inverse
+ * diagonal, Chebyshev steps, float32 copy) on the stream -- its recorded loops replay unchanged,
+ * which is how an operator rebuilt per call (ordito/linalg.py:1389-1396: "copied into a kept
+ * state of that shape, which replays too") avoids a new state and a new recording. */
+int ob_pcg_rebind(void* solver, const int32_t* offsets, const int32_t* columns,
+                  const double* values, long long nnz, ob_stream_t stream);
 /* solve_spd (linalg.py:1356): stops a column at |r| <= tol |b| (2-norm), or at maxiter rounds.
  * Host read-back of iterations[n_columns] and residual[n_columns] (|r| / |b|) when non-NULL. */
 int ob_pcg_solve(void* solver, const double* rhs, double* x, double tol, int maxiter,
@@ -315,6 +322,9 @@ int ob_shift_permuted(const double* phi, int n_vertices, int stride, const int32
                       int orient, double* out, ob_stream_t stream);
 int ob_chol_time_solve(void* factor, int n_columns, int reps, float* ms, ob_stream_t stream);
 int ob_chol_info(void* factor, long long* info);
+/* The work buffers' generation: it changes whenever ob_chol_work's pointers do (a wider k than
+ * any before reallocates them), so a graph recorded over them must be recorded again. */
+int ob_chol_work_generation(void* factor, long long* generation);
 
 /* ---- Smoothed-aggregation multigrid and the mixed-precision solve --------------------------
  *

@@ -72,6 +72,7 @@ SIGNATURES: dict[str, list] = {
     "ob_shift_noalloc": [P, I, P, I, P, I, I, P],
     "ob_pcg_create": [I, P, P, P, I, I, I, POINTER(c_void_p), P],
     "ob_pcg_destroy": [P],
+    "ob_pcg_rebind": [P, P, P, P, ctypes.c_longlong, P],
     "ob_pcg_solve": [P, P, P, D, I, POINTER(c_int), POINTER(c_double), P],
     "ob_pcg_settle": [P, P, P, I, D, I, I, POINTER(c_int), POINTER(c_int), P],
     "ob_pcg_time_matvec": [P, I, POINTER(c_float), P],
@@ -108,6 +109,7 @@ SIGNATURES: dict[str, list] = {
     "ob_shift_permuted": [P, I, I, P, P, P, I, I, P, P],
     "ob_chol_time_solve": [P, I, I, POINTER(c_float), P],
     "ob_chol_info": [P, POINTER(ctypes.c_longlong)],
+    "ob_chol_work_generation": [P, POINTER(ctypes.c_longlong)],
     "ob_march_solve": [I, P, P, P, P, P, POINTER(ctypes.c_longlong), P],
     "ob_amg_setup": [I, P, P, P, ctypes.c_uint, POINTER(c_void_p), P],
     "ob_amg_destroy": [P],

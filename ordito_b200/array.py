@@ -69,9 +69,13 @@ class CsrMatrix:
         return sp.csr_matrix((values, columns, offsets), shape=self.shape)
 
     def release(self) -> None:
-        """Drop the native solver states and factorization kept for this operator."""
-        for solver in self._solvers.values():
-            solver.close()
+        """Drop the native solver states (kept by shape for the next operator of this shape) and
+        the factorization kept for this operator."""
+        if self._solvers:
+            from ordito_b200.linalg import retire_solver  # noqa: PLC0415
+
+            for solver in self._solvers.values():
+                retire_solver(solver)
         self._solvers.clear()
         if self._factorization is not None:
             self._factorization.close()

@@ -114,6 +114,13 @@ class SparseCholesky:
                   stream if stream is not None else DEFAULT_STREAM)
         return int(b.value), int(x.value), int(stride.value), int(iperm.value), int(pinned.value)
 
+    @property
+    def generation(self) -> int:
+        """Changes whenever the buffers ``work`` points at are reallocated (``ob_chol_work_generation``)."""
+        value = ctypes.c_longlong(0)
+        _lib.call("ob_chol_work_generation", self.handle, ctypes.byref(value))
+        return int(value.value)
+
     def solve_in_place(self, n_columns: int, stream: Any = None) -> None:
         """``X = A^-1 B`` on the factor's own buffers, in its numbering (no read-back)."""
         _lib.call("ob_chol_solve_in_place", self.handle, int(n_columns),

@@ -604,6 +604,76 @@ tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ v
     tile_product(tiles[blockIdx.x], blockIdx.y * kTileCols, vals, idx, in, out, k, stage);
 }
 
+// The same tile product for a narrow batch (KP = 2, 4, 6 or 8 columns, the even stride of 1-8
+// right-hand sides), where a 64-column tensor-core tile would compute 8-32 times the flops it
+// needs: float64 FMAs in registers, the factor read once. A CTA per tile, 256 threads as (row,
+// inner-dimension slice) pairs: thread (i, s) sums A(i, kk) in[kk] over kk = k0 + s, k0 + s + 4,
+// ... for its KP columns, four steps at a time with every load of the four issued before their
+// FMAs (the kernel is load-latency bound); the slices meet in shared memory and the first applies
+// the tile's op.
+constexpr int kNarrowThreads = 256;
+constexpr int kNarrowSlices = kNarrowThreads / kTileRows;
+
+template <int KP>
+__global__ void __launch_bounds__(kNarrowThreads)
+narrow_tile_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
+                   const int* __restrict__ idx, const double* __restrict__ in, double* __restrict__ out) {
+    __shared__ double other[kNarrowSlices - 1][kTileRows][KP];
+    const Tile t = tiles[blockIdx.x];
+    const int i = threadIdx.x % kTileRows, slice = threadIdx.x / kTileRows;
+    double acc[KP];
+#pragma unroll
+    for (int c = 0; c < KP; ++c) acc[c] = 0.0;
+    if (i < t.rows) {
+        const double* M = vals + t.m;
+        auto value = [&](int kk) {
+            return t.trans ? __ldg(M + (size_t)kk * t.ld + t.r0 + i) : __ldg(M + (size_t)(t.r0 + i) * t.ld + kk);
+        };
+        auto row = [&](int kk) { return t.in_rows < 0 ? t.in_base + kk : __ldg(idx + t.in_rows + kk); };
+        auto add = [&](double a, int r) {
+            const double2* x = reinterpret_cast<const double2*>(in + (size_t)r * KP);
+#pragma unroll
+            for (int c = 0; c < KP / 2; ++c) {
+                const double2 v = __ldcg(x + c);
+                acc[2 * c] = fma(a, v.x, acc[2 * c]);
+                acc[2 * c + 1] = fma(a, v.y, acc[2 * c + 1]);
+            }
+        };
+        constexpr int kStep = kNarrowSlices;
+        int kk = t.k0 + slice;
+        for (; kk + 3 * kStep < t.k1; kk += 4 * kStep) {
+            const int r0 = row(kk), r1 = row(kk + kStep), r2 = row(kk + 2 * kStep), r3 = row(kk + 3 * kStep);
+            const double a0 = value(kk), a1 = value(kk + kStep), a2 = value(kk + 2 * kStep),
+                         a3 = value(kk + 3 * kStep);
+            add(a0, r0);
+            add(a1, r1);
+            add(a2, r2);
+            add(a3, r3);
+        }
+        for (; kk < t.k1; kk += kStep) add(value(kk), row(kk));
+    }
+    if (slice > 0) {
+#pragma unroll
+        for (int c = 0; c < KP; ++c) other[slice - 1][i][c] = acc[c];
+    }
+    __syncthreads();
+    if (slice > 0 || i >= t.rows) return;
+    const int r = t.out_rows < 0 ? t.out_base + t.r0 + i : idx[t.out_rows + t.r0 + i];
+    double* o = out + (size_t)r * KP;
+#pragma unroll
+    for (int c = 0; c < KP; ++c) {
+        double v = acc[c];
+#pragma unroll
+        for (int s2 = 0; s2 < kNarrowSlices - 1; ++s2) v += other[s2][i][c];
+        switch (t.op) {
+            case kAssign: o[c] = v; break;
+            case kAtomicSub: atomicAdd(o + c, -v); break;
+            case kSub: o[c] = __ldcg(o + c) - v; break;
+            default: atomicAdd(o + c, v); break;
+        }
+    }
+}
+
 // A phase of a triangular pass: its tiles and which work buffers (0 B, 1 Y, 2 X) it reads and
 // writes.
 struct Phase {
@@ -756,6 +826,9 @@ struct Factor {
     // RHS / SOL the caller's right-hand side and solution copied in / out (old numbering).
     int cap_k = 0;
     double *B = nullptr, *Y = nullptr, *X = nullptr, *R = nullptr, *RHS = nullptr, *SOL = nullptr;
+    // Bumped whenever the work buffers are reallocated: a graph recorded outside the factor (over
+    // ob_chol_work's pointers) is stale once it changes.
+    long long generation = 0;
     size_t bytes = 0;
     // Recorded solve graphs, keyed by (columns, refinement steps, operator arrays).
     struct Recorded {
@@ -986,6 +1059,7 @@ int ensure_work(Factor* F, int k, cudaStream_t stream) {
         if (st) return st;
     }
     F->cap_k = k;
+    ++F->generation;
     return OB_OK;
 }
 
@@ -1019,31 +1093,33 @@ int triangular_solves(Factor* F, int k, cudaStream_t stream) {
         zero_rows_kernel<<<F->n_zero, 256, 0, stream>>>(F->zero, F->n_zero, k, F->Y, F->X);
         OB_CHECK_LAUNCH("chol zero split rows");
     }
-    for (int l = 0; l < L; ++l) {
-        if (F->n_fwd_diag[l]) {
-            tile_product_kernel<<<dim3(F->n_fwd_diag[l], ct), threads, kStageBytes, stream>>>(
-                F->fwd_diag[l], F->vals, F->idx, F->B, F->Y, k);
-            OB_CHECK_LAUNCH("chol forward diagonal");
+    // A phase's launch: the float64 tensor-core tiles, or for a narrow batch (stride 2-8) the
+    // register kernel, which does not compute a 64-column tile's idle columns.
+    auto phase = [&](const Tile* tiles, int count, const double* in, double* out, const char* what) {
+        switch (k) {
+            case 2: narrow_tile_kernel<2><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, in, out); break;
+            case 4: narrow_tile_kernel<4><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, in, out); break;
+            case 6: narrow_tile_kernel<6><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, in, out); break;
+            case 8: narrow_tile_kernel<8><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, in, out); break;
+            default:
+                tile_product_kernel<<<dim3(count, ct), threads, kStageBytes, stream>>>(tiles, F->vals, F->idx,
+                                                                                     in, out, k);
         }
-        if (F->n_fwd_off[l]) {
-            tile_product_kernel<<<dim3(F->n_fwd_off[l], ct), threads, kStageBytes, stream>>>(
-                F->fwd_off[l], F->vals, F->idx, F->Y, F->B, k);
-            OB_CHECK_LAUNCH("chol forward update");
-        }
+        OB_CHECK_LAUNCH(what);
+        return OB_OK;
+    };
+    int st = OB_OK;
+    for (int l = 0; l < L && st == OB_OK; ++l) {
+        if (F->n_fwd_diag[l]) st = phase(F->fwd_diag[l], F->n_fwd_diag[l], F->B, F->Y, "chol forward diagonal");
+        if (st == OB_OK && F->n_fwd_off[l])
+            st = phase(F->fwd_off[l], F->n_fwd_off[l], F->Y, F->B, "chol forward update");
     }
-    for (int l = L - 1; l >= 0; --l) {
-        if (F->n_bwd_off[l]) {
-            tile_product_kernel<<<dim3(F->n_bwd_off[l], ct), threads, kStageBytes, stream>>>(
-                F->bwd_off[l], F->vals, F->idx, F->X, F->Y, k);
-            OB_CHECK_LAUNCH("chol backward gather");
-        }
-        if (F->n_bwd_diag[l]) {
-            tile_product_kernel<<<dim3(F->n_bwd_diag[l], ct), threads, kStageBytes, stream>>>(
-                F->bwd_diag[l], F->vals, F->idx, F->Y, F->X, k);
-            OB_CHECK_LAUNCH("chol backward diagonal");
-        }
+    for (int l = L - 1; l >= 0 && st == OB_OK; --l) {
+        if (F->n_bwd_off[l]) st = phase(F->bwd_off[l], F->n_bwd_off[l], F->X, F->Y, "chol backward gather");
+        if (st == OB_OK && F->n_bwd_diag[l])
+            st = phase(F->bwd_diag[l], F->n_bwd_diag[l], F->Y, F->X, "chol backward diagonal");
     }
-    return OB_OK;
+    return st;
 }
 
 int grid_for(long long total) {
@@ -1336,6 +1412,12 @@ int ob_chol_time_solve(void* factor, int n_columns, int reps, float* ms, ob_stre
     if (st) return st;
     if (e != cudaSuccess) return cuda_status(e, "ob_chol_time_solve");
     *ms = total / (float)reps;
+    return OB_OK;
+}
+
+int ob_chol_work_generation(void* factor, long long* generation) {
+    OB_REQUIRE(factor && generation, "ob_chol_work_generation: bad argument");
+    *generation = static_cast<Factor*>(factor)->generation;
     return OB_OK;
 }
 

@@ -489,6 +489,32 @@ struct Solver {
     std::vector<void*> owned;
 };
 
+// Copies an operator of the solver's shape into its own arrays and derives what the iteration
+// reads from the values: the inverse diagonal, the Chebyshev steps and the float32 copy.
+int bind_operator(Solver* S, const int* offsets, const int* columns, const double* values,
+                  cudaStream_t stream) {
+    const int n = S->n;
+    const long long nnz = S->nnz;
+    OB_CUDA(cudaMemcpyAsync(const_cast<int*>(S->offsets), offsets, sizeof(int) * (size_t)(n + 1),
+                            cudaMemcpyDeviceToDevice, stream));
+    if (nnz > 0) {
+        OB_CUDA(cudaMemcpyAsync(const_cast<int*>(S->columns), columns, sizeof(int) * (size_t)nnz,
+                                cudaMemcpyDeviceToDevice, stream));
+        OB_CUDA(cudaMemcpyAsync(const_cast<double*>(S->values), values, sizeof(double) * (size_t)nnz,
+                                cudaMemcpyDeviceToDevice, stream));
+    }
+    const int setup_blocks = std::max(1, std::min(ceil_div(n, kThreads), 4 * sm_count()));
+    jacobi_setup_kernel<<<setup_blocks, kThreads, 0, stream>>>(
+        n, S->offsets, S->columns, S->values, S->inv_diag, S->maxima, S->counters + 3,
+        kChebyshevDegree - 1, S->steps);
+    OB_CHECK_LAUNCH("pcg setup");
+    if (S->narrow && nnz > 0) {
+        narrow_kernel<<<ceil_div(nnz, kThreads), kThreads, 0, stream>>>(nnz, S->values, S->values32);
+        OB_CHECK_LAUNCH("pcg narrow");
+    }
+    return OB_OK;
+}
+
 int solver_alloc(Solver* S, void** out, size_t bytes, cudaStream_t stream) {
     OB_CUDA(cudaMallocAsync(out, bytes == 0 ? 8 : bytes, stream));
     S->owned.push_back(*out);
@@ -726,9 +752,6 @@ int ob_pcg_create(int n, const int32_t* offsets, const int32_t* columns, const d
     S->k = next_pow2(n_columns);
     S->precond = precond;
     S->narrow = narrow ? 1 : 0;
-    S->offsets = offsets;
-    S->columns = columns;
-    S->values = values;
     int nnz = 0;
     cudaError_t e = cudaMemcpyAsync(&nnz, offsets + n, sizeof(int), cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
@@ -745,6 +768,13 @@ int ob_pcg_create(int n, const int32_t* offsets, const int32_t* columns, const d
     auto A = [&](void** p, size_t bytes) {
         if (st == OB_OK) st = solver_alloc(S, p, bytes, stream);
     };
+    // The solver keeps its own copy of the operator (ob_pcg_rebind copies another of the same
+    // shape in): its recorded loops name these arrays.
+    int *own_offsets = nullptr, *own_columns = nullptr;
+    double* own_values = nullptr;
+    A((void**)&own_offsets, sizeof(int) * (size_t)(n + 1));
+    A((void**)&own_columns, sizeof(int) * (size_t)std::max(nnz, 1));
+    A((void**)&own_values, sizeof(double) * (size_t)std::max(nnz, 1));
     A((void**)&S->inv_diag, sizeof(double) * n);
     for (double** v : {&S->b, &S->x, &S->r, &S->u, &S->w, &S->p, &S->s, &S->previous})
         A((void**)v, vec);
@@ -775,23 +805,29 @@ int ob_pcg_create(int n, const int32_t* offsets, const int32_t* columns, const d
         solver_release(S);
         return cuda_status(e, "ob_pcg_create: memset");
     }
-    const int setup_blocks = std::max(1, std::min(ceil_div(n, kThreads), 4 * sm_count()));
-    jacobi_setup_kernel<<<setup_blocks, kThreads, 0, stream>>>(
-        n, offsets, columns, values, S->inv_diag, S->maxima, S->counters + 3,
-        kChebyshevDegree - 1, S->steps);
-    count_launch();
-    if (S->narrow && nnz > 0) {
-        narrow_kernel<<<ceil_div(nnz, kThreads), kThreads, 0, stream>>>(nnz, values, S->values32);
-        count_launch();
+    S->offsets = own_offsets;
+    S->columns = own_columns;
+    S->values = own_values;
+    st = bind_operator(S, offsets, columns, values, stream);
+    if (st == OB_OK) {
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) st = cuda_status(e, "ob_pcg_create: setup");
     }
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    if (e != cudaSuccess) {
+    if (st != OB_OK) {
         solver_release(S);
-        return cuda_status(e, "ob_pcg_create: setup");
+        return st;
     }
     *solver = S;
     return OB_OK;
+}
+
+int ob_pcg_rebind(void* solver, const int32_t* offsets, const int32_t* columns, const double* values,
+                  long long nnz, ob_stream_t stream_) {
+    OB_REQUIRE(solver && offsets && columns && values, "ob_pcg_rebind: bad argument");
+    Solver* S = static_cast<Solver*>(solver);
+    OB_REQUIRE(nnz == S->nnz, "ob_pcg_rebind: %lld stored entries, the solver's shape has %lld", nnz,
+               S->nnz);
+    return bind_operator(S, offsets, columns, values, as_stream(stream_));
 }
 
 int ob_pcg_destroy(void* solver) {

@@ -237,6 +237,15 @@ class HeatSolver:
                 ok = kept["factorization"].factor(self._sharing(role)) and ok
         return ok
 
+    def single_query(self, sources: DeviceArray) -> DeviceArray:
+        """Distances for one validated source set with both factors held (``_SingleQuery``)."""
+        query = getattr(self, "_single_query", None)
+        if query is None or sources.size > query.capacity:
+            if query is not None:
+                query.close()
+            query = self._single_query = _SingleQuery(self._mesh, self, max(64, sources.size))
+        return query(sources)
+
     @property
     def gradient_terms(self) -> DeviceArray:
         """The divergence's per-face terms ``[F][18]`` (``ob_face_gradient_terms``), built once."""
@@ -315,7 +324,29 @@ class HeatSolver:
             name="heat_geodesic",
         )
 
+    def dispose(self) -> None:
+        """Release this solver's device state now: its factorizations and recorded passes, its
+        multigrid hierarchy, and its operators (whose CG states go back to the pool kept by
+        shape for the next operators of this shape). The solver is unusable afterwards."""
+        self.release_factorizations()
+        multigrid = getattr(self, "_poisson_multigrid", None)
+        if multigrid is not None:
+            multigrid.close()
+            self._poisson_multigrid = None
+        if self._operators is not None:
+            for matrix in (self._operators.heat_system, self._operators.poisson_system,
+                           self._operators.laplacian):
+                matrix.release()
+            self._operators = None
+        self._systems.clear()
+        self._gradient_terms = None
+        self._mesh = None
+
     def release_factorizations(self) -> None:
+        query = getattr(self, "_single_query", None)
+        if query is not None:  # its graph names the factors' buffers
+            query.close()
+            self._single_query = None
         for kept in self._systems.values():
             kept["factorization"].release()
 
@@ -519,20 +550,33 @@ class BatchStep:
     contents between batches) and ``out`` (``(k, V)`` float64, rewritten by every replay). Built by
     running the pass once eagerly on ``stream`` (a created stream: that prepares the factors'
     buffers, the per-face terms and the corner index) and recording it on the same stream; the
-    graph then launches on any stream with no host work per step.
+    graph then launches on any stream with no host work per step. If a factor's work buffers are
+    reallocated afterwards (a wider batch elsewhere), the next launch records the pass again.
     """
 
     def __init__(self, mesh: Trimesh, solver: "HeatSolver", sources: DeviceArray,
                  offsets: DeviceArray, k: int, out: DeviceArray, stream: Any) -> None:
-        import ctypes  # noqa: PLC0415
-
         self.stream = stream
         self.k = k
         self.out = out
-        self._keep = (mesh, solver, sources, offsets)
+        self._args = (mesh, solver, sources, offsets)
+        self.handle = None
+        self._record()
+
+    def _generations(self) -> tuple[int, int]:
+        solver = self._args[1]
+        return solver.heat_factor.generation, solver.poisson_factor.generation
+
+    def _record(self) -> None:
+        import ctypes  # noqa: PLC0415
+
+        self.close()
+        mesh, solver, sources, offsets = self._args
+        k, out, stream = self.k, self.out, self.stream
         _lib.call("ob_device_synchronize")  # buffers allocated on other streams are ready
         _batch_columns(mesh, solver, sources, offsets, k, 0, True, stream=stream, out=out)
         _lib.call("ob_stream_synchronize", stream)
+        self._recorded = self._generations()
         _lib.call("ob_capture_begin", stream)
         error: BaseException | None = None
         try:
@@ -547,9 +591,15 @@ class BatchStep:
         self.handle = handle
         self.kernels = int(kernels.value)
 
-    def launch(self, stream: Any = None) -> DeviceArray:
-        """Replay the pass on ``stream`` (default: the recording stream); returns ``out``."""
-        _lib.call("ob_graph_launch", self.handle, self.stream if stream is None else stream)
+    RECORDING_STREAM = object()
+
+    def launch(self, stream: Any = RECORDING_STREAM) -> DeviceArray:
+        """Replay the pass on ``stream`` (``None``: the legacy default stream; by default the
+        recording stream); returns ``out``."""
+        if self._generations() != self._recorded:
+            self._record()
+        _lib.call("ob_graph_launch", self.handle,
+                  self.stream if stream is BatchStep.RECORDING_STREAM else stream)
         return self.out
 
     def close(self) -> None:
@@ -562,6 +612,42 @@ class BatchStep:
             self.close()
         except Exception:
             pass
+
+
+class _SingleQuery:
+    """``heat_geodesic(trimesh, sources)`` with both factors held: the single-column pass recorded
+    once (``BatchStep``, k = 1) and replayed on the default stream, after the sources are copied
+    into its buffer; the distances are copied into a new array for the caller."""
+
+    def __init__(self, mesh: Trimesh, solver: "HeatSolver", capacity: int) -> None:
+        import ctypes  # noqa: PLC0415
+
+        n = mesh.n_vertices
+        self.n = n
+        self.capacity = capacity
+        self.sources = DeviceArray.from_host(np.zeros(capacity, dtype=np.int32))
+        self.offsets = DeviceArray.from_host(np.array([0, 1], dtype=np.int32))
+        self.bounds = np.zeros(2, dtype=np.int32)
+        self.stream = ctypes.c_void_p(0)
+        _lib.call("ob_stream_create", ctypes.byref(self.stream))
+        self.step = BatchStep(mesh, solver, self.sources, self.offsets, 1,
+                              DeviceArray.empty((1, n), np.float64), self.stream)
+
+    def __call__(self, sources: DeviceArray) -> DeviceArray:
+        m = sources.size
+        self.bounds[1] = m
+        _lib.call("ob_memcpy", self.sources.ptr, sources.ptr, 4 * m, 2, DEFAULT_STREAM, 0)
+        _lib.call("ob_memcpy", self.offsets.ptr, self.bounds.ctypes.data, 8, 0, DEFAULT_STREAM, 0)
+        self.step.launch(DEFAULT_STREAM)
+        out = DeviceArray.empty(self.n, np.float64)
+        _lib.call("ob_memcpy", out.ptr, self.step.out.ptr, 8 * self.n, 2, DEFAULT_STREAM, 0)
+        return out
+
+    def close(self) -> None:
+        self.step.close()
+        if self.stream.value:
+            _lib.lib.ob_stream_destroy(self.stream)
+            self.stream.value = None
 
 
 def _transposed(array: DeviceArray, rows: int, cols: int) -> DeviceArray:
@@ -589,19 +675,45 @@ def heat_geodesic(
     """
     if method not in ("meshlab", "igl", "potpourri3d"):
         raise ValueError(f"method must be 'meshlab', 'igl' or 'potpourri3d', got {method!r}")
-    bound, _owned, src_arg = mesh_arguments("heat_geodesic", mesh, vertices, faces, sources)
+    bound, held, src_arg = mesh_arguments("heat_geodesic", mesh, vertices, faces, sources)
     if src_arg is None:
         raise TypeError("heat_geodesic: sources are required")
+    try:
+        return _heat_geodesic(bound, src_arg, t, use_robust, method)
+    finally:
+        if not held:
+            # The call's own mesh: released now rather than whenever a garbage collection finds
+            # its reference cycle (its CG states go back to the pool for the next call).
+            bound.dispose()
+
+
+def _heat_geodesic(bound: Trimesh, src_arg: Any, t: float | None, use_robust: bool,
+                   method: str) -> DeviceArray:
     n = bound.n_vertices
-    src = _require_sources(src_arg, n)
+    host_sources = None
+    if not hasattr(src_arg, "__cuda_array_interface__"):
+        host_sources = np.ascontiguousarray(src_arg, dtype=np.int32).reshape(-1)
+    src = _require_sources(src_arg if host_sources is None else host_sources, n)
     if n == 0 or bound.n_faces == 0 or src.size == 0:
         return DeviceArray.zeros(n, np.float64)
     _supported(method, use_robust)
     solver = bound.heat_solver(t, use_robust=use_robust, method=method)
+    held_factors = solver.heat_factor is not None and solver.poisson_factor is not None
+    # Host sources are checked on the host; device sources by one small read-back (the
+    # reference's 4-byte flag, ordito/heat.py:5488).
+    if host_sources is not None or held_factors:
+        checked = host_sources if host_sources is not None else src.numpy()
+        if checked.min() < 0 or checked.max() >= n:
+            raise ValueError(
+                "heat_geodesic: every entry of sources must be a vertex index in [0, n_vertices)"
+            )
+    if held_factors:
+        # Both systems factored (a warm resident mesh): the whole query is one recorded pass.
+        return solver.single_query(src)
     u0 = DeviceArray.empty(n, np.float64)
     invalid = DeviceArray.empty(1, np.int32)
     _lib.call("ob_seed", src.ptr, src.size, n, u0.ptr, invalid.ptr, DEFAULT_STREAM)
-    if int(invalid.numpy()[0]) != 0:
+    if host_sources is None and int(invalid.numpy()[0]) != 0:
         raise ValueError(
             "heat_geodesic: every entry of sources must be a vertex index in [0, n_vertices)"
         )

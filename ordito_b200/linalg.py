@@ -12,7 +12,9 @@ Several right-hand sides are laid out ``[n][n_columns]`` (one row's columns cont
 
 from __future__ import annotations
 
+import collections
 import ctypes
+import threading
 import warnings
 from typing import Any
 
@@ -147,7 +149,9 @@ def chebyshev_preconditioner(matrix: CsrMatrix, n_columns: int = 1) -> Precondit
 
 
 class NativeSolver:
-    """One ``ob_pcg_*`` solver state (owned work vectors and recorded loop graphs)."""
+    """One ``ob_pcg_*`` solver state: its own copy of the operator, work vectors and recorded loop
+    graphs. When its matrix is released the state goes back to a pool of kept states by shape,
+    and the next operator of that shape is copied into it (``rebind``) and replays its loops."""
 
     def __init__(self, matrix: CsrMatrix, kind: str, narrow: bool, n_columns: int) -> None:
         handle = ctypes.c_void_p(0)
@@ -159,7 +163,14 @@ class NativeSolver:
         self.handle = handle
         self.n = matrix.nrow
         self.n_columns = n_columns
-        self._matrix = matrix  # keep the borrowed CSR arrays alive
+        self.shape_key = (matrix.nrow, matrix.nnz, kind, bool(narrow), int(n_columns))
+        # In the pool of kept states: its finaliser must not close it (a dead matrix's objects
+        # are collected as one cycle, whose finalisers all run, after the matrix retired it).
+        self.pooled = False
+
+    def rebind(self, matrix: CsrMatrix) -> None:
+        _lib.call("ob_pcg_rebind", self.handle, matrix.offsets.ptr, matrix.columns.ptr,
+                  matrix.values.ptr, matrix.nnz, DEFAULT_STREAM)
 
     def close(self) -> None:
         if self.handle and self.handle.value:
@@ -167,6 +178,8 @@ class NativeSolver:
             self.handle = ctypes.c_void_p(0)
 
     def __del__(self) -> None:
+        if getattr(self, "pooled", False):
+            return
         try:
             self.close()
         except Exception:
@@ -190,12 +203,44 @@ class NativeSolver:
         return rounds.value, status.value
 
 
+# Solver states whose matrix was released, kept by shape for the next operator of that shape.
+_KEPT: "collections.OrderedDict[tuple, NativeSolver]" = collections.OrderedDict()
+_KEPT_LIMIT = 16
+_KEPT_LOCK = threading.Lock()
+
+
 def _solver(matrix: CsrMatrix, kind: str, narrow: bool, n_columns: int) -> NativeSolver:
     key = (kind, bool(narrow), int(n_columns))
     solver = matrix._solvers.get(key)
     if solver is None:
-        solver = matrix._solvers[key] = NativeSolver(matrix, kind, narrow, n_columns)
+        with _KEPT_LOCK:
+            solver = _KEPT.pop((matrix.nrow, matrix.nnz) + key, None)
+        if solver is not None:
+            solver.pooled = False
+            solver.rebind(matrix)
+        else:
+            solver = NativeSolver(matrix, kind, narrow, n_columns)
+        matrix._solvers[key] = solver
     return solver
+
+
+def retire_solver(solver: Any) -> None:
+    """A released matrix's solver state: kept for the next operator of its shape (a bounded
+    pool, least recently retired closed first), or closed."""
+    if not isinstance(solver, NativeSolver) or not (solver.handle and solver.handle.value):
+        return
+    closing = []
+    solver.pooled = True
+    with _KEPT_LOCK:
+        previous = _KEPT.pop(solver.shape_key, None)
+        if previous is not None:
+            closing.append(previous)
+        _KEPT[solver.shape_key] = solver
+        while len(_KEPT) > _KEPT_LIMIT:
+            closing.append(_KEPT.popitem(last=False)[1])
+    for old in closing:
+        old.pooled = False
+        old.close()
 
 
 def _kind(matrix: CsrMatrix, preconditioner: Preconditioner | None) -> str:

@@ -104,6 +104,17 @@ class Trimesh:
             solver = self._solvers[key] = HeatSolver(self, t, use_robust=use_robust, method=method)
         return solver
 
+    def dispose(self) -> None:
+        """Release every device resource this mesh holds now (solvers, factors, operators); the
+        mesh is unusable afterwards. ``heat_geodesic(vertices, faces, ...)`` disposes of the mesh
+        it builds for the call."""
+        for solver in self._solvers.values():
+            solver.dispose()
+        self._solvers.clear()
+        self._pattern = None
+        self._face_terms = None
+        self._corner_index = None
+
     def release_factorizations(self) -> None:
         """Drop every solver's factorizations (ordito/mesh.py:3457)."""
         for solver in self._solvers.values():

@@ -161,3 +161,39 @@ def test_launches_are_counted(gpu) -> None:
     v, f = creation.icosphere(2)
     gheat.heat_geodesic(v, f.reshape(-1), np.array([0], dtype=np.int32))
     assert _lib.launch_count() - before >= 10
+
+
+def test_solver_state_rebinds_to_an_operator_of_the_same_shape(gpu) -> None:
+    # A released operator's solver state serves the next operator of its shape (its own copy of
+    # the operator, rebound, its recorded loop replayed): the answers are the new operator's.
+    import scipy.sparse.linalg as spla
+
+    v, f = creation.icosphere(3)
+    n = v.shape[0]
+    rng = np.random.default_rng(2)
+    b = rng.normal(size=n)
+    for t in (1e-3, 4e-3):
+        ops = gheat.heat_operators(v, f.reshape(-1), t)
+        x = glap.DeviceArray.zeros(n, np.float64)
+        glinalg.solve_spd(ops.heat_system, b, x, tol=1e-12)
+        exact = spla.spsolve(ops.heat_system.to_scipy().tocsc(), b)
+        assert rel_err(x.numpy(), exact) <= 1e-9
+        ops.heat_system.release()  # the state goes back to the pool for the next t
+
+
+def test_single_query_with_held_factors(gpu) -> None:
+    v, f = meshes.small_torus()
+    n = v.shape[0]
+    mesh = Trimesh(v, f.reshape(-1))
+    solver = mesh.heat_solver(None, method="meshlab")
+    assert solver.factor()
+    for sources in ([3], [0, 17, 40], list(range(0, n, 7))):
+        got = gheat.heat_geodesic(mesh, np.array(sources, dtype=np.int32), method="meshlab").numpy()
+        batch = gheat.heat_geodesic_batch(mesh, [sources], refine=0).numpy()[0]
+        assert rel_err(got, batch) <= 1e-12
+        assert rel_err(got, hp.heat_geodesic(v, f, np.array(sources))) <= DISTANCE_TOL
+    device_sources = glap.DeviceArray.from_host(np.array([5, 9], dtype=np.int32))
+    got = gheat.heat_geodesic(mesh, device_sources, method="meshlab").numpy()
+    assert rel_err(got, hp.heat_geodesic(v, f, np.array([5, 9]))) <= DISTANCE_TOL
+    with pytest.raises(ValueError):
+        gheat.heat_geodesic(mesh, np.array([n], dtype=np.int32), method="meshlab")
