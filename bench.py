@@ -53,6 +53,8 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-precision", action="store_true")
     p.add_argument("--no-serving", action="store_true")
+    p.add_argument("--no-reference-benchmarks", action="store_true")
+    p.add_argument("--no-large-mesh", action="store_true")
     p.add_argument("--serving-requests", type=int, default=300)
     p.add_argument("--serving-warmup", type=int, default=150)
     p.add_argument("--serving-rate", type=float, default=40.0)
@@ -277,6 +279,125 @@ def _peaks() -> dict:
         return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
+# The reference's own published heat_geodesic timings (docs/benchmarks/heat.md:52-57; RTX 5090,
+# pytest-benchmark medians, synchronised; single source vertex 0): full = assembly inside the
+# call, amortized = a warm Trimesh holding both factors.
+REFERENCE_HEAT_MS = {
+    "sphere_small": (4, 3.47, 0.3243),
+    "sphere_med": (6, 6.60, 0.6897),
+    "sphere_large": (7, 21.63, 1.48),
+}
+
+
+def run_reference_benchmarks() -> dict:
+    """The reference's headline benchmark on its own meshes: heat_geodesic full and amortized on
+    icospheres of 2 562, 40 962 and 163 842 vertices, source 0, medians of timed calls each
+    followed by a device synchronise, beside the published numbers (another GPU)."""
+    from oracle import heat_path as hp
+    from ordito_b200 import creation
+    from ordito_b200 import heat as gheat
+    from ordito_b200.device import synchronize
+    from ordito_b200.mesh import Trimesh
+
+    src = np.array([0], dtype=np.int32)
+    out = {}
+    for name, (level, ref_full, ref_amortized) in REFERENCE_HEAT_MS.items():
+        v, f = creation.icosphere(level)
+        flat = f.reshape(-1)
+        full = []
+        for _ in range(8):
+            synchronize()
+            t0 = time.perf_counter()
+            gheat.heat_geodesic(v, flat, src)
+            synchronize()
+            full.append(time.perf_counter() - t0)
+        mesh = Trimesh(v, flat)
+        assert mesh.heat_solver(None, method="meshlab").factor()
+        warm = gheat.heat_geodesic(mesh, src).numpy()
+        amortized = []
+        for _ in range(30):
+            synchronize()
+            t0 = time.perf_counter()
+            gheat.heat_geodesic(mesh, src)
+            synchronize()
+            amortized.append(time.perf_counter() - t0)
+        full_ms = 1e3 * statistics.median(full[1:])
+        amortized_ms = 1e3 * statistics.median(amortized)
+        out[name] = {
+            "vertices": int(v.shape[0]),
+            "full_ms": full_ms,
+            "amortized_ms": amortized_ms,
+            "reference_full_ms": ref_full,
+            "reference_amortized_ms": ref_amortized,
+            "speedup_full": ref_full / full_ms,
+            "speedup_amortized": ref_amortized / amortized_ms,
+            "max_rel_linf_vs_fp64_oracle": hp.relative_linf(warm, hp.heat_geodesic(v, f, src)),
+        }
+        mesh.dispose()
+    out["note"] = ("reference numbers are ordito's published medians on an RTX 5090 "
+                   "(docs/benchmarks/heat.md:52-57), not run here")
+    return out
+
+
+def run_large_mesh() -> dict:
+    """The large single mesh: icosphere(9) (2 621 442 vertices) with 1 % seeded radial noise, 8
+    uniform sources, one query at a time on the resident mesh. Its factors (9.7 GB each) are over
+    the factorisation budget, so the heat solve is the settled CG with the band march behind it
+    and the Poisson solve the mixed-precision multigrid solve. The float64 host oracle cannot
+    factor this mesh in a bench run (SuperLU: minutes and tens of GB), so the same path -- the
+    budget forced below the factor's size -- is checked against the oracle on icosphere(6)."""
+    import oracle.heat_path as hp
+    from ordito_b200 import cholesky as gchol
+    from ordito_b200 import creation
+    from ordito_b200 import heat as gheat
+    from ordito_b200.device import synchronize
+    from ordito_b200.mesh import Trimesh
+
+    v, f = creation.icosphere(9)
+    v = creation.radial_noise(v, 0.01, 0)
+    n = v.shape[0]
+    sources = np.random.default_rng(5).choice(n, 8, replace=False).astype(np.int32)
+    t0 = time.perf_counter()
+    mesh = Trimesh(v, f.reshape(-1))
+    solver = mesh.heat_solver(None, method="meshlab")
+    factored = solver.factor()
+    synchronize()
+    setup_s = time.perf_counter() - t0
+    times = []
+    for s in sources:
+        synchronize()
+        t1 = time.perf_counter()
+        gheat.heat_geodesic(mesh, np.array([s], dtype=np.int32), method="meshlab").numpy()
+        times.append(time.perf_counter() - t1)
+    grid = solver.poisson_multigrid.grid if getattr(solver, "_poisson_multigrid", None) else None
+    mesh.dispose()
+    # The same path on icosphere(6), checked against the oracle.
+    budget = gchol.CHOLESKY_MEMORY_BUDGET
+    gchol.CHOLESKY_MEMORY_BUDGET = 1 << 10
+    try:
+        sv, sf = creation.icosphere(6)
+        sv = creation.radial_noise(sv, 0.01, 0)
+        small = Trimesh(sv, sf.reshape(-1))
+        got = gheat.heat_geodesic(small, np.array([7], dtype=np.int32), method="meshlab").numpy()
+        check = hp.relative_linf(got, hp.heat_geodesic(sv, sf, np.array([7])))
+        small.dispose()
+    finally:
+        gchol.CHOLESKY_MEMORY_BUDGET = budget
+    return {
+        "workload": "icosphere(9) + 1 % radial noise (2 621 442 V), 8 single-source queries",
+        "factored": factored,
+        "setup_s": setup_s,
+        "first_query_s": times[0],
+        "value": (len(times) - 1) / sum(times[1:]),
+        "unit": "solves/s",
+        "query_s": times,
+        "poisson_multigrid_levels": grid,
+        "path": "settled CG (float32 values) + backward-error check + band march (float64) for "
+                "the heat system; float32 CG + V-cycle inside float64 refinement (1e-8) for -L",
+        "max_rel_linf_vs_fp64_oracle_same_path_ico6": check,
+    }
+
+
 def run_serving(args: argparse.Namespace) -> dict:
     """The serving stream: Poisson arrivals, meshes log-uniform in size (icospheres and jittered
     tori), 70 % of requests on one of the last 50 meshes, 1-32 sources each, 150 GB HBM budget.
@@ -479,6 +600,15 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     serving = None
     if not args.no_serving and dist.world == 1:
         serving = run_serving(args)
+    reference_benchmarks = None
+    if not args.no_reference_benchmarks and dist.world == 1:
+        reference_benchmarks = run_reference_benchmarks()
+    large_mesh = None
+    if not args.no_large_mesh and dist.world == 1:
+        try:
+            large_mesh = run_large_mesh()
+        except Exception as exc:  # noqa: BLE001 -- reported on the line, not fatal to it
+            large_mesh = {"error": f"{type(exc).__name__}: {exc}"}
 
     if dist.rank == 0:
         line = {
@@ -525,6 +655,8 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
                                       "what": "heat_geodesic_batch(mesh, [[s]]): factors resident, k = 1"},
             "precision": precision,
             "serving": serving,
+            "reference_benchmarks": reference_benchmarks,
+            "large_mesh": large_mesh,
             "roofline": {
                 "bound": "hbm",
                 "kernel": "tile_product_kernel (Cholesky forward+backward pass, 64 columns)",
