@@ -366,6 +366,32 @@ int ob_amg_solve(void* amg, const double* b, double* x, int k, int ld, double to
 int ob_amg_host_setup(int n, const int32_t* offsets, const int32_t* columns, const double* values,
                       unsigned seed, long long* rows, long long* nnz, int capacity, int* levels);
 
+/* ---- Packed meshes: many meshes solved as one block-diagonal system -------------------------
+ * The batched form of ordito.heat.heat_geodesic over many meshes at once: the meshes' vertices
+ * and faces concatenated (each face offset by its mesh's first vertex), so the pattern, the face
+ * terms, the factorisation and the passes run once over the union; column c carries every mesh's
+ * c-th single-source query.
+ * ob_edge_sums_segments: ob_edge_sums per segment of rows (a mesh: rows [segments[s],
+ * segments[s + 1])), out[2 s], out[2 s + 1], added in a fixed order.
+ * ob_heat_rows_packed: ob_heat_rows with each row's own factor (its mesh's -t): L, H = factor L
+ * + M, P = -L and the mass, the same arithmetic per row.
+ * ob_shift_packed: ob_shift_permuted per (mesh, column): sources[m * n_columns + c] is the local
+ * source vertex of mesh m's query in column c (-1: none, its distances are written 0); each
+ * mesh's field is shifted by its source's value and oriented by its own mean
+ * (kernels/heat.py:3384-3424); out is (n_columns, V); sums is 2 * n_meshes * n_columns doubles
+ * of scratch. */
+int ob_edge_sums_segments(const int32_t* offsets, const int32_t* columns, const int32_t* run_start,
+                          const uint64_t* keys, int count, const float* xyz, int face_edges,
+                          const int32_t* segments, int n_segments, double* out, ob_stream_t stream);
+int ob_heat_rows_packed(const int32_t* offsets, const int32_t* columns, const int32_t* run_start,
+                        const uint64_t* keys, int count, const int32_t* order, int n_vertices,
+                        const float* cot, const double* row_factor, const double* area_sums,
+                        double mass_divisor, double* L, double* H, double* P, double* mass,
+                        ob_stream_t stream);
+int ob_shift_packed(const double* phi, int n_vertices, int stride, const int32_t* iperm,
+                    const int32_t* vertex_offsets, int n_meshes, const int32_t* sources,
+                    int n_columns, double* sums, double* out, ob_stream_t stream);
+
 /* ---- a12: the marched settled solve --------------------------------------------------------
  * Replaces ordito/linalg.py:2765 _march_settled (kernels/linalg.py:1229-1545): x = A^-1 rhs for
  * one column, band by band outward from rhs's support, every entry to its own relative

@@ -111,6 +111,9 @@ SIGNATURES: dict[str, list] = {
     "ob_chol_info": [P, POINTER(ctypes.c_longlong)],
     "ob_chol_work_generation": [P, POINTER(ctypes.c_longlong)],
     "ob_march_solve": [I, P, P, P, P, P, POINTER(ctypes.c_longlong), P],
+    "ob_edge_sums_segments": [P, P, P, P, I, P, I, P, I, P, P],
+    "ob_heat_rows_packed": [P, P, P, P, I, P, I, P, P, P, D, P, P, P, P, P],
+    "ob_shift_packed": [P, I, I, P, P, I, P, I, P, P, P],
     "ob_amg_setup": [I, P, P, P, ctypes.c_uint, POINTER(c_void_p), P],
     "ob_amg_destroy": [P],
     "ob_amg_info": [P, POINTER(ctypes.c_longlong)],

@@ -91,22 +91,14 @@ __global__ void edge_sums_kernel(const int* __restrict__ offsets, const int* __r
 // ordito/kernels/heat.py:299-465 (heat_system_rows, scalar_heat_row, scalar_heat_diagonal),
 // kernels/laplacian.py:971-989 (cotmatrix_offdiagonal), kernels/linalg.py:1594-1621
 // (shift_factor, shifted_scalar_entry): one thread per row walks its entries in row order.
-__global__ void heat_rows_kernel(const int* __restrict__ offsets, const int* __restrict__ columns,
-                                 const int* __restrict__ run_start,
-                                 const unsigned long long* __restrict__ keys, int count,
-                                 const int* __restrict__ order, int n, const float* __restrict__ cot,
-                                 double scale, const double* __restrict__ edge_sums, int from_edges,
-                                 const double* __restrict__ area_sums, double mass_divisor,
-                                 double* __restrict__ L, double* __restrict__ H,
-                                 double* __restrict__ P, double* __restrict__ mass) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double factor = scale;
-    if (from_edges) {
-        double h = 0.0;
-        if (edge_sums[1] > 0.0) h = edge_sums[0] / edge_sums[1];
-        factor = scale * (h * h);
-    }
+// Row i of L, H = factor L + M and P = -L (and its mass), the one arithmetic of both kernels below.
+__device__ __forceinline__ void heat_row(int i, const int* __restrict__ offsets, const int* __restrict__ columns,
+                                         const int* __restrict__ run_start,
+                                         const unsigned long long* __restrict__ keys, int count,
+                                         const int* __restrict__ order, const float* __restrict__ cot,
+                                         double factor, const double* __restrict__ area_sums,
+                                         double mass_divisor, double* __restrict__ L, double* __restrict__ H,
+                                         double* __restrict__ P, double* __restrict__ mass) {
     const double m = area_sums[i] / mass_divisor;
     mass[i] = m;
     const int start = offsets[i], end = offsets[i + 1];
@@ -131,6 +123,73 @@ __global__ void heat_rows_kernel(const int* __restrict__ offsets, const int* __r
         L[slot] = diagonal;
         H[slot] = __dmul_rn(factor, diagonal) + m;
         P[slot] = -diagonal;
+    }
+}
+
+__global__ void heat_rows_kernel(const int* __restrict__ offsets, const int* __restrict__ columns,
+                                 const int* __restrict__ run_start,
+                                 const unsigned long long* __restrict__ keys, int count,
+                                 const int* __restrict__ order, int n, const float* __restrict__ cot,
+                                 double scale, const double* __restrict__ edge_sums, int from_edges,
+                                 const double* __restrict__ area_sums, double mass_divisor,
+                                 double* __restrict__ L, double* __restrict__ H,
+                                 double* __restrict__ P, double* __restrict__ mass) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double factor = scale;
+    if (from_edges) {
+        double h = 0.0;
+        if (edge_sums[1] > 0.0) h = edge_sums[0] / edge_sums[1];
+        factor = scale * (h * h);
+    }
+    heat_row(i, offsets, columns, run_start, keys, count, order, cot, factor, area_sums, mass_divisor,
+             L, H, P, mass);
+}
+
+// Many meshes packed as one block-diagonal operator: each row's own factor (its mesh's -t).
+__global__ void heat_rows_packed_kernel(const int* __restrict__ offsets, const int* __restrict__ columns,
+                                        const int* __restrict__ run_start,
+                                        const unsigned long long* __restrict__ keys, int count,
+                                        const int* __restrict__ order, int n, const float* __restrict__ cot,
+                                        const double* __restrict__ row_factor,
+                                        const double* __restrict__ area_sums, double mass_divisor,
+                                        double* __restrict__ L, double* __restrict__ H,
+                                        double* __restrict__ P, double* __restrict__ mass) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    heat_row(i, offsets, columns, run_start, keys, count, order, cot, row_factor[i], area_sums,
+             mass_divisor, L, H, P, mass);
+}
+
+// Per segment of rows (a packed mesh): edge_sums_kernel's two sums over its strict upper
+// triangle, one block a segment, added in a fixed order.
+__global__ void edge_sums_segments_kernel(const int* __restrict__ offsets, const int* __restrict__ columns,
+                                          const int* __restrict__ run_start,
+                                          const unsigned long long* __restrict__ keys, int count,
+                                          const float* __restrict__ xyz, int face_edges,
+                                          const int* __restrict__ segments, double* __restrict__ out) {
+    __shared__ double scratch[32];
+    const int s = blockIdx.x;
+    double sum = 0.0, cnt = 0.0;
+    for (int row = segments[s] + threadIdx.x; row < segments[s + 1]; row += blockDim.x) {
+        const f3 vr = load_f3(xyz, row);
+        for (int k = offsets[row]; k < offsets[row + 1]; ++k) {
+            const int col = columns[k];
+            if (col <= row) continue;
+            double weight = 1.0;
+            if (face_edges) {
+                const int r = run_start[k];
+                weight = (double)(run_end(keys, r, count) - r);
+            }
+            sum += weight * (double)length(sub(load_f3(xyz, col), vr));
+            cnt += weight;
+        }
+    }
+    const double bs = block_sum(sum, scratch);
+    const double bc = block_sum(cnt, scratch);
+    if (threadIdx.x == 0) {
+        out[2 * s] = bs;
+        out[2 * s + 1] = bc;
     }
 }
 
@@ -178,6 +237,37 @@ int ob_edge_sums(const int32_t* offsets, const int32_t* columns, const int32_t* 
         offsets, columns, run_start, reinterpret_cast<const unsigned long long*>(keys), count,
         n_vertices, xyz, face_edges, partials, counter, out);
     OB_CHECK_LAUNCH("edge_sums");
+    return OB_OK;
+}
+
+int ob_edge_sums_segments(const int32_t* offsets, const int32_t* columns, const int32_t* run_start,
+                          const uint64_t* keys, int count, const float* xyz, int face_edges,
+                          const int32_t* segments, int n_segments, double* out, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_segments >= 0 && out, "ob_edge_sums_segments: bad argument");
+    if (n_segments == 0) return OB_OK;
+    OB_REQUIRE(offsets && columns && run_start && keys && xyz && segments, "ob_edge_sums_segments: null pointer");
+    edge_sums_segments_kernel<<<n_segments, kThreads, 0, stream>>>(
+        offsets, columns, run_start, reinterpret_cast<const unsigned long long*>(keys), count, xyz,
+        face_edges, segments, out);
+    OB_CHECK_LAUNCH("edge_sums_segments");
+    return OB_OK;
+}
+
+int ob_heat_rows_packed(const int32_t* offsets, const int32_t* columns, const int32_t* run_start,
+                        const uint64_t* keys, int count, const int32_t* order, int n_vertices,
+                        const float* cot, const double* row_factor, const double* area_sums,
+                        double mass_divisor, double* L, double* H, double* P, double* mass,
+                        ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    if (n_vertices <= 0) return OB_OK;
+    OB_REQUIRE(offsets && columns && run_start && keys && order && cot && row_factor && area_sums && L &&
+                   H && P && mass,
+               "ob_heat_rows_packed: null pointer");
+    heat_rows_packed_kernel<<<ceil_div(n_vertices, kThreads), kThreads, 0, stream>>>(
+        offsets, columns, run_start, reinterpret_cast<const unsigned long long*>(keys), count, order,
+        n_vertices, cot, row_factor, area_sums, mass_divisor, L, H, P, mass);
+    OB_CHECK_LAUNCH("heat_rows_packed");
     return OB_OK;
 }
 

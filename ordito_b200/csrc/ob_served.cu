@@ -294,6 +294,61 @@ __global__ void shift_out_kernel(const double* __restrict__ phi, int n, int stri
     }
 }
 
+// Packed meshes (many meshes as one block-diagonal system, column c = every mesh's c-th
+// single-source query): per (mesh, column) the sum of phi over the mesh's rows and phi at the
+// query's source, one block a mesh, threads owning column t % stride (blockDim a multiple of
+// stride), added in a fixed order.
+__global__ void shift_packed_sums_kernel(const double* __restrict__ phi, int stride, const int* __restrict__ iperm,
+                                         const int* __restrict__ vertex_offsets, const int* __restrict__ sources,
+                                         int k, double2* __restrict__ sums) {
+    __shared__ double tree[kThreads];
+    const int m = blockIdx.x;
+    const int c = threadIdx.x % stride;
+    const int v0 = vertex_offsets[m], v1 = vertex_offsets[m + 1];
+    double total = 0.0;
+    const int rows_per_pass = blockDim.x / stride;
+    for (int v = v0 + threadIdx.x / stride; v < v1; v += rows_per_pass)
+        total += phi[(size_t)row_of(iperm, v) * stride + c];
+    tree[threadIdx.x] = total;
+    __syncthreads();
+    if ((int)threadIdx.x < stride && (int)threadIdx.x < k) {
+        double column = 0.0;
+        for (int t = threadIdx.x; t < (int)blockDim.x; t += stride) column += tree[t];
+        const int s = sources[(size_t)m * k + threadIdx.x];
+        const double at = s >= 0 ? phi[(size_t)row_of(iperm, v0 + s) * stride + threadIdx.x] : 0.0;
+        sums[(size_t)m * k + threadIdx.x] = make_double2(at, column);
+    }
+}
+
+// out[c][v]: the shifted, oriented phi of vertex v in column c (kernels/heat.py:3406 per mesh);
+// zero where v's mesh has no query in column c.
+__global__ void shift_packed_out_kernel(const double* __restrict__ phi, int n, int stride,
+                                        const int* __restrict__ iperm, const int* __restrict__ vertex_offsets,
+                                        int n_meshes, const int* __restrict__ sources, int k,
+                                        const double2* __restrict__ sums, double* __restrict__ out) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)n * k) return;
+    const int c = (int)(t / n), v = (int)(t % n);
+    int lo = 0, hi = n_meshes - 1;  // the mesh holding v: vertex_offsets[m] <= v < [m + 1]
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (vertex_offsets[mid] <= v) lo = mid;
+        else hi = mid - 1;
+    }
+    const int m = lo;
+    if (sources[(size_t)m * k + c] < 0) {
+        out[t] = 0.0;
+        return;
+    }
+    const double2 s = sums[(size_t)m * k + c];
+    const double offset = s.x;
+    const double value = phi[(size_t)row_of(iperm, v) * stride + c];
+    double shifted = value - offset;
+    const int count = vertex_offsets[m + 1] - vertex_offsets[m];
+    if (s.y / (double)count - offset < 0.0) shifted = offset - value;
+    out[t] = shifted;
+}
+
 }  // namespace
 }  // namespace ob
 
@@ -395,6 +450,25 @@ int ob_grad_div_terms(const double* terms, const int32_t* faces, const int32_t* 
         terms, faces, corner_offsets, corner_slots, n_vertices, n_columns, u, u_stride, u_iperm, out,
         out_stride, out_iperm, out_pinned);
     OB_CHECK_LAUNCH("grad_div_terms");
+    return OB_OK;
+}
+
+int ob_shift_packed(const double* phi, int n_vertices, int stride, const int32_t* iperm,
+                    const int32_t* vertex_offsets, int n_meshes, const int32_t* sources, int n_columns,
+                    double* sums, double* out, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_vertices >= 1 && n_meshes >= 1 && n_columns >= 1 && stride >= n_columns && stride <= kThreads,
+               "ob_shift_packed: bad size");
+    OB_REQUIRE(phi && vertex_offsets && sources && sums && out, "ob_shift_packed: null pointer");
+    const int threads = (kThreads / stride) * stride;
+    shift_packed_sums_kernel<<<n_meshes, threads, 0, stream>>>(phi, stride, iperm, vertex_offsets, sources,
+                                                               n_columns, reinterpret_cast<double2*>(sums));
+    OB_CHECK_LAUNCH("shift_packed_sums");
+    const long long total = (long long)n_vertices * n_columns;
+    shift_packed_out_kernel<<<ceil_div(total, kThreads), kThreads, 0, stream>>>(
+        phi, n_vertices, stride, iperm, vertex_offsets, n_meshes, sources, n_columns,
+        reinterpret_cast<const double2*>(sums), out);
+    OB_CHECK_LAUNCH("shift_packed_out");
     return OB_OK;
 }
 

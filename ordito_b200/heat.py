@@ -132,6 +132,16 @@ def _diffusion_floor(mesh: Trimesh) -> float:
     return (math.dist(low, high) / _DIFFUSION_DECAY) ** 2
 
 
+def _diffusion_floor_length(vertices: np.ndarray) -> float:
+    """``|bounding-box diagonal| / 400`` of host vertices: the square root of the floor above
+    (float32 extremes widened to float64, exactly as the device's bounds)."""
+    if vertices.size == 0:
+        return 0.0
+    low = vertices.min(axis=0).astype(np.float64)
+    high = vertices.max(axis=0).astype(np.float64)
+    return math.dist(low, high) / _DIFFUSION_DECAY
+
+
 def _settle_window(t: float | None, default: float) -> int:
     """ordito/heat.py:5234: the settle window grows like ``sqrt(t / h^2)``."""
     if t is None or not t > default > 0.0:
