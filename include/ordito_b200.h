@@ -67,6 +67,8 @@ int ob_event_destroy(void* event);
 int ob_event_record(void* event, ob_stream_t stream);
 int ob_event_elapsed_ms(void* start, void* end, float* ms); /* synchronizes on end           */
 int ob_event_query(void* event, int* done);               /* done = 1 once the event has passed */
+int ob_event_synchronize(void* event);                    /* waits for the event on the host  */
+int ob_stream_wait_event(ob_stream_t stream, void* event); /* later work on stream waits for it */
 int ob_mem_info(size_t* free_bytes, size_t* total_bytes); /* the device's free / total memory  */
 /* Recording a sequence of this library's calls as one CUDA graph: ob_capture_begin(stream)
  * (a created stream), the calls on that stream, ob_capture_end -> a graph replayed by

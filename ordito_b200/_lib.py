@@ -55,6 +55,8 @@ SIGNATURES: dict[str, list] = {
     "ob_event_record": [P, P],
     "ob_event_elapsed_ms": [P, P, POINTER(c_float)],
     "ob_event_query": [P, POINTER(c_int)],
+    "ob_event_synchronize": [P],
+    "ob_stream_wait_event": [P, P],
     "ob_mem_info": [POINTER(c_size_t), POINTER(c_size_t)],
     "ob_capture_begin": [P],
     "ob_capture_end": [P, POINTER(c_void_p), POINTER(c_int)],

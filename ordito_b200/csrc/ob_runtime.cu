@@ -186,6 +186,18 @@ int ob_event_elapsed_ms(void* start, void* end, float* ms) {
     return OB_OK;
 }
 
+int ob_event_synchronize(void* event) {
+    OB_REQUIRE(event != nullptr, "ob_event_synchronize: null event");
+    OB_CUDA(cudaEventSynchronize(reinterpret_cast<cudaEvent_t>(event)));
+    return OB_OK;
+}
+
+int ob_stream_wait_event(ob_stream_t stream, void* event) {
+    OB_REQUIRE(event != nullptr, "ob_stream_wait_event: null event");
+    OB_CUDA(cudaStreamWaitEvent(as_stream(stream), reinterpret_cast<cudaEvent_t>(event), 0));
+    return OB_OK;
+}
+
 int ob_event_query(void* event, int* done) {
     OB_REQUIRE(event != nullptr && done != nullptr, "ob_event_query: bad argument");
     const cudaError_t e = cudaEventQuery(reinterpret_cast<cudaEvent_t>(event));

@@ -624,6 +624,98 @@ class BatchStep:
             pass
 
 
+class BatchPipeline:
+    """A stream of batches on one resident mesh, host arrays out, pipelined: the recorded pass of
+    batch i + 1 (``BatchStep``) runs while batch i's distances are copied to pinned host memory on
+    a second stream (two output buffers, ordered by events).
+
+    ``map(batches)`` yields, in order, each batch's ``(k, V)`` float64 distances as a view of a
+    pinned host buffer, valid until the generator has advanced twice more (copy it to keep it).
+    Every batch has exactly ``k`` source sets (each a list of source vertices; host-validated).
+    """
+
+    def __init__(self, mesh: Trimesh, k: int, *, method: str = "meshlab", max_sources: int = 0) -> None:
+        import ctypes  # noqa: PLC0415
+
+        from ordito_b200.device import PinnedArray  # noqa: PLC0415
+
+        solver = mesh.heat_solver(None, method=method)
+        if not solver.factor():
+            raise RuntimeError("BatchPipeline: the systems could not be factored (over budget)")
+        n = mesh.n_vertices
+        self.n, self.k = n, k
+        capacity = max(max_sources, 4 * k)
+        self.compute, self.copy = ctypes.c_void_p(0), ctypes.c_void_p(0)
+        _lib.call("ob_stream_create", ctypes.byref(self.compute))
+        _lib.call("ob_stream_create", ctypes.byref(self.copy))
+        self.capacity = capacity
+        self.slots = []
+        for _ in range(2):
+            src = DeviceArray.from_host(np.zeros(capacity, dtype=np.int32))
+            off = DeviceArray.from_host(np.arange(k + 1, dtype=np.int32))
+            out = DeviceArray.empty((k, n), np.float64)
+            step = BatchStep(mesh, solver, src, off, k, out, self.compute)
+            events = [ctypes.c_void_p(0), ctypes.c_void_p(0)]
+            for e in events:
+                _lib.call("ob_event_create", ctypes.byref(e))
+            self.slots.append({
+                "src": src, "off": off, "step": step, "host": PinnedArray((k, n), np.float64),
+                "h_src": PinnedArray(capacity, np.int32), "h_off": PinnedArray(k + 1, np.int32),
+                "computed": events[0], "copied": events[1], "busy": False,
+            })
+
+    def _enqueue(self, slot: dict, sets: Any) -> None:
+        if len(sets) != self.k:
+            raise ValueError(f"BatchPipeline: batches of {self.k} source sets")
+        arrays = [np.ascontiguousarray(s, dtype=np.int32).reshape(-1) for s in sets]
+        sizes = np.array([a.size for a in arrays], dtype=np.int32)
+        total = int(sizes.sum())
+        if total > self.capacity or sizes.min() < 1:
+            raise ValueError(f"BatchPipeline: 1 or more sources a set, {self.capacity} in all at most")
+        flat = np.concatenate(arrays)
+        if flat.min() < 0 or flat.max() >= self.n:
+            raise ValueError("BatchPipeline: source index out of range")
+        if slot["busy"]:
+            # This slot's last copy must be done before its buffers are written again.
+            _lib.call("ob_event_synchronize", slot["copied"])
+        slot["h_src"].array[:total] = flat
+        slot["h_off"].array[0] = 0
+        np.cumsum(sizes, out=slot["h_off"].array[1:])
+        _lib.call("ob_memcpy", slot["src"].ptr, slot["h_src"].ptr, 4 * total, 0, self.compute, 0)
+        _lib.call("ob_memcpy", slot["off"].ptr, slot["h_off"].ptr, 4 * (self.k + 1), 0, self.compute, 0)
+        slot["step"].launch(self.compute)
+        _lib.call("ob_event_record", slot["computed"], self.compute)
+        _lib.call("ob_stream_wait_event", self.copy, slot["computed"])
+        _lib.call("ob_memcpy", slot["host"].ptr, slot["step"].out.ptr, 8 * self.k * self.n, 1, self.copy, 0)
+        _lib.call("ob_event_record", slot["copied"], self.copy)
+        slot["busy"] = True
+
+    def map(self, batches: Any):
+        pending = None
+        for i, sets in enumerate(batches):
+            slot = self.slots[i % 2]
+            self._enqueue(slot, sets)
+            if pending is not None:
+                _lib.call("ob_event_synchronize", pending["copied"])
+                yield pending["host"].array
+            pending = slot
+        if pending is not None:
+            _lib.call("ob_event_synchronize", pending["copied"])
+            yield pending["host"].array
+
+    def close(self) -> None:
+        for slot in self.slots:
+            slot["step"].close()
+            for e in ("computed", "copied"):
+                _lib.lib.ob_event_destroy(slot[e])
+        self.slots = []
+        for stream in (self.compute, self.copy):
+            if stream.value:
+                _lib.lib.ob_stream_synchronize(stream)
+                _lib.lib.ob_stream_destroy(stream)
+                stream.value = None
+
+
 class _SingleQuery:
     """``heat_geodesic(trimesh, sources)`` with both factors held: the single-column pass recorded
     once (``BatchStep``, k = 1) and replayed on the default stream, after the sources are copied

@@ -220,3 +220,21 @@ def test_batched_modes_agree_and_repeat(gpu, refine: int) -> None:
         assert hp.relative_linf(first[c], ref) <= DISTANCE_TOL
     untransposed = gheat.heat_geodesic_batch(mesh, sets, refine=refine, transpose=False).numpy()
     assert np.allclose(untransposed.T, first, rtol=0, atol=1e-12 * np.abs(first).max())
+
+
+def test_batch_pipeline_matches_the_batched_pass(gpu) -> None:
+    v, f = meshes.small_torus()
+    n = v.shape[0]
+    mesh = Trimesh(v, f.reshape(-1))
+    rng = np.random.default_rng(4)
+    batches = [[rng.choice(n, size=int(s), replace=False).tolist() for s in rng.integers(1, 4, size=5)]
+               for _ in range(5)]
+    pipe = gheat.BatchPipeline(mesh, 5)
+    results = [r.copy() for r in pipe.map(batches)]
+    pipe.close()
+    assert len(results) == len(batches)
+    for sets, got in zip(batches, results):
+        expected = gheat.heat_geodesic_batch(mesh, sets, refine=0).numpy()
+        assert hp.relative_linf(got, expected) <= 1e-12
+    with pytest.raises(ValueError):
+        list(gheat.BatchPipeline(mesh, 2).map([[[0], [n]]]))
