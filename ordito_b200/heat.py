@@ -11,6 +11,8 @@ step is a CUDA kernel of ``libordito_b200.so``; the host only reads back the doc
 
 from __future__ import annotations
 
+import contextlib
+import gc
 import logging
 import math
 import warnings
@@ -551,6 +553,19 @@ def _batch_columns(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offset
     return out
 
 
+@contextlib.contextmanager
+def capture_guard():
+    """No garbage collection while this thread records a graph: a collection there would run
+    destructors (device frees, solver teardown) inside the capture, which the capture forbids."""
+    enabled = gc.isenabled()
+    gc.disable()
+    try:
+        yield
+    finally:
+        if enabled:
+            gc.enable()
+
+
 class BatchStep:
     """One served batch pass recorded as a CUDA graph and replayed with a single launch.
 
@@ -565,36 +580,41 @@ class BatchStep:
     """
 
     def __init__(self, mesh: Trimesh, solver: "HeatSolver", sources: DeviceArray,
-                 offsets: DeviceArray, k: int, out: DeviceArray, stream: Any) -> None:
+                 offsets: DeviceArray, k: int, out: DeviceArray, stream: Any, *,
+                 warm: bool = True) -> None:
         self.stream = stream
         self.k = k
         self.out = out
         self._args = (mesh, solver, sources, offsets)
         self.handle = None
-        self._record()
+        self._record(warm)
 
     def _generations(self) -> tuple[int, int]:
         solver = self._args[1]
         return solver.heat_factor.generation, solver.poisson_factor.generation
 
-    def _record(self) -> None:
+    def _record(self, warm: bool = True) -> None:
         import ctypes  # noqa: PLC0415
 
         self.close()
         mesh, solver, sources, offsets = self._args
         k, out, stream = self.k, self.out, self.stream
-        _lib.call("ob_device_synchronize")  # buffers allocated on other streams are ready
-        _batch_columns(mesh, solver, sources, offsets, k, 0, True, stream=stream, out=out)
-        _lib.call("ob_stream_synchronize", stream)
-        self._recorded = self._generations()
-        _lib.call("ob_capture_begin", stream)
-        error: BaseException | None = None
-        try:
+        if warm:
+            # One eager pass prepares what the recording must find ready (the factors' buffers,
+            # the per-face terms, the corner index); skipped when a wider step already did.
+            _lib.call("ob_device_synchronize")  # buffers allocated on other streams are ready
             _batch_columns(mesh, solver, sources, offsets, k, 0, True, stream=stream, out=out)
-        except BaseException as exc:  # noqa: BLE001 -- the capture must be closed first
-            error = exc
-        handle, kernels = ctypes.c_void_p(0), ctypes.c_int(0)
-        status = _lib.lib.ob_capture_end(stream, ctypes.byref(handle), ctypes.byref(kernels))
+            _lib.call("ob_stream_synchronize", stream)
+        self._recorded = self._generations()
+        with capture_guard():
+            _lib.call("ob_capture_begin", stream)
+            error: BaseException | None = None
+            try:
+                _batch_columns(mesh, solver, sources, offsets, k, 0, True, stream=stream, out=out)
+            except BaseException as exc:  # noqa: BLE001 -- the capture must be closed first
+                error = exc
+            handle, kernels = ctypes.c_void_p(0), ctypes.c_int(0)
+            status = _lib.lib.ob_capture_end(stream, ctypes.byref(handle), ctypes.byref(kernels))
         if error is not None:
             raise error
         _lib.check(status, "ob_capture_end")

@@ -27,7 +27,7 @@ from ordito_b200 import _lib
 from ordito_b200.array import CsrMatrix
 from ordito_b200.cholesky import CholeskyAnalysis, SparseCholesky
 from ordito_b200.device import DEFAULT_STREAM, DeviceArray
-from ordito_b200.heat import _diffusion_floor_length
+from ordito_b200.heat import _diffusion_floor_length, capture_guard
 from ordito_b200.laplacian import face_terms, mesh_operator_pattern
 
 
@@ -178,14 +178,15 @@ class PackedMeshes:
         self.run(k, stream)
         _lib.call("ob_stream_synchronize", stream)
         generations = (self.heat_factor.generation, self.poisson_factor.generation)
-        _lib.call("ob_capture_begin", stream)
-        error: BaseException | None = None
-        try:
-            self.run(k, stream)
-        except BaseException as exc:  # noqa: BLE001 -- the capture must be closed first
-            error = exc
-        handle, kernels = ctypes.c_void_p(0), ctypes.c_int(0)
-        status = _lib.lib.ob_capture_end(stream, ctypes.byref(handle), ctypes.byref(kernels))
+        with capture_guard():
+            _lib.call("ob_capture_begin", stream)
+            error: BaseException | None = None
+            try:
+                self.run(k, stream)
+            except BaseException as exc:  # noqa: BLE001 -- the capture must be closed first
+                error = exc
+            handle, kernels = ctypes.c_void_p(0), ctypes.c_int(0)
+            status = _lib.lib.ob_capture_end(stream, ctypes.byref(handle), ctypes.byref(kernels))
         if error is not None:
             raise error
         _lib.check(status, "ob_capture_end")

@@ -13,7 +13,10 @@ distance to the nearest of its sources) into one batched pass -- seeding, the tw
 the gathered divergence and the shift, all on the slot's stream -- and copies the distances back
 into pinned host memory. Requests that arrive while others are on the GPU join the next batch of
 their mesh; batches of different meshes overlap on the device. A new mesh is set up (operators,
-analysis, factorisation) on a separate host thread, so the slots keep running meanwhile.
+analysis, factorisation) on separate host threads, so the slots keep running meanwhile; its
+first requests are answered at once by the unfactored path (settled CG, then the Poisson CG) before
+it is factored -- the reference's rent-or-buy, which factors a system on its second solve
+(ordito/heat.py:4394-4404).
 
 Each result equals the same query run alone (``heat_geodesic_batch(mesh, [sources])``) up to the
 solves' rounding: columns of a batch never mix, and the device passes are per column.
@@ -27,6 +30,7 @@ import ctypes
 import hashlib
 import math
 import queue
+import sys
 import threading
 import time
 from dataclasses import dataclass, field
@@ -43,6 +47,13 @@ from ordito_b200.device import DeviceArray, PinnedArray
 ESTIMATED_BYTES_PER_VERTEX = 2 * 140 * 8 + 400
 # Device memory kept free beyond the budget's accounting (allocator slack, graphs, scratch).
 FREE_MEMORY_MARGIN = 2 << 30
+# The interpreter's thread switch interval while a server runs: the dispatch loop retakes the GIL
+# after every library call, and at the default 5 ms each retake could wait that long per busy
+# setup thread (warm p99 of 150-750 ms measured, 33 ms at this value). Process-wide; restored by
+# close().
+SWITCH_INTERVAL = 2e-4
+# How long a reading of the device's free memory is reused by admission (the margin covers it).
+FREE_MEMORY_REUSE_S = 0.1
 # Batch widths the passes are recorded for; a batch is padded up to the next one.
 _BUCKETS = (1, 2, 4, 8, 16, 32, 64, 128)
 
@@ -164,7 +175,6 @@ class _Resident:
     h_src: PinnedArray
     h_off: PinnedArray
     d_out: DeviceArray
-    h_out: PinnedArray
     pending: collections.deque = field(default_factory=collections.deque)
     busy: bool = False
     steps: dict = field(default_factory=dict)  # batch width -> recorded BatchStep
@@ -175,7 +185,7 @@ class _Resident:
         self.steps = {}
         self.solver.release_factorizations()
         self.mesh.release_factorizations()
-        for name in ("d_src", "d_off", "d_out", "h_src", "h_off", "h_out", "mesh", "solver"):
+        for name in ("d_src", "d_off", "d_out", "h_src", "h_off", "mesh", "solver"):
             setattr(self, name, None)
 
 
@@ -184,6 +194,7 @@ class _Slot:
     stream: ctypes.c_void_p
     event: ctypes.c_void_p
     batch: tuple | None = None
+    host: PinnedArray | None = None  # the batch's distances come back here (grown on demand)
 
 
 class GeodesicServer:
@@ -196,24 +207,32 @@ class GeodesicServer:
     """
 
     def __init__(self, *, hbm_budget: int = 150 << 30, max_columns: int = 64, slots: int = 4,
-                 max_sources: int = 32, method: str = "meshlab", setup_threads: int = 2) -> None:
+                 max_sources: int = 32, method: str = "meshlab", setup_threads: int = 3,
+                 plain_answers: int = 8, max_vertices: int = 1 << 18) -> None:
         if max_columns not in _BUCKETS:
             raise ValueError(f"max_columns must be one of {_BUCKETS}")
         self.max_columns = max_columns
         self.max_sources = max_sources
         self.method = method
+        self._switch_interval = sys.getswitchinterval()
+        sys.setswitchinterval(min(self._switch_interval, SWITCH_INTERVAL))
+        self._free_reading = (-1.0, 0)
         self.cache = MeshCache(hbm_budget, free_memory=self._free_memory)
         self._intake: queue.SimpleQueue = queue.SimpleQueue()
         self._setups: queue.SimpleQueue = queue.SimpleQueue()
         self._ready: queue.SimpleQueue = queue.SimpleQueue()
         self._waiting: dict[str, list[_Request]] = {}
+        self._waiting_lock = threading.Lock()  # the scheduler and the setup threads share it
+        self.plain_answers = plain_answers
         self._deferred: collections.deque = collections.deque()
         self._slots: list[_Slot] = []
         for _ in range(slots):
             stream, event = ctypes.c_void_p(0), ctypes.c_void_p(0)
             _lib.call("ob_stream_create", ctypes.byref(stream))
             _lib.call("ob_event_create", ctypes.byref(event))
-            self._slots.append(_Slot(stream, event))
+            # The slot's pinned landing buffer, page-locked now rather than in the dispatch loop
+            # (pinning ~100 MB stalls it); grown only for a mesh larger than max_vertices.
+            self._slots.append(_Slot(stream, event, host=PinnedArray(max_columns * max_vertices, np.float64)))
         self._latencies: list[float] = []
         self._cold: list[bool] = []
         self._batches: list[int] = []
@@ -275,6 +294,7 @@ class GeodesicServer:
         for entry in list(self.cache.entries.values()):
             entry.release()
         self.cache.entries.clear()
+        sys.setswitchinterval(self._switch_interval)
 
     def reset_stats(self) -> None:
         """Start a new measurement window (after a warm-up); the cache is kept."""
@@ -312,11 +332,13 @@ class GeodesicServer:
         }
 
     # -- scheduler thread -----------------------------------------------------------------------
-    @staticmethod
-    def _free_memory() -> int:
-        free, total = ctypes.c_size_t(0), ctypes.c_size_t(0)
-        _lib.call("ob_mem_info", ctypes.byref(free), ctypes.byref(total))
-        return int(free.value)
+    def _free_memory(self) -> int:
+        now = time.perf_counter()
+        if now - self._free_reading[0] > FREE_MEMORY_REUSE_S:
+            free, total = ctypes.c_size_t(0), ctypes.c_size_t(0)
+            _lib.call("ob_mem_info", ctypes.byref(free), ctypes.byref(total))
+            self._free_reading = (now, int(free.value))
+        return self._free_reading[1]
 
     def _schedule(self) -> None:
         while self._running or self._outstanding:
@@ -358,12 +380,13 @@ class GeodesicServer:
             entry.pending.append(request)
             return
         request.cold = True
-        if request.key in self._waiting:
-            self._hits += 1  # the mesh is being set up: no second setup
-            self._waiting[request.key].append(request)
-            return
-        self._misses += 1
-        self._waiting[request.key] = [request]
+        with self._waiting_lock:
+            if request.key in self._waiting:
+                self._hits += 1  # the mesh is being set up: no second setup
+                self._waiting[request.key].append(request)
+                return
+            self._misses += 1
+            self._waiting[request.key] = [request]
         self._deferred.append(request)
         self._retry_deferred()
 
@@ -389,7 +412,8 @@ class GeodesicServer:
         return progressed
 
     def _settle_setup(self, key: str, entry: _Resident | None, error: BaseException | None) -> None:
-        waiting = self._waiting.pop(key, [])
+        with self._waiting_lock:
+            waiting = self._waiting.pop(key, [])
         if error is not None:
             self.cache.cancel(key)
             for request in waiting:
@@ -399,7 +423,9 @@ class GeodesicServer:
         entry.pending.extend(waiting)
 
     def _fail_waiting(self, key: str, error: BaseException) -> None:
-        for request in self._waiting.pop(key, []):
+        with self._waiting_lock:
+            waiting = self._waiting.pop(key, [])
+        for request in waiting:
             self._complete(request, error=error)
 
     def _next_entry(self) -> _Resident | None:
@@ -430,7 +456,10 @@ class GeodesicServer:
         _lib.call("ob_memcpy", entry.d_src.ptr, entry.h_src.ptr, 4 * total, 0, st, 0)
         _lib.call("ob_memcpy", entry.d_off.ptr, entry.h_off.ptr, 4 * (kb + 1), 0, st, 0)
         entry.steps[kb].launch(st)  # the whole pass: one graph replay
-        _lib.call("ob_memcpy", entry.h_out.ptr, entry.d_out.ptr, 8 * k * entry.n, 1, st, 0)
+        need = k * entry.n
+        if slot.host is None or slot.host.array.size < need:
+            slot.host = PinnedArray(max(need, self.max_columns * entry.n), np.float64)
+        _lib.call("ob_memcpy", slot.host.ptr, entry.d_out.ptr, 8 * need, 1, st, 0)
         _lib.call("ob_event_record", slot.event, st)
         entry.busy = True
         slot.batch = (entry, requests)
@@ -439,9 +468,10 @@ class GeodesicServer:
     def _finish(self, slot: _Slot) -> None:
         entry, requests = slot.batch
         slot.batch = None
-        rows = entry.h_out.array
+        rows = slot.host.array
+        n = entry.n
         for c, request in enumerate(requests):
-            self._complete(request, result=rows[c].copy())
+            self._complete(request, result=rows[c * n:(c + 1) * n].copy())
         entry.busy = False
 
     def _complete(self, request: _Request, result: Any = None, error: BaseException | None = None) -> None:
@@ -472,6 +502,8 @@ class GeodesicServer:
             try:
                 mesh = Trimesh(request.vertices, request.faces)
                 solver = mesh.heat_solver(None, method=self.method)
+                solver.factor_on_second_solve = False
+                self._answer_plain(request.key, mesh)
                 if not solver.factor():
                     raise MemoryError("the mesh's systems could not be factored within the budget")
                 n = mesh.n_vertices
@@ -487,15 +519,37 @@ class GeodesicServer:
                     h_src=PinnedArray(cap_sources, np.int32),
                     h_off=PinnedArray(self.max_columns + 1, np.int32),
                     d_out=DeviceArray.empty((self.max_columns, n), np.float64),
-                    h_out=PinnedArray((self.max_columns, n), np.float64),
                 )
                 # Every batch width's pass recorded now, as one graph each.
                 self._record(entry, capture)
                 entry.nbytes = int(mesh.nbytes + solver.nbytes + entry.d_out.nbytes)
-                _lib.call("ob_device_synchronize")
+                _lib.call("ob_stream_synchronize", None)
+                _lib.call("ob_stream_synchronize", capture)
                 self._ready.put((request.key, entry, None))
             except BaseException as exc:  # noqa: BLE001 -- the error belongs to the requests
                 self._ready.put((request.key, None, exc))
+
+    def _answer_plain(self, key: str, mesh: Any) -> None:
+        """Answer up to ``plain_answers`` of the mesh's waiting requests by the unfactored path
+        (rent before buy); the rest wait for the factored batches."""
+        from ordito_b200 import heat as gheat  # noqa: PLC0415
+
+        answered = 0
+        while answered < self.plain_answers:
+            with self._waiting_lock:
+                waiting = self._waiting.get(key)
+                if not waiting:
+                    return
+                take = waiting[: self.plain_answers - answered]
+                del waiting[: len(take)]
+            for request in take:
+                try:
+                    distances = gheat.heat_geodesic(mesh, request.sources, method=self.method).numpy()
+                except Exception as exc:  # noqa: BLE001 -- the error belongs to the request
+                    self._complete(request, error=exc)
+                else:
+                    self._complete(request, result=distances)
+                answered += 1
 
     def _record(self, entry: _Resident, capture: ctypes.c_void_p) -> None:
         from ordito_b200 import heat as gheat  # noqa: PLC0415
@@ -511,7 +565,9 @@ class GeodesicServer:
             out = DeviceArray(entry.d_out.ptr, (width, entry.n), np.float64, owned=False, base=entry.d_out)
             src = DeviceArray(entry.d_src.ptr, (width,), np.int32, owned=False, base=entry.d_src)
             off = DeviceArray(entry.d_off.ptr, (width + 1,), np.int32, owned=False, base=entry.d_off)
-            entry.steps[width] = gheat.BatchStep(entry.mesh, entry.solver, src, off, width, out, capture)
+            # The widest first runs the pass once to prepare the mesh; the rest record directly.
+            entry.steps[width] = gheat.BatchStep(entry.mesh, entry.solver, src, off, width, out,
+                                                 capture, warm=not entry.steps)
 
 
 # -- synthetic serving workload ---------------------------------------------------------------
