@@ -718,23 +718,25 @@ __device__ bool grid_barrier(unsigned int* bar, int* status, unsigned int limit)
 // listed rows are zeroed, then each phase's (tile, column block) pairs are spread over the
 // resident CTAs with a grid barrier between phases.
 __global__ void __launch_bounds__(kTileThreads)
-pass_kernel(const Phase* __restrict__ phases, int n_phases, const int2* __restrict__ zero,
+pass_kernel(const Phase* __restrict__ phases, int p_lo, int p_hi, const int2* __restrict__ zero,
             int n_zero, const double* __restrict__ vals, const int* __restrict__ idx, double* B,
             double* Y, double* X, int k, unsigned int* bar, int* status, unsigned int limit) {
     extern __shared__ __align__(16) unsigned char shared_stages[];
     Stage* stage = reinterpret_cast<Stage*>(shared_stages);
     double* buffers[3] = {B, Y, X};
-    for (int z = blockIdx.x; z < n_zero; z += gridDim.x) {
-        const int2 range = zero[z];
-        const long long begin = (long long)range.x * k, end = (long long)(range.x + range.y) * k;
-        for (long long t = begin + threadIdx.x; t < end; t += blockDim.x) {
-            Y[t] = 0.0;
-            X[t] = 0.0;
+    if (n_zero > 0) {
+        for (int z = blockIdx.x; z < n_zero; z += gridDim.x) {
+            const int2 range = zero[z];
+            const long long begin = (long long)range.x * k, end = (long long)(range.x + range.y) * k;
+            for (long long t = begin + threadIdx.x; t < end; t += blockDim.x) {
+                Y[t] = 0.0;
+                X[t] = 0.0;
+            }
         }
+        if (!grid_barrier(bar, status, limit)) return;
     }
-    if (!grid_barrier(bar, status, limit)) return;
     const int column_blocks = (k + kTileCols - 1) / kTileCols;
-    for (int p = 0; p < n_phases; ++p) {
+    for (int p = p_lo; p < p_hi; ++p) {
         const Phase ph = phases[p];
         const int work = ph.count * column_blocks;
         for (int w = blockIdx.x; w < work; w += gridDim.x)
@@ -822,6 +824,10 @@ struct Factor {
     unsigned int* barrier = nullptr;
     int* status = nullptr;
     int pass_grid = 0;
+    // The hybrid pass: phases [hybrid_lo, hybrid_hi) (the tree levels from hybrid_level up, both
+    // directions) in one cooperative launch of at most hybrid_grid CTAs, the rest per phase.
+    std::vector<Phase> host_phases;
+    int hybrid_level = -1, hybrid_lo = -1, hybrid_hi = -1, hybrid_grid = 0, hybrid_tiles = 0;
     // Work buffers sized for `cap_k` columns: B, Y, X in the factor's numbering, R the residual,
     // RHS / SOL the caller's right-hand side and solution copied in / out (old numbering).
     int cap_k = 0;
@@ -841,6 +847,94 @@ struct Factor {
     std::vector<Recorded> graphs;
     cudaStream_t capture = nullptr;
 };
+
+__global__ void cooperative_probe_kernel(int* out) {
+    if (out != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *out = 1;
+}
+
+// Whether a cooperative launch can be recorded into a CUDA graph on this runtime (probed once: the
+// hybrid pass below is recorded inside every served pass).
+bool cooperative_recordable() {
+    static int state = -1;
+    std::lock_guard<std::recursive_mutex> guard(capture_mutex());
+    if (state >= 0) return state == 1;
+    cudaStream_t s = nullptr;
+    bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    if (ok) ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(2);
+        cfg.blockDim = dim3(32);
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const bool launched = cudaLaunchKernelEx(&cfg, cooperative_probe_kernel, (int*)nullptr) == cudaSuccess;
+        const bool ended = cudaStreamEndCapture(s, &graph) == cudaSuccess;
+        ok = launched && ended && graph != nullptr &&
+             cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (s) cudaStreamDestroy(s);
+    cudaGetLastError();
+    state = ok ? 1 : 0;
+    return ok;
+}
+
+// The hybrid pass's split (Factor::hybrid_*), opt-in through OB_CHOL_HYBRID_LEVEL: from that tree
+// level ("auto": the lowest at which every phase's tiles fit one wave of the co-resident grid)
+// both directions run in one cooperative launch with a bounded grid barrier between phases.
+// Measured on the 131k-vertex torus at 64 columns it is slower than a recorded launch per phase
+// (1.05-1.15 ms a pass against 0.92 ms): the barrier over the co-resident grid costs more than a
+// kernel boundary inside a graph.
+void choose_hybrid(Factor* F, const std::vector<int>& level) {
+    const char* knob = getenv("OB_CHOL_HYBRID_LEVEL");
+    if (knob == nullptr || std::strcmp(knob, "off") == 0) return;
+    int device = 0, cooperative = 0, per_sm = 0;
+    if (cudaGetDevice(&device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&cooperative, cudaDevAttrCooperativeLaunch, device) != cudaSuccess ||
+        !cooperative ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel, kTileThreads, kStageBytes) !=
+            cudaSuccess ||
+        per_sm <= 0) {
+        cudaGetLastError();
+        return;
+    }
+    const int grid = per_sm * sm_count();
+    const int L = F->analysis->levels;
+    const int n = (int)F->host_phases.size();
+    int c = -1;
+    if (std::strcmp(knob, "auto") != 0) {
+        c = std::atoi(knob);
+    } else {
+        for (int l = 0; l < L && c < 0; ++l) {
+            bool fits = true;
+            for (int p = 0; p < n; ++p)
+                if (level[p] >= l && F->host_phases[p].count > grid) fits = false;
+            if (fits) c = l;
+        }
+    }
+    if (c < 0 || c >= L) return;
+    int lo = -1, hi = -1, tiles = 0;
+    for (int p = 0; p < n; ++p)
+        if (level[p] >= c) {
+            if (lo < 0) lo = p;
+            hi = p + 1;
+            tiles = std::max(tiles, F->host_phases[p].count);
+        }
+    if (lo < 0 || hi - lo < 4 || tiles > grid) return;
+    if (!cooperative_recordable()) return;
+    F->hybrid_level = c;
+    F->hybrid_lo = lo;
+    F->hybrid_hi = hi;
+    F->hybrid_grid = grid;
+    F->hybrid_tiles = tiles;
+}
 
 int dev_alloc(Factor* F, void** p, size_t bytes, cudaStream_t stream) {
     OB_CUDA(cudaMallocAsync(p, std::max<size_t>(bytes, 8), stream));
@@ -995,15 +1089,21 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
     if (!st) st = push(bo, F->bwd_off, F->n_bwd_off);
     if (!st) st = push(bd, F->bwd_diag, F->n_bwd_diag);
     if (st) return st;
-    // The persistent pass's phase table, in the order the per-phase launches run.
+    // The persistent pass's phase table, in the order the per-phase launches run, and each
+    // phase's tree level.
     std::vector<Phase> phases;
+    std::vector<int> phase_level;
     for (int l = 0; l < L; ++l) {
         if (F->n_fwd_diag[l]) phases.push_back(Phase{F->fwd_diag[l], F->n_fwd_diag[l], 0, 1});
+        if (F->n_fwd_diag[l]) phase_level.push_back(l);
         if (F->n_fwd_off[l]) phases.push_back(Phase{F->fwd_off[l], F->n_fwd_off[l], 1, 0});
+        if (F->n_fwd_off[l]) phase_level.push_back(l);
     }
     for (int l = L - 1; l >= 0; --l) {
         if (F->n_bwd_off[l]) phases.push_back(Phase{F->bwd_off[l], F->n_bwd_off[l], 2, 1});
+        if (F->n_bwd_off[l]) phase_level.push_back(l);
         if (F->n_bwd_diag[l]) phases.push_back(Phase{F->bwd_diag[l], F->n_bwd_diag[l], 1, 2});
+        if (F->n_bwd_diag[l]) phase_level.push_back(l);
     }
     F->n_phases = (int)phases.size();
     st = dev_alloc(F, (void**)&F->phases, sizeof(Phase) * std::max<size_t>(phases.size(), 1), stream);
@@ -1028,6 +1128,8 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
         per_sm > 0)
         F->pass_grid = per_sm * sm_count();
     cudaGetLastError();
+    F->host_phases = phases;
+    choose_hybrid(F, phase_level);
     OB_CUDA(cudaStreamSynchronize(stream));  // host staging buffers go out of scope
     return OB_OK;
 }
@@ -1082,7 +1184,7 @@ int triangular_solves(Factor* F, int k, cudaStream_t stream) {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         const unsigned int limit = 1u << 23;
-        OB_CUDA(cudaLaunchKernelEx(&cfg, pass_kernel, (const Phase*)F->phases, F->n_phases,
+        OB_CUDA(cudaLaunchKernelEx(&cfg, pass_kernel, (const Phase*)F->phases, 0, F->n_phases,
                                    (const int2*)F->zero, F->n_zero, (const double*)F->vals,
                                    (const int*)F->idx, F->B, F->Y, F->X, k, F->barrier, F->status,
                                    limit));
@@ -1092,6 +1194,38 @@ int triangular_solves(Factor* F, int k, cudaStream_t stream) {
     if (F->n_zero > 0) {
         zero_rows_kernel<<<F->n_zero, 256, 0, stream>>>(F->zero, F->n_zero, k, F->Y, F->X);
         OB_CHECK_LAUNCH("chol zero split rows");
+    }
+    if (F->hybrid_lo >= 0 && k > 8) {
+        // The hybrid pass: the lower levels' phases one launch each, the upper levels' (both
+        // directions) in one cooperative launch with grid barriers between phases.
+        double* buffers[3] = {F->B, F->Y, F->X};
+        auto one = [&](int p) {
+            const Phase& ph = F->host_phases[p];
+            tile_product_kernel<<<dim3(ph.count, ct), threads, kStageBytes, stream>>>(
+                ph.tiles, F->vals, F->idx, buffers[ph.in], buffers[ph.out], k);
+            OB_CHECK_LAUNCH("chol pass phase");
+            return OB_OK;
+        };
+        int st = OB_OK;
+        for (int p = 0; p < F->hybrid_lo && st == OB_OK; ++p) st = one(p);
+        if (st) return st;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(std::min(F->hybrid_grid, F->hybrid_tiles * ct));
+        cfg.blockDim = threads;
+        cfg.dynamicSmemBytes = kStageBytes;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        const unsigned int limit = 1u << 23;
+        OB_CUDA(cudaLaunchKernelEx(&cfg, pass_kernel, (const Phase*)F->phases, F->hybrid_lo, F->hybrid_hi,
+                                   (const int2*)nullptr, 0, (const double*)F->vals, (const int*)F->idx,
+                                   F->B, F->Y, F->X, k, F->barrier, F->status, limit));
+        count_launch();
+        for (int p = F->hybrid_hi; p < (int)F->host_phases.size() && st == OB_OK; ++p) st = one(p);
+        return st;
     }
     // A phase's launch: the float64 tensor-core tiles, or for a narrow batch (stride 2-8) the
     // register kernel, which does not compute a 64-column tile's idle columns.
@@ -1182,9 +1316,10 @@ int solve_graph(Factor* F, int k, int refine, const int* offsets, const int* col
     if (graph) cudaGraphDestroy(graph);
     if (st != OB_OK || e != cudaSuccess) {
         cudaGetLastError();
-        if (F->pass_grid > 0) {
+        if (F->pass_grid > 0 || F->hybrid_lo >= 0) {
             // A cooperative launch this runtime cannot record: fall back to a launch per phase.
             F->pass_grid = 0;
+            F->hybrid_lo = F->hybrid_hi = -1;
             return solve_graph(F, k, refine, offsets, columns, values, out);
         }
         return st != OB_OK ? st : cuda_status(e, "ob_chol_solve: capture");
@@ -1427,10 +1562,10 @@ int ob_chol_info(void* factor, long long* info) {
     info[0] = F->n;
     info[1] = F->n_vals;
     info[2] = F->analysis->levels;
-    long long launches = 0;
-    for (int l = 0; l < F->analysis->levels; ++l)
-        launches += (F->n_fwd_diag[l] > 0) + (F->n_fwd_off[l] > 0) + (F->n_bwd_off[l] > 0) +
-                    (F->n_bwd_diag[l] > 0);
+    // Kernel launches a pass over a wide batch makes (a phase each, or with the hybrid pass the
+    // lower phases plus one cooperative launch for the upper ones).
+    long long launches = (long long)F->host_phases.size();
+    if (F->hybrid_lo >= 0) launches += 1 - (F->hybrid_hi - F->hybrid_lo);
     info[3] = launches;
     return OB_OK;
 }
