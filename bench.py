@@ -528,12 +528,23 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     # with one launch on its own stream; with refinement steps, the eager pass instead.
     stream = ctypes.c_void_p(0)
     _lib.call("ob_stream_create", ctypes.byref(stream))
+    in_flight = 1
     if args.refine == 0:
-        graph_step = gheat.BatchStep(mesh, solver, src, offsets, k,
-                                     DeviceArray.empty((k, n), np.float64), stream)
+        # Two batches in flight: the factors' two work sets, each pass recorded on its own stream,
+        # consecutive steps alternating between them (a served stream of batches).
+        second = ctypes.c_void_p(0)
+        _lib.call("ob_stream_create", ctypes.byref(second))
+        streams = [stream, second]
+        graph_steps = [gheat.BatchStep(mesh, solver, src, offsets, k,
+                                       DeviceArray.empty((k, n), np.float64), streams[w], work_set=w)
+                       for w in range(2)]
+        turn = [0]
+        in_flight = 2
 
         def step():
-            return graph_step.launch(stream)
+            w = turn[0]
+            turn[0] ^= 1
+            return graph_steps[w].launch(streams[w])
     else:
         stream = ctypes.c_void_p(0)  # the eager pass runs on the default stream
 
@@ -564,12 +575,29 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     launches0 = _lib.launch_count()
     with Clocks(dist.local_rank) as clocks:
         _lib.call("ob_event_record", start, stream)
+        if in_flight == 2:
+            _lib.call("ob_stream_wait_event", second, start)
         for _ in range(args.steps):
             out = step()
+        if in_flight == 2:
+            joined = ctypes.c_void_p(0)
+            _lib.call("ob_event_create", ctypes.byref(joined))
+            _lib.call("ob_event_record", joined, second)
+            _lib.call("ob_stream_wait_event", stream, joined)
         _lib.call("ob_event_record", end, stream)
         synchronize()
     launches = (_lib.launch_count() - launches0) // max(args.steps, 1)
     ms = _elapsed(start, end) / args.steps
+    single_ms = None
+    if in_flight == 2:
+        # The same steps one at a time (one stream, one work set), for the record.
+        synchronize()
+        _lib.call("ob_event_record", start, stream)
+        for _ in range(args.steps):
+            graph_steps[0].launch(stream)
+        _lib.call("ob_event_record", end, stream)
+        synchronize()
+        single_ms = _elapsed(start, end) / args.steps
     dist.barrier()
     ms_max = dist.max(ms)
     value = dist.world * k / (ms_max / 1e3)
@@ -704,6 +732,9 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
             "steps": args.steps,
             "warmup": args.warmup,
             "ms_per_step": ms_max,
+            "batches_in_flight": in_flight,
+            "one_in_flight": None if single_ms is None else {
+                "value": dist.world * k / (single_ms / 1e3), "ms_per_step": single_ms},
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,

@@ -112,6 +112,10 @@ SIGNATURES: dict[str, list] = {
     "ob_chol_time_solve": [P, I, I, POINTER(c_float), P],
     "ob_chol_info": [P, POINTER(ctypes.c_longlong)],
     "ob_chol_work_generation": [P, POINTER(ctypes.c_longlong)],
+    "ob_chol_work_set": [P, I, I, POINTER(c_void_p), POINTER(c_void_p), POINTER(c_int), POINTER(c_void_p),
+                         POINTER(c_void_p), P],
+    "ob_chol_solve_in_place_set": [P, I, I, P],
+    "ob_chol_work_generation_set": [P, I, POINTER(ctypes.c_longlong)],
     "ob_march_solve": [I, P, P, P, P, P, POINTER(ctypes.c_longlong), P],
     "ob_edge_sums_segments": [P, P, P, P, I, P, I, P, I, P, P],
     "ob_heat_rows_packed": [P, P, P, P, I, P, I, P, P, P, D, P, P, P, P, P],

@@ -104,26 +104,31 @@ class SparseCholesky:
                   ctypes.byref(sol), DEFAULT_STREAM)
         return int(rhs.value), int(sol.value)
 
-    def work(self, n_columns: int, stream: Any = None) -> tuple[int, int, int, int, int]:
-        """``(B, X, stride, iperm, pinned)`` device pointers of the factor's own buffers in its
-        numbering (``ob_chol_work``), for pipelines that stay in it."""
+    def work(self, n_columns: int, stream: Any = None, work_set: int = 0) -> tuple[int, int, int, int, int]:
+        """``(B, X, stride, iperm, pinned)`` device pointers of the factor's own buffers (of work
+        set ``work_set``, 0 or 1) in its numbering (``ob_chol_work_set``), for pipelines that stay
+        in it."""
         b, x, iperm, pinned = (ctypes.c_void_p(0) for _ in range(4))
         stride = ctypes.c_int(0)
-        _lib.call("ob_chol_work", self.handle, int(n_columns), ctypes.byref(b), ctypes.byref(x),
-                  ctypes.byref(stride), ctypes.byref(iperm), ctypes.byref(pinned),
+        _lib.call("ob_chol_work_set", self.handle, int(work_set), int(n_columns), ctypes.byref(b),
+                  ctypes.byref(x), ctypes.byref(stride), ctypes.byref(iperm), ctypes.byref(pinned),
                   stream if stream is not None else DEFAULT_STREAM)
         return int(b.value), int(x.value), int(stride.value), int(iperm.value), int(pinned.value)
 
     @property
     def generation(self) -> int:
         """Changes whenever the buffers ``work`` points at are reallocated (``ob_chol_work_generation``)."""
+        return self.work_generation(0)
+
+    def work_generation(self, work_set: int) -> int:
         value = ctypes.c_longlong(0)
-        _lib.call("ob_chol_work_generation", self.handle, ctypes.byref(value))
+        _lib.call("ob_chol_work_generation_set", self.handle, int(work_set), ctypes.byref(value))
         return int(value.value)
 
-    def solve_in_place(self, n_columns: int, stream: Any = None) -> None:
-        """``X = A^-1 B`` on the factor's own buffers, in its numbering (no read-back)."""
-        _lib.call("ob_chol_solve_in_place", self.handle, int(n_columns),
+    def solve_in_place(self, n_columns: int, stream: Any = None, work_set: int = 0) -> None:
+        """``X = A^-1 B`` on the factor's own buffers (work set ``work_set``), in its numbering
+        (no read-back)."""
+        _lib.call("ob_chol_solve_in_place_set", self.handle, int(work_set), int(n_columns),
                   stream if stream is not None else DEFAULT_STREAM)
 
     def solve_pointers(self, rhs: int, x: int, n_columns: int, refine: int, stream: Any = None) -> None:

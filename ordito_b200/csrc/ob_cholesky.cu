@@ -440,6 +440,7 @@ struct Tile {
 };
 
 constexpr int kTileRows = 64;   // output rows per tile
+constexpr int kWorkSets = 2;    // independent work-buffer sets a factor holds
 constexpr int kTileCols = 64;   // right-hand-side columns per tile
 // Inner-dimension step staged in shared memory. 16 (two stages, 39 KB, 4 CTAs per SM) measured
 // 0.82 ms a pass on the 131k torus at 64 columns, against 1.11 ms for 32 (74 KB, 3 CTAs per SM).
@@ -828,13 +829,6 @@ struct Factor {
     // directions) in one cooperative launch of at most hybrid_grid CTAs, the rest per phase.
     std::vector<Phase> host_phases;
     int hybrid_level = -1, hybrid_lo = -1, hybrid_hi = -1, hybrid_grid = 0, hybrid_tiles = 0;
-    // Work buffers sized for `cap_k` columns: B, Y, X in the factor's numbering, R the residual,
-    // RHS / SOL the caller's right-hand side and solution copied in / out (old numbering).
-    int cap_k = 0;
-    double *B = nullptr, *Y = nullptr, *X = nullptr, *R = nullptr, *RHS = nullptr, *SOL = nullptr;
-    // Bumped whenever the work buffers are reallocated: a graph recorded outside the factor (over
-    // ob_chol_work's pointers) is stale once it changes.
-    long long generation = 0;
     size_t bytes = 0;
     // Recorded solve graphs, keyed by (columns, refinement steps, operator arrays).
     struct Recorded {
@@ -844,7 +838,19 @@ struct Factor {
         cudaGraphExec_t exec;
         int launches;
     };
-    std::vector<Recorded> graphs;
+    // A set of work buffers sized for `cap_k` columns: B, Y, X in the factor's numbering, R the
+    // residual, RHS / SOL the caller's right-hand side and solution copied in / out (old
+    // numbering), and the solve graphs recorded over them. Passes on different sets are
+    // independent and may run concurrently (each set on one stream at a time).
+    struct WorkSet {
+        int cap_k = 0;
+        double *B = nullptr, *Y = nullptr, *X = nullptr, *R = nullptr, *RHS = nullptr, *SOL = nullptr;
+        // Bumped whenever the buffers are reallocated: a graph recorded outside the factor (over
+        // ob_chol_work's pointers) is stale once it changes.
+        long long generation = 0;
+        std::vector<Recorded> graphs;
+    };
+    WorkSet sets[kWorkSets];
     cudaStream_t capture = nullptr;
 };
 
@@ -949,7 +955,8 @@ void factor_release(Factor* F) {
         std::lock_guard<std::recursive_mutex> guard(capture_mutex());
         cudaDeviceSynchronize();
     }
-    for (auto& g : F->graphs) cudaGraphExecDestroy(g.exec);
+    for (auto& W : F->sets)
+        for (auto& g : W.graphs) cudaGraphExecDestroy(g.exec);
     if (F->capture) cudaStreamDestroy(F->capture);
     for (void* p : F->owned) cudaFree(p);
     delete F;
@@ -1137,15 +1144,15 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
 // The internal column stride of B, Y and X: even, so every row starts on 16 bytes.
 inline int even_columns(int k) { return (k + 1) & ~1; }
 
-int ensure_work(Factor* F, int k, cudaStream_t stream) {
-    if (k <= F->cap_k) return OB_OK;
+int ensure_work(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream) {
+    if (k <= W.cap_k) return OB_OK;
     // Growing the buffers invalidates every recorded graph (they name the old ones).
     OB_CUDA(cudaStreamSynchronize(stream));
-    for (auto& g : F->graphs) cudaGraphExecDestroy(g.exec);
-    F->graphs.clear();
+    for (auto& g : W.graphs) cudaGraphExecDestroy(g.exec);
+    W.graphs.clear();
     // The smaller buffers go (no graph names them any more): one set of six at the widest width.
-    const size_t old_vec = sizeof(double) * (size_t)F->n * (F->cap_k > 0 ? even_columns(F->cap_k) : 0);
-    for (double** p : {&F->B, &F->Y, &F->X, &F->R, &F->RHS, &F->SOL}) {
+    const size_t old_vec = sizeof(double) * (size_t)F->n * (W.cap_k > 0 ? even_columns(W.cap_k) : 0);
+    for (double** p : {&W.B, &W.Y, &W.X, &W.R, &W.RHS, &W.SOL}) {
         if (*p == nullptr) continue;
         auto it = std::find(F->owned.begin(), F->owned.end(), (void*)*p);
         if (it != F->owned.end()) {
@@ -1156,17 +1163,17 @@ int ensure_work(Factor* F, int k, cudaStream_t stream) {
         *p = nullptr;
     }
     const size_t vec = sizeof(double) * (size_t)F->n * even_columns(k);
-    for (double** p : {&F->B, &F->Y, &F->X, &F->R, &F->RHS, &F->SOL}) {
+    for (double** p : {&W.B, &W.Y, &W.X, &W.R, &W.RHS, &W.SOL}) {
         int st = dev_alloc(F, (void**)p, vec, stream);
         if (st) return st;
     }
-    F->cap_k = k;
-    ++F->generation;
+    W.cap_k = k;
+    ++W.generation;
     return OB_OK;
 }
 
 // x_new = A^-1 b_new in the factor's numbering (B is consumed); k is the even internal stride.
-int triangular_solves(Factor* F, int k, cudaStream_t stream) {
+int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream) {
     const int L = F->analysis->levels;
     const dim3 threads(kTileThreads);
     const int ct = (k + kTileCols - 1) / kTileCols;
@@ -1186,19 +1193,19 @@ int triangular_solves(Factor* F, int k, cudaStream_t stream) {
         const unsigned int limit = 1u << 23;
         OB_CUDA(cudaLaunchKernelEx(&cfg, pass_kernel, (const Phase*)F->phases, 0, F->n_phases,
                                    (const int2*)F->zero, F->n_zero, (const double*)F->vals,
-                                   (const int*)F->idx, F->B, F->Y, F->X, k, F->barrier, F->status,
+                                   (const int*)F->idx, W.B, W.Y, W.X, k, F->barrier, F->status,
                                    limit));
         count_launch();
         return OB_OK;
     }
     if (F->n_zero > 0) {
-        zero_rows_kernel<<<F->n_zero, 256, 0, stream>>>(F->zero, F->n_zero, k, F->Y, F->X);
+        zero_rows_kernel<<<F->n_zero, 256, 0, stream>>>(F->zero, F->n_zero, k, W.Y, W.X);
         OB_CHECK_LAUNCH("chol zero split rows");
     }
     if (F->hybrid_lo >= 0 && k > 8) {
         // The hybrid pass: the lower levels' phases one launch each, the upper levels' (both
         // directions) in one cooperative launch with grid barriers between phases.
-        double* buffers[3] = {F->B, F->Y, F->X};
+        double* buffers[3] = {W.B, W.Y, W.X};
         auto one = [&](int p) {
             const Phase& ph = F->host_phases[p];
             tile_product_kernel<<<dim3(ph.count, ct), threads, kStageBytes, stream>>>(
@@ -1222,7 +1229,7 @@ int triangular_solves(Factor* F, int k, cudaStream_t stream) {
         const unsigned int limit = 1u << 23;
         OB_CUDA(cudaLaunchKernelEx(&cfg, pass_kernel, (const Phase*)F->phases, F->hybrid_lo, F->hybrid_hi,
                                    (const int2*)nullptr, 0, (const double*)F->vals, (const int*)F->idx,
-                                   F->B, F->Y, F->X, k, F->barrier, F->status, limit));
+                                   W.B, W.Y, W.X, k, F->barrier, F->status, limit));
         count_launch();
         for (int p = F->hybrid_hi; p < (int)F->host_phases.size() && st == OB_OK; ++p) st = one(p);
         return st;
@@ -1244,14 +1251,14 @@ int triangular_solves(Factor* F, int k, cudaStream_t stream) {
     };
     int st = OB_OK;
     for (int l = 0; l < L && st == OB_OK; ++l) {
-        if (F->n_fwd_diag[l]) st = phase(F->fwd_diag[l], F->n_fwd_diag[l], F->B, F->Y, "chol forward diagonal");
+        if (F->n_fwd_diag[l]) st = phase(F->fwd_diag[l], F->n_fwd_diag[l], W.B, W.Y, "chol forward diagonal");
         if (st == OB_OK && F->n_fwd_off[l])
-            st = phase(F->fwd_off[l], F->n_fwd_off[l], F->Y, F->B, "chol forward update");
+            st = phase(F->fwd_off[l], F->n_fwd_off[l], W.Y, W.B, "chol forward update");
     }
     for (int l = L - 1; l >= 0 && st == OB_OK; --l) {
-        if (F->n_bwd_off[l]) st = phase(F->bwd_off[l], F->n_bwd_off[l], F->X, F->Y, "chol backward gather");
+        if (F->n_bwd_off[l]) st = phase(F->bwd_off[l], F->n_bwd_off[l], W.X, W.Y, "chol backward gather");
         if (st == OB_OK && F->n_bwd_diag[l])
-            st = phase(F->bwd_diag[l], F->n_bwd_diag[l], F->Y, F->X, "chol backward diagonal");
+            st = phase(F->bwd_diag[l], F->n_bwd_diag[l], W.Y, W.X, "chol backward diagonal");
     }
     return st;
 }
@@ -1261,35 +1268,35 @@ int grid_for(long long total) {
 }
 
 // The whole solve on the factor's own buffers: SOL = A^-1 RHS plus `refine` refinement steps.
-int enqueue_solve(Factor* F, int k, int refine, const int* offsets, const int* columns,
+int enqueue_solve(Factor* F, Factor::WorkSet& W, int k, int refine, const int* offsets, const int* columns,
                   const double* values, cudaStream_t stream) {
     const int n = F->n, kp = even_columns(k);
     const int grid = grid_for((long long)n * kp);
-    permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, F->pinned, F->RHS, F->B);
+    permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, F->pinned, W.RHS, W.B);
     OB_CHECK_LAUNCH("chol permute in");
-    int st = triangular_solves(F, kp, stream);
+    int st = triangular_solves(F, W, kp, stream);
     if (st) return st;
-    permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, F->X, F->SOL, 0);
+    permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, W.X, W.SOL, 0);
     OB_CHECK_LAUNCH("chol permute out");
     // Iterative refinement in float64: x += A^-1 (b - A x).
     for (int it = 0; it < refine; ++it) {
-        residual_kernel<<<grid, 256, 0, stream>>>(n, k, offsets, columns, values, F->RHS, F->SOL,
-                                                  F->R);
+        residual_kernel<<<grid, 256, 0, stream>>>(n, k, offsets, columns, values, W.RHS, W.SOL,
+                                                  W.R);
         OB_CHECK_LAUNCH("chol residual");
-        permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, F->pinned, F->R, F->B);
+        permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, F->pinned, W.R, W.B);
         OB_CHECK_LAUNCH("chol permute in");
-        st = triangular_solves(F, kp, stream);
+        st = triangular_solves(F, W, kp, stream);
         if (st) return st;
-        permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, F->X, F->SOL, 1);
+        permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, W.X, W.SOL, 1);
         OB_CHECK_LAUNCH("chol permute out");
     }
     return OB_OK;
 }
 
 // The recorded graph of enqueue_solve for (k, refine, operator), recorded on first use.
-int solve_graph(Factor* F, int k, int refine, const int* offsets, const int* columns,
+int solve_graph(Factor* F, Factor::WorkSet& W, int k, int refine, const int* offsets, const int* columns,
                 const double* values, Factor::Recorded** out) {
-    for (auto& g : F->graphs)
+    for (auto& g : W.graphs)
         if (g.k == k && g.refine == refine && g.offsets == offsets && g.columns == columns &&
             g.values == values) {
             *out = &g;
@@ -1302,8 +1309,8 @@ int solve_graph(Factor* F, int k, int refine, const int* offsets, const int* col
     cudaError_t e = cudaStreamBeginCapture(F->capture, cudaStreamCaptureModeThreadLocal);
     // refine < 0 records the bare triangular passes B -> X in the factor's own numbering.
     int st = e != cudaSuccess ? cuda_status(e, "ob_chol_solve: begin capture")
-             : refine < 0     ? triangular_solves(F, even_columns(k), F->capture)
-                              : enqueue_solve(F, k, refine, offsets, columns, values, F->capture);
+             : refine < 0     ? triangular_solves(F, W, even_columns(k), F->capture)
+                              : enqueue_solve(F, W, k, refine, offsets, columns, values, F->capture);
     cudaGraph_t graph = nullptr;
     if (e == cudaSuccess) e = cudaStreamEndCapture(F->capture, &graph);
     suppress_counting(-1);
@@ -1320,12 +1327,12 @@ int solve_graph(Factor* F, int k, int refine, const int* offsets, const int* col
             // A cooperative launch this runtime cannot record: fall back to a launch per phase.
             F->pass_grid = 0;
             F->hybrid_lo = F->hybrid_hi = -1;
-            return solve_graph(F, k, refine, offsets, columns, values, out);
+            return solve_graph(F, W, k, refine, offsets, columns, values, out);
         }
         return st != OB_OK ? st : cuda_status(e, "ob_chol_solve: capture");
     }
-    F->graphs.push_back(Factor::Recorded{k, refine, offsets, columns, values, exec, (int)nodes});
-    *out = &F->graphs.back();
+    W.graphs.push_back(Factor::Recorded{k, refine, offsets, columns, values, exec, (int)nodes});
+    *out = &W.graphs.back();
     return OB_OK;
 }
 
@@ -1448,31 +1455,39 @@ int ob_chol_solve(void* factor, const double* rhs, double* x, int n_columns, int
     OB_REQUIRE(refine == 0 || (offsets && columns && values),
                "ob_chol_solve: refinement needs the operator");
     Factor* F = static_cast<Factor*>(factor);
-    int st = ensure_work(F, n_columns, stream);
+    Factor::WorkSet& W = F->sets[0];
+    int st = ensure_work(F, W, n_columns, stream);
     if (st) return st;
     const size_t bytes = sizeof(double) * (size_t)F->n * n_columns;
-    if (rhs != nullptr && rhs != F->RHS)
-        OB_CUDA(cudaMemcpyAsync(F->RHS, rhs, bytes, cudaMemcpyDeviceToDevice, stream));
+    if (rhs != nullptr && rhs != W.RHS)
+        OB_CUDA(cudaMemcpyAsync(W.RHS, rhs, bytes, cudaMemcpyDeviceToDevice, stream));
     Factor::Recorded* g = nullptr;
-    st = solve_graph(F, n_columns, refine, refine ? offsets : nullptr, refine ? columns : nullptr,
+    st = solve_graph(F, W, n_columns, refine, refine ? offsets : nullptr, refine ? columns : nullptr,
                      refine ? values : nullptr, &g);
     if (st) return st;
     OB_CUDA(cudaGraphLaunch(g->exec, stream));
     count_launch((uint64_t)g->launches);
-    if (x != nullptr && x != F->SOL)
-        OB_CUDA(cudaMemcpyAsync(x, F->SOL, bytes, cudaMemcpyDeviceToDevice, stream));
+    if (x != nullptr && x != W.SOL)
+        OB_CUDA(cudaMemcpyAsync(x, W.SOL, bytes, cudaMemcpyDeviceToDevice, stream));
     return OB_OK;
 }
 
 int ob_chol_work(void* factor, int n_columns, double** rhs, double** solution, int* stride,
                  const int32_t** iperm, const char** pinned, ob_stream_t stream_) {
+    return ob_chol_work_set(factor, 0, n_columns, rhs, solution, stride, iperm, pinned, stream_);
+}
+
+int ob_chol_work_set(void* factor, int set, int n_columns, double** rhs, double** solution, int* stride,
+                     const int32_t** iperm, const char** pinned, ob_stream_t stream_) {
     OB_REQUIRE(factor && rhs && solution && stride && iperm && pinned && n_columns >= 1,
                "ob_chol_work: bad argument");
+    OB_REQUIRE(set >= 0 && set < kWorkSets, "ob_chol_work: set %d outside [0, %d)", set, kWorkSets);
     Factor* F = static_cast<Factor*>(factor);
-    int st = ensure_work(F, n_columns, as_stream(stream_));
+    Factor::WorkSet& W = F->sets[set];
+    int st = ensure_work(F, W, n_columns, as_stream(stream_));
     if (st) return st;
-    *rhs = F->B;
-    *solution = F->X;
+    *rhs = W.B;
+    *solution = W.X;
     *stride = even_columns(n_columns);
     *iperm = F->iperm;
     *pinned = F->pinned;
@@ -1493,22 +1508,28 @@ int ob_chol_check(void* factor, int* status, int* persistent, ob_stream_t stream
 }
 
 int ob_chol_solve_in_place(void* factor, int n_columns, ob_stream_t stream_) {
+    return ob_chol_solve_in_place_set(factor, 0, n_columns, stream_);
+}
+
+int ob_chol_solve_in_place_set(void* factor, int set, int n_columns, ob_stream_t stream_) {
     cudaStream_t stream = as_stream(stream_);
     OB_REQUIRE(factor && n_columns >= 1, "ob_chol_solve_in_place: bad argument");
+    OB_REQUIRE(set >= 0 && set < kWorkSets, "ob_chol_solve_in_place: set %d outside [0, %d)", set, kWorkSets);
     Factor* F = static_cast<Factor*>(factor);
+    Factor::WorkSet& W = F->sets[set];
     cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
     OB_CUDA(cudaStreamIsCapturing(stream, &capturing));
     if (capturing == cudaStreamCaptureStatusActive) {
         // Recorded into the caller's graph: the passes' kernels themselves (the buffers must
         // already hold n_columns: a capture cannot allocate them).
-        OB_REQUIRE(n_columns <= F->cap_k, "ob_chol_solve_in_place: %d columns not prepared before "
+        OB_REQUIRE(n_columns <= W.cap_k, "ob_chol_solve_in_place: %d columns not prepared before "
                    "capture (ob_chol_work first)", n_columns);
-        return triangular_solves(F, even_columns(n_columns), stream);
+        return triangular_solves(F, W, even_columns(n_columns), stream);
     }
-    int st = ensure_work(F, n_columns, stream);
+    int st = ensure_work(F, W, n_columns, stream);
     if (st) return st;
     Factor::Recorded* g = nullptr;
-    st = solve_graph(F, n_columns, -1, nullptr, nullptr, nullptr, &g);
+    st = solve_graph(F, W, n_columns, -1, nullptr, nullptr, nullptr, &g);
     if (st) return st;
     OB_CUDA(cudaGraphLaunch(g->exec, stream));
     count_launch((uint64_t)g->launches);
@@ -1519,10 +1540,11 @@ int ob_chol_buffers(void* factor, int n_columns, double** rhs, double** solution
                     ob_stream_t stream_) {
     OB_REQUIRE(factor && rhs && solution && n_columns >= 1, "ob_chol_buffers: bad argument");
     Factor* F = static_cast<Factor*>(factor);
-    int st = ensure_work(F, n_columns, as_stream(stream_));
+    Factor::WorkSet& W = F->sets[0];
+    int st = ensure_work(F, W, n_columns, as_stream(stream_));
     if (st) return st;
-    *rhs = F->RHS;
-    *solution = F->SOL;
+    *rhs = W.RHS;
+    *solution = W.SOL;
     return OB_OK;
 }
 
@@ -1530,14 +1552,15 @@ int ob_chol_time_solve(void* factor, int n_columns, int reps, float* ms, ob_stre
     cudaStream_t stream = as_stream(stream_);
     OB_REQUIRE(factor && ms && reps >= 1 && n_columns >= 1, "ob_chol_time_solve: bad argument");
     Factor* F = static_cast<Factor*>(factor);
-    int st = ensure_work(F, n_columns, stream);
+    Factor::WorkSet& W = F->sets[0];
+    int st = ensure_work(F, W, n_columns, stream);
     if (st) return st;
     cudaEvent_t start, end;
     OB_CUDA(cudaEventCreate(&start));
     OB_CUDA(cudaEventCreate(&end));
     cudaEventRecord(start, stream);
     for (int i = 0; i < reps && st == OB_OK; ++i)
-        st = triangular_solves(F, even_columns(n_columns), stream);
+        st = triangular_solves(F, W, even_columns(n_columns), stream);
     cudaEventRecord(end, stream);
     cudaError_t e = cudaEventSynchronize(end);
     float total = 0.0f;
@@ -1551,8 +1574,12 @@ int ob_chol_time_solve(void* factor, int n_columns, int reps, float* ms, ob_stre
 }
 
 int ob_chol_work_generation(void* factor, long long* generation) {
-    OB_REQUIRE(factor && generation, "ob_chol_work_generation: bad argument");
-    *generation = static_cast<Factor*>(factor)->generation;
+    return ob_chol_work_generation_set(factor, 0, generation);
+}
+
+int ob_chol_work_generation_set(void* factor, int set, long long* generation) {
+    OB_REQUIRE(factor && generation && set >= 0 && set < kWorkSets, "ob_chol_work_generation: bad argument");
+    *generation = static_cast<Factor*>(factor)->sets[set].generation;
     return OB_OK;
 }
 

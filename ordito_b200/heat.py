@@ -504,7 +504,7 @@ def _batch_multigrid(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offs
 
 def _batch_columns(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offsets: DeviceArray,
                    k: int, refine: int, transpose: bool, *, stream: Any = None,
-                   out: DeviceArray | None = None) -> DeviceArray:
+                   out: DeviceArray | None = None, work_set: int = 0) -> DeviceArray:
     """The batched pass over resident, validated source columns.
 
     Without refinement the pass stays in the factors' shared ordering from the seeds to the shift:
@@ -522,20 +522,20 @@ def _batch_columns(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offset
     heat_factor, poisson_factor = solver.heat_factor, solver.poisson_factor
     if refine == 0:
         st = stream if stream is not None else DEFAULT_STREAM
-        h_rhs, h_sol, h_stride, h_iperm, h_pinned = heat_factor.work(k, st)
-        p_rhs, p_sol, p_stride, p_iperm, p_pinned = poisson_factor.work(k, st)
+        h_rhs, h_sol, h_stride, h_iperm, h_pinned = heat_factor.work(k, st, work_set)
+        p_rhs, p_sol, p_stride, p_iperm, p_pinned = poisson_factor.work(k, st, work_set)
         _lib.call("ob_seed_permuted", src.ptr, offsets.ptr, k, n, h_iperm, h_pinned, h_stride,
                   h_rhs, st)
-        heat_factor.solve_in_place(k, st)
+        heat_factor.solve_in_place(k, st, work_set)
         _divergence(mesh, solver, k, h_sol, h_stride, h_iperm, p_rhs, p_stride, p_iperm, p_pinned, st)
-        poisson_factor.solve_in_place(k, st)
+        poisson_factor.solve_in_place(k, st, work_set)
         if out is None:
             out = DeviceArray.empty((k, n), np.float64)
         _lib.call("ob_shift_permuted", p_sol, n, p_stride, p_iperm, src.ptr, offsets.ptr, k, 1,
                   out.ptr, st)
         return out if transpose else _transposed(out, k, n)
-    if stream is not None or out is not None:
-        raise ValueError("_batch_columns: stream/out serve the refinement-free pass only")
+    if stream is not None or out is not None or work_set != 0:
+        raise ValueError("_batch_columns: stream/out/work_set serve the refinement-free pass only")
     heat_rhs, heat_sol = heat_factor.buffers(k)
     poisson_rhs, phi = poisson_factor.buffers(k)
     invalid = solver.scratch_flag()
@@ -581,17 +581,19 @@ class BatchStep:
 
     def __init__(self, mesh: Trimesh, solver: "HeatSolver", sources: DeviceArray,
                  offsets: DeviceArray, k: int, out: DeviceArray, stream: Any, *,
-                 warm: bool = True) -> None:
+                 warm: bool = True, work_set: int = 0) -> None:
         self.stream = stream
         self.k = k
         self.out = out
+        self.work_set = work_set
         self._args = (mesh, solver, sources, offsets)
         self.handle = None
         self._record(warm)
 
     def _generations(self) -> tuple[int, int]:
         solver = self._args[1]
-        return solver.heat_factor.generation, solver.poisson_factor.generation
+        return (solver.heat_factor.work_generation(self.work_set),
+                solver.poisson_factor.work_generation(self.work_set))
 
     def _record(self, warm: bool = True) -> None:
         import ctypes  # noqa: PLC0415
@@ -603,14 +605,16 @@ class BatchStep:
             # One eager pass prepares what the recording must find ready (the factors' buffers,
             # the per-face terms, the corner index); skipped when a wider step already did.
             _lib.call("ob_device_synchronize")  # buffers allocated on other streams are ready
-            _batch_columns(mesh, solver, sources, offsets, k, 0, True, stream=stream, out=out)
+            _batch_columns(mesh, solver, sources, offsets, k, 0, True, stream=stream, out=out,
+                           work_set=self.work_set)
             _lib.call("ob_stream_synchronize", stream)
         self._recorded = self._generations()
         with capture_guard():
             _lib.call("ob_capture_begin", stream)
             error: BaseException | None = None
             try:
-                _batch_columns(mesh, solver, sources, offsets, k, 0, True, stream=stream, out=out)
+                _batch_columns(mesh, solver, sources, offsets, k, 0, True, stream=stream, out=out,
+                               work_set=self.work_set)
             except BaseException as exc:  # noqa: BLE001 -- the capture must be closed first
                 error = exc
             handle, kernels = ctypes.c_void_p(0), ctypes.c_int(0)
@@ -645,9 +649,10 @@ class BatchStep:
 
 
 class BatchPipeline:
-    """A stream of batches on one resident mesh, host arrays out, pipelined: the recorded pass of
-    batch i + 1 (``BatchStep``) runs while batch i's distances are copied to pinned host memory on
-    a second stream (two output buffers, ordered by events).
+    """A stream of batches on one resident mesh, host arrays out, pipelined: consecutive batches
+    run on the factors' two work sets, each on its own stream (``BatchStep``), so batch i + 1's
+    pass overlaps batch i's pass and its copy of the distances to pinned host memory (a third
+    stream; ordered by events).
 
     ``map(batches)`` yields, in order, each batch's ``(k, V)`` float64 distances as a view of a
     pinned host buffer, valid until the generator has advanced twice more (copy it to keep it).
@@ -665,21 +670,23 @@ class BatchPipeline:
         n = mesh.n_vertices
         self.n, self.k = n, k
         capacity = max(max_sources, 4 * k)
-        self.compute, self.copy = ctypes.c_void_p(0), ctypes.c_void_p(0)
-        _lib.call("ob_stream_create", ctypes.byref(self.compute))
+        self.copy = ctypes.c_void_p(0)
         _lib.call("ob_stream_create", ctypes.byref(self.copy))
         self.capacity = capacity
         self.slots = []
-        for _ in range(2):
+        for work_set in range(2):
+            compute = ctypes.c_void_p(0)
+            _lib.call("ob_stream_create", ctypes.byref(compute))
             src = DeviceArray.from_host(np.zeros(capacity, dtype=np.int32))
             off = DeviceArray.from_host(np.arange(k + 1, dtype=np.int32))
             out = DeviceArray.empty((k, n), np.float64)
-            step = BatchStep(mesh, solver, src, off, k, out, self.compute)
+            step = BatchStep(mesh, solver, src, off, k, out, compute, work_set=work_set)
             events = [ctypes.c_void_p(0), ctypes.c_void_p(0)]
             for e in events:
                 _lib.call("ob_event_create", ctypes.byref(e))
             self.slots.append({
-                "src": src, "off": off, "step": step, "host": PinnedArray((k, n), np.float64),
+                "compute": compute, "src": src, "off": off, "step": step,
+                "host": PinnedArray((k, n), np.float64),
                 "h_src": PinnedArray(capacity, np.int32), "h_off": PinnedArray(k + 1, np.int32),
                 "computed": events[0], "copied": events[1], "busy": False,
             })
@@ -701,10 +708,11 @@ class BatchPipeline:
         slot["h_src"].array[:total] = flat
         slot["h_off"].array[0] = 0
         np.cumsum(sizes, out=slot["h_off"].array[1:])
-        _lib.call("ob_memcpy", slot["src"].ptr, slot["h_src"].ptr, 4 * total, 0, self.compute, 0)
-        _lib.call("ob_memcpy", slot["off"].ptr, slot["h_off"].ptr, 4 * (self.k + 1), 0, self.compute, 0)
-        slot["step"].launch(self.compute)
-        _lib.call("ob_event_record", slot["computed"], self.compute)
+        compute = slot["compute"]
+        _lib.call("ob_memcpy", slot["src"].ptr, slot["h_src"].ptr, 4 * total, 0, compute, 0)
+        _lib.call("ob_memcpy", slot["off"].ptr, slot["h_off"].ptr, 4 * (self.k + 1), 0, compute, 0)
+        slot["step"].launch(compute)
+        _lib.call("ob_event_record", slot["computed"], compute)
         _lib.call("ob_stream_wait_event", self.copy, slot["computed"])
         _lib.call("ob_memcpy", slot["host"].ptr, slot["step"].out.ptr, 8 * self.k * self.n, 1, self.copy, 0)
         _lib.call("ob_event_record", slot["copied"], self.copy)
@@ -724,14 +732,17 @@ class BatchPipeline:
             yield pending["host"].array
 
     def close(self) -> None:
+        streams = [self.copy] + [slot["compute"] for slot in self.slots]
+        for stream in streams:
+            if stream.value:
+                _lib.lib.ob_stream_synchronize(stream)
         for slot in self.slots:
             slot["step"].close()
             for e in ("computed", "copied"):
                 _lib.lib.ob_event_destroy(slot[e])
         self.slots = []
-        for stream in (self.compute, self.copy):
+        for stream in streams:
             if stream.value:
-                _lib.lib.ob_stream_synchronize(stream)
                 _lib.lib.ob_stream_destroy(stream)
                 stream.value = None
 

@@ -238,3 +238,36 @@ def test_batch_pipeline_matches_the_batched_pass(gpu) -> None:
         assert hp.relative_linf(got, expected) <= 1e-12
     with pytest.raises(ValueError):
         list(gheat.BatchPipeline(mesh, 2).map([[[0], [n]]]))
+
+
+def test_two_work_sets_give_the_same_answers(gpu) -> None:
+    import ctypes
+
+    from ordito_b200 import _lib
+
+    v, f = meshes.small_torus()
+    n = v.shape[0]
+    rng = np.random.default_rng(11)
+    sets = [rng.choice(n, size=2, replace=False).tolist() for _ in range(9)]
+    mesh = Trimesh(v, f.reshape(-1))
+    solver = mesh.heat_solver(None, method="meshlab")
+    assert solver.factor()
+    src, offsets, k = gheat._source_columns(sets, n)
+    streams = [ctypes.c_void_p(0), ctypes.c_void_p(0)]
+    for s in streams:
+        _lib.call("ob_stream_create", ctypes.byref(s))
+    steps = [gheat.BatchStep(mesh, solver, src, offsets, k, DeviceArray.empty((k, n), np.float64),
+                             streams[w], work_set=w) for w in range(2)]
+    for _ in range(3):  # both sets in flight at once
+        for w in range(2):
+            steps[w].launch(streams[w])
+    for s in streams:
+        _lib.call("ob_stream_synchronize", s)
+    a, b = steps[0].out.numpy(), steps[1].out.numpy()
+    assert hp.relative_linf(a, b) <= 1e-12
+    expected = gheat._batch_columns(mesh, solver, src, offsets, k, 0, True).numpy()
+    assert hp.relative_linf(a, expected) <= 1e-12
+    for step in steps:
+        step.close()
+    for s in streams:
+        _lib.call("ob_stream_destroy", s)
