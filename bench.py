@@ -49,6 +49,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--cols", type=int, default=512)
     p.add_argument("--rows", type=int, default=256)
     p.add_argument("--refine", type=int, default=0)
+    p.add_argument("--in-flight", type=int, default=3, choices=[1, 2, 3])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-precision", action="store_true")
@@ -530,20 +531,22 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     _lib.call("ob_stream_create", ctypes.byref(stream))
     in_flight = 1
     if args.refine == 0:
-        # Two batches in flight: the factors' two work sets, each pass recorded on its own stream,
-        # consecutive steps alternating between them (a served stream of batches).
-        second = ctypes.c_void_p(0)
-        _lib.call("ob_stream_create", ctypes.byref(second))
-        streams = [stream, second]
+        # Several batches in flight: the factors' work sets, each pass recorded on its own stream,
+        # consecutive steps taking them in turn (a served stream of batches).
+        in_flight = args.in_flight
+        streams = [stream]
+        for _ in range(in_flight - 1):
+            extra = ctypes.c_void_p(0)
+            _lib.call("ob_stream_create", ctypes.byref(extra))
+            streams.append(extra)
         graph_steps = [gheat.BatchStep(mesh, solver, src, offsets, k,
                                        DeviceArray.empty((k, n), np.float64), streams[w], work_set=w)
-                       for w in range(2)]
+                       for w in range(in_flight)]
         turn = [0]
-        in_flight = 2
 
         def step():
             w = turn[0]
-            turn[0] ^= 1
+            turn[0] = (w + 1) % in_flight
             return graph_steps[w].launch(streams[w])
     else:
         stream = ctypes.c_void_p(0)  # the eager pass runs on the default stream
@@ -575,21 +578,21 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     launches0 = _lib.launch_count()
     with Clocks(dist.local_rank) as clocks:
         _lib.call("ob_event_record", start, stream)
-        if in_flight == 2:
-            _lib.call("ob_stream_wait_event", second, start)
+        for other in streams[1:] if in_flight > 1 else []:
+            _lib.call("ob_stream_wait_event", other, start)
         for _ in range(args.steps):
             out = step()
-        if in_flight == 2:
+        for other in streams[1:] if in_flight > 1 else []:
             joined = ctypes.c_void_p(0)
             _lib.call("ob_event_create", ctypes.byref(joined))
-            _lib.call("ob_event_record", joined, second)
+            _lib.call("ob_event_record", joined, other)
             _lib.call("ob_stream_wait_event", stream, joined)
         _lib.call("ob_event_record", end, stream)
         synchronize()
     launches = (_lib.launch_count() - launches0) // max(args.steps, 1)
     ms = _elapsed(start, end) / args.steps
     single_ms = None
-    if in_flight == 2:
+    if in_flight > 1:
         # The same steps one at a time (one stream, one work set), for the record.
         synchronize()
         _lib.call("ob_event_record", start, stream)

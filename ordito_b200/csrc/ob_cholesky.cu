@@ -440,7 +440,7 @@ struct Tile {
 };
 
 constexpr int kTileRows = 64;   // output rows per tile
-constexpr int kWorkSets = 2;    // independent work-buffer sets a factor holds
+constexpr int kWorkSets = 3;    // independent work-buffer sets a factor holds
 constexpr int kTileCols = 64;   // right-hand-side columns per tile
 // Inner-dimension step staged in shared memory. 16 (two stages, 39 KB, 4 CTAs per SM) measured
 // 0.82 ms a pass on the 131k torus at 64 columns, against 1.11 ms for 32 (74 KB, 3 CTAs per SM).
