@@ -7,9 +7,9 @@ queries on the resident mesh -- the served + batched path: the mesh's operators 
 factors stay on the device, and the 64 queries run as one batched pass in the factors' ordering
 (seeding, the two float64 factored solves over 64 right-hand sides, the gathered divergence and the
 shift; ``--refine 1`` adds a float64 refinement step to each solve).
-``value`` is whole-job solves/s with the sources resident on the device; ``e2e`` is the same stream
-through the public API (``heat_geodesic_batch``) from host source lists to host distances, copies
-included. The plain drop-in (``heat_geodesic(vertices, faces, [s])``: assembly, solves and any
+``value`` is whole-job solves/s with the sources resident on the device, three batches in flight
+on three streams; ``e2e`` is the same stream through the public API (``heat.BatchPipeline``) from
+host source lists to pinned host distances, copies included. The plain drop-in (``heat_geodesic(vertices, faces, [s])``: assembly, solves and any
 factorisation inside every call) and the resident single query are timed beside it. A sample of
 the answers is checked against the float64 CPU oracle on every run.
 
@@ -57,6 +57,9 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-reference-benchmarks", action="store_true")
     p.add_argument("--no-large-mesh", action="store_true")
     p.add_argument("--no-packed", action="store_true")
+    p.add_argument("--no-kernel-rooflines", action="store_true")
+    # Only the per-kernel rooflines, on icosphere(LEVEL) with 1 % radial noise (a profiling case).
+    p.add_argument("--kernels-only", type=int, default=0, metavar="LEVEL")
     p.add_argument("--serving-requests", type=int, default=300)
     p.add_argument("--serving-warmup", type=int, default=150)
     p.add_argument("--serving-rate", type=float, default=40.0)
@@ -341,7 +344,149 @@ def run_reference_benchmarks() -> dict:
     return out
 
 
-def run_large_mesh() -> dict:
+def kernel_rooflines(mesh, solver, columns: int = 64, reps: int = 10) -> dict:
+    """Each kernel family of the path launched alone on this mesh, timed with CUDA events over
+    ``reps`` launches after one warm-up: achieved = algorithmic bytes (every input read and every
+    output written once, named per kernel) / average launch time, against the measured HBM copy
+    peak. Multi-column kernels run ``columns`` right-hand sides."""
+    from ordito_b200 import _lib
+    from ordito_b200.device import DeviceArray, synchronize
+
+    peak = _peaks()["hbm_gbs"]
+    n, f = mesh.n_vertices, mesh.n_faces
+    pattern = mesh.mesh_operator_pattern
+    terms_face = mesh.face_terms
+    ops = solver.operators
+    nnz = ops.heat_system.nnz
+    count = pattern.n_keys
+    start, end = _events()
+    out: dict = {"mesh": {"vertices": n, "faces": f, "stored_entries": nnz}, "columns": columns,
+                 "peak_gbs": peak, "kernels": {}}
+
+    def timed(name: str, nbytes: int, launch, what: str, launches: int = 1) -> None:
+        launch()
+        synchronize()
+        _lib.call("ob_event_record", start, None)
+        for _ in range(reps):
+            launch()
+        _lib.call("ob_event_record", end, None)
+        ms = _elapsed(start, end) / reps
+        record(name, ms, nbytes, what, launches)
+
+    def record(name: str, ms: float, nbytes: int, what: str, launches: int = 1) -> None:
+        gbs = nbytes / (ms / 1e3) / 1e9
+        out["kernels"][name] = {"ms": ms, "algorithmic_bytes": int(nbytes), "achieved_gbs": gbs,
+                                "frac": gbs / peak, "launches": launches, "bytes": what}
+
+    # a1: the pattern build (key kernel, radix sort, run flags, scan, placement).
+    offsets = DeviceArray.empty(n + 1, np.int32)
+    cols = DeviceArray.empty(count, np.int32)
+    run_start = DeviceArray.empty(count, np.int32)
+    keys = DeviceArray.empty(count, np.uint64)
+    order = DeviceArray.empty(count, np.int32)
+    size = ctypes.c_size_t(0)
+    _lib.call("ob_pattern_workspace", n, f, ctypes.byref(size))
+    workspace = DeviceArray.empty(int(size.value), np.uint8)
+    timed("pattern_build", 12 * f + 4 * (n + 1) + 20 * count,
+          lambda: _lib.call("ob_pattern_build", mesh.faces.ptr, f, n, offsets.ptr, cols.ptr,
+                            run_start.ptr, keys.ptr, order.ptr, workspace.ptr, int(size.value), None),
+          "faces in; offsets, columns, run starts, sorted keys and corner order out (the radix "
+          "sort's own passes are not counted)")
+    del offsets, cols, run_start, keys, order, workspace
+
+    # a2/a3: per-face cot table, normals, areas and the float64 corner sums.
+    cot = DeviceArray.empty(3 * f, np.float32)
+    normals = DeviceArray.empty(3 * f, np.float32)
+    areas = DeviceArray.empty(f, np.float32)
+    area_sums = DeviceArray.empty(n, np.float64)
+    timed("face_terms", 12 * n + 12 * f + 28 * f + 8 * n,
+          lambda: _lib.call("ob_face_terms", mesh.vertices.ptr, mesh.faces.ptr, f, n, cot.ptr,
+                            normals.ptr, areas.ptr, area_sums.ptr, None),
+          "positions and faces in; cot table, normals, areas and corner sums out")
+
+    # a5: the operator rows L, H, P and the lumped mass.
+    values = DeviceArray.empty(3 * count, np.float64)
+    mass = DeviceArray.empty(n, np.float64)
+    edge_sums = DeviceArray.empty(2, np.float64)
+    _lib.call("ob_edge_sums", pattern.offsets.ptr, pattern.columns.ptr, pattern.run_start.ptr,
+              pattern.keys.ptr, count, n, mesh.vertices.ptr, 1, edge_sums.ptr, None)
+    timed("heat_rows", 4 * (n + 1) + 8 * nnz + 16 * count + 12 * f + 8 * n + 24 * nnz + 8 * n,
+          lambda: _lib.call("ob_heat_rows", pattern.offsets.ptr, pattern.columns.ptr,
+                            pattern.run_start.ptr, pattern.keys.ptr, count, pattern.order.ptr, n,
+                            terms_face.cot.ptr, -1.0, edge_sums.ptr, 1, terms_face.area_sums.ptr,
+                            3.0, values.ptr, values.ptr + 8 * count, values.ptr + 16 * count,
+                            mass.ptr, None),
+          "pattern (offsets, columns, run starts, keys, corner order), cot table and corner sums "
+          "in; L, H, P values and mass out")
+    del values, mass, cot, normals, areas, area_sums
+
+    # a7/a9: the CG round's first node (y = A u and three column dots), float64 and float32 values.
+    H = ops.heat_system
+    for narrow in (0, 1):
+        handle = ctypes.c_void_p(0)
+        _lib.call("ob_pcg_create", n, H.offsets.ptr, H.columns.ptr, H.values.ptr, 1, 1, narrow,
+                  ctypes.byref(handle), None)
+        ms = ctypes.c_float(0.0)
+        _lib.call("ob_pcg_time_matvec", handle, 1, ctypes.byref(ms), None)
+        _lib.call("ob_pcg_time_matvec", handle, reps, ctypes.byref(ms), None)
+        _lib.lib.ob_pcg_destroy(handle)
+        record("pcg_matvec_dots_" + ("f32_values" if narrow else "f64"), ms.value,
+               4 * (n + 1) + (8 if narrow else 12) * nnz + 3 * 8 * n,
+               "offsets, columns and values once, u, r in and w out (float64), one column")
+
+    # a10: the V-cycle kernels of the Poisson hierarchy on `columns` float32 columns.
+    amg = solver.poisson_multigrid
+    if not amg.is_jacobi:
+        ms = (ctypes.c_float * 5)()
+        nbytes = (ctypes.c_longlong * 5)()
+        _lib.call("ob_amg_time_kernels", amg.handle, columns, reps, ms, nbytes, None)
+        for i, name in enumerate(("amg_sweep", "amg_residual", "amg_restrict", "amg_prolong")):
+            record(name, ms[i], nbytes[i], "finest level: offsets, columns, float32 values and "
+                   "every vector row once (float32, the columns padded to a power of two)")
+        out["amg_vcycle_ms"] = ms[4]
+        out["amg_levels"] = amg.grid
+
+    # a8: the divergence from the per-face terms, `columns` fields in and out (float64).
+    terms = solver.gradient_terms
+    corner_offsets, corner_slots = mesh.corner_index
+    u = DeviceArray.empty(n * columns, np.float64)
+    _lib.call("ob_memset", u.ptr, 0, 8 * n * columns, None)
+    div = DeviceArray.empty(n * columns, np.float64)
+    timed("grad_div_terms", 144 * f + 12 * f + 4 * (n + 1) + 12 * f + 2 * 8 * n * columns,
+          lambda: _lib.call("ob_grad_div_terms", terms.ptr, mesh.faces.ptr, corner_offsets.ptr,
+                            corner_slots.ptr, n, columns, u.ptr, columns, None, div.ptr, columns,
+                            None, None, None),
+          "per-face terms, faces and corner index in, u in and -div out (float64)")
+
+    # a13: the shift of `columns` fields to their sources, written transposed.
+    sources = DeviceArray.from_host(np.arange(columns, dtype=np.int32) * (n // columns))
+    source_offsets = DeviceArray.from_host(np.arange(columns + 1, dtype=np.int32))
+    iperm = DeviceArray.from_host(np.arange(n, dtype=np.int32))
+    timed("shift", 4 * n + 2 * 8 * n * columns,
+          lambda: _lib.call("ob_shift_permuted", u.ptr, n, columns, iperm.ptr, sources.ptr,
+                            source_offsets.ptr, columns, 1, div.ptr, None),
+          "phi in (float64, once), the numbering in, the shifted fields out", launches=2)
+    synchronize()
+    _lib.call("ob_event_destroy", start)
+    _lib.call("ob_event_destroy", end)
+    return out
+
+
+def run_kernels_only(level: int) -> None:
+    """The per-kernel rooflines alone on icosphere(level) with 1 % radial noise (seed 0)."""
+    from ordito_b200 import creation
+    from ordito_b200.mesh import Trimesh
+
+    v, f = creation.icosphere(level)
+    mesh = Trimesh(creation.radial_noise(v, 0.01, 0), f.reshape(-1))
+    solver = mesh.heat_solver(None, method="meshlab")
+    result = kernel_rooflines(mesh, solver, reps=3)
+    result["workload"] = f"icosphere({level}) + 1 % radial noise"
+    print(json.dumps(result), flush=True)
+    mesh.dispose()
+
+
+def run_large_mesh(with_rooflines: bool = True) -> tuple[dict, dict | None]:
     """The large single mesh: icosphere(9) (2 621 442 vertices) with 1 % seeded radial noise, 8
     uniform sources, one query at a time on the resident mesh. Its factors (9.7 GB each) are over
     the factorisation budget, so the heat solve is the settled CG with the band march behind it
@@ -372,6 +517,7 @@ def run_large_mesh() -> dict:
         gheat.heat_geodesic(mesh, np.array([s], dtype=np.int32), method="meshlab").numpy()
         times.append(time.perf_counter() - t1)
     grid = solver.poisson_multigrid.grid if getattr(solver, "_poisson_multigrid", None) else None
+    rooflines = kernel_rooflines(mesh, solver) if with_rooflines else None
     mesh.dispose()
     # The same path on icosphere(6), checked against the oracle.
     budget = gchol.CHOLESKY_MEMORY_BUDGET
@@ -397,7 +543,7 @@ def run_large_mesh() -> dict:
         "path": "settled CG (float32 values) + backward-error check + band march (float64) for "
                 "the heat system; float32 CG + V-cycle inside float64 refinement (1e-8) for -L",
         "max_rel_linf_vs_fp64_oracle_same_path_ico6": check,
-    }
+    }, rooflines
 
 
 def run_packed() -> dict:
@@ -719,10 +865,10 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
             packed = run_packed()
         except Exception as exc:  # noqa: BLE001 -- reported on the line, not fatal to it
             packed = {"error": f"{type(exc).__name__}: {exc}"}
-    large_mesh = None
+    large_mesh = rooflines = None
     if not args.no_large_mesh and dist.world == 1:
         try:
-            large_mesh = run_large_mesh()
+            large_mesh, rooflines = run_large_mesh(not args.no_kernel_rooflines)
         except Exception as exc:  # noqa: BLE001 -- reported on the line, not fatal to it
             large_mesh = {"error": f"{type(exc).__name__}: {exc}"}
 
@@ -779,6 +925,7 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
             "reference_benchmarks": reference_benchmarks,
             "large_mesh": large_mesh,
             "packed": packed,
+            "kernel_rooflines": rooflines,
             "roofline": {
                 "bound": "hbm",
                 "kernel": "tile_product_kernel (Cholesky forward+backward pass, 64 columns)",
@@ -818,7 +965,9 @@ def main() -> None:
     args = parse()
     dist = Dist()
     try:
-        if args.impl == "reference":
+        if args.kernels_only:
+            run_kernels_only(args.kernels_only)
+        elif args.impl == "reference":
             run_reference(args, dist)
         else:
             run_b200(args, dist)

@@ -271,14 +271,11 @@ int ob_chol_buffers(void* factor, int n_columns, double** rhs, double** solution
  * solution (X) hold row i of the factor's ordering at i * stride (stride = n_columns rounded up
  * to even; a pad column must be zero), iperm maps a vertex to its row, pinned marks the rows
  * whose right-hand side must be zero. ob_chol_solve_in_place: X = A^-1 B in that numbering (no
- * permutation, no refinement), recorded once per n_columns as a CUDA graph. B is consumed. */
+ * permutation, no refinement), recorded once per n_columns as a CUDA graph. B is consumed. The
+ * solution pointer depends on the stride: use the pointers of the n_columns the solve is given. */
 int ob_chol_work(void* factor, int n_columns, double** rhs, double** solution, int* stride,
                  const int32_t** iperm, const char** pinned, ob_stream_t stream);
 int ob_chol_solve_in_place(void* factor, int n_columns, ob_stream_t stream);
-/* The device status word of the factor's persistent passes (0, or OB_ERR_TIMEOUT when a bounded
- * grid-barrier wait gave up -- the pass's results are then invalid), read back and cleared;
- * *persistent = the cooperative grid size the passes use (0: a launch per phase). */
-int ob_chol_check(void* factor, int* status, int* persistent, ob_stream_t stream);
 
 /* ---- the served batch's per-query kernels (ordito_b200/csrc/ob_served.cu) ------------------
  * ob_corner_index: each vertex's corner slots (3 f + e) in ascending order -- a stable sort of
@@ -362,7 +359,14 @@ int ob_chol_work_generation_set(void* factor, int set, long long* generation);
  * statuses (OB_STATUS_CONVERGED, _CAPPED or _NONFINITE). Any pointer among the three may be NULL.
  *
  * ob_amg_host_setup builds the same hierarchy from host arrays and reports its level shape
- * (no device needed). */
+ * (no device needed).
+ *
+ * ob_amg_time_kernels (measurement; no counterpart in the reference): the finest level's V-cycle
+ * kernels on k float32 columns (zeroed inputs), each launched reps times after one warm-up and
+ * timed with CUDA events on stream: ms[0..4] = average milliseconds of a damped-Jacobi sweep,
+ * the residual, the restriction product, the prolongation product (accumulating) and one whole
+ * V-cycle; bytes[0..3] = each kernel's algorithmic bytes (every stored entry, offset and vector
+ * row read or written once; bytes[4] = 0). Needs a hierarchy of two levels or more. */
 int ob_amg_setup(int n, const int32_t* offsets, const int32_t* columns, const double* values,
                  unsigned seed, void** amg, ob_stream_t stream);
 int ob_amg_destroy(void* amg);
@@ -374,6 +378,7 @@ int ob_amg_solve(void* amg, const double* b, double* x, int k, int ld, double to
                  int* statuses, ob_stream_t stream);
 int ob_amg_host_setup(int n, const int32_t* offsets, const int32_t* columns, const double* values,
                       unsigned seed, long long* rows, long long* nnz, int capacity, int* levels);
+int ob_amg_time_kernels(void* amg, int k, int reps, float* ms, long long* bytes, ob_stream_t stream);
 
 /* ---- Packed meshes: many meshes solved as one block-diagonal system -------------------------
  * The batched form of ordito.heat.heat_geodesic over many meshes at once: the meshes' vertices

@@ -101,7 +101,6 @@ SIGNATURES: dict[str, list] = {
     "ob_chol_work": [P, I, POINTER(c_void_p), POINTER(c_void_p), POINTER(c_int), POINTER(c_void_p),
                      POINTER(c_void_p), P],
     "ob_chol_solve_in_place": [P, I, P],
-    "ob_chol_check": [P, POINTER(c_int), POINTER(c_int), P],
     "ob_corner_index_workspace": [I, I, POINTER(c_size_t)],
     "ob_corner_index": [P, I, I, P, P, P, c_size_t, P],
     "ob_grad_div_gather": [P, P, P, P, P, P, P, I, I, P, I, P, P, I, P, P, P],
@@ -124,6 +123,7 @@ SIGNATURES: dict[str, list] = {
     "ob_amg_destroy": [P],
     "ob_amg_info": [P, POINTER(ctypes.c_longlong)],
     "ob_amg_levels": [P, POINTER(ctypes.c_longlong), POINTER(ctypes.c_longlong), I],
+    "ob_amg_time_kernels": [P, I, I, POINTER(ctypes.c_float), POINTER(ctypes.c_longlong), P],
     "ob_amg_apply": [P, P, P, I, I, P],
     "ob_amg_solve": [P, P, P, I, I, D, I, I, D, P, P, P, P],
     "ob_amg_host_setup": [I, P, P, P, ctypes.c_uint, POINTER(ctypes.c_longlong),

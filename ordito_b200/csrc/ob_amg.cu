@@ -611,6 +611,7 @@ struct DeviceLevel {
     float* val = nullptr;
     float* damped = nullptr;
     int n_coarse = 0;
+    long long pnnz = 0, rnnz = 0;  // stored entries of the prolongation and the restriction
     int *poff = nullptr, *pcol = nullptr, *roff = nullptr, *rcol = nullptr;
     float *pval = nullptr, *rval = nullptr;
 };
@@ -1486,6 +1487,8 @@ int ob_amg_setup(int n, const int32_t* offsets, const int32_t* columns, const do
         if ((st = upload(M.get(), narrow(h.A.val), &d.val, stream))) break;
         if (!h.damped.empty()) {
             d.n_coarse = h.P.cols;
+            d.pnnz = h.P.nnz();
+            d.rnnz = h.R.nnz();
             if ((st = upload(M.get(), narrow(h.damped), &d.damped, stream))) break;
             if ((st = upload(M.get(), h.P.off, &d.poff, stream))) break;
             if ((st = upload(M.get(), h.P.col, &d.pcol, stream))) break;
@@ -1548,6 +1551,83 @@ int ob_amg_levels(void* amg, long long* rows, long long* nnz, int capacity) {
         rows[l] = M->levels[l].n;
         nnz[l] = M->levels[l].nnz;
     }
+    return OB_OK;
+}
+
+int ob_amg_time_kernels(void* amg, int k, int reps, float* ms, long long* bytes, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(amg && ms && bytes && reps >= 1 && k >= 1 && k <= kMaxColumns, "ob_amg_time_kernels: bad argument");
+    Amg* M = static_cast<Amg*>(amg);
+    OB_REQUIRE(M->usable && M->levels.size() >= 2, "ob_amg_time_kernels: no multigrid hierarchy");
+    std::lock_guard<std::mutex> guard(M->lock);
+    const int kp = padded_columns(k);
+    Work* W;
+    int st = ensure_work(M, kp, &W, stream);
+    if (st) return st;
+    const DeviceLevel& L = M->levels[0];
+    const DeviceLevel& C = M->levels[1];
+    const size_t vec = sizeof(float) * (size_t)L.n * kp, coarse = sizeof(float) * (size_t)C.n * kp;
+    // Defined inputs (zeros) for every vector the timed kernels read.
+    OB_CUDA(cudaMemsetAsync(W->res, 0, vec, stream));
+    OB_CUDA(cudaMemsetAsync(W->y[0], 0, vec, stream));
+    OB_CUDA(cudaMemsetAsync(W->z, 0, vec, stream));
+    OB_CUDA(cudaMemsetAsync(W->r[0], 0, vec, stream));
+    OB_CUDA(cudaMemsetAsync(W->x[1], 0, coarse, stream));
+    const int G = W->G;
+    const int grid = grid_for((long long)L.n * G), coarse_grid = grid_for((long long)C.n * G);
+    auto f4p = [](const float* p) { return reinterpret_cast<const float4*>(p); };
+    auto f4m = [](float* p) { return reinterpret_cast<float4*>(p); };
+    const long long matrix = 4LL * (L.n + 1) + 8LL * L.nnz;
+    // Algorithmic bytes: each stored entry (column + value) and offset once, every vector row once.
+    bytes[0] = matrix + 4LL * L.n + 3LL * (long long)vec;                             // sweep
+    bytes[1] = matrix + 3LL * (long long)vec;                                         // residual
+    bytes[2] = 4LL * (C.n + 1) + 8LL * L.rnnz + (long long)vec + (long long)coarse;   // restriction
+    bytes[3] = 4LL * (L.n + 1) + 8LL * L.pnnz + (long long)coarse + 2LL * (long long)vec;  // prolongation
+    bytes[4] = 0;                                                                     // whole V-cycle
+    cudaEvent_t marks[6];
+    for (auto& e : marks) OB_CUDA(cudaEventCreate(&e));
+    auto kernel = [&](int which) {
+        switch (which) {
+            case 0:
+                sweep_kernel<false><<<grid, kThreads, 0, stream>>>(L.n, G, L.off, L.col, L.val, L.damped, f4p(W->res),
+                                                                    f4p(W->y[0]), f4m(W->z), nullptr, nullptr,
+                                                                    nullptr);
+                break;
+            case 1:
+                residual_kernel<<<grid, kThreads, 0, stream>>>(L.n, G, L.off, L.col, L.val, f4p(W->res),
+                                                               f4p(W->z), f4m(W->r[0]));
+                break;
+            case 2:
+                spmm_kernel<false><<<coarse_grid, kThreads, 0, stream>>>(C.n, G, L.roff, L.rcol, L.rval,
+                                                                         f4p(W->r[0]), f4m(W->b[1]));
+                break;
+            case 3:
+                spmm_kernel<true><<<grid, kThreads, 0, stream>>>(L.n, G, L.poff, L.pcol, L.pval, f4p(W->x[1]),
+                                                                 f4m(W->z));
+                break;
+            default: {
+                int launches = 0;
+                return enqueue_cycle(M, W, 0, W->res, W->z, false, stream, &launches);
+            }
+        }
+        count_launch();
+        return cudaGetLastError() == cudaSuccess ? OB_OK : fail(OB_ERR_CUDA, "ob_amg_time_kernels: launch");
+    };
+    for (int which = 0; which < 5 && st == OB_OK; ++which) st = kernel(which);  // warm-up
+    for (int which = 0; which < 5 && st == OB_OK; ++which) {
+        cudaEventRecord(marks[which], stream);
+        for (int i = 0; i < reps && st == OB_OK; ++i) st = kernel(which);
+    }
+    cudaEventRecord(marks[5], stream);
+    cudaError_t e = cudaEventSynchronize(marks[5]);
+    for (int which = 0; which < 5 && e == cudaSuccess; ++which) {
+        float total = 0.0f;
+        e = cudaEventElapsedTime(&total, marks[which], marks[which + 1]);
+        ms[which] = total / (float)reps;
+    }
+    for (auto& m : marks) cudaEventDestroy(m);
+    if (st) return st;
+    if (e != cudaSuccess) return cuda_status(e, "ob_amg_time_kernels");
     return OB_OK;
 }
 

@@ -234,7 +234,7 @@ int analyse(int n, std::vector<int> offsets, std::vector<int> columns, const flo
 
 struct HostFactor {
     std::vector<std::vector<double>> inv;     // per node: nc x nc row-major inverse of L11
-    std::vector<std::vector<double>> off;     // per node: (m - nc) x nc row-major L21
+    std::vector<std::vector<double>> off;     // per node: (m - nc) x nc row-major -L21 L11^-1
     std::vector<std::vector<double>> update;  // per node: (m - nc)^2 column-major, for the parent
     std::vector<char> pinned;                 // per new index: identity row (pinned / empty)
 };
@@ -342,11 +342,24 @@ int factor_node(const Analysis& A, const double* values, int s, bool singular, H
     std::vector<double> inv((size_t)nc * nc);
     for (int c = 0; c < nc; ++c)
         for (int i = 0; i < nc; ++i) inv[(size_t)i * nc + c] = X[(size_t)c * nc + i];
+    // The off-diagonal block the solves use, G = -L21 L11^-1 (row r: minus the row of L21 times
+    // the lower-triangular inverse): with it both of a node's products in each direction read
+    // only inputs that are final when its level starts -- forward y1 = L11^-1 b1 and b2 += G b1,
+    // backward x1 = L11^-T y1 + G^T x2 -- so a tree level is one launch a direction.
+    std::vector<double> G((size_t)noff * nc, 0.0);
+    parallel_range(noff, m >= kThreadedFront, [&](long long begin, long long end) {
+        for (int r = (int)begin; r < (int)end; ++r) {
+            double* g = G.data() + (size_t)r * nc;
+            for (int k = 0; k < nc; ++k) {
+                const double a = F[(size_t)k * m + nc + r];
+                if (a == 0.0) continue;
+                const double* row = inv.data() + (size_t)k * nc;  // inverse row k: columns 0..k
+                for (int i = 0; i <= k; ++i) g[i] -= a * row[i];
+            }
+        }
+    });
     H.inv[s] = std::move(inv);
-    std::vector<double> L21((size_t)noff * nc);
-    for (int r = 0; r < noff; ++r)
-        for (int j = 0; j < nc; ++j) L21[(size_t)r * nc + j] = F[(size_t)j * m + nc + r];
-    H.off[s] = std::move(L21);
+    H.off[s] = std::move(G);
     std::vector<double> U((size_t)noff * noff);
     for (int b = 0; b < noff; ++b)
         for (int a = b; a < noff; ++a) U[(size_t)b * noff + a] = F[(size_t)(nc + b) * m + nc + a];
@@ -445,8 +458,7 @@ constexpr int kTileCols = 64;   // right-hand-side columns per tile
 // Inner-dimension step staged in shared memory. 16 (two stages, 39 KB, 4 CTAs per SM) measured
 // 0.82 ms a pass on the 131k torus at 64 columns, against 1.11 ms for 32 (74 KB, 3 CTAs per SM).
 constexpr int kTileK = 16;
-constexpr int kSplitK = 64;       // a leaf tile's inner-dimension range at most (split beyond)
-constexpr int kSplitKUpper = 64;  // the same above the leaves (32 measured slower: more atomics)
+constexpr int kSplitK = 64;  // a split tile's inner-dimension range (32 measured slower: more atomics)
 constexpr int kTileThreads = 128;
 // Shared rows of 72 doubles: the 8 x 4 fragment loads of a warp then touch every 8-byte bank
 // pair exactly twice (the minimum for 256 bytes).
@@ -463,7 +475,7 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 
 // 16-byte asynchronous global -> shared copies; bytes < 16 zero-fills the rest (0: all zeros, and
 // the source is not read). copy16 may cache in L1 (read-only data: the factor); copy16_l2 reads
-// through L2 only, for data other CTAs of a persistent launch wrote in an earlier phase.
+// through L2 only (the work vectors, which other launches' atomics update).
 __device__ __forceinline__ void copy16(void* smem, const void* gmem, int bytes) {
     const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(gmem), "r"(bytes));
@@ -491,12 +503,11 @@ struct Stage {
 // time into shared memory with asynchronous 16-byte copies (zero-filled at the edges), two stages
 // in flight: the next step's copies overlap the current step's MMAs. The output is assigned,
 // subtracted, or added atomically per the tile's op. `k` (the column stride) is even and every
-// block row starts on 16 bytes, so every copy is aligned. Vectors are read through L2, so a
-// persistent launch sees what other CTAs wrote before its last grid barrier.
+// block row starts on 16 bytes, so every copy is aligned. `in` and `out` are the same stacked
+// work buffer: the rows a launch's tiles read are never rows any tile of that launch writes.
 __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double* __restrict__ vals,
                                              const int* __restrict__ idx,
-                                             const double* __restrict__ in, double* __restrict__ out,
-                                             int k, Stage* stage) {
+                                             const double* in, double* out, int k, Stage* stage) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;  // the warp's quadrant
     const int fr = lane >> 2, fk = lane & 3;                 // fragment coordinates
@@ -598,11 +609,10 @@ constexpr int kStageBytes = 2 * (int)sizeof(Stage);
 // One launch per phase: a CTA per (tile, column block).
 __global__ void __launch_bounds__(kTileThreads)
 tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
-                    const int* __restrict__ idx, const double* __restrict__ in,
-                    double* __restrict__ out, int k) {
+                    const int* __restrict__ idx, double* rows, int k) {
     extern __shared__ __align__(16) unsigned char shared_stages[];
     Stage* stage = reinterpret_cast<Stage*>(shared_stages);
-    tile_product(tiles[blockIdx.x], blockIdx.y * kTileCols, vals, idx, in, out, k, stage);
+    tile_product(tiles[blockIdx.x], blockIdx.y * kTileCols, vals, idx, rows, rows, k, stage);
 }
 
 // The same tile product for a narrow batch (KP = 2, 4, 6 or 8 columns, the even stride of 1-8
@@ -618,7 +628,9 @@ constexpr int kNarrowSlices = kNarrowThreads / kTileRows;
 template <int KP>
 __global__ void __launch_bounds__(kNarrowThreads)
 narrow_tile_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
-                   const int* __restrict__ idx, const double* __restrict__ in, double* __restrict__ out) {
+                   const int* __restrict__ idx, double* rows) {
+    const double* in = rows;
+    double* out = rows;
     __shared__ double other[kNarrowSlices - 1][kTileRows][KP];
     const Tile t = tiles[blockIdx.x];
     const int i = threadIdx.x % kTileRows, slice = threadIdx.x / kTileRows;
@@ -672,78 +684,6 @@ narrow_tile_kernel(const Tile* __restrict__ tiles, const double* __restrict__ va
             case kSub: o[c] = __ldcg(o + c) - v; break;
             default: atomicAdd(o + c, v); break;
         }
-    }
-}
-
-// A phase of a triangular pass: its tiles and which work buffers (0 B, 1 Y, 2 X) it reads and
-// writes.
-struct Phase {
-    const Tile* tiles;
-    int count, in, out;
-};
-
-// Grid-wide barrier of a cooperative (co-resident) launch: bar[0] counts arrivals, bar[1] is the
-// generation. Every wait is bounded: after `limit` polls (or once another CTA has given up) the
-// CTA records OB_ERR_TIMEOUT in *status and returns false, and so do the rest at their next poll.
-__device__ bool grid_barrier(unsigned int* bar, int* status, unsigned int limit) {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        ok = 1;
-        volatile unsigned int* generation = bar + 1;
-        const unsigned int seen = *generation;
-        __threadfence();
-        const unsigned int arrived = atomicAdd(bar, 1u) + 1u;
-        if (arrived == gridDim.x) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            unsigned int polls = 0;
-            while (*generation == seen) {
-                if (++polls > limit || *(volatile int*)status != 0) {
-                    atomicExch(status, OB_ERR_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return ok != 0;
-}
-
-// A whole triangular pass (forward then backward, every level) in one cooperative launch: the
-// listed rows are zeroed, then each phase's (tile, column block) pairs are spread over the
-// resident CTAs with a grid barrier between phases.
-__global__ void __launch_bounds__(kTileThreads)
-pass_kernel(const Phase* __restrict__ phases, int p_lo, int p_hi, const int2* __restrict__ zero,
-            int n_zero, const double* __restrict__ vals, const int* __restrict__ idx, double* B,
-            double* Y, double* X, int k, unsigned int* bar, int* status, unsigned int limit) {
-    extern __shared__ __align__(16) unsigned char shared_stages[];
-    Stage* stage = reinterpret_cast<Stage*>(shared_stages);
-    double* buffers[3] = {B, Y, X};
-    if (n_zero > 0) {
-        for (int z = blockIdx.x; z < n_zero; z += gridDim.x) {
-            const int2 range = zero[z];
-            const long long begin = (long long)range.x * k, end = (long long)(range.x + range.y) * k;
-            for (long long t = begin + threadIdx.x; t < end; t += blockDim.x) {
-                Y[t] = 0.0;
-                X[t] = 0.0;
-            }
-        }
-        if (!grid_barrier(bar, status, limit)) return;
-    }
-    const int column_blocks = (k + kTileCols - 1) / kTileCols;
-    for (int p = p_lo; p < p_hi; ++p) {
-        const Phase ph = phases[p];
-        const int work = ph.count * column_blocks;
-        for (int w = blockIdx.x; w < work; w += gridDim.x)
-            tile_product(ph.tiles[w / column_blocks], (w % column_blocks) * kTileCols, vals, idx,
-                         buffers[ph.in], buffers[ph.out], k, stage);
-        if (!grid_barrier(bar, status, limit)) return;
     }
 }
 
@@ -812,23 +752,14 @@ struct Factor {
     int* iperm = nullptr;    // device: old -> new
     char* pinned = nullptr;  // device
     long long n_vals = 0;
-    // Tile lists per (direction, level, phase); host copies of counts, device tile arrays.
-    std::vector<Tile*> fwd_diag, fwd_off, bwd_off, bwd_diag;
-    std::vector<int> n_fwd_diag, n_fwd_off, n_bwd_off, n_bwd_diag;
+    // Tile lists per (direction, level): host copies of counts, device tile arrays. Tiles name
+    // rows of a work set's stacked [B; Y; X] buffer (B rows 0..n-1, Y rows n.., X rows 2n..).
+    std::vector<Tile*> fwd, bwd;
+    std::vector<int> n_fwd, n_bwd;
+    int launches_per_pass = 0;
     std::vector<void*> owned;
     int2* zero = nullptr;  // row ranges split tiles accumulate into (zeroed each pass)
     int n_zero = 0;
-    // The persistent pass: the phase table, barrier words [count, generation], the status word a
-    // timed-out barrier writes, and the cooperative grid size (0: launch each phase instead).
-    Phase* phases = nullptr;
-    int n_phases = 0;
-    unsigned int* barrier = nullptr;
-    int* status = nullptr;
-    int pass_grid = 0;
-    // The hybrid pass: phases [hybrid_lo, hybrid_hi) (the tree levels from hybrid_level up, both
-    // directions) in one cooperative launch of at most hybrid_grid CTAs, the rest per phase.
-    std::vector<Phase> host_phases;
-    int hybrid_level = -1, hybrid_lo = -1, hybrid_hi = -1, hybrid_grid = 0, hybrid_tiles = 0;
     size_t bytes = 0;
     // Recorded solve graphs, keyed by (columns, refinement steps, operator arrays).
     struct Recorded {
@@ -838,13 +769,18 @@ struct Factor {
         cudaGraphExec_t exec;
         int launches;
     };
-    // A set of work buffers sized for `cap_k` columns: B, Y, X in the factor's numbering, R the
-    // residual, RHS / SOL the caller's right-hand side and solution copied in / out (old
-    // numbering), and the solve graphs recorded over them. Passes on different sets are
-    // independent and may run concurrently (each set on one stream at a time).
+    // A set of work buffers sized for `cap_k` columns: B, Y, X in the factor's numbering (three
+    // consecutive n-row blocks of one allocation, BYX), R the residual, RHS / SOL the caller's
+    // right-hand side and solution copied in / out (old numbering), and the solve graphs recorded
+    // over them. Passes on different sets are independent and may run concurrently (each set on
+    // one stream at a time).
     struct WorkSet {
         int cap_k = 0;
-        double *B = nullptr, *Y = nullptr, *X = nullptr, *R = nullptr, *RHS = nullptr, *SOL = nullptr;
+        double *BYX = nullptr, *R = nullptr, *RHS = nullptr, *SOL = nullptr;
+        // B, Y and X at the even column stride kp of a call: n rows of kp doubles each.
+        double* B() const { return BYX; }
+        double* Y(int kp, int n) const { return BYX + (size_t)n * kp; }
+        double* X(int kp, int n) const { return BYX + 2 * (size_t)n * kp; }
         // Bumped whenever the buffers are reallocated: a graph recorded outside the factor (over
         // ob_chol_work's pointers) is stale once it changes.
         long long generation = 0;
@@ -853,94 +789,6 @@ struct Factor {
     WorkSet sets[kWorkSets];
     cudaStream_t capture = nullptr;
 };
-
-__global__ void cooperative_probe_kernel(int* out) {
-    if (out != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *out = 1;
-}
-
-// Whether a cooperative launch can be recorded into a CUDA graph on this runtime (probed once: the
-// hybrid pass below is recorded inside every served pass).
-bool cooperative_recordable() {
-    static int state = -1;
-    std::lock_guard<std::recursive_mutex> guard(capture_mutex());
-    if (state >= 0) return state == 1;
-    cudaStream_t s = nullptr;
-    bool ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    if (ok) ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-    if (ok) {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(2);
-        cfg.blockDim = dim3(32);
-        cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        const bool launched = cudaLaunchKernelEx(&cfg, cooperative_probe_kernel, (int*)nullptr) == cudaSuccess;
-        const bool ended = cudaStreamEndCapture(s, &graph) == cudaSuccess;
-        ok = launched && ended && graph != nullptr &&
-             cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
-    }
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    if (s) cudaStreamDestroy(s);
-    cudaGetLastError();
-    state = ok ? 1 : 0;
-    return ok;
-}
-
-// The hybrid pass's split (Factor::hybrid_*), opt-in through OB_CHOL_HYBRID_LEVEL: from that tree
-// level ("auto": the lowest at which every phase's tiles fit one wave of the co-resident grid)
-// both directions run in one cooperative launch with a bounded grid barrier between phases.
-// Measured on the 131k-vertex torus at 64 columns it is slower than a recorded launch per phase
-// (1.05-1.15 ms a pass against 0.92 ms): the barrier over the co-resident grid costs more than a
-// kernel boundary inside a graph.
-void choose_hybrid(Factor* F, const std::vector<int>& level) {
-    const char* knob = getenv("OB_CHOL_HYBRID_LEVEL");
-    if (knob == nullptr || std::strcmp(knob, "off") == 0) return;
-    int device = 0, cooperative = 0, per_sm = 0;
-    if (cudaGetDevice(&device) != cudaSuccess ||
-        cudaDeviceGetAttribute(&cooperative, cudaDevAttrCooperativeLaunch, device) != cudaSuccess ||
-        !cooperative ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel, kTileThreads, kStageBytes) !=
-            cudaSuccess ||
-        per_sm <= 0) {
-        cudaGetLastError();
-        return;
-    }
-    const int grid = per_sm * sm_count();
-    const int L = F->analysis->levels;
-    const int n = (int)F->host_phases.size();
-    int c = -1;
-    if (std::strcmp(knob, "auto") != 0) {
-        c = std::atoi(knob);
-    } else {
-        for (int l = 0; l < L && c < 0; ++l) {
-            bool fits = true;
-            for (int p = 0; p < n; ++p)
-                if (level[p] >= l && F->host_phases[p].count > grid) fits = false;
-            if (fits) c = l;
-        }
-    }
-    if (c < 0 || c >= L) return;
-    int lo = -1, hi = -1, tiles = 0;
-    for (int p = 0; p < n; ++p)
-        if (level[p] >= c) {
-            if (lo < 0) lo = p;
-            hi = p + 1;
-            tiles = std::max(tiles, F->host_phases[p].count);
-        }
-    if (lo < 0 || hi - lo < 4 || tiles > grid) return;
-    if (!cooperative_recordable()) return;
-    F->hybrid_level = c;
-    F->hybrid_lo = lo;
-    F->hybrid_hi = hi;
-    F->hybrid_grid = grid;
-    F->hybrid_tiles = tiles;
-}
 
 int dev_alloc(Factor* F, void** p, size_t bytes, cudaStream_t stream) {
     OB_CUDA(cudaMallocAsync(p, std::max<size_t>(bytes, 8), stream));
@@ -970,8 +818,6 @@ int allow_stage_memory() {
     if (device >= 0 && device < 64 && allowed[device]) return OB_OK;
     OB_CUDA(cudaFuncSetAttribute(tile_product_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kStageBytes));
-    OB_CUDA(cudaFuncSetAttribute(pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kStageBytes));
     if (device >= 0 && device < 64) allowed[device] = 1;
     return OB_OK;
 }
@@ -980,12 +826,15 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
     if (int st0 = allow_stage_memory()) return st0;
     const Analysis& A = *F->analysis;
     const int ns = (int)A.nodes.size();
-    // Every block row is padded to a multiple of 8 doubles (and every block starts on one), so
-    // the tile kernel's 16-byte asynchronous copies are always aligned.
+    const int n = A.n;
+    // Per node the stored block is [L11^-1; G] (nc + noff rows, G = -L21 L11^-1), every block row
+    // padded to a multiple of 8 doubles (and every block starting on one), so the tile kernel's
+    // 16-byte asynchronous copies are always aligned. idx holds per node its off-diagonal rows
+    // (B rows, the forward update's outputs) and the backward product's input rows: its own Y rows
+    // then its off-diagonal X rows, in the stacked [B; Y; X] numbering.
     std::vector<long long> inv_at(ns), off_at(ns);
-    std::vector<int> rows_at(ns), ld_at(ns);
-    long long total = 0;
-    int total_rows = 0;
+    std::vector<int> rows_at(ns), back_at(ns), ld_at(ns);
+    long long total = 0, total_rows = 0;
     for (int s = 0; s < ns; ++s) {
         const int nc = A.nodes[s].count, noff = (int)A.nodes[s].off_rows.size();
         const int ld = (nc + 7) / 8 * 8;
@@ -994,20 +843,26 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
         total += (long long)nc * ld;
         off_at[s] = total;
         total += (long long)noff * ld;
-        rows_at[s] = total_rows;
+        rows_at[s] = (int)total_rows;
         total_rows += noff;
+        back_at[s] = (int)total_rows;
+        total_rows += nc + noff;
     }
+    OB_REQUIRE(total_rows < (1LL << 31) && 3LL * n < (1LL << 31), "ob_chol_factor: factor too large");
     std::vector<double> vals(std::max<long long>(total, 1), 0.0);
-    std::vector<int> idx(std::max(total_rows, 1));
+    std::vector<int> idx(std::max<long long>(total_rows, 1));
     for (int s = 0; s < ns; ++s) {
-        const int nc = A.nodes[s].count, noff = (int)A.nodes[s].off_rows.size(), ld = ld_at[s];
+        const Node& nd = A.nodes[s];
+        const int nc = nd.count, noff = (int)nd.off_rows.size(), ld = ld_at[s];
         for (int i = 0; i < nc; ++i)
             std::copy(H.inv[s].begin() + (size_t)i * nc, H.inv[s].begin() + (size_t)(i + 1) * nc,
                       vals.begin() + inv_at[s] + (size_t)i * ld);
         for (int r = 0; r < noff; ++r)
             std::copy(H.off[s].begin() + (size_t)r * nc, H.off[s].begin() + (size_t)(r + 1) * nc,
                       vals.begin() + off_at[s] + (size_t)r * ld);
-        std::copy(A.nodes[s].off_rows.begin(), A.nodes[s].off_rows.end(), idx.begin() + rows_at[s]);
+        std::copy(nd.off_rows.begin(), nd.off_rows.end(), idx.begin() + rows_at[s]);
+        for (int i = 0; i < nc; ++i) idx[back_at[s] + i] = n + nd.start + i;
+        for (int r = 0; r < noff; ++r) idx[back_at[s] + nc + r] = 2 * n + nd.off_rows[r];
     }
     F->n_vals = total;
     int st = dev_alloc(F, (void**)&F->vals, sizeof(double) * vals.size(), stream);
@@ -1025,16 +880,25 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
     OB_CUDA(cudaMemcpyAsync(F->perm, A.perm.data(), sizeof(int) * A.n, cudaMemcpyHostToDevice,
                             stream));
     OB_CUDA(cudaMemcpyAsync(F->pinned, H.pinned.data(), A.n, cudaMemcpyHostToDevice, stream));
-    // Tiles per level and phase; an inner dimension beyond kSplitK is split over several tiles,
-    // which then accumulate atomically (into rows zeroed at the start of each pass).
+    // One launch per tree level and direction. Forward at a level: every node's
+    // Y[own] = L11^-1 B[own] and B[off rows] += G B[own] (atomic: siblings share ancestors' rows);
+    // backward: X[own] = [L11^-1; G]^T [Y[own]; X[off rows]], one product over nc + noff. Each
+    // reads only rows no tile of its launch writes. A level with few tiles has its long inner
+    // dimensions split over several tiles (more CTAs, each a shorter latency-bound chain), which
+    // then accumulate atomically into rows zeroed at the start of each pass; a level with two
+    // waves of tiles or more is not split.
     const int L = A.levels;
-    std::vector<std::vector<Tile>> fd(L), fo(L), bo(L), bd(L);
-    std::vector<int2> zero_ranges;
-    // Above the leaves a phase has few tiles, each a latency-bound chain of inner steps: split
-    // those finer, so more CTAs each walk fewer steps.
-    int chunk = kSplitK;
-    auto emit = [&chunk](std::vector<Tile>& list, Tile t, int K, int whole_op, int split_op) {
-        const bool split = K > chunk + chunk / 2;
+    const long long wave = 4LL * sm_count();
+    auto tiles_of = [](int rows) { return (rows + kTileRows - 1) / kTileRows; };
+    std::vector<long long> fwd_count(L, 0), bwd_count(L, 0);
+    for (const Node& nd : A.nodes) {
+        if (nd.count == 0) continue;
+        fwd_count[nd.level] += tiles_of(nd.count) + tiles_of((int)nd.off_rows.size());
+        bwd_count[nd.level] += tiles_of(nd.count);
+    }
+    auto emit = [](std::vector<Tile>& list, Tile t, int K, bool may_split, int whole_op, int split_op) {
+        const int chunk = kSplitK;
+        const bool split = may_split && K > chunk + chunk / 2;
         for (int k0 = 0; k0 < K; k0 += split ? chunk : K) {
             t.k0 = k0;
             t.k1 = split ? std::min(K, k0 + chunk) : K;
@@ -1043,31 +907,29 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
         }
         return split;
     };
+    std::vector<std::vector<Tile>> fw(L), bw(L);
+    std::vector<int2> zero_ranges;
     for (int s = 0; s < ns; ++s) {
         const Node& nd = A.nodes[s];
         const int nc = nd.count, noff = (int)nd.off_rows.size(), ld = ld_at[s];
         if (nc == 0) continue;
-        chunk = nd.level == 0 ? kSplitK : kSplitKUpper;
+        const bool split_fwd = fwd_count[nd.level] < 2 * wave, split_bwd = bwd_count[nd.level] < 2 * wave;
         bool zero = false;
         for (int r0 = 0; r0 < nc; r0 += kTileRows) {
             const int rows = std::min(kTileRows, nc - r0);
-            // Forward diagonal: Y[own] = inv B[own].
-            zero |= emit(fd[nd.level], Tile{inv_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, nd.start, -1, 0},
-                         nc, kAssign, kAtomicAdd);
-            // Backward diagonal: X[own] = inv^T Z[own].
-            emit(bd[nd.level], Tile{inv_at[s], ld, 1, r0, rows, 0, 0, nd.start, -1, nd.start, -1, 0},
-                 nc, kAssign, kAtomicAdd);
-            // Backward off-diagonal: Z[own] -= L21^T X[off rows].
-            if (noff > 0)
-                emit(bo[nd.level], Tile{off_at[s], ld, 1, r0, rows, 0, 0, 0, rows_at[s], nd.start, -1, 0},
-                     noff, kSub, kAtomicSub);
+            // Forward diagonal: Y[own] = L11^-1 B[own].
+            zero |= emit(fw[nd.level], Tile{inv_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, n + nd.start, -1, 0},
+                         nc, split_fwd, kAssign, kAtomicAdd);
+            // Backward: X[own] = [L11^-1; G]^T [Y[own]; X[off rows]].
+            zero |= emit(bw[nd.level], Tile{inv_at[s], ld, 1, r0, rows, 0, 0, 0, back_at[s], 2 * n + nd.start, -1, 0},
+                         nc + noff, split_bwd, kAssign, kAtomicAdd);
         }
         if (zero) zero_ranges.push_back(make_int2(nd.start, nc));
         for (int r0 = 0; r0 < noff; r0 += kTileRows) {
             const int rows = std::min(kTileRows, noff - r0);
-            // Forward off-diagonal: B[off rows] -= L21 Y[own].
-            emit(fo[nd.level], Tile{off_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, 0, rows_at[s], 0},
-                 nc, kAtomicSub, kAtomicSub);
+            // Forward update: B[off rows] += G B[own].
+            emit(fw[nd.level], Tile{off_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, 0, rows_at[s], 0},
+                 nc, split_fwd, kAtomicAdd, kAtomicAdd);
         }
     }
     F->n_zero = (int)zero_ranges.size();
@@ -1091,52 +953,11 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
         }
         return OB_OK;
     };
-    st = push(fd, F->fwd_diag, F->n_fwd_diag);
-    if (!st) st = push(fo, F->fwd_off, F->n_fwd_off);
-    if (!st) st = push(bo, F->bwd_off, F->n_bwd_off);
-    if (!st) st = push(bd, F->bwd_diag, F->n_bwd_diag);
+    st = push(fw, F->fwd, F->n_fwd);
+    if (!st) st = push(bw, F->bwd, F->n_bwd);
     if (st) return st;
-    // The persistent pass's phase table, in the order the per-phase launches run, and each
-    // phase's tree level.
-    std::vector<Phase> phases;
-    std::vector<int> phase_level;
-    for (int l = 0; l < L; ++l) {
-        if (F->n_fwd_diag[l]) phases.push_back(Phase{F->fwd_diag[l], F->n_fwd_diag[l], 0, 1});
-        if (F->n_fwd_diag[l]) phase_level.push_back(l);
-        if (F->n_fwd_off[l]) phases.push_back(Phase{F->fwd_off[l], F->n_fwd_off[l], 1, 0});
-        if (F->n_fwd_off[l]) phase_level.push_back(l);
-    }
-    for (int l = L - 1; l >= 0; --l) {
-        if (F->n_bwd_off[l]) phases.push_back(Phase{F->bwd_off[l], F->n_bwd_off[l], 2, 1});
-        if (F->n_bwd_off[l]) phase_level.push_back(l);
-        if (F->n_bwd_diag[l]) phases.push_back(Phase{F->bwd_diag[l], F->n_bwd_diag[l], 1, 2});
-        if (F->n_bwd_diag[l]) phase_level.push_back(l);
-    }
-    F->n_phases = (int)phases.size();
-    st = dev_alloc(F, (void**)&F->phases, sizeof(Phase) * std::max<size_t>(phases.size(), 1), stream);
-    if (!st) st = dev_alloc(F, (void**)&F->barrier, 4 * sizeof(unsigned int), stream);
-    if (st) return st;
-    F->status = reinterpret_cast<int*>(F->barrier + 2);
-    OB_CUDA(cudaMemcpyAsync(F->phases, phases.data(), sizeof(Phase) * phases.size(),
-                            cudaMemcpyHostToDevice, stream));
-    OB_CUDA(cudaMemsetAsync(F->barrier, 0, 4 * sizeof(unsigned int), stream));
-    // The persistent pass is opt-in (OB_CHOL_PERSISTENT=1): measured on the 131k-vertex torus its
-    // 46 grid barriers over 592 CTAs cost more (1.14 ms a pass) than the recorded per-phase
-    // launches (0.82 ms).
-    const char* knob = getenv("OB_CHOL_PERSISTENT");
-    int per_sm = 0;
-    int device = 0, cooperative = 0;
-    if (knob != nullptr && knob[0] == '1' && cudaGetDevice(&device) == cudaSuccess &&
-        cudaDeviceGetAttribute(&cooperative, cudaDevAttrCooperativeLaunch, device) == cudaSuccess &&
-        cooperative &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pass_kernel, kTileThreads,
-                                                      kStageBytes) ==
-            cudaSuccess &&
-        per_sm > 0)
-        F->pass_grid = per_sm * sm_count();
-    cudaGetLastError();
-    F->host_phases = phases;
-    choose_hybrid(F, phase_level);
+    F->launches_per_pass = 0;
+    for (int l = 0; l < L; ++l) F->launches_per_pass += (F->n_fwd[l] > 0) + (F->n_bwd[l] > 0);
     OB_CUDA(cudaStreamSynchronize(stream));  // host staging buffers go out of scope
     return OB_OK;
 }
@@ -1150,21 +971,21 @@ int ensure_work(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream) {
     OB_CUDA(cudaStreamSynchronize(stream));
     for (auto& g : W.graphs) cudaGraphExecDestroy(g.exec);
     W.graphs.clear();
-    // The smaller buffers go (no graph names them any more): one set of six at the widest width.
+    // The smaller buffers go (no graph names them any more): one set at the widest width.
     const size_t old_vec = sizeof(double) * (size_t)F->n * (W.cap_k > 0 ? even_columns(W.cap_k) : 0);
-    for (double** p : {&W.B, &W.Y, &W.X, &W.R, &W.RHS, &W.SOL}) {
+    for (double** p : {&W.BYX, &W.R, &W.RHS, &W.SOL}) {
         if (*p == nullptr) continue;
         auto it = std::find(F->owned.begin(), F->owned.end(), (void*)*p);
         if (it != F->owned.end()) {
             F->owned.erase(it);
-            F->bytes -= old_vec;
+            F->bytes -= (p == &W.BYX ? 3 : 1) * old_vec;
             OB_CUDA(cudaFreeAsync(*p, stream));
         }
         *p = nullptr;
     }
     const size_t vec = sizeof(double) * (size_t)F->n * even_columns(k);
-    for (double** p : {&W.B, &W.Y, &W.X, &W.R, &W.RHS, &W.SOL}) {
-        int st = dev_alloc(F, (void**)p, vec, stream);
+    for (double** p : {&W.BYX, &W.R, &W.RHS, &W.SOL}) {
+        int st = dev_alloc(F, (void**)p, (p == &W.BYX ? 3 : 1) * vec, stream);
         if (st) return st;
     }
     W.cap_k = k;
@@ -1175,91 +996,31 @@ int ensure_work(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream) {
 // x_new = A^-1 b_new in the factor's numbering (B is consumed); k is the even internal stride.
 int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream) {
     const int L = F->analysis->levels;
-    const dim3 threads(kTileThreads);
     const int ct = (k + kTileCols - 1) / kTileCols;
-    if (F->pass_grid > 0) {
-        // One cooperative launch for the whole pass (every CTA resident, so the grid barriers
-        // between phases cannot wait on a CTA that never runs).
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(F->pass_grid);
-        cfg.blockDim = threads;
-        cfg.dynamicSmemBytes = kStageBytes;
-        cfg.stream = stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        const unsigned int limit = 1u << 23;
-        OB_CUDA(cudaLaunchKernelEx(&cfg, pass_kernel, (const Phase*)F->phases, 0, F->n_phases,
-                                   (const int2*)F->zero, F->n_zero, (const double*)F->vals,
-                                   (const int*)F->idx, W.B, W.Y, W.X, k, F->barrier, F->status,
-                                   limit));
-        count_launch();
-        return OB_OK;
-    }
     if (F->n_zero > 0) {
-        zero_rows_kernel<<<F->n_zero, 256, 0, stream>>>(F->zero, F->n_zero, k, W.Y, W.X);
+        zero_rows_kernel<<<F->n_zero, 256, 0, stream>>>(F->zero, F->n_zero, k, W.Y(k, F->n), W.X(k, F->n));
         OB_CHECK_LAUNCH("chol zero split rows");
     }
-    if (F->hybrid_lo >= 0 && k > 8) {
-        // The hybrid pass: the lower levels' phases one launch each, the upper levels' (both
-        // directions) in one cooperative launch with grid barriers between phases.
-        double* buffers[3] = {W.B, W.Y, W.X};
-        auto one = [&](int p) {
-            const Phase& ph = F->host_phases[p];
-            tile_product_kernel<<<dim3(ph.count, ct), threads, kStageBytes, stream>>>(
-                ph.tiles, F->vals, F->idx, buffers[ph.in], buffers[ph.out], k);
-            OB_CHECK_LAUNCH("chol pass phase");
-            return OB_OK;
-        };
-        int st = OB_OK;
-        for (int p = 0; p < F->hybrid_lo && st == OB_OK; ++p) st = one(p);
-        if (st) return st;
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(std::min(F->hybrid_grid, F->hybrid_tiles * ct));
-        cfg.blockDim = threads;
-        cfg.dynamicSmemBytes = kStageBytes;
-        cfg.stream = stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        const unsigned int limit = 1u << 23;
-        OB_CUDA(cudaLaunchKernelEx(&cfg, pass_kernel, (const Phase*)F->phases, F->hybrid_lo, F->hybrid_hi,
-                                   (const int2*)nullptr, 0, (const double*)F->vals, (const int*)F->idx,
-                                   W.B, W.Y, W.X, k, F->barrier, F->status, limit));
-        count_launch();
-        for (int p = F->hybrid_hi; p < (int)F->host_phases.size() && st == OB_OK; ++p) st = one(p);
-        return st;
-    }
-    // A phase's launch: the float64 tensor-core tiles, or for a narrow batch (stride 2-8) the
+    // A level's launch: the float64 tensor-core tiles, or for a narrow batch (stride 2-8) the
     // register kernel, which does not compute a 64-column tile's idle columns.
-    auto phase = [&](const Tile* tiles, int count, const double* in, double* out, const char* what) {
+    auto level = [&](const Tile* tiles, int count, const char* what) {
         switch (k) {
-            case 2: narrow_tile_kernel<2><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, in, out); break;
-            case 4: narrow_tile_kernel<4><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, in, out); break;
-            case 6: narrow_tile_kernel<6><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, in, out); break;
-            case 8: narrow_tile_kernel<8><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, in, out); break;
+            case 2: narrow_tile_kernel<2><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX); break;
+            case 4: narrow_tile_kernel<4><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX); break;
+            case 6: narrow_tile_kernel<6><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX); break;
+            case 8: narrow_tile_kernel<8><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX); break;
             default:
-                tile_product_kernel<<<dim3(count, ct), threads, kStageBytes, stream>>>(tiles, F->vals, F->idx,
-                                                                                     in, out, k);
+                tile_product_kernel<<<dim3(count, ct), kTileThreads, kStageBytes, stream>>>(tiles, F->vals, F->idx,
+                                                                                          W.BYX, k);
         }
         OB_CHECK_LAUNCH(what);
         return OB_OK;
     };
     int st = OB_OK;
-    for (int l = 0; l < L && st == OB_OK; ++l) {
-        if (F->n_fwd_diag[l]) st = phase(F->fwd_diag[l], F->n_fwd_diag[l], W.B, W.Y, "chol forward diagonal");
-        if (st == OB_OK && F->n_fwd_off[l])
-            st = phase(F->fwd_off[l], F->n_fwd_off[l], W.Y, W.B, "chol forward update");
-    }
-    for (int l = L - 1; l >= 0 && st == OB_OK; --l) {
-        if (F->n_bwd_off[l]) st = phase(F->bwd_off[l], F->n_bwd_off[l], W.X, W.Y, "chol backward gather");
-        if (st == OB_OK && F->n_bwd_diag[l])
-            st = phase(F->bwd_diag[l], F->n_bwd_diag[l], W.Y, W.X, "chol backward diagonal");
-    }
+    for (int l = 0; l < L && st == OB_OK; ++l)
+        if (F->n_fwd[l]) st = level(F->fwd[l], F->n_fwd[l], "chol forward level");
+    for (int l = L - 1; l >= 0 && st == OB_OK; --l)
+        if (F->n_bwd[l]) st = level(F->bwd[l], F->n_bwd[l], "chol backward level");
     return st;
 }
 
@@ -1272,22 +1033,22 @@ int enqueue_solve(Factor* F, Factor::WorkSet& W, int k, int refine, const int* o
                   const double* values, cudaStream_t stream) {
     const int n = F->n, kp = even_columns(k);
     const int grid = grid_for((long long)n * kp);
-    permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, F->pinned, W.RHS, W.B);
+    permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, F->pinned, W.RHS, W.B());
     OB_CHECK_LAUNCH("chol permute in");
     int st = triangular_solves(F, W, kp, stream);
     if (st) return st;
-    permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, W.X, W.SOL, 0);
+    permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, W.X(kp, n), W.SOL, 0);
     OB_CHECK_LAUNCH("chol permute out");
     // Iterative refinement in float64: x += A^-1 (b - A x).
     for (int it = 0; it < refine; ++it) {
         residual_kernel<<<grid, 256, 0, stream>>>(n, k, offsets, columns, values, W.RHS, W.SOL,
                                                   W.R);
         OB_CHECK_LAUNCH("chol residual");
-        permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, F->pinned, W.R, W.B);
+        permute_in_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, F->pinned, W.R, W.B());
         OB_CHECK_LAUNCH("chol permute in");
         st = triangular_solves(F, W, kp, stream);
         if (st) return st;
-        permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, W.X, W.SOL, 1);
+        permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, W.X(kp, n), W.SOL, 1);
         OB_CHECK_LAUNCH("chol permute out");
     }
     return OB_OK;
@@ -1323,12 +1084,6 @@ int solve_graph(Factor* F, Factor::WorkSet& W, int k, int refine, const int* off
     if (graph) cudaGraphDestroy(graph);
     if (st != OB_OK || e != cudaSuccess) {
         cudaGetLastError();
-        if (F->pass_grid > 0 || F->hybrid_lo >= 0) {
-            // A cooperative launch this runtime cannot record: fall back to a launch per phase.
-            F->pass_grid = 0;
-            F->hybrid_lo = F->hybrid_hi = -1;
-            return solve_graph(F, W, k, refine, offsets, columns, values, out);
-        }
         return st != OB_OK ? st : cuda_status(e, "ob_chol_solve: capture");
     }
     W.graphs.push_back(Factor::Recorded{k, refine, offsets, columns, values, exec, (int)nodes});
@@ -1486,24 +1241,11 @@ int ob_chol_work_set(void* factor, int set, int n_columns, double** rhs, double*
     Factor::WorkSet& W = F->sets[set];
     int st = ensure_work(F, W, n_columns, as_stream(stream_));
     if (st) return st;
-    *rhs = W.B;
-    *solution = W.X;
+    *rhs = W.B();
+    *solution = W.X(even_columns(n_columns), F->n);
     *stride = even_columns(n_columns);
     *iperm = F->iperm;
     *pinned = F->pinned;
-    return OB_OK;
-}
-
-int ob_chol_check(void* factor, int* status, int* persistent, ob_stream_t stream_) {
-    cudaStream_t stream = as_stream(stream_);
-    OB_REQUIRE(factor && status, "ob_chol_check: bad argument");
-    Factor* F = static_cast<Factor*>(factor);
-    int word = 0;
-    OB_CUDA(cudaMemcpyAsync(&word, F->status, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    OB_CUDA(cudaStreamSynchronize(stream));
-    if (word != 0) OB_CUDA(cudaMemsetAsync(F->barrier, 0, 4 * sizeof(unsigned int), stream));
-    *status = word;
-    if (persistent) *persistent = F->pass_grid;
     return OB_OK;
 }
 
@@ -1589,11 +1331,8 @@ int ob_chol_info(void* factor, long long* info) {
     info[0] = F->n;
     info[1] = F->n_vals;
     info[2] = F->analysis->levels;
-    // Kernel launches a pass over a wide batch makes (a phase each, or with the hybrid pass the
-    // lower phases plus one cooperative launch for the upper ones).
-    long long launches = (long long)F->host_phases.size();
-    if (F->hybrid_lo >= 0) launches += 1 - (F->hybrid_hi - F->hybrid_lo);
-    info[3] = launches;
+    // Product launches a pass makes: one per tree level and direction.
+    info[3] = F->launches_per_pass;
     return OB_OK;
 }
 
@@ -1616,7 +1355,8 @@ int ob_chol_host_solve(int n, const int32_t* offsets, const int32_t* columns,
         info[2] = A.levels;
         info[3] = A.factor_entries;
     }
-    // The device algorithm, run on the host: forward by levels' postorder, backward reversed.
+    // The device algorithm, run on the host: forward by levels' postorder (y1 = L11^-1 b1,
+    // b2 += G b1), backward reversed (x1 = L11^-T y1 + G^T x2), G = -L21 L11^-1.
     std::vector<double> b(n), y(n, 0.0), xs(n, 0.0);
     for (int i = 0; i < n; ++i) b[i] = H.pinned[i] ? 0.0 : rhs[A.perm[i]];
     for (int s = 0; s < (int)A.nodes.size(); ++s) {
@@ -1629,22 +1369,17 @@ int ob_chol_host_solve(int n, const int32_t* offsets, const int32_t* columns,
         }
         for (int r = 0; r < noff; ++r) {
             double acc = 0.0;
-            for (int j = 0; j < nc; ++j) acc += H.off[s][(size_t)r * nc + j] * y[nd.start + j];
-            b[nd.off_rows[r]] -= acc;
+            for (int j = 0; j < nc; ++j) acc += H.off[s][(size_t)r * nc + j] * b[nd.start + j];
+            b[nd.off_rows[r]] += acc;
         }
     }
     for (int s = (int)A.nodes.size() - 1; s >= 0; --s) {
         const Node& nd = A.nodes[s];
         const int nc = nd.count, noff = (int)nd.off_rows.size();
-        std::vector<double> z(nc);
-        for (int j = 0; j < nc; ++j) {
-            double acc = y[nd.start + j];
-            for (int r = 0; r < noff; ++r) acc -= H.off[s][(size_t)r * nc + j] * xs[nd.off_rows[r]];
-            z[j] = acc;
-        }
         for (int i = 0; i < nc; ++i) {
             double acc = 0.0;
-            for (int j = 0; j < nc; ++j) acc += H.inv[s][(size_t)j * nc + i] * z[j];
+            for (int j = 0; j < nc; ++j) acc += H.inv[s][(size_t)j * nc + i] * y[nd.start + j];
+            for (int r = 0; r < noff; ++r) acc += H.off[s][(size_t)r * nc + i] * xs[nd.off_rows[r]];
             xs[nd.start + i] = acc;
         }
     }

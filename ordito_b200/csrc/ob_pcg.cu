@@ -896,14 +896,19 @@ int ob_pcg_time_matvec(void* solver, int reps, float* ms, ob_stream_t stream_) {
     cudaStream_t stream = as_stream(stream_);
     OB_REQUIRE(solver && ms && reps >= 1, "ob_pcg_time_matvec: bad argument");
     Solver* S = static_cast<Solver*>(solver);
-    OB_CUDA(cudaMemsetAsync(S->state, 0, sizeof(LoopState), stream));
+    // Each launch is timed alone, its loop state reset before it (a launch that finds the loop
+    // over returns at once, and a zero residual ends the loop after one launch).
     cudaEvent_t start, end;
     OB_CUDA(cudaEventCreate(&start));
     OB_CUDA(cudaEventCreate(&end));
     int st = OB_OK;
     const int B = S->blocks;
-    cudaEventRecord(start, stream);
-    for (int i = 0; i < reps && st == OB_OK; ++i) {
+    float total = 0.0f;
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < reps && st == OB_OK && e == cudaSuccess; ++i) {
+        e = cudaMemsetAsync(S->state, 0, sizeof(LoopState), stream);
+        if (e != cudaSuccess) break;
+        cudaEventRecord(start, stream);
         if (S->narrow)
             matvec_dots_kernel<float><<<B, kThreads, 0, stream>>>(
                 S->n, S->k, S->offsets, S->columns, S->values32, S->r, S->u, S->w, S->partials,
@@ -914,11 +919,12 @@ int ob_pcg_time_matvec(void* solver, int reps, float* ms, ob_stream_t stream_) {
                 S->counters, S->scalars, S->state, 0x7fffffff);
         count_launch();
         if (cudaGetLastError() != cudaSuccess) st = fail(OB_ERR_CUDA, "ob_pcg_time_matvec: launch");
+        cudaEventRecord(end, stream);
+        e = cudaEventSynchronize(end);
+        float one = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&one, start, end);
+        total += one;
     }
-    cudaEventRecord(end, stream);
-    cudaError_t e = cudaEventSynchronize(end);
-    float total = 0.0f;
-    if (e == cudaSuccess) e = cudaEventElapsedTime(&total, start, end);
     cudaEventDestroy(start);
     cudaEventDestroy(end);
     if (st) return st;

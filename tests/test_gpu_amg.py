@@ -152,3 +152,31 @@ def test_geodesic_with_multigrid_poisson(gpu) -> None:
     for c, s in enumerate(sources):
         ref = hp.heat_geodesic(v, f, np.array([s]), operators=ops)
         assert rel_err(got[c], ref) <= DISTANCE_TOL
+
+
+def test_time_kernels_reports_each_vcycle_kernel(gpu) -> None:
+    """ob_amg_time_kernels: positive times for the finest level's four kernels and the whole
+    V-cycle, algorithmic bytes at least the finest operator's stored entries and vectors."""
+    import ctypes
+
+    from ordito_b200 import _lib
+
+    v, f = creation.jittered_torus(128, 64, seed=0)
+    ops = _operators(v, f)
+    cycle = glinalg.multigrid_preconditioner(ops.poisson_system)
+    ms = (ctypes.c_float * 5)()
+    nbytes = (ctypes.c_longlong * 5)()
+    _lib.call("ob_amg_time_kernels", cycle.handle, 64, 2, ms, nbytes, None)
+    n, nnz = ops.poisson_system.nrow, ops.poisson_system.nnz
+    assert all(ms[i] > 0.0 for i in range(5))
+    assert nbytes[0] >= 8 * nnz + 3 * 4 * n * 64
+    assert nbytes[1] >= 8 * nnz + 3 * 4 * n * 64
+    assert nbytes[2] > 4 * n * 64 and nbytes[3] > 2 * 4 * n * 64
+    # The timed kernels leave the hierarchy usable: a solve still converges.
+    rhs = np.random.default_rng(0).normal(size=n)
+    rhs -= rhs.mean()
+    x = DeviceArray.zeros(n, np.float64)
+    glinalg.solve_spd(ops.poisson_system, DeviceArray.from_host(rhs), x, tol=1e-8,
+                      preconditioner=cycle)
+    A = ops.poisson_system.to_scipy()
+    assert np.linalg.norm(A @ x.numpy() - rhs) <= 1e-6 * np.linalg.norm(rhs)
