@@ -433,6 +433,26 @@ def kernel_rooflines(mesh, solver, columns: int = 64, reps: int = 10) -> dict:
         record("pcg_matvec_dots_" + ("f32_values" if narrow else "f64"), ms.value,
                4 * (n + 1) + (8 if narrow else 12) * nnz + 3 * 8 * n,
                "offsets, columns and values once, u, r in and w out (float64), one column")
+    # The same kernel on an operator of the same size in a local vertex order (a jittered torus
+    # 2048 x 1280, row by row): the mat-vec's gathers of u follow the vertex order, and the
+    # icosphere's subdivision order scatters each row's neighbours across the vector.
+    from ordito_b200 import creation
+    from ordito_b200.mesh import Trimesh
+
+    tv, tf = creation.jittered_torus(2048, 1280, 1.0, 0.3, 0.1, seed=0)
+    torus = Trimesh(tv, tf.reshape(-1))
+    T = torus.heat_solver(None, method="meshlab").operators.heat_system
+    handle = ctypes.c_void_p(0)
+    _lib.call("ob_pcg_create", T.nrow, T.offsets.ptr, T.columns.ptr, T.values.ptr, 1, 1, 0,
+              ctypes.byref(handle), None)
+    ms = ctypes.c_float(0.0)
+    _lib.call("ob_pcg_time_matvec", handle, 1, ctypes.byref(ms), None)
+    _lib.call("ob_pcg_time_matvec", handle, reps, ctypes.byref(ms), None)
+    _lib.lib.ob_pcg_destroy(handle)
+    record("pcg_matvec_dots_f64_torus_2048x1280", ms.value,
+           4 * (T.nrow + 1) + 12 * T.nnz + 3 * 8 * T.nrow,
+           "as pcg_matvec_dots_f64, on the heat system of a 2 621 440-vertex torus in row order")
+    torus.dispose()
 
     # a10: the V-cycle kernels of the Poisson hierarchy on `columns` float32 columns.
     amg = solver.poisson_multigrid

@@ -180,6 +180,10 @@ __device__ __forceinline__ double inverse_power_of_two(double largest) {
 
 // -div of the unit gradient at (vertex, column) from the per-face terms, summed over the vertex's
 // corners in ascending slot order: d_e = (W_e . s) / |s| with s = g 2^-e the rescaled gradient.
+// A thread takes CP adjacent columns of one vertex, so the per-corner index and term loads are
+// shared by CP columns (with CP > 1 the strides are even and u, out 16-byte aligned: u is read
+// and out written as double2). Columns from n_columns up are written as zero.
+template <int CP>
 __global__ void grad_div_terms_kernel(const double* __restrict__ terms, const int* __restrict__ faces,
                                       const int* __restrict__ corner_offsets,
                                       const int* __restrict__ corner_slots, int n, int k,
@@ -187,35 +191,67 @@ __global__ void grad_div_terms_kernel(const double* __restrict__ terms, const in
                                       const int* __restrict__ u_iperm, double* __restrict__ out,
                                       int out_stride, const int* __restrict__ out_iperm,
                                       const char* __restrict__ out_pinned) {
+    const int groups = out_stride / CP;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= (long long)n * out_stride) return;
-    const int v = (int)(t / out_stride), c = (int)(t % out_stride);
+    if (t >= (long long)n * groups) return;
+    const int v = (int)(t / groups), c0 = (int)(t % groups) * CP;
     const int row = row_of(out_iperm, v);
-    if (c >= k) {
-        out[(size_t)row * out_stride + c] = 0.0;  // a pad column stays zero
-        return;
+    double acc[CP];
+#pragma unroll
+    for (int j = 0; j < CP; ++j) acc[j] = 0.0;
+    auto load = [&](int r, double* dst) {
+        const double* src = u + (size_t)r * u_stride + c0;
+        if (CP == 1) {
+            dst[0] = src[0];
+        } else {
+#pragma unroll
+            for (int j = 0; j < CP; j += 2) {
+                // A pair starting below k lies inside the row (even strides).
+                const double2 p = (c0 + j < k) ? *reinterpret_cast<const double2*>(src + j) : make_double2(0.0, 0.0);
+                dst[j] = p.x;
+                dst[j + 1] = p.y;
+            }
+        }
+    };
+    if (c0 < k) {
+        const int end = corner_offsets[v + 1];
+        for (int p = corner_offsets[v]; p < end; ++p) {
+            const int q = corner_slots[p];
+            const int f = q / 3, e = q - 3 * f;
+            double u0[CP], u1[CP], u2[CP];
+            load(row_of(u_iperm, faces[3 * f]), u0);
+            load(row_of(u_iperm, faces[3 * f + 1]), u1);
+            load(row_of(u_iperm, faces[3 * f + 2]), u2);
+            const double* T = terms + (size_t)kFaceTerms * f;
+            const double a0 = T[0], a1 = T[1], a2 = T[2], b0 = T[3], b1 = T[4], b2 = T[5];
+            const double w0 = T[6], w1 = T[7], w2 = T[8];
+            const double* W = T + 9 + 3 * e;
+            const double W0 = W[0], W1 = W[1], W2 = W[2];
+#pragma unroll
+            for (int j = 0; j < CP; ++j) {
+                const double gx = fma(u0[j], a0, fma(u1[j], b0, u2[j] * w0));
+                const double gy = fma(u0[j], a1, fma(u1[j], b1, u2[j] * w1));
+                const double gz = fma(u0[j], a2, fma(u1[j], b2, u2[j] * w2));
+                const double largest = fmax(fabs(gx), fmax(fabs(gy), fabs(gz)));
+                if (largest == 0.0) continue;  // no gradient: the unit gradient is zero
+                const double scale = inverse_power_of_two(largest);
+                const double sx = gx * scale, sy = gy * scale, sz = gz * scale;
+                const double along = fma(sx, W0, fma(sy, W1, sz * W2));
+                acc[j] += along * rsqrt(fma(sx, sx, fma(sy, sy, sz * sz)));
+            }
+        }
     }
-    double acc = 0.0;
-    const int end = corner_offsets[v + 1];
-    for (int p = corner_offsets[v]; p < end; ++p) {
-        const int q = corner_slots[p];
-        const int f = q / 3, e = q - 3 * f;
-        const double u0 = u[(size_t)row_of(u_iperm, faces[3 * f]) * u_stride + c];
-        const double u1 = u[(size_t)row_of(u_iperm, faces[3 * f + 1]) * u_stride + c];
-        const double u2 = u[(size_t)row_of(u_iperm, faces[3 * f + 2]) * u_stride + c];
-        const double* T = terms + (size_t)kFaceTerms * f;
-        const double gx = fma(u0, T[0], fma(u1, T[3], u2 * T[6]));
-        const double gy = fma(u0, T[1], fma(u1, T[4], u2 * T[7]));
-        const double gz = fma(u0, T[2], fma(u1, T[5], u2 * T[8]));
-        const double largest = fmax(fabs(gx), fmax(fabs(gy), fabs(gz)));
-        if (largest == 0.0) continue;  // no gradient: the unit gradient is zero
-        const double scale = inverse_power_of_two(largest);
-        const double sx = gx * scale, sy = gy * scale, sz = gz * scale;
-        const double* W = T + 9 + 3 * e;
-        const double along = fma(sx, W[0], fma(sy, W[1], sz * W[2]));
-        acc += along * rsqrt(fma(sx, sx, fma(sy, sy, sz * sz)));
+    const bool pinned = out_pinned && out_pinned[row];
+    double* o = out + (size_t)row * out_stride + c0;
+#pragma unroll
+    for (int j = 0; j < CP; ++j)
+        if (pinned || c0 + j >= k) acc[j] = 0.0;
+    if (CP == 1) {
+        o[0] = acc[0];
+    } else {
+#pragma unroll
+        for (int j = 0; j < CP; j += 2) *reinterpret_cast<double2*>(o + j) = make_double2(acc[j], acc[j + 1]);
     }
-    out[(size_t)row * out_stride + c] = (out_pinned && out_pinned[row]) ? 0.0 : acc;
 }
 
 // Seeds of k source sets in a factor's numbering: rhs (stride `stride`, zeroed first) gets 1 at
@@ -247,8 +283,17 @@ __global__ void shift_sums_kernel(const double* __restrict__ phi, int n, int str
     double everywhere = 0.0;
     const long long total = (long long)n * stride;
     const long long step = (long long)gridDim.x * blockDim.x;  // a multiple of stride
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += step)
-        everywhere += phi[t];
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    // Four independent loads in flight a thread (the sum stays in index order per thread).
+    for (; t + 3 * step < total; t += 4 * step) {
+        const double a = phi[t], b = phi[t + step], d = phi[t + 2 * step],
+                     e = phi[t + 3 * step];
+        everywhere += a;
+        everywhere += b;
+        everywhere += d;
+        everywhere += e;
+    }
+    for (; t < total; t += step) everywhere += phi[t];
     tree[threadIdx.x] = everywhere;
     __syncthreads();
     if ((int)threadIdx.x < stride) {
@@ -257,15 +302,23 @@ __global__ void shift_sums_kernel(const double* __restrict__ phi, int n, int str
         partials[(size_t)blockIdx.x * stride + threadIdx.x] = column;
     }
     if (!last_block_arrived(counter, &last)) return;
+    // The last block: thread t folds column t % stride over blocks t / stride, t / stride + groups,
+    // ... in order; the groups' sums then meet in group order (a fixed order for a launch shape).
+    const int groups = blockDim.x / stride;
+    double part = 0.0;
+    for (int bx = threadIdx.x / stride; bx < (int)gridDim.x; bx += groups)
+        part += __ldcg(&partials[(size_t)bx * stride + c]);
+    __syncthreads();
+    tree[threadIdx.x] = part;
+    __syncthreads();
     for (int col = threadIdx.x; col < k; col += blockDim.x) {
         double g = 0.0;
-        for (int bx = 0; bx < (int)gridDim.x; ++bx) g += __ldcg(&partials[(size_t)bx * stride + col]);
+        for (int q = 0; q < groups; ++q) g += tree[q * stride + col];
         double s = 0.0;
         for (int i = source_offsets[col]; i < source_offsets[col + 1]; ++i)
             s += __ldcg(&phi[(size_t)iperm[sources[i]] * stride + col]);
         sums[col] = make_double2(s, g);
     }
-    (void)c;
 }
 
 // out[c][v] = the shifted, oriented phi of vertex v in column c (ordito/kernels/heat.py:3406).
@@ -445,10 +498,24 @@ int ob_grad_div_terms(const double* terms, const int32_t* faces, const int32_t* 
                "ob_grad_div_terms: bad size");
     if (n_vertices == 0) return OB_OK;
     OB_REQUIRE(terms && faces && corner_offsets && corner_slots && u && out, "ob_grad_div_terms: null pointer");
-    const long long total = (long long)n_vertices * out_stride;
-    grad_div_terms_kernel<<<ceil_div(total, kThreads), kThreads, 0, stream>>>(
-        terms, faces, corner_offsets, corner_slots, n_vertices, n_columns, u, u_stride, u_iperm, out,
-        out_stride, out_iperm, out_pinned);
+    // Columns a thread takes: 4 or 2 when the strides and pointers allow paired loads and stores.
+    const bool paired = u_stride % 2 == 0 && out_stride % 2 == 0 && ((uintptr_t)u & 15) == 0 &&
+                        ((uintptr_t)out & 15) == 0;
+    const int cp = !paired ? 1 : (out_stride % 4 == 0 ? 4 : 2);
+    const long long total = (long long)n_vertices * (out_stride / cp);
+    const int blocks = (int)ceil_div(total, kThreads);
+    if (cp == 4)
+        grad_div_terms_kernel<4><<<blocks, kThreads, 0, stream>>>(terms, faces, corner_offsets, corner_slots,
+                                                                  n_vertices, n_columns, u, u_stride, u_iperm,
+                                                                  out, out_stride, out_iperm, out_pinned);
+    else if (cp == 2)
+        grad_div_terms_kernel<2><<<blocks, kThreads, 0, stream>>>(terms, faces, corner_offsets, corner_slots,
+                                                                  n_vertices, n_columns, u, u_stride, u_iperm,
+                                                                  out, out_stride, out_iperm, out_pinned);
+    else
+        grad_div_terms_kernel<1><<<blocks, kThreads, 0, stream>>>(terms, faces, corner_offsets, corner_slots,
+                                                                  n_vertices, n_columns, u, u_stride, u_iperm,
+                                                                  out, out_stride, out_iperm, out_pinned);
     OB_CHECK_LAUNCH("grad_div_terms");
     return OB_OK;
 }
@@ -494,8 +561,8 @@ int ob_shift_permuted(const double* phi, int n_vertices, int stride, const int32
     OB_REQUIRE(stride <= kThreads, "ob_shift_permuted: stride above %d", kThreads);
     const int threads = (kThreads / stride) * stride;
     const long long total = (long long)n_vertices * stride;
-    const int blocks = (int)std::max(1LL, std::min((total + threads * 4 - 1) / (threads * 4),
-                                                   (long long)2 * sm_count()));
+    const int blocks = (int)std::max(1LL, std::min((total + threads * 8 - 1) / (threads * 8),
+                                                   (long long)4 * sm_count()));
     Scratch scratch(stream);
     double* partials = scratch.take<double>((size_t)blocks * stride);
     double2* sums = scratch.take<double2>(n_columns);
