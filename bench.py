@@ -9,7 +9,8 @@ factors stay on the device, and the 64 queries run as one batched pass in the fa
 shift; ``--refine 1`` adds a float64 refinement step to each solve).
 ``value`` is whole-job solves/s with the sources resident on the device, three batches in flight
 on three streams; ``e2e`` is the same stream through the public API (``heat.BatchPipeline``) from
-host source lists to pinned host distances, copies included. The plain drop-in (``heat_geodesic(vertices, faces, [s])``: assembly, solves and any
+host source lists to pinned host distances, copies included. The plain drop-in
+(``heat_geodesic(vertices, faces, [s])``: assembly, solves and any
 factorisation inside every call) and the resident single query are timed beside it. A sample of
 the answers is checked against the float64 CPU oracle on every run.
 

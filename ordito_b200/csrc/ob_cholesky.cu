@@ -148,31 +148,11 @@ struct Dissector {
     }
 };
 
-int analyse(int n, std::vector<int> offsets, std::vector<int> columns, const float* xyz,
-            int leaf_size, Analysis* out) {
-    Analysis& A = *out;
-    A.n = n;
-    A.offsets = std::move(offsets);
-    A.columns = std::move(columns);
-    // Adjacency without the diagonal, for the separators and the components.
-    std::vector<int> adj_off(n + 1, 0), adj;
-    adj.reserve(A.columns.size());
-    for (int i = 0; i < n; ++i) {
-        for (int e = A.offsets[i]; e < A.offsets[i + 1]; ++e)
-            if (A.columns[e] != i) adj.push_back(A.columns[e]);
-        adj_off[i + 1] = (int)adj.size();
-    }
-    Dissector D(adj_off, adj, xyz, n, leaf_size > 0 ? leaf_size : kDefaultLeafSize);
-    std::vector<int> all(n);
-    std::iota(all.begin(), all.end(), 0);
-    D.dissect(std::move(all));
-    A.perm = std::move(D.order);
-    A.nodes = std::move(D.tree);
-    A.iperm.assign(n, 0);
-    for (int i = 0; i < n; ++i) A.iperm[A.perm[i]] = i;
-    // Symbolic: each node's off-diagonal rows are its columns' later neighbours plus its
-    // children's off-diagonal rows past its own columns.
-    std::vector<int> mark(n, -1);
+// Symbolic analysis of a dissection: each node's off-diagonal rows are its columns' later
+// neighbours plus its children's off-diagonal rows past its own columns; its level is its height
+// above the leaves.
+void symbolic(Analysis& A, const std::vector<int>& adj_off, const std::vector<int>& adj) {
+    std::vector<int> mark(A.n, -1);
     A.factor_entries = 0;
     A.levels = 0;
     for (int s = 0; s < (int)A.nodes.size(); ++s) {
@@ -205,6 +185,142 @@ int analyse(int n, std::vector<int> offsets, std::vector<int> columns, const flo
         A.factor_entries += (long long)node.count * node.count +
                             (long long)node.off_rows.size() * node.count;
     }
+}
+
+// Level amalgamation. Each tree level costs the solves one dependent launch per direction (a
+// few microseconds of launch and pipeline latency however little work the level holds), so whole
+// levels above the leaves are merged into their parents while that is cheap: merging the nodes
+// of level l into their parents at l + 1 makes each parent one dense supernode of its own and
+// the merged children's columns (its off-diagonal rows stay the parent's), adding explicit zeros
+// to the stored factor. The cheapest level goes first, as long as it adds at most kMergeValues
+// stored values (about 12 us of float64 tensor work for a 64-column pass, against the ~20 us the
+// two launches cost) and the factor stays within kMergeGrowth of its unmerged size. Columns of a
+// merged node are renumbered to be contiguous (the merged children's columns, then the parent's):
+// siblings' separators never share an edge, so this changes no fill outside the merged fronts.
+constexpr long long kMergeValues = 1750000;
+constexpr double kMergeGrowth = 1.3;
+
+void amalgamate(Analysis& A, const std::vector<int>& adj_off, const std::vector<int>& adj) {
+    const int ns = (int)A.nodes.size();
+    if (A.levels < 3) return;
+    auto padded = [](long long c) { return (c + 7) / 8 * 8; };
+    std::vector<long long> nc(ns), noff(ns);
+    std::vector<std::vector<int>> kids(ns), cols_of(ns);
+    std::vector<char> alive(ns, 1);
+    long long total = 0;
+    for (int s = 0; s < ns; ++s) {
+        nc[s] = A.nodes[s].count;
+        noff[s] = (long long)A.nodes[s].off_rows.size();
+        kids[s] = A.nodes[s].children;
+        cols_of[s].assign(1, s);
+        total += (nc[s] + noff[s]) * padded(nc[s]);
+    }
+    const long long limit = (long long)(kMergeGrowth * (double)total);
+    std::vector<int> level(ns, 0);
+    bool merged_any = false;
+    for (;;) {
+        int top = 0;
+        for (int s = 0; s < ns; ++s) {
+            if (!alive[s]) continue;
+            int l = 0;
+            for (int c : kids[s]) l = std::max(l, level[c] + 1);
+            level[s] = l;
+            top = std::max(top, l);
+        }
+        // The merge cost of every level 1 .. top - 1 (leaves stay: merging them is dense work).
+        std::vector<long long> delta(top + 1, 0);
+        std::vector<char> candidate(top + 1, 0);
+        for (int p = 0; p < ns; ++p) {
+            if (!alive[p] || level[p] < 2) continue;
+            const int l = level[p] - 1;
+            long long m = nc[p], before = (nc[p] + noff[p]) * padded(nc[p]);
+            bool any = false;
+            for (int c : kids[p])
+                if (level[c] == l) {
+                    m += nc[c];
+                    before += (nc[c] + noff[c]) * padded(nc[c]);
+                    any = true;
+                }
+            if (!any) continue;
+            candidate[l] = 1;
+            delta[l] += (m + noff[p]) * padded(m) - before;
+        }
+        int best = -1;
+        for (int l = 1; l < top; ++l)
+            if (candidate[l] && (best < 0 || delta[l] < delta[best])) best = l;
+        if (best < 0 || delta[best] > kMergeValues || total + delta[best] > limit) break;
+        for (int p = 0; p < ns; ++p) {
+            if (!alive[p] || level[p] != best + 1) continue;
+            std::vector<int> next, absorbed;
+            for (int c : kids[p]) {
+                if (level[c] == best) {
+                    nc[p] += nc[c];
+                    alive[c] = 0;
+                    absorbed.insert(absorbed.end(), cols_of[c].begin(), cols_of[c].end());
+                    next.insert(next.end(), kids[c].begin(), kids[c].end());
+                } else {
+                    next.push_back(c);
+                }
+            }
+            absorbed.insert(absorbed.end(), cols_of[p].begin(), cols_of[p].end());
+            cols_of[p] = std::move(absorbed);
+            kids[p] = std::move(next);
+        }
+        total += delta[best];
+        merged_any = true;
+    }
+    if (!merged_any) return;
+    // Renumber: the surviving nodes in postorder (children first, each subtree contiguous), each
+    // node's columns those of the original nodes merged into it.
+    std::vector<int> order;
+    order.reserve(A.n);
+    std::vector<Node> tree;
+    std::function<int(int)> emit = [&](int s) -> int {
+        std::vector<int> children;
+        for (int c : kids[s]) children.push_back(emit(c));
+        Node node;
+        node.start = (int)order.size();
+        for (int o : cols_of[s])
+            for (int j = 0; j < A.nodes[o].count; ++j) order.push_back(A.perm[A.nodes[o].start + j]);
+        node.count = (int)order.size() - node.start;
+        node.children = children;
+        tree.push_back(node);
+        const int id = (int)tree.size() - 1;
+        for (int c : children) tree[c].parent = id;
+        return id;
+    };
+    for (int s = 0; s < ns; ++s)
+        if (alive[s] && A.nodes[s].parent < 0) emit(s);
+    A.perm = std::move(order);
+    A.nodes = std::move(tree);
+    for (int i = 0; i < A.n; ++i) A.iperm[A.perm[i]] = i;
+    symbolic(A, adj_off, adj);
+}
+
+int analyse(int n, std::vector<int> offsets, std::vector<int> columns, const float* xyz,
+            int leaf_size, Analysis* out) {
+    Analysis& A = *out;
+    A.n = n;
+    A.offsets = std::move(offsets);
+    A.columns = std::move(columns);
+    // Adjacency without the diagonal, for the separators and the components.
+    std::vector<int> adj_off(n + 1, 0), adj;
+    adj.reserve(A.columns.size());
+    for (int i = 0; i < n; ++i) {
+        for (int e = A.offsets[i]; e < A.offsets[i + 1]; ++e)
+            if (A.columns[e] != i) adj.push_back(A.columns[e]);
+        adj_off[i + 1] = (int)adj.size();
+    }
+    Dissector D(adj_off, adj, xyz, n, leaf_size > 0 ? leaf_size : kDefaultLeafSize);
+    std::vector<int> all(n);
+    std::iota(all.begin(), all.end(), 0);
+    D.dissect(std::move(all));
+    A.perm = std::move(D.order);
+    A.nodes = std::move(D.tree);
+    A.iperm.assign(n, 0);
+    for (int i = 0; i < n; ++i) A.iperm[A.perm[i]] = i;
+    symbolic(A, adj_off, adj);
+    amalgamate(A, adj_off, adj);
     // Components (for pinning a singular operator): the last vertex of each in the new order.
     A.component_last.assign(n, 0);
     std::vector<int> comp(n, -1);
