@@ -1048,6 +1048,15 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
                  nc, split_fwd, kAtomicAdd, kAtomicAdd);
         }
     }
+    // Adjacent ranges joined, then cut into pieces of at most 16 rows: one block each, so the
+    // zeroing launch is balanced however large a merged node is.
+    std::vector<int2> pieces;
+    for (size_t i = 0; i < zero_ranges.size();) {
+        int2 r = zero_ranges[i++];
+        while (i < zero_ranges.size() && zero_ranges[i].x == r.x + r.y) r.y += zero_ranges[i++].y;
+        for (int o = 0; o < r.y; o += 16) pieces.push_back(make_int2(r.x + o, std::min(16, r.y - o)));
+    }
+    zero_ranges.swap(pieces);
     F->n_zero = (int)zero_ranges.size();
     if (F->n_zero > 0) {
         st = dev_alloc(F, (void**)&F->zero, sizeof(int2) * zero_ranges.size(), stream);

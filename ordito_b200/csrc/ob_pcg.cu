@@ -207,7 +207,7 @@ __global__ void reset_kernel(int n, int k, int k_live, const double* __restrict_
 // block folds them per column in block order and derives (alpha, beta, step) (cg_step_scalars,
 // conjugate_gradient.py:549-579), then counts the round (cg_close_round :628-669).
 template <typename V>
-__global__ void matvec_dots_kernel(int n, int k, const int* __restrict__ offsets,
+__global__ void __launch_bounds__(kThreads, 8) matvec_dots_kernel(int n, int k, const int* __restrict__ offsets,
                                    const int* __restrict__ columns, const V* __restrict__ values,
                                    const double* __restrict__ r, const double* __restrict__ u,
                                    double* __restrict__ w, double* __restrict__ partials,
@@ -317,7 +317,7 @@ __global__ void matvec_dots_kernel(int n, int k, const int* __restrict__ offsets
 // The second node: p = u + beta p, s = w + beta s, x += alpha p, r -= alpha s and the Jacobi apply
 // D^-1 r into `scaled` (which is u itself under Jacobi, the polynomial's input under Chebyshev)
 // for every column that stepped (conjugate_gradient.py:797-838, cg_advance :413).
-__global__ void update_kernel(int n, int k, const ColumnScalars* __restrict__ scalars,
+__global__ void __launch_bounds__(kThreads, 8) update_kernel(int n, int k, const ColumnScalars* __restrict__ scalars,
                               const double* __restrict__ inv_diag, const double* __restrict__ w,
                               const double* u, double* __restrict__ p, double* __restrict__ s,
                               double* __restrict__ r, double* __restrict__ x, double* scaled) {
@@ -367,7 +367,7 @@ __global__ void chebyshev_step_kernel(int n, int k, const int* __restrict__ offs
 // The settle check (cg_settle_change / cg_settle_verdict, conjugate_gradient.py:1500-1580): the
 // largest |x - previous| / |x| over non-zero entries and their count, over every column; previous
 // advances to x. The last block applies the verdict.
-__global__ void settle_kernel(long long total, const double* __restrict__ x,
+__global__ void __launch_bounds__(kThreads, 8) settle_kernel(long long total, const double* __restrict__ x,
                               double* __restrict__ previous, double2* __restrict__ partials,
                               unsigned int* counter, SettleState* settle, LoopState* state,
                               int check_rounds, double change_tolerance, int settle_rounds) {

@@ -274,7 +274,7 @@ __global__ void seed_permuted_kernel(const int* __restrict__ sources,
 // rows, added by that last block.
 __global__ void shift_sums_kernel(const double* __restrict__ phi, int n, int stride,
                                   const int* __restrict__ iperm, const int* __restrict__ sources,
-                                  const int* __restrict__ source_offsets, int k,
+                                  const int* __restrict__ source_offsets, int k, int orient,
                                   double* __restrict__ partials, unsigned int* counter,
                                   double2* __restrict__ sums) {
     __shared__ double tree[kThreads];
@@ -317,15 +317,18 @@ __global__ void shift_sums_kernel(const double* __restrict__ phi, int n, int str
         double s = 0.0;
         for (int i = source_offsets[col]; i < source_offsets[col + 1]; ++i)
             s += __ldcg(&phi[(size_t)iperm[sources[i]] * stride + col]);
-        sums[col] = make_double2(s, g);
+        // The column's shift (the mean over its sources) and orientation: flipped (-1) when the
+        // whole field's mean lies below the shift.
+        const double offset = s / (double)(source_offsets[col + 1] - source_offsets[col]);
+        const double flip = (orient != 0 && g / (double)n - offset < 0.0) ? -1.0 : 1.0;
+        sums[col] = make_double2(offset, flip);
     }
 }
 
 // out[c][v] = the shifted, oriented phi of vertex v in column c (ordito/kernels/heat.py:3406).
 __global__ void shift_out_kernel(const double* __restrict__ phi, int n, int stride,
-                                 const int* __restrict__ iperm, const double2* __restrict__ sums,
-                                 const int* __restrict__ source_offsets, int k, int orient,
-                                 double* __restrict__ out) {
+                                 const int* __restrict__ iperm, const double2* __restrict__ shifts,
+                                 int k, double* __restrict__ out) {
     __shared__ double tile[32][33];
     // Tile of 32 vertices x 32 columns: read along columns (a factor row), write along vertices.
     const int v0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
@@ -337,13 +340,8 @@ __global__ void shift_out_kernel(const double* __restrict__ phi, int n, int stri
     for (int i = threadIdx.y; i < 32; i += blockDim.y) {
         const int c = c0 + i, v = v0 + threadIdx.x;
         if (v >= n || c >= k) continue;
-        const int count = source_offsets[c + 1] - source_offsets[c];
-        const double2 s = sums[c];
-        const double offset = s.x / (double)count;
-        const double value = tile[threadIdx.x][i];
-        double shifted = value - offset;
-        if (orient != 0 && s.y / (double)n - offset < 0.0) shifted = offset - value;
-        out[(size_t)c * n + v] = shifted;
+        const double2 s = shifts[c];  // (offset, +1 or -1): offset - value exactly when flipped
+        out[(size_t)c * n + v] = s.y * (tile[threadIdx.x][i] - s.x);
     }
 }
 
@@ -562,7 +560,7 @@ int ob_shift_permuted(const double* phi, int n_vertices, int stride, const int32
     const int threads = (kThreads / stride) * stride;
     const long long total = (long long)n_vertices * stride;
     const int blocks = (int)std::max(1LL, std::min((total + threads * 8 - 1) / (threads * 8),
-                                                   (long long)4 * sm_count()));
+                                                   (long long)8 * sm_count()));
     Scratch scratch(stream);
     double* partials = scratch.take<double>((size_t)blocks * stride);
     double2* sums = scratch.take<double2>(n_columns);
@@ -571,12 +569,11 @@ int ob_shift_permuted(const double* phi, int n_vertices, int stride, const int32
     if (st) return st;
     OB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned int), stream));
     shift_sums_kernel<<<blocks, threads, 0, stream>>>(phi, n_vertices, stride, iperm, sources,
-                                                       source_offsets, n_columns, partials,
+                                                       source_offsets, n_columns, orient, partials,
                                                        counter, sums);
     OB_CHECK_LAUNCH("shift_sums");
     shift_out_kernel<<<dim3(ceil_div(n_vertices, 32), ceil_div(n_columns, 32)), dim3(32, 8), 0,
-                       stream>>>(phi, n_vertices, stride, iperm, sums, source_offsets, n_columns,
-                                 orient, out);
+                       stream>>>(phi, n_vertices, stride, iperm, sums, n_columns, out);
     OB_CHECK_LAUNCH("shift_out");
     return OB_OK;
 }
