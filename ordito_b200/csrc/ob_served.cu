@@ -284,14 +284,13 @@ __global__ void shift_sums_kernel(const double* __restrict__ phi, int n, int str
     const long long total = (long long)n * stride;
     const long long step = (long long)gridDim.x * blockDim.x;  // a multiple of stride
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    // Four independent loads in flight a thread (the sum stays in index order per thread).
-    for (; t + 3 * step < total; t += 4 * step) {
-        const double a = phi[t], b = phi[t + step], d = phi[t + 2 * step],
-                     e = phi[t + 3 * step];
-        everywhere += a;
-        everywhere += b;
-        everywhere += d;
-        everywhere += e;
+    // Eight independent loads in flight a thread (the sum stays in index order per thread).
+    for (; t + 7 * step < total; t += 8 * step) {
+        double v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = phi[t + q * step];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) everywhere += v[q];
     }
     for (; t < total; t += step) everywhere += phi[t];
     tree[threadIdx.x] = everywhere;
@@ -305,9 +304,15 @@ __global__ void shift_sums_kernel(const double* __restrict__ phi, int n, int str
     // The last block: thread t folds column t % stride over blocks t / stride, t / stride + groups,
     // ... in order; the groups' sums then meet in group order (a fixed order for a launch shape).
     const int groups = blockDim.x / stride;
-    double part = 0.0;
-    for (int bx = threadIdx.x / stride; bx < (int)gridDim.x; bx += groups)
-        part += __ldcg(&partials[(size_t)bx * stride + c]);
+    // Four running sums (blocks b, b + groups, b + 2 groups, b + 3 groups of each round) so four
+    // loads are in flight, added together in a fixed order at the end.
+    double part4[4] = {0.0, 0.0, 0.0, 0.0};
+    int bx = threadIdx.x / stride;
+    for (; bx + 3 * groups < (int)gridDim.x; bx += 4 * groups)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) part4[q] += __ldcg(&partials[(size_t)(bx + q * groups) * stride + c]);
+    for (int q = 0; bx < (int)gridDim.x; bx += groups, ++q) part4[q] += __ldcg(&partials[(size_t)bx * stride + c]);
+    const double part = (part4[0] + part4[1]) + (part4[2] + part4[3]);
     __syncthreads();
     tree[threadIdx.x] = part;
     __syncthreads();
@@ -559,8 +564,8 @@ int ob_shift_permuted(const double* phi, int n_vertices, int stride, const int32
     OB_REQUIRE(stride <= kThreads, "ob_shift_permuted: stride above %d", kThreads);
     const int threads = (kThreads / stride) * stride;
     const long long total = (long long)n_vertices * stride;
-    const int blocks = (int)std::max(1LL, std::min((total + threads * 8 - 1) / (threads * 8),
-                                                   (long long)8 * sm_count()));
+    const int blocks = (int)std::max(1LL, std::min((total + threads * 16 - 1) / (threads * 16),
+                                                   (long long)2 * sm_count()));
     Scratch scratch(stream);
     double* partials = scratch.take<double>((size_t)blocks * stride);
     double2* sums = scratch.take<double2>(n_columns);
