@@ -20,7 +20,7 @@ INCLUDE = HERE.parent / "include"
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-mavx2,-mfma", "--expt-relaxed-constexpr",
          f"-I{INCLUDE}"]
 
 
@@ -30,7 +30,9 @@ def _headers() -> list[Path]:
 
 def _compile(source: Path, verbose: bool) -> Path:
     obj = BUILD / (source.stem + ".o")
-    newest = max([source.stat().st_mtime] + [h.stat().st_mtime for h in _headers()])
+    # This file holds the flags: a change to it rebuilds every object.
+    newest = max([source.stat().st_mtime, Path(__file__).stat().st_mtime] +
+                 [h.stat().st_mtime for h in _headers()])
     if obj.exists() and obj.stat().st_mtime >= newest:
         return obj
     cmd = [NVCC, *ARCH, *FLAGS, "-c", str(source), "-o", str(obj)]

@@ -361,6 +361,67 @@ constexpr int kThreadedFront = 384;
 
 // Dense partial Cholesky of the m x m column-major front F (lower part used): the first nc
 // columns are factored in place (L11, L21) and F22 becomes the Schur complement.
+// C -= A B^T on column-major blocks: C(i, j) at C[j * ldc + i] for i < M, j < N, A(i, kk) at
+// A[kk * lda + i], B(j, kk) at B[kk * ldb + j], kk < K. Register-blocked 8 x 4: each inner step
+// loads 8 consecutive rows of A's column kk and 4 entries of B's column kk and does 32
+// multiply-adds in registers (eight 4-wide vector accumulators), so the dense host work of the
+// factorisation streams from cache instead of re-reading a column per axpy. The sum over kk runs
+// in order for every entry.
+typedef double v4d __attribute__((vector_size(32)));
+
+inline void gemm_block_8x4(double* C, int ldc, const double* A, int lda, const double* B, int ldb, int K) {
+    v4d acc[4][2] = {};
+    for (int kk = 0; kk < K; ++kk) {
+        v4d a0, a1;
+        __builtin_memcpy(&a0, A + (size_t)kk * lda, sizeof(v4d));
+        __builtin_memcpy(&a1, A + (size_t)kk * lda + 4, sizeof(v4d));
+        const double* b = B + (size_t)kk * ldb;
+#pragma GCC unroll 4
+        for (int c = 0; c < 4; ++c) {
+            const v4d bc = {b[c], b[c], b[c], b[c]};
+            acc[c][0] += a0 * bc;
+            acc[c][1] += a1 * bc;
+        }
+    }
+#pragma GCC unroll 4
+    for (int c = 0; c < 4; ++c) {
+        double* out = C + (size_t)c * ldc;
+        v4d o0, o1;
+        __builtin_memcpy(&o0, out, sizeof(v4d));
+        __builtin_memcpy(&o1, out + 4, sizeof(v4d));
+        o0 -= acc[c][0];
+        o1 -= acc[c][1];
+        __builtin_memcpy(out, &o0, sizeof(v4d));
+        __builtin_memcpy(out + 4, &o1, sizeof(v4d));
+    }
+}
+
+void gemm_nt_minus(double* C, int ldc, const double* A, int lda, const double* B, int ldb, int M, int N,
+                   int K) {
+    constexpr int kR = 8, kC = 4;
+    for (int j0 = 0; j0 < N; j0 += kC) {
+        const int nj = std::min(kC, N - j0);
+        for (int i0 = 0; i0 < M; i0 += kR) {
+            const int ni = std::min(kR, M - i0);
+            if (ni == kR && nj == kC) {
+                gemm_block_8x4(C + (size_t)j0 * ldc + i0, ldc, A + i0, lda, B + j0, ldb, K);
+                continue;
+            }
+            double acc[kC][kR] = {};
+            for (int kk = 0; kk < K; ++kk) {
+                const double* a = A + (size_t)kk * lda + i0;
+                const double* b = B + (size_t)kk * ldb + j0;
+                for (int c = 0; c < nj; ++c)
+                    for (int r = 0; r < ni; ++r) acc[c][r] += a[r] * b[c];
+            }
+            for (int c = 0; c < nj; ++c) {
+                double* out = C + (size_t)(j0 + c) * ldc + i0;
+                for (int r = 0; r < ni; ++r) out[r] -= acc[c][r];
+            }
+        }
+    }
+}
+
 bool partial_cholesky(double* F, int m, int nc) {
     constexpr int kBlock = 48;
     for (int j0 = 0; j0 < nc; j0 += kBlock) {
@@ -381,19 +442,34 @@ bool partial_cholesky(double* F, int m, int nc) {
                     for (int i = k; i < m; ++i) ck[i] -= cj[i] * f;
             }
         }
-        // Update every later column with the panel: F[k:, k] -= L[k:, j0:j1] L[k, j0:j1]^T
-        // (independent columns: threaded on a large front).
-        parallel_range(m - j1, m >= kThreadedFront, [&](long long begin, long long end) {
-            for (int k = j1 + (int)begin; k < j1 + (int)end; ++k) {
-                double* ck = F + (size_t)k * m;
-                for (int j = j0; j < j1; ++j) {
-                    const double* cj = F + (size_t)j * m;
-                    const double f = cj[k];
-                    if (f != 0.0)
-                        for (int i = k; i < m; ++i) ck[i] -= cj[i] * f;
-                }
+        // Update every later column with the panel: F[k:, k] -= L[k:, j0:j1] L[k, j0:j1]^T, in
+        // blocks of 4 columns (rows from the block's first column down; the few entries above
+        // the diagonal it also writes are never read). On a large front the blocks are split
+        // over host threads in ranges of equal work (a column's work falls with its index).
+        const int blocks = (m - j1 + 3) / 4;
+        auto update = [&](int b0, int b1) {
+            for (int b = b0; b < b1; ++b) {
+                const int k0 = j1 + 4 * b, nk = std::min(4, m - k0);
+                gemm_nt_minus(F + (size_t)k0 * m + k0, m, F + (size_t)j0 * m + k0, m, F + (size_t)j0 * m + k0, m,
+                              m - k0, nk, j1 - j0);
             }
-        });
+        };
+        const int parts = m >= kThreadedFront ? std::min(host_threads(), std::max(1, blocks / 8)) : 1;
+        if (parts <= 1) {
+            update(0, blocks);
+        } else {
+            // Block b costs about (m - j1 - 4 b); cut where the running cost crosses p / parts.
+            std::vector<int> cut(parts + 1, blocks);
+            cut[0] = 0;
+            const double total = 0.5 * (double)blocks * (2.0 * (m - j1) - 4.0 * (blocks - 1));
+            double run = 0.0;
+            int next = 1;
+            for (int b = 0; b < blocks && next < parts; ++b) {
+                run += (double)(m - j1 - 4 * b);
+                if (run >= total * next / parts) cut[next++] = b + 1;
+            }
+            run_parts(parts, [&](int p) { update(cut[p], cut[p + 1]); });
+        }
     }
     return true;
 }
@@ -438,41 +514,48 @@ int factor_node(const Analysis& A, const double* values, int s, bool singular, H
         H.update[c].shrink_to_fit();
     }
     if (!partial_cholesky(F.data(), m, nc)) return OB_ERR_INDEFINITE;
-    // Inverse of L11 (lower triangular): column c of X = L^-1 by forward substitution, each step
-    // an axpy down a contiguous column of L (independent columns: threaded on a large front),
-    // then stored row-major.
-    std::vector<double> X((size_t)nc * nc, 0.0);
-    parallel_range(nc, m >= kThreadedFront, [&](long long begin, long long end) {
-        for (int c = (int)begin; c < (int)end; ++c) {
-            double* x = X.data() + (size_t)c * nc;
-            x[c] = 1.0;
-            for (int k = c; k < nc; ++k) {
-                const double* lk = F.data() + (size_t)k * m;
-                const double xk = x[k] / lk[k];
-                x[k] = xk;
-                if (xk != 0.0)
-                    for (int i = k + 1; i < nc; ++i) x[i] -= xk * lk[i];
-            }
+    // Inverse of L11 (lower triangular), row-major, by block forward substitution over rows:
+    // rows [i0, i1) of X = L^-1 are first reduced by the rows above them (X[I, :] -= L[I, 0:i0]
+    // X[0:i0, :], one blocked product, threaded over columns on a large front), then solved
+    // row by row against the diagonal block.
+    constexpr int kInvBlock = 48;
+    std::vector<double> inv((size_t)nc * nc, 0.0);
+    for (int i = 0; i < nc; ++i) inv[(size_t)i * nc + i] = 1.0;
+    for (int i0 = 0; i0 < nc; i0 += kInvBlock) {
+        const int i1 = std::min(nc, i0 + kInvBlock);
+        if (i0 > 0) {
+            // Transposed view: C(c, i) = inv[i][c] -= sum_kk inv[kk][c] L[i][kk] for the columns
+            // c < i0 that rows above can reach; threaded over columns on a large front.
+            parallel_range(i0, m >= kThreadedFront, [&](long long begin, long long end) {
+                gemm_nt_minus(inv.data() + (size_t)i0 * nc + begin, nc, inv.data() + begin, nc, F.data() + i0, m,
+                              (int)(end - begin), i1 - i0, i0);
+            });
         }
-    });
-    std::vector<double> inv((size_t)nc * nc);
-    for (int c = 0; c < nc; ++c)
-        for (int i = 0; i < nc; ++i) inv[(size_t)i * nc + c] = X[(size_t)c * nc + i];
+        for (int i = i0; i < i1; ++i) {
+            double* xi = inv.data() + (size_t)i * nc;
+            for (int kk = i0; kk < i; ++kk) {
+                const double l = F[(size_t)kk * m + i];
+                if (l == 0.0) continue;
+                const double* xk = inv.data() + (size_t)kk * nc;
+                for (int c = 0; c <= kk; ++c) xi[c] -= l * xk[c];
+            }
+            const double d = F[(size_t)i * m + i];
+            for (int c = 0; c <= i; ++c) xi[c] /= d;
+        }
+    }
     // The off-diagonal block the solves use, G = -L21 L11^-1 (row r: minus the row of L21 times
     // the lower-triangular inverse): with it both of a node's products in each direction read
     // only inputs that are final when its level starts -- forward y1 = L11^-1 b1 and b2 += G b1,
     // backward x1 = L11^-T y1 + G^T x2 -- so a tree level is one launch a direction.
+    // Transposed view: C(i, r) = G[r][i] -= sum_k inv[k][i] L21[r][k] (L21[r][k] = F column k,
+    // row nc + r), for 8 entries i at a time over k >= i only (inv is lower triangular); threaded
+    // over rows of G on a large front.
     std::vector<double> G((size_t)noff * nc, 0.0);
     parallel_range(noff, m >= kThreadedFront, [&](long long begin, long long end) {
-        for (int r = (int)begin; r < (int)end; ++r) {
-            double* g = G.data() + (size_t)r * nc;
-            for (int k = 0; k < nc; ++k) {
-                const double a = F[(size_t)k * m + nc + r];
-                if (a == 0.0) continue;
-                const double* row = inv.data() + (size_t)k * nc;  // inverse row k: columns 0..k
-                for (int i = 0; i <= k; ++i) g[i] -= a * row[i];
-            }
-        }
+        for (int i0 = 0; i0 < nc; i0 += 8)
+            gemm_nt_minus(G.data() + (size_t)begin * nc + i0, nc, inv.data() + (size_t)i0 * nc + i0, nc,
+                          F.data() + (size_t)i0 * m + nc + begin, m, std::min(8, nc - i0), (int)(end - begin),
+                          nc - i0);
     });
     H.inv[s] = std::move(inv);
     H.off[s] = std::move(G);

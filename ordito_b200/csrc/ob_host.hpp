@@ -25,4 +25,16 @@ void parallel_range(long long n, bool large, Fn fn) {
     for (auto& th : pool) th.join();
 }
 
+// Host threads parallel_range would use for a large job.
+inline int host_threads() { return (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency())); }
+
+// Runs fn(p) for p in [0, parts) on `parts` host threads (the caller's thread takes part 0).
+template <typename Fn>
+void run_parts(int parts, Fn fn) {
+    std::vector<std::thread> pool;
+    for (int p = 1; p < parts; ++p) pool.emplace_back([=]() { fn(p); });
+    if (parts > 0) fn(0);
+    for (auto& th : pool) th.join();
+}
+
 }  // namespace ob
