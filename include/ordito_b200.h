@@ -103,6 +103,31 @@ int ob_pattern_build(const int32_t* faces, int n_faces, int n_vertices, int32_t*
 int ob_face_terms(const float* xyz, const int32_t* faces, int n_faces, int n_vertices, float* cot,
                   float* normals, float* areas, double* area_sums, ob_stream_t stream);
 
+/* ---- method="igl" and method="potpourri3d": the operators' variants ---------------------------
+ * ob_voronoi_area_sums replaces kernels/heat.py:92 heat_face_terms at voronoi_mass = 1 (with
+ * kernels/triangles.py:276 face_voronoi_areas): area_sums[V] (zeroed here) gets each corner's
+ * Voronoi share of its face (Meyer et al.'s mixed areas: circumcentric split of a non-obtuse face,
+ * half to an obtuse corner and a quarter to the others, an even split of a degenerate face),
+ * formed in float64, rounded to float32 and added exactly in float64 -- the lumped mass itself
+ * (mass divisor 1 in ob_heat_rows).
+ * ob_rim_vertices replaces kernels/heat.py:469 rim_vertices: rim[V] = 1 where a vertex has an edge
+ * on a single face (a run of one key in the cotmatrix pattern), *n_rim (device) their count.
+ * ob_pinned_rows replaces kernels/heat.py:488 pinned_heat_rows: the heat system with the solution
+ * pinned to zero on the rim (rim rows the identity's, rim columns dropped), over the same pattern.
+ * ob_off_rim replaces kernels/heat.py:512 off_rim: out = in, zero on the rim.
+ * ob_add_to_diagonal replaces the add_to_diagonal kernel of heat.py:4098 (geometry-central's
+ * regularized Poisson system -L + 1e-6 I): out = values with shift added to the diagonal. */
+int ob_voronoi_area_sums(const float* xyz, const int32_t* faces, int n_faces, int n_vertices,
+                         double* area_sums, ob_stream_t stream);
+int ob_rim_vertices(const int32_t* offsets, const int32_t* columns, const int32_t* run_start,
+                    const uint64_t* keys, int count, int n_vertices, int32_t* rim, int32_t* n_rim,
+                    ob_stream_t stream);
+int ob_pinned_rows(const int32_t* offsets, const int32_t* columns, const int32_t* rim, const double* values,
+                   int n_vertices, double* out, ob_stream_t stream);
+int ob_off_rim(const double* in, const int32_t* rim, int n_vertices, double* out, ob_stream_t stream);
+int ob_add_to_diagonal(const int32_t* offsets, const int32_t* columns, const double* values, int n_vertices,
+                       double shift, double* out, ob_stream_t stream);
+
 /* ---- a4: edge-length sums for the default time step -----------------------------------------
  * Replaces kernels/heat.py:173 upper_edge_length_sum_and_count (heat.py:2248 _edge_length_sums):
  * out[0] = sum of weight * |v_col - v_row| over the strict upper triangle, out[1] = sum of

@@ -214,6 +214,51 @@ def area_sums(faces: np.ndarray, areas: np.ndarray, n_vertices: int) -> np.ndarr
     return out
 
 
+def voronoi_area_sums(vertices: np.ndarray, faces: np.ndarray, n_vertices: int) -> np.ndarray:
+    """Each corner's Voronoi share of its face, added in float64: the ``method="igl"`` lumped mass
+    (kernels/triangles.py:276-330 face_voronoi_areas, kernels/heat.py:128-129).
+
+    Shares are formed in float64 from the float32 corners (Meyer et al.'s mixed areas: the
+    circumcentric split of a non-obtuse face, half to an obtuse corner and a quarter to each other,
+    an even split of a face with a zero-length edge or zero circumcentre weights) and rounded once
+    to float32.
+    """
+    v = np.asarray(vertices, dtype=F32).reshape(-1, 3)
+    f = np.asarray(faces, dtype=np.int64).reshape(-1, 3)
+    p0, p1, p2 = (v[f[:, e]].astype(F64) for e in range(3))
+
+    def length(a: np.ndarray) -> np.ndarray:
+        return np.sqrt(a[:, 0] * a[:, 0] + a[:, 1] * a[:, 1] + a[:, 2] * a[:, 2])
+
+    l0, l1, l2 = length(p1 - p2), length(p2 - p0), length(p0 - p1)
+    area = 0.5 * length(np.cross(p1 - p0, p2 - p0))
+    q = np.repeat((area / 3.0)[:, None], 3, axis=1)
+    with np.errstate(all="ignore"):
+        ok = (l0 > 0) & (l1 > 0) & (l2 > 0)
+        c0 = (l2 * l2 + l1 * l1 - l0 * l0) / (2.0 * l1 * l2)
+        c1 = (l0 * l0 + l2 * l2 - l1 * l1) / (2.0 * l2 * l0)
+        c2 = (l1 * l1 + l0 * l0 - l2 * l2) / (2.0 * l0 * l1)
+        b0, b1, b2 = c0 * l0, c1 * l1, c2 * l2
+        weight = b0 + b1 + b2
+        split = ok & (weight != 0.0)
+        p_0, p_1, p_2 = b0 / weight * area, b1 / weight * area, b2 / weight * area
+        circ = np.stack([0.5 * (p_1 + p_2), 0.5 * (p_2 + p_0), 0.5 * (p_0 + p_1)], axis=1)
+    q[split] = circ[split]
+    half, quarter = 0.5 * area, 0.25 * area
+    for corner, c in enumerate((c0, c1, c2)):
+        obtuse = ok & (c < 0.0)
+        if corner > 0:
+            obtuse &= ~np.any(np.stack([c0, c1, c2][:corner], axis=1) < 0.0, axis=1)
+        share = np.repeat(quarter[:, None], 3, axis=1)
+        share[:, corner] = half
+        q[obtuse] = share[obtuse]
+    q = q.astype(F32).astype(F64)
+    out = np.zeros(n_vertices, dtype=F64)
+    for e in range(3):
+        np.add.at(out, f[:, e], q[:, e])
+    return out
+
+
 # --------------------------------------------------------------------------------------------
 # Time step: kernels/heat.py:143-237 (upper_edge_length_sum_and_count), kernels/linalg.py:1594
 # (shift_factor), heat.py:3714-3736 (_vertex_time), :5228-5243 (_diffusion_floor, _settle_window).
@@ -276,9 +321,17 @@ def settle_window(t: float | None, default: float) -> int:
     return math.ceil(HEAT_SETTLE_ROUNDS * math.sqrt(t / default))
 
 
-def vertex_time(vertices: np.ndarray, faces: np.ndarray, t: float | None) -> tuple[float | None, int]:
-    """``HeatSolver._vertex_time`` for ``method="meshlab"`` (heat.py:3714-3736)."""
-    mean = mean_face_edge_length(vertices, faces)
+def vertex_time(vertices: np.ndarray, faces: np.ndarray, t: float | None,
+                method: str = "meshlab") -> tuple[float | None, int]:
+    """``HeatSolver._vertex_time`` (heat.py:3714-3736): the mean over every face's three edges for
+    ``"meshlab"``, over the unique edges for ``"igl"`` and ``"potpourri3d"``."""
+    if method == "meshlab":
+        mean = mean_face_edge_length(vertices, faces)
+    else:
+        v = np.asarray(vertices, dtype=F32).reshape(-1, 3)
+        f = np.asarray(faces, dtype=np.int64).reshape(-1, 3)
+        total, count = edge_length_sums(v, mesh_operator_pattern(f, v.shape[0]), face_edges=False)
+        mean = total / count if count > 0 else 0.0
     default = mean**2
     if t is None:
         floor = diffusion_floor(vertices)
@@ -293,9 +346,12 @@ def vertex_time(vertices: np.ndarray, faces: np.ndarray, t: float | None) -> tup
 
 
 def heat_operators(
-    vertices: np.ndarray, faces: np.ndarray, t: float | None = None, *, mass_divisor: float = 3.0
+    vertices: np.ndarray, faces: np.ndarray, t: float | None = None, *, mass_divisor: float = 3.0,
+    method: str = "meshlab",
 ) -> dict[str, object]:
-    """The ``"meshlab"`` heat operators over the cotmatrix pattern (heat.py:2015-2245).
+    """The heat operators over the cotmatrix pattern (heat.py:2015-2245): barycentric mass and
+    the face-edge time step for ``"meshlab"``, the unique-edge time step for ``"potpourri3d"``,
+    the Voronoi mass (divisor 1) and the unique-edge time step for ``"igl"`` (heat.py:2002-2012).
 
     Returns the pattern, the float32 cot table, normals, areas, area sums, ``L``, ``H = M - t L``,
     ``P = -L`` (float64 values over the pattern), the lumped mass and the time ``t`` used.
@@ -306,9 +362,13 @@ def heat_operators(
     pattern = mesh_operator_pattern(f, n)
     cot = cotmatrix_entries(v, f)
     normals, areas = face_normals_and_areas(v, f)
-    sums = area_sums(f, areas, n)
+    if method == "igl":
+        sums = voronoi_area_sums(v, f, n)
+        mass_divisor = 1.0
+    else:
+        sums = area_sums(f, areas, n)
     if t is None:
-        total, count = edge_length_sums(v, pattern, face_edges=True)
+        total, count = edge_length_sums(v, pattern, face_edges=method == "meshlab")
         h = total / count if count > 0 else 0.0
         factor = -1.0 * (h * h)
         t_used = h * h
@@ -484,6 +544,47 @@ class PoissonFactor:
         return out
 
 
+def rim_vertices(pattern: dict[str, np.ndarray]) -> np.ndarray:
+    """1 where a vertex has an edge on a single face: one of its off-diagonal entries' runs holds
+    one key (kernels/heat.py:469-485, kernels/laplacian.py:1286-1321)."""
+    offsets = pattern["offsets"]
+    n = offsets.size - 1
+    columns = pattern["columns"][: offsets[-1]].astype(np.int64)
+    rows = np.repeat(np.arange(n), np.diff(offsets))
+    rs = pattern["run_start"][: offsets[-1]].astype(np.int64)
+    single = (run_ends(pattern["keys"], rs) - rs) == 1
+    rim = np.zeros(n, dtype=np.int32)
+    rim[rows[(columns != rows) & single]] = 1
+    return rim
+
+
+def pinned_heat_values(pattern: dict[str, np.ndarray], H: np.ndarray, rim: np.ndarray) -> np.ndarray:
+    """The heat system pinned to zero on the rim: rim rows the identity's, rim columns dropped
+    (kernels/heat.py:488-509)."""
+    offsets = pattern["offsets"]
+    n = offsets.size - 1
+    columns = pattern["columns"][: offsets[-1]].astype(np.int64)
+    rows = np.repeat(np.arange(n), np.diff(offsets))
+    out = np.asarray(H[: offsets[-1]], dtype=F64).copy()
+    out[rim[columns] != 0] = 0.0
+    on = rim[rows] != 0
+    out[on] = np.where(columns[on] == rows[on], 1.0, 0.0)
+    return out
+
+
+GEOMETRY_CENTRAL_POISSON_SHIFT = 1e-6  # heat.py:4090 (the +1e-6 I of HeatMethodDistanceSolver)
+
+
+def solve_regularized_poisson(pattern: dict[str, np.ndarray], P: np.ndarray, rhs: np.ndarray) -> np.ndarray:
+    """``(-L + 1e-6 I) phi = rhs`` directly (heat.py:4086-4116); empty rows stay zero."""
+    offsets = pattern["offsets"]
+    n = offsets.size - 1
+    columns = pattern["columns"][: offsets[-1]].astype(np.int64)
+    rows = np.repeat(np.arange(n), np.diff(offsets))
+    values = np.asarray(P[: offsets[-1]], dtype=F64) + np.where(columns == rows, GEOMETRY_CENTRAL_POISSON_SHIFT, 0.0)
+    return solve_heat(csr_matrix(pattern, values), rhs)
+
+
 def heat_geodesic(
     vertices: np.ndarray,
     faces: np.ndarray,
@@ -492,10 +593,14 @@ def heat_geodesic(
     *,
     operators: dict[str, object] | None = None,
     factors: tuple[object, PoissonFactor] | None = None,
+    method: str = "meshlab",
 ) -> np.ndarray:
-    """``heat_geodesic(vertices, faces, sources)``, ``method="meshlab"`` (heat.py:391-588).
+    """``heat_geodesic(vertices, faces, sources, method=...)`` (heat.py:391-588).
 
-    Both solves are direct. ``operators``/``factors`` may be passed to reuse them across queries.
+    Both solves are direct. ``"igl"`` averages the Neumann heat with the heat pinned to zero on
+    the rim when the mesh has one (heat.py:594-597, 4153-4198); ``"potpourri3d"`` solves
+    geometry-central's regularized Poisson system (heat.py:3124-3129). ``operators``/``factors``
+    may be passed to reuse them across queries (``factors`` for ``"meshlab"`` only).
     """
     v = np.asarray(vertices, dtype=F32).reshape(-1, 3)
     f = np.asarray(faces, dtype=np.int64).reshape(-1, 3)
@@ -505,18 +610,27 @@ def heat_geodesic(
         return np.zeros(n, dtype=F64)
     u0 = seed(src, n)
     if operators is None:
-        t_eff, _ = vertex_time(v, f, t)
-        operators = heat_operators(v, f, t_eff)
+        t_eff, _ = vertex_time(v, f, t, method)
+        operators = heat_operators(v, f, t_eff, method=method)
     ops = operators
     pattern = ops["pattern"]
     if factors is None:
         H = csr_matrix(pattern, ops["H"])
         P = csr_matrix(pattern, ops["P"])
         heat_lu = HeatFactor(H)
-        factors = (heat_lu, PoissonFactor(P))
+        factors = (heat_lu, PoissonFactor(P) if method != "potpourri3d" else None)
     heat = factors[0].solve(u0)
+    if method == "igl":
+        rim = rim_vertices(pattern)
+        if rim.any():
+            pinned = solve_heat(csr_matrix(pattern, pinned_heat_values(pattern, ops["H"], rim)),
+                                np.where(rim != 0, 0.0, u0))
+            heat = 0.5 * (heat + pinned)
     neg_div = unit_gradient_divergence(v, f, ops["normals"], ops["areas"], heat, ops["cot"])
-    phi = factors[1].solve(neg_div)
+    if method == "potpourri3d":
+        phi = solve_regularized_poisson(pattern, ops["P"], neg_div)
+    else:
+        phi = factors[1].solve(neg_div)
     return shift_to_sources(phi, src)
 
 

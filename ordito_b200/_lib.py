@@ -66,6 +66,11 @@ SIGNATURES: dict[str, list] = {
     "ob_pattern_workspace": [I, I, POINTER(c_size_t)],
     "ob_pattern_build": [P, I, I, P, P, P, P, P, P, c_size_t, P],
     "ob_face_terms": [P, P, I, I, P, P, P, P, P],
+    "ob_voronoi_area_sums": [P, P, I, I, P, P],
+    "ob_rim_vertices": [P, P, P, P, I, I, P, P, P],
+    "ob_pinned_rows": [P, P, P, P, I, P, P],
+    "ob_off_rim": [P, P, I, P, P],
+    "ob_add_to_diagonal": [P, P, P, I, D, P, P],
     "ob_edge_sums": [P, P, P, P, I, I, P, I, P, P],
     "ob_heat_rows": [P, P, P, P, I, P, I, P, D, P, I, P, D, P, P, P, P, P],
     "ob_seed": [P, I, I, P, P, P],

@@ -193,12 +193,181 @@ __global__ void edge_sums_segments_kernel(const int* __restrict__ offsets, const
     }
 }
 
+// ordito/kernels/triangles.py:276-330 (face_voronoi_areas): Meyer et al.'s mixed areas per
+// corner, formed in float64 from the float32 corners and rounded once to float32 -- a non-obtuse
+// face splits by its circumcentre weights, an obtuse one gives half its area to the obtuse
+// corner and a quarter to each other, a degenerate one splits evenly -- and each share added
+// exactly (float64 of the float32) into its corner's sum (kernels/heat.py:128-131).
+__global__ void voronoi_area_sums_kernel(const float* __restrict__ xyz, const int* __restrict__ faces,
+                                         int n_faces, double* __restrict__ area_sums) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n_faces) return;
+    const int i0 = faces[3 * f], i1 = faces[3 * f + 1], i2 = faces[3 * f + 2];
+    const f3 a = load_f3(xyz, i0), b = load_f3(xyz, i1), c = load_f3(xyz, i2);
+    const double p0x = a.x, p0y = a.y, p0z = a.z, p1x = b.x, p1y = b.y, p1z = b.z;
+    const double p2x = c.x, p2y = c.y, p2z = c.z;
+    auto length = [](double x, double y, double z) { return sqrt(x * x + y * y + z * z); };
+    const double l0 = length(p1x - p2x, p1y - p2y, p1z - p2z);
+    const double l1 = length(p2x - p0x, p2y - p0y, p2z - p0z);
+    const double l2 = length(p0x - p1x, p0y - p1y, p0z - p1z);
+    const double ex = p1x - p0x, ey = p1y - p0y, ez = p1z - p0z;
+    const double fx = p2x - p0x, fy = p2y - p0y, fz = p2z - p0z;
+    const double area = 0.5 * length(ey * fz - ez * fy, ez * fx - ex * fz, ex * fy - ey * fx);
+    const double even = area / 3.0;
+    double q0 = even, q1 = even, q2 = even;
+    if (l0 > 0.0 && l1 > 0.0 && l2 > 0.0) {
+        const double c0 = (l2 * l2 + l1 * l1 - l0 * l0) / (2.0 * l1 * l2);
+        const double c1 = (l0 * l0 + l2 * l2 - l1 * l1) / (2.0 * l2 * l0);
+        const double c2 = (l1 * l1 + l0 * l0 - l2 * l2) / (2.0 * l0 * l1);
+        const double b0 = c0 * l0, b1 = c1 * l1, b2 = c2 * l2;
+        const double weight = b0 + b1 + b2;
+        if (weight != 0.0) {
+            const double partial0 = b0 / weight * area, partial1 = b1 / weight * area;
+            const double partial2 = b2 / weight * area;
+            q0 = 0.5 * (partial1 + partial2);
+            q1 = 0.5 * (partial2 + partial0);
+            q2 = 0.5 * (partial0 + partial1);
+        }
+        const double half = 0.5 * area, quarter = 0.25 * area;
+        if (c0 < 0.0) {
+            q0 = half;
+            q1 = quarter;
+            q2 = quarter;
+        } else if (c1 < 0.0) {
+            q0 = quarter;
+            q1 = half;
+            q2 = quarter;
+        } else if (c2 < 0.0) {
+            q0 = quarter;
+            q1 = quarter;
+            q2 = half;
+        }
+    }
+    atomicAdd(&area_sums[i0], (double)(float)q0);
+    atomicAdd(&area_sums[i1], (double)(float)q1);
+    atomicAdd(&area_sums[i2], (double)(float)q2);
+}
+
+// ordito/kernels/heat.py:469-485 (rim_vertices) with kernels/laplacian.py:1286-1321
+// (pattern_row_on_rim): a vertex is on the rim when one of its off-diagonal entries' runs holds a
+// single corner key (that edge lies on one face); their count is added to *n_rim.
+__global__ void rim_vertices_kernel(const int* __restrict__ offsets, const int* __restrict__ columns,
+                                    const int* __restrict__ run_start, const unsigned long long* __restrict__ keys,
+                                    int count, int n, int* __restrict__ rim, int* __restrict__ n_rim) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int on_rim = 0;
+    for (int k = offsets[i]; k < offsets[i + 1] && !on_rim; ++k)
+        if (columns[k] != i && run_end(keys, run_start[k], count) - run_start[k] == 1) on_rim = 1;
+    rim[i] = on_rim;
+    if (on_rim) atomicAdd(n_rim, 1);
+}
+
+// ordito/kernels/heat.py:488-509 (pinned_heat_rows): the heat system with the solution pinned to
+// zero on the rim -- a rim row becomes the identity's, an interior row drops its rim columns.
+__global__ void pinned_rows_kernel(const int* __restrict__ offsets, const int* __restrict__ columns,
+                                   const int* __restrict__ rim, const double* __restrict__ values, int n,
+                                   double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int k = offsets[i]; k < offsets[i + 1]; ++k) {
+        const int c = columns[k];
+        double v = values[k];
+        if (rim[i] != 0)
+            v = (c == i) ? 1.0 : 0.0;
+        else if (rim[c] != 0)
+            v = 0.0;
+        out[k] = v;
+    }
+}
+
+// kernels/heat.py:512-515 (off_rim): the pinned solve's right-hand side, zero on the rim.
+__global__ void off_rim_kernel(const double* __restrict__ in, const int* __restrict__ rim, int n,
+                               double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = rim[i] != 0 ? 0.0 : in[i];
+}
+
+// ordito/heat.py:4098-4114 (add_to_diagonal): values + shift on the diagonal entries.
+__global__ void add_to_diagonal_kernel(const int* __restrict__ offsets, const int* __restrict__ columns,
+                                       const double* __restrict__ values, int n, double shift,
+                                       double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int k = offsets[i]; k < offsets[i + 1]; ++k) out[k] = values[k] + (columns[k] == i ? shift : 0.0);
+}
+
 }  // namespace
 }  // namespace ob
 
 using namespace ob;
 
 extern "C" {
+
+int ob_voronoi_area_sums(const float* xyz, const int32_t* faces, int n_faces, int n_vertices,
+                         double* area_sums, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_faces >= 0 && n_vertices >= 0, "ob_voronoi_area_sums: negative size");
+    if (n_vertices > 0) {
+        OB_REQUIRE(area_sums != nullptr, "ob_voronoi_area_sums: null area_sums");
+        OB_CUDA(cudaMemsetAsync(area_sums, 0, sizeof(double) * (size_t)n_vertices, stream));
+    }
+    if (n_faces == 0) return OB_OK;
+    OB_REQUIRE(xyz && faces, "ob_voronoi_area_sums: null pointer");
+    voronoi_area_sums_kernel<<<ceil_div(n_faces, kThreads), kThreads, 0, stream>>>(xyz, faces, n_faces,
+                                                                                   area_sums);
+    OB_CHECK_LAUNCH("voronoi_area_sums");
+    return OB_OK;
+}
+
+int ob_rim_vertices(const int32_t* offsets, const int32_t* columns, const int32_t* run_start,
+                    const uint64_t* keys, int count, int n_vertices, int32_t* rim, int32_t* n_rim,
+                    ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_vertices >= 0 && n_rim != nullptr, "ob_rim_vertices: bad argument");
+    OB_CUDA(cudaMemsetAsync(n_rim, 0, sizeof(int32_t), stream));
+    if (n_vertices == 0) return OB_OK;
+    OB_REQUIRE(offsets && columns && run_start && keys && rim, "ob_rim_vertices: null pointer");
+    rim_vertices_kernel<<<ceil_div(n_vertices, kThreads), kThreads, 0, stream>>>(
+        offsets, columns, run_start, reinterpret_cast<const unsigned long long*>(keys), count, n_vertices, rim,
+        n_rim);
+    OB_CHECK_LAUNCH("rim_vertices");
+    return OB_OK;
+}
+
+int ob_pinned_rows(const int32_t* offsets, const int32_t* columns, const int32_t* rim, const double* values,
+                   int n_vertices, double* out, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_vertices >= 0, "ob_pinned_rows: negative size");
+    if (n_vertices == 0) return OB_OK;
+    OB_REQUIRE(offsets && columns && rim && values && out, "ob_pinned_rows: null pointer");
+    pinned_rows_kernel<<<ceil_div(n_vertices, kThreads), kThreads, 0, stream>>>(offsets, columns, rim, values,
+                                                                                 n_vertices, out);
+    OB_CHECK_LAUNCH("pinned_rows");
+    return OB_OK;
+}
+
+int ob_off_rim(const double* in, const int32_t* rim, int n_vertices, double* out, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_vertices >= 0, "ob_off_rim: negative size");
+    if (n_vertices == 0) return OB_OK;
+    OB_REQUIRE(in && rim && out, "ob_off_rim: null pointer");
+    off_rim_kernel<<<ceil_div(n_vertices, kThreads), kThreads, 0, stream>>>(in, rim, n_vertices, out);
+    OB_CHECK_LAUNCH("off_rim");
+    return OB_OK;
+}
+
+int ob_add_to_diagonal(const int32_t* offsets, const int32_t* columns, const double* values, int n_vertices,
+                       double shift, double* out, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_vertices >= 0, "ob_add_to_diagonal: negative size");
+    if (n_vertices == 0) return OB_OK;
+    OB_REQUIRE(offsets && columns && values && out, "ob_add_to_diagonal: null pointer");
+    add_to_diagonal_kernel<<<ceil_div(n_vertices, kThreads), kThreads, 0, stream>>>(offsets, columns, values,
+                                                                                     n_vertices, shift, out);
+    OB_CHECK_LAUNCH("add_to_diagonal");
+    return OB_OK;
+}
 
 int ob_face_terms(const float* xyz, const int32_t* faces, int n_faces, int n_vertices, float* cot,
                   float* normals, float* areas, double* area_sums, ob_stream_t stream_) {

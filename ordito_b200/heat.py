@@ -42,6 +42,7 @@ _HEAT_CHECK_ROUNDS = 16  # :142
 _HEAT_CHANGE_TOLERANCE = 1e-6  # :146
 _HEAT_SETTLE_ROUNDS = 192  # :147
 _DIFFUSION_DECAY = 400.0  # :158
+_GEOMETRY_CENTRAL_POISSON_SHIFT = 1e-6  # :193 (geometry-central's Poisson system -L + 1e-6 I)
 
 
 class HeatOperators(NamedTuple):
@@ -69,16 +70,14 @@ def _heat_method_choices(method: str) -> tuple[str, str]:
 
 
 def _supported(method: str, use_robust: bool) -> None:
-    mass, _ = _heat_method_choices(method)
-    if mass == "voronoi":
-        raise NotImplementedError("method='igl' (Voronoi mass, rim-pinned heat) is not built yet")
+    _heat_method_choices(method)
     if use_robust:
         raise NotImplementedError("use_robust (mollified / intrinsic operators) is not built yet")
 
 
 def _assemble(mesh: Trimesh, t: float | None, method: str, cot_entries: Any = None,
               pattern: MeshOperatorPattern | None = None) -> tuple[HeatOperators, Any]:
-    _, timestep = _heat_method_choices(method)
+    mass, timestep = _heat_method_choices(method)
     if pattern is None:
         pattern = mesh.mesh_operator_pattern
     elif pattern.n_vertices != mesh.n_vertices or pattern.operator != "cotmatrix":
@@ -87,8 +86,16 @@ def _assemble(mesh: Trimesh, t: float | None, method: str, cot_entries: Any = No
         terms = mesh.face_terms
     else:
         terms = face_terms(mesh.vertices, mesh.faces, mesh.n_vertices, mesh.n_faces, cot_entries)
+    area_sums, mass_divisor = terms.area_sums, 3.0
+    if mass == "voronoi":
+        # ``method="igl"``: each corner's Voronoi share, the lumped mass itself (heat.py:2116,2169).
+        area_sums = DeviceArray.empty(mesh.n_vertices, np.float64)
+        _lib.call("ob_voronoi_area_sums", mesh.vertices.ptr, mesh.faces.ptr, mesh.n_faces,
+                  mesh.n_vertices, area_sums.ptr, DEFAULT_STREAM)
+        mass_divisor = 1.0
     built = assemble_rows(
-        pattern, mesh.vertices, terms.cot, terms.area_sums, t=t, face_edges=timestep == "face_edges"
+        pattern, mesh.vertices, terms.cot, area_sums, t=t, face_edges=timestep == "face_edges",
+        mass_divisor=mass_divisor,
     )
     operators = HeatOperators(
         built.heat,
@@ -116,7 +123,8 @@ def heat_operators(
     """Assemble the source-independent operators the heat method solves against.
 
     ``t`` None takes ``h ** 2`` formed on the device, ``h`` the mean edge length ``method`` names
-    (unique edges for ``"potpourri3d"``, every face's three edges for ``"meshlab"``).
+    (unique edges for ``"potpourri3d"`` and ``"igl"``, every face's three edges for ``"meshlab"``);
+    ``"igl"`` lumps the mass by Voronoi areas, the others barycentrically (ordito/heat.py:2002-2012).
     """
     if cot_entries is not None and use_robust:
         raise ValueError(
@@ -216,7 +224,12 @@ class HeatSolver:
 
         kept = self._systems.get(role)
         if kept is None:
-            matrix = self.operators.heat_system if role == "heat" else self.operators.poisson_system
+            matrix = {
+                "heat": lambda: self.operators.heat_system,
+                "poisson": lambda: self.operators.poisson_system,
+                "pinned": lambda: self._pinned_system()[0],
+                "poisson_regularized": lambda: self._regularized_system()[0],
+            }[role]()
             kept = self._systems[role] = {
                 "factorization": OperatorFactorization(
                     matrix, self._mesh.vertices, singular=role == "poisson"
@@ -237,8 +250,43 @@ class HeatSolver:
         return kept
 
     def _sharing(self, role: str) -> Any:
+        # Every other system is stored over the heat system's pattern: its analysis serves them.
         heat = self._systems.get("heat")
-        return heat["factorization"] if role == "poisson" and heat is not None else None
+        return heat["factorization"] if role != "heat" and heat is not None else None
+
+    def _pinned_system(self) -> tuple[Any, DeviceArray] | tuple[()]:
+        """``diffuse_pinned``'s system and rim mask, built on first use; ``()`` with no rim
+        (ordito/heat.py:4200-4233)."""
+        if getattr(self, "_pinned", None) is None:
+            mesh, heat = self._mesh, self.operators.heat_system
+            pattern = mesh.mesh_operator_pattern
+            rim = DeviceArray.empty(max(mesh.n_vertices, 1), np.int32)
+            n_rim = DeviceArray.empty(1, np.int32)
+            _lib.call("ob_rim_vertices", pattern.offsets.ptr, pattern.columns.ptr,
+                      pattern.run_start.ptr, pattern.keys.ptr, pattern.n_keys, mesh.n_vertices,
+                      rim.ptr, n_rim.ptr, DEFAULT_STREAM)
+            # One read-back per solver: a closed mesh has no rim and so no second solve.
+            if int(n_rim.numpy()[0]) == 0:
+                self._pinned = ()
+            else:
+                values = DeviceArray.empty(max(heat.nnz, 1), np.float64)
+                _lib.call("ob_pinned_rows", heat.offsets.ptr, heat.columns.ptr, rim.ptr,
+                          heat.values.ptr, mesh.n_vertices, values.ptr, DEFAULT_STREAM)
+                self._pinned = (heat.with_values(values), rim)
+        return self._pinned
+
+    def _regularized_system(self) -> tuple[Any, Any]:
+        """geometry-central's Poisson system ``-L + 1e-6 I`` and its Chebyshev preconditioner,
+        built over the Poisson operator's pattern on first use (ordito/heat.py:4086-4114)."""
+        if getattr(self, "_regularized", None) is None:
+            poisson = self.operators.poisson_system
+            values = DeviceArray.empty(max(poisson.nnz, 1), np.float64)
+            _lib.call("ob_add_to_diagonal", poisson.offsets.ptr, poisson.columns.ptr,
+                      poisson.values.ptr, poisson.nrow, _GEOMETRY_CENTRAL_POISSON_SHIFT, values.ptr,
+                      DEFAULT_STREAM)
+            system = poisson.with_values(values)
+            self._regularized = (system, twl.chebyshev_preconditioner(system))
+        return self._regularized
 
     def factor(self, roles: tuple[str, ...] = ("heat", "poisson")) -> bool:
         """Factor both systems now (ordito/heat.py:3863); False if either could not be."""
@@ -314,6 +362,50 @@ class HeatSolver:
                          or getattr(kept["factorization"], "iterate_rejected", False)):
             self._ill_conditioned = True
 
+    def diffuse_pinned(self, rhs: Any, solution: Any) -> bool:
+        """Solve the heat system with the heat pinned to zero on the mesh's rim, in place
+        (ordito/heat.py:4153-4198): ``(M - t L) u = rhs`` on the interior, ``u = 0`` on every
+        vertex with an edge on a single face, settled as ``diffuse``. Returns whether the mesh has
+        a rim (without one ``solution`` is left as it was)."""
+        pinned = self._pinned_system()
+        if not pinned:
+            return False
+        system, rim = pinned
+        n = self._mesh.n_vertices
+        rhs_ptr, keep_rhs = device_pointer(rhs, np.float64)
+        pinned_rhs = DeviceArray.empty(n, np.float64)
+        _lib.call("ob_off_rim", rhs_ptr, rim.ptr, n, pinned_rhs.ptr, DEFAULT_STREAM)
+        del keep_rhs
+        kept = self._kept("pinned")
+        twl.solve_spd_settled(
+            system,
+            pinned_rhs,
+            solution,
+            check_rounds=_HEAT_CHECK_ROUNDS,
+            change_tolerance=_HEAT_CHANGE_TOLERANCE,
+            settle_rounds=self._vertex_time()[1],
+            factorization=kept["factorization"],
+            narrow_values=True,
+        )
+        return True
+
+    def solve_regularized_poisson(self, rhs: Any, solution: Any) -> None:
+        """Solve geometry-central's ``(-L + 1e-6 I) phi = rhs``, warm-started from ``solution``, in
+        place (ordito/heat.py:4086-4150): factored when the heat system is, else by CG under its
+        Chebyshev polynomial."""
+        system, preconditioner = self._regularized_system()
+        kept = self._kept("poisson_regularized")
+        factorization = kept["factorization"]
+        heat = self._systems.get("heat")
+        if (factorization.factorization is None and heat is not None
+                and heat["factorization"].factorization is not None):
+            factorization.factor(self._sharing("poisson_regularized"))
+        if factorization.factorization is not None:
+            factorization.solve(rhs, solution, tol=twl.SETTLE_DIRECT_TOLERANCE)
+            return
+        twl.solve_spd(system, rhs, solution, tol=_CG_TOLERANCE, preconditioner=preconditioner,
+                      name="heat_geodesic")
+
     def solve_poisson(self, rhs: Any, solution: Any) -> None:
         """Solve ``(-L) phi = rhs`` (consistent), warm-started from ``solution``, in place."""
         operators = self.operators
@@ -345,9 +437,15 @@ class HeatSolver:
         if multigrid is not None:
             multigrid.close()
             self._poisson_multigrid = None
+        extra = []
+        if getattr(self, "_pinned", None):
+            extra.append(self._pinned[0])
+        if getattr(self, "_regularized", None) is not None:
+            extra.append(self._regularized[0])
+        self._pinned = self._regularized = None
         if self._operators is not None:
             for matrix in (self._operators.heat_system, self._operators.poisson_system,
-                           self._operators.laplacian):
+                           self._operators.laplacian, *extra):
                 matrix.release()
             self._operators = None
         self._systems.clear()
@@ -392,13 +490,17 @@ def _divergence(mesh: Trimesh, solver: "HeatSolver", k: int, u: int, u_stride: i
 def _distance_from_heat(mesh: Trimesh, solver: HeatSolver, sources: DeviceArray,
                         heat: DeviceArray, n_columns: int = 1,
                         source_offsets: DeviceArray | None = None) -> DeviceArray:
-    """Divergence, Poisson solve and shift (ordito/heat.py:3052-3131)."""
+    """Divergence, Poisson solve and shift (ordito/heat.py:3052-3131); ``method="potpourri3d"``
+    solves geometry-central's regularized Poisson system (:3124-3129)."""
     n = mesh.n_vertices
     neg_div = DeviceArray.empty(n * n_columns, np.float64)
     _divergence(mesh, solver, n_columns, heat.ptr, n_columns, None, neg_div.ptr, n_columns, None,
                 None, DEFAULT_STREAM)
     phi = DeviceArray.zeros(n * n_columns, np.float64)
-    solver.solve_poisson(neg_div, phi)
+    if solver.method == "potpourri3d":
+        solver.solve_regularized_poisson(neg_div, phi)
+    else:
+        solver.solve_poisson(neg_div, phi)
     _lib.call(
         "ob_shift", phi.ptr, n, sources.ptr, sources.size,
         source_offsets.ptr if source_offsets is not None else None, n_columns, 1, DEFAULT_STREAM,
@@ -451,6 +553,11 @@ def heat_geodesic_batch(
         raise TypeError("heat_geodesic_batch: serves a resident Trimesh")
     n = mesh.n_vertices
     _supported(method, False)
+    if method != "meshlab":
+        raise NotImplementedError(
+            "heat_geodesic_batch serves method='meshlab' (the batched pass has no rim-pinned heat "
+            "or regularized Poisson system); use heat_geodesic for 'igl' and 'potpourri3d'"
+        )
     if poisson not in ("factor", "multigrid"):
         raise ValueError(f"poisson must be 'factor' or 'multigrid', got {poisson!r}")
     src, offsets, k = _source_columns(source_sets, n)
@@ -662,6 +769,9 @@ class BatchPipeline:
     def __init__(self, mesh: Trimesh, k: int, *, method: str = "meshlab", max_sources: int = 0) -> None:
         import ctypes  # noqa: PLC0415
 
+        if method != "meshlab":
+            raise NotImplementedError("BatchPipeline serves method='meshlab' (the batched pass)")
+
         from ordito_b200.device import PinnedArray  # noqa: PLC0415
 
         solver = mesh.heat_solver(None, method=method)
@@ -831,7 +941,10 @@ def _heat_geodesic(bound: Trimesh, src_arg: Any, t: float | None, use_robust: bo
         return DeviceArray.zeros(n, np.float64)
     _supported(method, use_robust)
     solver = bound.heat_solver(t, use_robust=use_robust, method=method)
-    held_factors = solver.heat_factor is not None and solver.poisson_factor is not None
+    # The recorded single-query pass serves the default discretization (meshlab: Neumann heat,
+    # the pinned Poisson system); the others run their own extra solves below.
+    held_factors = (method == "meshlab" and solver.heat_factor is not None
+                    and solver.poisson_factor is not None)
     # Host sources are checked on the host; device sources by one small read-back (the
     # reference's 4-byte flag, ordito/heat.py:5488).
     if host_sources is not None or held_factors:
@@ -852,4 +965,10 @@ def _heat_geodesic(bound: Trimesh, src_arg: Any, t: float | None, use_robust: bo
         )
     heat = DeviceArray.zeros(n, np.float64)
     solver.diffuse(u0, heat)
+    if method == "igl":
+        # igl::heat_geodesics' boundary rule: the mean of the Neumann heat and the heat pinned to
+        # zero on the rim, when the mesh has one (ordito/heat.py:594-597).
+        pinned = DeviceArray.zeros(n, np.float64)
+        if solver.diffuse_pinned(u0, pinned):
+            _lib.call("ob_axpby", n, 0.5, pinned.ptr, 0.5, heat.ptr, heat.ptr, DEFAULT_STREAM)
     return _distance_from_heat(bound, solver, src, heat)

@@ -213,6 +213,9 @@ class GeodesicServer:
             raise ValueError(f"max_columns must be one of {_BUCKETS}")
         self.max_columns = max_columns
         self.max_sources = max_sources
+        if method != "meshlab":
+            raise NotImplementedError("GeodesicServer serves method='meshlab' (its batches are the "
+                                      "batched pass)")
         self.method = method
         self._switch_interval = sys.getswitchinterval()
         sys.setswitchinterval(min(self._switch_interval, SWITCH_INTERVAL))
