@@ -127,6 +127,15 @@ int ob_pinned_rows(const int32_t* offsets, const int32_t* columns, const int32_t
 int ob_off_rim(const double* in, const int32_t* rim, int n_vertices, double* out, ob_stream_t stream);
 int ob_add_to_diagonal(const int32_t* offsets, const int32_t* columns, const double* values, int n_vertices,
                        double shift, double* out, ob_stream_t stream);
+/* ob_mollified_cot replaces ordito.laplacian.mollify_intrinsic (ordito/laplacian.py:779) followed
+ * by cotmatrix_entries_intrinsic (:276), the use_robust operators' half-cotangent table: each
+ * face's float32 side lengths (lengths[F][3], column e opposite corner e; caller-provided scratch),
+ * delta = max(epsilon * mean length - smallest triangle-inequality margin, 0) added to every length
+ * (float32; the mean is summed in float64, the reference sums it in float32), and cot[F][3] the
+ * float32 half-cotangents by the law of cosines over Kahan's Heron area. *delta_out = delta (one
+ * synchronous read-back). */
+int ob_mollified_cot(const float* xyz, const int32_t* faces, int n_faces, double epsilon, float* lengths,
+                     float* cot, double* delta_out, ob_stream_t stream);
 
 /* ---- a4: edge-length sums for the default time step -----------------------------------------
  * Replaces kernels/heat.py:173 upper_edge_length_sum_and_count (heat.py:2248 _edge_length_sums):

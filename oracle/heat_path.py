@@ -192,6 +192,51 @@ def cotmatrix_entries(vertices: np.ndarray, faces: np.ndarray) -> np.ndarray:
     return out
 
 
+TOLERANCE_MOLLIFY = 1e-5  # ordito/constants.py:31
+
+
+def mollified_lengths(vertices: np.ndarray, faces: np.ndarray,
+                      epsilon: float = TOLERANCE_MOLLIFY) -> tuple[np.ndarray, float]:
+    """``laplacian.mollify_intrinsic`` (ordito/laplacian.py:779-874, kernels/laplacian.py:1585-1627):
+    each face's float32 side lengths (column e opposite corner e) plus the one constant
+    ``delta = max(epsilon * mean - min margin, 0)`` that gives every triangle a margin of
+    ``epsilon`` times the mean edge length (float32; the mean summed in float64 here)."""
+    v0, v1, v2 = face_corners(vertices, faces)
+    with np.errstate(all="ignore"):
+        lengths = np.stack([_length(v1 - v2), _length(v2 - v0), _length(v0 - v1)], axis=1).astype(F32)
+    if lengths.shape[0] == 0:
+        return lengths, 0.0
+    a, b, c = lengths[:, 0], lengths[:, 1], lengths[:, 2]
+    margin = np.min(np.minimum(np.minimum(a + b - c, b + c - a), c + a - b))
+    mean = float(lengths.astype(F64).sum()) / lengths.size
+    eps = F32(epsilon * mean)
+    delta = max(F32(eps - margin), F32(0.0))
+    if delta <= 0.0:
+        return lengths, 0.0
+    return (lengths + F32(delta)).astype(F32), float(delta)
+
+
+def cot_from_lengths(lengths: np.ndarray) -> np.ndarray:
+    """``cotmatrix_entries_intrinsic`` in float32 (kernels/laplacian.py:56-90, 225-249;
+    kernels/predicates.py:194-210): the law of cosines over Kahan's Heron double area, the
+    largest side first; a zero-area face weighs nothing."""
+    L = np.asarray(lengths, dtype=F32)
+    srt = np.sort(L, axis=1)
+    c, b, a = srt[:, 0], srt[:, 1], srt[:, 2]
+    with np.errstate(all="ignore"):
+        arg = (a + (b + c)) * (c - (a - b)) * (c + (a - b)) * (a + (b - c))
+        dbl = F32(0.5) * np.sqrt(np.maximum(arg, F32(0.0)))
+        dbl = np.where(np.isnan(dbl), F32(0.0), dbl).astype(F32)
+        den = F32(4.0) * dbl
+        sq = L * L
+        c0 = (sq[:, 1] + sq[:, 2] - sq[:, 0]) / den
+        c1 = (sq[:, 2] + sq[:, 0] - sq[:, 1]) / den
+        c2 = (sq[:, 0] + sq[:, 1] - sq[:, 2]) / den
+    cot = np.stack([c0, c1, c2], axis=1).astype(F32)
+    cot[den <= 0] = 0.0
+    return cot
+
+
 def face_normals_and_areas(vertices: np.ndarray, faces: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
     """Unit normals (zero if degenerate) and areas, float32 (kernels/triangles.py:333-359)."""
     with np.errstate(all="ignore"):
@@ -347,7 +392,7 @@ def vertex_time(vertices: np.ndarray, faces: np.ndarray, t: float | None,
 
 def heat_operators(
     vertices: np.ndarray, faces: np.ndarray, t: float | None = None, *, mass_divisor: float = 3.0,
-    method: str = "meshlab",
+    method: str = "meshlab", use_robust: bool = False,
 ) -> dict[str, object]:
     """The heat operators over the cotmatrix pattern (heat.py:2015-2245): barycentric mass and
     the face-edge time step for ``"meshlab"``, the unique-edge time step for ``"potpourri3d"``,
@@ -360,7 +405,9 @@ def heat_operators(
     f = np.asarray(faces, dtype=np.int64).reshape(-1, 3)
     n = v.shape[0]
     pattern = mesh_operator_pattern(f, n)
-    cot = cotmatrix_entries(v, f)
+    # use_robust: the half-cotangents of the mollified lengths (heat.py:2043-2056); the mass, the
+    # normals and the areas stay the positions' own.
+    cot = cot_from_lengths(mollified_lengths(v, f)[0]) if use_robust else cotmatrix_entries(v, f)
     normals, areas = face_normals_and_areas(v, f)
     if method == "igl":
         sums = voronoi_area_sums(v, f, n)
@@ -594,6 +641,7 @@ def heat_geodesic(
     operators: dict[str, object] | None = None,
     factors: tuple[object, PoissonFactor] | None = None,
     method: str = "meshlab",
+    use_robust: bool = False,
 ) -> np.ndarray:
     """``heat_geodesic(vertices, faces, sources, method=...)`` (heat.py:391-588).
 
@@ -611,7 +659,7 @@ def heat_geodesic(
     u0 = seed(src, n)
     if operators is None:
         t_eff, _ = vertex_time(v, f, t, method)
-        operators = heat_operators(v, f, t_eff, method=method)
+        operators = heat_operators(v, f, t_eff, method=method, use_robust=use_robust)
     ops = operators
     pattern = ops["pattern"]
     if factors is None:

@@ -71,6 +71,7 @@ SIGNATURES: dict[str, list] = {
     "ob_pinned_rows": [P, P, P, P, I, P, P],
     "ob_off_rim": [P, P, I, P, P],
     "ob_add_to_diagonal": [P, P, P, I, D, P, P],
+    "ob_mollified_cot": [P, P, I, D, P, P, POINTER(c_double), P],
     "ob_edge_sums": [P, P, P, P, I, I, P, I, P, P],
     "ob_heat_rows": [P, P, P, P, I, P, I, P, D, P, I, P, D, P, P, P, P, P],
     "ob_seed": [P, I, I, P, P, P],

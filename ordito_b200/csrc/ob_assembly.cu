@@ -1,4 +1,6 @@
 // a2-a5: per-face terms, the default time step's edge sums and the three operators' rows.
+#include <cstring>
+
 #include "ob_geometry.cuh"
 #include "ob_internal.cuh"
 #include "ob_scratch.cuh"
@@ -297,12 +299,134 @@ __global__ void add_to_diagonal_kernel(const int* __restrict__ offsets, const in
     for (int k = offsets[i]; k < offsets[i + 1]; ++k) out[k] = values[k] + (columns[k] == i ? shift : 0.0);
 }
 
+// ordito/laplacian.py:779-874 (mollify_intrinsic), kernels/laplacian.py:1585-1627
+// (face_edge_lengths_and_margin): each face's float32 side lengths, column e opposite corner e
+// (kernels/predicates.py:221), and the smallest triangle-inequality margin a + b - c over every
+// face and side (*margin, an order-preserving int encoding of a float, seeded +inf), with the
+// lengths' float64 sum (*total) for their mean.
+__device__ __forceinline__ int ordered_bits(float x) {
+    const int i = __float_as_int(x);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+inline float from_ordered_bits(int i) {
+    const int bits = i >= 0 ? i : i ^ 0x7fffffff;
+    float x;
+    std::memcpy(&x, &bits, sizeof(float));
+    return x;
+}
+
+__global__ void face_lengths_margin_kernel(const float* __restrict__ xyz, const int* __restrict__ faces,
+                                           int n_faces, float* __restrict__ lengths, int* __restrict__ margin,
+                                           double* __restrict__ total) {
+    __shared__ float low[kThreads / 32];
+    __shared__ double sum[kThreads / 32];
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    float m = INFINITY;
+    double s = 0.0;
+    if (f < n_faces) {
+        const f3 v0 = load_f3(xyz, faces[3 * f]), v1 = load_f3(xyz, faces[3 * f + 1]);
+        const f3 v2 = load_f3(xyz, faces[3 * f + 2]);
+        auto length = [](float x, float y, float z) { return sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z))); };
+        const float a = length(v1.x - v2.x, v1.y - v2.y, v1.z - v2.z);
+        const float b = length(v2.x - v0.x, v2.y - v0.y, v2.z - v0.z);
+        const float c = length(v0.x - v1.x, v0.y - v1.y, v0.z - v1.z);
+        lengths[3 * f] = a;
+        lengths[3 * f + 1] = b;
+        lengths[3 * f + 2] = c;
+        m = fminf(fminf(a + b - c, b + c - a), c + a - b);
+        s = (double)a + (double)b + (double)c;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        low[threadIdx.x / 32] = m;
+        sum[threadIdx.x / 32] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float bm = INFINITY;
+        double bs = 0.0;
+        for (int w = 0; w < (int)blockDim.x / 32; ++w) {
+            bm = fminf(bm, low[w]);
+            bs += sum[w];
+        }
+        atomicMin(margin, ordered_bits(bm));
+        atomicAdd(total, bs);
+    }
+}
+
+// ordito/kernels/laplacian.py:56-90 (cot_entries_from_l2, cot_entries_from_edge_lengths) and
+// kernels/predicates.py:194-210 (doublearea_from_lengths, Kahan's Heron with the largest side
+// first): the float32 half-cotangents of a face from its lengths plus delta.
+__global__ void intrinsic_cot_kernel(const float* __restrict__ lengths, int n_faces, float delta,
+                                     float* __restrict__ cot) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n_faces) return;
+    const float l0 = __fadd_rn(lengths[3 * f], delta), l1 = __fadd_rn(lengths[3 * f + 1], delta);
+    const float l2 = __fadd_rn(lengths[3 * f + 2], delta);
+    // Sorted ascending (c <= b <= a): the largest side first in Kahan's product.
+    float c = l0, b = l1, a = l2, t;
+    if (c > b) t = c, c = b, b = t;
+    if (b > a) t = b, b = a, a = t;
+    if (c > b) t = c, c = b, b = t;
+    const float arg = __fmul_rn(__fmul_rn(__fmul_rn(__fadd_rn(a, __fadd_rn(b, c)), __fsub_rn(c, __fsub_rn(a, b))),
+                                          __fadd_rn(c, __fsub_rn(a, b))),
+                                __fadd_rn(a, __fsub_rn(b, c)));
+    float dbl_area = __fmul_rn(0.5f, sqrtf(fmaxf(arg, 0.0f)));
+    if (isnan(dbl_area)) dbl_area = 0.0f;
+    const float denominator = __fmul_rn(4.0f, dbl_area);
+    float c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
+    if (denominator > 0.0f) {
+        const float s0 = __fmul_rn(l0, l0), s1 = __fmul_rn(l1, l1), s2 = __fmul_rn(l2, l2);
+        c0 = __fdiv_rn(__fsub_rn(__fadd_rn(s1, s2), s0), denominator);
+        c1 = __fdiv_rn(__fsub_rn(__fadd_rn(s2, s0), s1), denominator);
+        c2 = __fdiv_rn(__fsub_rn(__fadd_rn(s0, s1), s2), denominator);
+    }
+    cot[3 * f] = c0;
+    cot[3 * f + 1] = c1;
+    cot[3 * f + 2] = c2;
+}
+
 }  // namespace
 }  // namespace ob
 
 using namespace ob;
 
 extern "C" {
+
+int ob_mollified_cot(const float* xyz, const int32_t* faces, int n_faces, double epsilon, float* lengths,
+                     float* cot, double* delta_out, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_faces >= 0 && delta_out != nullptr, "ob_mollified_cot: bad argument");
+    *delta_out = 0.0;
+    if (n_faces == 0) return OB_OK;
+    OB_REQUIRE(xyz && faces && lengths && cot, "ob_mollified_cot: null pointer");
+    Scratch scratch(stream);
+    int* margin = scratch.take<int>(1);
+    double* total = scratch.take<double>(1);
+    int st = scratch.commit();
+    if (st) return st;
+    const int inf_bits = 0x7f800000;  // +inf, whose ordered encoding is its own bits
+    OB_CUDA(cudaMemcpyAsync(margin, &inf_bits, sizeof(int), cudaMemcpyHostToDevice, stream));
+    OB_CUDA(cudaMemsetAsync(total, 0, sizeof(double), stream));
+    face_lengths_margin_kernel<<<ceil_div(n_faces, kThreads), kThreads, 0, stream>>>(xyz, faces, n_faces, lengths,
+                                                                                   margin, total);
+    OB_CHECK_LAUNCH("face_lengths_margin");
+    int margin_bits = 0;
+    double sum = 0.0;
+    OB_CUDA(cudaMemcpyAsync(&margin_bits, margin, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    OB_CUDA(cudaMemcpyAsync(&sum, total, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    OB_CUDA(cudaStreamSynchronize(stream));
+    // delta = max(epsilon * mean length - margin, 0) in float32 (laplacian.py:864-867).
+    const float epsilon_scaled = (float)(epsilon * (sum / (3.0 * (double)n_faces)));
+    const float delta = std::max(epsilon_scaled - from_ordered_bits(margin_bits), 0.0f);
+    intrinsic_cot_kernel<<<ceil_div(n_faces, kThreads), kThreads, 0, stream>>>(lengths, n_faces, delta, cot);
+    OB_CHECK_LAUNCH("intrinsic_cot");
+    *delta_out = (double)delta;
+    return OB_OK;
+}
 
 int ob_voronoi_area_sums(const float* xyz, const int32_t* faces, int n_faces, int n_vertices,
                          double* area_sums, ob_stream_t stream_) {

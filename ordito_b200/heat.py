@@ -12,6 +12,7 @@ step is a CUDA kernel of ``libordito_b200.so``; the host only reads back the doc
 from __future__ import annotations
 
 import contextlib
+import ctypes
 import gc
 import logging
 import math
@@ -43,6 +44,7 @@ _HEAT_CHANGE_TOLERANCE = 1e-6  # :146
 _HEAT_SETTLE_ROUNDS = 192  # :147
 _DIFFUSION_DECAY = 400.0  # :158
 _GEOMETRY_CENTRAL_POISSON_SHIFT = 1e-6  # :193 (geometry-central's Poisson system -L + 1e-6 I)
+_TOLERANCE_MOLLIFY = 1e-5  # ordito/constants.py:31 (use_robust's margin, of the mean edge length)
 
 
 class HeatOperators(NamedTuple):
@@ -71,13 +73,31 @@ def _heat_method_choices(method: str) -> tuple[str, str]:
 
 def _supported(method: str, use_robust: bool) -> None:
     _heat_method_choices(method)
-    if use_robust:
-        raise NotImplementedError("use_robust (mollified / intrinsic operators) is not built yet")
+    if use_robust and method == "potpourri3d":
+        raise NotImplementedError(
+            "use_robust at method='potpourri3d' (geometry-central's intrinsic tufted cover) is not "
+            "built; 'meshlab' and 'igl' take the mollified half-cotangents"
+        )
+
+
+def _robust_cot(mesh: Trimesh) -> DeviceArray:
+    """The use_robust half-cotangent table: the law of cosines over the face side lengths with one
+    constant added to every length so that no triangle is degenerate (ordito/laplacian.py:779,
+    :276; heat.py:2043-2056). The mass, normals and areas stay the positions' own."""
+    lengths = DeviceArray.empty((max(mesh.n_faces, 1), 3), np.float32)
+    cot = DeviceArray.empty((max(mesh.n_faces, 1), 3), np.float32)
+    delta = ctypes.c_double(0.0)
+    _lib.call("ob_mollified_cot", mesh.vertices.ptr, mesh.faces.ptr, mesh.n_faces, _TOLERANCE_MOLLIFY,
+              lengths.ptr, cot.ptr, ctypes.byref(delta), DEFAULT_STREAM)
+    return cot if mesh.n_faces else DeviceArray.empty((0, 3), np.float32)
 
 
 def _assemble(mesh: Trimesh, t: float | None, method: str, cot_entries: Any = None,
-              pattern: MeshOperatorPattern | None = None) -> tuple[HeatOperators, Any]:
+              pattern: MeshOperatorPattern | None = None,
+              use_robust: bool = False) -> tuple[HeatOperators, Any]:
     mass, timestep = _heat_method_choices(method)
+    if use_robust:
+        cot_entries = _robust_cot(mesh)
     if pattern is None:
         pattern = mesh.mesh_operator_pattern
     elif pattern.n_vertices != mesh.n_vertices or pattern.operator != "cotmatrix":
@@ -133,7 +153,7 @@ def heat_operators(
         )
     _supported(method, use_robust)
     mesh = Trimesh(vertices, faces)
-    return _assemble(mesh, t, method, cot_entries, pattern)[0]
+    return _assemble(mesh, t, method, cot_entries, pattern, use_robust)[0]
 
 
 def _diffusion_floor(mesh: Trimesh) -> float:
@@ -215,7 +235,7 @@ class HeatSolver:
     def operators(self) -> HeatOperators:
         if self._operators is None:
             t, _ = self._vertex_time()
-            self._operators = _assemble(self._mesh, t, self.method)[0]
+            self._operators = _assemble(self._mesh, t, self.method, use_robust=self.use_robust)[0]
         return self._operators
 
     # -- solves --------------------------------------------------------------------------------

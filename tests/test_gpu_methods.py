@@ -111,3 +111,37 @@ def test_batched_paths_serve_meshlab_only(gpu) -> None:
     with pytest.raises(NotImplementedError):
         gheat.BatchPipeline(mesh, 2, method="potpourri3d")
     mesh.dispose()
+
+
+@pytest.mark.parametrize("name", ["saddle_graded", "degenerate"])
+def test_mollified_cotangents_match_the_oracle(gpu, name: str) -> None:
+    import ctypes
+
+    from ordito_b200 import _lib
+
+    v, f = meshes.ALL[name]()
+    nf = f.shape[0]
+    lengths = DeviceArray.empty((nf, 3), np.float32)
+    cot = DeviceArray.empty((nf, 3), np.float32)
+    delta = ctypes.c_double(0.0)
+    mesh = Trimesh(v, f.reshape(-1))
+    _lib.call("ob_mollified_cot", mesh.vertices.ptr, mesh.faces.ptr, nf, 1e-5, lengths.ptr, cot.ptr,
+              ctypes.byref(delta), None)
+    ref_lengths, ref_delta = hp.mollified_lengths(v, f)
+    assert np.isclose(delta.value, ref_delta, rtol=1e-6, atol=0.0)
+    assert (delta.value > 0.0) == (name == "degenerate")
+    ref = hp.cot_from_lengths(ref_lengths)
+    assert np.allclose(cot.numpy(), ref, rtol=1e-6, atol=1e-6 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("method", ["meshlab", "igl"])
+@pytest.mark.parametrize("name", ["saddle_graded", "degenerate"])
+def test_robust_heat_geodesic_matches_the_oracle(gpu, method: str, name: str) -> None:
+    v, f = meshes.ALL[name]()
+    src = np.array([5], dtype=np.int32)
+    ref = hp.heat_geodesic(v, f, src, method=method, use_robust=True)
+    got = gheat.heat_geodesic(v, f.reshape(-1), src, method=method, use_robust=True).numpy()
+    assert np.all(np.isfinite(got))
+    assert _range_err(got, ref) <= DISTANCE_TOL
+    with pytest.raises(NotImplementedError):
+        gheat.heat_geodesic(v, f.reshape(-1), src, method="potpourri3d", use_robust=True)

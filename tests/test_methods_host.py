@@ -83,3 +83,28 @@ def test_igl_averages_only_where_there_is_a_rim() -> None:
     P = hp.csr_matrix(ops["pattern"], ops["P"])
     plain = hp.heat_geodesic(v, f, src, operators=ops, factors=(hp.HeatFactor(H), hp.PoissonFactor(P)))
     assert np.allclose(hp.heat_geodesic(v, f, src, method="igl"), plain, rtol=0, atol=1e-12)
+
+
+def test_intrinsic_cotangents_and_mollification_known_answers() -> None:
+    # The reference's docstring examples (ordito/laplacian.py:318-324, 822-838): an equilateral
+    # triangle weighs every edge cot(60)/2, the 3-4-5 triangle gives its hypotenuse nothing; a
+    # box needs no repair, a collinear triangle gets every length lengthened by 1e-5 x 4/3.
+    cot = hp.cot_from_lengths(np.array([[1.0, 1.0, 1.0], [5.0, 4.0, 3.0]], dtype=np.float32))
+    assert np.allclose(cot[0], 1.0 / (2.0 * np.sqrt(3.0)), rtol=1e-6)
+    assert np.allclose(cot[1], [0.0, 0.375, 2.0 / 3.0], rtol=1e-6, atol=1e-7)
+    bv, bf = creation.box()
+    assert hp.mollified_lengths(bv, bf)[1] == 0.0
+    line = np.array([[0, 0, 0], [1, 0, 0], [2, 0, 0]], dtype=np.float32)
+    lengths, delta = hp.mollified_lengths(line, np.array([[0, 1, 2]]))
+    assert f"{delta:.2e}" == "1.33e-05"
+    assert np.allclose(lengths, np.array([[1.0, 2.0, 1.0]]) + delta, rtol=0, atol=1e-7)
+    # A repeated-vertex face has a zero margin, so every face of its mesh is lengthened; a clean
+    # mesh's intrinsic weights are its positional ones to float32 rounding.
+    dv, df = meshes.with_degenerate_face()
+    assert hp.mollified_lengths(dv, df)[1] > 0.0
+    sv, sf = meshes.saddle_graded()
+    lengths, delta = hp.mollified_lengths(sv, sf)
+    assert delta == 0.0
+    positional = hp.cotmatrix_entries(sv, sf)
+    intrinsic = hp.cot_from_lengths(lengths)
+    assert np.allclose(intrinsic, positional, rtol=1e-3, atol=1e-4 * np.abs(positional).max())
