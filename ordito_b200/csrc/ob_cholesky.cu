@@ -649,6 +649,10 @@ struct Tile {
     int out_base;    // output row index: out_rows == -1 -> out_base + i, else idx[out_rows + i]
     int out_rows;
     int op;          // TileOp
+    // Known-zero structure of the block, used to skip whole inner steps: 0 dense; 1 lower
+    // triangular (entry (i, kk) zero for kk > i: the forward L11^-1); 2 the backward
+    // [L11^-1; G]^T (entry (i, kk) zero for kk < i while kk < tri_k = nc).
+    int tri, tri_k;
 };
 
 constexpr int kTileRows = 64;   // output rows per tile
@@ -697,8 +701,9 @@ struct Stage {
     double b[kTileK * kLd];
 };
 
-// One 64 x 64 output tile for a CTA of four warps, each warp a 32 x 32 quadrant as 4 x 4 float64
-// MMA tiles. The tile's matrix block and its gathered input rows are copied 16 inner steps at a
+// One 64 x 64 output tile for a CTA of four warps, each warp a 16-row strip of all 64 columns as
+// 2 x 8 float64 MMA tiles (strips rather than quadrants, so a strip of padding rows, or of the
+// zero triangle of L11^-1 over an inner step, is skipped whole). The tile's matrix block and its gathered input rows are copied 16 inner steps at a
 // time into shared memory with asynchronous 16-byte copies (zero-filled at the edges), two stages
 // in flight: the next step's copies overlap the current step's MMAs. The output is assigned,
 // subtracted, or added atomically per the tile's op. `k` (the column stride) is even and every
@@ -708,13 +713,16 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
                                              const int* __restrict__ idx,
                                              const double* in, double* out, int k, Stage* stage) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int wr = (warp >> 1) * 32, wc = (warp & 1) * 32;  // the warp's quadrant
-    const int fr = lane >> 2, fk = lane & 3;                 // fragment coordinates
-    double acc[4][4][2];
+    const int wr = warp * 16;                  // the warp's strip: rows [wr, wr + 16), all 64 columns
+    const int fr = lane >> 2, fk = lane & 3;  // fragment coordinates
+    double acc[2][8][2];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int j = 0; j < 8; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    // Rows of the strip within the block, for its known-zero inner steps.
+    const int row_lo = t.r0 + wr, row_hi = row_lo + 15;
+    const bool live = wr < t.rows;
     const double* M = vals + t.m;
     // Each operand block is 64 x kTileK doubles in 16-byte chunks, kChunks per thread.
     constexpr int kChunks = kTileRows * kTileK / 2 / kTileThreads;
@@ -760,35 +768,43 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
         }
         __syncthreads();
         const Stage& s = stage[st & 1];
+        // A strip skips a whole inner step when all its products are known zeros: padding rows
+        // past the tile, or the zero triangle of L11^-1 (the decision is warp-uniform and taken
+        // outside the unrolled step, which stays branch-free).
+        const int kb = t.k0 + st * kTileK;
+        const bool zero = !live || (t.tri == 1 && kb > row_hi) ||
+                          (t.tri == 2 && kb + kTileK - 1 < row_lo && kb + kTileK - 1 < t.tri_k);
+        if (!zero) {
 #pragma unroll
-        for (int k4 = 0; k4 < kTileK; k4 += 4) {
-            double a[4], b[4];
-            if (t.trans) {
+            for (int k4 = 0; k4 < kTileK; k4 += 4) {
+                double a[2], b[8];
+                if (t.trans) {
 #pragma unroll
-                for (int i = 0; i < 4; ++i) a[i] = s.a[(k4 + fk) * kLd + wr + 8 * i + fr];
-            } else {
+                    for (int i = 0; i < 2; ++i) a[i] = s.a[(k4 + fk) * kLd + wr + 8 * i + fr];
+                } else {
 #pragma unroll
-                for (int i = 0; i < 4; ++i) a[i] = s.a[(wr + 8 * i + fr) * kLdK + k4 + fk];
+                    for (int i = 0; i < 2; ++i) a[i] = s.a[(wr + 8 * i + fr) * kLdK + k4 + fk];
+                }
+#pragma unroll
+                for (int j = 0; j < 8; ++j) b[j] = s.b[(k4 + fk) * kLd + 8 * j + fr];
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
             }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = s.b[(k4 + fk) * kLd + wc + 8 * j + fr];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < 2; ++i) {
         const int local = wr + 8 * i + fr;
         if (local >= t.rows) continue;
         const int r = t.out_rows < 0 ? t.out_base + t.r0 + local : idx[t.out_rows + t.r0 + local];
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < 8; ++j)
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                const int c = c0 + wc + 8 * j + 2 * fk + h;
+                const int c = c0 + 8 * j + 2 * fk + h;
                 if (c >= k) continue;
                 double* o = out + (size_t)r * k + c;
                 const double v = acc[i][j][h];
@@ -1117,17 +1133,17 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
         for (int r0 = 0; r0 < nc; r0 += kTileRows) {
             const int rows = std::min(kTileRows, nc - r0);
             // Forward diagonal: Y[own] = L11^-1 B[own].
-            zero |= emit(fw[nd.level], Tile{inv_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, n + nd.start, -1, 0},
+            zero |= emit(fw[nd.level], Tile{inv_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, n + nd.start, -1, 0, 1, nc},
                          nc, split_fwd, kAssign, kAtomicAdd);
             // Backward: X[own] = [L11^-1; G]^T [Y[own]; X[off rows]].
-            zero |= emit(bw[nd.level], Tile{inv_at[s], ld, 1, r0, rows, 0, 0, 0, back_at[s], 2 * n + nd.start, -1, 0},
+            zero |= emit(bw[nd.level], Tile{inv_at[s], ld, 1, r0, rows, 0, 0, 0, back_at[s], 2 * n + nd.start, -1, 0, 2, nc},
                          nc + noff, split_bwd, kAssign, kAtomicAdd);
         }
         if (zero) zero_ranges.push_back(make_int2(nd.start, nc));
         for (int r0 = 0; r0 < noff; r0 += kTileRows) {
             const int rows = std::min(kTileRows, noff - r0);
             // Forward update: B[off rows] += G B[own].
-            emit(fw[nd.level], Tile{off_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, 0, rows_at[s], 0},
+            emit(fw[nd.level], Tile{off_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, 0, rows_at[s], 0, 0, 0},
                  nc, split_fwd, kAtomicAdd, kAtomicAdd);
         }
     }
