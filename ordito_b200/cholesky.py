@@ -106,7 +106,7 @@ class SparseCholesky:
 
     def work(self, n_columns: int, stream: Any = None, work_set: int = 0) -> tuple[int, int, int, int, int]:
         """``(B, X, stride, iperm, pinned)`` device pointers of the factor's own buffers (of work
-        set ``work_set``, 0 or 1) in its numbering (``ob_chol_work_set``), for pipelines that stay
+        set ``work_set``, 0 to 2) in its numbering (``ob_chol_work_set``), for pipelines that stay
         in it."""
         b, x, iperm, pinned = (ctypes.c_void_p(0) for _ in range(4))
         stride = ctypes.c_int(0)
