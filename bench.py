@@ -62,6 +62,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-large-mesh", action="store_true")
     p.add_argument("--no-packed", action="store_true")
     p.add_argument("--no-kernel-rooflines", action="store_true")
+    p.add_argument("--no-serving-full-range", action="store_true")
     # Only the per-kernel rooflines, on icosphere(LEVEL) with 1 % radial noise (a profiling case).
     p.add_argument("--kernels-only", type=int, default=0, metavar="LEVEL")
     p.add_argument("--serving-requests", type=int, default=300)
@@ -631,22 +632,22 @@ def run_packed() -> dict:
     return result
 
 
-def run_serving(args: argparse.Namespace) -> dict:
+def run_serving(rate: float, v_max: float, warmup: int, requests: int) -> dict:
     """The serving stream: Poisson arrivals, meshes log-uniform in size (icospheres and jittered
     tori), 70 % of requests on one of the last 50 meshes, 1-32 sources each, 150 GB HBM budget.
-    The first ``serving_warmup`` requests fill the cache untimed (the steady state the stream
-    describes); the next ``serving_requests`` are timed at their arrival times."""
+    The first ``warmup`` requests fill the cache untimed (the steady state the stream describes);
+    the next ``requests`` are timed at their arrival times."""
     from ordito_b200.serving import GeodesicServer, mesh_for, serving_workload
 
-    total = args.serving_warmup + args.serving_requests
-    stream = serving_workload(2, total, args.serving_rate, v_min=1e3, v_max=args.serving_vmax)
+    total = warmup + requests
+    stream = serving_workload(2, total, rate, v_min=1e3, v_max=v_max)
     meshes = {spec: mesh_for(spec) for spec in {r.mesh for r in stream}}
     server = GeodesicServer(hbm_budget=150 << 30, max_columns=64, slots=4)
     try:
-        for r in stream[: args.serving_warmup]:
+        for r in stream[:warmup]:
             server.submit(*meshes[r.mesh], r.sources)
         server.reset_stats()
-        timed = stream[args.serving_warmup:]
+        timed = stream[warmup:]
         futures = []
         origin = time.perf_counter() - timed[0].arrival
         for r in timed:
@@ -661,11 +662,11 @@ def run_serving(args: argparse.Namespace) -> dict:
         server.close()
     stats.update({
         "unit": "solves/s",
-        "offered_rate_per_s": args.serving_rate,
-        "mesh_vertices": [1e3, args.serving_vmax],
+        "offered_rate_per_s": rate,
+        "mesh_vertices": [1e3, v_max],
         "reuse": 0.7,
         "hbm_budget_gb": 150,
-        "warmup_requests": args.serving_warmup,
+        "warmup_requests": warmup,
         "what": "GeodesicServer: continuous batching on 4 CUDA streams, resident factors keyed by "
                 "mesh hash, LRU eviction under the budget; latency = arrival to host result",
     })
@@ -817,6 +818,20 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     synchronize()
     single_value = len(single) / (_elapsed(start, end) / 1e3)
 
+    # The workload's other reading: one query whose source set is all 64 vertices (the distance
+    # to the nearest of them), through heat_geodesic on the resident mesh, against the oracle.
+    all_sources = np.asarray(sources, dtype=np.int32)
+    multi = gheat.heat_geodesic(mesh, all_sources).numpy()
+    synchronize()
+    _lib.call("ob_event_record", start, None)
+    for _ in range(10):
+        gheat.heat_geodesic(mesh, all_sources)
+    _lib.call("ob_event_record", end, None)
+    synchronize()
+    multi_ms = _elapsed(start, end) / 10
+    multi_error = hp.relative_linf(multi, hp.heat_geodesic(vertices, faces, all_sources, operators=ops,
+                                                            factors=factors))
+
     # Plain drop-in: heat_geodesic(vertices, faces, [s]) builds everything inside every call.
     plain = None
     if not args.no_plain:
@@ -884,7 +899,12 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
         reference_benchmarks = run_reference_benchmarks()
     serving = None
     if not args.no_serving and dist.world == 1:
-        serving = run_serving(args)
+        serving = run_serving(args.serving_rate, args.serving_vmax, args.serving_warmup,
+                              args.serving_requests)
+        if not args.no_serving_full_range:
+            # The stream's full size range (1e3 - 2e6 vertices): the largest meshes are past the
+            # factorisation budget or take seconds to factor on the host, so at a lower rate.
+            serving["full_range"] = run_serving(10.0, 2e6, 60, 120)
     packed = None
     if not args.no_packed and dist.world == 1:
         try:
@@ -944,6 +964,9 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
                 "what": "heat_geodesic(vertices, faces, [s]) per query: assembly, settled CG, the "
                         "backward-error check and its factored fallback inside every call",
             },
+            "multi_source_query": {"ms": multi_ms, "max_rel_linf_vs_fp64_oracle": multi_error,
+                                   "what": "heat_geodesic(mesh, sources) with all 64 sources in one "
+                                           "set: the distance to the nearest (factors resident)"},
             "resident_single_query": {"value": single_value, "unit": UNIT,
                                       "what": "heat_geodesic_batch(mesh, [[s]]): factors resident, k = 1"},
             "precision": precision,

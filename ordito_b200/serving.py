@@ -190,6 +190,28 @@ class _Resident:
 
 
 @dataclass
+class _Unfactored:
+    """A resident mesh whose systems are past the factorisation budget: its requests are answered
+    one at a time by the unfactored path (the band march for the heat system, the mixed-precision
+    multigrid solve for the Poisson system) on the setup threads, with its operators, multigrid
+    hierarchy and solver states kept for the next request. ``lock`` orders them per mesh."""
+
+    key: str
+    mesh: Any
+    nbytes: int
+    lock: threading.Lock = field(default_factory=threading.Lock)
+    pending: collections.deque = field(default_factory=collections.deque)  # always empty
+    busy: bool = False
+    queued: int = 0  # requests handed to the setup threads and not yet answered
+
+    def release(self) -> None:
+        with self.lock:
+            if self.mesh is not None:
+                self.mesh.dispose()
+            self.mesh = None
+
+
+@dataclass
 class _Slot:
     stream: ctypes.c_void_p
     event: ctypes.c_void_p
@@ -202,7 +224,9 @@ class GeodesicServer:
 
     ``submit(vertices, faces, sources)`` returns a ``concurrent.futures.Future`` whose result is
     the ``(V,)`` float64 host array of distances to the nearest source; invalid sources fail the
-    future with ``ValueError``, a mesh over the budget with ``MemoryError``. ``stats()`` reports
+    future with ``ValueError``, a mesh over the HBM budget with ``MemoryError``. A mesh whose
+    systems are past the factorisation budget stays resident unfactored and its requests are
+    answered one at a time on the setup threads (band march and multigrid). ``stats()`` reports
     request latencies (arrival to result, p50/p99), solves/s and cache behaviour.
     """
 
@@ -380,7 +404,11 @@ class GeodesicServer:
         entry = self.cache.get(request.key)
         if entry is not None:
             self._hits += 1
-            entry.pending.append(request)
+            if isinstance(entry, _Unfactored):
+                entry.queued += 1
+                self._setups.put((entry, request))  # answered on a setup thread
+            else:
+                entry.pending.append(request)
             return
         request.cold = True
         with self._waiting_lock:
@@ -400,7 +428,8 @@ class GeodesicServer:
             estimate = ESTIMATED_BYTES_PER_VERTEX * request.vertices.shape[0]
             try:
                 reserved, evicted = self.cache.admit(request.key, estimate,
-                                                     lambda e: not e.busy and not e.pending)
+                                                     lambda e: not e.busy and not e.pending
+                                                     and not getattr(e, "queued", 0))
             except MemoryError as exc:
                 self._fail_waiting(request.key, exc)
                 progressed = True
@@ -423,7 +452,12 @@ class GeodesicServer:
                 self._complete(request, error=error)
             return
         self.cache.commit(key, entry, entry.nbytes)
-        entry.pending.extend(waiting)
+        if isinstance(entry, _Unfactored):
+            for request in waiting:
+                entry.queued += 1
+                self._setups.put((entry, request))
+        else:
+            entry.pending.extend(waiting)
 
     def _fail_waiting(self, key: str, error: BaseException) -> None:
         with self._waiting_lock:
@@ -502,13 +536,19 @@ class GeodesicServer:
             if request is None:
                 _lib.call("ob_stream_destroy", capture)
                 return
+            if isinstance(request, tuple):
+                self._answer_unfactored(*request)
+                continue
             try:
                 mesh = Trimesh(request.vertices, request.faces)
                 solver = mesh.heat_solver(None, method=self.method)
                 solver.factor_on_second_solve = False
                 self._answer_plain(request.key, mesh)
                 if not solver.factor():
-                    raise MemoryError("the mesh's systems could not be factored within the budget")
+                    # Past the factorisation budget: kept resident, answered unfactored.
+                    unfactored = _Unfactored(request.key, mesh, int(mesh.nbytes))
+                    self._ready.put((request.key, unfactored, None))
+                    continue
                 n = mesh.n_vertices
                 mesh.corner_index  # built now, not on the first batch
                 cap_sources = self.max_columns * 2 * self.max_sources
@@ -531,6 +571,21 @@ class GeodesicServer:
                 self._ready.put((request.key, entry, None))
             except BaseException as exc:  # noqa: BLE001 -- the error belongs to the requests
                 self._ready.put((request.key, None, exc))
+
+    def _answer_unfactored(self, entry: _Unfactored, request: _Request) -> None:
+        from ordito_b200 import heat as gheat  # noqa: PLC0415
+
+        with entry.lock:
+            try:
+                if entry.mesh is None:
+                    raise RuntimeError("the mesh was evicted before its request ran")
+                distances = gheat.heat_geodesic(entry.mesh, request.sources, method=self.method).numpy()
+            except Exception as exc:  # noqa: BLE001 -- the error belongs to the request
+                self._complete(request, error=exc)
+            else:
+                self._complete(request, result=distances)
+            finally:
+                entry.queued -= 1
 
     def _answer_plain(self, key: str, mesh: Any) -> None:
         """Answer up to ``plain_answers`` of the mesh's waiting requests by the unfactored path

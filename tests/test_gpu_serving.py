@@ -102,3 +102,28 @@ def test_invalid_requests_fail_their_future(gpu) -> None:
     ok = server.submit(v, f, [0]).result(timeout=300)
     server.close()
     assert ok[0] == 0.0 and np.all(ok >= -1e-6)
+
+
+def test_a_mesh_past_the_factor_budget_is_served_unfactored(gpu) -> None:
+    # With the factorisation budget below the mesh's factor, its first requests are answered
+    # unfactored and so are all the later ones (kept resident, one at a time): more requests than
+    # plain answers, every one against the oracle.
+    from ordito_b200 import cholesky as gchol
+
+    v, f = mesh_for(SPECS[2])
+    budget = gchol.CHOLESKY_MEMORY_BUDGET
+    gchol.CHOLESKY_MEMORY_BUDGET = 1 << 10
+    try:
+        server = GeodesicServer(max_columns=4, slots=1, plain_answers=2)
+        rng = np.random.default_rng(7)
+        batches = [rng.choice(v.shape[0], size=int(rng.integers(1, 4)), replace=False).astype(np.int32)
+                   for _ in range(6)]
+        futures = [server.submit(v, f, s) for s in batches]
+        results = [fut.result(timeout=600) for fut in futures]
+        stats = server.stats()
+        server.close()
+    finally:
+        gchol.CHOLESKY_MEMORY_BUDGET = budget
+    for sources, got in zip(batches, results):
+        assert rel_err(got, hp.heat_geodesic(v, f, sources)) <= ORACLE_TOL
+    assert stats["resident_meshes"] == 1
