@@ -617,6 +617,7 @@ def run_packed() -> dict:
         "columns": k,
         "setup_s": setup_s,
         "factor_bytes": packed.nbytes,
+        "pass_schedule": {role: list(report["best"]) for role, report in packed.tuning.items()},
         "ms_per_step": ms,
         "value": queries / (ms / 1e3),
         "unit": "solves/s",
@@ -692,6 +693,8 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     mesh = Trimesh(vertices, faces.reshape(-1))
     solver = mesh.heat_solver(None, method="meshlab")
     assert solver.factor(), "factorisation refused"
+    # The passes' tile schedule tuned to this mesh's tree at the batch width (part of setup).
+    tuning = solver.tune(k)
     synchronize()
     setup_s = time.perf_counter() - t0
     src, offsets, _ = gheat._source_columns(sets, n)
@@ -946,6 +949,9 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
                 "l2": "no flush; per step the two 147 MB factors (294 MB) exceed the 126 MB L2",
                 "parallelism": f"replicas{dist.world}",
                 "setup_s": setup_s,
+                "pass_schedule": {role: {"best": list(report["best"]),
+                                         "ms": {f"{c}/{w}": round(t, 4) for (c, w), t in report["ms"].items()}}
+                                  for role, report in tuning.items()},
             },
             "accuracy": {"max_rel_linf_vs_fp64_oracle": max(errors), "checked_queries": len(check)},
             "e2e": {

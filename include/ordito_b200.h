@@ -354,6 +354,13 @@ int ob_shift_permuted(const double* phi, int n_vertices, int stride, const int32
                       const int32_t* sources, const int32_t* source_offsets, int n_columns,
                       int orient, double* out, ob_stream_t stream);
 int ob_chol_time_solve(void* factor, int n_columns, int reps, float* ms, ob_stream_t stream);
+/* ob_chol_tile (a tuning hook; no counterpart in the reference): rebuild the passes' tile lists
+ * with another split of long inner dimensions -- chunk: the inner range of a split tile (16 to
+ * 4096, or 0: never split), applied at levels with fewer tiles than `waves` waves of the resident
+ * grid (0 to 64). Waits for the device, drops the factor's recorded solves and moves every work
+ * set's generation (recordings over ob_chol_work buffers must be made again). The defaults after
+ * ob_chol_factor are chunk 64, waves 2. */
+int ob_chol_tile(void* factor, int chunk, int waves, ob_stream_t stream);
 int ob_chol_info(void* factor, long long* info);
 /* The work buffers' generation: it changes whenever ob_chol_work's pointers do (a wider k than
  * any before reallocates them), so a graph recorded over them must be recorded again. */

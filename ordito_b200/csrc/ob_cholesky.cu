@@ -973,8 +973,13 @@ struct Factor {
     std::vector<int> n_fwd, n_bwd;
     int launches_per_pass = 0;
     std::vector<void*> owned;
+    std::vector<void*> tile_owned;  // the tile lists and zero ranges (rebuilt by build_tiles)
     int2* zero = nullptr;  // row ranges split tiles accumulate into (zeroed each pass)
     int n_zero = 0;
+    int tile_chunk = 0, tile_waves = 0;  // the split parameters the tile lists were built with
+    // Per node: offsets of its [L11^-1; G] block in vals, of its row lists in idx, and its ld.
+    std::vector<long long> inv_at, off_at;
+    std::vector<int> rows_at, back_at, ld_at;
     size_t bytes = 0;
     // Recorded solve graphs, keyed by (columns, refinement steps, operator arrays).
     struct Recorded {
@@ -1012,6 +1017,12 @@ int dev_alloc(Factor* F, void** p, size_t bytes, cudaStream_t stream) {
     return OB_OK;
 }
 
+int tile_alloc(Factor* F, void** p, size_t bytes, cudaStream_t stream) {
+    OB_CUDA(cudaMallocAsync(p, std::max<size_t>(bytes, 8), stream));
+    F->tile_owned.push_back(*p);
+    return OB_OK;
+}
+
 void factor_release(Factor* F) {
     if (F == nullptr) return;
     {
@@ -1022,6 +1033,7 @@ void factor_release(Factor* F) {
         for (auto& g : W.graphs) cudaGraphExecDestroy(g.exec);
     if (F->capture) cudaStreamDestroy(F->capture);
     for (void* p : F->owned) cudaFree(p);
+    for (void* p : F->tile_owned) cudaFree(p);
     delete F;
 }
 
@@ -1034,6 +1046,111 @@ int allow_stage_memory() {
     OB_CUDA(cudaFuncSetAttribute(tile_product_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kStageBytes));
     if (device >= 0 && device < 64) allowed[device] = 1;
+    return OB_OK;
+}
+
+// The tile lists of the passes (and the row ranges their split tiles accumulate into), replacing
+// any built before. chunk: the inner-dimension range of a split tile (0: never split); waves:
+// levels with fewer tiles than that many waves of the resident grid (4 CTAs an SM) are split.
+int build_tiles(Factor* F, int chunk, int waves, cudaStream_t stream) {
+    for (void* p : F->tile_owned) OB_CUDA(cudaFreeAsync(p, stream));
+    F->tile_owned.clear();
+    F->zero = nullptr;
+    F->n_zero = 0;
+    // One launch per tree level and direction. Forward at a level: every node's
+    // Y[own] = L11^-1 B[own] and B[off rows] += G B[own] (atomic: siblings share ancestors' rows);
+    // backward: X[own] = [L11^-1; G]^T [Y[own]; X[off rows]], one product over nc + noff. Each
+    // reads only rows no tile of its launch writes. A level with few tiles has its long inner
+    // dimensions split over several tiles (more CTAs, each a shorter latency-bound chain), which
+    // then accumulate atomically into rows zeroed at the start of each pass; a level with `waves`
+    // waves of tiles or more is not split.
+    const Analysis& A = *F->analysis;
+    const int ns = (int)A.nodes.size(), n = A.n;
+    const std::vector<long long>&inv_at = F->inv_at, &off_at = F->off_at;
+    const std::vector<int>&rows_at = F->rows_at, &back_at = F->back_at, &ld_at = F->ld_at;
+    const int L = A.levels;
+    const long long wave = 4LL * sm_count();
+    auto tiles_of = [](int rows) { return (rows + kTileRows - 1) / kTileRows; };
+    std::vector<long long> fwd_count(L, 0), bwd_count(L, 0);
+    for (const Node& nd : A.nodes) {
+        if (nd.count == 0) continue;
+        fwd_count[nd.level] += tiles_of(nd.count) + tiles_of((int)nd.off_rows.size());
+        bwd_count[nd.level] += tiles_of(nd.count);
+    }
+    auto emit = [chunk](std::vector<Tile>& list, Tile t, int K, bool may_split, int whole_op, int split_op) {
+        const bool split = chunk > 0 && may_split && K > chunk + chunk / 2;
+        for (int k0 = 0; k0 < K; k0 += split ? chunk : K) {
+            t.k0 = k0;
+            t.k1 = split ? std::min(K, k0 + chunk) : K;
+            t.op = split ? split_op : whole_op;
+            list.push_back(t);
+        }
+        return split;
+    };
+    std::vector<std::vector<Tile>> fw(L), bw(L);
+    std::vector<int2> zero_ranges;
+    for (int s = 0; s < ns; ++s) {
+        const Node& nd = A.nodes[s];
+        const int nc = nd.count, noff = (int)nd.off_rows.size(), ld = ld_at[s];
+        if (nc == 0) continue;
+        const bool split_fwd = fwd_count[nd.level] < waves * wave, split_bwd = bwd_count[nd.level] < waves * wave;
+        bool zero = false;
+        for (int r0 = 0; r0 < nc; r0 += kTileRows) {
+            const int rows = std::min(kTileRows, nc - r0);
+            // Forward diagonal: Y[own] = L11^-1 B[own].
+            zero |= emit(fw[nd.level], Tile{inv_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, n + nd.start, -1, 0, 1, nc},
+                         nc, split_fwd, kAssign, kAtomicAdd);
+            // Backward: X[own] = [L11^-1; G]^T [Y[own]; X[off rows]].
+            zero |= emit(bw[nd.level], Tile{inv_at[s], ld, 1, r0, rows, 0, 0, 0, back_at[s], 2 * n + nd.start, -1, 0, 2, nc},
+                         nc + noff, split_bwd, kAssign, kAtomicAdd);
+        }
+        if (zero) zero_ranges.push_back(make_int2(nd.start, nc));
+        for (int r0 = 0; r0 < noff; r0 += kTileRows) {
+            const int rows = std::min(kTileRows, noff - r0);
+            // Forward update: B[off rows] += G B[own].
+            emit(fw[nd.level], Tile{off_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, 0, rows_at[s], 0, 0, 0},
+                 nc, split_fwd, kAtomicAdd, kAtomicAdd);
+        }
+    }
+    // Adjacent ranges joined, then cut into pieces of at most 16 rows: one block each, so the
+    // zeroing launch is balanced however large a merged node is.
+    std::vector<int2> pieces;
+    for (size_t i = 0; i < zero_ranges.size();) {
+        int2 r = zero_ranges[i++];
+        while (i < zero_ranges.size() && zero_ranges[i].x == r.x + r.y) r.y += zero_ranges[i++].y;
+        for (int o = 0; o < r.y; o += 16) pieces.push_back(make_int2(r.x + o, std::min(16, r.y - o)));
+    }
+    zero_ranges.swap(pieces);
+    F->n_zero = (int)zero_ranges.size();
+    int st = OB_OK;
+    if (F->n_zero > 0) {
+        st = tile_alloc(F, (void**)&F->zero, sizeof(int2) * zero_ranges.size(), stream);
+        if (st) return st;
+        OB_CUDA(cudaMemcpyAsync(F->zero, zero_ranges.data(), sizeof(int2) * zero_ranges.size(),
+                                cudaMemcpyHostToDevice, stream));
+    }
+    auto push = [&](std::vector<std::vector<Tile>>& lists, std::vector<Tile*>& dst,
+                    std::vector<int>& counts) -> int {
+        dst.assign(L, nullptr);
+        counts.assign(L, 0);
+        for (int l = 0; l < L; ++l) {
+            counts[l] = (int)lists[l].size();
+            if (lists[l].empty()) continue;
+            int st2 = tile_alloc(F, (void**)&dst[l], sizeof(Tile) * lists[l].size(), stream);
+            if (st2) return st2;
+            OB_CUDA(cudaMemcpyAsync(dst[l], lists[l].data(), sizeof(Tile) * lists[l].size(),
+                                    cudaMemcpyHostToDevice, stream));
+        }
+        return OB_OK;
+    };
+    st = push(fw, F->fwd, F->n_fwd);
+    if (!st) st = push(bw, F->bwd, F->n_bwd);
+    if (st) return st;
+    F->launches_per_pass = 0;
+    for (int l = 0; l < L; ++l) F->launches_per_pass += (F->n_fwd[l] > 0) + (F->n_bwd[l] > 0);
+    OB_CUDA(cudaStreamSynchronize(stream));  // host staging buffers go out of scope
+    F->tile_chunk = chunk;
+    F->tile_waves = waves;
     return OB_OK;
 }
 
@@ -1095,93 +1212,12 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
     OB_CUDA(cudaMemcpyAsync(F->perm, A.perm.data(), sizeof(int) * A.n, cudaMemcpyHostToDevice,
                             stream));
     OB_CUDA(cudaMemcpyAsync(F->pinned, H.pinned.data(), A.n, cudaMemcpyHostToDevice, stream));
-    // One launch per tree level and direction. Forward at a level: every node's
-    // Y[own] = L11^-1 B[own] and B[off rows] += G B[own] (atomic: siblings share ancestors' rows);
-    // backward: X[own] = [L11^-1; G]^T [Y[own]; X[off rows]], one product over nc + noff. Each
-    // reads only rows no tile of its launch writes. A level with few tiles has its long inner
-    // dimensions split over several tiles (more CTAs, each a shorter latency-bound chain), which
-    // then accumulate atomically into rows zeroed at the start of each pass; a level with two
-    // waves of tiles or more is not split.
-    const int L = A.levels;
-    const long long wave = 4LL * sm_count();
-    auto tiles_of = [](int rows) { return (rows + kTileRows - 1) / kTileRows; };
-    std::vector<long long> fwd_count(L, 0), bwd_count(L, 0);
-    for (const Node& nd : A.nodes) {
-        if (nd.count == 0) continue;
-        fwd_count[nd.level] += tiles_of(nd.count) + tiles_of((int)nd.off_rows.size());
-        bwd_count[nd.level] += tiles_of(nd.count);
-    }
-    auto emit = [](std::vector<Tile>& list, Tile t, int K, bool may_split, int whole_op, int split_op) {
-        const int chunk = kSplitK;
-        const bool split = may_split && K > chunk + chunk / 2;
-        for (int k0 = 0; k0 < K; k0 += split ? chunk : K) {
-            t.k0 = k0;
-            t.k1 = split ? std::min(K, k0 + chunk) : K;
-            t.op = split ? split_op : whole_op;
-            list.push_back(t);
-        }
-        return split;
-    };
-    std::vector<std::vector<Tile>> fw(L), bw(L);
-    std::vector<int2> zero_ranges;
-    for (int s = 0; s < ns; ++s) {
-        const Node& nd = A.nodes[s];
-        const int nc = nd.count, noff = (int)nd.off_rows.size(), ld = ld_at[s];
-        if (nc == 0) continue;
-        const bool split_fwd = fwd_count[nd.level] < 2 * wave, split_bwd = bwd_count[nd.level] < 2 * wave;
-        bool zero = false;
-        for (int r0 = 0; r0 < nc; r0 += kTileRows) {
-            const int rows = std::min(kTileRows, nc - r0);
-            // Forward diagonal: Y[own] = L11^-1 B[own].
-            zero |= emit(fw[nd.level], Tile{inv_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, n + nd.start, -1, 0, 1, nc},
-                         nc, split_fwd, kAssign, kAtomicAdd);
-            // Backward: X[own] = [L11^-1; G]^T [Y[own]; X[off rows]].
-            zero |= emit(bw[nd.level], Tile{inv_at[s], ld, 1, r0, rows, 0, 0, 0, back_at[s], 2 * n + nd.start, -1, 0, 2, nc},
-                         nc + noff, split_bwd, kAssign, kAtomicAdd);
-        }
-        if (zero) zero_ranges.push_back(make_int2(nd.start, nc));
-        for (int r0 = 0; r0 < noff; r0 += kTileRows) {
-            const int rows = std::min(kTileRows, noff - r0);
-            // Forward update: B[off rows] += G B[own].
-            emit(fw[nd.level], Tile{off_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, 0, rows_at[s], 0, 0, 0},
-                 nc, split_fwd, kAtomicAdd, kAtomicAdd);
-        }
-    }
-    // Adjacent ranges joined, then cut into pieces of at most 16 rows: one block each, so the
-    // zeroing launch is balanced however large a merged node is.
-    std::vector<int2> pieces;
-    for (size_t i = 0; i < zero_ranges.size();) {
-        int2 r = zero_ranges[i++];
-        while (i < zero_ranges.size() && zero_ranges[i].x == r.x + r.y) r.y += zero_ranges[i++].y;
-        for (int o = 0; o < r.y; o += 16) pieces.push_back(make_int2(r.x + o, std::min(16, r.y - o)));
-    }
-    zero_ranges.swap(pieces);
-    F->n_zero = (int)zero_ranges.size();
-    if (F->n_zero > 0) {
-        st = dev_alloc(F, (void**)&F->zero, sizeof(int2) * zero_ranges.size(), stream);
-        if (st) return st;
-        OB_CUDA(cudaMemcpyAsync(F->zero, zero_ranges.data(), sizeof(int2) * zero_ranges.size(),
-                                cudaMemcpyHostToDevice, stream));
-    }
-    auto push = [&](std::vector<std::vector<Tile>>& lists, std::vector<Tile*>& dst,
-                    std::vector<int>& counts) -> int {
-        dst.assign(L, nullptr);
-        counts.assign(L, 0);
-        for (int l = 0; l < L; ++l) {
-            counts[l] = (int)lists[l].size();
-            if (lists[l].empty()) continue;
-            int st2 = dev_alloc(F, (void**)&dst[l], sizeof(Tile) * lists[l].size(), stream);
-            if (st2) return st2;
-            OB_CUDA(cudaMemcpyAsync(dst[l], lists[l].data(), sizeof(Tile) * lists[l].size(),
-                                    cudaMemcpyHostToDevice, stream));
-        }
-        return OB_OK;
-    };
-    st = push(fw, F->fwd, F->n_fwd);
-    if (!st) st = push(bw, F->bwd, F->n_bwd);
-    if (st) return st;
-    F->launches_per_pass = 0;
-    for (int l = 0; l < L; ++l) F->launches_per_pass += (F->n_fwd[l] > 0) + (F->n_bwd[l] > 0);
+    F->inv_at = std::move(inv_at);
+    F->off_at = std::move(off_at);
+    F->rows_at = std::move(rows_at);
+    F->back_at = std::move(back_at);
+    F->ld_at = std::move(ld_at);
+    if ((st = build_tiles(F, kSplitK, 2, stream))) return st;
     OB_CUDA(cudaStreamSynchronize(stream));  // host staging buffers go out of scope
     return OB_OK;
 }
@@ -1537,6 +1573,27 @@ int ob_chol_time_solve(void* factor, int n_columns, int reps, float* ms, ob_stre
     if (e != cudaSuccess) return cuda_status(e, "ob_chol_time_solve");
     *ms = total / (float)reps;
     return OB_OK;
+}
+
+int ob_chol_tile(void* factor, int chunk, int waves, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(factor && (chunk == 0 || (chunk >= 16 && chunk <= 4096)) && waves >= 0 && waves <= 64,
+               "ob_chol_tile: bad argument");
+    Factor* F = static_cast<Factor*>(factor);
+    if (chunk == F->tile_chunk && waves == F->tile_waves) return OB_OK;
+    {
+        // No pass of this factor may be in flight while its tile lists are replaced.
+        std::lock_guard<std::recursive_mutex> guard(capture_mutex());
+        OB_CUDA(cudaDeviceSynchronize());
+    }
+    // Every recorded pass names the old lists: drop them, and move the work generations so the
+    // callers' own recordings are made again.
+    for (auto& W : F->sets) {
+        for (auto& g : W.graphs) cudaGraphExecDestroy(g.exec);
+        W.graphs.clear();
+        ++W.generation;
+    }
+    return build_tiles(F, chunk, waves, stream);
 }
 
 int ob_chol_work_generation(void* factor, long long* generation) {

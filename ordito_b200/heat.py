@@ -317,6 +317,15 @@ class HeatSolver:
                 ok = kept["factorization"].factor(self._sharing(role)) and ok
         return ok
 
+    def tune(self, k: int) -> dict:
+        """Tune both factors' pass schedules for batches of ``k`` columns (``tuning.tune_pass``);
+        factors them first if needed. Returns each system's tuning report."""
+        from ordito_b200.tuning import tune_pass  # noqa: PLC0415
+
+        if not self.factor():
+            raise RuntimeError("HeatSolver.tune: the systems could not be factored (over budget)")
+        return {"heat": tune_pass(self.heat_factor, k), "poisson": tune_pass(self.poisson_factor, k)}
+
     def single_query(self, sources: DeviceArray) -> DeviceArray:
         """Distances for one validated source set with both factors held (``_SingleQuery``)."""
         query = getattr(self, "_single_query", None)

@@ -97,6 +97,11 @@ class PackedMeshes:
         self.analysis = CholeskyAnalysis(self.heat_system, DeviceArray.from_host(shifted))
         self.heat_factor = SparseCholesky(self.heat_system, self.analysis, singular=False)
         self.poisson_factor = SparseCholesky(self.poisson_system, self.analysis, singular=True)
+        # The passes' tile schedule tuned to the union's tree at the batch width.
+        from ordito_b200.tuning import tune_pass  # noqa: PLC0415
+
+        self.tuning = {"heat": tune_pass(self.heat_factor, max_columns),
+                       "poisson": tune_pass(self.poisson_factor, max_columns)}
         # a8: the divergence's corner index and per-face terms over the union.
         self.corner_offsets = DeviceArray.empty(n + 1, np.int32)
         self.corner_slots = DeviceArray.empty(max(3 * self.n_faces, 1), np.int32)

@@ -1,0 +1,44 @@
+"""Autotuner of the batched pass's tile schedule (no counterpart in the reference).
+
+A factor's triangular pass is one launch per tree level and direction of 64 x 64 output tiles;
+on a level with few tiles, long inner dimensions are split over several tiles (more CTAs, shorter
+dependent chains, atomic accumulation). Which levels to split, and into how long pieces, depends
+on the tree -- its level sizes and separator widths -- and on the batch width. ``tune_pass`` times
+one pass of a factor at ``k`` columns for each candidate schedule (``ob_chol_tile`` + CUDA-event
+timing in ``ob_chol_time_solve``), keeps the fastest, and reports every candidate's time.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Any
+
+from ordito_b200 import _lib
+
+# (split chunk, waves): the inner range of a split tile (0: never split) and the level size, in
+# waves of the resident grid, below which a level is split. The factor's default is (64, 2).
+CANDIDATES: tuple[tuple[int, int], ...] = (
+    (64, 2), (0, 0), (32, 2), (128, 2), (64, 1), (64, 4), (128, 4), (32, 1),
+)
+
+
+def _time(factor: Any, k: int, reps: int) -> float:
+    ms = ctypes.c_float(0.0)
+    _lib.call("ob_chol_time_solve", factor.handle, int(k), 2, ctypes.byref(ms), None)  # warm
+    _lib.call("ob_chol_time_solve", factor.handle, int(k), int(reps), ctypes.byref(ms), None)
+    return float(ms.value)
+
+
+def tune_pass(factor: Any, k: int, *, reps: int = 10,
+              candidates: tuple[tuple[int, int], ...] = CANDIDATES) -> dict:
+    """Time ``factor``'s forward + backward pass at ``k`` columns under each candidate schedule
+    and keep the fastest. No pass of the factor may be in flight (retiling waits for the device
+    and makes every recording over the factor's buffers record again on its next launch).
+    Returns ``{"best": (chunk, waves), "ms": {(chunk, waves): ms, ...}}``."""
+    times: dict[tuple[int, int], float] = {}
+    for chunk, waves in candidates:
+        _lib.call("ob_chol_tile", factor.handle, int(chunk), int(waves), None)
+        times[(chunk, waves)] = _time(factor, k, reps)
+    best = min(times, key=times.get)
+    _lib.call("ob_chol_tile", factor.handle, best[0], best[1], None)
+    return {"best": best, "ms": times}

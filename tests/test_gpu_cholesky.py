@@ -271,3 +271,45 @@ def test_two_work_sets_give_the_same_answers(gpu) -> None:
         step.close()
     for s in streams:
         _lib.call("ob_stream_destroy", s)
+
+
+def test_pass_schedules_agree_and_the_tuner_keeps_one(gpu) -> None:
+    # Every tile schedule computes the same solve (split tiles only change the order of the
+    # atomic sums); the tuner keeps one of its candidates, and a recorded batch pass made before
+    # the retiling records again and still answers the same.
+    from ordito_b200 import _lib
+    from ordito_b200.tuning import CANDIDATES, tune_pass
+
+    v, f = meshes.small_torus()
+    n = v.shape[0]
+    mesh = Trimesh(v, f.reshape(-1))
+    solver = mesh.heat_solver(None, method="meshlab")
+    assert solver.factor()
+    rng = np.random.default_rng(2)
+    sets = [[int(s)] for s in rng.choice(n, size=8, replace=False)]
+    src, offsets, k = gheat._source_columns(sets, n)
+    import ctypes
+
+    stream = ctypes.c_void_p(0)
+    _lib.call("ob_stream_create", ctypes.byref(stream))
+    out = DeviceArray.empty((k, n), np.float64)
+    step = gheat.BatchStep(mesh, solver, src, offsets, k, out, stream)
+    step.launch()
+    _lib.call("ob_stream_synchronize", stream)
+    before = step.out.numpy()
+    answers = []
+    for chunk, waves in ((0, 0), (32, 4), (64, 2)):
+        _lib.call("ob_chol_tile", solver.heat_factor.handle, chunk, waves, None)
+        _lib.call("ob_chol_tile", solver.poisson_factor.handle, chunk, waves, None)
+        answers.append(gheat._batch_columns(mesh, solver, src, offsets, k, 0, True).numpy())
+    for a in answers:
+        assert np.allclose(a, before, rtol=0, atol=1e-12 * np.abs(before).max())
+    report = tune_pass(solver.heat_factor, k, reps=2)
+    assert report["best"] in CANDIDATES and set(report["ms"]) == set(CANDIDATES)
+    step.launch()
+    _lib.call("ob_stream_synchronize", stream)
+    after = step.out.numpy()
+    assert np.allclose(after, before, rtol=0, atol=1e-12 * np.abs(before).max())
+    step.close()
+    _lib.call("ob_stream_destroy", stream)
+    mesh.dispose()
