@@ -371,6 +371,13 @@ int ob_chol_work_generation(void* factor, long long* generation);
 int ob_chol_work_set(void* factor, int set, int n_columns, double** rhs, double** solution,
                      int* stride, const int32_t** iperm, const char** pinned, ob_stream_t stream);
 int ob_chol_solve_in_place_set(void* factor, int set, int n_columns, ob_stream_t stream);
+/* ob_chol_solve_in_place_sources: ob_chol_solve_in_place_set for a B that holds a batch of source
+ * indicators (as ob_seed_permuted writes them for sources / source_offsets, n_columns sets, vertex
+ * indices): the forward pass runs only the supernodes a source reaches -- its own and their
+ * ancestors -- since every other supernode's input block is zero (their Y rows are written as
+ * zero); the backward pass is full. Marks on the device (no host read), so it can be recorded. */
+int ob_chol_solve_in_place_sources(void* factor, int set, int n_columns, const int32_t* sources,
+                                   const int32_t* source_offsets, ob_stream_t stream);
 int ob_chol_work_generation_set(void* factor, int set, long long* generation);
 
 /* ---- Smoothed-aggregation multigrid and the mixed-precision solve --------------------------

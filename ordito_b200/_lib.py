@@ -116,6 +116,7 @@ SIGNATURES: dict[str, list] = {
     "ob_shift_permuted": [P, I, I, P, P, P, I, I, P, P],
     "ob_chol_time_solve": [P, I, I, POINTER(c_float), P],
     "ob_chol_tile": [P, I, I, P],
+    "ob_chol_solve_in_place_sources": [P, I, I, P, P, P],
     "ob_chol_info": [P, POINTER(ctypes.c_longlong)],
     "ob_chol_work_generation": [P, POINTER(ctypes.c_longlong)],
     "ob_chol_work_set": [P, I, I, POINTER(c_void_p), POINTER(c_void_p), POINTER(c_int), POINTER(c_void_p),

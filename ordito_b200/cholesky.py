@@ -131,6 +131,14 @@ class SparseCholesky:
         _lib.call("ob_chol_solve_in_place_set", self.handle, int(work_set), int(n_columns),
                   stream if stream is not None else DEFAULT_STREAM)
 
+    def solve_in_place_sources(self, n_columns: int, sources: Any, source_offsets: Any,
+                               stream: Any = None, work_set: int = 0) -> None:
+        """``solve_in_place`` for a right-hand side of source indicators (``ob_seed_permuted`` of
+        the same device ``sources`` / ``source_offsets``): the forward pass runs only the
+        supernodes the sources reach (``ob_chol_solve_in_place_sources``)."""
+        _lib.call("ob_chol_solve_in_place_sources", self.handle, int(work_set), int(n_columns),
+                  sources.ptr, source_offsets.ptr, stream if stream is not None else DEFAULT_STREAM)
+
     def solve_pointers(self, rhs: int, x: int, n_columns: int, refine: int, stream: Any = None) -> None:
         """``x = A^-1 rhs`` for ``n_columns`` interleaved columns ([n][n_columns]) plus ``refine``
         float64 refinement steps, all enqueued on the device (no read-back)."""

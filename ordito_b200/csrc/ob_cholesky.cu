@@ -653,6 +653,7 @@ struct Tile {
     // triangular (entry (i, kk) zero for kk > i: the forward L11^-1); 2 the backward
     // [L11^-1; G]^T (entry (i, kk) zero for kk < i while kk < tri_k = nc).
     int tri, tri_k;
+    int node;  // the supernode the tile belongs to (a forward pass may skip inactive nodes)
 };
 
 constexpr int kTileRows = 64;   // output rows per tile
@@ -821,12 +822,30 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
 // The two stages live in dynamic shared memory (kStageBytes, above the 48 KB static limit).
 constexpr int kStageBytes = 2 * (int)sizeof(Stage);
 
+// A forward pass over right-hand sides that are zero outside the marked supernodes (a batch of
+// source indicators: only a source's supernode and its ancestors receive anything): a tile of an
+// unmarked node has a zero input block. It writes zeros where it assigns and is skipped where it
+// accumulates. Returns whether the tile was handled so.
+__device__ __forceinline__ bool skip_inactive(const Tile& t, const unsigned char* active, int c0, int width,
+                                              const int* idx, double* out, int k) {
+    if (active == nullptr || active[t.node]) return false;
+    if (t.op == kAssign)
+        for (int e = threadIdx.x; e < t.rows * width; e += blockDim.x) {
+            const int i = e / width, c = c0 + e % width;
+            if (c >= k) continue;
+            const int r = t.out_rows < 0 ? t.out_base + t.r0 + i : idx[t.out_rows + t.r0 + i];
+            out[(size_t)r * k + c] = 0.0;
+        }
+    return true;
+}
+
 // One launch per phase: a CTA per (tile, column block).
 __global__ void __launch_bounds__(kTileThreads)
 tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
-                    const int* __restrict__ idx, double* rows, int k) {
+                    const int* __restrict__ idx, double* rows, int k, const unsigned char* active) {
     extern __shared__ __align__(16) unsigned char shared_stages[];
     Stage* stage = reinterpret_cast<Stage*>(shared_stages);
+    if (skip_inactive(tiles[blockIdx.x], active, blockIdx.y * kTileCols, kTileCols, idx, rows, k)) return;
     tile_product(tiles[blockIdx.x], blockIdx.y * kTileCols, vals, idx, rows, rows, k, stage);
 }
 
@@ -843,7 +862,8 @@ constexpr int kNarrowSlices = kNarrowThreads / kTileRows;
 template <int KP>
 __global__ void __launch_bounds__(kNarrowThreads)
 narrow_tile_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
-                   const int* __restrict__ idx, double* rows) {
+                   const int* __restrict__ idx, double* rows, const unsigned char* active) {
+    if (skip_inactive(tiles[blockIdx.x], active, 0, KP, idx, rows, KP)) return;
     const double* in = rows;
     double* out = rows;
     __shared__ double other[kNarrowSlices - 1][kTileRows][KP];
@@ -977,6 +997,11 @@ struct Factor {
     int2* zero = nullptr;  // row ranges split tiles accumulate into (zeroed each pass)
     int n_zero = 0;
     int tile_chunk = 0, tile_waves = 0;  // the split parameters the tile lists were built with
+    // Device: each row's supernode and each supernode's parent (-1 at a root), for marking the
+    // supernodes a batch of source indicators reaches.
+    int* node_of_row = nullptr;
+    int* parent_node = nullptr;
+    int n_nodes = 0;
     // Per node: offsets of its [L11^-1; G] block in vals, of its row lists in idx, and its ld.
     std::vector<long long> inv_at, off_at;
     std::vector<int> rows_at, back_at, ld_at;
@@ -997,6 +1022,7 @@ struct Factor {
     struct WorkSet {
         int cap_k = 0;
         double *BYX = nullptr, *R = nullptr, *RHS = nullptr, *SOL = nullptr;
+        unsigned char* active = nullptr;  // device, one flag a supernode (marked sources)
         // B, Y and X at the even column stride kp of a call: n rows of kp doubles each.
         double* B() const { return BYX; }
         double* Y(int kp, int n) const { return BYX + (size_t)n * kp; }
@@ -1098,17 +1124,17 @@ int build_tiles(Factor* F, int chunk, int waves, cudaStream_t stream) {
         for (int r0 = 0; r0 < nc; r0 += kTileRows) {
             const int rows = std::min(kTileRows, nc - r0);
             // Forward diagonal: Y[own] = L11^-1 B[own].
-            zero |= emit(fw[nd.level], Tile{inv_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, n + nd.start, -1, 0, 1, nc},
+            zero |= emit(fw[nd.level], Tile{inv_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, n + nd.start, -1, 0, 1, nc, s},
                          nc, split_fwd, kAssign, kAtomicAdd);
             // Backward: X[own] = [L11^-1; G]^T [Y[own]; X[off rows]].
-            zero |= emit(bw[nd.level], Tile{inv_at[s], ld, 1, r0, rows, 0, 0, 0, back_at[s], 2 * n + nd.start, -1, 0, 2, nc},
+            zero |= emit(bw[nd.level], Tile{inv_at[s], ld, 1, r0, rows, 0, 0, 0, back_at[s], 2 * n + nd.start, -1, 0, 2, nc, s},
                          nc + noff, split_bwd, kAssign, kAtomicAdd);
         }
         if (zero) zero_ranges.push_back(make_int2(nd.start, nc));
         for (int r0 = 0; r0 < noff; r0 += kTileRows) {
             const int rows = std::min(kTileRows, noff - r0);
             // Forward update: B[off rows] += G B[own].
-            emit(fw[nd.level], Tile{off_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, 0, rows_at[s], 0, 0, 0},
+            emit(fw[nd.level], Tile{off_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, 0, rows_at[s], 0, 0, 0, s},
                  nc, split_fwd, kAtomicAdd, kAtomicAdd);
         }
     }
@@ -1212,6 +1238,25 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
     OB_CUDA(cudaMemcpyAsync(F->perm, A.perm.data(), sizeof(int) * A.n, cudaMemcpyHostToDevice,
                             stream));
     OB_CUDA(cudaMemcpyAsync(F->pinned, H.pinned.data(), A.n, cudaMemcpyHostToDevice, stream));
+    // Each row's supernode and each supernode's parent, and a marking buffer per work set.
+    {
+        std::vector<int> node_of_row(std::max(n, 1), -1), parent(std::max(ns, 1), -1);
+        for (int s = 0; s < ns; ++s) {
+            parent[s] = A.nodes[s].parent;
+            for (int j = 0; j < A.nodes[s].count; ++j) node_of_row[A.nodes[s].start + j] = s;
+        }
+        if ((st = dev_alloc(F, (void**)&F->node_of_row, sizeof(int) * node_of_row.size(), stream)) ||
+            (st = dev_alloc(F, (void**)&F->parent_node, sizeof(int) * parent.size(), stream)))
+            return st;
+        OB_CUDA(cudaMemcpyAsync(F->node_of_row, node_of_row.data(), sizeof(int) * node_of_row.size(),
+                                cudaMemcpyHostToDevice, stream));
+        OB_CUDA(cudaMemcpyAsync(F->parent_node, parent.data(), sizeof(int) * parent.size(),
+                                cudaMemcpyHostToDevice, stream));
+        OB_CUDA(cudaStreamSynchronize(stream));
+        F->n_nodes = ns;
+        for (auto& W : F->sets)
+            if ((st = dev_alloc(F, (void**)&W.active, std::max(ns, 1), stream))) return st;
+    }
     F->inv_at = std::move(inv_at);
     F->off_at = std::move(off_at);
     F->rows_at = std::move(rows_at);
@@ -1254,7 +1299,28 @@ int ensure_work(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream) {
 }
 
 // x_new = A^-1 b_new in the factor's numbering (B is consumed); k is the even internal stride.
-int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream) {
+// Marks the supernodes a batch of source indicators reaches: each source's supernode (through
+// the factor's numbering) and every ancestor, up to one already marked (whose marker goes on to
+// the root). sources[source_offsets[0] .. source_offsets[n_columns]) are vertex indices.
+__global__ void mark_sources_kernel(const int* __restrict__ sources, const int* __restrict__ source_offsets,
+                                    int n_columns, const int* __restrict__ iperm, const int* __restrict__ node_of_row,
+                                    const int* __restrict__ parent, unsigned char* active) {
+    const int total = source_offsets[n_columns] - source_offsets[0];
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+        int node = node_of_row[iperm[sources[source_offsets[0] + i]]];
+        while (node >= 0) {
+            const unsigned char was = active[node];
+            active[node] = 1;
+            if (was) break;
+            node = parent[node];
+        }
+    }
+}
+
+// forward_active: the marked supernodes of a batch of source indicators (see skip_inactive), or
+// nullptr; the backward pass is always full.
+int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream,
+                      const unsigned char* forward_active = nullptr) {
     const int L = F->analysis->levels;
     const int ct = (k + kTileCols - 1) / kTileCols;
     if (F->n_zero > 0) {
@@ -1263,24 +1329,24 @@ int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream)
     }
     // A level's launch: the float64 tensor-core tiles, or for a narrow batch (stride 2-8) the
     // register kernel, which does not compute a 64-column tile's idle columns.
-    auto level = [&](const Tile* tiles, int count, const char* what) {
+    auto level = [&](const Tile* tiles, int count, const unsigned char* active, const char* what) {
         switch (k) {
-            case 2: narrow_tile_kernel<2><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX); break;
-            case 4: narrow_tile_kernel<4><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX); break;
-            case 6: narrow_tile_kernel<6><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX); break;
-            case 8: narrow_tile_kernel<8><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX); break;
+            case 2: narrow_tile_kernel<2><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active); break;
+            case 4: narrow_tile_kernel<4><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active); break;
+            case 6: narrow_tile_kernel<6><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active); break;
+            case 8: narrow_tile_kernel<8><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active); break;
             default:
                 tile_product_kernel<<<dim3(count, ct), kTileThreads, kStageBytes, stream>>>(tiles, F->vals, F->idx,
-                                                                                          W.BYX, k);
+                                                                                          W.BYX, k, active);
         }
         OB_CHECK_LAUNCH(what);
         return OB_OK;
     };
     int st = OB_OK;
     for (int l = 0; l < L && st == OB_OK; ++l)
-        if (F->n_fwd[l]) st = level(F->fwd[l], F->n_fwd[l], "chol forward level");
+        if (F->n_fwd[l]) st = level(F->fwd[l], F->n_fwd[l], forward_active, "chol forward level");
     for (int l = L - 1; l >= 0 && st == OB_OK; --l)
-        if (F->n_bwd[l]) st = level(F->bwd[l], F->n_bwd[l], "chol backward level");
+        if (F->n_bwd[l]) st = level(F->bwd[l], F->n_bwd[l], nullptr, "chol backward level");
     return st;
 }
 
@@ -1536,6 +1602,30 @@ int ob_chol_solve_in_place_set(void* factor, int set, int n_columns, ob_stream_t
     OB_CUDA(cudaGraphLaunch(g->exec, stream));
     count_launch((uint64_t)g->launches);
     return OB_OK;
+}
+
+int ob_chol_solve_in_place_sources(void* factor, int set, int n_columns, const int32_t* sources,
+                                   const int32_t* source_offsets, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(factor && n_columns >= 1 && sources && source_offsets, "ob_chol_solve_in_place_sources: bad argument");
+    OB_REQUIRE(set >= 0 && set < kWorkSets, "ob_chol_solve_in_place_sources: set %d outside [0, %d)", set,
+               kWorkSets);
+    Factor* F = static_cast<Factor*>(factor);
+    Factor::WorkSet& W = F->sets[set];
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    OB_CUDA(cudaStreamIsCapturing(stream, &capturing));
+    if (capturing == cudaStreamCaptureStatusActive) {
+        OB_REQUIRE(n_columns <= W.cap_k, "ob_chol_solve_in_place_sources: %d columns not prepared before "
+                   "capture (ob_chol_work first)", n_columns);
+    } else {
+        int st = ensure_work(F, W, n_columns, stream);
+        if (st) return st;
+    }
+    OB_CUDA(cudaMemsetAsync(W.active, 0, std::max(F->n_nodes, 1), stream));
+    mark_sources_kernel<<<1, 256, 0, stream>>>(sources, source_offsets, n_columns, F->iperm, F->node_of_row,
+                                              F->parent_node, W.active);
+    OB_CHECK_LAUNCH("chol mark sources");
+    return triangular_solves(F, W, even_columns(n_columns), stream, W.active);
 }
 
 int ob_chol_buffers(void* factor, int n_columns, double** rhs, double** solution,

@@ -662,7 +662,7 @@ def _batch_columns(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offset
         p_rhs, p_sol, p_stride, p_iperm, p_pinned = poisson_factor.work(k, st, work_set)
         _lib.call("ob_seed_permuted", src.ptr, offsets.ptr, k, n, h_iperm, h_pinned, h_stride,
                   h_rhs, st)
-        heat_factor.solve_in_place(k, st, work_set)
+        heat_factor.solve_in_place_sources(k, src, offsets, st, work_set)
         _divergence(mesh, solver, k, h_sol, h_stride, h_iperm, p_rhs, p_stride, p_iperm, p_pinned, st)
         poisson_factor.solve_in_place(k, st, work_set)
         if out is None:

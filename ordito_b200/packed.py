@@ -165,7 +165,7 @@ class PackedMeshes:
         p_rhs, p_sol, p_stride, p_iperm, p_pinned = pf.work(k, stream)
         _lib.call("ob_seed_permuted", self.d_sources.ptr, self.d_offsets.ptr, k, n, h_iperm, h_pinned,
                   h_stride, h_rhs, stream)
-        hf.solve_in_place(k, stream)
+        hf.solve_in_place_sources(k, self.d_sources, self.d_offsets, stream)
         _lib.call(
             "ob_grad_div_terms", self.gradient_terms.ptr, self.faces.ptr, self.corner_offsets.ptr,
             self.corner_slots.ptr, n, k, h_sol, h_stride, h_iperm, p_rhs, p_stride, p_iperm, p_pinned,

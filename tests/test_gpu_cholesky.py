@@ -313,3 +313,33 @@ def test_pass_schedules_agree_and_the_tuner_keeps_one(gpu) -> None:
     step.close()
     _lib.call("ob_stream_destroy", stream)
     mesh.dispose()
+
+
+def test_forward_pass_over_marked_sources_equals_the_full_pass(gpu) -> None:
+    # Source indicators leave every supernode off their paths to the root with a zero input
+    # block: the pass that runs only the marked ones (narrow and tensor-core kernels) answers as
+    # the full pass does.
+    from ordito_b200 import _lib
+
+    v, f = meshes.small_torus()
+    n = v.shape[0]
+    mesh = Trimesh(v, f.reshape(-1))
+    solver = mesh.heat_solver(None, method="meshlab")
+    assert solver.factor()
+    factor = solver.heat_factor
+    rng = np.random.default_rng(4)
+    for k in (1, 5, 64):
+        sets = [rng.choice(n, size=int(rng.integers(1, 4)), replace=False).tolist() for _ in range(k)]
+        src, offsets, _ = gheat._source_columns(sets, n)
+        results = []
+        for sparse in (False, True):
+            rhs, sol, stride, iperm, pinned = factor.work(k)
+            _lib.call("ob_seed_permuted", src.ptr, offsets.ptr, k, n, iperm, pinned, stride, rhs, None)
+            if sparse:
+                factor.solve_in_place_sources(k, src, offsets, None)
+            else:
+                factor.solve_in_place(k, None)
+            results.append(DeviceArray(sol, (n, stride), np.float64, owned=False).numpy()[:, :k].copy())
+        full, marked = results
+        assert np.allclose(marked, full, rtol=0, atol=1e-14 * np.abs(full).max())
+    mesh.dispose()
