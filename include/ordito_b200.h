@@ -70,6 +70,10 @@ int ob_event_query(void* event, int* done);               /* done = 1 once the e
 int ob_event_synchronize(void* event);                    /* waits for the event on the host  */
 int ob_stream_wait_event(ob_stream_t stream, void* event); /* later work on stream waits for it */
 int ob_mem_info(size_t* free_bytes, size_t* total_bytes); /* the device's free / total memory  */
+/* The library allocates from the current device's default stream-ordered pool and keeps what it
+ * frees there for its next allocations (ob_mem_info counts that memory as free). ob_mem_trim
+ * synchronises the device and hands all but keep_bytes of it back to the driver. */
+int ob_mem_trim(size_t keep_bytes);
 /* Recording a sequence of this library's calls as one CUDA graph: ob_capture_begin(stream)
  * (a created stream), the calls on that stream, ob_capture_end -> a graph replayed by
  * ob_graph_launch on any stream; *kernels = the kernel launches one replay makes (counted by

@@ -58,6 +58,7 @@ SIGNATURES: dict[str, list] = {
     "ob_event_synchronize": [P],
     "ob_stream_wait_event": [P, P],
     "ob_mem_info": [POINTER(c_size_t), POINTER(c_size_t)],
+    "ob_mem_trim": [c_size_t],
     "ob_capture_begin": [P],
     "ob_capture_end": [P, POINTER(c_void_p), POINTER(c_int)],
     "ob_graph_launch": [P, P],

@@ -1037,14 +1037,14 @@ struct Factor {
 };
 
 int dev_alloc(Factor* F, void** p, size_t bytes, cudaStream_t stream) {
-    OB_CUDA(cudaMallocAsync(p, std::max<size_t>(bytes, 8), stream));
+    OB_CUDA(pool_malloc(p, std::max<size_t>(bytes, 8), stream));
     F->owned.push_back(*p);
     F->bytes += bytes;
     return OB_OK;
 }
 
 int tile_alloc(Factor* F, void** p, size_t bytes, cudaStream_t stream) {
-    OB_CUDA(cudaMallocAsync(p, std::max<size_t>(bytes, 8), stream));
+    OB_CUDA(pool_malloc(p, std::max<size_t>(bytes, 8), stream));
     F->tile_owned.push_back(*p);
     return OB_OK;
 }

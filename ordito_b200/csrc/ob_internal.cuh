@@ -61,6 +61,13 @@ std::recursive_mutex& capture_mutex();
 // Number of SMs of the current device (cached per process; the library targets one device model).
 int sm_count();
 
+// Every device allocation of the library: stream-ordered, from the current device's default
+// memory pool. The first call on a device sets that pool to keep the memory freed into it across
+// synchronisations (the pool's default hands it back to the driver at every synchronise, and the
+// next call's allocations then map fresh pages: tens of milliseconds, varying from call to call,
+// for a call that allocates and frees its scratch each time). ob_mem_trim releases it.
+cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t stream);
+
 // Warp-level sum.
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {

@@ -218,7 +218,7 @@ struct Buffers {
     template <typename T>
     int take(T** p, size_t n) {
         void* q = nullptr;
-        const cudaError_t e = cudaMallocAsync(&q, sizeof(T) * std::max<size_t>(n, 1), stream);
+        const cudaError_t e = pool_malloc(&q, sizeof(T) * std::max<size_t>(n, 1), stream);
         if (e != cudaSuccess) return cuda_status(e, "ob_march_solve: allocation");
         owned.push_back(q);
         *p = static_cast<T*>(q);

@@ -516,7 +516,7 @@ int bind_operator(Solver* S, const int* offsets, const int* columns, const doubl
 }
 
 int solver_alloc(Solver* S, void** out, size_t bytes, cudaStream_t stream) {
-    OB_CUDA(cudaMallocAsync(out, bytes == 0 ? 8 : bytes, stream));
+    OB_CUDA(pool_malloc(out, bytes == 0 ? 8 : bytes, stream));
     S->owned.push_back(*out);
     return OB_OK;
 }

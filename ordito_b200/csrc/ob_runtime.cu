@@ -45,6 +45,37 @@ int sm_count() {
     return cached;
 }
 
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::atomic<int> g_pool_kept[kMaxDevices];
+
+// The current device's default pool, set (once per device) to keep freed memory.
+cudaError_t kept_pool(cudaMemPool_t* pool) {
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetDefaultMemPool(pool, device);
+    if (e != cudaSuccess) return e;
+    if (device >= 0 && device < kMaxDevices &&
+        g_pool_kept[device].load(std::memory_order_acquire) == 0) {
+        uint64_t keep = ~uint64_t(0);
+        e = cudaMemPoolSetAttribute(*pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) return e;
+        g_pool_kept[device].store(1, std::memory_order_release);
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t stream) {
+    cudaMemPool_t pool;
+    const cudaError_t e = kept_pool(&pool);
+    if (e != cudaSuccess) return e;
+    return cudaMallocAsync(p, bytes, stream);
+}
+
 }  // namespace ob
 
 using namespace ob;
@@ -82,7 +113,7 @@ int ob_malloc(size_t bytes, void** ptr, ob_stream_t stream) {
     if (bytes == 0) return OB_OK;
     // Stream-ordered pool allocation: freed blocks return to the device's default pool and are
     // reused without a driver call.
-    cudaError_t e = cudaMallocAsync(ptr, bytes, as_stream(stream));
+    cudaError_t e = pool_malloc(ptr, bytes, as_stream(stream));
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(e == cudaErrorMemoryAllocation ? OB_ERR_NOMEM : OB_ERR_CUDA,
@@ -214,6 +245,21 @@ int ob_event_query(void* event, int* done) {
 int ob_mem_info(size_t* free_bytes, size_t* total_bytes) {
     OB_REQUIRE(free_bytes != nullptr && total_bytes != nullptr, "ob_mem_info: bad argument");
     OB_CUDA(cudaMemGetInfo(free_bytes, total_bytes));
+    // Memory the library's pool keeps but no allocation uses is free to the library.
+    cudaMemPool_t pool;
+    OB_CUDA(kept_pool(&pool));
+    uint64_t reserved = 0, used = 0;
+    OB_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    OB_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+    if (reserved > used) *free_bytes += static_cast<size_t>(reserved - used);
+    return OB_OK;
+}
+
+int ob_mem_trim(size_t keep_bytes) {
+    cudaMemPool_t pool;
+    OB_CUDA(kept_pool(&pool));
+    OB_CUDA(cudaDeviceSynchronize());
+    OB_CUDA(cudaMemPoolTrimTo(pool, keep_bytes));
     return OB_OK;
 }
 

@@ -25,7 +25,7 @@ class Scratch {
             return nullptr;
         }
         void* p = nullptr;
-        cudaError_t e = cudaMallocAsync(&p, sizeof(T) * (n == 0 ? 1 : n), stream_);
+        cudaError_t e = pool_malloc(&p, sizeof(T) * (n == 0 ? 1 : n), stream_);
         if (e != cudaSuccess) {
             cudaGetLastError();
             status_ = cuda_status(e, "scratch allocation");

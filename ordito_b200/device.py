@@ -249,3 +249,9 @@ def element_count(obj: Any) -> int:
 
 def synchronize() -> None:
     _lib.call("ob_stream_synchronize", DEFAULT_STREAM)
+
+
+def trim_pool(keep_bytes: int = 0) -> None:
+    """Hand the device memory the library keeps for reuse back to the driver, all but
+    ``keep_bytes`` of it (after a device-wide synchronise)."""
+    _lib.call("ob_mem_trim", int(keep_bytes))

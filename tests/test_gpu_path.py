@@ -163,6 +163,35 @@ def test_launches_are_counted(gpu) -> None:
     assert _lib.launch_count() - before >= 10
 
 
+def test_freed_memory_stays_in_the_pool_and_counts_as_free(gpu) -> None:
+    # The library's pool keeps freed memory across synchronisations (reused by the next call
+    # without mapping pages again); ob_mem_info counts it as free, ob_mem_trim hands it back.
+    # Read against the driver's own free count, so other live allocations do not matter.
+    import ctypes
+
+    from cuda.bindings import driver
+
+    from ordito_b200.device import DeviceArray, synchronize, trim_pool
+
+    def kept_bytes() -> int:
+        free, total = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        _lib.call("ob_mem_info", ctypes.byref(free), ctypes.byref(total))
+        err, driver_free, _ = driver.cuMemGetInfo()
+        assert err == driver.CUresult.CUDA_SUCCESS
+        return int(free.value) - int(driver_free)
+
+    driver.cuInit(0)
+    block = DeviceArray.zeros(256 << 20, np.uint8)
+    del block
+    synchronize()
+    assert kept_bytes() >= 256 << 20
+    again = DeviceArray.empty(256 << 20, np.uint8)  # served from the kept memory
+    assert kept_bytes() >= 0
+    del again
+    trim_pool(0)
+    assert kept_bytes() < 256 << 20  # what stays is shared with live allocations
+
+
 def test_solver_state_rebinds_to_an_operator_of_the_same_shape(gpu) -> None:
     # A released operator's solver state serves the next operator of its shape (its own copy of
     # the operator, rebound, its recorded loop replayed): the answers are the new operator's.
