@@ -63,6 +63,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-packed", action="store_true")
     p.add_argument("--no-kernel-rooflines", action="store_true")
     p.add_argument("--no-serving-full-range", action="store_true")
+    p.add_argument("--no-tune", action="store_true")
     # Only the per-kernel rooflines, on icosphere(LEVEL) with 1 % radial noise (a profiling case).
     p.add_argument("--kernels-only", type=int, default=0, metavar="LEVEL")
     p.add_argument("--serving-requests", type=int, default=300)
@@ -157,7 +158,13 @@ class Clocks:
             )
         except OSError:
             self.proc = None
-        time.sleep(0.3)
+        # The timed region starts only once nvidia-smi samples: its start-up (NVML
+        # initialisation) takes driver locks that can stall this process's launches.
+        deadline = time.perf_counter() + 5.0
+        while (self.proc is not None and self.proc.poll() is None and time.perf_counter() < deadline
+               and os.path.getsize(self.path) == 0):
+            time.sleep(0.02)
+        time.sleep(0.1)
         return self
 
     def __exit__(self, *exc) -> None:
@@ -693,8 +700,9 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     mesh = Trimesh(vertices, faces.reshape(-1))
     solver = mesh.heat_solver(None, method="meshlab")
     assert solver.factor(), "factorisation refused"
-    # The passes' tile schedule tuned to this mesh's tree at the batch width (part of setup).
-    tuning = solver.tune(k)
+    # The passes' tile schedule tuned to this mesh's tree at the batch width (part of setup);
+    # --no-tune keeps the default schedule (short launch lists for profiling).
+    tuning = None if args.no_tune else solver.tune(k)
     synchronize()
     setup_s = time.perf_counter() - t0
     src, offsets, _ = gheat._source_columns(sets, n)
@@ -946,12 +954,13 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
                         "whole pass recorded once as a CUDA graph (one launch a step), "
                         f"{args.refine} float64 refinement step(s) per solve"
                         + (" (in-place passes in the factors' ordering)" if args.refine == 0 else ""),
-                "l2": "no flush; per step the two 147 MB factors (294 MB) exceed the 126 MB L2",
+                "l2": f"no flush; per step the two {8 * n_vals / 1e6:.0f} MB factors "
+                      f"({2 * 8 * n_vals / 1e6:.0f} MB) exceed the 126 MB L2",
                 "parallelism": f"replicas{dist.world}",
                 "setup_s": setup_s,
                 "pass_schedule": {role: {"best": list(report["best"]),
                                          "ms": {f"{c}/{w}": round(t, 4) for (c, w), t in report["ms"].items()}}
-                                  for role, report in tuning.items()},
+                                  for role, report in tuning.items()} if tuning else "default (not tuned)",
             },
             "accuracy": {"max_rel_linf_vs_fp64_oracle": max(errors), "checked_queries": len(check)},
             "e2e": {

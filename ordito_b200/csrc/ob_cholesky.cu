@@ -664,6 +664,9 @@ constexpr int kTileCols = 64;   // right-hand-side columns per tile
 constexpr int kTileK = 16;
 constexpr int kSplitK = 64;  // a split tile's inner-dimension range (32 measured slower: more atomics)
 constexpr int kTileThreads = 128;
+// Resident CTAs of the 64-column product an SM: at most 96 registers a thread and two stages of
+// 19.5 KB hold five (126 registers held four).
+constexpr int kTileCtasPerSm = 5;
 // Shared rows of 72 doubles: the 8 x 4 fragment loads of a warp then touch every 8-byte bank
 // pair exactly twice (the minimum for 256 bytes).
 constexpr int kLd = kTileCols + 8;
@@ -727,7 +730,17 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
     const double* M = vals + t.m;
     // Each operand block is 64 x kTileK doubles in 16-byte chunks, kChunks per thread.
     constexpr int kChunks = kTileRows * kTileK / 2 / kTileThreads;
-    auto issue = [&](int kb, Stage& s) {
+    // The input rows of this thread's chunks of an inner step (-1 past the inner range), read
+    // one step ahead of the copies that use them, so a gathered index's load latency is not
+    // paid in front of every step's copies.
+    auto input_rows = [&](int kb, int* r) {
+#pragma unroll
+        for (int q = 0; q < kChunks; ++q) {
+            const int kk = (threadIdx.x + q * kTileThreads) / (kTileCols / 2);
+            r[q] = kb + kk < t.k1 ? (t.in_rows < 0 ? t.in_base + kb + kk : idx[t.in_rows + kb + kk]) : -1;
+        }
+    };
+    auto issue = [&](int kb, const int* in_row, Stage& s) {
 #pragma unroll
         for (int q = 0; q < kChunks; ++q) {
             const int chunk = threadIdx.x + q * kTileThreads;
@@ -749,9 +762,8 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
             const int kk = chunk / (kTileCols / 2), c2 = 2 * (chunk % (kTileCols / 2));
             int valid = 0;
             const double* src = in;
-            if (kb + kk < t.k1 && c0 + c2 < k) {
-                const int r = t.in_rows < 0 ? t.in_base + kb + kk : idx[t.in_rows + kb + kk];
-                src = in + (size_t)r * k + c0 + c2;
+            if (in_row[q] >= 0 && c0 + c2 < k) {
+                src = in + (size_t)in_row[q] * k + c0 + c2;
                 valid = 16;
             }
             copy16_l2(&s.b[kk * kLd + c2], src, valid);
@@ -759,10 +771,22 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
         copy_commit();
     };
     const int steps = (t.k1 - t.k0 + kTileK - 1) / kTileK;
-    issue(t.k0, stage[0]);
+    int first_rows[kChunks], next_rows[kChunks];
+    input_rows(t.k0, first_rows);
+    issue(t.k0, first_rows, stage[0]);
+    if (steps > 1) input_rows(t.k0 + kTileK, next_rows);
+    // The output rows, read before the products so the epilogue does not wait on them.
+    int out_row[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const int local = wr + 8 * i + fr;
+        out_row[i] = local >= t.rows ? -1
+                     : (t.out_rows < 0 ? t.out_base + t.r0 + local : idx[t.out_rows + t.r0 + local]);
+    }
     for (int st = 0; st < steps; ++st) {
         if (st + 1 < steps) {
-            issue(t.k0 + (st + 1) * kTileK, stage[(st + 1) & 1]);
+            issue(t.k0 + (st + 1) * kTileK, next_rows, stage[(st + 1) & 1]);
+            if (st + 2 < steps) input_rows(t.k0 + (st + 2) * kTileK, next_rows);
             copy_wait<1>();
         } else {
             copy_wait<0>();
@@ -798,9 +822,8 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
     }
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
-        const int local = wr + 8 * i + fr;
-        if (local >= t.rows) continue;
-        const int r = t.out_rows < 0 ? t.out_base + t.r0 + local : idx[t.out_rows + t.r0 + local];
+        const int r = out_row[i];
+        if (r < 0) continue;
 #pragma unroll
         for (int j = 0; j < 8; ++j)
 #pragma unroll
@@ -840,7 +863,7 @@ __device__ __forceinline__ bool skip_inactive(const Tile& t, const unsigned char
 }
 
 // One launch per phase: a CTA per (tile, column block).
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kTileThreads, kTileCtasPerSm)
 tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
                     const int* __restrict__ idx, double* rows, int k, const unsigned char* active) {
     extern __shared__ __align__(16) unsigned char shared_stages[];
@@ -1071,13 +1094,15 @@ int allow_stage_memory() {
     if (device >= 0 && device < 64 && allowed[device]) return OB_OK;
     OB_CUDA(cudaFuncSetAttribute(tile_product_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kStageBytes));
+    OB_CUDA(cudaFuncSetAttribute(tile_product_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared));
     if (device >= 0 && device < 64) allowed[device] = 1;
     return OB_OK;
 }
 
 // The tile lists of the passes (and the row ranges their split tiles accumulate into), replacing
 // any built before. chunk: the inner-dimension range of a split tile (0: never split); waves:
-// levels with fewer tiles than that many waves of the resident grid (4 CTAs an SM) are split.
+// levels with fewer tiles than that many waves of the resident grid (kTileCtasPerSm an SM) are split.
 int build_tiles(Factor* F, int chunk, int waves, cudaStream_t stream) {
     for (void* p : F->tile_owned) OB_CUDA(cudaFreeAsync(p, stream));
     F->tile_owned.clear();
@@ -1095,7 +1120,7 @@ int build_tiles(Factor* F, int chunk, int waves, cudaStream_t stream) {
     const std::vector<long long>&inv_at = F->inv_at, &off_at = F->off_at;
     const std::vector<int>&rows_at = F->rows_at, &back_at = F->back_at, &ld_at = F->ld_at;
     const int L = A.levels;
-    const long long wave = 4LL * sm_count();
+    const long long wave = (long long)kTileCtasPerSm * sm_count();
     auto tiles_of = [](int rows) { return (rows + kTileRows - 1) / kTileRows; };
     std::vector<long long> fwd_count(L, 0), bwd_count(L, 0);
     for (const Node& nd : A.nodes) {

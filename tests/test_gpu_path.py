@@ -165,31 +165,47 @@ def test_launches_are_counted(gpu) -> None:
 
 def test_freed_memory_stays_in_the_pool_and_counts_as_free(gpu) -> None:
     # The library's pool keeps freed memory across synchronisations (reused by the next call
-    # without mapping pages again); ob_mem_info counts it as free, ob_mem_trim hands it back.
-    # Read against the driver's own free count, so other live allocations do not matter.
+    # without mapping pages again) instead of handing it back to the driver; ob_mem_info adds the
+    # pool's unused reservation to the driver's free count; ob_mem_trim hands it back. Read
+    # against the pool's and the driver's own counts, so other live allocations do not matter.
     import ctypes
 
     from cuda.bindings import driver
 
-    from ordito_b200.device import DeviceArray, synchronize, trim_pool
+    from ordito_b200.device import synchronize, trim_pool
 
-    def kept_bytes() -> int:
+    assert driver.cuInit(0)[0] == driver.CUresult.CUDA_SUCCESS
+
+    def counts() -> dict:
         free, total = ctypes.c_size_t(0), ctypes.c_size_t(0)
         _lib.call("ob_mem_info", ctypes.byref(free), ctypes.byref(total))
         err, driver_free, _ = driver.cuMemGetInfo()
         assert err == driver.CUresult.CUDA_SUCCESS
-        return int(free.value) - int(driver_free)
+        err, device = driver.cuCtxGetDevice()
+        err, pool = driver.cuDeviceGetDefaultMemPool(device)
+        attr = driver.CUmemPool_attribute
+        reserved = int(driver.cuMemPoolGetAttribute(pool, attr.CU_MEMPOOL_ATTR_RESERVED_MEM_CURRENT)[1])
+        used = int(driver.cuMemPoolGetAttribute(pool, attr.CU_MEMPOOL_ATTR_USED_MEM_CURRENT)[1])
+        threshold = int(driver.cuMemPoolGetAttribute(pool, attr.CU_MEMPOOL_ATTR_RELEASE_THRESHOLD)[1])
+        return {"free": int(free.value), "driver_free": int(driver_free), "reserved": reserved,
+                "used": used, "threshold": threshold}
 
-    driver.cuInit(0)
-    block = DeviceArray.zeros(256 << 20, np.uint8)
-    del block
+    size = 256 << 20
+    ptr = ctypes.c_void_p(0)
+    _lib.call("ob_malloc", size, ctypes.byref(ptr), None)
+    held = counts()
+    assert held["threshold"] == 2**64 - 1, held
+    _lib.call("ob_free", ptr, None)
     synchronize()
-    assert kept_bytes() >= 256 << 20
-    again = DeviceArray.empty(256 << 20, np.uint8)  # served from the kept memory
-    assert kept_bytes() >= 0
-    del again
+    freed = counts()
+    assert freed["used"] <= held["used"] - size, (held, freed)  # freed into the pool
+    assert freed["driver_free"] < held["driver_free"] + size, (held, freed)  # and kept there
+    assert freed["free"] == freed["driver_free"] + max(0, freed["reserved"] - freed["used"]), freed
     trim_pool(0)
-    assert kept_bytes() < 256 << 20  # what stays is shared with live allocations
+    trimmed = counts()
+    # What trimming can hand back depends on how the pool laid out other live allocations.
+    assert trimmed["reserved"] <= freed["reserved"], (freed, trimmed)
+    assert trimmed["driver_free"] >= freed["driver_free"], (freed, trimmed)
 
 
 def test_solver_state_rebinds_to_an_operator_of_the_same_shape(gpu) -> None:
