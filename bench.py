@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes
+import gc
 import json
 import os
 import statistics
@@ -40,7 +41,9 @@ UNIT = "solves/s"
 WORKLOAD = "jittered torus 512x256 (131072 V, 262144 F), 64 single-source queries per step"
 # DRAM bytes (read + write) of one triangular pass of this workload's heat factor at 64 columns,
 # measured once by ncu (dram__bytes_read.sum + dram__bytes_write.sum over the pass's 14 launches).
-PASS_TRAFFIC_BYTES = 626_375_424
+PASS_TRAFFIC_BYTES = 618_604_544
+# Timed windows of K steps each; the line's value is the median window's.
+TIMED_WINDOWS = 3
 
 
 def parse() -> argparse.Namespace:
@@ -64,6 +67,8 @@ def parse() -> argparse.Namespace:
     p.add_argument("--no-kernel-rooflines", action="store_true")
     p.add_argument("--no-serving-full-range", action="store_true")
     p.add_argument("--no-tune", action="store_true")
+    p.add_argument("--pass-schedule", default="", metavar="CHUNK/WAVES",
+                   help="a fixed split schedule of the passes instead of the tuned one")
     # Only the per-kernel rooflines, on icosphere(LEVEL) with 1 % radial noise (a profiling case).
     p.add_argument("--kernels-only", type=int, default=0, metavar="LEVEL")
     p.add_argument("--serving-requests", type=int, default=300)
@@ -702,7 +707,11 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     assert solver.factor(), "factorisation refused"
     # The passes' tile schedule tuned to this mesh's tree at the batch width (part of setup);
     # --no-tune keeps the default schedule (short launch lists for profiling).
-    tuning = None if args.no_tune else solver.tune(k)
+    tuning = None if args.no_tune or args.pass_schedule else solver.tune(k)
+    if args.pass_schedule:
+        chunk, waves = (int(x) for x in args.pass_schedule.split("/"))
+        for factor in (solver.heat_factor, solver.poisson_factor):
+            _lib.call("ob_chol_tile", factor.handle, chunk, waves, None)
     synchronize()
     setup_s = time.perf_counter() - t0
     src, offsets, _ = gheat._source_columns(sets, n)
@@ -757,22 +766,34 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     start, end = _events()
     dist.barrier()
     synchronize()
+    # No garbage collection inside the timed regions: a collection there pauses the launching
+    # thread while the device drains (the setup above leaves much garbage behind).
+    gc.collect()
+    gc.disable()
+    # Three windows of exactly K steps, each bracketed by a barrier and a device synchronise; the
+    # line reports the median window and lists all three (a one-off stall of a few hundred
+    # milliseconds inside a window was seen on some boxes, cause not identified).
+    windows = []
     launches0 = _lib.launch_count()
     with Clocks(dist.local_rank) as clocks:
-        _lib.call("ob_event_record", start, stream)
-        for other in streams[1:] if in_flight > 1 else []:
-            _lib.call("ob_stream_wait_event", other, start)
-        for _ in range(args.steps):
-            out = step()
-        for other in streams[1:] if in_flight > 1 else []:
-            joined = ctypes.c_void_p(0)
-            _lib.call("ob_event_create", ctypes.byref(joined))
-            _lib.call("ob_event_record", joined, other)
-            _lib.call("ob_stream_wait_event", stream, joined)
-        _lib.call("ob_event_record", end, stream)
-        synchronize()
-    launches = (_lib.launch_count() - launches0) // max(args.steps, 1)
-    ms = _elapsed(start, end) / args.steps
+        for _ in range(TIMED_WINDOWS):
+            dist.barrier()
+            synchronize()
+            _lib.call("ob_event_record", start, stream)
+            for other in streams[1:] if in_flight > 1 else []:
+                _lib.call("ob_stream_wait_event", other, start)
+            for _ in range(args.steps):
+                out = step()
+            for other in streams[1:] if in_flight > 1 else []:
+                joined = ctypes.c_void_p(0)
+                _lib.call("ob_event_create", ctypes.byref(joined))
+                _lib.call("ob_event_record", joined, other)
+                _lib.call("ob_stream_wait_event", stream, joined)
+            _lib.call("ob_event_record", end, stream)
+            synchronize()
+            windows.append(_elapsed(start, end) / args.steps)
+    launches = (_lib.launch_count() - launches0) // max(args.steps * TIMED_WINDOWS, 1)
+    ms = statistics.median(windows)
     single_ms = None
     if in_flight > 1:
         # The same steps one at a time (one stream, one work set), for the record.
@@ -818,6 +839,7 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
         e2e_path = ("heat.BatchPipeline: host source lists in, pinned host distances out, the pass "
                     "of one batch overlapping the copy back of the one before")
     e2e_value = dist.world * k / (e2e_ms / 1e3)
+    gc.enable()
 
     # Resident single query (the same factors, one right-hand side at a time).
     single = [[int(s)] for s in sources[:16]]
@@ -938,6 +960,7 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
             "steps": args.steps,
             "warmup": args.warmup,
             "ms_per_step": ms_max,
+            "timed_windows_ms_per_step": [round(w, 4) for w in windows],
             "batches_in_flight": in_flight,
             "one_in_flight": None if single_ms is None else {
                 "value": dist.world * k / (single_ms / 1e3), "ms_per_step": single_ms},
@@ -960,7 +983,7 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
                 "setup_s": setup_s,
                 "pass_schedule": {role: {"best": list(report["best"]),
                                          "ms": {f"{c}/{w}": round(t, 4) for (c, w), t in report["ms"].items()}}
-                                  for role, report in tuning.items()} if tuning else "default (not tuned)",
+                                  for role, report in tuning.items()} if tuning else (args.pass_schedule or "default (not tuned)"),
             },
             "accuracy": {"max_rel_linf_vs_fp64_oracle": max(errors), "checked_queries": len(check)},
             "e2e": {

@@ -329,6 +329,11 @@ int ob_chol_solve_in_place(void* factor, int n_columns, ob_stream_t stream);
  * right-hand side in its numbering (zeroed first; pinned rows stay 0).
  * ob_shift_permuted: heat.py:3134 _shift_to_sources for n_columns columns of phi held in a
  * factor's numbering (stride, iperm), written out transposed as out[c * V + v]. */
+/* ob_renumber: out[i] = map[indices[i]] for count indices (no reference counterpart: the served
+ * pass renumbers the face buffer into the factors' ordering once per mesh, so its divergence
+ * reads and writes factor rows with no inverse permutation per corner). */
+int ob_renumber(const int32_t* indices, long long count, const int32_t* map, int32_t* out,
+                ob_stream_t stream);
 int ob_corner_index_workspace(int n_vertices, int n_faces, size_t* bytes);
 int ob_corner_index(const int32_t* faces, int n_faces, int n_vertices, int32_t* corner_offsets,
                     int32_t* corner_slots, void* workspace, size_t workspace_bytes,

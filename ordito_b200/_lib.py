@@ -108,6 +108,7 @@ SIGNATURES: dict[str, list] = {
     "ob_chol_work": [P, I, POINTER(c_void_p), POINTER(c_void_p), POINTER(c_int), POINTER(c_void_p),
                      POINTER(c_void_p), P],
     "ob_chol_solve_in_place": [P, I, P],
+    "ob_renumber": [P, ctypes.c_longlong, P, P, P],
     "ob_corner_index_workspace": [I, I, POINTER(c_size_t)],
     "ob_corner_index": [P, I, I, P, P, P, c_size_t, P],
     "ob_grad_div_gather": [P, P, P, P, P, P, P, I, I, P, I, P, P, I, P, P, P],

@@ -131,6 +131,14 @@ __global__ void grad_div_gather_kernel(const float* __restrict__ xyz, const int*
     out[(size_t)row * out_stride + c] = (out_pinned && out_pinned[row]) ? 0.0 : acc;
 }
 
+// out[i] = map[indices[i]]: a face buffer renumbered into a factor's ordering (grid-stride).
+__global__ void renumber_kernel(const int* __restrict__ indices, long long count,
+                                const int* __restrict__ map, int* __restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = map[indices[i]];
+}
+
 // Per-face terms of the divergence that do not depend on u (once per mesh), 18 doubles a face:
 // the gradient bases n x e_k (e_0 = v2 - v1, e_1 = v0 - v2, e_2 = v1 - v0; zero for a face of
 // no area, whose gradient is zero) and, per corner e, the cotangent-weighted edge sum W_e with
@@ -420,6 +428,17 @@ int ob_corner_index_workspace(int n_vertices, int n_faces, size_t* bytes) {
         OB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const int*)nullptr, (int*)nullptr,
                                                 (const int*)nullptr, (int*)nullptr, corners));
     *bytes = align_up(sort_bytes) + 3 * align_up(sizeof(int) * (size_t)std::max(corners, 1)) + 256;
+    return OB_OK;
+}
+
+int ob_renumber(const int32_t* indices, long long count, const int32_t* map, int32_t* out,
+                ob_stream_t stream) {
+    OB_REQUIRE(count >= 0, "ob_renumber: negative count");
+    if (count == 0) return OB_OK;
+    OB_REQUIRE(indices && map && out, "ob_renumber: null pointer");
+    const int blocks = (int)std::min<long long>((count + kThreads - 1) / kThreads, 8LL * sm_count());
+    renumber_kernel<<<blocks, kThreads, 0, as_stream(stream)>>>(indices, count, map, out);
+    OB_CHECK_LAUNCH("renumber");
     return OB_OK;
 }
 

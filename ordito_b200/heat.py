@@ -516,6 +516,41 @@ def _divergence(mesh: Trimesh, solver: "HeatSolver", k: int, u: int, u_stride: i
     )  # fmt: skip
 
 
+def _corners_in_factor_rows(mesh: Trimesh, solver: "HeatSolver", h_iperm: int,
+                            p_iperm: int) -> tuple[DeviceArray, DeviceArray, DeviceArray] | None:
+    """The face buffer and the corner index renumbered into the factors' shared ordering (built
+    once per solver and ordering, outside any recording: the first eager pass builds it), so
+    the served divergence reads the heat rows and writes the Poisson rows with no inverse
+    permutation per corner; None when the two factors' orderings differ. A vertex's corners keep
+    their ascending slot order, so the sums are the same bits as in the vertex numbering."""
+    # Kept on the heat factor (its lifetime is the ordering's), keyed by both orderings.
+    holder = solver.heat_factor
+    key = (h_iperm, p_iperm, id(solver.poisson_factor))
+    cached = getattr(holder, "_factor_row_corners", None)
+    if cached is not None and cached[0] == key:
+        return cached[1]
+    n = mesh.n_vertices
+    same = h_iperm == p_iperm or np.array_equal(
+        DeviceArray(h_iperm, (n,), np.int32, owned=False).numpy(),
+        DeviceArray(p_iperm, (n,), np.int32, owned=False).numpy())
+    result = None
+    if same:
+        corners = 3 * mesh.n_faces
+        faces = DeviceArray.empty(max(corners, 1), np.int32)
+        _lib.call("ob_renumber", mesh.faces.ptr, corners, h_iperm, faces.ptr, DEFAULT_STREAM)
+        offsets = DeviceArray.empty(n + 1, np.int32)
+        slots = DeviceArray.empty(max(corners, 1), np.int32)
+        size = ctypes.c_size_t(0)
+        _lib.call("ob_corner_index_workspace", n, mesh.n_faces, ctypes.byref(size))
+        workspace = DeviceArray.empty(int(size.value), np.uint8)
+        _lib.call("ob_corner_index", faces.ptr, mesh.n_faces, n, offsets.ptr, slots.ptr,
+                  workspace.ptr, int(size.value), DEFAULT_STREAM)
+        _lib.call("ob_stream_synchronize", DEFAULT_STREAM)  # the arrays serve other streams
+        result = (faces, offsets, slots)
+    holder._factor_row_corners = (key, result)
+    return result
+
+
 def _distance_from_heat(mesh: Trimesh, solver: HeatSolver, sources: DeviceArray,
                         heat: DeviceArray, n_columns: int = 1,
                         source_offsets: DeviceArray | None = None) -> DeviceArray:
@@ -663,7 +698,16 @@ def _batch_columns(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offset
         _lib.call("ob_seed_permuted", src.ptr, offsets.ptr, k, n, h_iperm, h_pinned, h_stride,
                   h_rhs, st)
         heat_factor.solve_in_place_sources(k, src, offsets, st, work_set)
-        _divergence(mesh, solver, k, h_sol, h_stride, h_iperm, p_rhs, p_stride, p_iperm, p_pinned, st)
+        rows = _corners_in_factor_rows(mesh, solver, h_iperm, p_iperm)
+        if rows is None:
+            _divergence(mesh, solver, k, h_sol, h_stride, h_iperm, p_rhs, p_stride, p_iperm,
+                        p_pinned, st)
+        else:
+            faces_rows, corner_offsets, corner_slots = rows
+            _lib.call(
+                "ob_grad_div_terms", solver.gradient_terms.ptr, faces_rows.ptr, corner_offsets.ptr,
+                corner_slots.ptr, n, k, h_sol, h_stride, None, p_rhs, p_stride, None, p_pinned, st,
+            )  # fmt: skip
         poisson_factor.solve_in_place(k, st, work_set)
         if out is None:
             out = DeviceArray.empty((k, n), np.float64)
