@@ -191,8 +191,10 @@ __device__ __forceinline__ double inverse_power_of_two(double largest) {
 // A thread takes CP adjacent columns of one vertex, so the per-corner index and term loads are
 // shared by CP columns (with CP > 1 the strides are even and u, out 16-byte aligned: u is read
 // and out written as double2). Columns from n_columns up are written as zero.
+// CP = 4 is held to 64 registers a thread (4 blocks of 256 an SM instead of 3; a few bytes
+// spill to L1): 3.15 -> 2.91 ms on a 2.6M-vertex mesh at 64 columns.
 template <int CP>
-__global__ void grad_div_terms_kernel(const double* __restrict__ terms, const int* __restrict__ faces,
+__global__ void __launch_bounds__(256, CP == 4 ? 4 : 1) grad_div_terms_kernel(const double* __restrict__ terms, const int* __restrict__ faces,
                                       const int* __restrict__ corner_offsets,
                                       const int* __restrict__ corner_slots, int n, int k,
                                       const double* __restrict__ u, int u_stride,
