@@ -708,8 +708,8 @@ struct Stage {
 // One 64 x 64 output tile for a CTA of four warps, each warp a 16-row strip of all 64 columns as
 // 2 x 8 float64 MMA tiles (strips rather than quadrants, so a strip of padding rows, or of the
 // zero triangle of L11^-1 over an inner step, is skipped whole). The tile's matrix block and its gathered input rows are copied 16 inner steps at a
-// time into shared memory with asynchronous 16-byte copies (zero-filled at the edges), two stages
-// in flight: the next step's copies overlap the current step's MMAs. The output is assigned,
+// time into shared memory with asynchronous 16-byte copies (zero-filled at the edges), two stages:
+// the next step's copies, issued after the step's one barrier, overlap the current step's MMAs. The output is assigned,
 // subtracted, or added atomically per the tile's op. `k` (the column stride) is even and every
 // block row starts on 16 bytes, so every copy is aligned. `in` and `out` are the same stacked
 // work buffer: the rows a launch's tiles read are never rows any tile of that launch writes.
@@ -784,14 +784,14 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
                      : (t.out_rows < 0 ? t.out_base + t.r0 + local : idx[t.out_rows + t.r0 + local]);
     }
     for (int st = 0; st < steps; ++st) {
+        copy_wait<0>();
+        // Every thread's copies of step st have landed, and every warp is past the products of
+        // step st - 1, whose stage the next copies reuse: one barrier a step.
+        __syncthreads();
         if (st + 1 < steps) {
             issue(t.k0 + (st + 1) * kTileK, next_rows, stage[(st + 1) & 1]);
             if (st + 2 < steps) input_rows(t.k0 + (st + 2) * kTileK, next_rows);
-            copy_wait<1>();
-        } else {
-            copy_wait<0>();
         }
-        __syncthreads();
         const Stage& s = stage[st & 1];
         // A strip skips a whole inner step when all its products are known zeros: padding rows
         // past the tile, or the zero triangle of L11^-1 (the decision is warp-uniform and taken
@@ -818,7 +818,6 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
                     for (int j = 0; j < 8; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
             }
         }
-        __syncthreads();
     }
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
