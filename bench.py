@@ -230,18 +230,56 @@ def cpu_stream(vertices: np.ndarray, faces: np.ndarray, sources: np.ndarray) -> 
     return 1.0 / per_query, {"setup_s": setup, "per_query_s": per_query}
 
 
+_ORACLE_STATE = None
+
+
+def _oracle_worker_init(cols: int, rows: int, queries: int) -> None:
+    """A reference-arm worker: the workload and its two float64 factorisations, built once."""
+    global _ORACLE_STATE
+    from oracle import heat_path as hp
+
+    vertices, faces, _ = workload(argparse.Namespace(cols=cols, rows=rows, queries=queries))
+    t_eff, _ = hp.vertex_time(vertices, faces, None)
+    ops = hp.heat_operators(vertices, faces, t_eff)
+    factors = (hp.HeatFactor(hp.csr_matrix(ops["pattern"], ops["H"])),
+               hp.PoissonFactor(hp.csr_matrix(ops["pattern"], ops["P"])))
+    _ORACLE_STATE = (vertices, faces, ops, factors)
+
+
+def _oracle_worker_solve(share: list[int]) -> tuple[int, float]:
+    from oracle import heat_path as hp
+
+    vertices, faces, ops, factors = _ORACLE_STATE
+    t0 = time.perf_counter()
+    for s in share:
+        hp.heat_geodesic(vertices, faces, np.array([s]), operators=ops, factors=factors)
+    return len(share), time.perf_counter() - t0
+
+
 def run_reference(args: argparse.Namespace, dist: Dist) -> None:
+    """The oracle port on every host core: one worker process a core (spawned), each holding its
+    own factorisations (setup excluded), a step's queries shared among them; a step's time is
+    the slowest worker's."""
     if dist.rank != 0:
         return
+    import multiprocessing
+
     vertices, faces, sources = workload(args)
-    sample = sources[:4]
-    values, detail = [], {}
-    for _ in range(max(1, args.steps)):
-        v, detail = cpu_stream(vertices, faces, sample)
-        values.append(v)
-        if len(values) >= 3:
-            break
+    workers = max(1, min(len(os.sched_getaffinity(0)), len(sources)))
+    shares = [[int(s) for s in sources[w::workers]] for w in range(workers)]
+    ctx = multiprocessing.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(workers, initializer=_oracle_worker_init,
+                  initargs=(args.cols, args.rows, args.queries)) as pool:
+        pool.map(_oracle_worker_solve, [[s[0]] for s in shares], chunksize=1)  # every worker set up
+        setup = time.perf_counter() - t0
+        values = []
+        for _ in range(min(max(1, args.steps), 3)):
+            done = pool.map(_oracle_worker_solve, shares, chunksize=1)
+            values.append(sum(n for n, _ in done) / max(t for _, t in done))
     value = statistics.median(values)
+    sample = sources
+    detail = {"setup_s": setup}
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -260,10 +298,11 @@ def run_reference(args: argparse.Namespace, dist: Dist) -> None:
         "cpu_baseline": {
             "value": value,
             "unit": UNIT,
-            "cores": 1,
+            "cores": workers,
             "kind": "port",
-            "sample": f"{len(sample)} of the {len(sources)} queries per step, float64 scipy SuperLU "
-                      f"factorisations reused (their {detail.get('setup_s', 0):.2f} s setup excluded)",
+            "sample": f"all {len(sample)} queries of a step shared by {workers} worker processes, "
+                      f"float64 scipy SuperLU factorisations reused (their {detail.get('setup_s', 0):.2f} s "
+                      "setup excluded)",
         },
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
