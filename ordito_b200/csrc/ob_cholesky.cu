@@ -911,18 +911,38 @@ narrow_tile_kernel(const Tile* __restrict__ tiles, const double* __restrict__ va
                 acc[2 * c + 1] = fma(a, v.y, acc[2 * c + 1]);
             }
         };
-        constexpr int kStep = kNarrowSlices;
-        int kk = t.k0 + slice;
-        for (; kk + 3 * kStep < t.k1; kk += 4 * kStep) {
-            const int r0 = row(kk), r1 = row(kk + kStep), r2 = row(kk + 2 * kStep), r3 = row(kk + 3 * kStep);
-            const double a0 = value(kk), a1 = value(kk + kStep), a2 = value(kk + 2 * kStep),
-                         a3 = value(kk + 3 * kStep);
-            add(a0, r0);
-            add(a1, r1);
-            add(a2, r2);
-            add(a3, r3);
+        if (t.trans) {
+            // Column-major reads: the 64 threads of a slice read 64 consecutive values.
+            constexpr int kStep = kNarrowSlices;
+            int kk = t.k0 + slice;
+            for (; kk + 3 * kStep < t.k1; kk += 4 * kStep) {
+                const int r0 = row(kk), r1 = row(kk + kStep), r2 = row(kk + 2 * kStep), r3 = row(kk + 3 * kStep);
+                const double a0 = value(kk), a1 = value(kk + kStep), a2 = value(kk + 2 * kStep),
+                             a3 = value(kk + 3 * kStep);
+                add(a0, r0);
+                add(a1, r1);
+                add(a2, r2);
+                add(a3, r3);
+            }
+            for (; kk < t.k1; kk += kStep) add(value(kk), row(kk));
+        } else {
+            // Row-major reads: a thread reads four consecutive values of its row as two 16-byte
+            // loads (every block row starts on 16 bytes and k0 is even), slice s taking elements
+            // 4 s .. 4 s + 3 of every 16; the one group that straddles k1 is read element by
+            // element by its slice.
+            constexpr int kGroup = 4 * kNarrowSlices;
+            int kk = t.k0 + 4 * slice;
+            for (; kk + 3 < t.k1; kk += kGroup) {
+                const double2* p = reinterpret_cast<const double2*>(M + (size_t)(t.r0 + i) * t.ld + kk);
+                const int r0 = row(kk), r1 = row(kk + 1), r2 = row(kk + 2), r3 = row(kk + 3);
+                const double2 v01 = __ldg(p), v23 = __ldg(p + 1);
+                add(v01.x, r0);
+                add(v01.y, r1);
+                add(v23.x, r2);
+                add(v23.y, r3);
+            }
+            for (; kk < t.k1; ++kk) add(value(kk), row(kk));  // kk + 3 >= k1: at most 3
         }
-        for (; kk < t.k1; kk += kStep) add(value(kk), row(kk));
     }
     if (slice > 0) {
 #pragma unroll
