@@ -811,7 +811,7 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     gc.disable()
     # Three windows of exactly K steps, each bracketed by a barrier and a device synchronise; the
     # line reports the median window and lists all three (a one-off stall of a few hundred
-    # milliseconds inside a window was seen on some boxes, cause not identified).
+    # milliseconds inside a window was seen in some runs, cause not identified).
     windows = []
     launches0 = _lib.launch_count()
     with Clocks(dist.local_rank) as clocks:
