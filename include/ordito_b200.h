@@ -192,7 +192,8 @@ int ob_shift(double* phi, int n_vertices, const int32_t* sources, int n_sources,
  * OB_ERR_INVALID). Its scratch is a static device array of about 129 KiB that every device
  * loading the library holds until exit, shared by every call on that device: calls whose work
  * overlaps on the device race on it and must be ordered by the caller. The first call on each
- * device looks the array's address up (make it before any stream capture). */
+ * device looks the array's address up, and so does the first call after the device's context
+ * changed (a cudaDeviceReset by the host): make those calls before any stream capture. */
 int ob_shift_noalloc(double* phi, int n_vertices, const int32_t* sources, int n_sources,
                      const int32_t* source_offsets, int n_columns, int orient, ob_stream_t stream);
 
@@ -247,6 +248,10 @@ int ob_cast_scale(const void* in, int in_type, void* out, int out_type, long lon
  * (replaces kernels/heat.py:614 seed_source_indicator for several columns). */
 int ob_axpby(long long n, double a, const double* x, double b, const double* y, double* out,
              ob_stream_t stream);
+/* values[i] = max(values[i], floor) over n float32 values: the clamp of
+ * ordito.laplacian.cotmatrix_entries(nonnegative_weights=True) (kernels/laplacian.py:146-163,
+ * store_half_cotangents), applied to the half-cotangent table. */
+int ob_floor_f32(float* values, long long n, float floor, ob_stream_t stream);
 /* Measurement hook: the device's float64 FMA throughput (TFLOP/s) from a register-resident FMA
  * loop over every SM (the compute roofline of the float64 dense products). */
 int ob_fp64_peak(float* tflops, ob_stream_t stream);
@@ -268,9 +273,14 @@ int ob_spmv(int n, const int32_t* offsets, const int32_t* columns, const double*
  * NULL; dissection leaves of at most leaf_size vertices, <= 0 for the default) and the supernodal
  * structure; host work, reads the pattern back. info[0..4] = n,
  * supernodes, tree levels, factor entries, widest front.
- * ob_chol_factor: numeric factorisation of `values` over the analysed pattern; singular != 0 pins
- * the last vertex of each connected component (the Poisson system). OB_ERR_INDEFINITE on a
- * non-positive pivot. The factor (partitioned inverse) is uploaded to the device.
+ * ob_chol_factor: numeric factorisation of sign * values over the analysed pattern (sign = -1 when
+ * negated != 0: a negative (semi-)definite operator such as a cotangent Laplacian; the solves
+ * still answer A x = rhs), on the device (multifrontal, level by level, float64 tensor-core
+ * products; ordito/cholesky.py:1399 _factor). singular: 0 pins nothing, 1 pins the last vertex of
+ * every connected component, 2 pins it on the components whose rows all sum to zero (|row sum| <=
+ * 1e-10 |diagonal|, ordito/cholesky.py:76) -- a singular component is then solved up to a
+ * constant. A row with no (or a zero) diagonal is always pinned. OB_ERR_INDEFINITE on a pivot
+ * that is not positive (one read-back at the end; the call returns when the factor is ready).
  * ob_chol_solve: x = A^-1 rhs for n_columns interleaved columns ([n][n_columns]), then `refine`
  * float64 refinement steps x += A^-1 (rhs - A x) with the operator's CSR arrays (may be NULL when
  * refine == 0); level-scheduled batched dense products on the device, recorded once per
@@ -290,9 +300,13 @@ int ob_chol_host_analyse(int n, const int32_t* offsets, const int32_t* columns, 
                          int leaf_size, void** analysis);
 int ob_chol_analysis_nodes(void* analysis, int32_t* out);
 int ob_chol_analysis_destroy(void* analysis);
-int ob_chol_factor(void* analysis, const double* values, int singular, void** factor,
+int ob_chol_factor(void* analysis, const double* values, int singular, int negated, void** factor,
                    ob_stream_t stream);
 int ob_chol_nbytes(void* factor, size_t* bytes);
+/* The factor's stored values (every supernode's [L11^-1; G] block, padded rows included) copied
+ * into out (a device buffer of capacity doubles; NULL only asks *count). An inspection hook (no
+ * counterpart in the reference). */
+int ob_chol_values(void* factor, double* out, long long capacity, long long* count, ob_stream_t stream);
 /* Host check of the same analysis, factorisation and solve algorithm on host arrays (no device;
  * a test hook, no counterpart in the reference): x = A^-1 rhs for one column; info[0..3] as
  * ob_chol_analysis_info's first four (may be NULL). */
@@ -364,8 +378,8 @@ int ob_shift_permuted(const double* phi, int n_vertices, int stride, const int32
                       int orient, double* out, ob_stream_t stream);
 int ob_chol_time_solve(void* factor, int n_columns, int reps, float* ms, ob_stream_t stream);
 /* ob_chol_tile (a tuning hook; no counterpart in the reference): rebuild the passes' tile lists
- * with another split of long inner dimensions -- chunk: the inner range of a split tile (16 to
- * 4096, or 0: never split), applied at levels with fewer tiles than `waves` waves of the resident
+ * with another split of long inner dimensions -- chunk: the inner range of a split tile (a
+ * multiple of 8 from 16 to 4096, or 0: never split; other values are OB_ERR_INVALID), applied at levels with fewer tiles than `waves` waves of the resident
  * grid (0 to 64). Waits for the device, drops the factor's recorded solves and moves every work
  * set's generation (recordings over ob_chol_work buffers must be made again). The defaults after
  * ob_chol_factor are chunk 64, waves 2. */

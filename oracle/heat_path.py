@@ -392,11 +392,13 @@ def vertex_time(vertices: np.ndarray, faces: np.ndarray, t: float | None,
 
 def heat_operators(
     vertices: np.ndarray, faces: np.ndarray, t: float | None = None, *, mass_divisor: float = 3.0,
-    method: str = "meshlab", use_robust: bool = False,
+    method: str = "meshlab", use_robust: bool = False, cot: np.ndarray | None = None,
 ) -> dict[str, object]:
     """The heat operators over the cotmatrix pattern (heat.py:2015-2245): barycentric mass and
     the face-edge time step for ``"meshlab"``, the unique-edge time step for ``"potpourri3d"``,
     the Voronoi mass (divisor 1) and the unique-edge time step for ``"igl"`` (heat.py:2002-2012).
+    ``cot`` replaces the half-cotangent table the rows are summed from (a caller's own weights,
+    as ``cotmatrix(cot_entries=...)`` takes them, laplacian.py:371).
 
     Returns the pattern, the float32 cot table, normals, areas, area sums, ``L``, ``H = M - t L``,
     ``P = -L`` (float64 values over the pattern), the lumped mass and the time ``t`` used.
@@ -407,7 +409,8 @@ def heat_operators(
     pattern = mesh_operator_pattern(f, n)
     # use_robust: the half-cotangents of the mollified lengths (heat.py:2043-2056); the mass, the
     # normals and the areas stay the positions' own.
-    cot = cot_from_lengths(mollified_lengths(v, f)[0]) if use_robust else cotmatrix_entries(v, f)
+    if cot is None:
+        cot = cot_from_lengths(mollified_lengths(v, f)[0]) if use_robust else cotmatrix_entries(v, f)
     normals, areas = face_normals_and_areas(v, f)
     if method == "igl":
         sums = voronoi_area_sums(v, f, n)

@@ -7,12 +7,12 @@
 over ``CHOLESKY_MEMORY_BUDGET``, or not positive definite), ``solve(rhs, solution)`` solves by it.
 
 The ordering is a nested dissection of the operator's graph (geometric, from the vertex positions
-when given) and the supernodes are the dissection tree's nodes; the analysis and the numeric
-factorisation run on the host (``ob_chol_analyse`` / ``ob_chol_factor``), the triangular solves on
-the device, level by level, as batched dense products over all right-hand sides at once
-(``ob_chol_solve``). A singular operator (the Poisson system ``-L``) has one vertex per connected
-component pinned, so its solution is the consistent system's up to a constant per component
-(ordito/cholesky.py:17-20).
+when given) and the supernodes are the dissection tree's nodes; the analysis runs on the host
+(``ob_chol_analyse``), the numeric factorisation on the device (``ob_chol_factor``: multifrontal,
+level by level, float64 tensor-core products), and the triangular solves on the device, level by
+level, as batched dense products over all right-hand sides at once (``ob_chol_solve``). A singular
+operator (the Poisson system ``-L``) has one vertex per connected component pinned, so its
+solution is the consistent system's up to a constant per component (ordito/cholesky.py:17-20).
 """
 
 from __future__ import annotations
@@ -74,14 +74,28 @@ class CholeskyAnalysis:
             pass
 
 
-class SparseCholesky:
-    """A device-resident factor of one operator (ordito/cholesky.py:121)."""
+# ob_chol_factor's singular modes: pin nothing, pin every component, pin the zero-sum ones.
+_PIN_NONE, _PIN_ALL, _PIN_ZERO_SUM = 0, 1, 2
+# Rows whose diagonal ``sparse_cholesky(negated=None)`` sums to choose the sign it tries first
+# (ordito/cholesky.py:78).
+_SIGN_PROBE_ROWS = 64
 
-    def __init__(self, matrix: CsrMatrix, analysis: CholeskyAnalysis, *, singular: bool) -> None:
+
+class SparseCholesky:
+    """A device-resident factor of one operator (ordito/cholesky.py:121).
+
+    ``singular``: ``False`` pins nothing, ``True`` pins one vertex of every connected component,
+    ``None`` pins it on the components whose rows all sum to zero (the reference's rule,
+    ordito/cholesky.py:76). ``negated`` factors ``-matrix``; solves still answer ``matrix x = rhs``.
+    """
+
+    def __init__(self, matrix: CsrMatrix, analysis: CholeskyAnalysis, *, singular: bool | None = None,
+                 negated: bool = False) -> None:
         if analysis.n != matrix.nrow:
             raise ValueError("analysis was built for another operator size")
+        mode = _PIN_ZERO_SUM if singular is None else (_PIN_ALL if singular else _PIN_NONE)
         handle = ctypes.c_void_p(0)
-        status = _lib.lib.ob_chol_factor(analysis.handle, matrix.values.ptr, int(singular),
+        status = _lib.lib.ob_chol_factor(analysis.handle, matrix.values.ptr, mode, int(bool(negated)),
                                          ctypes.byref(handle), DEFAULT_STREAM)
         if status == _lib.OB_ERR_INDEFINITE:
             raise NotPositiveDefiniteError("sparse_cholesky: the operator is not positive definite")
@@ -89,7 +103,13 @@ class SparseCholesky:
         self.handle = handle
         self.matrix = matrix
         self.analysis = analysis
-        self.singular = singular
+        self.singular = singular is not False
+        self.negated = bool(negated)
+
+    @property
+    def n(self) -> int:
+        """Rows of the factored operator."""
+        return self.matrix.nrow
 
     @property
     def nbytes(self) -> int:
@@ -196,19 +216,49 @@ class SparseCholesky:
             pass
 
 
+def _leading_diagonal_negative(matrix: CsrMatrix) -> bool:
+    """Whether the diagonal of the first ``_SIGN_PROBE_ROWS`` rows sums below zero
+    (ordito/cholesky.py:642-660 tries that sign first)."""
+    rows = min(matrix.nrow, _SIGN_PROBE_ROWS)
+    if rows == 0:
+        return False
+    offsets = matrix.offsets.view(0, rows + 1).numpy()
+    end = int(offsets[-1])
+    columns = matrix.columns.view(0, end).numpy()
+    values = matrix.values.view(0, end).numpy()
+    total = 0.0
+    for r in range(rows):
+        span = slice(int(offsets[r]), int(offsets[r + 1]))
+        total += float(values[span][columns[span] == r].sum())
+    return total < 0.0
+
+
 def sparse_cholesky(matrix: CsrMatrix, coordinates: Any = None, *, negated: bool | None = False,
-                    singular: bool | None = None) -> SparseCholesky:
-    """Factor ``matrix`` (ordito/cholesky.py:538). ``singular`` None tries the operator as it is
-    and, on a non-positive pivot, again with one vertex per connected component pinned."""
-    if negated:
-        raise NotImplementedError("negated operators are not on the heat-geodesic path")
-    analysis = CholeskyAnalysis(matrix, coordinates)
-    if singular is None:
-        try:
-            return SparseCholesky(matrix, analysis, singular=False)
-        except NotPositiveDefiniteError:
-            return SparseCholesky(matrix, analysis, singular=True)
-    return SparseCholesky(matrix, analysis, singular=singular)
+                    expandable: bool = False) -> SparseCholesky:
+    """Factor ``matrix`` on the device (ordito/cholesky.py:538).
+
+    ``negated`` factors ``-matrix`` (a negative semi-definite operator such as a cotangent
+    Laplacian); solves still answer ``matrix x = rhs``. ``negated=None`` factors whichever sign
+    is positive definite over one analysis, the sign of the leading diagonal first. A component
+    whose rows all sum to zero is solved up to a constant (one of its vertices pinned).
+    ``expandable`` orders with leaves of half ``CHOLESKY_LEAF_ROWS`` rows (ordito orders so for a
+    later 2 x 2 block expansion of the operator; here it only changes the leaf size).
+    Raises ``NotPositiveDefiniteError`` when the operator (with ``negated=None``: either sign) is
+    not positive definite."""
+    if matrix.nrow != matrix.ncol:
+        raise ValueError("sparse_cholesky: matrix must be square")
+    if np.dtype(matrix.scalar_type) != np.float64:
+        raise ValueError("sparse_cholesky: matrix must hold float64 values")
+    leaf = CHOLESKY_LEAF_ROWS // 2 if expandable else CHOLESKY_LEAF_ROWS
+    analysis = CholeskyAnalysis(matrix, coordinates, leaf_size=leaf)
+    if negated is not None:
+        return SparseCholesky(matrix, analysis, singular=None, negated=bool(negated))
+    first = _leading_diagonal_negative(matrix)
+    try:
+        return SparseCholesky(matrix, analysis, singular=None, negated=first)
+    except NotPositiveDefiniteError:
+        pass
+    return SparseCholesky(matrix, analysis, singular=None, negated=not first)
 
 
 class OperatorFactorization:
@@ -241,15 +291,9 @@ class OperatorFactorization:
         if self.exceeds_budget():
             self.refused = True
             return False
-        singular = self.singular
         try:
-            if singular is None:
-                try:
-                    self.factorization = SparseCholesky(self.matrix, self.analysis, singular=False)
-                except NotPositiveDefiniteError:
-                    self.factorization = SparseCholesky(self.matrix, self.analysis, singular=True)
-            else:
-                self.factorization = SparseCholesky(self.matrix, self.analysis, singular=singular)
+            # singular None: the components whose rows all sum to zero are pinned.
+            self.factorization = SparseCholesky(self.matrix, self.analysis, singular=self.singular)
         except NotPositiveDefiniteError:
             self.indefinite = True
             self.refused = True

@@ -23,6 +23,7 @@
 #include <thread>
 #include <vector>
 
+#include "ob_chol.cuh"
 #include "ob_host.hpp"
 #include "ob_internal.cuh"
 
@@ -32,24 +33,8 @@ namespace {
 // Vertices a dissection leaf holds when the caller asks for the default (leaf_size <= 0).
 constexpr int kDefaultLeafSize = 96;
 
-struct Node {
-    int start = 0, count = 0;          // own columns [start, start + count) in the new numbering
-    int parent = -1;
-    std::vector<int> children;
-    std::vector<int> off_rows;         // ascending, > start + count - 1
-    int level = 0;                     // height from the leaves (leaf = 0)
-};
-
-struct Analysis {
-    int n = 0;
-    std::vector<int> perm;   // new -> old
-    std::vector<int> iperm;  // old -> new
-    std::vector<int> offsets, columns;  // the operator's pattern (old numbering)
-    std::vector<Node> nodes;            // postorder: children before parents
-    std::vector<int> component_last;    // per vertex (old): is it its component's pin (1/0)
-    long long factor_entries = 0;       // sum of nc * nc + (m - nc) * nc
-    int levels = 0;
-};
+using Node = CholNode;
+using Analysis = CholAnalysis;
 
 // ------------------------------------------------------------------------------------------
 // Ordering: recursive coordinate bisection with one-sided vertex separators.
@@ -321,13 +306,15 @@ int analyse(int n, std::vector<int> offsets, std::vector<int> columns, const flo
     for (int i = 0; i < n; ++i) A.iperm[A.perm[i]] = i;
     symbolic(A, adj_off, adj);
     amalgamate(A, adj_off, adj);
-    // Components (for pinning a singular operator): the last vertex of each in the new order.
+    // Components (for pinning a singular operator): each vertex's component label and the last
+    // vertex of each in the new order.
     A.component_last.assign(n, 0);
     std::vector<int> comp(n, -1);
     std::vector<int> queue;
+    A.n_components = 0;
     for (int seed = 0; seed < n; ++seed) {
         if (comp[seed] >= 0) continue;
-        comp[seed] = seed;
+        comp[seed] = A.n_components++;
         queue.assign(1, seed);
         int last = seed;
         for (size_t h = 0; h < queue.size(); ++h) {
@@ -335,12 +322,13 @@ int analyse(int n, std::vector<int> offsets, std::vector<int> columns, const flo
             if (A.iperm[v] > A.iperm[last]) last = v;
             for (int e = adj_off[v]; e < adj_off[v + 1]; ++e)
                 if (comp[adj[e]] < 0) {
-                    comp[adj[e]] = seed;
+                    comp[adj[e]] = comp[seed];
                     queue.push_back(adj[e]);
                 }
         }
         A.component_last[last] = 1;
     }
+    A.component = std::move(comp);
     return OB_OK;
 }
 
@@ -671,15 +659,6 @@ constexpr int kTileCtasPerSm = 5;
 // pair exactly twice (the minimum for 256 bytes).
 constexpr int kLd = kTileCols + 8;
 
-// D (8 x 8) += A (8 x 4) B (4 x 8) in float64 on the tensor cores (mma.sync m8n8k4 .f64, the
-// float64 matrix instruction sm_100 offers). Fragments: a = A[lane / 4][lane % 4],
-// b = B[lane % 4][lane / 4], d = D[lane / 4][2 (lane % 4) + {0, 1}].
-__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
-}
-
 // 16-byte asynchronous global -> shared copies; bytes < 16 zero-fills the rest (0: all zeros, and
 // the source is not read). Both read through L2 only: a factor block is read once per tile, and
 // with the shared-memory carveout at its maximum the L1 left over is small (caching the factor
@@ -995,13 +974,13 @@ __global__ void permute_in_kernel(int n, int k, int kp, const int* __restrict__ 
 
 __global__ void permute_out_kernel(int n, int k, int kp, const int* __restrict__ perm,
                                    const double* __restrict__ src, double* __restrict__ dst,
-                                   int accumulate) {
+                                   int accumulate, double scale) {
     const long long total = (long long)n * k;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(t / k), c = (int)(t % k);
         double* d = dst + (size_t)perm[i] * k + c;
-        const double v = src[(size_t)i * kp + c];
+        const double v = scale * src[(size_t)i * kp + c];
         *d = accumulate ? *d + v : v;
     }
 }
@@ -1026,6 +1005,7 @@ struct Factor {
     const Analysis* analysis = nullptr;
     int n = 0;
     bool singular = false;
+    double sign = 1.0;       // the factor is of sign * A: solves scale its answers by sign
     double* vals = nullptr;  // device: all inverses and panels
     int* idx = nullptr;      // device: off-diagonal row lists
     int* perm = nullptr;     // device: new -> old
@@ -1227,9 +1207,12 @@ int build_tiles(Factor* F, int chunk, int waves, cudaStream_t stream) {
     return OB_OK;
 }
 
-int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
+// The device factor: its block layout and row lists (from the analysis), then the numeric
+// factorisation of sign * values on the device (device_factor, ob_chol_factor.cu), then the
+// passes' tile lists.
+int setup_factor(Factor* F, const double* values, double sign, int pin_mode, cudaStream_t stream) {
     if (int st0 = allow_stage_memory()) return st0;
-    const Analysis& A = *F->analysis;
+    Analysis& A = *const_cast<Analysis*>(F->analysis);
     const int ns = (int)A.nodes.size();
     const int n = A.n;
     // Per node the stored block is [L11^-1; G] (nc + noff rows, G = -L21 L11^-1), every block row
@@ -1237,78 +1220,52 @@ int upload_factor(Factor* F, const HostFactor& H, cudaStream_t stream) {
     // 16-byte asynchronous copies are always aligned. idx holds per node its off-diagonal rows
     // (B rows, the forward update's outputs) and the backward product's input rows: its own Y rows
     // then its off-diagonal X rows, in the stacked [B; Y; X] numbering.
-    std::vector<long long> inv_at(ns), off_at(ns);
-    std::vector<int> rows_at(ns), back_at(ns), ld_at(ns);
-    long long total = 0, total_rows = 0;
-    for (int s = 0; s < ns; ++s) {
-        const int nc = A.nodes[s].count, noff = (int)A.nodes[s].off_rows.size();
-        const int ld = (nc + 7) / 8 * 8;
-        ld_at[s] = ld;
-        inv_at[s] = total;
-        total += (long long)nc * ld;
-        off_at[s] = total;
-        total += (long long)noff * ld;
-        rows_at[s] = (int)total_rows;
-        total_rows += noff;
-        back_at[s] = (int)total_rows;
-        total_rows += nc + noff;
-    }
-    OB_REQUIRE(total_rows < (1LL << 31) && 3LL * n < (1LL << 31), "ob_chol_factor: factor too large");
-    std::vector<double> vals(std::max<long long>(total, 1), 0.0);
-    std::vector<int> idx(std::max<long long>(total_rows, 1));
+    BlockLayout layout = block_layout(A);
+    OB_REQUIRE(layout.total_rows < (1LL << 31) && 3LL * n < (1LL << 31), "ob_chol_factor: factor too large");
+    std::vector<int> idx(std::max<long long>(layout.total_rows, 1));
     for (int s = 0; s < ns; ++s) {
         const Node& nd = A.nodes[s];
-        const int nc = nd.count, noff = (int)nd.off_rows.size(), ld = ld_at[s];
-        for (int i = 0; i < nc; ++i)
-            std::copy(H.inv[s].begin() + (size_t)i * nc, H.inv[s].begin() + (size_t)(i + 1) * nc,
-                      vals.begin() + inv_at[s] + (size_t)i * ld);
-        for (int r = 0; r < noff; ++r)
-            std::copy(H.off[s].begin() + (size_t)r * nc, H.off[s].begin() + (size_t)(r + 1) * nc,
-                      vals.begin() + off_at[s] + (size_t)r * ld);
-        std::copy(nd.off_rows.begin(), nd.off_rows.end(), idx.begin() + rows_at[s]);
-        for (int i = 0; i < nc; ++i) idx[back_at[s] + i] = n + nd.start + i;
-        for (int r = 0; r < noff; ++r) idx[back_at[s] + nc + r] = 2 * n + nd.off_rows[r];
+        const int nc = nd.count, noff = (int)nd.off_rows.size();
+        std::copy(nd.off_rows.begin(), nd.off_rows.end(), idx.begin() + layout.rows_at[s]);
+        for (int i = 0; i < nc; ++i) idx[layout.back_at[s] + i] = n + nd.start + i;
+        for (int r = 0; r < noff; ++r) idx[layout.back_at[s] + nc + r] = 2 * n + nd.off_rows[r];
     }
-    F->n_vals = total;
-    int st = dev_alloc(F, (void**)&F->vals, sizeof(double) * vals.size(), stream);
+    F->n_vals = layout.total;
+    int st = dev_alloc(F, (void**)&F->vals, sizeof(double) * std::max<long long>(layout.total, 1), stream);
     if (!st) st = dev_alloc(F, (void**)&F->idx, sizeof(int) * idx.size(), stream);
     if (!st) st = dev_alloc(F, (void**)&F->perm, sizeof(int) * A.n, stream);
     if (!st) st = dev_alloc(F, (void**)&F->iperm, sizeof(int) * A.n, stream);
     if (!st) st = dev_alloc(F, (void**)&F->pinned, std::max(A.n, 1), stream);
     if (st) return st;
-    OB_CUDA(cudaMemcpyAsync(F->vals, vals.data(), sizeof(double) * vals.size(),
-                            cudaMemcpyHostToDevice, stream));
     OB_CUDA(cudaMemcpyAsync(F->idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice,
                             stream));
     OB_CUDA(cudaMemcpyAsync(F->iperm, A.iperm.data(), sizeof(int) * A.n, cudaMemcpyHostToDevice,
                             stream));
     OB_CUDA(cudaMemcpyAsync(F->perm, A.perm.data(), sizeof(int) * A.n, cudaMemcpyHostToDevice,
                             stream));
-    OB_CUDA(cudaMemcpyAsync(F->pinned, H.pinned.data(), A.n, cudaMemcpyHostToDevice, stream));
     // Each row's supernode and each supernode's parent, and a marking buffer per work set.
-    {
-        std::vector<int> node_of_row(std::max(n, 1), -1), parent(std::max(ns, 1), -1);
-        for (int s = 0; s < ns; ++s) {
-            parent[s] = A.nodes[s].parent;
-            for (int j = 0; j < A.nodes[s].count; ++j) node_of_row[A.nodes[s].start + j] = s;
-        }
-        if ((st = dev_alloc(F, (void**)&F->node_of_row, sizeof(int) * node_of_row.size(), stream)) ||
-            (st = dev_alloc(F, (void**)&F->parent_node, sizeof(int) * parent.size(), stream)))
-            return st;
-        OB_CUDA(cudaMemcpyAsync(F->node_of_row, node_of_row.data(), sizeof(int) * node_of_row.size(),
-                                cudaMemcpyHostToDevice, stream));
-        OB_CUDA(cudaMemcpyAsync(F->parent_node, parent.data(), sizeof(int) * parent.size(),
-                                cudaMemcpyHostToDevice, stream));
-        OB_CUDA(cudaStreamSynchronize(stream));
-        F->n_nodes = ns;
-        for (auto& W : F->sets)
-            if ((st = dev_alloc(F, (void**)&W.active, std::max(ns, 1), stream))) return st;
+    std::vector<int> node_of_row(std::max(n, 1), -1), parent(std::max(ns, 1), -1);
+    for (int s = 0; s < ns; ++s) {
+        parent[s] = A.nodes[s].parent;
+        for (int j = 0; j < A.nodes[s].count; ++j) node_of_row[A.nodes[s].start + j] = s;
     }
-    F->inv_at = std::move(inv_at);
-    F->off_at = std::move(off_at);
-    F->rows_at = std::move(rows_at);
-    F->back_at = std::move(back_at);
-    F->ld_at = std::move(ld_at);
+    if ((st = dev_alloc(F, (void**)&F->node_of_row, sizeof(int) * node_of_row.size(), stream)) ||
+        (st = dev_alloc(F, (void**)&F->parent_node, sizeof(int) * parent.size(), stream)))
+        return st;
+    OB_CUDA(cudaMemcpyAsync(F->node_of_row, node_of_row.data(), sizeof(int) * node_of_row.size(),
+                            cudaMemcpyHostToDevice, stream));
+    OB_CUDA(cudaMemcpyAsync(F->parent_node, parent.data(), sizeof(int) * parent.size(),
+                            cudaMemcpyHostToDevice, stream));
+    F->n_nodes = ns;
+    for (auto& W : F->sets)
+        if ((st = dev_alloc(F, (void**)&W.active, std::max(ns, 1), stream))) return st;
+    F->inv_at = std::move(layout.inv_at);
+    F->off_at = std::move(layout.off_at);
+    F->rows_at = std::move(layout.rows_at);
+    F->back_at = std::move(layout.back_at);
+    F->ld_at = std::move(layout.ld_at);
+    // The numeric factorisation (synchronises once, to read its pivot status).
+    if ((st = device_factor(A, values, sign, pin_mode, F->vals, F->pinned, stream))) return st;
     if ((st = build_tiles(F, kSplitK, 2, stream))) return st;
     OB_CUDA(cudaStreamSynchronize(stream));  // host staging buffers go out of scope
     return OB_OK;
@@ -1410,7 +1367,7 @@ int enqueue_solve(Factor* F, Factor::WorkSet& W, int k, int refine, const int* o
     OB_CHECK_LAUNCH("chol permute in");
     int st = triangular_solves(F, W, kp, stream);
     if (st) return st;
-    permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, W.X(kp, n), W.SOL, 0);
+    permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, W.X(kp, n), W.SOL, 0, F->sign);
     OB_CHECK_LAUNCH("chol permute out");
     // Iterative refinement in float64: x += A^-1 (b - A x).
     for (int it = 0; it < refine; ++it) {
@@ -1421,7 +1378,7 @@ int enqueue_solve(Factor* F, Factor::WorkSet& W, int k, int refine, const int* o
         OB_CHECK_LAUNCH("chol permute in");
         st = triangular_solves(F, W, kp, stream);
         if (st) return st;
-        permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, W.X(kp, n), W.SOL, 1);
+        permute_out_kernel<<<grid, 256, 0, stream>>>(n, k, kp, F->perm, W.X(kp, n), W.SOL, 1, F->sign);
         OB_CHECK_LAUNCH("chol permute out");
     }
     return OB_OK;
@@ -1548,27 +1505,23 @@ int ob_chol_analysis_destroy(void* analysis) {
     return OB_OK;
 }
 
-int ob_chol_factor(void* analysis, const double* values, int singular, void** factor,
+int ob_chol_factor(void* analysis, const double* values, int singular, int negated, void** factor,
                    ob_stream_t stream_) {
     cudaStream_t stream = as_stream(stream_);
     OB_REQUIRE(analysis && values && factor, "ob_chol_factor: bad argument");
+    OB_REQUIRE(singular >= kPinNone && singular <= kPinZeroSum, "ob_chol_factor: singular = %d outside [0, 2]",
+               singular);
     *factor = nullptr;
-    const Analysis* A = static_cast<Analysis*>(analysis);
-    std::vector<double> host(std::max(A->offsets[A->n], 1));
-    OB_CUDA(cudaMemcpyAsync(host.data(), values, sizeof(double) * A->offsets[A->n],
-                            cudaMemcpyDeviceToHost, stream));
-    OB_CUDA(cudaStreamSynchronize(stream));
-    HostFactor H;
-    int st = numeric(*A, host.data(), singular != 0, &H);
-    if (st == OB_ERR_INDEFINITE) return fail(OB_ERR_INDEFINITE, "ob_chol_factor: not positive definite");
-    if (st) return st;
+    Analysis* A = static_cast<Analysis*>(analysis);
     Factor* F = new Factor();
     F->analysis = A;
     F->n = A->n;
-    F->singular = singular != 0;
-    st = upload_factor(F, H, stream);
+    F->singular = singular != kPinNone;
+    F->sign = negated ? -1.0 : 1.0;
+    int st = setup_factor(F, values, F->sign, singular, stream);
     if (st) {
         factor_release(F);
+        if (st == OB_ERR_INDEFINITE) return fail(OB_ERR_INDEFINITE, "ob_chol_factor: not positive definite");
         return st;
     }
     *factor = F;
@@ -1714,8 +1667,11 @@ int ob_chol_time_solve(void* factor, int n_columns, int reps, float* ms, ob_stre
 
 int ob_chol_tile(void* factor, int chunk, int waves, ob_stream_t stream_) {
     cudaStream_t stream = as_stream(stream_);
-    OB_REQUIRE(factor && (chunk == 0 || (chunk >= 16 && chunk <= 4096)) && waves >= 0 && waves <= 64,
-               "ob_chol_tile: bad argument");
+    OB_REQUIRE(factor != nullptr && waves >= 0 && waves <= 64, "ob_chol_tile: bad argument");
+    // A split tile's inner range starts at a multiple of chunk, and the tile kernels read the
+    // factor's rows from there in 16-byte pieces: chunk must keep every start on 16 bytes.
+    OB_REQUIRE(chunk == 0 || (chunk >= 16 && chunk <= 4096 && chunk % 8 == 0),
+               "ob_chol_tile: chunk %d is not 0 or a multiple of 8 in [16, 4096]", chunk);
     Factor* F = static_cast<Factor*>(factor);
     if (chunk == F->tile_chunk && waves == F->tile_waves) return OB_OK;
     {
@@ -1802,6 +1758,17 @@ int ob_chol_host_solve(int n, const int32_t* offsets, const int32_t* columns,
         }
     }
     for (int i = 0; i < n; ++i) x[A.perm[i]] = xs[i];
+    return OB_OK;
+}
+
+int ob_chol_values(void* factor, double* out, long long capacity, long long* count, ob_stream_t stream_) {
+    OB_REQUIRE(factor && count, "ob_chol_values: bad argument");
+    Factor* F = static_cast<Factor*>(factor);
+    *count = F->n_vals;
+    if (out == nullptr) return OB_OK;
+    OB_REQUIRE(capacity >= F->n_vals, "ob_chol_values: %lld values need room, %lld given", F->n_vals, capacity);
+    OB_CUDA(cudaMemcpyAsync(out, F->vals, sizeof(double) * (size_t)F->n_vals, cudaMemcpyDeviceToDevice,
+                            as_stream(stream_)));
     return OB_OK;
 }
 

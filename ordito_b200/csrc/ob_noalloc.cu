@@ -14,8 +14,12 @@
 // 129 KiB) until the process exits. Every call on a device shares that copy: the fold counter is
 // cleared at the start of each call and every other slot is written before it is read, but two
 // calls whose work overlaps on the device (different streams, no ordering between them) race on
-// it, so callers must order them. The array's device address is looked up once per device, on
-// the first call made with that device current; make that first call before any stream capture.
+// it, so callers must order them. The array's device address is looked up on the first call made
+// with a device current, and again whenever that device's context has changed since (a host that
+// reset the device gets a new context, in which the old address means nothing); make the first
+// call on each device, and the first after a reset, before any stream capture.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "ob_internal.cuh"
@@ -37,20 +41,48 @@ static __device__ __align__(256) double g_shift_scratch[kScratchDoubles];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_address_mutex;
+// Per device: the scratch's address and the context it was looked up in.
 double* g_address[kMaxDevices] = {};
+CUcontext g_context[kMaxDevices] = {};
 
-// The device address of g_shift_scratch for the current device (looked up once per device).
+// The driver's cuCtxGetCurrent, reached through the runtime (the library does not link the driver
+// library itself, so it still loads on a machine without one).
+typedef CUresult (*CtxGetCurrent)(CUcontext*);
+
+CUcontext current_context() {
+    static CtxGetCurrent fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, []() {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult found = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &found) == cudaSuccess &&
+            found == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrent>(p);
+        else
+            cudaGetLastError();
+    });
+    CUcontext context = nullptr;
+    if (fn == nullptr || fn(&context) != CUDA_SUCCESS) return nullptr;
+    return context;
+}
+
+// The device address of g_shift_scratch for the current device, looked up when the device has no
+// cached address or its current context is not the one the cached address belongs to.
 int scratch_address(double** out) {
     int device = 0;
     OB_CUDA(cudaGetDevice(&device));
     OB_REQUIRE(device >= 0 && device < kMaxDevices, "ob_shift_noalloc: device %d out of range",
                device);
     std::lock_guard<std::mutex> lock(g_address_mutex);
-    if (g_address[device] == nullptr) {
+    CUcontext context = current_context();
+    if (g_address[device] == nullptr || context == nullptr || context != g_context[device]) {
         void* address = nullptr;
+        // Also makes the device's primary context current when no runtime call has yet.
         cudaError_t e = cudaGetSymbolAddress(&address, g_shift_scratch);
         if (e != cudaSuccess) return cuda_status(e, "ob_shift_noalloc: cudaGetSymbolAddress");
+        context = current_context();
         g_address[device] = static_cast<double*>(address);
+        g_context[device] = context;
     }
     *out = g_address[device];
     return OB_OK;

@@ -13,6 +13,12 @@ __global__ void cast_scale_kernel(long long n, const S* __restrict__ in, T* __re
         out[i] = (T)((double)in[i] * scale);
 }
 
+__global__ void floor_kernel(long long n, float* __restrict__ values, float floor) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        values[i] = fmaxf(values[i], floor);
+}
+
 __global__ void axpby_kernel(long long n, double a, const double* __restrict__ x, double b,
                              const double* y, double* out) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -211,6 +217,16 @@ int ob_cast_scale(const void* in, int in_type, void* out, int out_type, long lon
     else
         cast_scale_kernel<<<blocks, 256, 0, stream>>>(n, (const double*)in, (double*)out, scale);
     OB_CHECK_LAUNCH("cast_scale");
+    return OB_OK;
+}
+
+int ob_floor_f32(float* values, long long n, float floor, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    if (n <= 0) return OB_OK;
+    OB_REQUIRE(values, "ob_floor_f32: null pointer");
+    const int blocks = (int)std::min((n + 255) / 256, (long long)8 * sm_count());
+    floor_kernel<<<blocks, 256, 0, stream>>>(n, values, floor);
+    OB_CHECK_LAUNCH("floor");
     return OB_OK;
 }
 

@@ -106,14 +106,18 @@ def face_terms(xyz: DeviceArray, tri: DeviceArray, n_vertices: int, n_faces: int
     return FaceTerms(cot, normals, areas, area_sums)
 
 
-def cotmatrix_entries(vertices: Any, faces: Any, dtype: Any = np.float32) -> DeviceArray:
+def cotmatrix_entries(vertices: Any, faces: Any, dtype: Any = np.float32, *,
+                      nonnegative_weights: bool = False) -> DeviceArray:
     """``(n_faces, 3)`` half-cotangent weights, column ``e`` for the edge opposite corner ``e``.
 
     Computed in float32 (the vertex precision) as ordito/laplacian.py:189 does; ``dtype`` float64
-    widens the float32 values.
+    widens the float32 values. ``nonnegative_weights`` clamps an obtuse angle's negative weight to
+    zero (kernels/laplacian.py:146-163).
     """
     xyz, tri, n_vertices, n_faces = mesh_arrays(vertices, faces)
     terms = face_terms(xyz, tri, n_vertices, n_faces)
+    if nonnegative_weights:
+        _lib.call("ob_floor_f32", terms.cot.ptr, terms.cot.size, 0.0, DEFAULT_STREAM)
     return cast(terms.cot, dtype)
 
 
@@ -179,24 +183,40 @@ def cotmatrix(
     vertices: Any,
     faces: Any,
     cot_entries: Any = None,
-    dtype: Any = np.float64,
+    dtype: Any = np.float32,
     *,
     pattern: MeshOperatorPattern | None = None,
+    nonnegative_weights: bool = False,
 ) -> CsrMatrix:
-    """The cotangent stiffness ``L`` (igl sign convention: negative diagonal), float64 values.
+    """The cotangent stiffness ``L`` (igl sign convention: negative diagonal).
 
     ordito/laplacian.py:371; off-diagonal ``L_ij`` sums the entry's half-cotangents in face order,
-    the diagonal is minus the row's off-diagonal sum.
+    the diagonal is minus the row's off-diagonal sum. The weights are the float32 half-cotangent
+    table (or ``cot_entries``); the rows are summed in float64, and ``dtype`` float32 (the
+    reference's default) rounds those float64 sums once (the reference sums in float32: the two
+    agree within float32 rounding). ``nonnegative_weights`` assembles from the weights clamped at
+    zero (only for weights computed here).
     """
-    if np.dtype(dtype) != np.float64:
-        raise ValueError("cotmatrix on the heat-geodesic path is assembled in float64")
+    dtype = np.dtype(dtype)
+    if dtype not in (np.dtype(np.float32), np.dtype(np.float64)):
+        raise ValueError(f"cotmatrix: dtype must be float32 or float64, got {dtype}")
+    if nonnegative_weights and cot_entries is not None:
+        raise ValueError(
+            "cotmatrix: nonnegative_weights clamps the weights it computes; pass cot_entries from "
+            "cotmatrix_entries(..., nonnegative_weights=True) instead"
+        )
     xyz, tri, n_vertices, n_faces = mesh_arrays(vertices, faces)
     if pattern is None:
         pattern = mesh_operator_pattern(tri, n_vertices)
     elif pattern.n_vertices != n_vertices or pattern.operator != "cotmatrix":
         raise ValueError("pattern was built for another operator or vertex count")
     terms = face_terms(xyz, tri, n_vertices, n_faces, cot_entries)
-    return assemble_rows(pattern, xyz, terms.cot, terms.area_sums, t=0.0, face_edges=False).laplacian
+    if nonnegative_weights:
+        _lib.call("ob_floor_f32", terms.cot.ptr, terms.cot.size, 0.0, DEFAULT_STREAM)
+    laplacian = assemble_rows(pattern, xyz, terms.cot, terms.area_sums, t=0.0, face_edges=False).laplacian
+    if dtype == np.float64:
+        return laplacian
+    return laplacian.with_values(cast(laplacian.values, dtype))
 
 
 def cast(array: DeviceArray, dtype: Any, scale: float = 1.0) -> DeviceArray:

@@ -24,7 +24,7 @@ def test_heat_system_factor_solves_many_columns(gpu, name: str, k: int) -> None:
     v, f = meshes.ALL[name]()
     n = v.shape[0]
     ops = gheat.heat_operators(v, f.reshape(-1), method="meshlab")
-    chol = sparse_cholesky(ops.heat_system, v, singular=False)
+    chol = sparse_cholesky(ops.heat_system, v)
     rng = np.random.default_rng(k)
     B = np.zeros((n, k))
     for c in range(k):

@@ -51,3 +51,13 @@ def test_a_call_without_a_device_returns_a_status() -> None:
     else:
         assert status == _lib.OB_ERR_CUDA
         assert _lib.lib.ob_last_error()
+
+
+@pytest.mark.parametrize("chunk", [17, 20, 12, 4100])
+def test_split_chunk_must_keep_copies_aligned(chunk: int) -> None:
+    # A split tile starts its inner range at a multiple of chunk and the tile kernels read from
+    # there in 16-byte pieces, so only multiples of 8 doubles in [16, 4096] (or 0) pass. The
+    # arguments are checked before the handle is touched, so a placeholder handle is enough.
+    status = _lib.lib.ob_chol_tile(ctypes.c_void_p(1), chunk, 2, None)
+    assert status == _lib.OB_ERR_INVALID
+    assert b"chunk" in _lib.lib.ob_last_error()

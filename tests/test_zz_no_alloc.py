@@ -50,6 +50,43 @@ def test_no_alloc_shift_matches_the_allocating_one(gpu) -> None:
         np.testing.assert_allclose(got, expected, rtol=RTOL, atol=RTOL * np.abs(expected).max())
 
 
+def test_no_alloc_shift_takes_nothing_from_the_pool(gpu) -> None:
+    # Its promise: a call allocates nothing. Read the device pool's used and reserved bytes
+    # around a run of calls made on their own (after one warm-up call), with every input made
+    # beforehand; neither may move.
+    from cuda.bindings import driver
+
+    from ordito_b200.device import synchronize
+
+    assert driver.cuInit(0)[0] == driver.CUresult.CUDA_SUCCESS
+    rng = np.random.default_rng(5)
+    n, k = 50_000, 16
+    phi = DeviceArray.from_host((rng.normal(size=(n, k)) + 2.0).reshape(-1))
+    counts = rng.integers(1, 5, size=k)
+    offsets = DeviceArray.from_host(np.concatenate(([0], np.cumsum(counts))).astype(np.int32))
+    sources = DeviceArray.from_host(rng.integers(0, n, size=int(counts.sum())).astype(np.int32))
+
+    def pool() -> tuple[int, int]:
+        synchronize()
+        err, device = driver.cuCtxGetDevice()
+        assert err == driver.CUresult.CUDA_SUCCESS
+        err, handle = driver.cuDeviceGetDefaultMemPool(device)
+        assert err == driver.CUresult.CUDA_SUCCESS
+        attr = driver.CUmemPool_attribute
+        used = int(driver.cuMemPoolGetAttribute(handle, attr.CU_MEMPOOL_ATTR_USED_MEM_CURRENT)[1])
+        reserved = int(driver.cuMemPoolGetAttribute(handle, attr.CU_MEMPOOL_ATTR_RESERVED_MEM_CURRENT)[1])
+        return used, reserved
+
+    def call() -> None:
+        _lib.call("ob_shift_noalloc", phi.ptr, n, sources.ptr, sources.size, offsets.ptr, k, 1, None)
+
+    call()
+    before = pool()
+    for _ in range(20):
+        call()
+    assert pool() == before
+
+
 def test_no_alloc_shift_rejects_too_many_columns(gpu) -> None:
     phi = DeviceArray.zeros(10 * 65, np.float64)
     src = DeviceArray.from_host(np.zeros(65, dtype=np.int32))
