@@ -370,6 +370,21 @@ int ob_grad_div_terms(const double* terms, const int32_t* faces, const int32_t* 
                       const int32_t* corner_slots, int n_vertices, int n_columns, const double* u,
                       int u_stride, const int32_t* u_iperm, double* out, int out_stride,
                       const int32_t* out_iperm, const char* out_pinned, ob_stream_t stream);
+/* ob_divergence_tiles / ob_grad_div_tiled: ob_grad_div_terms face by face over tiles of 32
+ * consecutive vertices (no reference counterpart: a layout of the same arithmetic). Set-up, once
+ * per face buffer and corner index: tile_faces[3 F] (each tile's distinct faces, stored over the
+ * start of its corner range), tile_counts[ceil(V / 32)] and corner_codes[3 F]. ob_grad_div_tiled
+ * then forms each distinct face's unit gradient once per column and tile (kernels/heat.py:626-687)
+ * and sums each vertex's corners in ascending slot order: ob_grad_div_terms' arguments and
+ * result (to rounding: the corner contributions are rounded before they are added), no atomics,
+ * the same bits on every run. */
+int ob_divergence_tiles(const int32_t* corner_offsets, const int32_t* corner_slots, int n_vertices,
+                        int32_t* tile_faces, int32_t* tile_counts, int32_t* corner_codes, ob_stream_t stream);
+int ob_grad_div_tiled(const double* terms, const int32_t* faces, const int32_t* corner_offsets,
+                      const int32_t* corner_slots, const int32_t* tile_faces, const int32_t* tile_counts,
+                      const int32_t* corner_codes, int n_vertices, int n_columns, const double* u, int u_stride,
+                      const int32_t* u_iperm, double* out, int out_stride, const int32_t* out_iperm,
+                      const char* out_pinned, ob_stream_t stream);
 int ob_seed_permuted(const int32_t* sources, const int32_t* source_offsets, int n_columns,
                      int n_vertices, const int32_t* iperm, const char* pinned, int stride,
                      double* rhs, ob_stream_t stream);

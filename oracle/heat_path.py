@@ -571,9 +571,10 @@ def solve_heat(H: sp.csr_matrix, rhs: np.ndarray) -> np.ndarray:
 
 
 class PoissonFactor:
-    """``-L`` with the lowest vertex of each connected component pinned, factored once."""
+    """``-L`` with the lowest vertex of each connected component pinned, factored once (with
+    ``vertices``, in a geometric nested-dissection ordering, as ``HeatFactor``)."""
 
-    def __init__(self, P: sp.csr_matrix) -> None:
+    def __init__(self, P: sp.csr_matrix, vertices: np.ndarray | None = None) -> None:
         active = _active_rows(P)
         n_comp, labels = csgraph.connected_components(P[active][:, active], directed=False)
         pinned = np.zeros(active.size, dtype=bool)
@@ -585,7 +586,13 @@ class PoissonFactor:
         self.n = P.shape[0]
         self.free = active[~pinned]
         sub = P[self.free][:, self.free].tocsc()
-        self.lu = spla.splu(sub, permc_spec="COLAMD") if self.free.size else None
+        if not self.free.size:
+            self.lu = None
+        elif vertices is not None:
+            order = dissection_order(np.asarray(vertices).reshape(-1, 3)[self.free], sub.tocsr())
+            self.lu = _Ordered(sub, order)
+        else:
+            self.lu = spla.splu(sub, permc_spec="COLAMD")
 
     def solve(self, rhs: np.ndarray) -> np.ndarray:
         out = np.zeros(self.n, dtype=F64)
@@ -685,14 +692,89 @@ def heat_geodesic(
     return shift_to_sources(phi, src)
 
 
-class HeatFactor:
-    """``M - t L`` factored once (empty rows excluded)."""
+def dissection_order(vertices: np.ndarray, matrix: sp.csr_matrix, leaf: int = 64) -> np.ndarray:
+    """A geometric nested-dissection ordering (new -> old) of a mesh operator's rows, for direct
+    solves of meshes too large for SuperLU's own column ordering (the fallback of the float64
+    oracle on the 2.6 M-vertex sphere).
 
-    def __init__(self, H: sp.csr_matrix) -> None:
+    Level by level every part larger than ``leaf`` is split at the median of its widest
+    coordinate; the vertices of the first half adjacent to the second form the part's separator,
+    ordered after both halves (a one-sided vertex separator, the kind the reference's ordering
+    takes, cholesky.py:2227). The ordering changes only the fill and the rounding of the exact
+    factorisation, not what it solves.
+    """
+    v = np.asarray(vertices, dtype=F64).reshape(-1, 3)
+    n = v.shape[0]
+    coo = matrix.tocoo()
+    off = coo.row != coo.col
+    ei, ej = coo.row[off].astype(np.int64), coo.col[off].astype(np.int64)
+    part = np.zeros(n, dtype=np.int64)  # the part of every still-undecided vertex
+    # Every vertex's path, one base-3 digit a level (0 / 1 the halves, 2 the separator; a
+    # decided vertex appends 0), so sorting the keys puts each subtree before its separator.
+    key = np.zeros(n, dtype=np.int64)
+    done = np.zeros(n, dtype=bool)
+    while True:
+        live = np.flatnonzero(~done)
+        if live.size:
+            labels, counts = np.unique(part[live], return_counts=True)
+            done[live[~np.isin(part[live], labels[counts > leaf])]] = True
+            live = np.flatnonzero(~done)
+        if live.size == 0:
+            break
+        live = live[np.argsort(part[live], kind="stable")]
+        p = part[live]
+        starts = np.flatnonzero(np.r_[True, p[1:] != p[:-1]])
+        sizes = np.diff(np.r_[starts, live.size])
+        lo = np.minimum.reduceat(v[live], starts, axis=0)
+        hi = np.maximum.reduceat(v[live], starts, axis=0)
+        axis = np.argmax(hi - lo, axis=1)
+        group = np.repeat(np.arange(starts.size), sizes)
+        order = np.lexsort((live, v[live, axis[group]], group))
+        live, group = live[order], group[order]
+        side = ((np.arange(live.size) - starts[group]) >= sizes[group] // 2).astype(np.int64)
+        side_of = np.full(n, -1, dtype=np.int64)
+        side_of[live] = side
+        cut = (side_of[ei] == 0) & (side_of[ej] == 1) & (part[ei] == part[ej])
+        sep = np.zeros(n, dtype=bool)
+        sep[ei[cut]] = True
+        key *= 3
+        key[live] += np.where(sep[live], 2, side)
+        done[live[sep[live]]] = True
+        part[live] = part[live] * 2 + side
+    return np.lexsort((np.arange(n), key))
+
+
+class _Ordered:
+    """SuperLU over rows renumbered by ``order`` (new -> old) with no column reordering of its own
+    and no pivoting (the operators are symmetric positive definite on the rows factored)."""
+
+    def __init__(self, sub: sp.csc_matrix, order: np.ndarray) -> None:
+        self.order = order
+        permuted = sub[order][:, order].tocsc()
+        self.lu = spla.splu(permuted, permc_spec="NATURAL", diag_pivot_thresh=0.0,
+                            options={"SymmetricMode": True})
+
+    def solve(self, rhs: np.ndarray) -> np.ndarray:
+        out = np.empty_like(rhs)
+        out[self.order] = self.lu.solve(rhs[self.order])
+        return out
+
+
+class HeatFactor:
+    """``M - t L`` factored once (empty rows excluded); ``vertices`` given, in a geometric
+    nested-dissection ordering (``dissection_order``), else in SuperLU's COLAMD ordering."""
+
+    def __init__(self, H: sp.csr_matrix, vertices: np.ndarray | None = None) -> None:
         self.n = H.shape[0]
         self.active = _active_rows(H)
         sub = H[self.active][:, self.active].tocsc()
-        self.lu = spla.splu(sub, permc_spec="COLAMD") if self.active.size else None
+        if not self.active.size:
+            self.lu = None
+        elif vertices is not None:
+            order = dissection_order(np.asarray(vertices).reshape(-1, 3)[self.active], sub.tocsr())
+            self.lu = _Ordered(sub, order)
+        else:
+            self.lu = spla.splu(sub, permc_spec="COLAMD")
 
     def solve(self, rhs: np.ndarray) -> np.ndarray:
         out = np.zeros(self.n, dtype=F64)

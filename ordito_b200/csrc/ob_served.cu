@@ -264,6 +264,159 @@ __global__ void __launch_bounds__(256, CP == 4 ? 4 : 1) grad_div_terms_kernel(co
     }
 }
 
+// ---- The divergence face by face over tiles of vertices ------------------------------------
+// The per-corner form above recomputes a face's unit gradient at each of its three corners. Here
+// a CTA takes kTileVertices consecutive vertices, forms the unit gradient of each distinct face
+// they touch once per column (into shared memory, as its three corner contributions d_e), then
+// sums each vertex's corners from there in ascending slot order: the same terms in the same
+// order, a third of the gradients, normalisations and reciprocal square roots.
+constexpr int kTileVertices = 32;   // vertices a tile
+constexpr int kTileColumns = 16;    // columns a pass over a tile's faces takes
+constexpr int kTileFaces = 192;     // distinct faces a tile holds in shared memory
+constexpr int kTileCorners = 1024;  // corners the set-up deduplicates in shared memory
+constexpr int kTileSmem = kTileFaces * 3 * kTileColumns * (int)sizeof(double);
+
+// Set-up, once per face buffer and corner index: tile t's distinct faces in first-corner order,
+// stored over the start of the tile's own corner range of tile_faces (a tile has no more distinct
+// faces than corners), their count (-1 past kTileCorners corners or kTileFaces faces: the
+// divergence takes the per-corner form on such a tile), and each corner's code, its face's place
+// in the list times 3 plus its corner.
+__global__ void __launch_bounds__(256) divergence_tiles_kernel(const int* __restrict__ corner_offsets,
+                                                               const int* __restrict__ corner_slots, int n,
+                                                               int* __restrict__ tile_faces,
+                                                               int* __restrict__ tile_counts,
+                                                               int* __restrict__ corner_codes) {
+    __shared__ int face[kTileCorners];
+    __shared__ int first[kTileCorners];
+    const int t = blockIdx.x;
+    const int v0 = t * kTileVertices, v1 = min(n, v0 + kTileVertices);
+    const int p0 = corner_offsets[v0], m = corner_offsets[v1] - p0;
+    if (m > kTileCorners) {
+        if (threadIdx.x == 0) tile_counts[t] = -1;
+        return;
+    }
+    for (int i = threadIdx.x; i < m; i += blockDim.x) face[i] = corner_slots[p0 + i] / 3;
+    __syncthreads();
+    // Each corner's first corner of the same face in the tile.
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const int f = face[i];
+        int j = 0;
+        while (face[j] != f) ++j;
+        first[i] = j;
+    }
+    __syncthreads();
+    // Places in first-corner order (one thread: a few hundred corners, once per mesh); a first
+    // corner's entry becomes -(place + 1).
+    if (threadIdx.x == 0) {
+        int count = 0;
+        for (int i = 0; i < m; ++i)
+            if (first[i] == i) {
+                tile_faces[p0 + count] = face[i];
+                first[i] = -(count + 1);
+                ++count;
+            }
+        tile_counts[t] = count > kTileFaces ? -1 : count;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const int j = first[i];
+        const int place = j < 0 ? -j - 1 : -first[j] - 1;
+        corner_codes[p0 + i] = 3 * place + corner_slots[p0 + i] % 3;
+    }
+}
+
+// The unit gradient of face f at column c, as its three corner contributions d_e = (W_e . s) / |s|
+// (zero where the gradient is zero): the arithmetic of grad_div_terms_kernel.
+__device__ __forceinline__ void face_contributions(const double* __restrict__ T, double u0, double u1, double u2,
+                                                   double* d) {
+    const double gx = fma(u0, T[0], fma(u1, T[3], u2 * T[6]));
+    const double gy = fma(u0, T[1], fma(u1, T[4], u2 * T[7]));
+    const double gz = fma(u0, T[2], fma(u1, T[5], u2 * T[8]));
+    const double largest = fmax(fabs(gx), fmax(fabs(gy), fabs(gz)));
+    if (largest == 0.0) {
+        d[0] = d[1] = d[2] = 0.0;
+        return;
+    }
+    const double scale = inverse_power_of_two(largest);
+    const double sx = gx * scale, sy = gy * scale, sz = gz * scale;
+    const double r = rsqrt(fma(sx, sx, fma(sy, sy, sz * sz)));
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        const double* W = T + 9 + 3 * e;
+        d[e] = fma(sx, W[0], fma(sy, W[1], sz * W[2])) * r;
+    }
+}
+
+__global__ void __launch_bounds__(256) grad_div_tiled_kernel(
+    const double* __restrict__ terms, const int* __restrict__ faces, const int* __restrict__ corner_offsets,
+    const int* __restrict__ corner_slots, const int* __restrict__ tile_faces, const int* __restrict__ tile_counts,
+    const int* __restrict__ corner_codes, int n, int k, const double* __restrict__ u, int u_stride,
+    const int* __restrict__ u_iperm, double* __restrict__ out, int out_stride, const int* __restrict__ out_iperm,
+    const char* __restrict__ out_pinned) {
+    extern __shared__ double contributions[];  // [place * 3 + corner][column of the pass]
+    const int t = blockIdx.x;
+    const int v0 = t * kTileVertices, v1 = min(n, v0 + kTileVertices);
+    const int count = tile_counts[t];
+    if (count < 0) {
+        // A crowded tile: each (vertex, column) sums its corners' own gradients.
+        for (int item = threadIdx.x; item < (v1 - v0) * out_stride; item += blockDim.x) {
+            const int v = v0 + item / out_stride, c = item % out_stride;
+            double acc = 0.0;
+            if (c < k)
+                for (int p = corner_offsets[v]; p < corner_offsets[v + 1]; ++p) {
+                    const int q = corner_slots[p], f = q / 3, e = q - 3 * f;
+                    double d[3];
+                    face_contributions(terms + (size_t)kFaceTerms * f,
+                                       u[(size_t)row_of(u_iperm, faces[3 * f]) * u_stride + c],
+                                       u[(size_t)row_of(u_iperm, faces[3 * f + 1]) * u_stride + c],
+                                       u[(size_t)row_of(u_iperm, faces[3 * f + 2]) * u_stride + c], d);
+                    acc += d[e];
+                }
+            const int row = row_of(out_iperm, v);
+            out[(size_t)row * out_stride + c] = ((out_pinned && out_pinned[row]) || c >= k) ? 0.0 : acc;
+        }
+        return;
+    }
+    const int p0 = corner_offsets[v0];
+    for (int c0 = 0; c0 < out_stride; c0 += kTileColumns) {
+        for (int item = threadIdx.x; item < count * kTileColumns; item += blockDim.x) {
+            const int place = item / kTileColumns, j = item % kTileColumns, c = c0 + j;
+            double d[3] = {0.0, 0.0, 0.0};
+            if (c < k) {
+                const int f = tile_faces[p0 + place];
+                face_contributions(terms + (size_t)kFaceTerms * f,
+                                   u[(size_t)row_of(u_iperm, faces[3 * f]) * u_stride + c],
+                                   u[(size_t)row_of(u_iperm, faces[3 * f + 1]) * u_stride + c],
+                                   u[(size_t)row_of(u_iperm, faces[3 * f + 2]) * u_stride + c], d);
+            }
+#pragma unroll
+            for (int e = 0; e < 3; ++e) contributions[(3 * place + e) * kTileColumns + j] = d[e];
+        }
+        __syncthreads();
+        const int width = min(kTileColumns, out_stride - c0);
+        for (int item = threadIdx.x; item < (v1 - v0) * kTileColumns; item += blockDim.x) {
+            const int v = v0 + item / kTileColumns, j = item % kTileColumns, c = c0 + j;
+            if (j >= width) continue;
+            double acc = 0.0;
+            const int end = corner_offsets[v + 1];
+            for (int p = corner_offsets[v]; p < end; ++p) acc += contributions[corner_codes[p] * kTileColumns + j];
+            const int row = row_of(out_iperm, v);
+            out[(size_t)row * out_stride + c] = ((out_pinned && out_pinned[row]) || c >= k) ? 0.0 : acc;
+        }
+        __syncthreads();
+    }
+}
+
+int allow_tile_memory() {
+    static int allowed[64] = {};
+    int device = 0;
+    OB_CUDA(cudaGetDevice(&device));
+    if (device >= 0 && device < 64 && allowed[device]) return OB_OK;
+    OB_CUDA(cudaFuncSetAttribute(grad_div_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
+    if (device >= 0 && device < 64) allowed[device] = 1;
+    return OB_OK;
+}
+
 // Seeds of k source sets in a factor's numbering: rhs (stride `stride`, zeroed first) gets 1 at
 // each source's row, 0 at pinned rows.
 __global__ void seed_permuted_kernel(const int* __restrict__ sources,
@@ -541,6 +694,39 @@ int ob_grad_div_terms(const double* terms, const int32_t* faces, const int32_t* 
                                                                   n_vertices, n_columns, u, u_stride, u_iperm,
                                                                   out, out_stride, out_iperm, out_pinned);
     OB_CHECK_LAUNCH("grad_div_terms");
+    return OB_OK;
+}
+
+int ob_divergence_tiles(const int32_t* corner_offsets, const int32_t* corner_slots, int n_vertices,
+                        int32_t* tile_faces, int32_t* tile_counts, int32_t* corner_codes, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_vertices >= 0, "ob_divergence_tiles: bad size");
+    if (n_vertices == 0) return OB_OK;
+    OB_REQUIRE(corner_offsets && corner_slots && tile_faces && tile_counts && corner_codes,
+               "ob_divergence_tiles: null pointer");
+    divergence_tiles_kernel<<<ceil_div(n_vertices, kTileVertices), 256, 0, stream>>>(
+        corner_offsets, corner_slots, n_vertices, tile_faces, tile_counts, corner_codes);
+    OB_CHECK_LAUNCH("divergence tiles");
+    return OB_OK;
+}
+
+int ob_grad_div_tiled(const double* terms, const int32_t* faces, const int32_t* corner_offsets,
+                      const int32_t* corner_slots, const int32_t* tile_faces, const int32_t* tile_counts,
+                      const int32_t* corner_codes, int n_vertices, int n_columns, const double* u, int u_stride,
+                      const int32_t* u_iperm, double* out, int out_stride, const int32_t* out_iperm,
+                      const char* out_pinned, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_vertices >= 0 && n_columns >= 1 && u_stride >= n_columns && out_stride >= n_columns,
+               "ob_grad_div_tiled: bad size");
+    if (n_vertices == 0) return OB_OK;
+    OB_REQUIRE(terms && faces && corner_offsets && corner_slots && tile_faces && tile_counts && corner_codes && u &&
+                   out,
+               "ob_grad_div_tiled: null pointer");
+    if (int st = allow_tile_memory()) return st;
+    grad_div_tiled_kernel<<<ceil_div(n_vertices, kTileVertices), 256, kTileSmem, stream>>>(
+        terms, faces, corner_offsets, corner_slots, tile_faces, tile_counts, corner_codes, n_vertices, n_columns, u,
+        u_stride, u_iperm, out, out_stride, out_iperm, out_pinned);
+    OB_CHECK_LAUNCH("grad_div_tiled");
     return OB_OK;
 }
 

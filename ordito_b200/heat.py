@@ -502,18 +502,61 @@ def _require_sources(sources: Any, n_vertices: int) -> DeviceArray:
     return src.reshape(src.size)
 
 
+# The divergence's form: per corner (ob_grad_div_terms, the default: measured faster -- 3.7 against
+# 10.4 ms on icosphere(9) at 64 columns -- since a tile of 32 vertices still forms 1.7-2 times as
+# many face gradients as there are faces and its shared-memory passes hold fewer warps) or face by
+# face over vertex tiles (ob_grad_div_tiled).
+_TILED_DIVERGENCE = False
+
+
+def divergence_tiles(corner_offsets: DeviceArray, corner_slots: DeviceArray, n: int,
+                     n_faces: int) -> tuple[DeviceArray, DeviceArray, DeviceArray]:
+    """``(tile_faces, tile_counts, corner_codes)`` of a corner index (``ob_divergence_tiles``):
+    the distinct faces of every tile of 32 consecutive vertices, for ``ob_grad_div_tiled``."""
+    corners = max(3 * n_faces, 1)
+    tile_faces = DeviceArray.empty(corners, np.int32)
+    tile_counts = DeviceArray.empty(max((n + 31) // 32, 1), np.int32)
+    corner_codes = DeviceArray.empty(corners, np.int32)
+    _lib.call("ob_divergence_tiles", corner_offsets.ptr, corner_slots.ptr, n, tile_faces.ptr,
+              tile_counts.ptr, corner_codes.ptr, DEFAULT_STREAM)
+    return tile_faces, tile_counts, corner_codes
+
+
+def _grad_div(solver: "HeatSolver", faces: DeviceArray, index: tuple, n: int, k: int, u: int,
+              u_stride: int, u_iperm: Any, out: int, out_stride: int, out_iperm: Any, out_pinned: Any,
+              stream: Any) -> None:
+    _grad_div_index(solver.gradient_terms, faces, index, n, k, u, u_stride, u_iperm, out,
+                    out_stride, out_iperm, out_pinned, stream)
+
+
+def _grad_div_index(terms: DeviceArray, faces: DeviceArray, index: tuple, n: int, k: int, u: int,
+                    u_stride: int, u_iperm: Any, out: int, out_stride: int, out_iperm: Any,
+                    out_pinned: Any, stream: Any) -> None:
+    """``-div`` of the per-face unit gradients of ``k`` heat columns over a corner index and its
+    tiles ``(offsets, slots, tile_faces, tile_counts, codes)``, from per-face terms: each vertex's
+    corners summed in ascending slot order (no atomics: the same bits on every run, the reference's
+    deterministic mode, ordito/heat.py:3170-3232, as the only mode), per corner
+    (``ob_grad_div_terms``) or face by face over the tiles (``ob_grad_div_tiled``)."""
+    corner_offsets, corner_slots, tile_faces, tile_counts, codes = index
+    if _TILED_DIVERGENCE:
+        _lib.call(
+            "ob_grad_div_tiled", terms.ptr, faces.ptr, corner_offsets.ptr,
+            corner_slots.ptr, tile_faces.ptr, tile_counts.ptr, codes.ptr, n, k, u, u_stride, u_iperm,
+            out, out_stride, out_iperm, out_pinned, stream,
+        )  # fmt: skip
+        return
+    _lib.call(
+        "ob_grad_div_terms", terms.ptr, faces.ptr, corner_offsets.ptr,
+        corner_slots.ptr, n, k, u, u_stride, u_iperm, out, out_stride, out_iperm, out_pinned,
+        stream,
+    )  # fmt: skip
+
+
 def _divergence(mesh: Trimesh, solver: "HeatSolver", k: int, u: int, u_stride: int, u_iperm: Any,
                 out: int, out_stride: int, out_iperm: Any, out_pinned: Any, stream: Any) -> None:
-    """``-div`` of the per-face unit gradients of ``k`` heat columns, gathered per vertex over its
-    corners in ascending slot order (no atomics: the same bits on every run, the reference's
-    deterministic mode, ordito/heat.py:3170-3232, as the only mode), from the solver's per-face
-    terms (``ob_grad_div_terms``)."""
-    corner_offsets, corner_slots = mesh.corner_index
-    _lib.call(
-        "ob_grad_div_terms", solver.gradient_terms.ptr, mesh.faces.ptr, corner_offsets.ptr,
-        corner_slots.ptr, mesh.n_vertices, k, u, u_stride, u_iperm, out, out_stride, out_iperm,
-        out_pinned, stream,
-    )  # fmt: skip
+    """``_grad_div`` over the mesh's own numbering (its corner index and tiles, made once)."""
+    _grad_div(solver, mesh.faces, mesh.corner_tiles, mesh.n_vertices, k, u, u_stride, u_iperm, out,
+              out_stride, out_iperm, out_pinned, stream)
 
 
 def _corners_in_factor_rows(mesh: Trimesh, solver: "HeatSolver", h_iperm: int,
@@ -545,8 +588,9 @@ def _corners_in_factor_rows(mesh: Trimesh, solver: "HeatSolver", h_iperm: int,
         workspace = DeviceArray.empty(int(size.value), np.uint8)
         _lib.call("ob_corner_index", faces.ptr, mesh.n_faces, n, offsets.ptr, slots.ptr,
                   workspace.ptr, int(size.value), DEFAULT_STREAM)
+        tiles = divergence_tiles(offsets, slots, n, mesh.n_faces)
         _lib.call("ob_stream_synchronize", DEFAULT_STREAM)  # the arrays serve other streams
-        result = (faces, offsets, slots)
+        result = (faces, (offsets, slots) + tiles)
     holder._factor_row_corners = (key, result)
     return result
 
@@ -703,11 +747,9 @@ def _batch_columns(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offset
             _divergence(mesh, solver, k, h_sol, h_stride, h_iperm, p_rhs, p_stride, p_iperm,
                         p_pinned, st)
         else:
-            faces_rows, corner_offsets, corner_slots = rows
-            _lib.call(
-                "ob_grad_div_terms", solver.gradient_terms.ptr, faces_rows.ptr, corner_offsets.ptr,
-                corner_slots.ptr, n, k, h_sol, h_stride, None, p_rhs, p_stride, None, p_pinned, st,
-            )  # fmt: skip
+            faces_rows, index = rows
+            _grad_div(solver, faces_rows, index, n, k, h_sol, h_stride, None, p_rhs, p_stride, None,
+                      p_pinned, st)
         poisson_factor.solve_in_place(k, st, work_set)
         if out is None:
             out = DeviceArray.empty((k, n), np.float64)

@@ -66,6 +66,18 @@ class Trimesh:
         return self._corner_index
 
     @property
+    def corner_tiles(self) -> tuple[DeviceArray, ...]:
+        """The corner index and its divergence tiles, ``(corner_offsets, corner_slots, tile_faces,
+        tile_counts, corner_codes)`` (``ob_divergence_tiles``), made once."""
+        if getattr(self, "_corner_tiles", None) is None:
+            from ordito_b200.heat import divergence_tiles  # noqa: PLC0415
+
+            offsets, slots = self.corner_index
+            self._corner_tiles = (offsets, slots) + divergence_tiles(offsets, slots, self.n_vertices,
+                                                                     self.n_faces)
+        return self._corner_tiles
+
+    @property
     def mean_edge_length(self) -> float:
         """Mean over all ``3 n_faces`` per-face edges (ordito/mesh.py:1179), read back once."""
         if self._mean_edge_length is None:

@@ -110,6 +110,10 @@ class PackedMeshes:
         workspace = DeviceArray.empty(int(size.value), np.uint8)
         _lib.call("ob_corner_index", self.faces.ptr, self.n_faces, n, self.corner_offsets.ptr,
                   self.corner_slots.ptr, workspace.ptr, int(size.value), DEFAULT_STREAM)
+        from ordito_b200.heat import divergence_tiles  # noqa: PLC0415
+
+        self.tile_faces, self.tile_counts, self.corner_codes = divergence_tiles(
+            self.corner_offsets, self.corner_slots, n, self.n_faces)
         self.gradient_terms = DeviceArray.empty((max(self.n_faces, 1), 18), np.float64)
         _lib.call("ob_face_gradient_terms", self.xyz.ptr, self.faces.ptr, self.n_faces,
                   terms.normals.ptr, terms.areas.ptr, terms.cot.ptr, self.gradient_terms.ptr,
@@ -166,11 +170,12 @@ class PackedMeshes:
         _lib.call("ob_seed_permuted", self.d_sources.ptr, self.d_offsets.ptr, k, n, h_iperm, h_pinned,
                   h_stride, h_rhs, stream)
         hf.solve_in_place_sources(k, self.d_sources, self.d_offsets, stream)
-        _lib.call(
-            "ob_grad_div_terms", self.gradient_terms.ptr, self.faces.ptr, self.corner_offsets.ptr,
-            self.corner_slots.ptr, n, k, h_sol, h_stride, h_iperm, p_rhs, p_stride, p_iperm, p_pinned,
-            stream,
-        )  # fmt: skip
+        from ordito_b200.heat import _grad_div_index  # noqa: PLC0415
+
+        _grad_div_index(self.gradient_terms, self.faces,
+                        (self.corner_offsets, self.corner_slots, self.tile_faces, self.tile_counts,
+                         self.corner_codes), n, k, h_sol, h_stride, h_iperm, p_rhs, p_stride, p_iperm,
+                        p_pinned, stream)
         pf.solve_in_place(k, stream)
         _lib.call("ob_shift_packed", p_sol, n, p_stride, p_iperm, self.d_vertex_offsets.ptr,
                   self.n_meshes, self.d_shift.ptr, k, self.d_sums.ptr, self.out.ptr, stream)

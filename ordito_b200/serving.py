@@ -550,7 +550,7 @@ class GeodesicServer:
                     self._ready.put((request.key, unfactored, None))
                     continue
                 n = mesh.n_vertices
-                mesh.corner_index  # built now, not on the first batch
+                mesh.corner_tiles  # built now, not on the first batch
                 cap_sources = self.max_columns * 2 * self.max_sources
                 # The widest first: the factors' work buffers are then allocated once.
                 solver.heat_factor.work(self.max_columns)

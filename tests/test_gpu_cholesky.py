@@ -162,6 +162,45 @@ def test_divergence_from_face_terms(gpu, k: int) -> None:
     assert np.array_equal(outs[0], outs[1])
     assert np.array_equal(outs[0], outs[2])
     assert np.allclose(outs[0], reference, rtol=1e-12, atol=1e-12 * np.abs(reference).max())
+    # Face by face over tiles: the same sums to rounding, the same bits on every run.
+    tiles = mesh.corner_tiles
+    tiled = []
+    for field in (u, u, tiny):
+        out = DeviceArray.empty(n * k, np.float64)
+        _lib.call("ob_grad_div_tiled", table.ptr, mesh.faces.ptr, *(a.ptr for a in tiles), n, k,
+                  field.ptr, k, None, out.ptr, k, None, None, None)
+        tiled.append(out.numpy())
+    assert np.array_equal(tiled[0], tiled[1])
+    assert np.array_equal(tiled[0], tiled[2])
+    assert np.allclose(tiled[0], outs[0], rtol=1e-13, atol=1e-13 * np.abs(outs[0]).max())
+
+
+def test_tiled_divergence_on_a_crowded_fan(gpu) -> None:
+    # A vertex on 1 500 faces: its tile has too many corners for shared memory and takes the
+    # per-corner form; every other tile the face-major one. Both against the per-corner kernel.
+    from ordito_b200 import _lib
+
+    ring = 1500
+    angle = 2.0 * np.pi * np.arange(ring) / ring
+    rim = np.column_stack((np.cos(angle), np.sin(angle), 0.1 * np.sin(7 * angle)))
+    v = np.vstack(([[0.0, 0.0, 0.3]], rim)).astype(np.float32)
+    f = np.array([[0, 1 + i, 1 + (i + 1) % ring] for i in range(ring)], dtype=np.int32)
+    n, k = v.shape[0], 6
+    mesh = Trimesh(v, f.reshape(-1))
+    terms = mesh.face_terms
+    table = DeviceArray.empty((mesh.n_faces, 18), np.float64)
+    _lib.call("ob_face_gradient_terms", mesh.vertices.ptr, mesh.faces.ptr, mesh.n_faces,
+              terms.normals.ptr, terms.areas.ptr, terms.cot.ptr, table.ptr, None)
+    u = DeviceArray.from_host(np.random.default_rng(3).random(n * k))
+    offsets, slots, tile_faces, tile_counts, codes = mesh.corner_tiles
+    assert tile_counts.numpy()[0] == -1 and (tile_counts.numpy()[1:] > 0).all()
+    expected, got = DeviceArray.empty(n * k, np.float64), DeviceArray.empty(n * k, np.float64)
+    _lib.call("ob_grad_div_terms", table.ptr, mesh.faces.ptr, offsets.ptr, slots.ptr, n, k, u.ptr, k,
+              None, expected.ptr, k, None, None, None)
+    _lib.call("ob_grad_div_tiled", table.ptr, mesh.faces.ptr, offsets.ptr, slots.ptr, tile_faces.ptr,
+              tile_counts.ptr, codes.ptr, n, k, u.ptr, k, None, got.ptr, k, None, None, None)
+    e = expected.numpy()
+    assert np.allclose(got.numpy(), e, rtol=1e-13, atol=1e-13 * np.abs(e).max())
 
 
 def test_recorded_batch_step_matches_the_eager_pass(gpu) -> None:

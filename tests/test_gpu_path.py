@@ -66,7 +66,10 @@ def test_face_terms_and_operators(gpu, name: str) -> None:
     for key, matrix in (("L", built.laplacian), ("H", built.heat), ("P", built.poisson)):
         got = matrix.values.numpy()[:nnz]
         assert np.allclose(got, ref[key], rtol=VALUE_RTOL, atol=VALUE_RTOL * scale), key
-    assert np.allclose(built.mass.numpy(), ref["mass"], rtol=1e-12)
+    # The mass is a third of those exact sums; against the oracle it carries the areas' rounding
+    # (a needle's float32 area can differ by an ulp from the oracle's).
+    assert np.allclose(built.mass.numpy(), own / 3.0, rtol=1e-15, atol=0.0)
+    assert np.allclose(built.mass.numpy(), ref["mass"], rtol=VALUE_RTOL)
     total, count = built.edge_sums.numpy()
     # Each length is a float32 sqrt of a float32 dot (fused on the device): h agrees to a few
     # float32 ulps averaged over the edges.
@@ -82,7 +85,7 @@ def test_golden_ico3_fixture(gpu) -> None:
 @pytest.mark.parametrize(
     ("name", "sources"),
     [("ico3", [0]), ("saddle_graded", [17]), ("bumpy_sphere", [5]), ("small_torus", [0, 400, 900]),
-     ("grid", [3]), ("unreferenced", [1])],
+     ("grid", [3]), ("unreferenced", [1]), ("sphere_irregular", [0, 250]), ("torus_irregular", [7])],
 )
 def test_heat_geodesic_matches_the_oracle(gpu, name: str, sources: list[int]) -> None:
     v, f = meshes.ALL[name]()
@@ -242,3 +245,80 @@ def test_single_query_with_held_factors(gpu) -> None:
     assert rel_err(got, hp.heat_geodesic(v, f, np.array([5, 9]))) <= DISTANCE_TOL
     with pytest.raises(ValueError):
         gheat.heat_geodesic(mesh, np.array([n], dtype=np.int32), method="meshlab")
+
+
+@pytest.mark.parametrize(("name", "t"), [("sphere_irregular", None), ("saddle_graded", None),
+                                         ("sphere_irregular", 0.05), ("torus_irregular", None)])
+def test_device_heat_operators_are_the_matrices_they_name(gpu, name: str, t) -> None:
+    """ordito tests/test_heat.py:126-188 on the device's operators (the reference's default
+    method, potpourri3d): P is -L bit for bit, L is the float64 cotmatrix bit for bit, H is M - t L
+    for one t (read off an off-diagonal entry) to 1e-12, that t is the squared mean unique edge
+    length to 1e-6 (or the explicit t as given), normals and areas match a float64 computation
+    from the same float32 positions to 1e-5."""
+    from ordito_b200 import laplacian as glap
+
+    v, f = meshes.ALL[name]()
+    ops = gheat.heat_operators(v, f.reshape(-1), t)
+    L = ops.laplacian.to_scipy().toarray()
+    H = ops.heat_system.to_scipy().toarray()
+    P = ops.poisson_system.to_scipy().toarray()
+    assert np.array_equal(L, glap.cotmatrix(v, f.reshape(-1), dtype=np.float64).to_scipy().toarray())
+    assert np.array_equal(P, -L)
+    row, col = np.argwhere(np.triu(L, k=1) != 0.0)[0]
+    diffusion_time = float(-H[row, col] / L[row, col])
+    v64, f64 = v.astype(np.float64), f.astype(np.int64)
+    edges = np.unique(np.sort(np.concatenate([f64[:, [0, 1]], f64[:, [1, 2]], f64[:, [2, 0]]]), axis=1), axis=0)
+    unique_mean = float(np.linalg.norm(v64[edges[:, 0]] - v64[edges[:, 1]], axis=1).mean())
+    assert np.isclose(diffusion_time, unique_mean**2 if t is None else t, rtol=1e-6, atol=0.0)
+    if t is not None:
+        diffusion_time = t
+    mass = glap.mass_matrix_entries(v, f.reshape(-1), dtype=np.float64).numpy()
+    assert np.allclose(H, np.diag(mass) - diffusion_time * L, rtol=1e-12, atol=1e-15)
+    corners = v64[f64]
+    cross = np.cross(corners[:, 1] - corners[:, 0], corners[:, 2] - corners[:, 0])
+    norm = np.linalg.norm(cross, axis=1)
+    assert ops.cot_entries.shape == (f.shape[0], 3)
+    assert np.allclose(ops.face_normals.numpy().reshape(-1, 3), cross / norm[:, None], rtol=1e-5, atol=1e-5)
+    assert np.allclose(ops.face_areas.numpy(), 0.5 * norm, rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.parametrize("name", ["saddle_graded", "sphere_irregular", "torus_irregular"])
+def test_device_distance_is_zero_at_the_source_and_nonnegative(gpu, name: str) -> None:
+    """ordito tests/test_heat.py:653-663, and against the oracle, on the reference's fixtures."""
+    v, f = meshes.ALL[name]()
+    d = gheat.heat_geodesic(v, f.reshape(-1), np.array([0], dtype=np.int32)).numpy()
+    assert np.all(d >= -1e-6)
+    assert abs(d[0]) <= 1e-4
+    assert hp.relative_linf(d, hp.heat_geodesic(v, f, np.array([0]))) <= 1e-5
+
+
+def test_torch_cuda_tensors_cross_zero_copy(gpu) -> None:
+    """Arrays from another framework (PyTorch CUDA tensors, through __cuda_array_interface__) are
+    read in place, and ``solution`` is written in place: its pointer is the tensor's own."""
+    import torch
+
+    from ordito_b200.device import device_pointer
+
+    v, f = creation.icosphere(3)
+    n = v.shape[0]
+    tv = torch.from_numpy(v).cuda()
+    tf = torch.from_numpy(f.reshape(-1).copy()).cuda()
+    ts = torch.tensor([0], dtype=torch.int32, device="cuda")
+    for tensor, dtype in ((tv, np.float32), (tf, np.int32), (ts, np.int32)):
+        pointer, keep = device_pointer(tensor, dtype)
+        assert pointer == tensor.data_ptr() and keep is tensor
+    distance = gheat.heat_geodesic(tv, tf, ts).numpy()
+    assert hp.relative_linf(distance, gheat.heat_geodesic(v, f.reshape(-1), np.array([0], dtype=np.int32)).numpy()) == 0.0
+    assert hp.relative_linf(distance, hp.heat_geodesic(v, f, np.array([0]))) <= 1e-5
+    # solve_spd warm-starts from `solution` and writes it in place.
+    ops = gheat.heat_operators(tv, tf)
+    mass = torch.from_numpy(glap.mass_matrix_entries(v, f.reshape(-1), dtype=np.float64).numpy()).cuda()
+    solution = torch.zeros(n, dtype=torch.float64, device="cuda")
+    before = solution.data_ptr()
+    glinalg.solve_spd(ops.heat_system, mass, solution, tol=1e-12, preconditioner=ops.heat_preconditioner)
+    torch.cuda.synchronize()
+    assert solution.data_ptr() == before
+    assert torch.max(torch.abs(solution - 1.0)).item() <= 1e-9
+    # A tensor of the wrong dtype is refused, not converted behind the caller's back.
+    with pytest.raises(ValueError):
+        gheat.heat_geodesic(tv.double(), tf, ts)
