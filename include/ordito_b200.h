@@ -400,6 +400,14 @@ int ob_chol_time_solve(void* factor, int n_columns, int reps, float* ms, ob_stre
  * ob_chol_factor are chunk 64, waves 2. */
 int ob_chol_tile(void* factor, int chunk, int waves, ob_stream_t stream);
 int ob_chol_info(void* factor, long long* info);
+/* Deterministic passes (ordito.config.set_deterministic, ordito/config.py:125, for the factored
+ * solves): on != 0 rebuilds the passes with no split tiles and with each supernode's forward
+ * update written to its own rows, then added into its target rows by one gather launch a tree
+ * level in supernode order -- no atomics in a pass, so every solve repeats bit for bit (slower:
+ * the long inner dimensions of the upper levels are no longer split). Waits for the device, drops
+ * the recorded solves, moves every work set's generation and reallocates the work buffers made
+ * so far (deterministic ones hold the update rows too). */
+int ob_chol_set_deterministic(void* factor, int on, ob_stream_t stream);
 /* The work buffers' generation: it changes whenever ob_chol_work's pointers do (a wider k than
  * any before reallocates them), so a graph recorded over them must be recorded again. */
 int ob_chol_work_generation(void* factor, long long* generation);
@@ -491,6 +499,18 @@ int ob_heat_rows_packed(const int32_t* offsets, const int32_t* columns, const in
 int ob_shift_packed(const double* phi, int n_vertices, int stride, const int32_t* iperm,
                     const int32_t* vertex_offsets, int n_meshes, const int32_t* sources,
                     int n_columns, double* sums, double* out, ob_stream_t stream);
+
+/* ---- f3: scalar extension -------------------------------------------------------------------
+ * ob_extend_seed replaces kernels/heat.py:3858 seed_source_scalars (ordito/heat.py:2426
+ * _extend_scalar): rhs[V][2] (zeroed here) gets column 0 = the indicator of the sources, column 1
+ * = the values they carry (a repeated source adds up), range[0..1] = the values' min and max and
+ * range[2] = 0; an index outside [0, V) sets invalid[0] (zeroed here).
+ * ob_extend_ratio replaces kernels/heat.py:3933 extend_from_ratio: extended[i] = diffused[i][1] /
+ * diffused[i][0] (0 where the diffused indicator is exactly 0), and range[2] = the largest excess
+ * of the extension over [range[0], range[1]] at vertices the indicator reaches. */
+int ob_extend_seed(const int32_t* sources, const double* values, int n_sources, int n_vertices, double* rhs,
+                   double* range, int32_t* invalid, ob_stream_t stream);
+int ob_extend_ratio(const double* diffused, int n_vertices, double* range, double* extended, ob_stream_t stream);
 
 /* ---- a12: the marched settled solve --------------------------------------------------------
  * Replaces ordito/linalg.py:2765 _march_settled (kernels/linalg.py:1229-1545): x = A^-1 rhs for

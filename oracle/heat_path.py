@@ -789,3 +789,30 @@ def relative_linf(value: np.ndarray, reference: np.ndarray) -> float:
     if scale == 0.0:
         return float(np.max(np.abs(value))) if value.size else 0.0
     return float(np.max(np.abs(np.asarray(value, dtype=F64) - reference)) / scale)
+
+
+def extend_scalar(vertices: np.ndarray, faces: np.ndarray, sources: np.ndarray, values: np.ndarray,
+                  t: float | None = None) -> tuple[np.ndarray, float]:
+    """``extend_scalar`` (heat.py:2321-2500, kernels/heat.py:3858 and :3933): the indicator of the
+    sources and the values they carry diffused through ``M - t L`` (the solver's default
+    discretization, potpourri3d's unique-edge time step) in one exact solve, the extension their
+    quotient (0 where the indicator is exactly 0). Returns the field and its largest excess over
+    the source values' range at vertices the indicator reaches."""
+    v = np.asarray(vertices, dtype=F32).reshape(-1, 3)
+    f = np.asarray(faces, dtype=np.int64).reshape(-1, 3)
+    n = v.shape[0]
+    src = np.asarray(sources, dtype=np.int64)
+    vals = np.asarray(values, dtype=F64)
+    t_eff, _ = vertex_time(v, f, t, "potpourri3d")
+    ops = heat_operators(v, f, t_eff, method="potpourri3d")
+    rhs = np.zeros((n, 2), dtype=F64)
+    np.add.at(rhs[:, 0], src, 1.0)
+    np.add.at(rhs[:, 1], src, vals)
+    diffused = solve_heat(csr_matrix(ops["pattern"], ops["H"]), rhs)
+    reached = diffused[:, 0] != 0.0
+    extended = np.zeros(n, dtype=F64)
+    extended[reached] = diffused[reached, 1] / diffused[reached, 0]
+    excess = 0.0
+    if reached.any():
+        excess = float(max(0.0, np.max(np.maximum(extended[reached] - vals.max(), vals.min() - extended[reached]))))
+    return extended, excess

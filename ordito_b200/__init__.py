@@ -7,7 +7,9 @@ Drop-in modules for the path: ``laplacian`` (pattern, cotangent weights, Laplaci
 ``include/ordito_b200.h`` (``libordito_b200.so``, built by ``python -m ordito_b200.build``).
 """
 
-from ordito_b200 import creation  # noqa: F401  (host-only mesh generators)
+from ordito_b200 import config, creation  # noqa: F401  (host-only: settings, mesh generators)
+from ordito_b200.config import deterministic, is_deterministic, set_deterministic  # noqa: F401
 
-__all__ = ["array", "cholesky", "creation", "device", "heat", "laplacian", "linalg", "mesh"]
+__all__ = ["array", "cholesky", "config", "creation", "device", "heat", "laplacian", "linalg", "mesh",
+           "deterministic", "is_deterministic", "set_deterministic"]
 __version__ = "0.1.0"

@@ -103,6 +103,9 @@ SIGNATURES: dict[str, list] = {
     "ob_chol_values": [P, P, ctypes.c_longlong, POINTER(ctypes.c_longlong), P],
     "ob_divergence_tiles": [P, P, I, P, P, P, P],
     "ob_grad_div_tiled": [P, P, P, P, P, P, P, I, I, P, I, P, P, I, P, P, P],
+    "ob_extend_seed": [P, P, I, I, P, P, P, P],
+    "ob_extend_ratio": [P, I, P, P, P],
+    "ob_chol_set_deterministic": [P, I, P],
     "ob_floor_f32": [P, ctypes.c_longlong, c_float, P],
     "ob_chol_nbytes": [P, POINTER(c_size_t)],
     "ob_chol_host_solve": [I, P, P, P, P, I, I, P, P, POINTER(ctypes.c_longlong)],

@@ -22,7 +22,7 @@ from typing import Any
 
 import numpy as np
 
-from ordito_b200 import _lib
+from ordito_b200 import _lib, config
 from ordito_b200.array import CsrMatrix
 from ordito_b200.device import DEFAULT_STREAM, DeviceArray, device_pointer, element_count
 
@@ -105,6 +105,10 @@ class SparseCholesky:
         self.analysis = analysis
         self.singular = singular is not False
         self.negated = bool(negated)
+        # The determinism setting in force when the factorization is built (ordito_b200.config).
+        self.deterministic = config.is_deterministic()
+        if self.deterministic:
+            _lib.call("ob_chol_set_deterministic", handle, 1, DEFAULT_STREAM)
 
     @property
     def n(self) -> int:

@@ -959,6 +959,21 @@ __global__ void zero_rows_kernel(const int2* __restrict__ ranges, int n_ranges, 
     (void)n_ranges;
 }
 
+// The deterministic forward update's gather: B[rows[t]] += the update rows src[offsets[t] ..
+// offsets[t + 1]) in that order (a warp a target row, its lanes the columns).
+__global__ void gather_updates_kernel(const int* __restrict__ offsets, const int* __restrict__ rows,
+                                      const int* __restrict__ src, int n_targets, int k, double* work) {
+    const int t = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    if (t >= n_targets) return;
+    const int lane = threadIdx.x & 31;
+    double* out = work + (size_t)rows[t] * k;
+    for (int c = lane; c < k; c += 32) {
+        double acc = out[c];
+        for (int j = offsets[t]; j < offsets[t + 1]; ++j) acc += work[(size_t)src[j] * k + c];
+        out[c] = acc;
+    }
+}
+
 // Gathers rows of x (old numbering, k columns) into the factor's numbering at the even internal
 // stride kp (a pad column is zero), zeroing pinned rows; or scatters back.
 __global__ void permute_in_kernel(int n, int k, int kp, const int* __restrict__ perm,
@@ -1022,6 +1037,14 @@ struct Factor {
     int2* zero = nullptr;  // row ranges split tiles accumulate into (zeroed each pass)
     int n_zero = 0;
     int tile_chunk = 0, tile_waves = 0;  // the split parameters the tile lists were built with
+    // Deterministic passes: no split tiles, and each node's forward update G B[own] written to its
+    // own rows U of the work buffer (rows 3n ..), then added into its target rows by one gather a
+    // level, every target row's contributions in node order -- no atomics anywhere in a pass.
+    bool deterministic = false;
+    long long n_update_rows = 0;               // rows of U (every node's off-diagonal rows)
+    std::vector<int*> gather_offsets;          // per level: device CSR over its target rows
+    std::vector<int*> gather_rows, gather_src;
+    std::vector<int> n_gather;                 // per level: target rows
     // Device: each row's supernode and each supernode's parent (-1 at a root), for marking the
     // supernodes a batch of source indicators reaches.
     int* node_of_row = nullptr;
@@ -1046,6 +1069,7 @@ struct Factor {
     // one stream at a time).
     struct WorkSet {
         int cap_k = 0;
+        long long rows = 0;  // rows of the BYX allocation (3 n, plus U in a deterministic factor)
         double *BYX = nullptr, *R = nullptr, *RHS = nullptr, *SOL = nullptr;
         unsigned char* active = nullptr;  // device, one flag a supernode (marked sources)
         // B, Y and X at the even column stride kp of a call: n rows of kp doubles each.
@@ -1110,6 +1134,12 @@ int build_tiles(Factor* F, int chunk, int waves, cudaStream_t stream) {
     F->tile_owned.clear();
     F->zero = nullptr;
     F->n_zero = 0;
+    F->gather_offsets.clear();
+    F->gather_rows.clear();
+    F->gather_src.clear();
+    F->n_gather.clear();
+    const int requested_chunk = chunk;
+    if (F->deterministic) chunk = 0;  // split tiles accumulate atomically
     // One launch per tree level and direction. Forward at a level: every node's
     // Y[own] = L11^-1 B[own] and B[off rows] += G B[own] (atomic: siblings share ancestors' rows);
     // backward: X[own] = [L11^-1; G]^T [Y[own]; X[off rows]], one product over nc + noff. Each
@@ -1142,6 +1172,12 @@ int build_tiles(Factor* F, int chunk, int waves, cudaStream_t stream) {
     };
     std::vector<std::vector<Tile>> fw(L), bw(L);
     std::vector<int2> zero_ranges;
+    // A deterministic factor's update rows: node s's at 3 n + u_at[s] .. + noff.
+    std::vector<int> u_at(ns, 0);
+    for (int s = 0, total = 0; s < ns; ++s) {
+        u_at[s] = total;
+        total += (int)A.nodes[s].off_rows.size();
+    }
     for (int s = 0; s < ns; ++s) {
         const Node& nd = A.nodes[s];
         const int nc = nd.count, noff = (int)nd.off_rows.size(), ld = ld_at[s];
@@ -1160,9 +1196,54 @@ int build_tiles(Factor* F, int chunk, int waves, cudaStream_t stream) {
         if (zero) zero_ranges.push_back(make_int2(nd.start, nc));
         for (int r0 = 0; r0 < noff; r0 += kTileRows) {
             const int rows = std::min(kTileRows, noff - r0);
+            if (F->deterministic) {
+                // Forward update: U[node] = G B[own], added into B[off rows] by the level's gather.
+                emit(fw[nd.level], Tile{off_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, 3 * n + u_at[s], -1, 0, 0, 0, s},
+                     nc, false, kAssign, kAssign);
+                continue;
+            }
             // Forward update: B[off rows] += G B[own].
             emit(fw[nd.level], Tile{off_at[s], ld, 0, r0, rows, 0, 0, nd.start, -1, 0, rows_at[s], 0, 0, 0, s},
                  nc, split_fwd, kAtomicAdd, kAtomicAdd);
+        }
+    }
+    if (F->deterministic) {
+        // Per level, every target row's update rows (U rows 3n + u_at[s] + r), nodes in index
+        // order: the gather adds them in that order.
+        std::vector<std::vector<std::pair<int, int>>> targets(L);
+        for (int s = 0; s < ns; ++s) {
+            const Node& nd = A.nodes[s];
+            if (nd.count == 0) continue;
+            for (int r = 0; r < (int)nd.off_rows.size(); ++r)
+                targets[nd.level].push_back({nd.off_rows[r], 3 * n + u_at[s] + r});
+        }
+        F->gather_offsets.assign(L, nullptr);
+        F->gather_rows.assign(L, nullptr);
+        F->gather_src.assign(L, nullptr);
+        F->n_gather.assign(L, 0);
+        for (int l = 0; l < L; ++l) {
+            auto& list = targets[l];
+            if (list.empty()) continue;
+            std::stable_sort(list.begin(), list.end(),
+                             [](const std::pair<int, int>& a, const std::pair<int, int>& b) { return a.first < b.first; });
+            std::vector<int> offsets, rows, src;
+            for (size_t i = 0; i < list.size(); ++i) {
+                if (i == 0 || list[i].first != list[i - 1].first) {
+                    offsets.push_back((int)i);
+                    rows.push_back(list[i].first);
+                }
+                src.push_back(list[i].second);
+            }
+            offsets.push_back((int)list.size());
+            F->n_gather[l] = (int)rows.size();
+            for (auto* vec : {&offsets, &rows, &src}) {
+                int* d = nullptr;
+                int st2 = tile_alloc(F, (void**)&d, sizeof(int) * vec->size(), stream);
+                if (st2) return st2;
+                OB_CUDA(cudaMemcpyAsync(d, vec->data(), sizeof(int) * vec->size(), cudaMemcpyHostToDevice, stream));
+                (vec == &offsets ? F->gather_offsets : vec == &rows ? F->gather_rows : F->gather_src)[l] = d;
+            }
+            OB_CUDA(cudaStreamSynchronize(stream));  // the host lists go out of scope
         }
     }
     // Adjacent ranges joined, then cut into pieces of at most 16 rows: one block each, so the
@@ -1200,9 +1281,10 @@ int build_tiles(Factor* F, int chunk, int waves, cudaStream_t stream) {
     if (!st) st = push(bw, F->bwd, F->n_bwd);
     if (st) return st;
     F->launches_per_pass = 0;
-    for (int l = 0; l < L; ++l) F->launches_per_pass += (F->n_fwd[l] > 0) + (F->n_bwd[l] > 0);
+    for (int l = 0; l < L; ++l)
+        F->launches_per_pass += (F->n_fwd[l] > 0) + (F->n_bwd[l] > 0) + (F->deterministic && F->n_gather[l] > 0);
     OB_CUDA(cudaStreamSynchronize(stream));  // host staging buffers go out of scope
-    F->tile_chunk = chunk;
+    F->tile_chunk = requested_chunk;
     F->tile_waves = waves;
     return OB_OK;
 }
@@ -1259,6 +1341,9 @@ int setup_factor(Factor* F, const double* values, double sign, int pin_mode, cud
     F->n_nodes = ns;
     for (auto& W : F->sets)
         if ((st = dev_alloc(F, (void**)&W.active, std::max(ns, 1), stream))) return st;
+    long long update_rows = 0;
+    for (const Node& nd : A.nodes) update_rows += (long long)nd.off_rows.size();
+    F->n_update_rows = update_rows;
     F->inv_at = std::move(layout.inv_at);
     F->off_at = std::move(layout.off_at);
     F->rows_at = std::move(layout.rows_at);
@@ -1275,28 +1360,31 @@ int setup_factor(Factor* F, const double* values, double sign, int pin_mode, cud
 inline int even_columns(int k) { return (k + 1) & ~1; }
 
 int ensure_work(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream) {
-    if (k <= W.cap_k) return OB_OK;
+    const long long rows = 3LL * F->n + (F->deterministic ? F->n_update_rows : 0);
+    if (k <= W.cap_k && rows == W.rows) return OB_OK;
+    if (W.cap_k > k) k = W.cap_k;  // a change of rows keeps the widest width
     // Growing the buffers invalidates every recorded graph (they name the old ones).
     OB_CUDA(cudaStreamSynchronize(stream));
     for (auto& g : W.graphs) cudaGraphExecDestroy(g.exec);
     W.graphs.clear();
     // The smaller buffers go (no graph names them any more): one set at the widest width.
-    const size_t old_vec = sizeof(double) * (size_t)F->n * (W.cap_k > 0 ? even_columns(W.cap_k) : 0);
+    const size_t old_row = sizeof(double) * (size_t)(W.cap_k > 0 ? even_columns(W.cap_k) : 0);
     for (double** p : {&W.BYX, &W.R, &W.RHS, &W.SOL}) {
         if (*p == nullptr) continue;
         auto it = std::find(F->owned.begin(), F->owned.end(), (void*)*p);
         if (it != F->owned.end()) {
             F->owned.erase(it);
-            F->bytes -= (p == &W.BYX ? 3 : 1) * old_vec;
+            F->bytes -= old_row * (size_t)(p == &W.BYX ? W.rows : F->n);
             OB_CUDA(cudaFreeAsync(*p, stream));
         }
         *p = nullptr;
     }
-    const size_t vec = sizeof(double) * (size_t)F->n * even_columns(k);
+    const size_t row = sizeof(double) * (size_t)even_columns(k);
     for (double** p : {&W.BYX, &W.R, &W.RHS, &W.SOL}) {
-        int st = dev_alloc(F, (void**)p, (p == &W.BYX ? 3 : 1) * vec, stream);
+        int st = dev_alloc(F, (void**)p, row * (size_t)(p == &W.BYX ? rows : F->n), stream);
         if (st) return st;
     }
+    W.rows = rows;
     W.cap_k = k;
     ++W.generation;
     return OB_OK;
@@ -1326,6 +1414,11 @@ __global__ void mark_sources_kernel(const int* __restrict__ sources, const int* 
 int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream,
                       const unsigned char* forward_active = nullptr) {
     const int L = F->analysis->levels;
+    // The tiles address rows up to 3 n (plus the update rows of a deterministic factor): the work
+    // buffer must have been allocated for the factor's present mode.
+    OB_REQUIRE(W.BYX != nullptr && W.rows == 3LL * F->n + (F->deterministic ? F->n_update_rows : 0) &&
+                   k <= even_columns(W.cap_k),
+               "chol pass: work buffers not prepared for %d columns in this mode", k);
     const int ct = (k + kTileCols - 1) / kTileCols;
     if (F->n_zero > 0) {
         zero_rows_kernel<<<F->n_zero, 256, 0, stream>>>(F->zero, F->n_zero, k, W.Y(k, F->n), W.X(k, F->n));
@@ -1347,8 +1440,14 @@ int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream,
         return OB_OK;
     };
     int st = OB_OK;
-    for (int l = 0; l < L && st == OB_OK; ++l)
+    for (int l = 0; l < L && st == OB_OK; ++l) {
         if (F->n_fwd[l]) st = level(F->fwd[l], F->n_fwd[l], forward_active, "chol forward level");
+        if (st == OB_OK && F->deterministic && F->n_gather[l] > 0) {
+            gather_updates_kernel<<<ceil_div(F->n_gather[l], 8), 256, 0, stream>>>(
+                F->gather_offsets[l], F->gather_rows[l], F->gather_src[l], F->n_gather[l], k, W.BYX);
+            OB_CHECK_LAUNCH("chol deterministic gather");
+        }
+    }
     for (int l = L - 1; l >= 0 && st == OB_OK; --l)
         if (F->n_bwd[l]) st = level(F->bwd[l], F->n_bwd[l], nullptr, "chol backward level");
     return st;
@@ -1687,6 +1786,31 @@ int ob_chol_tile(void* factor, int chunk, int waves, ob_stream_t stream_) {
         ++W.generation;
     }
     return build_tiles(F, chunk, waves, stream);
+}
+
+int ob_chol_set_deterministic(void* factor, int on, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(factor != nullptr, "ob_chol_set_deterministic: bad argument");
+    Factor* F = static_cast<Factor*>(factor);
+    if (F->deterministic == (on != 0)) return OB_OK;
+    {
+        // No pass of this factor may be in flight while its tiles and buffers are replaced.
+        std::lock_guard<std::recursive_mutex> guard(capture_mutex());
+        OB_CUDA(cudaDeviceSynchronize());
+    }
+    for (auto& W : F->sets) {
+        for (auto& g : W.graphs) cudaGraphExecDestroy(g.exec);
+        W.graphs.clear();
+        ++W.generation;
+    }
+    F->deterministic = on != 0;
+    int st = build_tiles(F, F->tile_chunk, F->tile_waves, stream);
+    // Work buffers already made are remade at the new row count now (a recording made later
+    // cannot allocate them).
+    for (auto& W : F->sets)
+        if (!st && W.cap_k > 0) st = ensure_work(F, W, W.cap_k, stream);
+    if (!st) OB_CUDA(cudaStreamSynchronize(stream));
+    return st;
 }
 
 int ob_chol_work_generation(void* factor, long long* generation) {

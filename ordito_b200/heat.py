@@ -1087,3 +1087,79 @@ def _heat_geodesic(bound: Trimesh, src_arg: Any, t: float | None, use_robust: bo
         if solver.diffuse_pinned(u0, pinned):
             _lib.call("ob_axpby", n, 0.5, pinned.ptr, 0.5, heat.ptr, heat.ptr, DEFAULT_STREAM)
     return _distance_from_heat(bound, solver, src, heat)
+
+
+# extend_scalar warns when the extension leaves the source values' range by more than this
+# fraction of their scale (ordito/heat.py:166): the diffusion is a convex average only while every
+# cotangent weight is non-negative.
+_EXTEND_RANGE_TOLERANCE = 1e-4
+
+
+def extend_scalar(
+    mesh: Any = None,
+    faces: Any = None,
+    sources: Any = None,
+    values: Any = None,
+    t: float | None = None,
+    *,
+    vertices: Any = None,
+) -> DeviceArray:
+    """Extend values from a few source vertices over the whole surface by nearest-source
+    interpolation (ordito/heat.py:2321; potpourri3d's ``MeshVectorHeatSolver.extend_scalar``).
+
+    ``extend_scalar(trimesh, sources, values, t=...)`` or ``extend_scalar(vertices, faces, sources,
+    values, t)``. The values and an indicator of the sources diffuse through the heat system for
+    the same short time ``t`` (one two-column settled solve); their quotient is the extension.
+    Returns the ``(n_vertices,)`` float64 field on the device. Raises ``ValueError`` when
+    ``values`` is not as long as ``sources`` or a source is not a vertex index; warns
+    (``UserWarning``) when the field leaves the source values' range (negative cotangent weights).
+    """
+    if isinstance(mesh, Trimesh):
+        if vertices is not None or values is not None:
+            raise TypeError("extend_scalar: pass (trimesh, sources, values) or (vertices, faces, sources, values)")
+        bound, held, src_arg, val_arg = mesh, True, faces, sources
+    else:
+        verts = mesh if vertices is None else vertices
+        if verts is None or faces is None:
+            raise TypeError("extend_scalar: needs a Trimesh, or vertices and faces")
+        bound, held, src_arg, val_arg = Trimesh(verts, faces), False, sources, values
+    try:
+        return _extend_scalar(bound, src_arg, val_arg, t)
+    finally:
+        if not held:
+            bound.dispose()
+
+
+def _extend_scalar(bound: Trimesh, src_arg: Any, val_arg: Any, t: float | None) -> DeviceArray:
+    n = bound.n_vertices
+    src = _require_sources(src_arg if hasattr(src_arg, "__cuda_array_interface__")
+                           else np.ascontiguousarray(src_arg, dtype=np.int32).reshape(-1), n)
+    if n == 0 or bound.n_faces == 0 or src.size == 0:
+        return DeviceArray.zeros(n, np.float64)
+    vals = as_device(val_arg if hasattr(val_arg, "__cuda_array_interface__")
+                     else np.ascontiguousarray(val_arg, dtype=np.float64).reshape(-1), np.float64)
+    if vals.size != src.size:
+        raise ValueError(f"extend_scalar: values must hold one value per source ({src.size}), got {vals.size}")
+    rhs = DeviceArray.empty((n, 2), np.float64)
+    value_range = DeviceArray.empty(3, np.float64)
+    invalid = DeviceArray.empty(1, np.int32)
+    _lib.call("ob_extend_seed", src.ptr, vals.ptr, src.size, n, rhs.ptr, value_range.ptr, invalid.ptr,
+              DEFAULT_STREAM)
+    if int(invalid.numpy()[0]) != 0:
+        raise ValueError("extend_scalar: every entry of sources must be a vertex index in [0, n_vertices)")
+    solver = bound.heat_solver(t)
+    diffused = DeviceArray.zeros((n, 2), np.float64)
+    solver.diffuse(rhs, diffused)
+    extended = DeviceArray.empty(n, np.float64)
+    _lib.call("ob_extend_ratio", diffused.ptr, n, value_range.ptr, extended.ptr, DEFAULT_STREAM)
+    low, high, excess = (float(x) for x in value_range.numpy())
+    scale = max(high - low, abs(low), abs(high))
+    if excess > _EXTEND_RANGE_TOLERANCE * scale:
+        warnings.warn(
+            f"extend_scalar: the extended field leaves the source values' range [{low:.6g}, {high:.6g}] "
+            f"by {excess:.3g}. The cotangent weights of obtuse triangles are negative here, so the "
+            "diffusion is not a convex average.",
+            UserWarning,
+            stacklevel=3,
+        )
+    return extended

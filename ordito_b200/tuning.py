@@ -36,6 +36,10 @@ def tune_pass(factor: Any, k: int, *, reps: int = 10,
     and makes every recording over the factor's buffers record again on its next launch).
     Returns ``{"best": (chunk, waves), "ms": {(chunk, waves): ms, ...}}``."""
     times: dict[tuple[int, int], float] = {}
+    if getattr(factor, "deterministic", False):
+        # A deterministic factor never splits (its passes take no atomics): one schedule.
+        times[(0, 0)] = _time(factor, k, reps)
+        return {"best": (0, 0), "ms": times}
     for chunk, waves in candidates:
         _lib.call("ob_chol_tile", factor.handle, int(chunk), int(waves), None)
         times[(chunk, waves)] = _time(factor, k, reps)

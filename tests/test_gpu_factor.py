@@ -187,3 +187,29 @@ def test_cotmatrix_signature_and_weights(gpu) -> None:
     assert np.array_equal(entries, np.maximum(signed, np.float32(0.0)))
     with pytest.raises(ValueError):
         glap.cotmatrix(v, f.reshape(-1), cot_entries=cot.astype(np.float32), nonnegative_weights=True)
+
+
+def test_deterministic_passes_repeat_bit_for_bit(gpu) -> None:
+    """ordito.config.set_deterministic for the factored solves: with the setting on when the
+    factors are built, the passes take no atomics (no split tiles; forward updates gathered in
+    supernode order), so repeated batches return identical arrays; they agree with the default
+    passes to rounding."""
+    from ordito_b200 import config
+    from ordito_b200.mesh import Trimesh
+
+    v, f = creation.jittered_torus(128, 64, seed=6)
+    n = v.shape[0]
+    rng = np.random.default_rng(2)
+    sets = [[int(s)] for s in rng.choice(n, size=12, replace=False)]
+    fast = gheat.heat_geodesic_batch(Trimesh(v, f.reshape(-1)), sets, refine=0).numpy()
+    with config.deterministic(True):
+        mesh = Trimesh(v, f.reshape(-1))
+        first = gheat.heat_geodesic_batch(mesh, sets, refine=0).numpy()
+        assert mesh.heat_solver(None, method="meshlab").heat_factor.deterministic
+    runs = [gheat.heat_geodesic_batch(mesh, sets, refine=0).numpy() for _ in range(3)]
+    for again in runs:
+        assert np.array_equal(again, first)
+    assert np.max(np.abs(first - fast)) <= 1e-12 * np.abs(fast).max()
+    # A single column takes the narrow kernel, with the same tiles.
+    one = [gheat.heat_geodesic_batch(mesh, [sets[0]], refine=0).numpy() for _ in range(2)]
+    assert np.array_equal(one[0], one[1])

@@ -239,3 +239,16 @@ def test_dissection_ordering_solves_as_the_default_ordering() -> None:
     r -= r.mean()
     x, y = hp.PoissonFactor(P).solve(r), hp.PoissonFactor(P, v).solve(r)
     assert hp.relative_linf(y - y.mean(), x - x.mean()) <= 1e-12
+
+
+def test_extend_scalar_between_the_poles(known: dict) -> None:
+    """ordito/heat.py:2394-2411: +1 at the north pole, -1 at the south; each hemisphere away from
+    the equator takes its pole's value."""
+    item = known["extend_scalar_poles_icosphere3"]
+    v, f = creation.icosphere(3)
+    heights = v[:, 2]
+    poles = np.array([np.argmax(heights), np.argmin(heights)])
+    extended, excess = hp.extend_scalar(v, f, poles, np.array(item["values"]))
+    assert f"{extended[heights > 0.5].min():.2f}" == item["north_min"]
+    assert f"{extended[heights < -0.5].max():.2f}" == item["south_max"]
+    assert excess <= 1e-4
