@@ -674,7 +674,8 @@ def run_packed() -> dict:
         "columns": k,
         "setup_s": setup_s,
         "factor_bytes": packed.nbytes,
-        "pass_schedule": {role: list(report["best"]) for role, report in packed.tuning.items()},
+        "pass_schedule": {role: {"split": list(report["best"]), "narrow_waves": report["narrow_waves"]}
+                          for role, report in packed.tuning.items()},
         "ms_per_step": ms,
         "value": queries / (ms / 1e3),
         "unit": "solves/s",
@@ -1052,6 +1053,8 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
                 "parallelism": f"replicas{dist.world}",
                 "setup_s": setup_s,
                 "pass_schedule": {role: {"best": list(report["best"]),
+                                         "narrow_waves": report["narrow_waves"],
+                                         "width_ms": {str(w): round(t, 4) for w, t in report["width_ms"].items()},
                                          "ms": {f"{c}/{w}": round(t, 4) for (c, w), t in report["ms"].items()}}
                                   for role, report in tuning.items()} if tuning else (args.pass_schedule or "default (not tuned)"),
             },

@@ -646,7 +646,8 @@ struct Tile {
 
 constexpr int kTileRows = 64;   // output rows per tile
 constexpr int kWorkSets = 3;    // independent work-buffer sets a factor holds
-constexpr int kTileCols = 64;   // right-hand-side columns per tile
+constexpr int kTileCols = 64;   // right-hand-side columns per tile (the wide form)
+constexpr int kTileColsNarrow = 32;  // the narrow form: twice the CTAs, half the columns each
 // Inner-dimension step staged in shared memory. 16 (two stages, 39 KB, 4 CTAs per SM) measured
 // 0.82 ms a pass on the 131k torus at 64 columns, against 1.11 ms for 32 (74 KB, 3 CTAs per SM).
 constexpr int kTileK = 16;
@@ -655,9 +656,12 @@ constexpr int kTileThreads = 128;
 // Resident CTAs of the 64-column product an SM: at most 96 registers a thread and two stages of
 // 19.5 KB hold five (126 registers held four).
 constexpr int kTileCtasPerSm = 5;
-// Shared rows of 72 doubles: the 8 x 4 fragment loads of a warp then touch every 8-byte bank
-// pair exactly twice (the minimum for 256 bytes).
-constexpr int kLd = kTileCols + 8;
+// Shared rows of 72 doubles (a transposed matrix block's 64 output rows, a 64-column input row):
+// the 8 x 4 fragment loads of a warp then touch every 8-byte bank pair exactly twice (the minimum
+// for 256 bytes); 40 for a 32-column input row.
+constexpr int kLd = kTileRows + 8;
+template <int TC>
+constexpr int input_ld() { return TC + 8; }
 
 // 16-byte asynchronous global -> shared copies; bytes < 16 zero-fills the rest (0: all zeros, and
 // the source is not read). Both read through L2 only: a factor block is read once per tile, and
@@ -681,9 +685,10 @@ __device__ __forceinline__ void copy_wait() {
 // Shared staging of one inner-dimension step: the matrix block (row-major [64][kLdK] for a
 // row-major matrix, k-major [16][kLd] for a transposed one) and the 16 gathered input rows.
 constexpr int kLdK = kTileK + 4;  // row-major staging: fragment loads touch each bank pair twice
+template <int TC>
 struct Stage {
     double a[kTileRows * kLdK > kTileK * kLd ? kTileRows * kLdK : kTileK * kLd];
-    double b[kTileK * kLd];
+    double b[kTileK * input_ld<TC>()];
 };
 
 // One 64 x 64 output tile for a CTA of four warps, each warp a 16-row strip of all 64 columns as
@@ -694,34 +699,39 @@ struct Stage {
 // subtracted, or added atomically per the tile's op. `k` (the column stride) is even and every
 // block row starts on 16 bytes, so every copy is aligned. `in` and `out` are the same stacked
 // work buffer: the rows a launch's tiles read are never rows any tile of that launch writes.
+template <int TC>
 __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double* __restrict__ vals,
                                              const int* __restrict__ idx,
-                                             const double* in, double* out, int k, Stage* stage) {
+                                             const double* in, double* out, int k, Stage<TC>* stage) {
+    constexpr int kJ = TC / 8;             // 8-column MMA tiles a warp strip holds
+    constexpr int kLdB = input_ld<TC>();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wr = warp * 16;                  // the warp's strip: rows [wr, wr + 16), all 64 columns
     const int fr = lane >> 2, fk = lane & 3;  // fragment coordinates
-    double acc[2][8][2];
+    double acc[2][kJ][2];
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int j = 0; j < kJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     // Rows of the strip within the block, for its known-zero inner steps.
     const int row_lo = t.r0 + wr, row_hi = row_lo + 15;
     const bool live = wr < t.rows;
     const double* M = vals + t.m;
-    // Each operand block is 64 x kTileK doubles in 16-byte chunks, kChunks per thread.
+    // The matrix block is 64 x kTileK doubles in 16-byte chunks, kChunks per thread; the input
+    // block kTileK x TC, kChunksB per thread.
     constexpr int kChunks = kTileRows * kTileK / 2 / kTileThreads;
+    constexpr int kChunksB = TC * kTileK / 2 / kTileThreads;
     // The input rows of this thread's chunks of an inner step (-1 past the inner range), read
     // one step ahead of the copies that use them, so a gathered index's load latency is not
     // paid in front of every step's copies.
     auto input_rows = [&](int kb, int* r) {
 #pragma unroll
-        for (int q = 0; q < kChunks; ++q) {
-            const int kk = (threadIdx.x + q * kTileThreads) / (kTileCols / 2);
+        for (int q = 0; q < kChunksB; ++q) {
+            const int kk = (threadIdx.x + q * kTileThreads) / (TC / 2);
             r[q] = kb + kk < t.k1 ? (t.in_rows < 0 ? t.in_base + kb + kk : idx[t.in_rows + kb + kk]) : -1;
         }
     };
-    auto issue = [&](int kb, const int* in_row, Stage& s) {
+    auto issue = [&](int kb, const int* in_row, Stage<TC>& s) {
 #pragma unroll
         for (int q = 0; q < kChunks; ++q) {
             const int chunk = threadIdx.x + q * kTileThreads;
@@ -739,20 +749,24 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
                 const double* src = valid ? M + (size_t)(t.r0 + i) * t.ld + kb + c2 : M;
                 copy16(&s.a[i * kLdK + c2], src, 8 * valid);
             }
+        }
+#pragma unroll
+        for (int q = 0; q < kChunksB; ++q) {
+            const int chunk = threadIdx.x + q * kTileThreads;
             // Input rows: row kk of the step, columns c0 + 2 c .. + 1.
-            const int kk = chunk / (kTileCols / 2), c2 = 2 * (chunk % (kTileCols / 2));
+            const int kk = chunk / (TC / 2), c2 = 2 * (chunk % (TC / 2));
             int valid = 0;
             const double* src = in;
             if (in_row[q] >= 0 && c0 + c2 < k) {
                 src = in + (size_t)in_row[q] * k + c0 + c2;
                 valid = 16;
             }
-            copy16_l2(&s.b[kk * kLd + c2], src, valid);
+            copy16_l2(&s.b[kk * kLdB + c2], src, valid);
         }
         copy_commit();
     };
     const int steps = (t.k1 - t.k0 + kTileK - 1) / kTileK;
-    int first_rows[kChunks], next_rows[kChunks];
+    int first_rows[kChunksB], next_rows[kChunksB];
     input_rows(t.k0, first_rows);
     issue(t.k0, first_rows, stage[0]);
     if (steps > 1) input_rows(t.k0 + kTileK, next_rows);
@@ -773,7 +787,7 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
             issue(t.k0 + (st + 1) * kTileK, next_rows, stage[(st + 1) & 1]);
             if (st + 2 < steps) input_rows(t.k0 + (st + 2) * kTileK, next_rows);
         }
-        const Stage& s = stage[st & 1];
+        const Stage<TC>& s = stage[st & 1];
         // A strip skips a whole inner step when all its products are known zeros: padding rows
         // past the tile, or the zero triangle of L11^-1 (the decision is warp-uniform and taken
         // outside the unrolled step, which stays branch-free).
@@ -783,7 +797,7 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
         if (!zero) {
 #pragma unroll
             for (int k4 = 0; k4 < kTileK; k4 += 4) {
-                double a[2], b[8];
+                double a[2], b[kJ];
                 if (t.trans) {
 #pragma unroll
                     for (int i = 0; i < 2; ++i) a[i] = s.a[(k4 + fk) * kLd + wr + 8 * i + fr];
@@ -792,11 +806,11 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
                     for (int i = 0; i < 2; ++i) a[i] = s.a[(wr + 8 * i + fr) * kLdK + k4 + fk];
                 }
 #pragma unroll
-                for (int j = 0; j < 8; ++j) b[j] = s.b[(k4 + fk) * kLd + 8 * j + fr];
+                for (int j = 0; j < kJ; ++j) b[j] = s.b[(k4 + fk) * kLdB + 8 * j + fr];
 #pragma unroll
                 for (int i = 0; i < 2; ++i)
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+                    for (int j = 0; j < kJ; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
             }
         }
     }
@@ -805,7 +819,7 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
         const int r = out_row[i];
         if (r < 0) continue;
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
+        for (int j = 0; j < kJ; ++j)
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int c = c0 + 8 * j + 2 * fk + h;
@@ -822,8 +836,9 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
     }
 }
 
-// The two stages live in dynamic shared memory (kStageBytes, above the 48 KB static limit).
-constexpr int kStageBytes = 2 * (int)sizeof(Stage);
+// The two stages live in dynamic shared memory (stage_bytes, above the 48 KB static limit).
+template <int TC>
+constexpr int stage_bytes() { return 2 * (int)sizeof(Stage<TC>); }
 
 // A forward pass over right-hand sides that are zero outside the marked supernodes (a batch of
 // source indicators: only a source's supernode and its ancestors receive anything): a tile of an
@@ -842,14 +857,15 @@ __device__ __forceinline__ bool skip_inactive(const Tile& t, const unsigned char
     return true;
 }
 
-// One launch per phase: a CTA per (tile, column block).
-__global__ void __launch_bounds__(kTileThreads, kTileCtasPerSm)
+// One launch per phase: a CTA per (tile, column block of TC columns).
+template <int TC>
+__global__ void __launch_bounds__(kTileThreads, TC == kTileCols ? kTileCtasPerSm : 8)
 tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
                     const int* __restrict__ idx, double* rows, int k, const unsigned char* active) {
     extern __shared__ __align__(16) unsigned char shared_stages[];
-    Stage* stage = reinterpret_cast<Stage*>(shared_stages);
-    if (skip_inactive(tiles[blockIdx.x], active, blockIdx.y * kTileCols, kTileCols, idx, rows, k)) return;
-    tile_product(tiles[blockIdx.x], blockIdx.y * kTileCols, vals, idx, rows, rows, k, stage);
+    Stage<TC>* stage = reinterpret_cast<Stage<TC>*>(shared_stages);
+    if (skip_inactive(tiles[blockIdx.x], active, blockIdx.y * TC, TC, idx, rows, k)) return;
+    tile_product<TC>(tiles[blockIdx.x], blockIdx.y * TC, vals, idx, rows, rows, k, stage);
 }
 
 // The same tile product for a narrow batch (KP = 2, 4, 6 or 8 columns, the even stride of 1-8
@@ -1037,6 +1053,10 @@ struct Factor {
     int2* zero = nullptr;  // row ranges split tiles accumulate into (zeroed each pass)
     int n_zero = 0;
     int tile_chunk = 0, tile_waves = 0;  // the split parameters the tile lists were built with
+    // Column width of each level's tiles a direction (kTileCols or kTileColsNarrow): levels with
+    // fewer tiles than narrow_waves waves of the resident grid take the narrow form (0: none).
+    int narrow_waves = 0;
+    std::vector<int> fwd_cols, bwd_cols;
     // Deterministic passes: no split tiles, and each node's forward update G B[own] written to its
     // own rows U of the work buffer (rows 3n ..), then added into its target rows by one gather a
     // level, every target row's contributions in node order -- no atomics anywhere in a pass.
@@ -1118,10 +1138,14 @@ int allow_stage_memory() {
     int device = 0;
     OB_CUDA(cudaGetDevice(&device));
     if (device >= 0 && device < 64 && allowed[device]) return OB_OK;
-    OB_CUDA(cudaFuncSetAttribute(tile_product_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kStageBytes));
-    OB_CUDA(cudaFuncSetAttribute(tile_product_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+    OB_CUDA(cudaFuncSetAttribute(tile_product_kernel<kTileCols>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 stage_bytes<kTileCols>()));
+    OB_CUDA(cudaFuncSetAttribute(tile_product_kernel<kTileCols>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  (int)cudaSharedmemCarveoutMaxShared));
+    OB_CUDA(cudaFuncSetAttribute(tile_product_kernel<kTileColsNarrow>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, stage_bytes<kTileColsNarrow>()));
+    OB_CUDA(cudaFuncSetAttribute(tile_product_kernel<kTileColsNarrow>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
     if (device >= 0 && device < 64) allowed[device] = 1;
     return OB_OK;
 }
@@ -1280,6 +1304,12 @@ int build_tiles(Factor* F, int chunk, int waves, cudaStream_t stream) {
     st = push(fw, F->fwd, F->n_fwd);
     if (!st) st = push(bw, F->bwd, F->n_bwd);
     if (st) return st;
+    F->fwd_cols.assign(L, kTileCols);
+    F->bwd_cols.assign(L, kTileCols);
+    for (int l = 0; l < L; ++l) {
+        if (F->n_fwd[l] < (long long)F->narrow_waves * wave) F->fwd_cols[l] = kTileColsNarrow;
+        if (F->n_bwd[l] < (long long)F->narrow_waves * wave) F->bwd_cols[l] = kTileColsNarrow;
+    }
     F->launches_per_pass = 0;
     for (int l = 0; l < L; ++l)
         F->launches_per_pass += (F->n_fwd[l] > 0) + (F->n_bwd[l] > 0) + (F->deterministic && F->n_gather[l] > 0);
@@ -1419,21 +1449,26 @@ int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream,
     OB_REQUIRE(W.BYX != nullptr && W.rows == 3LL * F->n + (F->deterministic ? F->n_update_rows : 0) &&
                    k <= even_columns(W.cap_k),
                "chol pass: work buffers not prepared for %d columns in this mode", k);
-    const int ct = (k + kTileCols - 1) / kTileCols;
     if (F->n_zero > 0) {
         zero_rows_kernel<<<F->n_zero, 256, 0, stream>>>(F->zero, F->n_zero, k, W.Y(k, F->n), W.X(k, F->n));
         OB_CHECK_LAUNCH("chol zero split rows");
     }
     // A level's launch: the float64 tensor-core tiles, or for a narrow batch (stride 2-8) the
     // register kernel, which does not compute a 64-column tile's idle columns.
-    auto level = [&](const Tile* tiles, int count, const unsigned char* active, const char* what) {
+    auto level = [&](const Tile* tiles, int count, int cols, const unsigned char* active, const char* what) {
         switch (k) {
             case 2: narrow_tile_kernel<2><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active); break;
             case 4: narrow_tile_kernel<4><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active); break;
             case 6: narrow_tile_kernel<6><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active); break;
             case 8: narrow_tile_kernel<8><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active); break;
             default:
-                tile_product_kernel<<<dim3(count, ct), kTileThreads, kStageBytes, stream>>>(tiles, F->vals, F->idx,
+                if (cols == kTileColsNarrow)
+                    tile_product_kernel<kTileColsNarrow>
+                        <<<dim3(count, ceil_div(k, kTileColsNarrow)), kTileThreads, stage_bytes<kTileColsNarrow>(),
+                           stream>>>(tiles, F->vals, F->idx, W.BYX, k, active);
+                else
+                    tile_product_kernel<kTileCols><<<dim3(count, ceil_div(k, kTileCols)), kTileThreads,
+                                                      stage_bytes<kTileCols>(), stream>>>(tiles, F->vals, F->idx,
                                                                                           W.BYX, k, active);
         }
         OB_CHECK_LAUNCH(what);
@@ -1441,7 +1476,7 @@ int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream,
     };
     int st = OB_OK;
     for (int l = 0; l < L && st == OB_OK; ++l) {
-        if (F->n_fwd[l]) st = level(F->fwd[l], F->n_fwd[l], forward_active, "chol forward level");
+        if (F->n_fwd[l]) st = level(F->fwd[l], F->n_fwd[l], F->fwd_cols[l], forward_active, "chol forward level");
         if (st == OB_OK && F->deterministic && F->n_gather[l] > 0) {
             gather_updates_kernel<<<ceil_div(F->n_gather[l], 8), 256, 0, stream>>>(
                 F->gather_offsets[l], F->gather_rows[l], F->gather_src[l], F->n_gather[l], k, W.BYX);
@@ -1449,7 +1484,7 @@ int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream,
         }
     }
     for (int l = L - 1; l >= 0 && st == OB_OK; --l)
-        if (F->n_bwd[l]) st = level(F->bwd[l], F->n_bwd[l], nullptr, "chol backward level");
+        if (F->n_bwd[l]) st = level(F->bwd[l], F->n_bwd[l], F->bwd_cols[l], nullptr, "chol backward level");
     return st;
 }
 
@@ -1786,6 +1821,24 @@ int ob_chol_tile(void* factor, int chunk, int waves, ob_stream_t stream_) {
         ++W.generation;
     }
     return build_tiles(F, chunk, waves, stream);
+}
+
+int ob_chol_tile_columns(void* factor, int narrow_waves, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(factor != nullptr && narrow_waves >= 0 && narrow_waves <= 64, "ob_chol_tile_columns: bad argument");
+    Factor* F = static_cast<Factor*>(factor);
+    if (narrow_waves == F->narrow_waves) return OB_OK;
+    {
+        std::lock_guard<std::recursive_mutex> guard(capture_mutex());
+        OB_CUDA(cudaDeviceSynchronize());
+    }
+    for (auto& W : F->sets) {
+        for (auto& g : W.graphs) cudaGraphExecDestroy(g.exec);
+        W.graphs.clear();
+        ++W.generation;
+    }
+    F->narrow_waves = narrow_waves;
+    return build_tiles(F, F->tile_chunk, F->tile_waves, stream);
 }
 
 int ob_chol_set_deterministic(void* factor, int on, ob_stream_t stream_) {

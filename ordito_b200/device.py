@@ -248,7 +248,10 @@ def element_count(obj: Any) -> int:
 
 
 def synchronize() -> None:
-    _lib.call("ob_stream_synchronize", DEFAULT_STREAM)
+    """Wait for all of the library's work on the current device, on every stream (the served and
+    batched passes run on created non-blocking streams, which the legacy default stream does not
+    wait for)."""
+    _lib.call("ob_device_synchronize")
 
 
 def trim_pool(keep_bytes: int = 0) -> None:

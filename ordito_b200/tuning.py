@@ -1,11 +1,19 @@
-"""Autotuner of the batched pass's tile schedule (no counterpart in the reference).
+"""Autotuner of the batched pass's tile shapes and schedule (no counterpart in the reference).
 
-A factor's triangular pass is one launch per tree level and direction of 64 x 64 output tiles;
-on a level with few tiles, long inner dimensions are split over several tiles (more CTAs, shorter
-dependent chains, atomic accumulation). Which levels to split, and into how long pieces, depends
-on the tree -- its level sizes and separator widths -- and on the batch width. ``tune_pass`` times
-one pass of a factor at ``k`` columns for each candidate schedule (``ob_chol_tile`` + CUDA-event
-timing in ``ob_chol_time_solve``), keeps the fastest, and reports every candidate's time.
+A factor's triangular pass is one launch per tree level and direction of 64-row output tiles on
+the float64 tensor cores. Two choices shape it, and the best of each depends on the tree -- its
+level sizes and separator widths -- and on the batch width:
+
+- the split schedule: on a level with few tiles, long inner dimensions are split over several
+  tiles (more CTAs, shorter dependent chains, atomic accumulation): which levels, and into how
+  long pieces (``ob_chol_tile``);
+- the tile width, the right-hand sides a CTA takes: 64 columns, or 32 (twice the CTAs, half the
+  columns each, 64 instead of 96 registers a thread) on the levels with fewer tiles than some
+  number of waves of the resident grid (``ob_chol_tile_columns``).
+
+``tune_pass`` times one pass of a factor at ``k`` columns (CUDA events, ``ob_chol_time_solve``)
+for each candidate split schedule, then, under the fastest, for each candidate width rule, keeps
+the fastest of all and reports every candidate's time.
 """
 
 from __future__ import annotations
@@ -20,6 +28,9 @@ from ordito_b200 import _lib
 CANDIDATES: tuple[tuple[int, int], ...] = (
     (64, 2), (0, 0), (32, 2), (128, 2), (64, 1), (64, 4), (128, 4), (32, 1),
 )
+# Width rules: the levels with fewer tiles than this many waves take 32-column tiles (0: none,
+# 64: every level).
+WIDTHS: tuple[int, ...] = (0, 1, 2, 4, 64)
 
 
 def _time(factor: Any, k: int, reps: int) -> float:
@@ -36,13 +47,21 @@ def tune_pass(factor: Any, k: int, *, reps: int = 10,
     and makes every recording over the factor's buffers record again on its next launch).
     Returns ``{"best": (chunk, waves), "ms": {(chunk, waves): ms, ...}}``."""
     times: dict[tuple[int, int], float] = {}
+    widths: dict[int, float] = {}
+    _lib.call("ob_chol_tile_columns", factor.handle, 0, None)
     if getattr(factor, "deterministic", False):
         # A deterministic factor never splits (its passes take no atomics): one schedule.
         times[(0, 0)] = _time(factor, k, reps)
-        return {"best": (0, 0), "ms": times}
-    for chunk, waves in candidates:
-        _lib.call("ob_chol_tile", factor.handle, int(chunk), int(waves), None)
-        times[(chunk, waves)] = _time(factor, k, reps)
-    best = min(times, key=times.get)
-    _lib.call("ob_chol_tile", factor.handle, best[0], best[1], None)
-    return {"best": best, "ms": times}
+        best = (0, 0)
+    else:
+        for chunk, waves in candidates:
+            _lib.call("ob_chol_tile", factor.handle, int(chunk), int(waves), None)
+            times[(chunk, waves)] = _time(factor, k, reps)
+        best = min(times, key=times.get)
+        _lib.call("ob_chol_tile", factor.handle, best[0], best[1], None)
+    for narrow in WIDTHS if k > 8 else (0,):
+        _lib.call("ob_chol_tile_columns", factor.handle, int(narrow), None)
+        widths[narrow] = times[best] if narrow == 0 else _time(factor, k, reps)
+    width = min(widths, key=widths.get)
+    _lib.call("ob_chol_tile_columns", factor.handle, int(width), None)
+    return {"best": best, "ms": times, "narrow_waves": width, "width_ms": widths}

@@ -213,3 +213,24 @@ def test_deterministic_passes_repeat_bit_for_bit(gpu) -> None:
     # A single column takes the narrow kernel, with the same tiles.
     one = [gheat.heat_geodesic_batch(mesh, [sets[0]], refine=0).numpy() for _ in range(2)]
     assert np.array_equal(one[0], one[1])
+
+
+@pytest.mark.parametrize("k", [12, 40, 64])
+def test_tile_widths_solve_alike(gpu, k: int) -> None:
+    """The 32-column tiles (ob_chol_tile_columns) on every level against the 64-column ones."""
+    v, f = creation.jittered_torus(96, 48, seed=1)
+    n = v.shape[0]
+    ops = gheat.heat_operators(v, f.reshape(-1), method="meshlab")
+    chol = sparse_cholesky(ops.heat_system, v)
+    rng = np.random.default_rng(k)
+    B = rng.random((n, k))
+    answers = []
+    for narrow in (0, 64, 2):
+        _lib.call("ob_chol_tile_columns", chol.handle, narrow, None)
+        x = DeviceArray.zeros(n * k, np.float64)
+        chol.solve(B.reshape(-1), x, refine=False)
+        answers.append(x.numpy())
+    ref = hp.solve_heat(ops.heat_system.to_scipy(), B).reshape(-1)
+    for got in answers:
+        assert np.max(np.abs(got - answers[0])) <= 1e-12 * np.abs(answers[0]).max()
+        assert np.max(np.abs(got - ref)) <= 1e-9 * np.abs(ref).max()
