@@ -469,6 +469,13 @@ int ob_chol_work_generation_set(void* factor, int set, long long* generation);
  * row read or written once; bytes[4] = 0). Needs a hierarchy of two levels or more. */
 int ob_amg_setup(int n, const int32_t* offsets, const int32_t* columns, const double* values,
                  unsigned seed, void** amg, ob_stream_t stream);
+/* Where ob_amg_setup builds a hierarchy's levels of 32 768 rows or more (process-wide; no
+ * counterpart in the reference, which builds on the device): on_device != 0 (the default) on the
+ * device -- strength, the MIS-2 rounds, the label spread, the power steps, the smoothed
+ * prolongator, its transpose and the Galerkin products assembled by sort-and-segment, each with
+ * the host build's arithmetic in its order -- then the smaller levels and the coarse
+ * pseudo-inverse on the host; 0 the whole build on host threads. */
+int ob_amg_build_mode(int on_device);
 int ob_amg_destroy(void* amg);
 int ob_amg_info(void* amg, long long* info);
 int ob_amg_levels(void* amg, long long* rows, long long* nnz, int capacity);

@@ -107,6 +107,7 @@ SIGNATURES: dict[str, list] = {
     "ob_extend_ratio": [P, I, P, P, P],
     "ob_chol_set_deterministic": [P, I, P],
     "ob_chol_tile_columns": [P, I, P],
+    "ob_amg_build_mode": [I],
     "ob_floor_f32": [P, ctypes.c_longlong, c_float, P],
     "ob_chol_nbytes": [P, POINTER(c_size_t)],
     "ob_chol_host_solve": [I, P, P, P, P, I, I, P, P, POINTER(ctypes.c_longlong)],

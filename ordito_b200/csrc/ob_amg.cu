@@ -49,8 +49,13 @@
 #include <utility>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_reduce.cuh>
+#include <cub/device/device_scan.cuh>
+
 #include "ob_host.hpp"
 #include "ob_internal.cuh"
+#include "ob_scratch.cuh"
 
 namespace ob {
 namespace {
@@ -87,27 +92,27 @@ struct HCsr {
     bool long_row(int i) const { return off[i + 1] - off[i] >= kLongRow; }
 };
 
-uint64_t splitmix64(uint64_t z) {
+__host__ __device__ inline uint64_t splitmix64(uint64_t z) {
     z += 0x9E3779B97F4A7C15ull;
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
     return z ^ (z >> 31);
 }
 
-uint32_t row_priority(uint32_t seed, int i) {
+__host__ __device__ inline uint32_t row_priority(uint32_t seed, int i) {
     return (uint32_t)(splitmix64(((uint64_t)seed << 32) | (uint32_t)i) >> 36);  // 28 bits
 }
 
-double row_sign(uint32_t seed, int i) {
+__host__ __device__ inline double row_sign(uint32_t seed, int i) {
     return (splitmix64(((uint64_t)(seed ^ 0xA5A5A5A5u) << 32) | (uint32_t)i) >> 63) ? -1.0 : 1.0;
 }
 
 // The packed comparison key of multigrid.py:122: state in bits 60-61, priority 32-59, index 0-31.
-inline int64_t mis_key(int state, uint32_t priority, int i) {
+__host__ __device__ inline int64_t mis_key(int state, uint32_t priority, int i) {
     return ((int64_t)state << 60) | ((int64_t)(priority & 0x0FFFFFFFu) << 32) | (int64_t)(uint32_t)i;
 }
 
-inline double inverse_or_one(double d) { return d != 0.0 ? 1.0 / d : 1.0; }
+__host__ __device__ inline double inverse_or_one(double d) { return d != 0.0 ? 1.0 / d : 1.0; }
 
 // Builds a CSR row by row: fn(i, entries) appends row i's (column, value) pairs already summed,
 // sorted and pruned. Rows are produced by host threads in contiguous chunks and concatenated.
@@ -537,20 +542,17 @@ struct HostHierarchy {
     bool usable = false;
 };
 
-void build_hierarchy(HCsr fine, uint32_t seed, HostHierarchy* H) {
-    H->jacobi.resize(fine.rows);
-    for (int i = 0; i < fine.rows; ++i) {
-        double d = 0.0;
-        for (int k = fine.off[i]; k < fine.off[i + 1]; ++k)
-            if (fine.col[k] == i) d += fine.val[k];
-        H->jacobi[i] = inverse_or_one(d);
-    }
-    std::vector<int> weights;
-    HCsr A = std::move(fine);
+void finish_hierarchy(HostHierarchy* H);
+
+// The hierarchy from level `first_level` on (levels before it were built elsewhere: on the
+// device), A that level's operator and `weights` its rows' aggregate sizes (empty on the finest
+// level); may_coarsen = false keeps A as the coarsest level.
+void build_hierarchy_from(HCsr A, uint32_t seed, std::vector<int> weights, int first_level, bool may_coarsen,
+                          HostHierarchy* H) {
     while (true) {
         H->levels.emplace_back();
         HostLevel& level = H->levels.back();
-        if (A.rows <= kMaxCoarse || (int)H->levels.size() >= kMaxLevels) {
+        if (!may_coarsen || A.rows <= kMaxCoarse || first_level + (int)H->levels.size() >= kMaxLevels) {
             level.A = std::move(A);
             break;
         }
@@ -574,6 +576,23 @@ void build_hierarchy(HCsr fine, uint32_t seed, HostHierarchy* H) {
         weights = std::move(G.sizes);
         A = std::move(coarse);
     }
+    finish_hierarchy(H);
+}
+
+void build_hierarchy(HCsr fine, uint32_t seed, HostHierarchy* H) {
+    H->jacobi.resize(fine.rows);
+    for (int i = 0; i < fine.rows; ++i) {
+        double d = 0.0;
+        for (int k = fine.off[i]; k < fine.off[i + 1]; ++k)
+            if (fine.col[k] == i) d += fine.val[k];
+        H->jacobi[i] = inverse_or_one(d);
+    }
+    build_hierarchy_from(std::move(fine), seed, {}, 0, true, H);
+}
+
+// The coarsest level's dense pseudo-inverse over its active rows (the hierarchy is usable only
+// with it).
+void finish_hierarchy(HostHierarchy* H) {
     const HCsr& last = H->levels.back().A;
     // A single level (an operator of <= 384 rows, or one whose first aggregation stalls) is solved
     // by its dense pseudo-inverse alone, as the reference's one-level cycle is.
@@ -597,6 +616,645 @@ void build_hierarchy(HCsr fine, uint32_t seed, HostHierarchy* H) {
     if (m > 0 && !symmetric_pseudo_inverse(dense, m, &H->inverse)) return;
     H->active = std::move(active);
     H->usable = true;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Device hierarchy: the levels of at least kDeviceLevelRows rows are built on the device, with the
+// host's arithmetic in the host's order (the same aggregates, prolongators and Galerkin operators
+// as build_hierarchy for the same seed); the smaller levels and the coarse pseudo-inverse follow
+// on the host from where the device stopped.
+// ---------------------------------------------------------------------------------------------
+
+constexpr int kDeviceLevelRows = 32768;
+
+struct DevCsr {
+    int rows = 0, cols = 0;
+    long long nnz = 0;
+    const int* off = nullptr;
+    const int* col = nullptr;
+    const double* val = nullptr;
+};
+
+struct DevLevel {
+    DevCsr A, P, R;               // P, R empty on the last level
+    const double* damped = nullptr;
+};
+
+struct DevBuild {
+    std::vector<DevLevel> levels;  // the last one is where the host takes over (its A only)
+    std::vector<int> weights;      // the last level's row weights (empty: the finest level)
+    bool stopped = false;          // the device loop itself ended the hierarchy at the last level
+    std::vector<void*> owned;      // pool allocations of the kept arrays
+};
+
+template <typename T>
+int keep_alloc(DevBuild* B, T** p, size_t n, cudaStream_t stream) {
+    void* q = nullptr;
+    OB_CUDA(pool_malloc(&q, sizeof(T) * std::max<size_t>(n, 1), stream));
+    B->owned.push_back(q);
+    *p = static_cast<T*>(q);
+    return OB_OK;
+}
+
+__device__ __forceinline__ bool strong_edge(int i, int j, double a, const double* __restrict__ scaled) {
+    return j != i && fabs(a) >= kTheta * scaled[i] * scaled[j];
+}
+
+__global__ void dev_setup_kernel(int n, const int* __restrict__ off, const int* __restrict__ col,
+                                 const double* __restrict__ val, uint32_t seed, double* __restrict__ l1,
+                                 double* __restrict__ scaled, uint32_t* __restrict__ priority, int* __restrict__ state) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d = 0.0, off_sum = 0.0;
+    for (int k = off[i]; k < off[i + 1]; ++k) {
+        if (col[k] == i) d += val[k];
+        else off_sum += fabs(val[k]);
+    }
+    const double l = fabs(d) + off_sum;
+    l1[i] = d < 0.0 ? -l : l;
+    scaled[i] = sqrt(fabs(d));
+    priority[i] = row_priority(seed, i);
+    state[i] = off_sum == 0.0 ? kExcluded : kUndecided;
+}
+
+__global__ void dev_mis_keys_kernel(int n, const int* __restrict__ off, const int* __restrict__ col,
+                                    const double* __restrict__ val, const double* __restrict__ scaled,
+                                    const int* __restrict__ state, const uint32_t* __restrict__ priority,
+                                    int64_t* __restrict__ key) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int64_t best = mis_key(state[i], priority[i], i);
+    for (int k = off[i]; k < off[i + 1]; ++k) {
+        const int j = col[k];
+        if (strong_edge(i, j, val[k], scaled)) best = max(best, mis_key(state[j], priority[j], j));
+    }
+    key[i] = best;
+}
+
+__global__ void dev_mis_decide_kernel(int n, const int* __restrict__ off, const int* __restrict__ col,
+                                      const double* __restrict__ val, const double* __restrict__ scaled,
+                                      const int* __restrict__ state, const uint32_t* __restrict__ priority,
+                                      const int64_t* __restrict__ key, int* __restrict__ next, int* undecided) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (state[i] != kUndecided) {
+        next[i] = state[i];
+        return;
+    }
+    int64_t best = key[i];
+    for (int k = off[i]; k < off[i + 1]; ++k) {
+        const int j = col[k];
+        if (strong_edge(i, j, val[k], scaled)) best = max(best, key[j]);
+    }
+    int verdict = kUndecided;
+    if ((int)(best >> 60) == kRoot) verdict = kExcluded;
+    else if (best == mis_key(kUndecided, priority[i], i)) verdict = kRoot;
+    next[i] = verdict;
+    if (verdict == kUndecided) atomicAdd(undecided, 1);
+}
+
+__global__ void dev_root_flags_kernel(int n, const int* __restrict__ state, int* __restrict__ flags) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flags[i] = state[i] != kExcluded ? 1 : 0;
+}
+
+__global__ void dev_first_labels_kernel(int n, const int* __restrict__ flags, const int* __restrict__ scan,
+                                        int* __restrict__ label) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) label[i] = flags[i] ? scan[i] : -1;
+}
+
+// One hop of the label spread over the strong graph, the largest label winning.
+__global__ void dev_spread_kernel(int n, const int* __restrict__ off, const int* __restrict__ col,
+                                  const double* __restrict__ val, const double* __restrict__ scaled,
+                                  const int* __restrict__ in, int* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int best = in[i];
+    if (best < 0)
+        for (int k = off[i]; k < off[i + 1]; ++k)
+            if (strong_edge(i, col[k], val[k], scaled)) best = max(best, in[col[k]]);
+    out[i] = best;
+}
+
+__global__ void dev_sizes_kernel(int n, const int* __restrict__ label, const int* __restrict__ weights,
+                                 int* __restrict__ sizes) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && label[i] >= 0) atomicAdd(&sizes[label[i]], weights ? weights[i] : 1);
+}
+
+__global__ void dev_signs_kernel(int n, uint32_t seed, double* __restrict__ x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = row_sign(seed, i);
+}
+
+__global__ void dev_power_kernel(int n, const int* __restrict__ off, const int* __restrict__ col,
+                                 const double* __restrict__ val, const double* __restrict__ l1,
+                                 const double* __restrict__ x, double* __restrict__ y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double t = 0.0;
+    for (int k = off[i]; k < off[i + 1]; ++k) t += val[k] * x[col[k]];
+    y[i] = inverse_or_one(l1[i]) * t;
+}
+
+__global__ void dev_damped_kernel(int n, const double* __restrict__ l1, double omega, double* __restrict__ damped) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) damped[i] = omega * inverse_or_one(l1[i]);
+}
+
+// Rows assembled from (column, value) contributions in slot order: FILL == false counts each row's
+// non-zero contributions (and, in raw, every contribution, for the key budget); FILL == true writes
+// them from the row's start as keys row * cols + col and values.
+
+// The prolongator's contributions (prolongator(): A's entries, then the row's own aggregate).
+template <bool FILL>
+__global__ void dev_prolongator_kernel(int n, int n_coarse, const int* __restrict__ off, const int* __restrict__ col,
+                                       const double* __restrict__ val, const int* __restrict__ label,
+                                       const int* __restrict__ weights, const int* __restrict__ sizes,
+                                       const double* __restrict__ damped, long long* __restrict__ count,
+                                       const long long* __restrict__ start, unsigned long long* __restrict__ keys,
+                                       double* __restrict__ values) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double scale = -damped[i];
+    const bool long_i = off[i + 1] - off[i] >= kLongRow;
+    long long c = 0, e = FILL ? start[i] : 0;
+    auto emit = [&](int a, double v) {
+        if (v == 0.0) return;
+        if (FILL) {
+            keys[e] = (unsigned long long)i * (unsigned long long)n_coarse + (unsigned long long)a;
+            values[e] = v;
+            ++e;
+        }
+        ++c;
+    };
+    for (int k = off[i]; k < off[i + 1]; ++k) {
+        const int j = col[k];
+        const int a = label[j];
+        const bool hub = j != i && (long_i || off[j + 1] - off[j] >= kLongRow);
+        if (a < 0 || hub) continue;
+        const double scale_j = weights ? sqrt((double)weights[j]) : 1.0;
+        emit(a, scale * val[k] * scale_j / sqrt((double)sizes[a]));
+    }
+    const int own = label[i];
+    if (own >= 0) emit(own, (weights ? sqrt((double)weights[i]) : 1.0) / sqrt((double)sizes[own]));
+    if (!FILL) count[i] = c;
+}
+
+// A B's contributions (galerkin()'s A P and R (A P)): row i, for each of its entries (j, a) in
+// order, B's row j in order, a * b.
+template <bool FILL>
+__global__ void dev_product_kernel(int n, int cols, const int* __restrict__ aoff, const int* __restrict__ acol,
+                                   const double* __restrict__ aval, const int* __restrict__ boff,
+                                   const int* __restrict__ bcol, const double* __restrict__ bval,
+                                   long long* __restrict__ count, long long* __restrict__ raw,
+                                   const long long* __restrict__ start, unsigned long long* __restrict__ keys,
+                                   double* __restrict__ values) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long long c = 0, all = 0, e = FILL ? start[i] : 0;
+    for (int k = aoff[i]; k < aoff[i + 1]; ++k) {
+        const int j = acol[k];
+        const double a = aval[k];
+        all += boff[j + 1] - boff[j];
+        for (int b = boff[j]; b < boff[j + 1]; ++b) {
+            const double v = a * bval[b];
+            if (v == 0.0) continue;
+            if (FILL) {
+                keys[e] = (unsigned long long)i * (unsigned long long)cols + (unsigned long long)bcol[b];
+                values[e] = v;
+                ++e;
+            }
+            ++c;
+        }
+    }
+    if (!FILL) {
+        count[i] = c;
+        raw[i] = all;
+    }
+}
+
+__global__ void dev_run_flags_kernel(long long total, const unsigned long long* __restrict__ keys, int* __restrict__ flags) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e < total) flags[e] = (e == 0 || keys[e] != keys[e - 1]) ? 1 : 0;
+}
+
+__global__ void dev_run_starts_kernel(long long total, const int* __restrict__ flags, const int* __restrict__ run,
+                                      long long* __restrict__ first) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e < total && flags[e]) first[run[e]] = e;
+}
+
+// Each run (one output entry): its contributions summed in sorted order (slot order: the sort is
+// stable), kept when the sum is not zero (sum_sorted()).
+__global__ void dev_run_sums_kernel(int runs, long long total, const long long* __restrict__ first,
+                                    const unsigned long long* __restrict__ keys, const int* __restrict__ perm,
+                                    const double* __restrict__ values, int cols, double* __restrict__ sum,
+                                    int* __restrict__ keep, int* __restrict__ row_count) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= runs) return;
+    const long long b = first[r], e = r + 1 < runs ? first[r + 1] : total;
+    double s = 0.0;
+    for (long long t = b; t < e; ++t) s += values[perm[t]];
+    sum[r] = s;
+    keep[r] = s != 0.0 ? 1 : 0;
+    if (s != 0.0) atomicAdd(&row_count[(int)(keys[b] / (unsigned long long)cols)], 1);
+}
+
+__global__ void dev_place_kernel(int runs, const long long* __restrict__ first, const unsigned long long* __restrict__ keys,
+                                 const double* __restrict__ sum, const int* __restrict__ keep,
+                                 const int* __restrict__ pos, int cols, int* __restrict__ col, double* __restrict__ val) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= runs || !keep[r]) return;
+    col[pos[r]] = (int)(keys[first[r]] % (unsigned long long)cols);
+    val[pos[r]] = sum[r];
+}
+
+__global__ void dev_entry_rows_kernel(int rows, const int* __restrict__ off, int* __restrict__ row) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    for (int k = off[i]; k < off[i + 1]; ++k) row[k] = i;
+}
+
+__global__ void dev_transpose_keys_kernel(long long nnz, const int* __restrict__ col, const int* __restrict__ row,
+                                          int rows, unsigned long long* __restrict__ keys, int* __restrict__ index,
+                                          int* __restrict__ count) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    keys[e] = (unsigned long long)col[e] * (unsigned long long)rows + (unsigned long long)row[e];
+    index[e] = (int)e;
+    atomicAdd(&count[col[e]], 1);
+}
+
+__global__ void dev_transpose_place_kernel(long long nnz, const unsigned long long* __restrict__ keys,
+                                           const int* __restrict__ index, const double* __restrict__ val, int rows,
+                                           int* __restrict__ tcol, double* __restrict__ tval) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    tcol[e] = (int)(keys[e] % (unsigned long long)rows);
+    tval[e] = val[index[e]];
+}
+
+__global__ void dev_iota_kernel(long long total, int* __restrict__ index) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e < total) index[e] = (int)e;
+}
+
+int bits_for(unsigned long long value) {
+    int bits = 1;
+    while (bits < 64 && (value >> bits) != 0) ++bits;
+    return bits;
+}
+
+int grid_of(long long n) { return (int)std::max(1LL, (n + kThreads - 1) / kThreads); }
+
+// Exclusive scan of n ints (or long longs) into out (n + 1 entries, the total last).
+template <typename T>
+int exclusive_scan(const T* in, T* out, int n, cudaStream_t stream) {
+    Scratch scratch(stream);
+    size_t bytes = 0;
+    OB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n + 1, stream));
+    void* temp = scratch.take<unsigned char>(bytes);
+    if (int st = scratch.commit()) return st;
+    // The scan covers n + 1 entries: the input's entry n must be 0 (callers allocate n + 1 zeroed
+    // at the end).
+    OB_CUDA(cub::DeviceScan::ExclusiveSum(temp, bytes, in, out, n + 1, stream));
+    return OB_OK;
+}
+
+template <typename T>
+T read_one(const T* p, cudaStream_t stream, int* status) {
+    T v{};
+    cudaError_t e = cudaMemcpyAsync(&v, p, sizeof(T), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) *status = cuda_status(e, "amg device build: read back");
+    return v;
+}
+
+// CSR rows x cols from per-row contributions: count (rows + 1, the last 0) is filled by the
+// counting pass; fill(start, keys, values) writes them. Contributions of one entry are summed in
+// their slot order (a stable radix sort over the key bits), exact-zero sums are dropped.
+template <typename Fill>
+int assemble(int rows, int cols, long long* count, Fill fill, DevBuild* B, DevCsr* out, cudaStream_t stream) {
+    int st = OB_OK;
+    Scratch scratch(stream);
+    long long* start = scratch.take<long long>((size_t)rows + 1);
+    if ((st = scratch.commit())) return st;
+    if ((st = exclusive_scan(count, start, rows, stream))) return st;
+    const long long total = read_one(start + rows, stream, &st);
+    if (st) return st;
+    OB_REQUIRE(total < (1LL << 31), "amg device build: %lld contributions past the index range", total);
+    int* row_off = nullptr;
+    if ((st = keep_alloc(B, &row_off, (size_t)rows + 1, stream))) return st;
+    int* col = nullptr;
+    double* val = nullptr;
+    if (total == 0) {
+        OB_CUDA(cudaMemsetAsync(row_off, 0, sizeof(int) * ((size_t)rows + 1), stream));
+        if ((st = keep_alloc(B, &col, 1, stream)) || (st = keep_alloc(B, &val, 1, stream))) return st;
+        *out = DevCsr{rows, cols, 0, row_off, col, val};
+        return OB_OK;
+    }
+    unsigned long long* keys = scratch.take<unsigned long long>((size_t)total);
+    unsigned long long* sorted = scratch.take<unsigned long long>((size_t)total);
+    double* values = scratch.take<double>((size_t)total);
+    int* index = scratch.take<int>((size_t)total);
+    int* perm = scratch.take<int>((size_t)total);
+    int* flags = scratch.take<int>((size_t)total + 1);
+    int* run = scratch.take<int>((size_t)total + 1);
+    if ((st = scratch.commit())) return st;
+    fill(start, keys, values);
+    OB_CHECK_LAUNCH("amg device build: contributions");
+    dev_iota_kernel<<<grid_of(total), kThreads, 0, stream>>>(total, index);
+    OB_CHECK_LAUNCH("amg device build: positions");
+    OB_CUDA(cudaMemsetAsync(flags + total, 0, sizeof(int), stream));
+    {
+        Scratch sort_scratch(stream);
+        size_t bytes = 0;
+        const int end_bit = bits_for((unsigned long long)rows * (unsigned long long)cols);
+        OB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys, sorted, index, perm, (int)total, 0, end_bit,
+                                                stream));
+        void* temp = sort_scratch.take<unsigned char>(bytes);
+        if ((st = sort_scratch.commit())) return st;
+        OB_CUDA(cub::DeviceRadixSort::SortPairs(temp, bytes, keys, sorted, index, perm, (int)total, 0, end_bit,
+                                                stream));
+    }
+    dev_run_flags_kernel<<<grid_of(total), kThreads, 0, stream>>>(total, sorted, flags);
+    OB_CHECK_LAUNCH("amg device build: run flags");
+    if ((st = exclusive_scan(flags, run, (int)total, stream))) return st;
+    const int runs = read_one(run + total, stream, &st);
+    if (st) return st;
+    long long* first = scratch.take<long long>((size_t)runs + 1);
+    double* sum = scratch.take<double>((size_t)runs + 1);
+    int* keep = scratch.take<int>((size_t)runs + 1);
+    int* pos = scratch.take<int>((size_t)runs + 1);
+    int* row_count = scratch.take<int>((size_t)rows + 1);
+    if ((st = scratch.commit())) return st;
+    dev_run_starts_kernel<<<grid_of(total), kThreads, 0, stream>>>(total, flags, run, first);
+    OB_CHECK_LAUNCH("amg device build: run starts");
+    OB_CUDA(cudaMemsetAsync(row_count, 0, sizeof(int) * ((size_t)rows + 1), stream));
+    OB_CUDA(cudaMemsetAsync(keep + runs, 0, sizeof(int), stream));
+    dev_run_sums_kernel<<<grid_of(runs), kThreads, 0, stream>>>(runs, total, first, sorted, perm, values, cols, sum,
+                                                                keep, row_count);
+    OB_CHECK_LAUNCH("amg device build: run sums");
+    if ((st = exclusive_scan(row_count, row_off, rows, stream))) return st;
+    if ((st = exclusive_scan(keep, pos, runs, stream))) return st;
+    const int kept = read_one(pos + runs, stream, &st);
+    if (st) return st;
+    if ((st = keep_alloc(B, &col, (size_t)kept, stream)) || (st = keep_alloc(B, &val, (size_t)kept, stream))) return st;
+    dev_place_kernel<<<grid_of(runs), kThreads, 0, stream>>>(runs, first, sorted, sum, keep, pos, cols, col, val);
+    OB_CHECK_LAUNCH("amg device build: place");
+    *out = DevCsr{rows, cols, kept, row_off, col, val};
+    return OB_OK;
+}
+
+// The transpose of a device CSR (rows x cols) in row order within each column (transpose()).
+int transpose_device(const DevCsr& M, DevBuild* B, DevCsr* out, cudaStream_t stream) {
+    int st = OB_OK;
+    Scratch scratch(stream);
+    const long long nnz = M.nnz;
+    int* row = scratch.take<int>((size_t)std::max(nnz, 1LL));
+    unsigned long long* keys = scratch.take<unsigned long long>((size_t)std::max(nnz, 1LL));
+    unsigned long long* sorted = scratch.take<unsigned long long>((size_t)std::max(nnz, 1LL));
+    int* index = scratch.take<int>((size_t)std::max(nnz, 1LL));
+    int* perm = scratch.take<int>((size_t)std::max(nnz, 1LL));
+    int* count = scratch.take<int>((size_t)M.cols + 1);
+    if ((st = scratch.commit())) return st;
+    int *off = nullptr, *col = nullptr;
+    double* val = nullptr;
+    if ((st = keep_alloc(B, &off, (size_t)M.cols + 1, stream)) || (st = keep_alloc(B, &col, (size_t)nnz, stream)) ||
+        (st = keep_alloc(B, &val, (size_t)nnz, stream)))
+        return st;
+    OB_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * ((size_t)M.cols + 1), stream));
+    if (nnz > 0) {
+        dev_entry_rows_kernel<<<grid_of(M.rows), kThreads, 0, stream>>>(M.rows, M.off, row);
+        OB_CHECK_LAUNCH("amg device build: entry rows");
+        dev_transpose_keys_kernel<<<grid_of(nnz), kThreads, 0, stream>>>(nnz, M.col, row, M.rows, keys, index, count);
+        OB_CHECK_LAUNCH("amg device build: transpose keys");
+        Scratch sort_scratch(stream);
+        size_t bytes = 0;
+        const int end_bit = bits_for((unsigned long long)M.cols * (unsigned long long)M.rows);
+        OB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys, sorted, index, perm, (int)nnz, 0, end_bit,
+                                                stream));
+        void* temp = sort_scratch.take<unsigned char>(bytes);
+        if ((st = sort_scratch.commit())) return st;
+        OB_CUDA(cub::DeviceRadixSort::SortPairs(temp, bytes, keys, sorted, index, perm, (int)nnz, 0, end_bit, stream));
+        dev_transpose_place_kernel<<<grid_of(nnz), kThreads, 0, stream>>>(nnz, sorted, perm, M.val, M.rows, col, val);
+        OB_CHECK_LAUNCH("amg device build: transpose place");
+    }
+    if ((st = exclusive_scan(count, off, M.cols, stream))) return st;
+    *out = DevCsr{M.cols, M.rows, nnz, off, col, val};
+    return OB_OK;
+}
+
+// Levels of the hierarchy of the n x n operator (device CSR, float64) built on the device while
+// a level has at least min_rows rows (and the host's stopping rules do not end it): aggregate()
+// (strength, MIS-2 rounds, two hops of the label spread, aggregate sizes), damped_diagonal() (the
+// power steps on the device, the growth summed on the host in row order), prolongator(),
+// transpose() and galerkin(), each level's arithmetic as the host's.
+int build_device_levels(const DevCsr& fine, uint32_t seed, int min_rows, DevBuild* B, cudaStream_t stream) {
+    int st = OB_OK;
+    DevCsr A = fine;
+    const int* weights = nullptr;  // device, the current level's row weights (null: every row 1)
+    std::vector<int> host_weights;
+    while (true) {
+        const int n = A.rows;
+        if (n < min_rows || n <= kMaxCoarse || (int)B->levels.size() + 1 >= kMaxLevels) {
+            // Below min_rows the host takes over (it stops at once where the rules end here).
+            B->stopped = n <= kMaxCoarse || (int)B->levels.size() + 1 >= kMaxLevels;
+            B->levels.push_back(DevLevel{A});
+            break;
+        }
+        Scratch scratch(stream);
+        double* l1 = scratch.take<double>(n);
+        double* scaled = scratch.take<double>(n);
+        uint32_t* priority = scratch.take<uint32_t>(n);
+        int* state = scratch.take<int>(n);
+        int* next = scratch.take<int>(n);
+        int64_t* key = scratch.take<int64_t>(n);
+        int* undecided = scratch.take<int>(1);
+        int* flags = scratch.take<int>((size_t)n + 1);
+        int* scan = scratch.take<int>((size_t)n + 1);
+        int* label0 = scratch.take<int>(n);
+        int* hop = scratch.take<int>(n);
+        double* x = scratch.take<double>(n);
+        double* y = scratch.take<double>(n);
+        long long* count = scratch.take<long long>((size_t)n + 1);
+        long long* raw = scratch.take<long long>((size_t)n + 1);
+        if ((st = scratch.commit())) return st;
+        int* label = nullptr;
+        double* damped = nullptr;
+        if ((st = keep_alloc(B, &label, n, stream)) || (st = keep_alloc(B, &damped, n, stream))) return st;
+        const int grid = grid_of(n);
+        dev_setup_kernel<<<grid, kThreads, 0, stream>>>(n, A.off, A.col, A.val, seed, l1, scaled, priority, state);
+        OB_CHECK_LAUNCH("amg device build: setup");
+        for (int round = 0; round < kMisRounds; ++round) {
+            OB_CUDA(cudaMemsetAsync(undecided, 0, sizeof(int), stream));
+            dev_mis_keys_kernel<<<grid, kThreads, 0, stream>>>(n, A.off, A.col, A.val, scaled, state, priority, key);
+            OB_CHECK_LAUNCH("amg device build: MIS keys");
+            dev_mis_decide_kernel<<<grid, kThreads, 0, stream>>>(n, A.off, A.col, A.val, scaled, state, priority, key,
+                                                                  next, undecided);
+            OB_CHECK_LAUNCH("amg device build: MIS decide");
+            std::swap(state, next);
+            const int left = read_one(undecided, stream, &st);
+            if (st) return st;
+            if (left == 0) break;
+        }
+        OB_CUDA(cudaMemsetAsync(flags + n, 0, sizeof(int), stream));
+        dev_root_flags_kernel<<<grid, kThreads, 0, stream>>>(n, state, flags);
+        OB_CHECK_LAUNCH("amg device build: root flags");
+        if ((st = exclusive_scan(flags, scan, n, stream))) return st;
+        const int n_aggregates = read_one(scan + n, stream, &st);
+        if (st) return st;
+        if (n_aggregates == 0 || n_aggregates >= kMinCoarsening * n) {
+            B->stopped = true;
+            B->levels.push_back(DevLevel{A});
+            break;
+        }
+        dev_first_labels_kernel<<<grid, kThreads, 0, stream>>>(n, flags, scan, label0);
+        dev_spread_kernel<<<grid, kThreads, 0, stream>>>(n, A.off, A.col, A.val, scaled, label0, hop);
+        dev_spread_kernel<<<grid, kThreads, 0, stream>>>(n, A.off, A.col, A.val, scaled, hop, label);
+        OB_CHECK_LAUNCH("amg device build: labels");
+        int* sizes = nullptr;
+        if ((st = keep_alloc(B, &sizes, n_aggregates, stream))) return st;
+        OB_CUDA(cudaMemsetAsync(sizes, 0, sizeof(int) * n_aggregates, stream));
+        dev_sizes_kernel<<<grid, kThreads, 0, stream>>>(n, label, weights, sizes);
+        OB_CHECK_LAUNCH("amg device build: sizes");
+        // omega from the power steps' growth, summed on the host in row order.
+        dev_signs_kernel<<<grid, kThreads, 0, stream>>>(n, seed, x);
+        for (int step = 0; step < kPowerSteps; ++step) {
+            dev_power_kernel<<<grid, kThreads, 0, stream>>>(n, A.off, A.col, A.val, l1, x, y);
+            std::swap(x, y);
+        }
+        OB_CHECK_LAUNCH("amg device build: power steps");
+        std::vector<double> host_x(n);
+        OB_CUDA(cudaMemcpyAsync(host_x.data(), x, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+        OB_CUDA(cudaStreamSynchronize(stream));
+        double growth = 0.0;
+        for (int i = 0; i < n; ++i) growth += host_x[i] * host_x[i];
+        double rho = 1.0;
+        if (growth > 0.0 && std::isfinite(growth)) rho = std::pow(std::sqrt(growth / (double)n), 1.0 / kPowerSteps);
+        dev_damped_kernel<<<grid, kThreads, 0, stream>>>(n, l1, kJacobiFactor / rho, damped);
+        OB_CHECK_LAUNCH("amg device build: damped diagonal");
+        // P, R = P^T, then A P and R (A P).
+        DevCsr P, R, AP, coarse;
+        OB_CUDA(cudaMemsetAsync(count + n, 0, sizeof(long long), stream));
+        dev_prolongator_kernel<false><<<grid, kThreads, 0, stream>>>(n, n_aggregates, A.off, A.col, A.val, label,
+                                                                     weights, sizes, damped, count, nullptr, nullptr,
+                                                                     nullptr);
+        OB_CHECK_LAUNCH("amg device build: prolongator counts");
+        st = assemble(n, n_aggregates, count,
+                      [&](const long long* start, unsigned long long* keys, double* values) {
+                          dev_prolongator_kernel<true><<<grid, kThreads, 0, stream>>>(
+                              n, n_aggregates, A.off, A.col, A.val, label, weights, sizes, damped, nullptr, start, keys,
+                              values);
+                      },
+                      B, &P, stream);
+        if (st || (st = transpose_device(P, B, &R, stream))) return st;
+        // galerkin(): the key budget of each product (every contribution counted) against the
+        // fallback's cap.
+        const long long budget = kTripletFactor * (A.nnz + n);
+        const bool capped = (long long)n * n_aggregates > kDenseOutputCap;
+        Scratch sums(stream);
+        long long* total = sums.take<long long>(1);
+        size_t reduce_bytes = 0;
+        OB_CUDA(cub::DeviceReduce::Sum(nullptr, reduce_bytes, raw, total, n, stream));
+        void* reduce_temp = sums.take<unsigned char>(reduce_bytes);
+        if ((st = sums.commit())) return st;
+        OB_CUDA(cudaMemsetAsync(count + n, 0, sizeof(long long), stream));
+        dev_product_kernel<false><<<grid, kThreads, 0, stream>>>(n, n_aggregates, A.off, A.col, A.val, P.off, P.col,
+                                                                 P.val, count, raw, nullptr, nullptr, nullptr);
+        OB_CHECK_LAUNCH("amg device build: A P counts");
+        OB_CUDA(cub::DeviceReduce::Sum(reduce_temp, reduce_bytes, raw, total, n, stream));
+        const long long ap_contributions = read_one(total, stream, &st);
+        if (st) return st;
+        if (ap_contributions > budget && capped) {
+            B->stopped = true;
+            B->levels.push_back(DevLevel{A});
+            break;
+        }
+        st = assemble(n, n_aggregates, count,
+                      [&](const long long* start, unsigned long long* keys, double* values) {
+                          dev_product_kernel<true><<<grid, kThreads, 0, stream>>>(
+                              n, n_aggregates, A.off, A.col, A.val, P.off, P.col, P.val, nullptr, nullptr, start, keys,
+                              values);
+                      },
+                      B, &AP, stream);
+        if (st) return st;
+        const int nc = n_aggregates;
+        Scratch rap(stream);
+        long long* ccount = rap.take<long long>((size_t)nc + 1);
+        long long* craw = rap.take<long long>((size_t)nc + 1);
+        size_t cbytes = 0;
+        OB_CUDA(cub::DeviceReduce::Sum(nullptr, cbytes, craw, total, nc, stream));
+        void* ctemp = rap.take<unsigned char>(cbytes);
+        if ((st = rap.commit())) return st;
+        OB_CUDA(cudaMemsetAsync(ccount + nc, 0, sizeof(long long), stream));
+        dev_product_kernel<false><<<grid_of(nc), kThreads, 0, stream>>>(nc, nc, R.off, R.col, R.val, AP.off, AP.col,
+                                                                        AP.val, ccount, craw, nullptr, nullptr, nullptr);
+        OB_CHECK_LAUNCH("amg device build: R A P counts");
+        OB_CUDA(cub::DeviceReduce::Sum(ctemp, cbytes, craw, total, nc, stream));
+        const long long rap_contributions = read_one(total, stream, &st);
+        if (st) return st;
+        if (rap_contributions > budget && capped) {
+            B->stopped = true;
+            B->levels.push_back(DevLevel{A});
+            break;
+        }
+        st = assemble(nc, nc, ccount,
+                      [&](const long long* start, unsigned long long* keys, double* values) {
+                          dev_product_kernel<true><<<grid_of(nc), kThreads, 0, stream>>>(
+                              nc, nc, R.off, R.col, R.val, AP.off, AP.col, AP.val, nullptr, nullptr, start, keys,
+                              values);
+                      },
+                      B, &coarse, stream);
+        if (st) return st;
+        B->levels.push_back(DevLevel{A, P, R, damped});
+        weights = sizes;
+        host_weights.assign(nc, 0);
+        OB_CUDA(cudaMemcpyAsync(host_weights.data(), sizes, sizeof(int) * nc, cudaMemcpyDeviceToHost, stream));
+        OB_CUDA(cudaStreamSynchronize(stream));
+        A = coarse;
+    }
+    B->weights = std::move(host_weights);
+    return OB_OK;
+}
+
+void release_build(DevBuild* B) {
+    for (void* p : B->owned) cudaFree(p);
+    B->owned.clear();
+}
+
+__global__ void dev_narrow_kernel(long long n, const double* __restrict__ in, float* __restrict__ out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (float)in[i];
+}
+
+__global__ void dev_jacobi_kernel(int n, const int* __restrict__ off, const int* __restrict__ col,
+                                  const double* __restrict__ val, float* __restrict__ jacobi) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d = 0.0;
+    for (int k = off[i]; k < off[i + 1]; ++k)
+        if (col[k] == i) d += val[k];
+    jacobi[i] = (float)inverse_or_one(d);
+}
+
+HCsr download(const DevCsr& M, cudaStream_t stream, int* status) {
+    HCsr H;
+    H.rows = M.rows;
+    H.cols = M.cols;
+    H.off.resize((size_t)M.rows + 1);
+    H.col.resize((size_t)M.nnz);
+    H.val.resize((size_t)M.nnz);
+    cudaError_t e = cudaMemcpyAsync(H.off.data(), M.off, sizeof(int) * H.off.size(), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess && M.nnz)
+        e = cudaMemcpyAsync(H.col.data(), M.col, sizeof(int) * (size_t)M.nnz, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess && M.nnz)
+        e = cudaMemcpyAsync(H.val.data(), M.val, sizeof(double) * (size_t)M.nnz, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) *status = cuda_status(e, "amg device build: download");
+    return H;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1443,11 +2101,140 @@ using namespace ob;
 
 extern "C" {
 
+// The hierarchy of a large operator: its levels of at least kDeviceLevelRows rows built on the
+// device (build_device_levels), the rest on the host from the level the device handed over.
+// Where the large levels of a hierarchy are built (ob_amg_build_mode): 1 the device (default),
+// 0 the host (the comparison of the two).
+std::atomic<int> g_build_on_device{1};
+bool amg_build_on_device() { return g_build_on_device.load() != 0; }
+
+int setup_on_device(Amg* M, int n, long long nnz, const int32_t* offsets, const int32_t* columns,
+                    const double* values, unsigned seed, cudaStream_t stream) {
+    DevBuild B;
+    int st = build_device_levels(DevCsr{n, n, nnz, offsets, columns, values}, seed, kDeviceLevelRows, &B, stream);
+    // Whatever the build kept is the handle's from here (released with it).
+    M->allocations.insert(M->allocations.end(), B.owned.begin(), B.owned.end());
+    B.owned.clear();
+    if (st) return st;
+    void* p = nullptr;
+    OB_CUDA(cudaMalloc(&p, sizeof(float) * (size_t)n));
+    M->allocations.push_back(p);
+    M->jacobi = static_cast<float*>(p);
+    dev_jacobi_kernel<<<grid_of(n), kThreads, 0, stream>>>(n, offsets, columns, values, M->jacobi);
+    OB_CHECK_LAUNCH("amg jacobi");
+    // The host's part, from the last device level on.
+    const int device_levels = (int)B.levels.size() - 1;
+    HCsr handover = download(B.levels.back().A, stream, &st);
+    if (st) return st;
+    HostHierarchy H;
+    build_hierarchy_from(std::move(handover), seed, B.weights, device_levels, !B.stopped, &H);
+    M->usable = H.usable;
+    if (!H.usable) {
+        // The Jacobi preconditioner in its place: level 0 only, as the host build leaves it.
+        M->levels.resize(1);
+        DeviceLevel& d = M->levels[0];
+        d.n = n;
+        d.nnz = nnz;
+        d.off = const_cast<int*>(offsets);
+        d.col = const_cast<int*>(columns);
+        OB_CUDA(cudaMalloc(&p, sizeof(float) * (size_t)std::max(nnz, 1LL)));
+        M->allocations.push_back(p);
+        d.val = static_cast<float*>(p);
+        dev_narrow_kernel<<<grid_of(nnz), kThreads, 0, stream>>>(nnz, values, d.val);
+        OB_CHECK_LAUNCH("amg narrow");
+        OB_CUDA(cudaStreamSynchronize(stream));
+        return OB_OK;
+    }
+    M->levels.resize((size_t)device_levels + H.levels.size());
+    auto narrow_to = [&](const double* in, long long count, float** out) -> int {
+        void* q = nullptr;
+        OB_CUDA(cudaMalloc(&q, sizeof(float) * (size_t)std::max(count, 1LL)));
+        M->allocations.push_back(q);
+        *out = static_cast<float*>(q);
+        if (count > 0) {
+            dev_narrow_kernel<<<grid_of(count), kThreads, 0, stream>>>(count, in, *out);
+            OB_CHECK_LAUNCH("amg narrow");
+        }
+        return OB_OK;
+    };
+    for (int l = 0; l < device_levels && st == OB_OK; ++l) {
+        const DevLevel& g = B.levels[l];
+        DeviceLevel& d = M->levels[l];
+        d.n = g.A.rows;
+        d.nnz = g.A.nnz;
+        d.off = const_cast<int*>(g.A.off);
+        d.col = const_cast<int*>(g.A.col);
+        d.n_coarse = g.P.cols;
+        d.pnnz = g.P.nnz;
+        d.rnnz = g.R.nnz;
+        d.poff = const_cast<int*>(g.P.off);
+        d.pcol = const_cast<int*>(g.P.col);
+        d.roff = const_cast<int*>(g.R.off);
+        d.rcol = const_cast<int*>(g.R.col);
+        if ((st = narrow_to(g.A.val, g.A.nnz, &d.val)) || (st = narrow_to(g.damped, g.A.rows, &d.damped)) ||
+            (st = narrow_to(g.P.val, g.P.nnz, &d.pval)) || (st = narrow_to(g.R.val, g.R.nnz, &d.rval)))
+            break;
+    }
+    for (size_t h = 0; h < H.levels.size() && st == OB_OK; ++h) {
+        HostLevel& hl = H.levels[h];
+        DeviceLevel& d = M->levels[(size_t)device_levels + h];
+        d.n = hl.A.rows;
+        d.nnz = hl.A.nnz();
+        if ((st = upload(M, hl.A.off, &d.off, stream)) || (st = upload(M, hl.A.col, &d.col, stream)) ||
+            (st = upload(M, narrow(hl.A.val), &d.val, stream)))
+            break;
+        if (!hl.damped.empty()) {
+            d.n_coarse = hl.P.cols;
+            d.pnnz = hl.P.nnz();
+            d.rnnz = hl.R.nnz();
+            if ((st = upload(M, narrow(hl.damped), &d.damped, stream)) || (st = upload(M, hl.P.off, &d.poff, stream)) ||
+                (st = upload(M, hl.P.col, &d.pcol, stream)) || (st = upload(M, narrow(hl.P.val), &d.pval, stream)) ||
+                (st = upload(M, hl.R.off, &d.roff, stream)) || (st = upload(M, hl.R.col, &d.rcol, stream)) ||
+                (st = upload(M, narrow(hl.R.val), &d.rval, stream)))
+                break;
+        }
+    }
+    if (st) return st;
+    const int rows = H.levels.back().A.rows;
+    M->coarse_rows = rows;
+    M->n_active = (int)H.active.size();
+    std::vector<int> slots(rows + std::max<size_t>(H.active.size(), 1), -1);
+    for (size_t t = 0; t < H.active.size(); ++t) {
+        slots[H.active[t]] = (int)t;
+        slots[rows + t] = H.active[t];
+    }
+    if ((st = upload(M, slots, &M->slots, stream))) return st;
+    if ((st = upload(M, narrow(H.inverse.empty() ? std::vector<double>(1, 0.0) : H.inverse), &M->inverse, stream)))
+        return st;
+    OB_CUDA(cudaStreamSynchronize(stream));
+    return OB_OK;
+}
+
 int ob_amg_setup(int n, const int32_t* offsets, const int32_t* columns, const double* values, unsigned seed,
                  void** amg, ob_stream_t stream_) {
     cudaStream_t stream = as_stream(stream_);
     OB_REQUIRE(n >= 1 && offsets && columns && values && amg, "ob_amg_setup: bad argument");
     *amg = nullptr;
+    if (n >= kDeviceLevelRows && amg_build_on_device()) {
+        int nnz_host = 0;
+        OB_CUDA(cudaMemcpyAsync(&nnz_host, offsets + n, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        OB_CUDA(cudaStreamSynchronize(stream));
+        OB_REQUIRE(nnz_host >= 0, "ob_amg_setup: bad offsets");
+        auto M = std::make_unique<Amg>();
+        M->n = n;
+        M->nnz = nnz_host;
+        M->off64 = offsets;
+        M->col64 = columns;
+        M->val64 = values;
+        int st = setup_on_device(M.get(), n, nnz_host, offsets, columns, values, seed, stream);
+        if (st) {
+            cudaStreamSynchronize(stream);
+            release(M.get());
+            return st;
+        }
+        *amg = M.release();
+        return OB_OK;
+    }
     HCsr fine;
     fine.rows = fine.cols = n;
     fine.off.resize(n + 1);
@@ -1520,6 +2307,11 @@ int ob_amg_setup(int n, const int32_t* offsets, const int32_t* columns, const do
         return st;
     }
     *amg = M.release();
+    return OB_OK;
+}
+
+int ob_amg_build_mode(int on_device) {
+    g_build_on_device.store(on_device != 0);
     return OB_OK;
 }
 

@@ -57,7 +57,8 @@ class MultigridPreconditioner(Preconditioner):
 
     The hierarchy (strength 0.05, distance-2 aggregation, l1-Jacobi smoothing with the damping from
     a power iteration, smoothed prolongation, Galerkin coarse operators, a dense pseudo-inverse at
-    <= 384 rows) is built once on the host (``ob_amg_setup``) and held on the device in float32.
+    <= 384 rows) is built once (``ob_amg_setup``: its levels of 32 768 rows or more on the device,
+    the rest on the host) and held on the device in float32.
     An operator that does not coarsen gets a Jacobi preconditioner in its place, as the reference
     returns one (ordito/linalg.py:5118-5119); ``grid`` then has a single level. ``matvec(x, y, z,
     1, 0)`` applies one cycle, ``z = M x``; other ``alpha``/``beta`` raise ``ValueError``.
@@ -84,6 +85,13 @@ class MultigridPreconditioner(Preconditioner):
         nnz = (ctypes.c_longlong * levels)()
         _lib.call("ob_amg_levels", self.handle, rows, nnz, levels)
         return [int(r) for r in rows]
+
+    @property
+    def stored_entries(self) -> int:
+        """Stored entries of every level's operator together."""
+        info = (ctypes.c_longlong * 4)()
+        _lib.call("ob_amg_info", self.handle, info)
+        return int(info[3])
 
     @property
     def is_jacobi(self) -> bool:

@@ -180,3 +180,39 @@ def test_time_kernels_reports_each_vcycle_kernel(gpu) -> None:
                       preconditioner=cycle)
     A = ops.poisson_system.to_scipy()
     assert np.linalg.norm(A @ x.numpy() - rhs) <= 1e-6 * np.linalg.norm(rhs)
+
+
+@pytest.mark.parametrize("name", ["torus", "sphere"])
+def test_device_hierarchy_matches_the_host_build(gpu, name: str) -> None:
+    """The levels of 32 768 rows or more built on the device (ob_amg_build_mode(1), the default)
+    against the whole build on host threads, same seed: the same aggregates (level sizes and
+    stored entries), and the same mixed-precision solve to its refinement's tolerance."""
+    import ctypes
+
+    from ordito_b200 import _lib
+
+    if name == "torus":
+        v, f = creation.jittered_torus(512, 256, seed=0)
+    else:
+        v, f = creation.icosphere(7)
+    ops = _operators(v, f)
+    n = v.shape[0]
+    rng = np.random.default_rng(6)
+    b = rng.normal(size=n)
+    b -= b.mean()
+    shapes, answers = [], []
+    try:
+        for mode in (0, 1):
+            _lib.call("ob_amg_build_mode", mode)
+            cycle = glinalg.multigrid_preconditioner(ops.poisson_system)
+            shapes.append(list(cycle.grid) + [cycle.stored_entries])
+            x = DeviceArray.zeros(n, np.float64)
+            glinalg.solve_spd(ops.poisson_system, b, x, tol=SOLVE_TOL, preconditioner=cycle)
+            answers.append(x.numpy())
+            cycle.close()
+    finally:
+        _lib.call("ob_amg_build_mode", 1)
+    assert shapes[0] == shapes[1]
+    assert len(shapes[0]) >= 4  # at least two device levels on these meshes
+    got, ref = answers[1] - answers[1].mean(), answers[0] - answers[0].mean()
+    assert hp.relative_linf(got, ref) <= 1e-8
