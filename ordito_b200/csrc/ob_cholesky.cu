@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <numeric>
 #include <thread>
 #include <vector>
@@ -45,12 +46,21 @@ struct Dissector {
     const std::vector<int>& col;
     const float* xyz;  // may be null: breadth-first level bisection instead
     int leaf_size;
-    std::vector<int> side;  // scratch marks per vertex
+    // Marks per vertex: a separator search stamps one side's vertices with its own number, so
+    // subtrees dissected on different host threads (disjoint vertex sets) never see each other's
+    // marks; the breadth-first bisection (no positions) runs on one thread with 1 / 2 marks.
+    std::unique_ptr<std::atomic<int>[]> side;
+    std::atomic<int> stamps{3};
     std::vector<Node> tree;  // built in postorder
     std::vector<int> order;  // new -> old, filled in postorder
 
     Dissector(const std::vector<int>& o, const std::vector<int>& c, const float* p, int n, int leaf)
-        : off(o), col(c), xyz(p), leaf_size(leaf), side(n, 0) {}
+        : off(o), col(c), xyz(p), leaf_size(leaf), side(new std::atomic<int>[std::max(n, 1)]) {
+        for (int v = 0; v < n; ++v) side[v].store(0, std::memory_order_relaxed);
+    }
+
+    int mark(int v) const { return side[v].load(std::memory_order_relaxed); }
+    void set(int v, int value) { side[v].store(value, std::memory_order_relaxed); }
 
     // Splits `verts` into (a, b) halves: by the median of the widest coordinate, or by BFS levels.
     void bisect(std::vector<int>& verts, std::vector<int>& a, std::vector<int>& b) {
@@ -70,67 +80,98 @@ struct Dissector {
                              [&](int x, int y) { return key(x) < key(y); });
         } else {
             // Breadth-first order from the first vertex; the first half of the visit is `a`.
-            for (int v : verts) side[v] = 1;
+            for (int v : verts) set(v, 1);
             std::vector<int> queue;
             queue.reserve(verts.size());
             std::vector<int> visited;
             for (int seed : verts) {
-                if (side[seed] != 1) continue;
-                side[seed] = 2;
+                if (mark(seed) != 1) continue;
+                set(seed, 2);
                 queue.push_back(seed);
                 for (size_t h = visited.size(); h < queue.size(); ++h) {
                     const int v = queue[h];
                     for (int e = off[v]; e < off[v + 1]; ++e)
-                        if (side[col[e]] == 1) {
-                            side[col[e]] = 2;
+                        if (mark(col[e]) == 1) {
+                            set(col[e], 2);
                             queue.push_back(col[e]);
                         }
                 }
                 visited = queue;
             }
-            for (int v : verts) side[v] = 0;
+            for (int v : verts) set(v, 0);
             verts = queue;
         }
         a.assign(verts.begin(), verts.begin() + half);
         b.assign(verts.begin() + half, verts.end());
     }
 
-    // Returns the index of the node built for `verts` (postorder append).
-    int dissect(std::vector<int> verts) {
+    // Subtrees of at least this many vertices, down to this depth, are dissected on a thread of
+    // their own (geometric bisection only); the tree and the ordering are the same as one
+    // thread's: each subtree is built into its own lists and appended in postorder.
+    static constexpr int kParallelDepth = 4;
+    static constexpr size_t kParallelVertices = 8192;
+
+    // Builds the subtree of `verts` into `tree` / `order` (postorder, indices within the lists);
+    // returns its root's index.
+    int dissect(std::vector<int> verts, std::vector<Node>& tree_out, std::vector<int>& order_out, int depth) {
         if ((int)verts.size() <= leaf_size) {
             std::sort(verts.begin(), verts.end());
             Node leaf;
-            leaf.start = (int)order.size();
+            leaf.start = (int)order_out.size();
             leaf.count = (int)verts.size();
-            order.insert(order.end(), verts.begin(), verts.end());
-            tree.push_back(leaf);
-            return (int)tree.size() - 1;
+            order_out.insert(order_out.end(), verts.begin(), verts.end());
+            tree_out.push_back(leaf);
+            return (int)tree_out.size() - 1;
         }
         std::vector<int> a, b;
         bisect(verts, a, b);
         // One-sided separator: the vertices of the smaller-boundary side adjacent to the other.
-        for (int v : b) side[v] = 2;
+        const int stamp = stamps.fetch_add(1);
+        for (int v : b) set(v, stamp);
         std::vector<int> sep, rest_a;
         for (int v : a) {
             bool cut = false;
-            for (int e = off[v]; e < off[v + 1] && !cut; ++e) cut = side[col[e]] == 2;
+            for (int e = off[v]; e < off[v + 1] && !cut; ++e) cut = mark(col[e]) == stamp;
             (cut ? sep : rest_a).push_back(v);
         }
-        for (int v : b) side[v] = 0;
         std::vector<int> children;
-        if (!rest_a.empty()) children.push_back(dissect(std::move(rest_a)));
-        if (!b.empty()) children.push_back(dissect(std::move(b)));
+        const bool parallel = xyz != nullptr && depth < kParallelDepth && !rest_a.empty() && !b.empty() &&
+                              std::min(rest_a.size(), b.size()) >= kParallelVertices;
+        if (parallel) {
+            std::vector<Node> tree_a, tree_b;
+            std::vector<int> order_a, order_b;
+            std::thread worker([&]() { dissect(std::move(rest_a), tree_a, order_a, depth + 1); });
+            dissect(std::move(b), tree_b, order_b, depth + 1);
+            worker.join();
+            for (auto* piece : {&tree_a, &tree_b}) {
+                const auto& order_piece = piece == &tree_a ? order_a : order_b;
+                const int node_shift = (int)tree_out.size(), start_shift = (int)order_out.size();
+                for (Node nd : *piece) {
+                    nd.start += start_shift;
+                    for (int& c : nd.children) c += node_shift;
+                    if (nd.parent >= 0) nd.parent += node_shift;
+                    tree_out.push_back(std::move(nd));
+                }
+                order_out.insert(order_out.end(), order_piece.begin(), order_piece.end());
+                children.push_back((int)tree_out.size() - 1);
+            }
+        } else {
+            if (!rest_a.empty()) children.push_back(dissect(std::move(rest_a), tree_out, order_out, depth + 1));
+            if (!b.empty()) children.push_back(dissect(std::move(b), tree_out, order_out, depth + 1));
+        }
         std::sort(sep.begin(), sep.end());
         Node node;
-        node.start = (int)order.size();
+        node.start = (int)order_out.size();
         node.count = (int)sep.size();
         node.children = children;
-        order.insert(order.end(), sep.begin(), sep.end());
-        tree.push_back(node);
-        const int id = (int)tree.size() - 1;
-        for (int c : children) tree[c].parent = id;
+        order_out.insert(order_out.end(), sep.begin(), sep.end());
+        tree_out.push_back(node);
+        const int id = (int)tree_out.size() - 1;
+        for (int c : children) tree_out[c].parent = id;
         return id;
     }
+
+    int dissect(std::vector<int> verts) { return dissect(std::move(verts), tree, order, 0); }
 };
 
 // Symbolic analysis of a dissection: each node's off-diagonal rows are its columns' later
