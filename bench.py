@@ -56,7 +56,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--cols", type=int, default=512)
     p.add_argument("--rows", type=int, default=256)
     p.add_argument("--refine", type=int, default=0)
-    p.add_argument("--in-flight", type=int, default=3, choices=[1, 2, 3])
+    p.add_argument("--in-flight", type=int, default=3, choices=[1, 2, 3, 4, 5, 6])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-precision", action="store_true")

@@ -417,7 +417,7 @@ int ob_chol_set_deterministic(void* factor, int on, ob_stream_t stream);
 /* The work buffers' generation: it changes whenever ob_chol_work's pointers do (a wider k than
  * any before reallocates them), so a graph recorded over them must be recorded again. */
 int ob_chol_work_generation(void* factor, long long* generation);
-/* A factor holds three independent sets of work buffers (set 0 is the one every call above uses):
+/* A factor holds six independent sets of work buffers (set 0 is the one every call above uses):
  * passes on different sets share only the read-only factor, so they may run concurrently on two
  * streams -- two batches of one mesh in flight at once (each set on one stream at a time). */
 int ob_chol_work_set(void* factor, int set, int n_columns, double** rhs, double** solution,

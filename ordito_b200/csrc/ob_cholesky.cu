@@ -686,7 +686,7 @@ struct Tile {
 };
 
 constexpr int kTileRows = 64;   // output rows per tile
-constexpr int kWorkSets = 3;    // independent work-buffer sets a factor holds
+constexpr int kWorkSets = 6;    // independent work-buffer sets a factor holds
 constexpr int kTileCols = 64;   // right-hand-side columns per tile (the wide form)
 constexpr int kTileColsNarrow = 32;  // the narrow form: twice the CTAs, half the columns each
 // Inner-dimension step staged in shared memory. 16 (two stages, 39 KB, 4 CTAs per SM) measured
