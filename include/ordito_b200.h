@@ -292,6 +292,12 @@ int ob_spmv(int n, const int32_t* offsets, const int32_t* columns, const double*
  * product launches per pass. */
 int ob_chol_analyse(int n, const int32_t* offsets, const int32_t* columns, const float* xyz,
                     int leaf_size, void** analysis, ob_stream_t stream);
+/* ob_chol_analyse_blocked: the analysis of an operator whose rows come in groups of `block`
+ * consecutive rows, one group a mesh vertex (xyz holds n / block points) -- the vector heat
+ * system's two tangent components a vertex. The dissection runs over the vertices and each
+ * vertex's rows stay consecutive in the ordering. ob_chol_analyse is block 1. */
+int ob_chol_analyse_blocked(int n, int block, const int32_t* offsets, const int32_t* columns, const float* xyz,
+                            int leaf_size, void** analysis, ob_stream_t stream);
 int ob_chol_analysis_info(void* analysis, long long* info);
 /* The same analysis from host arrays (no device), and the supernodes of an analysis as
  * out[4 s .. 4 s + 3] = (tree level, own columns, off-diagonal rows, parent or -1), postorder.
@@ -524,6 +530,95 @@ int ob_shift_packed(const double* phi, int n_vertices, int stride, const int32_t
 int ob_extend_seed(const int32_t* sources, const double* values, int n_sources, int n_vertices, double* rhs,
                    double* range, int32_t* invalid, ob_stream_t stream);
 int ob_extend_ratio(const double* diffused, int n_vertices, double* range, double* extended, ob_stream_t stream);
+
+/* ---- f3: the vector heat method (transport_tangent_vectors, log_map) ----------------------
+ * Halfedge h = 3 f + k runs faces[3 f + k] -> faces[3 f + (k + 1) % 3].
+ * ob_halfedge_twins replaces ordito/halfedge.py:59 halfedge_twins, from the operator pattern
+ * (ob_pattern_build's offsets, columns, run_start, sorted keys and order): twins[3F] = the
+ * opposite halfedge, -1 on the boundary; defects[0] = edges carried by three or more halfedges,
+ * defects[1] = edges whose two halfedges run the same way (a caller rejects the mesh when either
+ * is non-zero, as the reference raises ValueError).
+ * ob_vertex_one_rings replaces ordito/halfedge.py:284 vertex_one_rings: ring_halfedges[3F] laid
+ * out by the corner index (ob_corner_index: each vertex's degree and ascending corners), each
+ * vertex's outgoing halfedges counter-clockwise from its outgoing boundary halfedge on a rim, else
+ * from its lowest-indexed one; is_boundary[V]; defects[0] = pinched vertices (their remaining
+ * slots -1).
+ * ob_halfedge_tangent_angles replaces ordito/tangent_space.py:254 halfedge_tangent_angles: each
+ * halfedge's float64 polar angle in its origin's frame (corner_angles[3F] is scratch; a caller's
+ * float32 face_angles[F][3], or NULL to form them in float64 from the positions).
+ * ob_vertex_tangent_frames replaces ordito/tangent_space.py:38 vertex_tangent_frames: basis_x,
+ * basis_y float32 [V][3] around given_normals[V][3], or (NULL) around the angle-weighted normals
+ * gathered over the rings and written to normals[V][3].
+ * ob_tangent_to_world replaces heat.py tangent_to_world (kernels/heat.py:583): out[V][3] =
+ * tangent[v][0] basis_x[v] + tangent[v][1] basis_y[v].
+ * ob_halfedge_transport replaces ordito/tangent_space.py:363 halfedge_transport_angles and
+ * heat.py:1958 _transport_rotations: rho[3F] and rotations[3F][2] = (cos, sin); either may be
+ * NULL.
+ * ob_polar_unit: rotations[n][2] = (cos, sin) of caller-supplied transport angles (heat.py:1958).
+ * ob_half_cot_f64: the float64 half-cotangent table [F][3] (kernels/laplacian.py:130).
+ * ob_block_pattern: the pattern expanded to 2 V rows (vertex v's rows 2v and 2v + 1, entry k's
+ * 2 x 2 block at columns 2c, 2c + 1): block_offsets[2V + 1], block_columns[4 nnz].
+ * ob_vector_heat_rows replaces kernels/heat.py:524 vector_heat_system_rows: the values[4 nnz] of
+ * M + factor L_connection over the expanded pattern, factor = scale or, with from_edges,
+ * scale * (edge_sums[0] / edge_sums[1])^2; mass[V] is the scalar bundle's lumped mass.
+ * ob_transport_seed replaces kernels/heat.py:3881 seed_transport_sources: field[2V] (the vectors,
+ * interleaved) and scalars[V][2] (indicator, magnitude), both zeroed here; invalid[0] set by an
+ * out-of-range source.
+ * ob_transport_tail replaces kernels/heat.py:3975 transported_and_resolved: transported[V][2]
+ * float32 and resolved[V] (uint8).
+ * ob_vertex_unit_gradient replaces kernels/heat.py:3999 scatter_unit_gradient_to_vertices with
+ * the corner sum in ascending corner order: out[V][3] float32 (face_scratch [F][3] float32).
+ * ob_log_map_angles replaces kernels/heat.py:4030 log_map_from_angles: out[V][2] float32.
+ * ob_log_map_outward_ball replaces kernels/heat.py:4088 seed_log_map_outward_ball: rhs[2V][2]
+ * (zeroed here), column 0 the outward ball, column 1 the source's reference direction.
+ * ob_radial_divergence replaces kernels/heat.py:4193 radial_field_divergence over fields[2V][2]
+ * (corner_scratch [3F] float64; summed per vertex in ascending corner order).
+ * ob_log_map_fields replaces kernels/heat.py:4228 log_map_from_vector_fields: out[V][2] float32. */
+int ob_halfedge_twins(const int32_t* offsets, const int32_t* columns, const int32_t* run_start, const uint64_t* keys,
+                      int n_keys, const int32_t* order, const int32_t* faces, int n_faces, int n_vertices,
+                      int32_t* twins, int32_t* defects, ob_stream_t stream);
+int ob_vertex_one_rings(const int32_t* corner_offsets, const int32_t* corner_slots, const int32_t* twins,
+                        int n_vertices, int32_t* ring_halfedges, uint8_t* is_boundary, int32_t* defects,
+                        ob_stream_t stream);
+int ob_halfedge_tangent_angles(const float* xyz, const int32_t* faces, int n_faces, int n_vertices,
+                               const int32_t* ring_offsets, const int32_t* ring_halfedges, const uint8_t* is_boundary,
+                               const float* face_angles, double* corner_angles, double* angles, ob_stream_t stream);
+int ob_vertex_tangent_frames(const float* xyz, const int32_t* faces, int n_faces, int n_vertices,
+                             const int32_t* ring_offsets, const int32_t* ring_halfedges, const uint8_t* is_boundary,
+                             const float* given_normals, float* basis_x, float* basis_y, float* normals,
+                             ob_stream_t stream);
+int ob_tangent_to_world(const float* tangent, const float* basis_x, const float* basis_y, int n_vertices, float* out,
+                        ob_stream_t stream);
+int ob_halfedge_transport(const int32_t* twins, const double* tangent_angles, int n_halfedges, double* rho,
+                          double* rotations, ob_stream_t stream);
+int ob_polar_unit(const double* angles, int n, double* rotations, ob_stream_t stream);
+int ob_half_cot_f64(const float* xyz, const int32_t* faces, int n_faces, double* cot, ob_stream_t stream);
+int ob_block_pattern(const int32_t* offsets, const int32_t* columns, int n_vertices, int32_t* block_offsets,
+                     int32_t* block_columns, ob_stream_t stream);
+int ob_vector_heat_rows(const int32_t* offsets, const int32_t* columns, const int32_t* run_start, const uint64_t* keys,
+                        int n_keys, const int32_t* order, int n_vertices, const int32_t* faces, const double* cot,
+                        const double* rotations, const double* mass, double scale, const double* edge_sums,
+                        int from_edges, double* values, ob_stream_t stream);
+int ob_transport_seed(const int32_t* sources, const float* vectors, int n_sources, int n_vertices, double* field,
+                      double* scalars, int32_t* invalid, ob_stream_t stream);
+int ob_transport_tail(const double* field, const double* scalars, int n_vertices, double resolved_fraction,
+                      float* transported, uint8_t* resolved, ob_stream_t stream);
+int ob_vertex_unit_gradient(const float* xyz, const int32_t* faces, int n_faces, int n_vertices, const float* normals,
+                            const float* areas, const double* values, const int32_t* corner_offsets,
+                            const int32_t* corner_slots, float* face_scratch, float* out, ob_stream_t stream);
+int ob_log_map_angles(const float* vertex_gradient, const float* basis_x, const float* basis_y,
+                      const double* transported, const double* distance, int n_vertices, float* out,
+                      ob_stream_t stream);
+int ob_log_map_outward_ball(const float* xyz, const int32_t* faces, const int32_t* ring_offsets,
+                            const int32_t* ring_halfedges, const double* tangent_angles,
+                            const double* transport_angles, int source, int n_vertices, double* rhs,
+                            ob_stream_t stream);
+int ob_radial_divergence(const float* xyz, const int32_t* faces, int n_faces, int n_vertices,
+                         const double* tangent_angles, const double* transport_angles, const double* fields, int source,
+                         const float* cot, const int32_t* corner_offsets, const int32_t* corner_slots,
+                         double* corner_scratch, double* divergence, ob_stream_t stream);
+int ob_log_map_fields(const double* fields, const double* distance, int source, int n_vertices, float* out,
+                      ob_stream_t stream);
 
 /* ---- a12: the marched settled solve --------------------------------------------------------
  * Replaces ordito/linalg.py:2765 _march_settled (kernels/linalg.py:1229-1545): x = A^-1 rhs for

@@ -104,6 +104,24 @@ SIGNATURES: dict[str, list] = {
     "ob_divergence_tiles": [P, P, I, P, P, P, P],
     "ob_grad_div_tiled": [P, P, P, P, P, P, P, I, I, P, I, P, P, I, P, P, P],
     "ob_extend_seed": [P, P, I, I, P, P, P, P],
+    "ob_halfedge_twins": [P, P, P, P, I, P, P, I, I, P, P, P],
+    "ob_vertex_one_rings": [P, P, P, I, P, P, P, P],
+    "ob_halfedge_tangent_angles": [P, P, I, I, P, P, P, P, P, P, P],
+    "ob_vertex_tangent_frames": [P, P, I, I, P, P, P, P, P, P, P, P],
+    "ob_tangent_to_world": [P, P, P, I, P, P],
+    "ob_halfedge_transport": [P, P, I, P, P, P],
+    "ob_half_cot_f64": [P, P, I, P, P],
+    "ob_polar_unit": [P, I, P, P],
+    "ob_block_pattern": [P, P, I, P, P, P],
+    "ob_vector_heat_rows": [P, P, P, P, I, P, I, P, P, P, P, D, P, I, P, P],
+    "ob_transport_seed": [P, P, I, I, P, P, P, P],
+    "ob_transport_tail": [P, P, I, D, P, P, P],
+    "ob_vertex_unit_gradient": [P, P, I, I, P, P, P, P, P, P, P, P],
+    "ob_log_map_angles": [P, P, P, P, P, I, P, P],
+    "ob_log_map_outward_ball": [P, P, P, P, P, P, I, I, P, P],
+    "ob_radial_divergence": [P, P, I, I, P, P, P, I, P, P, P, P, P, P],
+    "ob_log_map_fields": [P, P, I, I, P, P],
+    "ob_chol_analyse_blocked": [I, I, P, P, P, I, POINTER(c_void_p), P],
     "ob_extend_ratio": [P, I, P, P, P],
     "ob_chol_set_deterministic": [P, I, P],
     "ob_chol_tile_columns": [P, I, P],

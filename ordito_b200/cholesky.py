@@ -40,16 +40,20 @@ class NotPositiveDefiniteError(ValueError):
 class CholeskyAnalysis:
     """The ordering and symbolic structure of one pattern, shareable by every operator on it."""
 
-    def __init__(self, matrix: CsrMatrix, coordinates: Any = None, leaf_size: int | None = None) -> None:
+    def __init__(self, matrix: CsrMatrix, coordinates: Any = None, leaf_size: int | None = None,
+                 block: int = 1) -> None:
+        """``block`` > 1: the rows come in groups of ``block``, one group a vertex of
+        ``coordinates`` (the vector heat system's two tangent components a vertex); each vertex's
+        rows stay consecutive in the ordering."""
         if leaf_size is None:
             leaf_size = CHOLESKY_LEAF_ROWS
         handle = ctypes.c_void_p(0)
         xyz = 0
         keep = None
         if coordinates is not None:
-            xyz, keep = device_pointer(coordinates, np.float32, 3 * matrix.nrow)
-        _lib.call("ob_chol_analyse", matrix.nrow, matrix.offsets.ptr, matrix.columns.ptr, xyz,
-                  int(leaf_size), ctypes.byref(handle), DEFAULT_STREAM)
+            xyz, keep = device_pointer(coordinates, np.float32, 3 * (matrix.nrow // block))
+        _lib.call("ob_chol_analyse_blocked", matrix.nrow, int(block), matrix.offsets.ptr,
+                  matrix.columns.ptr, xyz, int(leaf_size), ctypes.byref(handle), DEFAULT_STREAM)
         del keep
         self.handle = handle
         info = (ctypes.c_longlong * 5)()
@@ -268,10 +272,12 @@ def sparse_cholesky(matrix: CsrMatrix, coordinates: Any = None, *, negated: bool
 class OperatorFactorization:
     """The factorization slot of one operator (ordito/linalg.py:2191)."""
 
-    def __init__(self, matrix: CsrMatrix, coordinates: Any = None, *, singular: bool | None = None) -> None:
+    def __init__(self, matrix: CsrMatrix, coordinates: Any = None, *, singular: bool | None = None,
+                 block: int = 1) -> None:
         self.matrix = matrix
         self.coordinates = coordinates
         self.singular = singular
+        self.block = block
         self.factorization: SparseCholesky | None = None
         self.analysis: CholeskyAnalysis | None = None
         self.refused = False
@@ -281,7 +287,7 @@ class OperatorFactorization:
     def exceeds_budget(self) -> bool:
         """Whether the factor would exceed ``CHOLESKY_MEMORY_BUDGET`` (asks the analysis)."""
         if self.analysis is None:
-            self.analysis = CholeskyAnalysis(self.matrix, self.coordinates)
+            self.analysis = CholeskyAnalysis(self.matrix, self.coordinates, block=self.block)
         return self.analysis.factor_bytes > CHOLESKY_MEMORY_BUDGET
 
     def factor(self, sharing: "OperatorFactorization | None" = None) -> bool:

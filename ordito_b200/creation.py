@@ -181,6 +181,41 @@ def grid(count: tuple[int, int] = (2, 2)) -> tuple[np.ndarray, np.ndarray]:
     return vertices, np.asarray(faces, dtype=np.int32)
 
 
+def flat_grid(count: tuple[int, int] = (10, 10), extents: tuple[float, float] = (1.0, 1.0),
+              center: bool = True) -> tuple[np.ndarray, np.ndarray]:
+    """ordito's ``creation.grid`` patch (``ordito/creation.py:385``, ``kernels/creation.py:70``):
+    ``nx x ny`` vertices in the z = 0 plane numbered ``i * ny + j`` (X the slow axis) at
+    ``origin + extent * (k / (n - 1))``, cell ``(i, j)`` split into ``(c, c + ny, c + ny + 1)`` and
+    ``(c, c + ny + 1, c + 1)``, both wound counter-clockwise seen from +Z. Vertex and face
+    numbering matter to the tangent frames (their gauge starts at each vertex's highest face)."""
+    nx, ny = int(count[0]), int(count[1])
+    if nx < 2 or ny < 2:
+        raise ValueError(f"count must be at least 2 along each axis, got {count}")
+    width, height = float(extents[0]), float(extents[1])
+    x0 = -0.5 * width if center else 0.0
+    y0 = -0.5 * height if center else 0.0
+    i, j = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+    x = x0 + width * (i.astype(np.float64) / (nx - 1))
+    y = y0 + height * (j.astype(np.float64) / (ny - 1))
+    vertices = np.stack((x.ravel(), y.ravel(), np.zeros(nx * ny)), axis=1).astype(np.float32)
+    corner = (i[:-1, :-1] * ny + j[:-1, :-1]).ravel()
+    faces = np.empty((2 * corner.size, 3), dtype=np.int32)
+    faces[0::2] = np.stack((corner, corner + ny, corner + ny + 1), axis=1)
+    faces[1::2] = np.stack((corner, corner + ny + 1, corner + 1), axis=1)
+    return vertices, faces
+
+
+def octahedron() -> tuple[np.ndarray, np.ndarray]:
+    """The unit octahedron: vertices +x, +y, +z, -x, -y, -z and the 8 outward faces in ordito's
+    numbering (``ordito/creation.py:215-229``; the ring and frame known answers depend on it)."""
+    vertices = np.array([[1, 0, 0], [0, 1, 0], [0, 0, 1], [-1, 0, 0], [0, -1, 0], [0, 0, -1]],
+                        dtype=np.float32)
+    # Faces around +x (vertex 0), then around -x (vertex 3), each counter-clockwise from outside.
+    faces = np.array([[0, 1, 2], [0, 2, 4], [0, 4, 5], [0, 5, 1],
+                      [3, 1, 5], [3, 5, 4], [3, 4, 2], [3, 2, 1]], dtype=np.int32)
+    return vertices, faces
+
+
 def box() -> tuple[np.ndarray, np.ndarray]:
     """The unit cube ``[0, 1]^3`` as 8 vertices and 12 outward-wound triangles."""
     vertices = np.array(

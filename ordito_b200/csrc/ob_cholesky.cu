@@ -323,8 +323,11 @@ void amalgamate(Analysis& A, const std::vector<int>& adj_off, const std::vector<
     symbolic(A, adj_off, adj);
 }
 
+// `block` > 1: the operator's rows come in groups of `block` consecutive rows, one group a mesh
+// vertex (xyz holds n / block points), as in a system of tangent vectors. The dissection then runs
+// over the vertices' graph and every vertex's rows stay together, consecutive in the ordering.
 int analyse(int n, std::vector<int> offsets, std::vector<int> columns, const float* xyz,
-            int leaf_size, Analysis* out) {
+            int leaf_size, Analysis* out, int block = 1) {
     Analysis& A = *out;
     A.n = n;
     A.offsets = std::move(offsets);
@@ -337,12 +340,41 @@ int analyse(int n, std::vector<int> offsets, std::vector<int> columns, const flo
             if (A.columns[e] != i) adj.push_back(A.columns[e]);
         adj_off[i + 1] = (int)adj.size();
     }
-    Dissector D(adj_off, adj, xyz, n, leaf_size > 0 ? leaf_size : kDefaultLeafSize);
-    std::vector<int> all(n);
-    std::iota(all.begin(), all.end(), 0);
-    D.dissect(std::move(all));
-    A.perm = std::move(D.order);
-    A.nodes = std::move(D.tree);
+    if (leaf_size <= 0) leaf_size = kDefaultLeafSize;
+    if (block > 1) {
+        const int nv = n / block;
+        std::vector<int> vadj_off(nv + 1, 0), vadj, seen(nv, -1);
+        for (int v = 0; v < nv; ++v) {
+            for (int r = block * v; r < block * v + block; ++r)
+                for (int e = A.offsets[r]; e < A.offsets[r + 1]; ++e) {
+                    const int u = A.columns[e] / block;
+                    if (u != v && seen[u] != v) {
+                        seen[u] = v;
+                        vadj.push_back(u);
+                    }
+                }
+            vadj_off[v + 1] = (int)vadj.size();
+        }
+        Dissector D(vadj_off, vadj, xyz, nv, std::max(1, leaf_size / block));
+        std::vector<int> all(nv);
+        std::iota(all.begin(), all.end(), 0);
+        D.dissect(std::move(all));
+        A.perm.resize(n);
+        for (int p = 0; p < nv; ++p)
+            for (int b = 0; b < block; ++b) A.perm[block * p + b] = block * D.order[p] + b;
+        A.nodes = std::move(D.tree);
+        for (Node& node : A.nodes) {
+            node.start *= block;
+            node.count *= block;
+        }
+    } else {
+        Dissector D(adj_off, adj, xyz, n, leaf_size);
+        std::vector<int> all(n);
+        std::iota(all.begin(), all.end(), 0);
+        D.dissect(std::move(all));
+        A.perm = std::move(D.order);
+        A.nodes = std::move(D.tree);
+    }
     A.iperm.assign(n, 0);
     for (int i = 0; i < n; ++i) A.iperm[A.perm[i]] = i;
     symbolic(A, adj_off, adj);
@@ -1606,10 +1638,16 @@ extern "C" {
 
 int ob_chol_analyse(int n, const int32_t* offsets, const int32_t* columns, const float* xyz,
                     int leaf_size, void** analysis, ob_stream_t stream_) {
+    return ob_chol_analyse_blocked(n, 1, offsets, columns, xyz, leaf_size, analysis, stream_);
+}
+
+int ob_chol_analyse_blocked(int n, int block, const int32_t* offsets, const int32_t* columns, const float* xyz,
+                            int leaf_size, void** analysis, ob_stream_t stream_) {
     cudaStream_t stream = as_stream(stream_);
     OB_REQUIRE(analysis != nullptr, "ob_chol_analyse: null output");
     *analysis = nullptr;
     OB_REQUIRE(n >= 1 && offsets && columns, "ob_chol_analyse: bad argument");
+    OB_REQUIRE(block >= 1 && n % block == 0, "ob_chol_analyse_blocked: %d rows are not groups of %d", n, block);
     std::vector<int> off(n + 1);
     OB_CUDA(cudaMemcpyAsync(off.data(), offsets, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost,
                             stream));
@@ -1619,14 +1657,14 @@ int ob_chol_analyse(int n, const int32_t* offsets, const int32_t* columns, const
     OB_CUDA(cudaMemcpyAsync(col.data(), columns, sizeof(int) * off[n], cudaMemcpyDeviceToHost,
                             stream));
     if (xyz != nullptr) {
-        pts.resize(3 * (size_t)n);
-        OB_CUDA(cudaMemcpyAsync(pts.data(), xyz, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost,
-                                stream));
+        pts.resize(3 * (size_t)(n / block));
+        OB_CUDA(cudaMemcpyAsync(pts.data(), xyz, sizeof(float) * 3 * (size_t)(n / block),
+                                cudaMemcpyDeviceToHost, stream));
     }
     OB_CUDA(cudaStreamSynchronize(stream));
     col.resize(off[n]);
     Analysis* A = new Analysis();
-    int st = analyse(n, std::move(off), std::move(col), xyz ? pts.data() : nullptr, leaf_size, A);
+    int st = analyse(n, std::move(off), std::move(col), xyz ? pts.data() : nullptr, leaf_size, A, block);
     if (st) {
         delete A;
         return st;

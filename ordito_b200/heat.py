@@ -235,8 +235,49 @@ class HeatSolver:
     def operators(self) -> HeatOperators:
         if self._operators is None:
             t, _ = self._vertex_time()
-            self._operators = _assemble(self._mesh, t, self.method, use_robust=self.use_robust)[0]
+            self._operators, self._built = _assemble(self._mesh, t, self.method, use_robust=self.use_robust)
         return self._operators
+
+    # -- the vector heat method (ordito/heat.py:3677, 3952-4060) -------------------------------
+    def _require_vector_discretization(self, what: str) -> None:
+        """The vector heat method is defined on the potpourri3d discretization (heat.py:4443)."""
+        if self.use_robust:
+            raise ValueError(f"HeatSolver: no use_robust variant of {what}")
+        if self.method != "potpourri3d":
+            raise ValueError(f"HeatSolver: no method={self.method!r} variant of {what}")
+
+    @property
+    def vector_operators(self) -> "VectorHeatOperators":
+        """``vector_heat_operators`` for the mesh at this solver's ``t`` (ordito/heat.py:3677): its
+        scalar bundle is ``operators``, one assembly."""
+        self._require_vector_discretization("the vector heat operators")
+        if getattr(self, "_vector_operators", None) is None:
+            operators = self.operators
+            mesh = self._mesh
+            t, _ = self._vertex_time()
+            system = _vector_system(mesh, mesh.mesh_operator_pattern, mesh.halfedge_transport[1],
+                                    self._built.mass, t, self._built.edge_sums)
+            self._vector_operators = VectorHeatOperators(system, operators, mesh.vertex_tangent_frames,
+                                                         twl.jacobi_preconditioner(system))
+        return self._vector_operators
+
+    def diffuse_tangent(self, rhs: Any, solution: Any) -> None:
+        """Solve the vector heat system ``(M + t L_connection) X = rhs`` to settled entries, in place:
+        ``rhs`` and ``solution`` hold ``2 V`` rows (vertex v's tangent components in rows ``2v`` and
+        ``2v + 1``), one column or several row-interleaved (ordito/heat.py:3952-4060). Factored on
+        its second solve, as the heat system is; past the budget the band march answers."""
+        system = self.vector_operators.vector_system
+        kept = self._kept("vector")
+        twl.solve_spd_settled(
+            system,
+            rhs,
+            solution,
+            check_rounds=_HEAT_CHECK_ROUNDS,
+            change_tolerance=_HEAT_CHANGE_TOLERANCE,
+            settle_rounds=self._vertex_time()[1],
+            factorization=kept["factorization"],
+            narrow_values=True,
+        )
 
     # -- solves --------------------------------------------------------------------------------
     def _system(self, role: str) -> Any:
@@ -249,10 +290,13 @@ class HeatSolver:
                 "poisson": lambda: self.operators.poisson_system,
                 "pinned": lambda: self._pinned_system()[0],
                 "poisson_regularized": lambda: self._regularized_system()[0],
+                "vector": lambda: self.vector_operators.vector_system,
             }[role]()
             kept = self._systems[role] = {
+                # The vector system's two tangent rows a vertex are analysed as one (block 2).
                 "factorization": OperatorFactorization(
-                    matrix, self._mesh.vertices, singular=role == "poisson"
+                    matrix, self._mesh.vertices, singular=role == "poisson",
+                    block=2 if role == "vector" else 1,
                 ),
                 "solves": 0,
             }
@@ -270,9 +314,10 @@ class HeatSolver:
         return kept
 
     def _sharing(self, role: str) -> Any:
-        # Every other system is stored over the heat system's pattern: its analysis serves them.
+        # Every other scalar system is stored over the heat system's pattern: its analysis serves
+        # them (the vector system's expanded pattern has an analysis of its own).
         heat = self._systems.get("heat")
-        return heat["factorization"] if role != "heat" and heat is not None else None
+        return heat["factorization"] if role not in ("heat", "vector") and heat is not None else None
 
     def _pinned_system(self) -> tuple[Any, DeviceArray] | tuple[()]:
         """``diffuse_pinned``'s system and rim mask, built on first use; ``()`` with no rim
@@ -472,6 +517,9 @@ class HeatSolver:
         if getattr(self, "_regularized", None) is not None:
             extra.append(self._regularized[0])
         self._pinned = self._regularized = None
+        if getattr(self, "_vector_operators", None) is not None:
+            self._vector_operators.vector_system.release()
+            self._vector_operators = None
         if self._operators is not None:
             for matrix in (self._operators.heat_system, self._operators.poisson_system,
                            self._operators.laplacian, *extra):
@@ -1163,3 +1211,266 @@ def _extend_scalar(bound: Trimesh, src_arg: Any, val_arg: Any, t: float | None) 
             stacklevel=3,
         )
     return extended
+
+
+# --------------------------------------------------------------------------------------------
+# The vector heat method (Sharp, Soliman and Crane 2019): transport_tangent_vectors and log_map
+# (ordito/heat.py:1740-3027), on the potpourri3d discretization.
+# --------------------------------------------------------------------------------------------
+
+# A transported direction is resolved where the diffused vector is longer than this fraction of
+# the diffused magnitudes at the same vertex (ordito/heat.py:1726).
+_RESOLVED_FRACTION = 1e-4
+LOG_MAP_METHODS = ("heat_geodesic", "potpourri3d")
+
+
+class VectorHeatOperators(NamedTuple):
+    """What ``vector_heat_operators`` returns (ordito/heat.py:1740-1955). ``vector_system`` is
+    ``M + t L_connection`` as the real ``2V x 2V`` CSR matrix (vertex v's tangent components in
+    rows ``2v`` and ``2v + 1``: the reference's ``mat22d`` blocks written out), ``scalar`` the
+    heat operators at the same ``t``, ``frames`` ``(basis_x, basis_y, normal)``."""
+
+    vector_system: CsrMatrix
+    scalar: HeatOperators
+    frames: tuple[DeviceArray, DeviceArray, DeviceArray]
+    preconditioner: twl.Preconditioner
+
+
+def _vector_system(mesh: Trimesh, pattern: MeshOperatorPattern, rotations: DeviceArray, mass: DeviceArray,
+                   t: float | None, edge_sums: DeviceArray | None) -> CsrMatrix:
+    """``M + t L_connection`` over the expanded pattern (``ob_block_pattern``, ``ob_half_cot_f64``,
+    ``ob_vector_heat_rows``); ``t`` None takes the device's ``h ** 2`` from ``edge_sums``."""
+    n = mesh.n_vertices
+    nnz = int(pattern.offsets.view(n, n + 1).numpy()[0]) if n else 0
+    offsets = DeviceArray.empty(2 * n + 1, np.int32)
+    columns = DeviceArray.empty(max(4 * nnz, 1), np.int32)
+    _lib.call("ob_block_pattern", pattern.offsets.ptr, pattern.columns.ptr, n, offsets.ptr, columns.ptr,
+              DEFAULT_STREAM)
+    cot = DeviceArray.empty((max(mesh.n_faces, 1), 3), np.float64)
+    _lib.call("ob_half_cot_f64", mesh.vertices.ptr, mesh.faces.ptr, mesh.n_faces, cot.ptr, DEFAULT_STREAM)
+    values = DeviceArray.empty(max(4 * nnz, 1), np.float64)
+    if t is None and edge_sums is None:
+        raise ValueError("_vector_system: t None needs the edge sums")
+    _lib.call(
+        "ob_vector_heat_rows", pattern.offsets.ptr, pattern.columns.ptr, pattern.run_start.ptr, pattern.keys.ptr,
+        pattern.n_keys, pattern.order.ptr, n, mesh.faces.ptr, cot.ptr, rotations.ptr, mass.ptr,
+        1.0 if t is None else float(t), edge_sums.ptr if t is None else None, 1 if t is None else 0, values.ptr,
+        DEFAULT_STREAM,
+    )  # fmt: skip
+    return CsrMatrix(2 * n, 2 * n, offsets, columns, values, 4 * nnz)
+
+
+def vector_heat_operators(vertices: Any, faces: Any, t: float | None = None, *, scalar_operators: Any = None,
+                          frames: Any = None, pattern: MeshOperatorPattern | None = None,
+                          transport_angles: Any = None) -> VectorHeatOperators:
+    """Everything the vector solvers need before their solves (ordito/heat.py:1740): the vector
+    heat system ``M + t L_connection``, the scalar heat operators at the same ``t`` (or the
+    caller's ``scalar_operators``, which must be at that ``t``), the vertex tangent frames (or the
+    caller's ``frames``) and the vector system's Jacobi preconditioner. ``t`` None: the squared
+    unique-edge mean. ``pattern`` and ``transport_angles`` may be passed prebuilt. Raises
+    ``ValueError`` for a pattern of another operator or vertex count."""
+    mesh = Trimesh(vertices, faces)
+    if pattern is not None:
+        if pattern.operator != "cotmatrix" or pattern.n_vertices != mesh.n_vertices:
+            raise ValueError(
+                f"pattern was built for operator={pattern.operator!r} over {pattern.n_vertices} vertices; the "
+                f"heat operators need operator='cotmatrix' over {mesh.n_vertices}"
+            )
+        mesh._pattern = pattern
+    operators, built = _assemble(mesh, t, "potpourri3d")
+    if mesh.n_faces == 0:
+        system = CsrMatrix(2 * mesh.n_vertices, 2 * mesh.n_vertices,
+                           DeviceArray.zeros(2 * mesh.n_vertices + 1, np.int32), DeviceArray.empty(1, np.int32),
+                           DeviceArray.empty(1, np.float64), 0)
+    else:
+        if transport_angles is None:
+            rotations = mesh.halfedge_transport[1]
+        else:
+            angles = as_device(transport_angles, np.float64)
+            if angles.size != 3 * mesh.n_faces:
+                raise ValueError(f"transport_angles must hold one angle per halfedge ({3 * mesh.n_faces})")
+            rotations = DeviceArray.empty((3 * mesh.n_faces, 2), np.float64)
+            _lib.call("ob_polar_unit", angles.ptr, angles.size, rotations.ptr, DEFAULT_STREAM)
+        system = _vector_system(mesh, mesh.mesh_operator_pattern, rotations, built.mass, t, built.edge_sums)
+    return VectorHeatOperators(
+        system,
+        scalar_operators if scalar_operators is not None else operators,
+        tuple(frames) if frames is not None else mesh.vertex_tangent_frames,
+        twl.jacobi_preconditioner(system),
+    )
+
+
+def tangent_to_world(tangent: Any, basis_x: Any, basis_y: Any) -> DeviceArray:
+    """A tangent field ``(V, 2)`` as world vectors ``(V, 3)``: ``a * basis_x + b * basis_y``."""
+    from ordito_b200.tangent_space import tangent_to_world as _to_world  # noqa: PLC0415
+
+    return _to_world(tangent, basis_x, basis_y)
+
+
+def transport_tangent_vectors(
+    mesh: Any = None,
+    faces: Any = None,
+    sources: Any = None,
+    vectors: Any = None,
+    t: float | None = None,
+    *,
+    vertices: Any = None,
+) -> tuple[DeviceArray, DeviceArray]:
+    """Parallel-transport tangent vectors from a few source vertices to every vertex
+    (ordito/heat.py:2526; potpourri3d's ``MeshVectorHeatSolver.transport_tangent_vectors``).
+
+    ``transport_tangent_vectors(trimesh, sources, vectors, t=...)`` or
+    ``transport_tangent_vectors(vertices, faces, sources, vectors, t)``; ``vectors`` ``(k, 2)``, each
+    in its own source's frame. The vector heat system diffuses the source vectors (their
+    directions) and the heat system their indicator and magnitudes (the lengths), as two settled
+    solves. Returns ``(transported float32 (V, 2), resolved bool (V,))`` on the device, each vector
+    in its vertex's frame (``vertex_tangent_frames``); ``resolved`` is False where the direction
+    cannot be told from round-off (nothing arrived, or copies cancel on the cut locus). Raises
+    ``ValueError`` when ``vectors`` is not as long as ``sources`` or a source is not a vertex."""
+    if isinstance(mesh, Trimesh):
+        if vertices is not None or vectors is not None:
+            raise TypeError("transport_tangent_vectors: pass (trimesh, sources, vectors) or "
+                            "(vertices, faces, sources, vectors)")
+        bound, held, src_arg, vec_arg = mesh, True, faces, sources
+    else:
+        verts = mesh if vertices is None else vertices
+        if verts is None or faces is None:
+            raise TypeError("transport_tangent_vectors: needs a Trimesh, or vertices and faces")
+        bound, held, src_arg, vec_arg = Trimesh(verts, faces), False, sources, vectors
+    try:
+        return _transport_tangent_vectors(bound, src_arg, vec_arg, t)
+    finally:
+        if not held:
+            bound.dispose()
+
+
+def _transport_tangent_vectors(bound: Trimesh, src_arg: Any, vec_arg: Any,
+                               t: float | None) -> tuple[DeviceArray, DeviceArray]:
+    n = bound.n_vertices
+    src = _require_sources(src_arg if hasattr(src_arg, "__cuda_array_interface__")
+                           else np.ascontiguousarray(src_arg, dtype=np.int32).reshape(-1), n)
+    if n == 0 or bound.n_faces == 0 or src.size == 0:
+        return DeviceArray.zeros((n, 2), np.float32), DeviceArray.zeros(n, np.bool_)
+    vec = as_device(vec_arg if hasattr(vec_arg, "__cuda_array_interface__")
+                    else np.ascontiguousarray(vec_arg, dtype=np.float32).reshape(-1), np.float32)
+    if vec.size != 2 * src.size:
+        raise ValueError(f"transport_tangent_vectors: vectors must hold one 2D vector per source ({src.size}), "
+                         f"got {vec.size // 2}")
+    field_rhs = DeviceArray.empty(2 * n, np.float64)
+    scalar_rhs = DeviceArray.empty((n, 2), np.float64)
+    invalid = DeviceArray.empty(1, np.int32)
+    _lib.call("ob_transport_seed", src.ptr, vec.ptr, src.size, n, field_rhs.ptr, scalar_rhs.ptr, invalid.ptr,
+              DEFAULT_STREAM)
+    if int(invalid.numpy()[0]) != 0:
+        raise ValueError("transport_tangent_vectors: every entry of sources must be a vertex index in "
+                         "[0, n_vertices)")
+    solver = bound.heat_solver(t)
+    field = DeviceArray.zeros(2 * n, np.float64)
+    solver.diffuse_tangent(field_rhs, field)
+    scalars = DeviceArray.zeros((n, 2), np.float64)
+    solver.diffuse(scalar_rhs, scalars)
+    transported = DeviceArray.empty((n, 2), np.float32)
+    resolved = DeviceArray.empty(n, np.bool_)
+    _lib.call("ob_transport_tail", field.ptr, scalars.ptr, n, _RESOLVED_FRACTION, transported.ptr, resolved.ptr,
+              DEFAULT_STREAM)
+    return transported, resolved
+
+
+def log_map(
+    mesh: Any = None,
+    faces: Any = None,
+    source: int | None = None,
+    t: float | None = None,
+    *,
+    vertices: Any = None,
+    method: str = "heat_geodesic",
+) -> DeviceArray:
+    """Every vertex's position in the source vertex's tangent plane (ordito/heat.py:2745): length
+    the geodesic distance, direction the initial direction of the geodesic, as float32 ``(V, 2)``
+    in the source's frame, ``(0, 0)`` at the source.
+
+    ``method="heat_geodesic"`` (default): radius and radial direction from ``heat_geodesic``'s
+    distance at the vector heat method's ``t``, the angle against the source's reference direction
+    parallel-transported outwards. ``"potpourri3d"``: geometry-central's construction -- a second
+    vector diffusion of an outward ball gives the radial direction, its divergence integrated by
+    one Poisson solve the radius. Raises ``ValueError`` for a source outside ``[0, V)`` or an
+    unknown ``method``."""
+    if method not in LOG_MAP_METHODS:
+        raise ValueError(f"log_map: method must be 'heat_geodesic' or 'potpourri3d', got {method!r}")
+    if isinstance(mesh, Trimesh):
+        if vertices is not None:
+            raise TypeError("log_map: pass (trimesh, source) or (vertices, faces, source)")
+        bound, held, src = mesh, True, faces
+    else:
+        verts = mesh if vertices is None else vertices
+        if verts is None or faces is None:
+            raise TypeError("log_map: needs a Trimesh, or vertices and faces")
+        bound, held, src = Trimesh(verts, faces), False, source
+    try:
+        return _log_map(bound, int(src), t, method)
+    finally:
+        if not held:
+            bound.dispose()
+
+
+def _log_map(bound: Trimesh, source: int, t: float | None, method: str) -> DeviceArray:
+    n = bound.n_vertices
+    if n == 0 or bound.n_faces == 0:
+        return DeviceArray.zeros((n, 2), np.float32)
+    if not 0 <= source < n:
+        raise ValueError(f"log_map: source must be a vertex index in [0, {n}), got {source}")
+    solver = bound.heat_solver(t)
+    if method == "potpourri3d":
+        return _log_map_vector_heat(bound, solver, source)
+    operators = solver.vector_operators
+    invalid = DeviceArray.empty(1, np.int32)
+    sources = DeviceArray.from_host(np.array([source, 2 * source], dtype=np.int32))
+    field_rhs = DeviceArray.empty(2 * n, np.float64)
+    _lib.call("ob_seed", sources.view(1, 2).ptr, 1, 2 * n, field_rhs.ptr, invalid.ptr, DEFAULT_STREAM)
+    heat_rhs = DeviceArray.empty(n, np.float64)
+    _lib.call("ob_seed", sources.ptr, 1, n, heat_rhs.ptr, invalid.ptr, DEFAULT_STREAM)
+    transported = DeviceArray.zeros(2 * n, np.float64)
+    solver.diffuse_tangent(field_rhs, transported)
+    heat = DeviceArray.zeros(n, np.float64)
+    solver.diffuse(heat_rhs, heat)
+    distance = _distance_from_heat(bound, solver, sources.view(0, 1), heat)
+    # The radial direction: the distance's unit face gradients, area-weighted onto the vertices.
+    scalar = operators.scalar
+    corner_offsets, corner_slots = bound.corner_index
+    face_scratch = DeviceArray.empty((bound.n_faces, 3), np.float32)
+    gradient = DeviceArray.empty((n, 3), np.float32)
+    _lib.call("ob_vertex_unit_gradient", bound.vertices.ptr, bound.faces.ptr, bound.n_faces, n,
+              scalar.face_normals.ptr, scalar.face_areas.ptr, distance.ptr, corner_offsets.ptr, corner_slots.ptr,
+              face_scratch.ptr, gradient.ptr, DEFAULT_STREAM)
+    basis_x, basis_y, _ = operators.frames
+    out = DeviceArray.empty((n, 2), np.float32)
+    _lib.call("ob_log_map_angles", gradient.ptr, basis_x.ptr, basis_y.ptr, transported.ptr, distance.ptr, n,
+              out.ptr, DEFAULT_STREAM)
+    return out
+
+
+def _log_map_vector_heat(bound: Trimesh, solver: HeatSolver, source: int) -> DeviceArray:
+    """``log_map(method="potpourri3d")`` (ordito/heat.py:2952): the outward ball and the reference
+    direction diffused as two columns of one vector solve, the unit radial field's divergence
+    integrated by the Poisson solve, the angle the radial direction's against the reference's."""
+    n, n_faces = bound.n_vertices, bound.n_faces
+    operators = solver.vector_operators
+    ring, ring_offsets, _ = bound.vertex_one_rings
+    tangent = bound.halfedge_tangent_angles
+    transport = bound.halfedge_transport_angles
+    rhs = DeviceArray.empty((2 * n, 2), np.float64)
+    _lib.call("ob_log_map_outward_ball", bound.vertices.ptr, bound.faces.ptr, ring_offsets.ptr, ring.ptr,
+              tangent.ptr, transport.ptr, source, n, rhs.ptr, DEFAULT_STREAM)
+    fields = DeviceArray.zeros((2 * n, 2), np.float64)
+    solver.diffuse_tangent(rhs, fields)
+    corner_offsets, corner_slots = bound.corner_index
+    corner_scratch = DeviceArray.empty(3 * n_faces, np.float64)
+    divergence = DeviceArray.empty(n, np.float64)
+    _lib.call("ob_radial_divergence", bound.vertices.ptr, bound.faces.ptr, n_faces, n, tangent.ptr, transport.ptr,
+              fields.ptr, source, operators.scalar.cot_entries.ptr, corner_offsets.ptr, corner_slots.ptr,
+              corner_scratch.ptr, divergence.ptr, DEFAULT_STREAM)
+    distance = DeviceArray.zeros(n, np.float64)
+    solver.solve_poisson(divergence, distance)
+    out = DeviceArray.empty((n, 2), np.float32)
+    _lib.call("ob_log_map_fields", fields.ptr, distance.ptr, source, n, out.ptr, DEFAULT_STREAM)
+    return out

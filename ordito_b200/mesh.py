@@ -77,6 +77,65 @@ class Trimesh:
                                                                      self.n_faces)
         return self._corner_tiles
 
+    # -- the vector heat method's tables (ordito/mesh.py:2187 caches them the same way) ----------
+    @property
+    def halfedge_twins(self) -> DeviceArray:
+        """Each halfedge's opposite, -1 on the boundary (``halfedge.halfedge_twins``), made once."""
+        if getattr(self, "_twins", None) is None:
+            from ordito_b200.halfedge import twins_from_pattern  # noqa: PLC0415
+
+            self._twins = twins_from_pattern(self.mesh_operator_pattern, self.faces, self.n_faces)
+        return self._twins
+
+    @property
+    def vertex_one_rings(self) -> tuple[DeviceArray, DeviceArray, DeviceArray]:
+        """``(ring_halfedges, offsets, is_boundary)`` (``halfedge.vertex_one_rings``), made once."""
+        if getattr(self, "_rings", None) is None:
+            from ordito_b200.halfedge import rings_from_twins  # noqa: PLC0415
+
+            self._rings = rings_from_twins(self.faces, self.n_faces, self.n_vertices, self.halfedge_twins,
+                                           self.corner_index)
+        return self._rings
+
+    @property
+    def halfedge_tangent_angles(self) -> DeviceArray:
+        """Every halfedge's float64 polar angle in its origin's frame, made once."""
+        if getattr(self, "_tangent_angles", None) is None:
+            from ordito_b200.tangent_space import tangent_angles_of  # noqa: PLC0415
+
+            self._tangent_angles = tangent_angles_of(self.vertices.reshape(3 * self.n_vertices), self.faces,
+                                                     self.n_faces, self.n_vertices, self.vertex_one_rings)
+        return self._tangent_angles
+
+    @property
+    def halfedge_transport(self) -> tuple[DeviceArray, DeviceArray]:
+        """``(transport_angles (3F,), rotations (3F, 2))``: the connection, made once."""
+        if getattr(self, "_transport", None) is None:
+            from ordito_b200.tangent_space import transport_of  # noqa: PLC0415
+
+            self._transport = transport_of(self.halfedge_twins, self.halfedge_tangent_angles, 3 * self.n_faces,
+                                           angles=True, rotations=True)
+        return self._transport
+
+    @property
+    def halfedge_transport_angles(self) -> DeviceArray:
+        return self.halfedge_transport[0]
+
+    @property
+    def vertex_tangent_frames(self) -> tuple[DeviceArray, DeviceArray, DeviceArray]:
+        """``(basis_x, basis_y, normal)`` float32 ``(V, 3)`` each, made once."""
+        if getattr(self, "_frames", None) is None:
+            from ordito_b200.tangent_space import frames_of  # noqa: PLC0415
+
+            self._frames = frames_of(self.vertices.reshape(3 * self.n_vertices), self.faces, self.n_vertices,
+                                     self.vertex_one_rings)
+        return self._frames
+
+    @property
+    def vector_heat_operators(self) -> Any:
+        """The default solver's ``vector_heat_operators`` (ordito/mesh.py's cached bundle)."""
+        return self.heat_solver().vector_operators
+
     @property
     def mean_edge_length(self) -> float:
         """Mean over all ``3 n_faces`` per-face edges (ordito/mesh.py:1179), read back once."""
@@ -126,6 +185,7 @@ class Trimesh:
         self._pattern = None
         self._face_terms = None
         self._corner_index = None
+        self._twins = self._rings = self._tangent_angles = self._transport = self._frames = None
 
     def release_factorizations(self) -> None:
         """Drop every solver's factorizations (ordito/mesh.py:3457)."""
