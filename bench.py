@@ -57,6 +57,7 @@ def parse() -> argparse.Namespace:
     p.add_argument("--rows", type=int, default=256)
     p.add_argument("--refine", type=int, default=0)
     p.add_argument("--in-flight", type=int, default=3, choices=[1, 2, 3, 4, 5, 6])
+    p.add_argument("--no-vector-heat", action="store_true", help="skip the transport / log map timings")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-precision", action="store_true")
@@ -732,6 +733,33 @@ def run_serving(rate: float, v_max: float, warmup: int, requests: int) -> dict:
     return stats
 
 
+def run_vector_heat(mesh, source: int) -> dict:
+    """transport_tangent_vectors and log_map (both constructions) on a resident mesh: the first
+    call (tables, vector system, settled solves) and the median of 5 warm calls, host wall time
+    with a device synchronise around each call."""
+    def timed(fn) -> tuple[float, float]:
+        times = []
+        for _ in range(7):
+            synchronize()
+            t0 = time.perf_counter()
+            fn()
+            synchronize()
+            times.append((time.perf_counter() - t0) * 1e3)
+        return times[0], statistics.median(times[2:])
+
+    src = np.array([source], dtype=np.int32)
+    vec = np.array([[0.6, 0.8]], dtype=np.float32)
+    out = {"mesh_vertices": mesh.n_vertices}
+    first, warm = timed(lambda: gheat.transport_tangent_vectors(mesh, src, vec))
+    out["transport_tangent_vectors"] = {"first_ms": first, "warm_ms": warm}
+    for method in gheat.LOG_MAP_METHODS:
+        first, warm = timed(lambda: gheat.log_map(mesh, source, method=method))
+        out[f"log_map_{method}"] = {"first_ms": first, "warm_ms": warm}
+    out["what"] = ("warm = the vector heat system (2V rows) and the heat system factored on the "
+                   "device, two solves a call plus the per-vertex kernels")
+    return out
+
+
 def run_b200(args: argparse.Namespace, dist: Dist) -> None:
     from oracle import heat_path as hp
     from ordito_b200 import _lib
@@ -944,6 +972,12 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
             plain_times.append(time.perf_counter() - t_plain)
         plain = 1.0 / statistics.median(plain_times)
 
+    # The vector heat method on the same resident mesh (f3): transport of one tangent vector and
+    # both log maps, warm (each call's systems factored by the calls before it).
+    vector_heat = None
+    if not args.no_vector_heat:
+        vector_heat = run_vector_heat(mesh, int(sources[0]))
+
     # Roofline of the dominant kernel: the factored triangular passes (batched dense products over
     # 64 columns), timed standalone with CUDA events on the heat factor.
     heat_factor = solver.heat_factor
@@ -1060,6 +1094,7 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
             },
             "accuracy": {"max_rel_linf_vs_fp64_oracle": max(errors), "checked_queries": len(check)},
             "factorization": factorization,
+            "vector_heat": vector_heat,
             "e2e": {
                 "value": e2e_value,
                 "unit": UNIT,
