@@ -737,6 +737,9 @@ def run_vector_heat(mesh, source: int) -> dict:
     """transport_tangent_vectors and log_map (both constructions) on a resident mesh: the first
     call (tables, vector system, settled solves) and the median of 5 warm calls, host wall time
     with a device synchronise around each call."""
+    from ordito_b200 import heat as gheat
+    from ordito_b200.device import synchronize
+
     def timed(fn) -> tuple[float, float]:
         times = []
         for _ in range(7):

