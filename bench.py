@@ -401,6 +401,21 @@ def run_reference_benchmarks() -> dict:
     return out
 
 
+def _sell_entries(handle) -> int:
+    """The sliced-ELL entries (padding included) a CG solver's mat-vecs read."""
+    from ordito_b200 import _lib
+
+    info = (ctypes.c_longlong * 6)()
+    _lib.call("ob_pcg_info", handle, info)
+    return int(info[5])
+
+
+def _sell_bytes(n: int, entries: int, value_bytes: int) -> int:
+    """Bytes of one CG mat-vec with its dots over one column: the slice starts, every sliced-ELL
+    entry's column and value once, u and r in and w out (float64)."""
+    return 8 * ((n + 31) // 32 + 1) + (4 + value_bytes) * entries + 3 * 8 * n
+
+
 def kernel_rooflines(mesh, solver, columns: int = 64, reps: int = 10) -> dict:
     """Each kernel family of the path launched alone on this mesh, timed with CUDA events over
     ``reps`` launches after one warm-up: achieved = algorithmic bytes (every input read and every
@@ -486,10 +501,12 @@ def kernel_rooflines(mesh, solver, columns: int = 64, reps: int = 10) -> dict:
         ms = ctypes.c_float(0.0)
         _lib.call("ob_pcg_time_matvec", handle, 1, ctypes.byref(ms), None)
         _lib.call("ob_pcg_time_matvec", handle, reps, ctypes.byref(ms), None)
+        entries = _sell_entries(handle)
         _lib.lib.ob_pcg_destroy(handle)
         record("pcg_matvec_dots_" + ("f32_values" if narrow else "f64"), ms.value,
-               4 * (n + 1) + (8 if narrow else 12) * nnz + 3 * 8 * n,
-               "offsets, columns and values once, u, r in and w out (float64), one column")
+               _sell_bytes(n, entries, 4 if narrow else 8),
+               "sliced-ELL operator once (slice starts, columns and values, padding included: "
+               f"{entries} entries for {nnz} stored), u, r in and w out (float64), one column")
     # The same kernel on an operator of the same size in a local vertex order (a jittered torus
     # 2048 x 1280, row by row): the mat-vec's gathers of u follow the vertex order, and the
     # icosphere's subdivision order scatters each row's neighbours across the vector.
@@ -505,9 +522,9 @@ def kernel_rooflines(mesh, solver, columns: int = 64, reps: int = 10) -> dict:
     ms = ctypes.c_float(0.0)
     _lib.call("ob_pcg_time_matvec", handle, 1, ctypes.byref(ms), None)
     _lib.call("ob_pcg_time_matvec", handle, reps, ctypes.byref(ms), None)
+    entries = _sell_entries(handle)
     _lib.lib.ob_pcg_destroy(handle)
-    record("pcg_matvec_dots_f64_torus_2048x1280", ms.value,
-           4 * (T.nrow + 1) + 12 * T.nnz + 3 * 8 * T.nrow,
+    record("pcg_matvec_dots_f64_torus_2048x1280", ms.value, _sell_bytes(T.nrow, entries, 8),
            "as pcg_matvec_dots_f64, on the heat system of a 2 621 440-vertex torus in row order")
     torus.dispose()
 

@@ -160,6 +160,13 @@ int ob_heat_rows(const int32_t* offsets, const int32_t* columns, const int32_t* 
                  const float* cot, double scale, const double* edge_sums, int from_edges,
                  const double* area_sums, double mass_divisor, double* L, double* H, double* P,
                  double* mass, ob_stream_t stream);
+/* ob_heat_rows over a float64 half-cotangent table: the intrinsic cover's rows
+ * (ordito/heat.py:3786-3813, HEAT_SYSTEM_ROWS[wp.float64]). */
+int ob_heat_rows_f64(const int32_t* offsets, const int32_t* columns, const int32_t* run_start,
+                     const uint64_t* keys, int count, const int32_t* order, int n_vertices,
+                     const double* cot, double scale, const double* edge_sums, int from_edges,
+                     const double* area_sums, double mass_divisor, double* L, double* H, double* P,
+                     double* mass, ob_stream_t stream);
 
 /* ---- a6: source indicator -------------------------------------------------------------------
  * Replaces kernels/heat.py:614 seed_source_indicator: u0[V] zeroed then u0[s] = 1 for each source;
@@ -201,7 +208,9 @@ int ob_shift_noalloc(double* phi, int n_vertices, const int32_t* sources, int n_
  * Replaces ordito/linalg.py:3619 _BatchedCg with the kernels of
  * kernels/algorithms/conjugate_gradient.py (cg_matvec_dots :453, cg_update :797, settle
  * :1509/:1564) and the Jacobi-Chebyshev preconditioner (linalg.py:5135, multigrid.py:988).
- * A solver borrows the CSR arrays (they must outlive it) and owns its work vectors.
+ * A solver copies the CSR arrays into its own and owns its work vectors; its iteration's mat-vecs
+ * read a sliced-ELL copy it builds from them (slices of 32 rows as wide as their widest row,
+ * column-major within a slice, padded with zero entries on the row itself).
  * precond: 0 Jacobi, 1 Jacobi-Chebyshev (degree 12, interval [max(min(80/n, .5), 1-r), 1+r]).
  * narrow != 0 iterates on float32 copies of the values (vectors, dots, scalars stay float64).
  * n_columns right-hand sides are solved together; rhs/x are laid out [n][n_columns]. */
@@ -210,7 +219,8 @@ int ob_pcg_create(int n, const int32_t* offsets, const int32_t* columns, const d
 int ob_pcg_destroy(void* solver);
 /* A solver keeps its own copy of the operator it was created for. ob_pcg_rebind copies another
  * operator of the same shape (n, nnz) into it and redoes the value-dependent setup (inverse
- * diagonal, Chebyshev steps, float32 copy) on the stream -- its recorded loops replay unchanged,
+ * diagonal, Chebyshev steps, sliced-ELL copy; reading back the copy's size synchronises the
+ * stream, and a copy that must grow drops the recorded loops) -- its recorded loops replay unchanged,
  * which is how an operator rebuilt per call (ordito/linalg.py:1389-1396: "copied into a kept
  * state of that shape, which replays too") avoids a new state and a new recording. */
 int ob_pcg_rebind(void* solver, const int32_t* offsets, const int32_t* columns,
@@ -227,7 +237,8 @@ int ob_pcg_settle(void* solver, const double* rhs, double* x, int check_rounds,
                   int* status, ob_stream_t stream);
 /* Measurement hooks (no counterpart in the reference): the average duration of `reps` standalone
  * launches of the solver's round mat-vec-with-dots kernel on its current vectors (CUDA events on
- * `stream`), and the solver's shape: info[0..4] = n, padded columns, nnz, narrow, blocks. */
+ * `stream`), and the solver's shape: info[0..5] = n, padded columns, nnz, narrow, blocks, and the
+ * sliced-ELL copy's entries (padding included). */
 int ob_pcg_time_matvec(void* solver, int reps, float* ms, ob_stream_t stream);
 int ob_pcg_info(void* solver, long long* info);
 /* backward_error_exceeds (kernels/linalg.py:1167): flag[0] = 1 when some row has
@@ -631,6 +642,38 @@ int ob_log_map_fields(const double* fields, const double* distance, int source, 
  * band rows solved. Synchronises the stream (the loop reads each band's size back). */
 int ob_march_solve(int n, const int32_t* offsets, const int32_t* columns, const double* values,
                    const double* rhs, double* x, long long* info, ob_stream_t stream);
+
+/* ---- f4: the intrinsic tufted cover (use_robust at method="potpourri3d") --------------------
+ * ob_cover_build replaces ordito/heat.py:5084 _tufted_intrinsic_delaunay (kernels/heat.py:749-1130:
+ * tufted_cover, glue_nonmanifold_cover_edges, length_sum_and_violation, mollify_cover_lengths,
+ * cover_flip_candidates / _commit / _fixup). From the mesh's operator pattern (ob_pattern_build:
+ * its runs give each edge's halfedges) and its float32 positions: cover_faces[6 F] (cover face
+ * f < F the front copy of face f, F + f its back copy (c0, c2, c1)), lengths[6 F] (float64, slot
+ * 3 g + e the edge of cover face g opposite its corner e) and twin[6 F], mollified by
+ * max(0, worst violation + epsilon_mollify * mean front length) and flipped to intrinsic Delaunay
+ * (an edge flips while its two facing half-cotangents sum below -epsilon_delaunay) in rounds of
+ * independent sets -- the lowest candidate of each face claims it -- until a round flips nothing
+ * or max_rounds ran; *rounds (may be NULL) = rounds run. Every float64 step rounds once (no fused
+ * multiply-adds). Synchronises the stream (each round's flip count is read back). An edge of more
+ * than 64 faces is rejected (OB_ERR_INVALID).
+ * ob_cover_face_terms replaces kernels/heat.py:1133 cover_face_terms: cot[3 n_cover] the float64
+ * half-cotangents, area_sums[V] each vertex's corner areas (Heron, in float64) summed in ascending
+ * corner order (corner index of cover_faces from ob_corner_index), length_sums[2] (device) the sum
+ * and count of every slot's length -- the mean cover edge of the default time step.
+ * ob_cover_divergence replaces kernels/heat.py:1154 cover_unit_gradient_divergence: out[V][k] =
+ * div of the unit gradient of u[V][k] on the cover, each face laid out in the plane from its
+ * lengths, every vertex's corner terms summed in ascending corner order. */
+int ob_cover_build(const int32_t* offsets, const int32_t* columns, const int32_t* run_start,
+                   const uint64_t* keys, int n_keys, const int32_t* order, int n_vertices,
+                   const float* xyz, const int32_t* faces, int n_faces, double epsilon_mollify,
+                   double epsilon_delaunay, int max_rounds, int32_t* cover_faces, double* lengths,
+                   int32_t* twin, int32_t* rounds, ob_stream_t stream);
+int ob_cover_face_terms(const int32_t* cover_faces, const double* lengths, int n_cover, int n_vertices,
+                        const int32_t* corner_offsets, const int32_t* corner_slots, double* cot,
+                        double* area_sums, double* length_sums, ob_stream_t stream);
+int ob_cover_divergence(const int32_t* cover_faces, const double* lengths, const double* cot, int n_vertices,
+                        const int32_t* corner_offsets, const int32_t* corner_slots, const double* u,
+                        int n_columns, double* out, ob_stream_t stream);
 
 #ifdef __cplusplus
 }

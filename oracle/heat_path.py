@@ -393,12 +393,14 @@ def vertex_time(vertices: np.ndarray, faces: np.ndarray, t: float | None,
 def heat_operators(
     vertices: np.ndarray, faces: np.ndarray, t: float | None = None, *, mass_divisor: float = 3.0,
     method: str = "meshlab", use_robust: bool = False, cot: np.ndarray | None = None,
+    area_sums: np.ndarray | None = None,
 ) -> dict[str, object]:
     """The heat operators over the cotmatrix pattern (heat.py:2015-2245): barycentric mass and
     the face-edge time step for ``"meshlab"``, the unique-edge time step for ``"potpourri3d"``,
     the Voronoi mass (divisor 1) and the unique-edge time step for ``"igl"`` (heat.py:2002-2012).
     ``cot`` replaces the half-cotangent table the rows are summed from (a caller's own weights,
-    as ``cotmatrix(cot_entries=...)`` takes them, laplacian.py:371).
+    as ``cotmatrix(cot_entries=...)`` takes them, laplacian.py:371); ``area_sums`` the per-vertex
+    area sums the lumped mass divides (the intrinsic cover's, heat.py:3783-3784).
 
     Returns the pattern, the float32 cot table, normals, areas, area sums, ``L``, ``H = M - t L``,
     ``P = -L`` (float64 values over the pattern), the lumped mass and the time ``t`` used.
@@ -412,11 +414,13 @@ def heat_operators(
     if cot is None:
         cot = cot_from_lengths(mollified_lengths(v, f)[0]) if use_robust else cotmatrix_entries(v, f)
     normals, areas = face_normals_and_areas(v, f)
-    if method == "igl":
+    if area_sums is not None:
+        sums = np.asarray(area_sums, dtype=F64)
+    elif method == "igl":
         sums = voronoi_area_sums(v, f, n)
         mass_divisor = 1.0
     else:
-        sums = area_sums(f, areas, n)
+        sums = globals()["area_sums"](f, areas, n)
     if t is None:
         total, count = edge_length_sums(v, pattern, face_edges=method == "meshlab")
         h = total / count if count > 0 else 0.0

@@ -75,6 +75,10 @@ SIGNATURES: dict[str, list] = {
     "ob_mollified_cot": [P, P, I, D, P, P, POINTER(c_double), P],
     "ob_edge_sums": [P, P, P, P, I, I, P, I, P, P],
     "ob_heat_rows": [P, P, P, P, I, P, I, P, D, P, I, P, D, P, P, P, P, P],
+    "ob_heat_rows_f64": [P, P, P, P, I, P, I, P, D, P, I, P, D, P, P, P, P, P],
+    "ob_cover_build": [P, P, P, P, I, P, I, P, P, I, D, D, I, P, P, P, POINTER(c_int), P],
+    "ob_cover_face_terms": [P, P, I, I, P, P, P, P, P, P],
+    "ob_cover_divergence": [P, P, P, I, P, P, P, I, P, P],
     "ob_seed": [P, I, I, P, P, P],
     "ob_grad_div": [P, P, I, I, P, P, P, P, I, P, P],
     "ob_shift": [P, I, P, I, P, I, I, P],

@@ -94,10 +94,11 @@ __global__ void edge_sums_kernel(const int* __restrict__ offsets, const int* __r
 // kernels/laplacian.py:971-989 (cotmatrix_offdiagonal), kernels/linalg.py:1594-1621
 // (shift_factor, shifted_scalar_entry): one thread per row walks its entries in row order.
 // Row i of L, H = factor L + M and P = -L (and its mass), the one arithmetic of both kernels below.
+template <typename C>
 __device__ __forceinline__ void heat_row(int i, const int* __restrict__ offsets, const int* __restrict__ columns,
                                          const int* __restrict__ run_start,
                                          const unsigned long long* __restrict__ keys, int count,
-                                         const int* __restrict__ order, const float* __restrict__ cot,
+                                         const int* __restrict__ order, const C* __restrict__ cot,
                                          double factor, const double* __restrict__ area_sums,
                                          double mass_divisor, double* __restrict__ L, double* __restrict__ H,
                                          double* __restrict__ P, double* __restrict__ mass) {
@@ -128,10 +129,13 @@ __device__ __forceinline__ void heat_row(int i, const int* __restrict__ offsets,
     }
 }
 
+// The half-cotangent table is float32 (the extrinsic path, as the reference's) or float64 (the
+// intrinsic cover's, formed from float64 lengths: kernels/heat.py:1133, HEAT_SYSTEM_ROWS[float64]).
+template <typename C>
 __global__ void heat_rows_kernel(const int* __restrict__ offsets, const int* __restrict__ columns,
                                  const int* __restrict__ run_start,
                                  const unsigned long long* __restrict__ keys, int count,
-                                 const int* __restrict__ order, int n, const float* __restrict__ cot,
+                                 const int* __restrict__ order, int n, const C* __restrict__ cot,
                                  double scale, const double* __restrict__ edge_sums, int from_edges,
                                  const double* __restrict__ area_sums, double mass_divisor,
                                  double* __restrict__ L, double* __restrict__ H,
@@ -575,11 +579,30 @@ int ob_heat_rows(const int32_t* offsets, const int32_t* columns, const int32_t* 
                    P && mass,
                "ob_heat_rows: null pointer");
     OB_REQUIRE(!from_edges || edge_sums != nullptr, "ob_heat_rows: from_edges needs edge_sums");
-    heat_rows_kernel<<<ceil_div(n_vertices, kThreads), kThreads, 0, stream>>>(
+    heat_rows_kernel<float><<<ceil_div(n_vertices, kThreads), kThreads, 0, stream>>>(
         offsets, columns, run_start, reinterpret_cast<const unsigned long long*>(keys), count,
         order, n_vertices, cot, scale, edge_sums, from_edges, area_sums, mass_divisor, L, H, P,
         mass);
     OB_CHECK_LAUNCH("heat_rows");
+    return OB_OK;
+}
+
+int ob_heat_rows_f64(const int32_t* offsets, const int32_t* columns, const int32_t* run_start,
+                     const uint64_t* keys, int count, const int32_t* order, int n_vertices,
+                     const double* cot, double scale, const double* edge_sums, int from_edges,
+                     const double* area_sums, double mass_divisor, double* L, double* H, double* P,
+                     double* mass, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    if (n_vertices <= 0) return OB_OK;
+    OB_REQUIRE(offsets && columns && run_start && keys && order && cot && area_sums && L && H &&
+                   P && mass,
+               "ob_heat_rows_f64: null pointer");
+    OB_REQUIRE(!from_edges || edge_sums != nullptr, "ob_heat_rows_f64: from_edges needs edge_sums");
+    heat_rows_kernel<double><<<ceil_div(n_vertices, kThreads), kThreads, 0, stream>>>(
+        offsets, columns, run_start, reinterpret_cast<const unsigned long long*>(keys), count,
+        order, n_vertices, cot, scale, edge_sums, from_edges, area_sums, mass_divisor, L, H, P,
+        mass);
+    OB_CHECK_LAUNCH("heat_rows_f64");
     return OB_OK;
 }
 

@@ -13,7 +13,14 @@
 // Layout: vectors hold n_columns interleaved columns, [row][column], so the threads of one row's
 // columns gather the same neighbours' contiguous column blocks (coalesced) while the row's
 // indices and values are broadcast. The column count is padded to a power of two (<= 256); pad
-// columns have a zero right-hand side and never step.
+// columns have a zero right-hand side and never step. The iteration's mat-vecs read a sliced-ELL
+// copy of the operator the solver builds from the CSR arrays it is given (slices of 32 rows, each
+// as wide as its longest row, column-major within the slice): the 32 rows a warp serves at one
+// column read an entry index's values and columns as one contiguous 256- and 128-byte access,
+// where the CSR rows' entries would be 32 scattered ones.
+#include <cub/cub.cuh>
+
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -82,6 +89,68 @@ __device__ __forceinline__ double row_dot(const int* __restrict__ offsets,
     return acc;
 }
 
+// Sliced ELL: slice s holds rows [32 s, 32 s + 32); entry j of its row l sits at
+// start[s] + 32 j + l, start[s + 1] - start[s] = 32 x the slice's widest row. Padding entries
+// name the row itself with a zero value, so a row's sum is the CSR row's, in the same order,
+// followed by exact zeros.
+constexpr int kSlice = 32;
+
+template <typename V>
+struct Sell {
+    const long long* __restrict__ start;
+    const int* __restrict__ columns;
+    const V* __restrict__ values;
+};
+
+template <typename V>
+__device__ __forceinline__ double sell_row_dot(const Sell<V> A, const double* __restrict__ x, int row,
+                                               int k, int c) {
+    const int slice = row / kSlice, lane = row % kSlice;
+    const long long base = A.start[slice];
+    const int width = (int)((A.start[slice + 1] - base) / kSlice);
+    const int* __restrict__ cols = A.columns + base + lane;
+    const V* __restrict__ vals = A.values + base + lane;
+    double acc = 0.0;
+#pragma unroll 4
+    for (int j = 0; j < width; ++j)
+        acc = fma((double)__ldg(vals + (size_t)kSlice * j), x[(size_t)__ldg(cols + (size_t)kSlice * j) * k + c], acc);
+    return acc;
+}
+
+// 32 x the widest row of each slice (entry n_slices: 0, for the scan's total).
+__global__ void slice_width_kernel(int n, int n_slices, const int* __restrict__ offsets,
+                                   long long* __restrict__ width) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s > n_slices) return;
+    int w = 0;
+    if (s < n_slices) {
+        const int end = min(n, (s + 1) * kSlice);
+        for (int r = s * kSlice; r < end; ++r) w = max(w, offsets[r + 1] - offsets[r]);
+    }
+    width[s] = (long long)w * kSlice;
+}
+
+// Writes the sliced-ELL copy (and its float32 values when `values32` is given), a thread a row.
+__global__ void slice_fill_kernel(int n, const int* __restrict__ offsets, const int* __restrict__ columns,
+                                  const double* __restrict__ values, const long long* __restrict__ start,
+                                  int* __restrict__ sell_columns, double* __restrict__ sell_values,
+                                  float* __restrict__ sell_values32) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= n) return;
+    const int slice = row / kSlice, lane = row % kSlice;
+    const long long base = start[slice];
+    const int width = (int)((start[slice + 1] - base) / kSlice);
+    const int o = offsets[row], d = offsets[row + 1] - o;
+    for (int j = 0; j < width; ++j) {
+        const long long at = base + (long long)kSlice * j + lane;
+        const int col = j < d ? columns[o + j] : row;
+        const double v = j < d ? values[o + j] : 0.0;
+        sell_columns[at] = col;
+        sell_values[at] = v;
+        if (sell_values32) sell_values32[at] = (float)v;
+    }
+}
+
 // Jacobi setup (ordito/kernels/linalg.py jacobi_dominance_bound and chebyshev_steps :1530-1583):
 // D^-1 (0 for a row without a diagonal entry), the rows' largest Gershgorin ratio
 // sum_{j != i} |A_ij| / |A_ii|, and the Chebyshev steps fitted to it by the last block.
@@ -130,11 +199,6 @@ __global__ void jacobi_setup_kernel(int n, const int* __restrict__ offsets,
         steps[index] = make_double4(scale, previous_scale, rho_next * rho, 2.0 * rho_next / delta);
         rho = rho_next;
     }
-}
-
-__global__ void narrow_kernel(long long nnz, const double* __restrict__ in, float* __restrict__ out) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < nnz) out[i] = (float)in[i];
 }
 
 // r = b - A x (float64 values), u = D^-1 r (Jacobi) or scaled = D^-1 r (polynomial input).
@@ -207,8 +271,7 @@ __global__ void reset_kernel(int n, int k, int k_live, const double* __restrict_
 // block folds them per column in block order and derives (alpha, beta, step) (cg_step_scalars,
 // conjugate_gradient.py:549-579), then counts the round (cg_close_round :628-669).
 template <typename V>
-__global__ void __launch_bounds__(kThreads, 8) matvec_dots_kernel(int n, int k, const int* __restrict__ offsets,
-                                   const int* __restrict__ columns, const V* __restrict__ values,
+__global__ void __launch_bounds__(kThreads, 8) matvec_dots_kernel(int n, int k, const Sell<V> A,
                                    const double* __restrict__ r, const double* __restrict__ u,
                                    double* __restrict__ w, double* __restrict__ partials,
                                    unsigned int* counter, ColumnScalars* __restrict__ scalars,
@@ -226,7 +289,7 @@ __global__ void __launch_bounds__(kThreads, 8) matvec_dots_kernel(int n, int k, 
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += stride) {
         const int row = (int)(t / k);
-        const double wi = row_dot(offsets, columns, values, u, row, k, c);
+        const double wi = sell_row_dot(A, u, row, k, c);
         w[t] = wi;
         const double ri = r[t], ui = u[t];
         ag = fma(ri, ui, ag);
@@ -344,8 +407,7 @@ __global__ void __launch_bounds__(kThreads, 8) update_kernel(int n, int k, const
 // + step (source - s D^-1 A x), steps[index] = (s, s_prev, momentum, step). `out` may alias
 // `x_prev` but not `x`.
 template <typename V>
-__global__ void chebyshev_step_kernel(int n, int k, const int* __restrict__ offsets,
-                                      const int* __restrict__ columns, const V* __restrict__ values,
+__global__ void chebyshev_step_kernel(int n, int k, const Sell<V> A,
                                       const double* __restrict__ inv_diag,
                                       const double4* __restrict__ steps, int index,
                                       const double* __restrict__ source,
@@ -358,7 +420,7 @@ __global__ void chebyshev_step_kernel(int n, int k, const int* __restrict__ offs
     const int c = threadIdx.x % k;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += stride) {
         const int row = (int)(t / k);
-        const double ax = row_dot(offsets, columns, values, x, row, k, c) * inv_diag[row];
+        const double ax = sell_row_dot(A, x, row, k, c) * inv_diag[row];
         const double current = st.x * x[t];
         out[t] = current + st.z * (current - st.y * x_prev[t]) + st.w * (source[t] - st.x * ax);
     }
@@ -465,7 +527,15 @@ struct Solver {
     const int* offsets = nullptr;
     const int* columns = nullptr;
     const double* values = nullptr;
-    float* values32 = nullptr;
+    // The sliced-ELL copy the iteration's mat-vecs read (its float32 values when narrow), grown
+    // when a rebound operator's slices need more entries than it holds.
+    int n_slices = 0;
+    long long* sell_start = nullptr;
+    int* sell_columns = nullptr;
+    double* sell_values = nullptr;
+    float* sell_values32 = nullptr;
+    long long sell_capacity = 0;
+    long long sell_entries = 0;  // the current operator's (padding included)
     double *inv_diag = nullptr, *b = nullptr, *x = nullptr, *r = nullptr, *u = nullptr,
            *w = nullptr, *p = nullptr, *s = nullptr, *scaled = nullptr, *t0 = nullptr,
            *t1 = nullptr, *previous = nullptr, *partials = nullptr, *maxima = nullptr;
@@ -489,8 +559,73 @@ struct Solver {
     std::vector<void*> owned;
 };
 
+void release_sell(Solver* S) {
+    for (void* p : {(void*)S->sell_columns, (void*)S->sell_values, (void*)S->sell_values32})
+        if (p) cudaFree(p);
+    S->sell_columns = nullptr;
+    S->sell_values = nullptr;
+    S->sell_values32 = nullptr;
+    S->sell_capacity = 0;
+}
+
+void drop_graphs(Solver* S) {
+    for (int i = 0; i < 2; ++i) {
+        if (S->exec[i]) cudaGraphExecDestroy(S->exec[i]);
+        if (S->graph[i]) cudaGraphDestroy(S->graph[i]);
+        S->exec[i] = nullptr;
+        S->graph[i] = nullptr;
+    }
+}
+
+// Builds the sliced-ELL copy of the solver's CSR operator: slice widths, their scan (read back
+// once, to size the copy), the fill. A copy that must grow is reallocated, and the recorded loops
+// that name the old one are dropped (rebuilt at the next solve).
+int build_sell(Solver* S, cudaStream_t stream) {
+    const int n_slices = S->n_slices;
+    {
+        Scratch scratch(stream);
+        long long* width = scratch.take<long long>((size_t)n_slices + 1);
+        size_t bytes = 0;
+        OB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, width, S->sell_start, n_slices + 1, stream));
+        void* temp = scratch.take<unsigned char>(bytes);
+        if (int st = scratch.commit()) return st;
+        slice_width_kernel<<<ceil_div(n_slices + 1, kThreads), kThreads, 0, stream>>>(S->n, n_slices, S->offsets,
+                                                                                       width);
+        OB_CHECK_LAUNCH("pcg slice widths");
+        OB_CUDA(cub::DeviceScan::ExclusiveSum(temp, bytes, width, S->sell_start, n_slices + 1, stream));
+    }
+    long long total = 0;
+    OB_CUDA(cudaMemcpyAsync(&total, S->sell_start + n_slices, sizeof(long long), cudaMemcpyDeviceToHost,
+                            stream));
+    OB_CUDA(cudaStreamSynchronize(stream));
+    if (total > S->sell_capacity) {
+        drop_graphs(S);
+        release_sell(S);
+        const size_t entries = (size_t)std::max(total, 1LL);
+        cudaError_t e = pool_malloc((void**)&S->sell_columns, sizeof(int) * entries, stream);
+        if (e == cudaSuccess) e = pool_malloc((void**)&S->sell_values, sizeof(double) * entries, stream);
+        if (e == cudaSuccess && S->narrow)
+            e = pool_malloc((void**)&S->sell_values32, sizeof(float) * entries, stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            release_sell(S);
+            return cuda_status(e, "pcg sliced-ELL copy");
+        }
+        S->sell_capacity = total;
+    }
+    S->sell_entries = total;
+    slice_fill_kernel<<<ceil_div(S->n, kThreads), kThreads, 0, stream>>>(
+        S->n, S->offsets, S->columns, S->values, S->sell_start, S->sell_columns, S->sell_values,
+        S->narrow ? S->sell_values32 : nullptr);
+    OB_CHECK_LAUNCH("pcg slice fill");
+    return OB_OK;
+}
+
+Sell<double> sell64(const Solver* S) { return Sell<double>{S->sell_start, S->sell_columns, S->sell_values}; }
+Sell<float> sell32(const Solver* S) { return Sell<float>{S->sell_start, S->sell_columns, S->sell_values32}; }
+
 // Copies an operator of the solver's shape into its own arrays and derives what the iteration
-// reads from the values: the inverse diagonal, the Chebyshev steps and the float32 copy.
+// reads from it: the inverse diagonal, the Chebyshev steps and the sliced-ELL copy.
 int bind_operator(Solver* S, const int* offsets, const int* columns, const double* values,
                   cudaStream_t stream) {
     const int n = S->n;
@@ -508,11 +643,7 @@ int bind_operator(Solver* S, const int* offsets, const int* columns, const doubl
         n, S->offsets, S->columns, S->values, S->inv_diag, S->maxima, S->counters + 3,
         kChebyshevDegree - 1, S->steps);
     OB_CHECK_LAUNCH("pcg setup");
-    if (S->narrow && nnz > 0) {
-        narrow_kernel<<<ceil_div(nnz, kThreads), kThreads, 0, stream>>>(nnz, S->values, S->values32);
-        OB_CHECK_LAUNCH("pcg narrow");
-    }
-    return OB_OK;
+    return build_sell(S, stream);
 }
 
 int solver_alloc(Solver* S, void** out, size_t bytes, cudaStream_t stream) {
@@ -522,10 +653,8 @@ int solver_alloc(Solver* S, void** out, size_t bytes, cudaStream_t stream) {
 }
 
 void solver_release(Solver* S) {
-    for (int i = 0; i < 2; ++i) {
-        if (S->exec[i]) cudaGraphExecDestroy(S->exec[i]);
-        if (S->graph[i]) cudaGraphDestroy(S->graph[i]);
-    }
+    drop_graphs(S);
+    release_sell(S);
     for (void* p : S->owned) cudaFree(p);
     if (S->host_state) cudaFreeHost(S->host_state);
     if (S->host_scalars) cudaFreeHost(S->host_scalars);
@@ -538,12 +667,12 @@ int enqueue_round(Solver* S, cudaStream_t stream, int maxiter) {
     const int B = S->blocks;
     if (S->narrow)
         matvec_dots_kernel<float><<<B, kThreads, 0, stream>>>(
-            S->n, S->k, S->offsets, S->columns, S->values32, S->r, S->u, S->w, S->partials,
-            S->counters, S->scalars, S->state, maxiter);
+            S->n, S->k, sell32(S), S->r, S->u, S->w, S->partials, S->counters, S->scalars, S->state,
+            maxiter);
     else
         matvec_dots_kernel<double><<<B, kThreads, 0, stream>>>(
-            S->n, S->k, S->offsets, S->columns, S->values, S->r, S->u, S->w, S->partials,
-            S->counters, S->scalars, S->state, maxiter);
+            S->n, S->k, sell64(S), S->r, S->u, S->w, S->partials, S->counters, S->scalars, S->state,
+            maxiter);
     OB_CHECK_LAUNCH("matvec_dots");
     double* target = (S->precond == 1) ? S->scaled : S->u;
     update_kernel<<<B, kThreads, 0, stream>>>(S->n, S->k, S->scalars, S->inv_diag, S->w, S->u,
@@ -558,12 +687,12 @@ int enqueue_round(Solver* S, cudaStream_t stream, int maxiter) {
             double* out = (index == n_steps - 1) ? S->u : bufs[index & 1];
             if (S->narrow)
                 chebyshev_step_kernel<float><<<B, kThreads, 0, stream>>>(
-                    S->n, S->k, S->offsets, S->columns, S->values32, S->inv_diag, S->steps, index,
-                    S->scaled, in, prev, out, S->state);
+                    S->n, S->k, sell32(S), S->inv_diag, S->steps, index, S->scaled, in, prev, out,
+                    S->state);
             else
                 chebyshev_step_kernel<double><<<B, kThreads, 0, stream>>>(
-                    S->n, S->k, S->offsets, S->columns, S->values, S->inv_diag, S->steps, index,
-                    S->scaled, in, prev, out, S->state);
+                    S->n, S->k, sell64(S), S->inv_diag, S->steps, index, S->scaled, in, prev, out,
+                    S->state);
             OB_CHECK_LAUNCH("chebyshev_step");
             prev = in;
             in = out;
@@ -583,12 +712,12 @@ int enqueue_polynomial(Solver* S, cudaStream_t stream) {
         double* out = (index == n_steps - 1) ? S->u : bufs[index & 1];
         if (S->narrow)
             chebyshev_step_kernel<float><<<B, kThreads, 0, stream>>>(
-                S->n, S->k, S->offsets, S->columns, S->values32, S->inv_diag, S->steps, index,
-                S->scaled, in, prev, out, S->state);
+                S->n, S->k, sell32(S), S->inv_diag, S->steps, index, S->scaled, in, prev, out,
+                S->state);
         else
             chebyshev_step_kernel<double><<<B, kThreads, 0, stream>>>(
-                S->n, S->k, S->offsets, S->columns, S->values, S->inv_diag, S->steps, index,
-                S->scaled, in, prev, out, S->state);
+                S->n, S->k, sell64(S), S->inv_diag, S->steps, index, S->scaled, in, prev, out,
+                S->state);
         OB_CHECK_LAUNCH("chebyshev_step");
         prev = in;
         in = out;
@@ -788,7 +917,8 @@ int ob_pcg_create(int n, const int32_t* offsets, const int32_t* columns, const d
     A((void**)&S->state, sizeof(LoopState));
     A((void**)&S->settle, sizeof(SettleState));
     A((void**)&S->counters, sizeof(unsigned int) * 8);
-    if (S->narrow) A((void**)&S->values32, sizeof(float) * (size_t)std::max(nnz, 1));
+    S->n_slices = ceil_div(n, kSlice);
+    A((void**)&S->sell_start, sizeof(long long) * ((size_t)S->n_slices + 1));
     if (st != OB_OK) {
         solver_release(S);
         return st;
@@ -911,12 +1041,12 @@ int ob_pcg_time_matvec(void* solver, int reps, float* ms, ob_stream_t stream_) {
         cudaEventRecord(start, stream);
         if (S->narrow)
             matvec_dots_kernel<float><<<B, kThreads, 0, stream>>>(
-                S->n, S->k, S->offsets, S->columns, S->values32, S->r, S->u, S->w, S->partials,
-                S->counters, S->scalars, S->state, 0x7fffffff);
+                S->n, S->k, sell32(S), S->r, S->u, S->w, S->partials, S->counters, S->scalars,
+                S->state, 0x7fffffff);
         else
             matvec_dots_kernel<double><<<B, kThreads, 0, stream>>>(
-                S->n, S->k, S->offsets, S->columns, S->values, S->r, S->u, S->w, S->partials,
-                S->counters, S->scalars, S->state, 0x7fffffff);
+                S->n, S->k, sell64(S), S->r, S->u, S->w, S->partials, S->counters, S->scalars,
+                S->state, 0x7fffffff);
         count_launch();
         if (cudaGetLastError() != cudaSuccess) st = fail(OB_ERR_CUDA, "ob_pcg_time_matvec: launch");
         cudaEventRecord(end, stream);
@@ -943,6 +1073,7 @@ int ob_pcg_info(void* solver, long long* info) {
     info[2] = S->nnz;
     info[3] = S->narrow;
     info[4] = S->blocks;
+    info[5] = S->sell_entries;
     return OB_OK;
 }
 

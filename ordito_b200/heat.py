@@ -73,11 +73,6 @@ def _heat_method_choices(method: str) -> tuple[str, str]:
 
 def _supported(method: str, use_robust: bool) -> None:
     _heat_method_choices(method)
-    if use_robust and method == "potpourri3d":
-        raise NotImplementedError(
-            "use_robust at method='potpourri3d' (geometry-central's intrinsic tufted cover) is not "
-            "built; 'meshlab' and 'igl' take the mollified half-cotangents"
-        )
 
 
 def _robust_cot(mesh: Trimesh) -> DeviceArray:
@@ -195,6 +190,7 @@ class HeatSolver:
         self.use_robust = use_robust
         self.method = method
         self._operators: HeatOperators | None = None
+        self._cover = None  # the intrinsic tufted cover (use_robust at method="potpourri3d")
         self._resolved: tuple[float | None, int] | None = None
         self._systems: dict[str, Any] = {}
         self._ill_conditioned = False
@@ -233,10 +229,47 @@ class HeatSolver:
 
     @property
     def operators(self) -> HeatOperators:
+        """``heat_operators`` for the mesh at ``t``; at ``method="potpourri3d"`` with
+        ``use_robust``, the same systems on the mesh's intrinsic tufted cover (ordito/heat.py:3651-
+        3663), whose per-face tables are empty: the cover's faces are not the mesh's."""
         if self._operators is None:
             t, _ = self._vertex_time()
-            self._operators, self._built = _assemble(self._mesh, t, self.method, use_robust=self.use_robust)
+            if self.use_robust and self.method == "potpourri3d":
+                self._operators, self._built = self._cover_operators(t)
+            else:
+                self._operators, self._built = _assemble(self._mesh, t, self.method,
+                                                         use_robust=self.use_robust)
         return self._operators
+
+    @property
+    def cover(self) -> Any:
+        """The intrinsic tufted cover the operators are built on (``None`` unless ``use_robust``
+        at ``method="potpourri3d"``)."""
+        if self.use_robust and self.method == "potpourri3d":
+            self.operators  # noqa: B018 -- builds the cover with the operators
+            return self._cover
+        return None
+
+    def _cover_operators(self, t: float | None) -> tuple[HeatOperators, Any]:
+        """geometry-central's ``HeatMethodDistanceSolver`` with ``useRobustLaplacian``
+        (ordito/heat.py:3749-3830): the mass, the Laplacian and the default time's mean edge all
+        from the cover's flipped float64 lengths."""
+        from ordito_b200 import cover as gcover  # noqa: PLC0415
+
+        self._cover, area_sums, edge_sums = gcover.build_cover(self._mesh)
+        built = gcover.cover_rows(self._mesh, self._cover, area_sums, edge_sums, t)
+        empty32 = DeviceArray.empty((0, 3), np.float32)
+        operators = HeatOperators(
+            built.heat,
+            twl.jacobi_preconditioner(built.heat),
+            built.laplacian,
+            built.poisson,
+            twl.chebyshev_preconditioner(built.poisson),
+            empty32,
+            empty32,
+            DeviceArray.empty(0, np.float32),
+        )
+        return operators, built
 
     # -- the vector heat method (ordito/heat.py:3677, 3952-4060) -------------------------------
     def _require_vector_discretization(self, what: str) -> None:
@@ -441,6 +474,11 @@ class HeatSolver:
         (ordito/heat.py:4153-4198): ``(M - t L) u = rhs`` on the interior, ``u = 0`` on every
         vertex with an edge on a single face, settled as ``diffuse``. Returns whether the mesh has
         a rim (without one ``solution`` is left as it was)."""
+        if self.method == "potpourri3d" and self.use_robust:
+            raise ValueError(
+                "HeatSolver.diffuse_pinned: no use_robust variant at method='potpourri3d', whose "
+                "intrinsic cover has no rim"
+            )
         pinned = self._pinned_system()
         if not pinned:
             return False
@@ -650,8 +688,16 @@ def _distance_from_heat(mesh: Trimesh, solver: HeatSolver, sources: DeviceArray,
     solves geometry-central's regularized Poisson system (:3124-3129)."""
     n = mesh.n_vertices
     neg_div = DeviceArray.empty(n * n_columns, np.float64)
-    _divergence(mesh, solver, n_columns, heat.ptr, n_columns, None, neg_div.ptr, n_columns, None,
-                None, DEFAULT_STREAM)
+    cover = solver.cover
+    if cover is not None:
+        # The divergence on the cover, from its lengths (ordito/heat.py:3080-3097): positive, the
+        # same right-hand side as the extrinsic kernel's negated sum.
+        from ordito_b200 import cover as gcover  # noqa: PLC0415
+
+        gcover.cover_divergence(cover, heat, neg_div, n_columns)
+    else:
+        _divergence(mesh, solver, n_columns, heat.ptr, n_columns, None, neg_div.ptr, n_columns, None,
+                    None, DEFAULT_STREAM)
     phi = DeviceArray.zeros(n * n_columns, np.float64)
     if solver.method == "potpourri3d":
         solver.solve_regularized_poisson(neg_div, phi)

@@ -143,5 +143,3 @@ def test_robust_heat_geodesic_matches_the_oracle(gpu, method: str, name: str) ->
     got = gheat.heat_geodesic(v, f.reshape(-1), src, method=method, use_robust=True).numpy()
     assert np.all(np.isfinite(got))
     assert _range_err(got, ref) <= DISTANCE_TOL
-    with pytest.raises(NotImplementedError):
-        gheat.heat_geodesic(v, f.reshape(-1), src, method="potpourri3d", use_robust=True)
