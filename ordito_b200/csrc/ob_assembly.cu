@@ -92,34 +92,52 @@ __global__ void edge_sums_kernel(const int* __restrict__ offsets, const int* __r
 
 // ordito/kernels/heat.py:299-465 (heat_system_rows, scalar_heat_row, scalar_heat_diagonal),
 // kernels/laplacian.py:971-989 (cotmatrix_offdiagonal), kernels/linalg.py:1594-1621
-// (shift_factor, shifted_scalar_entry): one thread per row walks its entries in row order.
-// Row i of L, H = factor L + M and P = -L (and its mass), the one arithmetic of both kernels below.
+// (shift_factor, shifted_scalar_entry).
+// Row i of L, H = factor L + M and P = -L (and its mass), the one arithmetic of both kernels below:
+// each off-diagonal entry the sum of its run's half-cotangents in sorted order, the diagonal minus
+// the row's off-diagonal sum in entry order. A group of kRowLanes lanes takes a row (entries
+// base + lane, base + lane + kRowLanes, ...), so its columns, run starts and L/H/P entries are read
+// and written as one contiguous run per group, where a thread a row would touch a line per entry;
+// every lane of the group folds each chunk's off-diagonal values in entry order through shuffles.
+constexpr int kRowLanes = 8;
+
 template <typename C>
-__device__ __forceinline__ void heat_row(int i, const int* __restrict__ offsets, const int* __restrict__ columns,
-                                         const int* __restrict__ run_start,
-                                         const unsigned long long* __restrict__ keys, int count,
-                                         const int* __restrict__ order, const C* __restrict__ cot,
-                                         double factor, const double* __restrict__ area_sums,
-                                         double mass_divisor, double* __restrict__ L, double* __restrict__ H,
-                                         double* __restrict__ P, double* __restrict__ mass) {
+__device__ __forceinline__ void heat_row_lanes(int i, const int* __restrict__ offsets, const int* __restrict__ columns,
+                                               const int* __restrict__ run_start,
+                                               const unsigned long long* __restrict__ keys, int count,
+                                               const int* __restrict__ order, const C* __restrict__ cot,
+                                               double factor, const double* __restrict__ area_sums,
+                                               double mass_divisor, double* __restrict__ L, double* __restrict__ H,
+                                               double* __restrict__ P, double* __restrict__ mass) {
+    const int lane = threadIdx.x % kRowLanes;
+    const unsigned group = 0xFFu << (threadIdx.x & 31 & ~(kRowLanes - 1));
     const double m = area_sums[i] / mass_divisor;
-    mass[i] = m;
+    if (lane == 0) mass[i] = m;
     const int start = offsets[i], end = offsets[i + 1];
     double total = 0.0;
     int slot = -1;
-    for (int k = start; k < end; ++k) {
-        if (columns[k] == i) {
-            slot = k;
-            continue;
-        }
-        const int s = run_start[k];
-        const int e = run_end(keys, s, count);
+    for (int base = start; base < end; base += kRowLanes) {
+        const int k = base + lane;
         double value = 0.0;
-        for (int p = s; p < e; ++p) value += (double)cot[order[p]];
-        L[k] = value;
-        total += value;
-        H[k] = factor * value;
-        P[k] = -value;
+        int off = 0;
+        if (k < end) {
+            if (columns[k] == i) {
+                slot = k;
+            } else {
+                const int s = run_start[k];
+                const int e = run_end(keys, s, count);
+                for (int p = s; p < e; ++p) value += (double)cot[order[p]];
+                L[k] = value;
+                H[k] = factor * value;
+                P[k] = -value;
+                off = 1;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kRowLanes; ++j) {
+            const double v = __shfl_sync(group, value, j, kRowLanes);
+            if (__shfl_sync(group, off, j, kRowLanes)) total += v;
+        }
     }
     if (slot >= 0) {
         const double diagonal = -total;
@@ -140,7 +158,7 @@ __global__ void heat_rows_kernel(const int* __restrict__ offsets, const int* __r
                                  const double* __restrict__ area_sums, double mass_divisor,
                                  double* __restrict__ L, double* __restrict__ H,
                                  double* __restrict__ P, double* __restrict__ mass) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) / kRowLanes);
     if (i >= n) return;
     double factor = scale;
     if (from_edges) {
@@ -148,8 +166,8 @@ __global__ void heat_rows_kernel(const int* __restrict__ offsets, const int* __r
         if (edge_sums[1] > 0.0) h = edge_sums[0] / edge_sums[1];
         factor = scale * (h * h);
     }
-    heat_row(i, offsets, columns, run_start, keys, count, order, cot, factor, area_sums, mass_divisor,
-             L, H, P, mass);
+    heat_row_lanes(i, offsets, columns, run_start, keys, count, order, cot, factor, area_sums, mass_divisor,
+                   L, H, P, mass);
 }
 
 // Many meshes packed as one block-diagonal operator: each row's own factor (its mesh's -t).
@@ -161,10 +179,10 @@ __global__ void heat_rows_packed_kernel(const int* __restrict__ offsets, const i
                                         const double* __restrict__ area_sums, double mass_divisor,
                                         double* __restrict__ L, double* __restrict__ H,
                                         double* __restrict__ P, double* __restrict__ mass) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) / kRowLanes);
     if (i >= n) return;
-    heat_row(i, offsets, columns, run_start, keys, count, order, cot, row_factor[i], area_sums,
-             mass_divisor, L, H, P, mass);
+    heat_row_lanes(i, offsets, columns, run_start, keys, count, order, cot, row_factor[i], area_sums,
+                   mass_divisor, L, H, P, mass);
 }
 
 // Per segment of rows (a packed mesh): edge_sums_kernel's two sums over its strict upper
@@ -561,7 +579,7 @@ int ob_heat_rows_packed(const int32_t* offsets, const int32_t* columns, const in
     OB_REQUIRE(offsets && columns && run_start && keys && order && cot && row_factor && area_sums && L &&
                    H && P && mass,
                "ob_heat_rows_packed: null pointer");
-    heat_rows_packed_kernel<<<ceil_div(n_vertices, kThreads), kThreads, 0, stream>>>(
+    heat_rows_packed_kernel<<<ceil_div((long long)n_vertices * kRowLanes, kThreads), kThreads, 0, stream>>>(
         offsets, columns, run_start, reinterpret_cast<const unsigned long long*>(keys), count, order,
         n_vertices, cot, row_factor, area_sums, mass_divisor, L, H, P, mass);
     OB_CHECK_LAUNCH("heat_rows_packed");
@@ -579,7 +597,7 @@ int ob_heat_rows(const int32_t* offsets, const int32_t* columns, const int32_t* 
                    P && mass,
                "ob_heat_rows: null pointer");
     OB_REQUIRE(!from_edges || edge_sums != nullptr, "ob_heat_rows: from_edges needs edge_sums");
-    heat_rows_kernel<float><<<ceil_div(n_vertices, kThreads), kThreads, 0, stream>>>(
+    heat_rows_kernel<float><<<ceil_div((long long)n_vertices * kRowLanes, kThreads), kThreads, 0, stream>>>(
         offsets, columns, run_start, reinterpret_cast<const unsigned long long*>(keys), count,
         order, n_vertices, cot, scale, edge_sums, from_edges, area_sums, mass_divisor, L, H, P,
         mass);
@@ -598,7 +616,7 @@ int ob_heat_rows_f64(const int32_t* offsets, const int32_t* columns, const int32
                    P && mass,
                "ob_heat_rows_f64: null pointer");
     OB_REQUIRE(!from_edges || edge_sums != nullptr, "ob_heat_rows_f64: from_edges needs edge_sums");
-    heat_rows_kernel<double><<<ceil_div(n_vertices, kThreads), kThreads, 0, stream>>>(
+    heat_rows_kernel<double><<<ceil_div((long long)n_vertices * kRowLanes, kThreads), kThreads, 0, stream>>>(
         offsets, columns, run_start, reinterpret_cast<const unsigned long long*>(keys), count,
         order, n_vertices, cot, scale, edge_sums, from_edges, area_sums, mass_divisor, L, H, P,
         mass);

@@ -766,49 +766,41 @@ struct Stage {
 
 // One 64 x 64 output tile for a CTA of four warps, each warp a 16-row strip of all 64 columns as
 // 2 x 8 float64 MMA tiles (strips rather than quadrants, so a strip of padding rows, or of the
-// zero triangle of L11^-1 over an inner step, is skipped whole). The tile's matrix block and its gathered input rows are copied 16 inner steps at a
-// time into shared memory with asynchronous 16-byte copies (zero-filled at the edges), two stages:
-// the next step's copies, issued after the step's one barrier, overlap the current step's MMAs. The output is assigned,
-// subtracted, or added atomically per the tile's op. `k` (the column stride) is even and every
-// block row starts on 16 bytes, so every copy is aligned. `in` and `out` are the same stacked
-// work buffer: the rows a launch's tiles read are never rows any tile of that launch writes.
+// zero triangle of L11^-1 over an inner step, is skipped whole). The tile's matrix block and its
+// gathered input rows are copied 16 inner steps at a time into shared memory with asynchronous
+// 16-byte copies (zero-filled at the edges), two stages: the next step's copies, issued after the
+// step's one barrier, overlap the current step's MMAs. The output is assigned, subtracted, or
+// added atomically per the tile's op. `k` (the column stride) is even and every block row starts
+// on 16 bytes, so every copy is aligned. `in` and `out` are the same stacked work buffer: the rows
+// a launch's tiles read are never rows any tile of that launch writes.
 template <int TC>
-__device__ __forceinline__ void tile_product(const Tile& t, int c0, const double* __restrict__ vals,
-                                             const int* __restrict__ idx,
-                                             const double* in, double* out, int k, Stage<TC>* stage) {
-    constexpr int kJ = TC / 8;             // 8-column MMA tiles a warp strip holds
-    constexpr int kLdB = input_ld<TC>();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int wr = warp * 16;                  // the warp's strip: rows [wr, wr + 16), all 64 columns
-    const int fr = lane >> 2, fk = lane & 3;  // fragment coordinates
-    double acc[2][kJ][2];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < kJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-    // Rows of the strip within the block, for its known-zero inner steps.
-    const int row_lo = t.r0 + wr, row_hi = row_lo + 15;
-    const bool live = wr < t.rows;
-    const double* M = vals + t.m;
+struct TileOps {
+    static constexpr int kJ = TC / 8;  // 8-column MMA tiles a warp strip holds
+    static constexpr int kLdB = input_ld<TC>();
     // The matrix block is 64 x kTileK doubles in 16-byte chunks, kChunks per thread; the input
     // block kTileK x TC, kChunksB per thread.
-    constexpr int kChunks = kTileRows * kTileK / 2 / kTileThreads;
-    constexpr int kChunksB = TC * kTileK / 2 / kTileThreads;
-    // The input rows of this thread's chunks of an inner step (-1 past the inner range), read
-    // one step ahead of the copies that use them, so a gathered index's load latency is not
-    // paid in front of every step's copies.
-    auto input_rows = [&](int kb, int* r) {
+    static constexpr int kChunks = kTileRows * kTileK / 2 / kTileThreads;
+    static constexpr int kChunksB = TC * kTileK / 2 / kTileThreads;
+    using Acc = double[2][kJ][2];
+
+    __device__ static int steps(const Tile& t) { return (t.k1 - t.k0 + kTileK - 1) / kTileK; }
+
+    // The input rows of this thread's chunks of the inner step from kb (-1 past the inner range).
+    __device__ static void input_rows(const Tile& t, int kb, const int* __restrict__ idx, int* r) {
 #pragma unroll
         for (int q = 0; q < kChunksB; ++q) {
             const int kk = (threadIdx.x + q * kTileThreads) / (TC / 2);
             r[q] = kb + kk < t.k1 ? (t.in_rows < 0 ? t.in_base + kb + kk : idx[t.in_rows + kb + kk]) : -1;
         }
-    };
-    auto issue = [&](int kb, const int* in_row, Stage<TC>& s) {
+    }
+
+    // Issues (and commits as one group) the copies of the inner step from kb into a stage.
+    __device__ static void issue(const Tile& t, int c0, int kb, const int* in_row, const double* __restrict__ vals,
+                                 const double* in, int k, Stage<TC>& s) {
+        const double* M = vals + t.m;
 #pragma unroll
         for (int q = 0; q < kChunks; ++q) {
             const int chunk = threadIdx.x + q * kTileThreads;
-            // Matrix block.
             if (t.trans) {
                 // Row kk of the stored matrix, elements r0 + 2 c .. + 1: k-major staging.
                 const int kk = chunk / (kTileRows / 2), c2 = 2 * (chunk % (kTileRows / 2));
@@ -837,76 +829,111 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
             copy16_l2(&s.b[kk * kLdB + c2], src, valid);
         }
         copy_commit();
-    };
-    const int steps = (t.k1 - t.k0 + kTileK - 1) / kTileK;
-    int first_rows[kChunksB], next_rows[kChunksB];
-    input_rows(t.k0, first_rows);
-    issue(t.k0, first_rows, stage[0]);
-    if (steps > 1) input_rows(t.k0 + kTileK, next_rows);
+    }
+
+    // The output rows of this thread's accumulator rows (-1 past the tile).
+    __device__ static void output_rows(const Tile& t, const int* __restrict__ idx, int* out_row) {
+        const int lane = threadIdx.x & 31, wr = (threadIdx.x >> 5) * 16;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int local = wr + 8 * i + (lane >> 2);
+            out_row[i] = local >= t.rows ? -1
+                         : (t.out_rows < 0 ? t.out_base + t.r0 + local : idx[t.out_rows + t.r0 + local]);
+        }
+    }
+
+    // The MMAs of the inner step from kb out of its stage. A strip skips a whole inner step when
+    // all its products are known zeros: padding rows past the tile, or the zero triangle of
+    // L11^-1 (the decision is warp-uniform and taken outside the unrolled step, which stays
+    // branch-free).
+    __device__ static void compute(const Tile& t, int kb, const Stage<TC>& s, Acc& acc) {
+        const int lane = threadIdx.x & 31, wr = (threadIdx.x >> 5) * 16;
+        const int fr = lane >> 2, fk = lane & 3;  // fragment coordinates
+        const int row_lo = t.r0 + wr, row_hi = row_lo + 15;
+        const bool zero = wr >= t.rows || (t.tri == 1 && kb > row_hi) ||
+                          (t.tri == 2 && kb + kTileK - 1 < row_lo && kb + kTileK - 1 < t.tri_k);
+        if (zero) return;
+#pragma unroll
+        for (int k4 = 0; k4 < kTileK; k4 += 4) {
+            double a[2], b[kJ];
+            if (t.trans) {
+#pragma unroll
+                for (int i = 0; i < 2; ++i) a[i] = s.a[(k4 + fk) * kLd + wr + 8 * i + fr];
+            } else {
+#pragma unroll
+                for (int i = 0; i < 2; ++i) a[i] = s.a[(wr + 8 * i + fr) * kLdK + k4 + fk];
+            }
+#pragma unroll
+            for (int j = 0; j < kJ; ++j) b[j] = s.b[(k4 + fk) * kLdB + 8 * j + fr];
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < kJ; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        }
+    }
+
+    __device__ static void clear(Acc& acc) {
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < kJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    }
+
+    // Applies the tile's op to its outputs.
+    __device__ static void store(const Tile& t, int c0, const int* out_row, double* out, int k, const Acc& acc) {
+        const int fk = threadIdx.x & 3;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int r = out_row[i];
+            if (r < 0) continue;
+#pragma unroll
+            for (int j = 0; j < kJ; ++j)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int c = c0 + 8 * j + 2 * fk + h;
+                    if (c >= k) continue;
+                    double* o = out + (size_t)r * k + c;
+                    const double v = acc[i][j][h];
+                    switch (t.op) {
+                        case kAssign: *o = v; break;
+                        case kAtomicSub: atomicAdd(o, -v); break;
+                        case kSub: *o = __ldcg(o) - v; break;
+                        default: atomicAdd(o, v); break;
+                    }
+                }
+        }
+    }
+};
+
+template <int TC>
+__device__ __forceinline__ void tile_product(const Tile& t, int c0, const double* __restrict__ vals,
+                                             const int* __restrict__ idx,
+                                             const double* in, double* out, int k, Stage<TC>* stage) {
+    using Ops = TileOps<TC>;
+    typename Ops::Acc acc;
+    Ops::clear(acc);
+    const int steps = Ops::steps(t);
+    // The input rows of a step's chunks are read one step ahead of the copies that use them, so
+    // a gathered index's load latency is not paid in front of every step's copies.
+    int first_rows[Ops::kChunksB], next_rows[Ops::kChunksB];
+    Ops::input_rows(t, t.k0, idx, first_rows);
+    Ops::issue(t, c0, t.k0, first_rows, vals, in, k, stage[0]);
+    if (steps > 1) Ops::input_rows(t, t.k0 + kTileK, idx, next_rows);
     // The output rows, read before the products so the epilogue does not wait on them.
     int out_row[2];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-        const int local = wr + 8 * i + fr;
-        out_row[i] = local >= t.rows ? -1
-                     : (t.out_rows < 0 ? t.out_base + t.r0 + local : idx[t.out_rows + t.r0 + local]);
-    }
+    Ops::output_rows(t, idx, out_row);
     for (int st = 0; st < steps; ++st) {
         copy_wait<0>();
         // Every thread's copies of step st have landed, and every warp is past the products of
         // step st - 1, whose stage the next copies reuse: one barrier a step.
         __syncthreads();
         if (st + 1 < steps) {
-            issue(t.k0 + (st + 1) * kTileK, next_rows, stage[(st + 1) & 1]);
-            if (st + 2 < steps) input_rows(t.k0 + (st + 2) * kTileK, next_rows);
+            Ops::issue(t, c0, t.k0 + (st + 1) * kTileK, next_rows, vals, in, k, stage[(st + 1) & 1]);
+            if (st + 2 < steps) Ops::input_rows(t, t.k0 + (st + 2) * kTileK, idx, next_rows);
         }
-        const Stage<TC>& s = stage[st & 1];
-        // A strip skips a whole inner step when all its products are known zeros: padding rows
-        // past the tile, or the zero triangle of L11^-1 (the decision is warp-uniform and taken
-        // outside the unrolled step, which stays branch-free).
-        const int kb = t.k0 + st * kTileK;
-        const bool zero = !live || (t.tri == 1 && kb > row_hi) ||
-                          (t.tri == 2 && kb + kTileK - 1 < row_lo && kb + kTileK - 1 < t.tri_k);
-        if (!zero) {
-#pragma unroll
-            for (int k4 = 0; k4 < kTileK; k4 += 4) {
-                double a[2], b[kJ];
-                if (t.trans) {
-#pragma unroll
-                    for (int i = 0; i < 2; ++i) a[i] = s.a[(k4 + fk) * kLd + wr + 8 * i + fr];
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 2; ++i) a[i] = s.a[(wr + 8 * i + fr) * kLdK + k4 + fk];
-                }
-#pragma unroll
-                for (int j = 0; j < kJ; ++j) b[j] = s.b[(k4 + fk) * kLdB + 8 * j + fr];
-#pragma unroll
-                for (int i = 0; i < 2; ++i)
-#pragma unroll
-                    for (int j = 0; j < kJ; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
-            }
-        }
+        Ops::compute(t, t.k0 + st * kTileK, stage[st & 1], acc);
     }
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-        const int r = out_row[i];
-        if (r < 0) continue;
-#pragma unroll
-        for (int j = 0; j < kJ; ++j)
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int c = c0 + 8 * j + 2 * fk + h;
-                if (c >= k) continue;
-                double* o = out + (size_t)r * k + c;
-                const double v = acc[i][j][h];
-                switch (t.op) {
-                    case kAssign: *o = v; break;
-                    case kAtomicSub: atomicAdd(o, -v); break;
-                    case kSub: *o = __ldcg(o) - v; break;
-                    default: atomicAdd(o, v); break;
-                }
-            }
-    }
+    Ops::store(t, c0, out_row, out, k, acc);
 }
 
 // The two stages live in dynamic shared memory (stage_bytes, above the 48 KB static limit).

@@ -44,6 +44,24 @@ def test_pattern_is_bit_exact(gpu, name: str) -> None:
     assert np.array_equal(order[in_face], ref["order"][in_face])
 
 
+def test_pattern_of_a_high_degree_vertex_is_bit_exact(gpu) -> None:
+    # A fan of 600 triangles around one vertex: its row holds 1201 keys (each rim edge both ways
+    # and the diagonal), far past the short rows of a mesh.
+    rim = 600
+    angle = np.linspace(0.0, 2.0 * np.pi, rim, endpoint=False)
+    v = np.vstack([[0.0, 0.0, 0.0], np.column_stack([np.cos(angle), np.sin(angle), np.zeros(rim)])])
+    f = np.array([[0, 1 + i, 1 + (i + 1) % rim] for i in range(rim)], dtype=np.int32)
+    n = v.shape[0]
+    ref = hp.mesh_operator_pattern(f, n)
+    got = glap.mesh_operator_pattern(f.reshape(-1), n)
+    nnz = int(ref["offsets"][-1])
+    assert np.array_equal(got.offsets.numpy(), ref["offsets"])
+    assert np.array_equal(got.columns.numpy()[:nnz], ref["columns"])
+    assert np.array_equal(got.run_start.numpy()[:nnz], ref["run_start"])
+    assert np.array_equal(got.keys.numpy(), ref["keys"])
+    assert np.array_equal(got.order.numpy(), ref["order"])
+
+
 @pytest.mark.parametrize("name", sorted(meshes.ALL))
 def test_face_terms_and_operators(gpu, name: str) -> None:
     v, f = meshes.ALL[name]()
