@@ -398,11 +398,12 @@ class HeatSolver:
     def tune(self, k: int) -> dict:
         """Tune both factors' pass schedules for batches of ``k`` columns (``tuning.tune_pass``);
         factors them first if needed. Returns each system's tuning report."""
-        from ordito_b200.tuning import tune_pass  # noqa: PLC0415
+        from ordito_b200.tuning import tune_shared  # noqa: PLC0415
 
         if not self.factor():
             raise RuntimeError("HeatSolver.tune: the systems could not be factored (over budget)")
-        return {"heat": tune_pass(self.heat_factor, k), "poisson": tune_pass(self.poisson_factor, k)}
+        # The two factors share the heat system's analysis: one search serves both (tune_shared).
+        return tune_shared({"heat": self.heat_factor, "poisson": self.poisson_factor}, k)
 
     def single_query(self, sources: DeviceArray) -> DeviceArray:
         """Distances for one validated source set with both factors held (``_SingleQuery``)."""

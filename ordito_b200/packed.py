@@ -98,10 +98,12 @@ class PackedMeshes:
         self.heat_factor = SparseCholesky(self.heat_system, self.analysis, singular=False)
         self.poisson_factor = SparseCholesky(self.poisson_system, self.analysis, singular=True)
         # The passes' tile schedule tuned to the union's tree at the batch width.
-        from ordito_b200.tuning import tune_pass  # noqa: PLC0415
+        from ordito_b200.tuning import tune_shared  # noqa: PLC0415
 
-        self.tuning = {"heat": tune_pass(self.heat_factor, max_columns),
-                       "poisson": tune_pass(self.poisson_factor, max_columns)}
+        # Both factors share the union's analysis: one search (five timed passes a candidate: a
+        # packed pass takes milliseconds) serves both.
+        self.tuning = tune_shared({"heat": self.heat_factor, "poisson": self.poisson_factor}, max_columns,
+                                  reps=5)
         # a8: the divergence's corner index and per-face terms over the union.
         self.corner_offsets = DeviceArray.empty(n + 1, np.int32)
         self.corner_slots = DeviceArray.empty(max(3 * self.n_faces, 1), np.int32)

@@ -13,7 +13,10 @@ level sizes and separator widths -- and on the batch width:
 
 ``tune_pass`` times one pass of a factor at ``k`` columns (CUDA events, ``ob_chol_time_solve``)
 for each candidate split schedule, then, under the fastest, for each candidate width rule, keeps
-the fastest of all and reports every candidate's time.
+the fastest of all and reports every candidate's time. ``tune_shared`` tunes one factor and gives
+its schedule to the factors sharing its analysis: the heat and Poisson factors of a mesh have one
+supernodal tree and one block layout, so their passes are the same launches over different values
+(the tuner's timings of the two differ by noise) and one search serves both.
 """
 
 from __future__ import annotations
@@ -38,6 +41,24 @@ def _time(factor: Any, k: int, reps: int) -> float:
     _lib.call("ob_chol_time_solve", factor.handle, int(k), 2, ctypes.byref(ms), None)  # warm
     _lib.call("ob_chol_time_solve", factor.handle, int(k), int(reps), ctypes.byref(ms), None)
     return float(ms.value)
+
+
+def apply_schedule(factor: Any, report: dict) -> None:
+    """Give ``factor`` the schedule ``tune_pass`` chose for a factor of the same analysis."""
+    _lib.call("ob_chol_tile", factor.handle, int(report["best"][0]), int(report["best"][1]), None)
+    _lib.call("ob_chol_tile_columns", factor.handle, int(report["narrow_waves"]), None)
+
+
+def tune_shared(factors: dict[str, Any], k: int, *, reps: int = 10) -> dict:
+    """Tune the first of ``factors`` (role -> factor, all of one analysis) and apply its schedule
+    to the others; every role's entry is the first's report, the others marked ``shared``."""
+    roles = list(factors)
+    report = tune_pass(factors[roles[0]], k, reps=reps)
+    out = {roles[0]: report}
+    for role in roles[1:]:
+        apply_schedule(factors[role], report)
+        out[role] = dict(report, shared=roles[0])
+    return out
 
 
 def tune_pass(factor: Any, k: int, *, reps: int = 10,
