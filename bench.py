@@ -551,11 +551,20 @@ def kernel_rooflines(mesh, solver, columns: int = 64, reps: int = 10) -> dict:
                             corner_slots.ptr, n, columns, u.ptr, columns, None, div.ptr, columns,
                             None, None, None),
           "per-corner form: per-face terms, faces and corner index in, u in and -div out (float64)")
+    from ordito_b200.heat import corner_records
+
+    records, ids = corner_records(terms, mesh.faces, corner_slots, f)
+    timed("grad_div_records", 144 * f + 12 * f + 4 * (n + 1) + 12 * f + 2 * 8 * n * columns,
+          lambda: _lib.call("ob_grad_div_records", records.ptr, ids.ptr, corner_offsets.ptr, n, columns, u.ptr,
+                            columns, None, div.ptr, columns, None, None, None),
+          "corner-record form (the served pass's): the per-corner form's algorithmic bytes (the records "
+          "themselves hold 336 B a face against the terms' 144), u in and -div out (float64)")
+    del records, ids
     timed("grad_div_tiled", 144 * f + 12 * f + 4 * (n + 1) + 2 * 12 * f + 2 * 8 * n * columns,
           lambda: _lib.call("ob_grad_div_tiled", terms.ptr, mesh.faces.ptr, corner_offsets.ptr,
                             corner_slots.ptr, tile_faces.ptr, tile_counts.ptr, codes.ptr, n, columns,
                             u.ptr, columns, None, div.ptr, columns, None, None, None),
-          "face-major form (the path's): per-face terms, faces, corner index, tile lists and corner "
+          "face-major form (built, off): per-face terms, faces, corner index, tile lists and corner "
           "codes in, u in and -div out (float64)")
 
     # a13: the shift of `columns` fields to their sources, written transposed.

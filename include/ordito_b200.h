@@ -387,6 +387,17 @@ int ob_grad_div_terms(const double* terms, const int32_t* faces, const int32_t* 
                       const int32_t* corner_slots, int n_vertices, int n_columns, const double* u,
                       int u_stride, const int32_t* u_iperm, double* out, int out_stride,
                       const int32_t* out_iperm, const char* out_pinned, ob_stream_t stream);
+/* ob_corner_records / ob_grad_div_records: ob_grad_div_terms over corner records (no reference
+ * counterpart: a layout of the same arithmetic). Set-up, once per face buffer and corner index:
+ * records[3 F][12] float64, corner p's twelve terms (its face's gradient bases a, b, w and its
+ * W_e) for corner_slots[p], and ids[3 F][4] int32, that face's three vertices (and a zero), both
+ * 16-byte aligned. ob_grad_div_records then takes ob_grad_div_terms' arguments with the records,
+ * ids and corner offsets in place of the terms, faces and corner index, and returns its bits. */
+int ob_corner_records(const double* terms, const int32_t* faces, const int32_t* corner_slots, int n_faces,
+                      double* records, int32_t* ids, ob_stream_t stream);
+int ob_grad_div_records(const double* records, const int32_t* ids, const int32_t* corner_offsets, int n_vertices,
+                        int n_columns, const double* u, int u_stride, const int32_t* u_iperm, double* out,
+                        int out_stride, const int32_t* out_iperm, const char* out_pinned, ob_stream_t stream);
 /* ob_divergence_tiles / ob_grad_div_tiled: ob_grad_div_terms face by face over tiles of 32
  * consecutive vertices (no reference counterpart: a layout of the same arithmetic). Set-up, once
  * per face buffer and corner index: tile_faces[3 F] (each tile's distinct faces, stored over the

@@ -145,6 +145,8 @@ SIGNATURES: dict[str, list] = {
     "ob_grad_div_gather": [P, P, P, P, P, P, P, I, I, P, I, P, P, I, P, P, P],
     "ob_face_gradient_terms": [P, P, I, P, P, P, P, P],
     "ob_grad_div_terms": [P, P, P, P, I, I, P, I, P, P, I, P, P, P],
+    "ob_corner_records": [P, P, P, I, P, P, P],
+    "ob_grad_div_records": [P, P, P, I, I, P, I, P, P, I, P, P, P],
     "ob_seed_permuted": [P, P, I, I, P, P, I, P, P],
     "ob_shift_permuted": [P, I, I, P, P, P, I, I, P, P],
     "ob_chol_time_solve": [P, I, I, POINTER(c_float), P],

@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "ob_chol.cuh"
+#include "ob_host.hpp"
 #include "ob_scratch.cuh"
 
 namespace ob {
@@ -165,18 +166,21 @@ int build_plan(const CholAnalysis& A, FactorPlan* P, cudaStream_t stream) {
     std::vector<long long> entry_dest(nnz, -1);
     std::vector<int2> entry_rc(nnz);
     std::vector<int> diag_pos(n, -1);
-    for (int ro = 0; ro < n; ++ro) {
-        const int j = A.iperm[ro];
-        const int s = node_of[j];
-        for (int e = A.offsets[ro]; e < A.offsets[ro + 1]; ++e) {
-            const int co = A.columns[e];
-            const int r = A.iperm[co];
-            entry_rc[e] = make_int2(j, r);
-            if (co == ro) diag_pos[ro] = e;
-            if (r < j) continue;
-            entry_dest[e] = front_at[s] + (long long)(j - A.nodes[s].start) * fld[s] + local(s, r);
+    // Rows on host threads: each writes only its own entries and its own diagonal position.
+    parallel_range(n, nnz > (1LL << 18), [&](long long lo, long long hi) {
+        for (int ro = (int)lo; ro < (int)hi; ++ro) {
+            const int j = A.iperm[ro];
+            const int s = node_of[j];
+            for (int e = A.offsets[ro]; e < A.offsets[ro + 1]; ++e) {
+                const int co = A.columns[e];
+                const int r = A.iperm[co];
+                entry_rc[e] = make_int2(j, r);
+                if (co == ro) diag_pos[ro] = e;
+                if (r < j) continue;
+                entry_dest[e] = front_at[s] + (long long)(j - A.nodes[s].start) * fld[s] + local(s, r);
+            }
         }
-    }
+    });
     std::vector<long long> diag_dest(n);
     for (int i = 0; i < n; ++i) {
         const int s = node_of[i];

@@ -264,6 +264,102 @@ __global__ void __launch_bounds__(256, CP == 4 ? 4 : 1) grad_div_terms_kernel(co
     }
 }
 
+// ---- The divergence over corner records ----------------------------------------------------
+// The per-corner form above reads, at each corner, its slot, its face's three vertices and twelve
+// of the face's eighteen terms through that slot: 16 loads a corner, each behind the slot's. The
+// records copy, once per face buffer and corner index, each corner's twelve terms (the face's
+// gradient bases a, b, w and the corner's W_e) into 96 contiguous bytes and its face's vertices
+// into an int4, both in the corner index's order: a vertex's corners are then consecutive records,
+// read as six 16-byte loads and one (no slot indirection). The arithmetic and the corner order are
+// the per-corner form's, so the results are its bits.
+constexpr int kRecordPairs = 6;  // double2 a record: a0 a1 | a2 b0 | b1 b2 | w0 w1 | w2 W0 | W1 W2
+
+__global__ void corner_records_kernel(const double* __restrict__ terms, const int* __restrict__ faces,
+                                      const int* __restrict__ corner_slots, long long n_corners,
+                                      double2* __restrict__ records, int4* __restrict__ ids) {
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= n_corners) return;
+    const int q = corner_slots[p];
+    const int f = q / 3, e = q - 3 * f;
+    const double* T = terms + (size_t)kFaceTerms * f;
+    const double* W = T + 9 + 3 * e;
+    double2* R = records + (size_t)kRecordPairs * p;
+    R[0] = make_double2(T[0], T[1]);
+    R[1] = make_double2(T[2], T[3]);
+    R[2] = make_double2(T[4], T[5]);
+    R[3] = make_double2(T[6], T[7]);
+    R[4] = make_double2(T[8], W[0]);
+    R[5] = make_double2(W[1], W[2]);
+    ids[p] = make_int4(faces[3 * f], faces[3 * f + 1], faces[3 * f + 2], 0);
+}
+
+template <int CP>
+__global__ void __launch_bounds__(256, CP == 4 ? 4 : 1)
+grad_div_records_kernel(const double2* __restrict__ records, const int4* __restrict__ ids,
+                        const int* __restrict__ corner_offsets, int n, int k, const double* __restrict__ u,
+                        int u_stride, const int* __restrict__ u_iperm, double* __restrict__ out, int out_stride,
+                        const int* __restrict__ out_iperm, const char* __restrict__ out_pinned) {
+    const int groups = out_stride / CP;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)n * groups) return;
+    const int v = (int)(t / groups), c0 = (int)(t % groups) * CP;
+    const int row = row_of(out_iperm, v);
+    double acc[CP];
+#pragma unroll
+    for (int j = 0; j < CP; ++j) acc[j] = 0.0;
+    auto load = [&](int r, double* dst) {
+        const double* src = u + (size_t)r * u_stride + c0;
+        if (CP == 1) {
+            dst[0] = src[0];
+        } else {
+#pragma unroll
+            for (int j = 0; j < CP; j += 2) {
+                // A pair starting below k lies inside the row (even strides).
+                const double2 p = (c0 + j < k) ? *reinterpret_cast<const double2*>(src + j) : make_double2(0.0, 0.0);
+                dst[j] = p.x;
+                dst[j + 1] = p.y;
+            }
+        }
+    };
+    if (c0 < k) {
+        const int end = corner_offsets[v + 1];
+        for (int p = corner_offsets[v]; p < end; ++p) {
+            const int4 id = ids[p];
+            double u0[CP], u1[CP], u2[CP];
+            load(row_of(u_iperm, id.x), u0);
+            load(row_of(u_iperm, id.y), u1);
+            load(row_of(u_iperm, id.z), u2);
+            const double2* R = records + (size_t)kRecordPairs * p;
+            const double2 r0 = R[0], r1 = R[1], r2 = R[2], r3 = R[3], r4 = R[4], r5 = R[5];
+            const double a0 = r0.x, a1 = r0.y, a2 = r1.x, b0 = r1.y, b1 = r2.x, b2 = r2.y;
+            const double w0 = r3.x, w1 = r3.y, w2 = r4.x, W0 = r4.y, W1 = r5.x, W2 = r5.y;
+#pragma unroll
+            for (int j = 0; j < CP; ++j) {
+                const double gx = fma(u0[j], a0, fma(u1[j], b0, u2[j] * w0));
+                const double gy = fma(u0[j], a1, fma(u1[j], b1, u2[j] * w1));
+                const double gz = fma(u0[j], a2, fma(u1[j], b2, u2[j] * w2));
+                const double largest = fmax(fabs(gx), fmax(fabs(gy), fabs(gz)));
+                if (largest == 0.0) continue;  // no gradient: the unit gradient is zero
+                const double scale = inverse_power_of_two(largest);
+                const double sx = gx * scale, sy = gy * scale, sz = gz * scale;
+                const double along = fma(sx, W0, fma(sy, W1, sz * W2));
+                acc[j] += along * rsqrt(fma(sx, sx, fma(sy, sy, sz * sz)));
+            }
+        }
+    }
+    const bool pinned = out_pinned && out_pinned[row];
+    double* o = out + (size_t)row * out_stride + c0;
+#pragma unroll
+    for (int j = 0; j < CP; ++j)
+        if (pinned || c0 + j >= k) acc[j] = 0.0;
+    if (CP == 1) {
+        o[0] = acc[0];
+    } else {
+#pragma unroll
+        for (int j = 0; j < CP; j += 2) *reinterpret_cast<double2*>(o + j) = make_double2(acc[j], acc[j + 1]);
+    }
+}
+
 // ---- The divergence face by face over tiles of vertices ------------------------------------
 // The per-corner form above recomputes a face's unit gradient at each of its three corners. Here
 // a CTA takes kTileVertices consecutive vertices, forms the unit gradient of each distinct face
@@ -694,6 +790,54 @@ int ob_grad_div_terms(const double* terms, const int32_t* faces, const int32_t* 
                                                                   n_vertices, n_columns, u, u_stride, u_iperm,
                                                                   out, out_stride, out_iperm, out_pinned);
     OB_CHECK_LAUNCH("grad_div_terms");
+    return OB_OK;
+}
+
+int ob_corner_records(const double* terms, const int32_t* faces, const int32_t* corner_slots, int n_faces,
+                      double* records, int32_t* ids, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_faces >= 0, "ob_corner_records: bad size");
+    if (n_faces == 0) return OB_OK;
+    OB_REQUIRE(terms && faces && corner_slots && records && ids, "ob_corner_records: null pointer");
+    OB_REQUIRE(((uintptr_t)records & 15) == 0 && ((uintptr_t)ids & 15) == 0,
+               "ob_corner_records: records and ids must start on 16 bytes");
+    const long long corners = 3LL * n_faces;
+    corner_records_kernel<<<ceil_div(corners, kThreads), kThreads, 0, stream>>>(
+        terms, faces, corner_slots, corners, reinterpret_cast<double2*>(records), reinterpret_cast<int4*>(ids));
+    OB_CHECK_LAUNCH("corner_records");
+    return OB_OK;
+}
+
+int ob_grad_div_records(const double* records, const int32_t* ids, const int32_t* corner_offsets, int n_vertices,
+                        int n_columns, const double* u, int u_stride, const int32_t* u_iperm, double* out,
+                        int out_stride, const int32_t* out_iperm, const char* out_pinned, ob_stream_t stream_) {
+    cudaStream_t stream = as_stream(stream_);
+    OB_REQUIRE(n_vertices >= 0 && n_columns >= 1 && u_stride >= n_columns && out_stride >= n_columns,
+               "ob_grad_div_records: bad size");
+    if (n_vertices == 0) return OB_OK;
+    OB_REQUIRE(records && ids && corner_offsets && u && out, "ob_grad_div_records: null pointer");
+    OB_REQUIRE(((uintptr_t)records & 15) == 0 && ((uintptr_t)ids & 15) == 0,
+               "ob_grad_div_records: records and ids must start on 16 bytes");
+    const bool paired = u_stride % 2 == 0 && out_stride % 2 == 0 && ((uintptr_t)u & 15) == 0 &&
+                        ((uintptr_t)out & 15) == 0;
+    const int cp = !paired ? 1 : (out_stride % 4 == 0 ? 4 : 2);
+    const long long total = (long long)n_vertices * (out_stride / cp);
+    const int blocks = (int)ceil_div(total, kThreads);
+    const double2* R = reinterpret_cast<const double2*>(records);
+    const int4* I = reinterpret_cast<const int4*>(ids);
+    if (cp == 4)
+        grad_div_records_kernel<4><<<blocks, kThreads, 0, stream>>>(R, I, corner_offsets, n_vertices, n_columns, u,
+                                                                    u_stride, u_iperm, out, out_stride, out_iperm,
+                                                                    out_pinned);
+    else if (cp == 2)
+        grad_div_records_kernel<2><<<blocks, kThreads, 0, stream>>>(R, I, corner_offsets, n_vertices, n_columns, u,
+                                                                    u_stride, u_iperm, out, out_stride, out_iperm,
+                                                                    out_pinned);
+    else
+        grad_div_records_kernel<1><<<blocks, kThreads, 0, stream>>>(R, I, corner_offsets, n_vertices, n_columns, u,
+                                                                    u_stride, u_iperm, out, out_stride, out_iperm,
+                                                                    out_pinned);
+    OB_CHECK_LAUNCH("grad_div_records");
     return OB_OK;
 }
 

@@ -609,6 +609,18 @@ def divergence_tiles(corner_offsets: DeviceArray, corner_slots: DeviceArray, n: 
     return tile_faces, tile_counts, corner_codes
 
 
+def corner_records(terms: DeviceArray, faces: DeviceArray, corner_slots: DeviceArray,
+                   n_faces: int) -> tuple[DeviceArray, DeviceArray]:
+    """``(records, ids)`` of a corner index (``ob_corner_records``): each corner's twelve divergence
+    terms and its face's vertices, in the index's order, for ``ob_grad_div_records``."""
+    corners = max(3 * n_faces, 1)
+    records = DeviceArray.empty(12 * corners, np.float64)
+    ids = DeviceArray.empty(4 * corners, np.int32)
+    _lib.call("ob_corner_records", terms.ptr, faces.ptr, corner_slots.ptr, n_faces, records.ptr, ids.ptr,
+              DEFAULT_STREAM)
+    return records, ids
+
+
 def _grad_div(solver: "HeatSolver", faces: DeviceArray, index: tuple, n: int, k: int, u: int,
               u_stride: int, u_iperm: Any, out: int, out_stride: int, out_iperm: Any, out_pinned: Any,
               stream: Any) -> None:
@@ -647,12 +659,13 @@ def _divergence(mesh: Trimesh, solver: "HeatSolver", k: int, u: int, u_stride: i
 
 
 def _corners_in_factor_rows(mesh: Trimesh, solver: "HeatSolver", h_iperm: int,
-                            p_iperm: int) -> tuple[DeviceArray, DeviceArray, DeviceArray] | None:
+                            p_iperm: int) -> tuple[DeviceArray, tuple, tuple] | None:
     """The face buffer and the corner index renumbered into the factors' shared ordering (built
-    once per solver and ordering, outside any recording: the first eager pass builds it), so
-    the served divergence reads the heat rows and writes the Poisson rows with no inverse
-    permutation per corner; None when the two factors' orderings differ. A vertex's corners keep
-    their ascending slot order, so the sums are the same bits as in the vertex numbering."""
+    once per solver and ordering, outside any recording: the first eager pass builds it), with
+    the index's corner records (``corner_records``), so the served divergence reads the heat rows
+    and writes the Poisson rows with no inverse permutation per corner; None when the two
+    factors' orderings differ. A vertex's corners keep their ascending slot order, so the sums
+    are the same bits as in the vertex numbering."""
     # Kept on the heat factor (its lifetime is the ordering's), keyed by both orderings.
     holder = solver.heat_factor
     key = (h_iperm, p_iperm, id(solver.poisson_factor))
@@ -676,8 +689,9 @@ def _corners_in_factor_rows(mesh: Trimesh, solver: "HeatSolver", h_iperm: int,
         _lib.call("ob_corner_index", faces.ptr, mesh.n_faces, n, offsets.ptr, slots.ptr,
                   workspace.ptr, int(size.value), DEFAULT_STREAM)
         tiles = divergence_tiles(offsets, slots, n, mesh.n_faces)
+        records = corner_records(solver.gradient_terms, faces, slots, mesh.n_faces)
         _lib.call("ob_stream_synchronize", DEFAULT_STREAM)  # the arrays serve other streams
-        result = (faces, (offsets, slots) + tiles)
+        result = (faces, (offsets, slots) + tiles, records)
     holder._factor_row_corners = (key, result)
     return result
 
@@ -842,9 +856,9 @@ def _batch_columns(mesh: Trimesh, solver: "HeatSolver", src: DeviceArray, offset
             _divergence(mesh, solver, k, h_sol, h_stride, h_iperm, p_rhs, p_stride, p_iperm,
                         p_pinned, st)
         else:
-            faces_rows, index = rows
-            _grad_div(solver, faces_rows, index, n, k, h_sol, h_stride, None, p_rhs, p_stride, None,
-                      p_pinned, st)
+            _, index, (records, ids) = rows
+            _lib.call("ob_grad_div_records", records.ptr, ids.ptr, index[0].ptr, n, k, h_sol, h_stride, None,
+                      p_rhs, p_stride, None, p_pinned, st)
         poisson_factor.solve_in_place(k, st, work_set)
         if out is None:
             out = DeviceArray.empty((k, n), np.float64)

@@ -173,6 +173,15 @@ def test_divergence_from_face_terms(gpu, k: int) -> None:
     assert np.array_equal(tiled[0], tiled[1])
     assert np.array_equal(tiled[0], tiled[2])
     assert np.allclose(tiled[0], outs[0], rtol=1e-13, atol=1e-13 * np.abs(outs[0]).max())
+    # Over corner records: the per-corner form's arithmetic in its corner order, so its bits.
+    from ordito_b200.heat import corner_records
+
+    records, ids = corner_records(table, mesh.faces, slots, mesh.n_faces)
+    for field, expected in ((u, outs[0]), (tiny, outs[2])):
+        out = DeviceArray.empty(n * k, np.float64)
+        _lib.call("ob_grad_div_records", records.ptr, ids.ptr, offsets.ptr, n, k, field.ptr, k, None, out.ptr, k,
+                  None, None, None)
+        assert np.array_equal(out.numpy(), expected)
 
 
 def test_tiled_divergence_on_a_crowded_fan(gpu) -> None:
