@@ -906,19 +906,29 @@ struct TileOps {
 };
 
 template <int TC>
-__device__ __forceinline__ void tile_product(const Tile& t, int c0, const double* __restrict__ vals,
+__device__ __forceinline__ void tile_product(const Tile& t, int k0, int c0, const double* __restrict__ vals,
                                              const int* __restrict__ idx,
                                              const double* in, double* out, int k, Stage<TC>* stage) {
     using Ops = TileOps<TC>;
     typename Ops::Acc acc;
     Ops::clear(acc);
-    const int steps = Ops::steps(t);
+    // Inner steps from k0 (the tile's own, or past a zero Y block: first_inner).
+    const int steps = (t.k1 - k0 + kTileK - 1) / kTileK;
+    if (steps <= 0) {
+        // Nothing to multiply: an assigned output is zero, an accumulated one unchanged.
+        if (t.op == kAssign) {
+            int rows_out[2];
+            Ops::output_rows(t, idx, rows_out);
+            Ops::store(t, c0, rows_out, out, k, acc);
+        }
+        return;
+    }
     // The input rows of a step's chunks are read one step ahead of the copies that use them, so
     // a gathered index's load latency is not paid in front of every step's copies.
     int first_rows[Ops::kChunksB], next_rows[Ops::kChunksB];
-    Ops::input_rows(t, t.k0, idx, first_rows);
-    Ops::issue(t, c0, t.k0, first_rows, vals, in, k, stage[0]);
-    if (steps > 1) Ops::input_rows(t, t.k0 + kTileK, idx, next_rows);
+    Ops::input_rows(t, k0, idx, first_rows);
+    Ops::issue(t, c0, k0, first_rows, vals, in, k, stage[0]);
+    if (steps > 1) Ops::input_rows(t, k0 + kTileK, idx, next_rows);
     // The output rows, read before the products so the epilogue does not wait on them.
     int out_row[2];
     Ops::output_rows(t, idx, out_row);
@@ -928,10 +938,10 @@ __device__ __forceinline__ void tile_product(const Tile& t, int c0, const double
         // step st - 1, whose stage the next copies reuse: one barrier a step.
         __syncthreads();
         if (st + 1 < steps) {
-            Ops::issue(t, c0, t.k0 + (st + 1) * kTileK, next_rows, vals, in, k, stage[(st + 1) & 1]);
-            if (st + 2 < steps) Ops::input_rows(t, t.k0 + (st + 2) * kTileK, idx, next_rows);
+            Ops::issue(t, c0, k0 + (st + 1) * kTileK, next_rows, vals, in, k, stage[(st + 1) & 1]);
+            if (st + 2 < steps) Ops::input_rows(t, k0 + (st + 2) * kTileK, idx, next_rows);
         }
-        Ops::compute(t, t.k0 + st * kTileK, stage[st & 1], acc);
+        Ops::compute(t, k0 + st * kTileK, stage[st & 1], acc);
     }
     Ops::store(t, c0, out_row, out, k, acc);
 }
@@ -942,12 +952,16 @@ constexpr int stage_bytes() { return 2 * (int)sizeof(Stage<TC>); }
 
 // A forward pass over right-hand sides that are zero outside the marked supernodes (a batch of
 // source indicators: only a source's supernode and its ancestors receive anything): a tile of an
-// unmarked node has a zero input block. It writes zeros where it assigns and is skipped where it
-// accumulates. Returns whether the tile was handled so.
-__device__ __forceinline__ bool skip_inactive(const Tile& t, const unsigned char* active, int c0, int width,
-                                              const int* idx, double* out, int k) {
-    if (active == nullptr || active[t.node]) return false;
-    if (t.op == kAssign)
+// unmarked node has a zero input block. Its update rows of a deterministic factor are written as
+// zeros (the level's gather adds them), its Y rows too unless the backward pass is trimmed (and so
+// does not read them: first_inner), and a tile that accumulates is skipped. Returns whether the tile was
+// handled so.
+__device__ __forceinline__ bool skip_inactive(const Tile& t, const unsigned char* active, int trimmed, int c0,
+                                              int width, const int* idx, double* out, int k) {
+    // A backward tile of an unmarked node is trimmed instead (first_inner); when the backward pass
+    // trims, the Y rows of the forward diagonal tile, read by nothing else, are not written.
+    if (active == nullptr || active[t.node] || t.tri == 2) return false;
+    if (t.op == kAssign && (t.tri != 1 || !trimmed))
         for (int e = threadIdx.x; e < t.rows * width; e += blockDim.x) {
             const int i = e / width, c = c0 + e % width;
             if (c >= k) continue;
@@ -957,15 +971,23 @@ __device__ __forceinline__ bool skip_inactive(const Tile& t, const unsigned char
     return true;
 }
 
+// The first inner index a tile's product runs from. The backward tile of an unmarked node (its Y
+// block zero: nothing reached it in the forward pass, which left its Y rows unwritten) starts past
+// the Y block, at the node's off-diagonal rows.
+__device__ __forceinline__ int first_inner(const Tile& t, const unsigned char* active) {
+    return (active != nullptr && t.tri == 2 && !active[t.node]) ? max(t.k0, t.tri_k) : t.k0;
+}
+
 // One launch per phase: a CTA per (tile, column block of TC columns).
 template <int TC>
 __global__ void __launch_bounds__(kTileThreads, TC == kTileCols ? kTileCtasPerSm : 8)
 tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
-                    const int* __restrict__ idx, double* rows, int k, const unsigned char* active) {
+                    const int* __restrict__ idx, double* rows, int k, const unsigned char* active, int trimmed) {
     extern __shared__ __align__(16) unsigned char shared_stages[];
     Stage<TC>* stage = reinterpret_cast<Stage<TC>*>(shared_stages);
-    if (skip_inactive(tiles[blockIdx.x], active, blockIdx.y * TC, TC, idx, rows, k)) return;
-    tile_product<TC>(tiles[blockIdx.x], blockIdx.y * TC, vals, idx, rows, rows, k, stage);
+    const Tile& t = tiles[blockIdx.x];
+    if (skip_inactive(t, active, trimmed, blockIdx.y * TC, TC, idx, rows, k)) return;
+    tile_product<TC>(t, first_inner(t, active), blockIdx.y * TC, vals, idx, rows, rows, k, stage);
 }
 
 // The same tile product for a narrow batch (KP = 2, 4, 6 or 8 columns, the even stride of 1-8
@@ -981,8 +1003,8 @@ constexpr int kNarrowSlices = kNarrowThreads / kTileRows;
 template <int KP>
 __global__ void __launch_bounds__(kNarrowThreads)
 narrow_tile_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
-                   const int* __restrict__ idx, double* rows, const unsigned char* active) {
-    if (skip_inactive(tiles[blockIdx.x], active, 0, KP, idx, rows, KP)) return;
+                   const int* __restrict__ idx, double* rows, const unsigned char* active, int trimmed) {
+    if (skip_inactive(tiles[blockIdx.x], active, trimmed, 0, KP, idx, rows, KP)) return;
     const double* in = rows;
     double* out = rows;
     __shared__ double other[kNarrowSlices - 1][kTileRows][KP];
@@ -1010,7 +1032,7 @@ narrow_tile_kernel(const Tile* __restrict__ tiles, const double* __restrict__ va
             // Column-major reads: the 64 threads of a slice read 64 consecutive values. Values a
             // thread alone reads go through L2 only (`__ldcg`): caching them in L1 measured slower.
             constexpr int kStep = kNarrowSlices;
-            int kk = t.k0 + slice;
+            int kk = first_inner(t, active) + slice;
             for (; kk + 3 * kStep < t.k1; kk += 4 * kStep) {
                 const int r0 = row(kk), r1 = row(kk + kStep), r2 = row(kk + 2 * kStep), r3 = row(kk + 3 * kStep);
                 const double a0 = value(kk), a1 = value(kk + kStep), a2 = value(kk + 2 * kStep),
@@ -1539,8 +1561,8 @@ __global__ void mark_sources_kernel(const int* __restrict__ sources, const int* 
     }
 }
 
-// forward_active: the marked supernodes of a batch of source indicators (see skip_inactive), or
-// nullptr; the backward pass is always full.
+// forward_active: the marked supernodes of a batch of source indicators (see skip_inactive and
+// first_inner), or nullptr.
 int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream,
                       const unsigned char* forward_active = nullptr) {
     const int L = F->analysis->levels;
@@ -1555,21 +1577,25 @@ int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream,
     }
     // A level's launch: the float64 tensor-core tiles, or for a narrow batch (stride 2-8) the
     // register kernel, which does not compute a 64-column tile's idle columns.
+    // The backward pass is trimmed past the zero Y blocks of unmarked nodes, except in a
+    // deterministic factor: there a query's sums must not depend on the marks other queries of its
+    // batch add (trimming changes how the tensor-core steps group the inner dimension).
+    const int trimmed = forward_active != nullptr && !F->deterministic;
     auto level = [&](const Tile* tiles, int count, int cols, const unsigned char* active, const char* what) {
         switch (k) {
-            case 2: narrow_tile_kernel<2><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active); break;
-            case 4: narrow_tile_kernel<4><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active); break;
-            case 6: narrow_tile_kernel<6><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active); break;
-            case 8: narrow_tile_kernel<8><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active); break;
+            case 2: narrow_tile_kernel<2><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active, trimmed); break;
+            case 4: narrow_tile_kernel<4><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active, trimmed); break;
+            case 6: narrow_tile_kernel<6><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active, trimmed); break;
+            case 8: narrow_tile_kernel<8><<<count, kNarrowThreads, 0, stream>>>(tiles, F->vals, F->idx, W.BYX, active, trimmed); break;
             default:
                 if (cols == kTileColsNarrow)
                     tile_product_kernel<kTileColsNarrow>
                         <<<dim3(count, ceil_div(k, kTileColsNarrow)), kTileThreads, stage_bytes<kTileColsNarrow>(),
-                           stream>>>(tiles, F->vals, F->idx, W.BYX, k, active);
+                           stream>>>(tiles, F->vals, F->idx, W.BYX, k, active, trimmed);
                 else
                     tile_product_kernel<kTileCols><<<dim3(count, ceil_div(k, kTileCols)), kTileThreads,
                                                       stage_bytes<kTileCols>(), stream>>>(tiles, F->vals, F->idx,
-                                                                                          W.BYX, k, active);
+                                                                                          W.BYX, k, active, trimmed);
         }
         OB_CHECK_LAUNCH(what);
         return OB_OK;
@@ -1583,8 +1609,10 @@ int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream,
             OB_CHECK_LAUNCH("chol deterministic gather");
         }
     }
+    // The backward pass starts past the zero Y block of every node the forward pass left unmarked.
     for (int l = L - 1; l >= 0 && st == OB_OK; --l)
-        if (F->n_bwd[l]) st = level(F->bwd[l], F->n_bwd[l], F->bwd_cols[l], nullptr, "chol backward level");
+        if (F->n_bwd[l])
+            st = level(F->bwd[l], F->n_bwd[l], F->bwd_cols[l], trimmed ? forward_active : nullptr, "chol backward level");
     return st;
 }
 
