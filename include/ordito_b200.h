@@ -455,7 +455,9 @@ int ob_chol_solve_in_place_set(void* factor, int set, int n_columns, ob_stream_t
  * indicators (as ob_seed_permuted writes them for sources / source_offsets, n_columns sets, vertex
  * indices): the forward pass runs only the supernodes a source reaches -- its own and their
  * ancestors -- since every other supernode's input block is zero (their Y rows are written as
- * zero); the backward pass is full. Marks on the device (no host read), so it can be recorded. */
+ * zero). On a factor analysed without the deterministic flag the backward pass of such a supernode
+ * starts past its own zero Y block (only the G^T X[off] part of X = [L11^-1; G]^T [Y; X[off]]
+ * runs). Marks on the device (no host read), so it can be recorded. */
 int ob_chol_solve_in_place_sources(void* factor, int set, int n_columns, const int32_t* sources,
                                    const int32_t* source_offsets, ob_stream_t stream);
 int ob_chol_work_generation_set(void* factor, int set, long long* generation);
