@@ -132,83 +132,171 @@ int upload(FactorPlan* P, T** out, const std::vector<T>& host, cudaStream_t stre
     return OB_OK;
 }
 
-// The device tables and the launch schedule of an analysis (host work, once).
+template <typename T>
+int allocate(FactorPlan* P, T** out, size_t count, cudaStream_t stream) {
+    void* p = nullptr;
+    OB_CUDA(pool_malloc(&p, sizeof(T) * std::max<size_t>(count, 1), stream));
+    P->owned.push_back(p);
+    *out = static_cast<T*>(p);
+    return OB_OK;
+}
+
+template <typename T>
+int upload_scratch(Scratch& scratch, const T** out, const std::vector<T>& host, cudaStream_t stream) {
+    T* p = scratch.take<T>(host.size());
+    if (int st = scratch.commit()) return st;
+    if (!host.empty())
+        OB_CUDA(cudaMemcpyAsync(p, host.data(), sizeof(T) * host.size(), cudaMemcpyHostToDevice, stream));
+    *out = p;
+    return OB_OK;
+}
+
+// The tree as the plan kernels read it: per supernode its first column, own columns, front
+// offset and leading dimension, and its off-diagonal rows (ascending) at rows + row_at[s] ..
+// row_at[s + 1]; per new column its supernode.
+struct PlanTree {
+    const int* start;
+    const int* nc;
+    const long long* front_at;
+    const int* fld;
+    const int* row_at;
+    const int* rows;
+    const int* node_of;
+};
+
+// Row r's position in supernode s's front: its own column r - start, else nc + its index among
+// the off-diagonal rows (which hold r: the symbolic structure puts it there).
+__device__ __forceinline__ int front_position(const PlanTree& T, int s, int r) {
+    const int start = T.start[s], count = T.nc[s];
+    if (r < start + count) return r - start;
+    int lo = T.row_at[s], hi = T.row_at[s + 1];
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (T.rows[mid] < r) lo = mid + 1;
+        else hi = mid;
+    }
+    return count + (lo - T.row_at[s]);
+}
+
+// node_of[j] = s for each own column j of supernode s (a warp a supernode).
+__global__ void node_of_kernel(int ns, const int* __restrict__ start, const int* __restrict__ nc, int* node_of) {
+    const int s = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    if (s >= ns) return;
+    for (int j = threadIdx.x & 31; j < nc[s]; j += 32) node_of[start[s] + j] = s;
+}
+
+// Per CSR entry e of old row ro (a group of 8 lanes a row): its new (row, column) and its slot
+// in the front of its row's supernode (-1 in the upper triangle, which the lower one mirrors);
+// per old row the CSR position of its diagonal (left -1 when it has none).
+constexpr int kEntryLanes = 8;
+__global__ void entries_kernel(int n, const int* __restrict__ offsets, const int* __restrict__ columns,
+                               const int* __restrict__ iperm, const PlanTree T, long long* __restrict__ dest,
+                               int2* __restrict__ rc, int* __restrict__ diag_pos) {
+    const long long lane_id = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int ro = (int)(lane_id / kEntryLanes);
+    if (ro >= n) return;
+    const int lane = (int)(lane_id % kEntryLanes);
+    const int j = iperm[ro];
+    const int s = T.node_of[j];
+    const long long column_at = T.front_at[s] + (long long)(j - T.start[s]) * T.fld[s];
+    for (int e = offsets[ro] + lane; e < offsets[ro + 1]; e += kEntryLanes) {
+        const int co = columns[e];
+        const int r = iperm[co];
+        rc[e] = make_int2(j, r);
+        if (co == ro) diag_pos[ro] = e;
+        dest[e] = r < j ? -1LL : column_at + front_position(T, s, r);
+    }
+}
+
+// rel: each child's off-diagonal rows as positions in its parent's front (a warp a supernode;
+// a root's entries are left unset: nothing reads them).
+__global__ void rel_kernel(int ns, const int* __restrict__ parent, const PlanTree T, int* __restrict__ rel) {
+    const int s = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    if (s >= ns || parent[s] < 0) return;
+    for (int i = T.row_at[s] + (threadIdx.x & 31); i < T.row_at[s + 1]; i += 32)
+        rel[i] = front_position(T, parent[s], T.rows[i]);
+}
+
+// Each new column's diagonal slot in its supernode's front.
+__global__ void diag_dest_kernel(int n, const PlanTree T, long long* __restrict__ diag_dest) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int s = T.node_of[j];
+    const long long lj = j - T.start[s];
+    diag_dest[j] = T.front_at[s] + lj * T.fld[s] + lj;
+}
+
+// The device tables and the launch schedule of an analysis (once). The per-entry and per-row
+// tables are built on the device from the tree; the host builds the launch schedule.
 int build_plan(const CholAnalysis& A, FactorPlan* P, cudaStream_t stream) {
     const int n = A.n, ns = (int)A.nodes.size();
     const BlockLayout layout = block_layout(A);
     // Front arena: node s is m x m column-major at front_at[s], leading dimension fld (m rounded
     // up to 8 doubles, so every front column starts on 64 bytes).
     std::vector<long long> front_at(ns);
-    std::vector<int> fld(ns), nc(ns), noff(ns), node_of(n, -1);
+    std::vector<int> fld(ns), nc(ns), noff(ns), start(ns), parent(ns), row_at(ns + 1, 0);
     long long total = 0;
     for (int s = 0; s < ns; ++s) {
         const CholNode& nd = A.nodes[s];
         nc[s] = nd.count;
+        start[s] = nd.start;
+        parent[s] = nd.parent;
         noff[s] = (int)nd.off_rows.size();
+        row_at[s + 1] = row_at[s] + noff[s];
         const int m = nc[s] + noff[s];
         fld[s] = (m + 7) / 8 * 8;
         front_at[s] = total;
         total += (long long)fld[s] * m;
-        for (int j = 0; j < nd.count; ++j) node_of[nd.start + j] = s;
     }
     P->front_total = total;
-    // A row's position in node s's front: own column r - start, else nc + its off-row index.
-    auto local = [&](int s, int r) -> int {
-        const CholNode& nd = A.nodes[s];
-        if (r < nd.start + nd.count) return r - nd.start;
-        const auto it = std::lower_bound(nd.off_rows.begin(), nd.off_rows.end(), r);
-        return nd.count + (int)(it - nd.off_rows.begin());
-    };
-    // Entry destinations: entry (old row ro, old column co) with j = iperm[ro], r = iperm[co]
-    // belongs to column j's front when r >= j (the lower triangle in the new numbering).
-    const long long nnz = A.offsets[n];
-    P->n_entries = nnz;
-    std::vector<long long> entry_dest(nnz, -1);
-    std::vector<int2> entry_rc(nnz);
-    std::vector<int> diag_pos(n, -1);
-    // Rows on host threads: each writes only its own entries and its own diagonal position.
-    parallel_range(n, nnz > (1LL << 18), [&](long long lo, long long hi) {
-        for (int ro = (int)lo; ro < (int)hi; ++ro) {
-            const int j = A.iperm[ro];
-            const int s = node_of[j];
-            for (int e = A.offsets[ro]; e < A.offsets[ro + 1]; ++e) {
-                const int co = A.columns[e];
-                const int r = A.iperm[co];
-                entry_rc[e] = make_int2(j, r);
-                if (co == ro) diag_pos[ro] = e;
-                if (r < j) continue;
-                entry_dest[e] = front_at[s] + (long long)(j - A.nodes[s].start) * fld[s] + local(s, r);
-            }
-        }
+    std::vector<int> rows(row_at[ns]);
+    parallel_range(ns, row_at[ns] > (1 << 18), [&](long long lo, long long hi) {
+        for (long long s = lo; s < hi; ++s)
+            std::copy(A.nodes[s].off_rows.begin(), A.nodes[s].off_rows.end(), rows.begin() + row_at[s]);
     });
-    std::vector<long long> diag_dest(n);
-    for (int i = 0; i < n; ++i) {
-        const int s = node_of[i];
-        const long long lj = i - A.nodes[s].start;
-        diag_dest[i] = front_at[s] + lj * fld[s] + lj;
-    }
-    // Each child's off-diagonal rows as positions in its parent's front (ascending: the parent's
-    // own columns come before its off-diagonal rows in both numberings).
-    std::vector<int> rel_at(ns, 0), rel;
-    for (int s = 0; s < ns; ++s) {
-        rel_at[s] = (int)rel.size();
-        const int p = A.nodes[s].parent;
-        if (p < 0) continue;
-        for (int r : A.nodes[s].off_rows) rel.push_back(local(p, r));
-    }
     std::vector<char> component_last(n);
     for (int i = 0; i < n; ++i) component_last[i] = (char)A.component_last[i];
+    const long long nnz = A.offsets[n];
+    P->n_entries = nnz;
     int st = OB_OK;
-    if ((st = upload(P, &P->entry_dest, entry_dest, stream)) || (st = upload(P, &P->entry_rc, entry_rc, stream)) ||
-        (st = upload(P, &P->diag_dest, diag_dest, stream)) || (st = upload(P, &P->diag_pos, diag_pos, stream)) ||
-        (st = upload(P, &P->component, A.component, stream)) ||
+    if ((st = upload(P, &P->component, A.component, stream)) ||
         (st = upload(P, &P->component_last, component_last, stream)) ||
         (st = upload(P, &P->perm, A.perm, stream)) || (st = upload(P, &P->offsets, A.offsets, stream)) ||
         (st = upload(P, &P->front_at, front_at, stream)) ||
         (st = upload(P, &P->fld, fld, stream)) || (st = upload(P, &P->nc, nc, stream)) ||
-        (st = upload(P, &P->noff, noff, stream)) || (st = upload(P, &P->rel_at, rel_at, stream)) ||
-        (st = upload(P, &P->rel, rel, stream)))
+        (st = upload(P, &P->noff, noff, stream)) || (st = upload(P, &P->rel_at, row_at, stream)) ||
+        (st = allocate(P, &P->rel, (size_t)row_at[ns], stream)) ||
+        (st = allocate(P, &P->entry_dest, (size_t)nnz, stream)) ||
+        (st = allocate(P, &P->entry_rc, (size_t)nnz, stream)) ||
+        (st = allocate(P, &P->diag_pos, (size_t)n, stream)) ||
+        (st = allocate(P, &P->diag_dest, (size_t)n, stream)))
         return st;
+    {
+        // The tree and the pattern, for the table kernels only.
+        Scratch scratch(stream);
+        const int *d_start = nullptr, *d_parent = nullptr, *d_rows = nullptr, *d_iperm = nullptr,
+                  *d_columns = nullptr;
+        int* d_node_of = scratch.take<int>((size_t)n);
+        if ((st = scratch.commit()) || (st = upload_scratch(scratch, &d_start, start, stream)) ||
+            (st = upload_scratch(scratch, &d_parent, parent, stream)) ||
+            (st = upload_scratch(scratch, &d_rows, rows, stream)) ||
+            (st = upload_scratch(scratch, &d_iperm, A.iperm, stream)) ||
+            (st = upload_scratch(scratch, &d_columns, A.columns, stream)))
+            return st;
+        const PlanTree T{d_start, P->nc, P->front_at, P->fld, P->rel_at, d_rows, d_node_of};
+        const int threads = 256;
+        node_of_kernel<<<ceil_div(32LL * ns, threads), threads, 0, stream>>>(ns, d_start, P->nc, d_node_of);
+        OB_CHECK_LAUNCH("chol plan node_of");
+        OB_CUDA(cudaMemsetAsync(P->diag_pos, 0xFF, sizeof(int) * (size_t)n, stream));
+        entries_kernel<<<ceil_div((long long)kEntryLanes * n, threads), threads, 0, stream>>>(
+            n, P->offsets, d_columns, d_iperm, T, P->entry_dest, P->entry_rc, P->diag_pos);
+        OB_CHECK_LAUNCH("chol plan entries");
+        rel_kernel<<<ceil_div(32LL * ns, threads), threads, 0, stream>>>(ns, d_parent, T, P->rel);
+        OB_CHECK_LAUNCH("chol plan rel");
+        diag_dest_kernel<<<ceil_div(n, threads), threads, 0, stream>>>(n, T, P->diag_dest);
+        OB_CHECK_LAUNCH("chol plan diagonal slots");
+        // The scratch is released in stream order, after these kernels.
+    }
     // The schedule, level by level.
     std::vector<std::vector<int>> at_level(A.levels);
     for (int s = 0; s < ns; ++s) at_level[A.nodes[s].level].push_back(s);

@@ -108,7 +108,7 @@ struct Dissector {
     // Subtrees of at least this many vertices, down to this depth, are dissected on a thread of
     // their own (geometric bisection only); the tree and the ordering are the same as one
     // thread's: each subtree is built into its own lists and appended in postorder.
-    static constexpr int kParallelDepth = 4;
+    static constexpr int kParallelDepth = 5;
     static constexpr size_t kParallelVertices = 8192;
 
     // Builds the subtree of `verts` into `tree` / `order` (postorder, indices within the lists);
@@ -176,41 +176,56 @@ struct Dissector {
 
 // Symbolic analysis of a dissection: each node's off-diagonal rows are its columns' later
 // neighbours plus its children's off-diagonal rows past its own columns; its level is its height
-// above the leaves.
+// above the leaves. The nodes of one level depend only on the levels below, so each level's
+// nodes run across host threads (each node's rows sorted and deduplicated on its own).
 void symbolic(Analysis& A, const std::vector<int>& adj_off, const std::vector<int>& adj) {
-    std::vector<int> mark(A.n, -1);
-    A.factor_entries = 0;
-    A.levels = 0;
-    for (int s = 0; s < (int)A.nodes.size(); ++s) {
-        Node& node = A.nodes[s];
-        const int end = node.start + node.count;
-        std::vector<int> rows;
-        for (int j = node.start; j < end; ++j) {
-            const int old = A.perm[j];
-            for (int e = adj_off[old]; e < adj_off[old + 1]; ++e) {
-                const int r = A.iperm[adj[e]];
-                if (r >= end && mark[r] != s) {
-                    mark[r] = s;
-                    rows.push_back(r);
-                }
-            }
-        }
+    const int ns = (int)A.nodes.size();
+    // Heights (the nodes are in postorder: children first), then the nodes bucketed by height.
+    std::vector<int> height(ns, 0);
+    int top = 0;
+    for (int s = 0; s < ns; ++s) {
         int level = 0;
-        for (int c : node.children) {
-            level = std::max(level, A.nodes[c].level + 1);
-            for (int r : A.nodes[c].off_rows)
-                if (r >= end && mark[r] != s) {
-                    mark[r] = s;
-                    rows.push_back(r);
-                }
-        }
-        std::sort(rows.begin(), rows.end());
-        node.off_rows = std::move(rows);
-        node.level = level;
-        A.levels = std::max(A.levels, level + 1);
-        A.factor_entries += (long long)node.count * node.count +
-                            (long long)node.off_rows.size() * node.count;
+        for (int c : A.nodes[s].children) level = std::max(level, height[c] + 1);
+        height[s] = level;
+        top = std::max(top, level);
     }
+    std::vector<int> first(top + 2, 0), bucket(ns);
+    for (int s = 0; s < ns; ++s) ++first[height[s] + 1];
+    for (int l = 0; l <= top; ++l) first[l + 1] += first[l];
+    {
+        std::vector<int> fill(first.begin(), first.end() - 1);
+        for (int s = 0; s < ns; ++s) bucket[fill[height[s]]++] = s;
+    }
+    for (int l = 0; l <= top; ++l) {
+        const int* nodes = bucket.data() + first[l];
+        const long long count = first[l + 1] - first[l];
+        parallel_range(count, A.n > (1 << 16), [&](long long lo, long long hi) {
+            std::vector<int> rows;
+            for (long long i = lo; i < hi; ++i) {
+                Node& node = A.nodes[nodes[i]];
+                const int end = node.start + node.count;
+                rows.clear();
+                for (int j = node.start; j < end; ++j) {
+                    const int old = A.perm[j];
+                    for (int e = adj_off[old]; e < adj_off[old + 1]; ++e) {
+                        const int r = A.iperm[adj[e]];
+                        if (r >= end) rows.push_back(r);
+                    }
+                }
+                for (int c : node.children)
+                    for (int r : A.nodes[c].off_rows)
+                        if (r >= end) rows.push_back(r);
+                std::sort(rows.begin(), rows.end());
+                rows.erase(std::unique(rows.begin(), rows.end()), rows.end());
+                node.off_rows.assign(rows.begin(), rows.end());
+                node.level = l;
+            }
+        });
+    }
+    A.levels = top + 1;
+    A.factor_entries = 0;
+    for (const Node& node : A.nodes)
+        A.factor_entries += (long long)node.count * node.count + (long long)node.off_rows.size() * node.count;
 }
 
 // Level amalgamation. Each tree level costs the solves one dependent launch per direction (a
@@ -332,14 +347,26 @@ int analyse(int n, std::vector<int> offsets, std::vector<int> columns, const flo
     A.n = n;
     A.offsets = std::move(offsets);
     A.columns = std::move(columns);
-    // Adjacency without the diagonal, for the separators and the components.
-    std::vector<int> adj_off(n + 1, 0), adj;
-    adj.reserve(A.columns.size());
-    for (int i = 0; i < n; ++i) {
-        for (int e = A.offsets[i]; e < A.offsets[i + 1]; ++e)
-            if (A.columns[e] != i) adj.push_back(A.columns[e]);
-        adj_off[i + 1] = (int)adj.size();
-    }
+    // Adjacency without the diagonal, for the separators and the components: each row's count,
+    // their prefix sum, then each row's entries in place (rows across host threads).
+    std::vector<int> adj_off(n + 1, 0);
+    const bool large = A.columns.size() > (1u << 18);
+    parallel_range(n, large, [&](long long lo, long long hi) {
+        for (long long i = lo; i < hi; ++i) {
+            int count = 0;
+            for (int e = A.offsets[i]; e < A.offsets[i + 1]; ++e) count += A.columns[e] != (int)i;
+            adj_off[i + 1] = count;
+        }
+    });
+    for (int i = 0; i < n; ++i) adj_off[i + 1] += adj_off[i];
+    std::vector<int> adj(adj_off[n]);
+    parallel_range(n, large, [&](long long lo, long long hi) {
+        for (long long i = lo; i < hi; ++i) {
+            int at = adj_off[i];
+            for (int e = A.offsets[i]; e < A.offsets[i + 1]; ++e)
+                if (A.columns[e] != (int)i) adj[at++] = A.columns[e];
+        }
+    });
     if (leaf_size <= 0) leaf_size = kDefaultLeafSize;
     if (block > 1) {
         const int nv = n / block;

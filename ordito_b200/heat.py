@@ -157,14 +157,10 @@ def _diffusion_floor(mesh: Trimesh) -> float:
     return (math.dist(low, high) / _DIFFUSION_DECAY) ** 2
 
 
-def _diffusion_floor_length(vertices: np.ndarray) -> float:
-    """``|bounding-box diagonal| / 400`` of host vertices: the square root of the floor above
-    (float32 extremes widened to float64, exactly as the device's bounds)."""
-    if vertices.size == 0:
-        return 0.0
-    low = vertices.min(axis=0).astype(np.float64)
-    high = vertices.max(axis=0).astype(np.float64)
-    return math.dist(low, high) / _DIFFUSION_DECAY
+def _bounds_floor_length(low: np.ndarray, high: np.ndarray) -> float:
+    """``|bounding-box diagonal| / 400`` of a box's float32 corners: the square root of the floor
+    above (the float32 extremes widened to float64, exactly as the device's bounds)."""
+    return math.dist(low.astype(np.float64), high.astype(np.float64)) / _DIFFUSION_DECAY
 
 
 def _settle_window(t: float | None, default: float) -> int:

@@ -27,7 +27,7 @@ from ordito_b200 import _lib
 from ordito_b200.array import CsrMatrix
 from ordito_b200.cholesky import CholeskyAnalysis, SparseCholesky
 from ordito_b200.device import DEFAULT_STREAM, DeviceArray
-from ordito_b200.heat import _diffusion_floor_length, capture_guard
+from ordito_b200.heat import _bounds_floor_length, capture_guard
 from ordito_b200.laplacian import face_terms, mesh_operator_pattern
 
 
@@ -68,8 +68,16 @@ class PackedMeshes:
         s = sums.numpy().reshape(self.n_meshes, 2)
         h = np.where(s[:, 1] > 0, s[:, 0] / np.where(s[:, 1] > 0, s[:, 1], 1.0), 0.0)
         t = h * h
-        for m, v in enumerate(verts):
-            floor = _diffusion_floor_length(v) ** 2
+        # Each mesh's bounding box in one pass over the union (float32 extremes, as per mesh).
+        nonempty = np.flatnonzero(counts > 0)
+        low = np.zeros((self.n_meshes, 3), dtype=np.float32)
+        high = np.zeros((self.n_meshes, 3), dtype=np.float32)
+        if nonempty.size:
+            starts = self.vertex_offsets[nonempty]
+            low[nonempty] = np.minimum.reduceat(xyz, starts, axis=0)
+            high[nonempty] = np.maximum.reduceat(xyz, starts, axis=0)
+        for m in nonempty:
+            floor = _bounds_floor_length(low[m], high[m]) ** 2
             if floor > t[m]:
                 t[m] = floor
         self.time_steps = t
@@ -89,21 +97,20 @@ class PackedMeshes:
         self.heat_system = laplacian.with_values(H)
         self.poisson_system = laplacian.with_values(P)
         # a11: one analysis (the meshes translated apart for it) for both factors.
-        extent = max(float(np.ptp(v, axis=0).max()) if v.size else 0.0 for v in verts)
+        extent = float((high - low).max()) if nonempty.size else 0.0
         spacing = 4.0 * max(extent, 1.0)
         shifted = xyz.copy()
-        for m in range(self.n_meshes):
-            shifted[self.vertex_offsets[m]:self.vertex_offsets[m + 1], 0] += m * spacing
+        shifted[:, 0] += np.repeat((np.arange(self.n_meshes) * spacing).astype(np.float32), counts)
         self.analysis = CholeskyAnalysis(self.heat_system, DeviceArray.from_host(shifted))
         self.heat_factor = SparseCholesky(self.heat_system, self.analysis, singular=False)
         self.poisson_factor = SparseCholesky(self.poisson_system, self.analysis, singular=True)
         # The passes' tile schedule tuned to the union's tree at the batch width.
         from ordito_b200.tuning import tune_shared  # noqa: PLC0415
 
-        # Both factors share the union's analysis: one search (five timed passes a candidate: a
+        # Both factors share the union's analysis: one search (three timed passes a candidate: a
         # packed pass takes milliseconds) serves both.
         self.tuning = tune_shared({"heat": self.heat_factor, "poisson": self.poisson_factor}, max_columns,
-                                  reps=5)
+                                  reps=3)
         # a8: the divergence's corner index and per-face terms over the union.
         self.corner_offsets = DeviceArray.empty(n + 1, np.int32)
         self.corner_slots = DeviceArray.empty(max(3 * self.n_faces, 1), np.int32)

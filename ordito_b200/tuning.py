@@ -38,7 +38,7 @@ WIDTHS: tuple[int, ...] = (0, 1, 2, 4, 64)
 
 def _time(factor: Any, k: int, reps: int) -> float:
     ms = ctypes.c_float(0.0)
-    _lib.call("ob_chol_time_solve", factor.handle, int(k), 2, ctypes.byref(ms), None)  # warm
+    _lib.call("ob_chol_time_solve", factor.handle, int(k), 1, ctypes.byref(ms), None)  # warm
     _lib.call("ob_chol_time_solve", factor.handle, int(k), int(reps), ctypes.byref(ms), None)
     return float(ms.value)
 
