@@ -752,10 +752,22 @@ constexpr int kTileColsNarrow = 32;  // the narrow form: twice the CTAs, half th
 // 0.82 ms a pass on the 131k torus at 64 columns, against 1.11 ms for 32 (74 KB, 3 CTAs per SM).
 constexpr int kTileK = 16;
 constexpr int kSplitK = 64;  // a split tile's inner-dimension range (32 measured slower: more atomics)
-constexpr int kTileThreads = 128;
-// Resident CTAs of the 64-column product an SM: at most 96 registers a thread and two stages of
-// 19.5 KB hold five (126 registers held four).
-constexpr int kTileCtasPerSm = 5;
+constexpr int kTileThreads = 128;  // the narrow form's CTA: four warps, each a 16-row strip
+// The wide form's CTA: eight warps, a 16-row strip of 32 of the 64 columns each, so the matrix
+// block staged once feeds 64 columns while a warp holds half the accumulators (64 registers).
+constexpr int kTileThreadsWide = 256;
+template <int TC>
+constexpr int tile_threads() { return TC == kTileCols ? kTileThreadsWide : kTileThreads; }
+// Resident CTAs of the 64-column product an SM: three of eight warps at up to 80 registers a
+// thread, two stages of 19.5 KB each (the 131k torus at 64 columns, a pass: 0.397 ms; four CTAs
+// at 64 registers 0.401 ms; the four-warp CTA, five an SM at 96 registers, 0.428 ms; three
+// stages at three CTAs 0.410 ms).
+constexpr int kTileCtasPerSm = 3;
+// Resident CTAs of the 32-column product an SM: four warps at up to 73 registers a thread, two
+// stages of 15 KB (seven fill the shared memory). The tuner picks this form for every level of the
+// 131k torus at 64 columns: 0.381 ms a pass, against 0.392 ms at six an SM and 0.398 ms at eight
+// (64 registers, with spills).
+constexpr int kTileCtasPerSmNarrow = 7;
 // Shared rows of 72 doubles (a transposed matrix block's 64 output rows, a 64-column input row):
 // the 8 x 4 fragment loads of a warp then touch every 8-byte bank pair exactly twice (the minimum
 // for 256 bytes); 40 for a 32-column input row.
@@ -791,9 +803,10 @@ struct Stage {
     double b[kTileK * input_ld<TC>()];
 };
 
-// One 64 x 64 output tile for a CTA of four warps, each warp a 16-row strip of all 64 columns as
-// 2 x 8 float64 MMA tiles (strips rather than quadrants, so a strip of padding rows, or of the
-// zero triangle of L11^-1 over an inner step, is skipped whole). The tile's matrix block and its
+// One 64 x TC output tile for a CTA of four 16-row strips of warps, each strip one warp (TC = 32,
+// 2 x 4 float64 MMA tiles) or two (TC = 64: a warp each 32 of the columns, 2 x 4 MMA tiles);
+// strips rather than quadrants, so a strip of padding rows, or of the zero triangle of L11^-1
+// over an inner step, is skipped whole. The tile's matrix block and its
 // gathered input rows are copied 16 inner steps at a time into shared memory with asynchronous
 // 16-byte copies (zero-filled at the edges), two stages: the next step's copies, issued after the
 // step's one barrier, overlap the current step's MMAs. The output is assigned, subtracted, or
@@ -802,12 +815,14 @@ struct Stage {
 // a launch's tiles read are never rows any tile of that launch writes.
 template <int TC>
 struct TileOps {
-    static constexpr int kJ = TC / 8;  // 8-column MMA tiles a warp strip holds
+    static constexpr int kThreads = tile_threads<TC>();
+    static constexpr int kGroups = kThreads / kTileThreads;  // column groups of warps
+    static constexpr int kJ = TC / 8 / kGroups;               // 8-column MMA tiles a warp holds
     static constexpr int kLdB = input_ld<TC>();
     // The matrix block is 64 x kTileK doubles in 16-byte chunks, kChunks per thread; the input
     // block kTileK x TC, kChunksB per thread.
-    static constexpr int kChunks = kTileRows * kTileK / 2 / kTileThreads;
-    static constexpr int kChunksB = TC * kTileK / 2 / kTileThreads;
+    static constexpr int kChunks = kTileRows * kTileK / 2 / kThreads;
+    static constexpr int kChunksB = TC * kTileK / 2 / kThreads;
     using Acc = double[2][kJ][2];
 
     __device__ static int steps(const Tile& t) { return (t.k1 - t.k0 + kTileK - 1) / kTileK; }
@@ -816,7 +831,7 @@ struct TileOps {
     __device__ static void input_rows(const Tile& t, int kb, const int* __restrict__ idx, int* r) {
 #pragma unroll
         for (int q = 0; q < kChunksB; ++q) {
-            const int kk = (threadIdx.x + q * kTileThreads) / (TC / 2);
+            const int kk = (threadIdx.x + q * kThreads) / (TC / 2);
             r[q] = kb + kk < t.k1 ? (t.in_rows < 0 ? t.in_base + kb + kk : idx[t.in_rows + kb + kk]) : -1;
         }
     }
@@ -827,7 +842,7 @@ struct TileOps {
         const double* M = vals + t.m;
 #pragma unroll
         for (int q = 0; q < kChunks; ++q) {
-            const int chunk = threadIdx.x + q * kTileThreads;
+            const int chunk = threadIdx.x + q * kThreads;
             if (t.trans) {
                 // Row kk of the stored matrix, elements r0 + 2 c .. + 1: k-major staging.
                 const int kk = chunk / (kTileRows / 2), c2 = 2 * (chunk % (kTileRows / 2));
@@ -844,7 +859,7 @@ struct TileOps {
         }
 #pragma unroll
         for (int q = 0; q < kChunksB; ++q) {
-            const int chunk = threadIdx.x + q * kTileThreads;
+            const int chunk = threadIdx.x + q * kThreads;
             // Input rows: row kk of the step, columns c0 + 2 c .. + 1.
             const int kk = chunk / (TC / 2), c2 = 2 * (chunk % (TC / 2));
             int valid = 0;
@@ -859,8 +874,11 @@ struct TileOps {
     }
 
     // The output rows of this thread's accumulator rows (-1 past the tile).
+    __device__ static int strip() { return ((threadIdx.x >> 5) & 3) * 16; }
+    __device__ static int group_column() { return (threadIdx.x >> 7) * (TC / kGroups); }
+
     __device__ static void output_rows(const Tile& t, const int* __restrict__ idx, int* out_row) {
-        const int lane = threadIdx.x & 31, wr = (threadIdx.x >> 5) * 16;
+        const int lane = threadIdx.x & 31, wr = strip();
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
             const int local = wr + 8 * i + (lane >> 2);
@@ -874,7 +892,7 @@ struct TileOps {
     // L11^-1 (the decision is warp-uniform and taken outside the unrolled step, which stays
     // branch-free).
     __device__ static void compute(const Tile& t, int kb, const Stage<TC>& s, Acc& acc) {
-        const int lane = threadIdx.x & 31, wr = (threadIdx.x >> 5) * 16;
+        const int lane = threadIdx.x & 31, wr = strip(), cg = group_column();
         const int fr = lane >> 2, fk = lane & 3;  // fragment coordinates
         const int row_lo = t.r0 + wr, row_hi = row_lo + 15;
         const bool zero = wr >= t.rows || (t.tri == 1 && kb > row_hi) ||
@@ -891,7 +909,7 @@ struct TileOps {
                 for (int i = 0; i < 2; ++i) a[i] = s.a[(wr + 8 * i + fr) * kLdK + k4 + fk];
             }
 #pragma unroll
-            for (int j = 0; j < kJ; ++j) b[j] = s.b[(k4 + fk) * kLdB + 8 * j + fr];
+            for (int j = 0; j < kJ; ++j) b[j] = s.b[(k4 + fk) * kLdB + cg + 8 * j + fr];
 #pragma unroll
             for (int i = 0; i < 2; ++i)
 #pragma unroll
@@ -908,7 +926,7 @@ struct TileOps {
 
     // Applies the tile's op to its outputs.
     __device__ static void store(const Tile& t, int c0, const int* out_row, double* out, int k, const Acc& acc) {
-        const int fk = threadIdx.x & 3;
+        const int fk = threadIdx.x & 3, cg = group_column();
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
             const int r = out_row[i];
@@ -917,7 +935,7 @@ struct TileOps {
             for (int j = 0; j < kJ; ++j)
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    const int c = c0 + 8 * j + 2 * fk + h;
+                    const int c = c0 + cg + 8 * j + 2 * fk + h;
                     if (c >= k) continue;
                     double* o = out + (size_t)r * k + c;
                     const double v = acc[i][j][h];
@@ -1007,12 +1025,14 @@ __device__ __forceinline__ int first_inner(const Tile& t, const unsigned char* a
 
 // One launch per phase: a CTA per (tile, column block of TC columns).
 template <int TC>
-__global__ void __launch_bounds__(kTileThreads, TC == kTileCols ? kTileCtasPerSm : 8)
+__global__ void __launch_bounds__(tile_threads<TC>(), TC == kTileCols ? kTileCtasPerSm : kTileCtasPerSmNarrow)
 tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
                     const int* __restrict__ idx, double* rows, int k, const unsigned char* active, int trimmed) {
     extern __shared__ __align__(16) unsigned char shared_stages[];
     Stage<TC>* stage = reinterpret_cast<Stage<TC>*>(shared_stages);
-    const Tile& t = tiles[blockIdx.x];
+    // The tile's fields in registers: read through a reference, the loop would load them again
+    // from global memory after every barrier (0.420 -> 0.401 ms a pass on the 131k torus).
+    const Tile t = tiles[blockIdx.x];
     if (skip_inactive(t, active, trimmed, blockIdx.y * TC, TC, idx, rows, k)) return;
     tile_product<TC>(t, first_inner(t, active), blockIdx.y * TC, vals, idx, rows, rows, k, stage);
 }
@@ -1203,8 +1223,9 @@ struct Factor {
     int n_zero = 0;
     int tile_chunk = 0, tile_waves = 0;  // the split parameters the tile lists were built with
     // Column width of each level's tiles a direction (kTileCols or kTileColsNarrow): levels with
-    // fewer tiles than narrow_waves waves of the resident grid take the narrow form (0: none).
-    int narrow_waves = 0;
+    // fewer tiles than narrow_waves waves of the resident grid take the narrow form (0: none; the
+    // default, 64, every level: on the 131k torus at 64 columns 0.375 against 0.401 ms a pass).
+    int narrow_waves = 64;
     std::vector<int> fwd_cols, bwd_cols;
     // Deterministic passes: no split tiles, and each node's forward update G B[own] written to its
     // own rows U of the work buffer (rows 3n ..), then added into its target rows by one gather a
@@ -1617,10 +1638,11 @@ int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream,
             default:
                 if (cols == kTileColsNarrow)
                     tile_product_kernel<kTileColsNarrow>
-                        <<<dim3(count, ceil_div(k, kTileColsNarrow)), kTileThreads, stage_bytes<kTileColsNarrow>(),
+                        <<<dim3(count, ceil_div(k, kTileColsNarrow)), tile_threads<kTileColsNarrow>(),
+                           stage_bytes<kTileColsNarrow>(),
                            stream>>>(tiles, F->vals, F->idx, W.BYX, k, active, trimmed);
                 else
-                    tile_product_kernel<kTileCols><<<dim3(count, ceil_div(k, kTileCols)), kTileThreads,
+                    tile_product_kernel<kTileCols><<<dim3(count, ceil_div(k, kTileCols)), tile_threads<kTileCols>(),
                                                       stage_bytes<kTileCols>(), stream>>>(tiles, F->vals, F->idx,
                                                                                           W.BYX, k, active, trimmed);
         }

@@ -32,8 +32,9 @@ CANDIDATES: tuple[tuple[int, int], ...] = (
     (64, 2), (0, 0), (32, 2), (128, 2), (64, 1), (64, 4), (128, 4), (32, 1),
 )
 # Width rules: the levels with fewer tiles than this many waves take 32-column tiles (0: none,
-# 64: every level).
-WIDTHS: tuple[int, ...] = (0, 1, 2, 4, 64)
+# 64: every level, the factor's default, under which the split schedules are timed).
+WIDTHS: tuple[int, ...] = (64, 0, 1, 2, 4)
+DEFAULT_WIDTH = 64
 
 
 def _time(factor: Any, k: int, reps: int) -> float:
@@ -69,7 +70,7 @@ def tune_pass(factor: Any, k: int, *, reps: int = 10,
     Returns ``{"best": (chunk, waves), "ms": {(chunk, waves): ms, ...}}``."""
     times: dict[tuple[int, int], float] = {}
     widths: dict[int, float] = {}
-    _lib.call("ob_chol_tile_columns", factor.handle, 0, None)
+    _lib.call("ob_chol_tile_columns", factor.handle, DEFAULT_WIDTH, None)
     if getattr(factor, "deterministic", False):
         # A deterministic factor never splits (its passes take no atomics): one schedule.
         times[(0, 0)] = _time(factor, k, reps)
@@ -80,9 +81,9 @@ def tune_pass(factor: Any, k: int, *, reps: int = 10,
             times[(chunk, waves)] = _time(factor, k, reps)
         best = min(times, key=times.get)
         _lib.call("ob_chol_tile", factor.handle, best[0], best[1], None)
-    for narrow in WIDTHS if k > 8 else (0,):
+    for narrow in WIDTHS if k > 8 else (DEFAULT_WIDTH,):
         _lib.call("ob_chol_tile_columns", factor.handle, int(narrow), None)
-        widths[narrow] = times[best] if narrow == 0 else _time(factor, k, reps)
+        widths[narrow] = times[best] if narrow == DEFAULT_WIDTH else _time(factor, k, reps)
     width = min(widths, key=widths.get)
     _lib.call("ob_chol_tile_columns", factor.handle, int(width), None)
     return {"best": best, "ms": times, "narrow_waves": width, "width_ms": widths}
