@@ -1023,7 +1023,10 @@ __device__ __forceinline__ int first_inner(const Tile& t, const unsigned char* a
     return (active != nullptr && t.tri == 2 && !active[t.node]) ? max(t.k0, t.tri_k) : t.k0;
 }
 
-// One launch per phase: a CTA per (tile, column block of TC columns).
+// One launch per phase: a CTA per (tile, column block of TC columns), the column block varying
+// fastest, so a tile's blocks run side by side and its matrix block, read by each, comes from
+// DRAM once (tile-major with the blocks apart, the second read missed L2: 757 against 619 MB a
+// pass on the 131k torus at 64 columns in 32-column blocks).
 template <int TC>
 __global__ void __launch_bounds__(tile_threads<TC>(), TC == kTileCols ? kTileCtasPerSm : kTileCtasPerSmNarrow)
 tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ vals,
@@ -1032,9 +1035,11 @@ tile_product_kernel(const Tile* __restrict__ tiles, const double* __restrict__ v
     Stage<TC>* stage = reinterpret_cast<Stage<TC>*>(shared_stages);
     // The tile's fields in registers: read through a reference, the loop would load them again
     // from global memory after every barrier (0.420 -> 0.401 ms a pass on the 131k torus).
-    const Tile t = tiles[blockIdx.x];
-    if (skip_inactive(t, active, trimmed, blockIdx.y * TC, TC, idx, rows, k)) return;
-    tile_product<TC>(t, first_inner(t, active), blockIdx.y * TC, vals, idx, rows, rows, k, stage);
+    const int blocks = (k + TC - 1) / TC;
+    const Tile t = tiles[blockIdx.x / blocks];
+    const int c0 = (int)(blockIdx.x % blocks) * TC;
+    if (skip_inactive(t, active, trimmed, c0, TC, idx, rows, k)) return;
+    tile_product<TC>(t, first_inner(t, active), c0, vals, idx, rows, rows, k, stage);
 }
 
 // The same tile product for a narrow batch (KP = 2, 4, 6 or 8 columns, the even stride of 1-8
@@ -1638,11 +1643,11 @@ int triangular_solves(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream,
             default:
                 if (cols == kTileColsNarrow)
                     tile_product_kernel<kTileColsNarrow>
-                        <<<dim3(count, ceil_div(k, kTileColsNarrow)), tile_threads<kTileColsNarrow>(),
+                        <<<(unsigned)count * ceil_div(k, kTileColsNarrow), tile_threads<kTileColsNarrow>(),
                            stage_bytes<kTileColsNarrow>(),
                            stream>>>(tiles, F->vals, F->idx, W.BYX, k, active, trimmed);
                 else
-                    tile_product_kernel<kTileCols><<<dim3(count, ceil_div(k, kTileCols)), tile_threads<kTileCols>(),
+                    tile_product_kernel<kTileCols><<<(unsigned)count * ceil_div(k, kTileCols), tile_threads<kTileCols>(),
                                                       stage_bytes<kTileCols>(), stream>>>(tiles, F->vals, F->idx,
                                                                                           W.BYX, k, active, trimmed);
         }
