@@ -431,7 +431,7 @@ int ob_chol_tile(void* factor, int chunk, int waves, ob_stream_t stream);
  * 64-row tensor-core tiles per tree level -- levels with fewer tiles than narrow_waves waves of
  * the resident grid (0 to 64; 0: none) take 32-column tiles (twice the CTAs, each half the
  * columns) instead of 64; the default after ob_chol_factor is 64 (every level). Batches of 1-8
- * columns always take the register kernel. Waits for the device, drops the recorded solves and
+ * columns always take the register kernel, batches of 9-16 columns 16-column tiles. Waits for the device, drops the recorded solves and
  * moves the work generations as ob_chol_tile does. */
 int ob_chol_tile_columns(void* factor, int narrow_waves, ob_stream_t stream);
 int ob_chol_info(void* factor, long long* info);
