@@ -1070,6 +1070,10 @@ def run_b200(args: argparse.Namespace, dist: Dist) -> None:
         reference_benchmarks = run_reference_benchmarks()
     serving = None
     if not args.no_serving and dist.world == 1:
+        # The earlier sections' meshes and factors freed now, not by a collection inside the
+        # stream's window (a factor's release waits for the device).
+        gc.collect()
+        synchronize()
         serving = run_serving(args.serving_rate, args.serving_vmax, args.serving_warmup,
                               args.serving_requests)
         if not args.no_serving_full_range:
