@@ -531,7 +531,9 @@ int ob_amg_time_kernels(void* amg, int k, int reps, float* ms, long long* bytes,
  * source vertex of mesh m's query in column c (-1: none, its distances are written 0); each
  * mesh's field is shifted by its source's value and oriented by its own mean
  * (kernels/heat.py:3384-3424); out is (n_columns, V); sums is 2 * n_meshes * n_columns doubles
- * of scratch. */
+ * of scratch. A mesh's sum is taken over chunks of 2048 of its rows (each chunk's sums apart,
+ * then added in chunk order: the same order for a given packing), so large meshes do not hold
+ * the launch; the call allocates its chunk table in stream order. */
 int ob_edge_sums_segments(const int32_t* offsets, const int32_t* columns, const int32_t* run_start,
                           const uint64_t* keys, int count, const float* xyz, int face_edges,
                           const int32_t* segments, int n_segments, double* out, ob_stream_t stream);

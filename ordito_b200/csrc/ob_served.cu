@@ -611,57 +611,122 @@ __global__ void shift_out_kernel(const double* __restrict__ phi, int n, int stri
 
 // Packed meshes (many meshes as one block-diagonal system, column c = every mesh's c-th
 // single-source query): per (mesh, column) the sum of phi over the mesh's rows and phi at the
-// query's source, one block a mesh, threads owning column t % stride (blockDim a multiple of
-// stride), added in a fixed order.
-__global__ void shift_packed_sums_kernel(const double* __restrict__ phi, int stride, const int* __restrict__ iperm,
-                                         const int* __restrict__ vertex_offsets, const int* __restrict__ sources,
-                                         int k, double2* __restrict__ sums) {
+// query's source. Each mesh's rows are cut into chunks of kPackedChunk (a block a chunk, so a
+// large mesh is summed by many blocks and the grid does not wait on the largest mesh), each
+// chunk's per-column sums written apart, then folded per mesh in chunk order: a fixed order for a
+// given packing.
+constexpr int kPackedChunk = 2048;
+
+// The chunk table: chunk_first[m] = mesh m's first chunk (chunk_first[n_meshes] = the count) and
+// per chunk (mesh, first row, end row). One block; the meshes' chunk counts are scanned in
+// order, kThreads meshes at a time.
+__global__ void packed_chunks_kernel(const int* __restrict__ vertex_offsets, int n_meshes,
+                                     int* __restrict__ chunk_first, int4* __restrict__ chunks) {
+    __shared__ int scan[kThreads];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < n_meshes; base += blockDim.x) {
+        const int m = base + threadIdx.x;
+        const int v0 = m < n_meshes ? vertex_offsets[m] : 0, v1 = m < n_meshes ? vertex_offsets[m + 1] : 0;
+        const int count = (v1 - v0 + kPackedChunk - 1) / kPackedChunk;
+        scan[threadIdx.x] = count;
+        __syncthreads();
+        for (int d = 1; d < (int)blockDim.x; d <<= 1) {  // inclusive scan (Hillis-Steele)
+            const int add = threadIdx.x >= (unsigned)d ? scan[threadIdx.x - d] : 0;
+            __syncthreads();
+            scan[threadIdx.x] += add;
+            __syncthreads();
+        }
+        const int first = carry + scan[threadIdx.x] - count;
+        if (m < n_meshes) {
+            chunk_first[m] = first;
+            for (int j = 0; j < count; ++j)
+                chunks[first + j] = make_int4(m, v0 + j * kPackedChunk, min(v1, v0 + (j + 1) * kPackedChunk), 0);
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry += scan[threadIdx.x];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) chunk_first[n_meshes] = carry;
+}
+
+// A chunk's per-column sums of phi: threads own column t % stride (blockDim a multiple of
+// stride), rows t / stride + j (blockDim / stride) in order, then the row groups added in order.
+__global__ void packed_partials_kernel(const double* __restrict__ phi, int stride, const int* __restrict__ iperm,
+                                       const int* __restrict__ chunk_first, int n_meshes,
+                                       const int4* __restrict__ chunks, double* __restrict__ partials) {
     __shared__ double tree[kThreads];
-    const int m = blockIdx.x;
-    const int c = threadIdx.x % stride;
-    const int v0 = vertex_offsets[m], v1 = vertex_offsets[m + 1];
+    if ((int)blockIdx.x >= chunk_first[n_meshes]) return;
+    const int4 chunk = chunks[blockIdx.x];
+    const int c = threadIdx.x % stride, rows_per_pass = blockDim.x / stride;
     double total = 0.0;
-    const int rows_per_pass = blockDim.x / stride;
-    for (int v = v0 + threadIdx.x / stride; v < v1; v += rows_per_pass)
+    for (int v = chunk.y + threadIdx.x / stride; v < chunk.z; v += rows_per_pass)
         total += phi[(size_t)row_of(iperm, v) * stride + c];
     tree[threadIdx.x] = total;
     __syncthreads();
-    if ((int)threadIdx.x < stride && (int)threadIdx.x < k) {
+    if ((int)threadIdx.x < stride) {
         double column = 0.0;
         for (int t = threadIdx.x; t < (int)blockDim.x; t += stride) column += tree[t];
-        const int s = sources[(size_t)m * k + threadIdx.x];
-        const double at = s >= 0 ? phi[(size_t)row_of(iperm, v0 + s) * stride + threadIdx.x] : 0.0;
-        sums[(size_t)m * k + threadIdx.x] = make_double2(at, column);
+        partials[(size_t)blockIdx.x * stride + threadIdx.x] = column;
+    }
+}
+
+// sums[m][c] = (phi at mesh m's c-th source, or 0 without one; the mesh's chunks' sums in chunk
+// order): a block a mesh, a thread a column.
+__global__ void packed_fold_kernel(const double* __restrict__ phi, int stride, const int* __restrict__ iperm,
+                                   const int* __restrict__ vertex_offsets, const int* __restrict__ sources, int k,
+                                   const int* __restrict__ chunk_first, const double* __restrict__ partials,
+                                   double2* __restrict__ sums) {
+    const int m = blockIdx.x;
+    for (int c = threadIdx.x; c < k; c += blockDim.x) {
+        double column = 0.0;
+        for (int b = chunk_first[m]; b < chunk_first[m + 1]; ++b) column += partials[(size_t)b * stride + c];
+        const int s = sources[(size_t)m * k + c];
+        const double at = s >= 0 ? phi[(size_t)row_of(iperm, vertex_offsets[m] + s) * stride + c] : 0.0;
+        sums[(size_t)m * k + c] = make_double2(at, column);
     }
 }
 
 // out[c][v]: the shifted, oriented phi of vertex v in column c (kernels/heat.py:3406 per mesh);
-// zero where v's mesh has no query in column c.
+// zero where v's mesh has no query in column c. Tiles of 32 vertices x 32 columns: phi read along
+// a row's columns, out written along vertices, each vertex's mesh found once a tile.
 __global__ void shift_packed_out_kernel(const double* __restrict__ phi, int n, int stride,
                                         const int* __restrict__ iperm, const int* __restrict__ vertex_offsets,
                                         int n_meshes, const int* __restrict__ sources, int k,
                                         const double2* __restrict__ sums, double* __restrict__ out) {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= (long long)n * k) return;
-    const int c = (int)(t / n), v = (int)(t % n);
-    int lo = 0, hi = n_meshes - 1;  // the mesh holding v: vertex_offsets[m] <= v < [m + 1]
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) / 2;
-        if (vertex_offsets[mid] <= v) lo = mid;
-        else hi = mid - 1;
+    __shared__ double tile[32][33];
+    __shared__ int mesh_of[32];
+    const int v0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+    if (threadIdx.y == 0) {
+        const int v = v0 + threadIdx.x;
+        int lo = 0, hi = n_meshes - 1;  // the mesh holding v: vertex_offsets[m] <= v < [m + 1]
+        if (v < n)
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) / 2;
+                if (vertex_offsets[mid] <= v) lo = mid;
+                else hi = mid - 1;
+            }
+        mesh_of[threadIdx.x] = lo;
     }
-    const int m = lo;
-    if (sources[(size_t)m * k + c] < 0) {
-        out[t] = 0.0;
-        return;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int v = v0 + i, c = c0 + threadIdx.x;
+        if (v < n && c < k) tile[i][threadIdx.x] = phi[(size_t)row_of(iperm, v) * stride + c];
     }
-    const double2 s = sums[(size_t)m * k + c];
-    const double offset = s.x;
-    const double value = phi[(size_t)row_of(iperm, v) * stride + c];
-    double shifted = value - offset;
-    const int count = vertex_offsets[m + 1] - vertex_offsets[m];
-    if (s.y / (double)count - offset < 0.0) shifted = offset - value;
-    out[t] = shifted;
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int c = c0 + i, v = v0 + threadIdx.x;
+        if (v >= n || c >= k) continue;
+        const int m = mesh_of[threadIdx.x];
+        double shifted = 0.0;
+        if (sources[(size_t)m * k + c] >= 0) {
+            const double2 s = sums[(size_t)m * k + c];
+            const double value = tile[threadIdx.x][i];
+            const int count = vertex_offsets[m + 1] - vertex_offsets[m];
+            shifted = (s.y / (double)count - s.x < 0.0) ? s.x - value : value - s.x;
+        }
+        out[(size_t)c * n + v] = shifted;
+    }
 }
 
 }  // namespace
@@ -881,12 +946,23 @@ int ob_shift_packed(const double* phi, int n_vertices, int stride, const int32_t
     OB_REQUIRE(n_vertices >= 1 && n_meshes >= 1 && n_columns >= 1 && stride >= n_columns && stride <= kThreads,
                "ob_shift_packed: bad size");
     OB_REQUIRE(phi && vertex_offsets && sources && sums && out, "ob_shift_packed: null pointer");
+    // At most one partial chunk a mesh beyond the full ones.
+    const long long chunk_bound = (long long)n_vertices / kPackedChunk + n_meshes;
+    Scratch scratch(stream);
+    int* chunk_first = scratch.take<int>((size_t)n_meshes + 1);
+    int4* chunks = scratch.take<int4>((size_t)chunk_bound);
+    double* partials = scratch.take<double>((size_t)chunk_bound * stride);
+    if (int st = scratch.commit()) return st;
+    packed_chunks_kernel<<<1, kThreads, 0, stream>>>(vertex_offsets, n_meshes, chunk_first, chunks);
+    OB_CHECK_LAUNCH("shift_packed chunks");
     const int threads = (kThreads / stride) * stride;
-    shift_packed_sums_kernel<<<n_meshes, threads, 0, stream>>>(phi, stride, iperm, vertex_offsets, sources,
-                                                               n_columns, reinterpret_cast<double2*>(sums));
-    OB_CHECK_LAUNCH("shift_packed_sums");
-    const long long total = (long long)n_vertices * n_columns;
-    shift_packed_out_kernel<<<ceil_div(total, kThreads), kThreads, 0, stream>>>(
+    packed_partials_kernel<<<(unsigned)chunk_bound, threads, 0, stream>>>(phi, stride, iperm, chunk_first, n_meshes,
+                                                                        chunks, partials);
+    OB_CHECK_LAUNCH("shift_packed partials");
+    packed_fold_kernel<<<n_meshes, 32, 0, stream>>>(phi, stride, iperm, vertex_offsets, sources, n_columns,
+                                                    chunk_first, partials, reinterpret_cast<double2*>(sums));
+    OB_CHECK_LAUNCH("shift_packed fold");
+    shift_packed_out_kernel<<<dim3(ceil_div(n_vertices, 32), ceil_div(n_columns, 32)), dim3(32, 8), 0, stream>>>(
         phi, n_vertices, stride, iperm, vertex_offsets, n_meshes, sources, n_columns,
         reinterpret_cast<const double2*>(sums), out);
     OB_CHECK_LAUNCH("shift_packed_out");

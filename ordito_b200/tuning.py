@@ -81,7 +81,9 @@ def tune_pass(factor: Any, k: int, *, reps: int = 10,
             times[(chunk, waves)] = _time(factor, k, reps)
         best = min(times, key=times.get)
         _lib.call("ob_chol_tile", factor.handle, best[0], best[1], None)
-    for narrow in WIDTHS if k > 8 else (DEFAULT_WIDTH,):
+    # Batches of up to 16 columns take the register kernel or the 16-column tiles whatever the
+    # width rule: nothing to search.
+    for narrow in WIDTHS if k > 16 else (DEFAULT_WIDTH,):
         _lib.call("ob_chol_tile_columns", factor.handle, int(narrow), None)
         widths[narrow] = times[best] if narrow == DEFAULT_WIDTH else _time(factor, k, reps)
     width = min(widths, key=widths.get)
