@@ -1605,12 +1605,15 @@ int ensure_work(Factor* F, Factor::WorkSet& W, int k, cudaStream_t stream) {
 // x_new = A^-1 b_new in the factor's numbering (B is consumed); k is the even internal stride.
 // Marks the supernodes a batch of source indicators reaches: each source's supernode (through
 // the factor's numbering) and every ancestor, up to one already marked (whose marker goes on to
-// the root). sources[source_offsets[0] .. source_offsets[n_columns]) are vertex indices.
+// the root). sources[source_offsets[0] .. source_offsets[n_columns]) are vertex indices, a thread
+// a source over the grid (the walks run side by side: two that meet both write 1, and one that
+// stops at a marked node leaves the rest of the chain to the thread that marked it).
+constexpr int kMarkBlocks = 32;
 __global__ void mark_sources_kernel(const int* __restrict__ sources, const int* __restrict__ source_offsets,
                                     int n_columns, const int* __restrict__ iperm, const int* __restrict__ node_of_row,
                                     const int* __restrict__ parent, unsigned char* active) {
     const int total = source_offsets[n_columns] - source_offsets[0];
-    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         int node = node_of_row[iperm[sources[source_offsets[0] + i]]];
         while (node >= 0) {
             const unsigned char was = active[node];
@@ -1955,7 +1958,7 @@ int ob_chol_solve_in_place_sources(void* factor, int set, int n_columns, const i
         if (st) return st;
     }
     OB_CUDA(cudaMemsetAsync(W.active, 0, std::max(F->n_nodes, 1), stream));
-    mark_sources_kernel<<<1, 256, 0, stream>>>(sources, source_offsets, n_columns, F->iperm, F->node_of_row,
+    mark_sources_kernel<<<kMarkBlocks, 256, 0, stream>>>(sources, source_offsets, n_columns, F->iperm, F->node_of_row,
                                               F->parent_node, W.active);
     OB_CHECK_LAUNCH("chol mark sources");
     return triangular_solves(F, W, even_columns(n_columns), stream, W.active);
