@@ -31,6 +31,22 @@ from ordito_b200.heat import _bounds_floor_length, capture_guard
 from ordito_b200.laplacian import face_terms, mesh_operator_pattern
 
 
+def mesh_bounds(xyz: np.ndarray, vertex_offsets: np.ndarray) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Each packed mesh's bounding box in one pass over the union's float32 vertices (``xyz``,
+    mesh m's rows ``vertex_offsets[m] .. vertex_offsets[m + 1]``): its low and high corners (the
+    float32 extremes a per-mesh ``min`` / ``max`` gives; zeros for an empty mesh) and the indices
+    of the meshes that have vertices."""
+    counts = np.diff(vertex_offsets)
+    nonempty = np.flatnonzero(counts > 0)
+    low = np.zeros((counts.size, 3), dtype=np.float32)
+    high = np.zeros((counts.size, 3), dtype=np.float32)
+    if nonempty.size:
+        starts = np.asarray(vertex_offsets)[nonempty]
+        low[nonempty] = np.minimum.reduceat(xyz, starts, axis=0)
+        high[nonempty] = np.maximum.reduceat(xyz, starts, axis=0)
+    return low, high, nonempty
+
+
 class PackedMeshes:
     """Meshes ``[(vertices, faces), ...]`` held on the device as one block-diagonal system with
     both factors, for batches of single-source queries (``solve``)."""
@@ -68,14 +84,7 @@ class PackedMeshes:
         s = sums.numpy().reshape(self.n_meshes, 2)
         h = np.where(s[:, 1] > 0, s[:, 0] / np.where(s[:, 1] > 0, s[:, 1], 1.0), 0.0)
         t = h * h
-        # Each mesh's bounding box in one pass over the union (float32 extremes, as per mesh).
-        nonempty = np.flatnonzero(counts > 0)
-        low = np.zeros((self.n_meshes, 3), dtype=np.float32)
-        high = np.zeros((self.n_meshes, 3), dtype=np.float32)
-        if nonempty.size:
-            starts = self.vertex_offsets[nonempty]
-            low[nonempty] = np.minimum.reduceat(xyz, starts, axis=0)
-            high[nonempty] = np.maximum.reduceat(xyz, starts, axis=0)
+        low, high, nonempty = mesh_bounds(xyz, self.vertex_offsets)
         for m in nonempty:
             floor = _bounds_floor_length(low[m], high[m]) ** 2
             if floor > t[m]:

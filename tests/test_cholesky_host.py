@@ -74,3 +74,46 @@ def test_an_indefinite_operator_is_refused() -> None:
     with pytest.raises(_lib.CudaError):
         # -H is negative definite: the first pivot is negative.
         host_solve(ops["pattern"], -ops["H"], v, False, np.ones(v.shape[0]))
+
+
+def _host_analysis_nodes(pattern, vertices):
+    n = pattern["offsets"].size - 1
+    off = np.ascontiguousarray(pattern["offsets"], dtype=np.int32)
+    col = np.ascontiguousarray(pattern["columns"], dtype=np.int32)
+    xyz = np.ascontiguousarray(vertices, dtype=np.float32)
+    handle = ctypes.c_void_p(0)
+    _lib.call("ob_chol_host_analyse", n, off.ctypes.data, col.ctypes.data, xyz.ctypes.data, 0,
+              ctypes.byref(handle))
+    try:
+        info = (ctypes.c_longlong * 5)()
+        _lib.call("ob_chol_analysis_info", handle, info)
+        nodes = np.zeros((int(info[1]), 4), dtype=np.int32)
+        _lib.call("ob_chol_analysis_nodes", handle, nodes.ctypes.data)
+        return [int(i) for i in info], nodes
+    finally:
+        _lib.lib.ob_chol_analysis_destroy(handle)
+
+
+def test_threaded_analysis_of_a_large_mesh_is_reproducible_and_solves() -> None:
+    """A mesh past the sizes where the analysis spreads its adjacency and symbolic passes over
+    host threads (65 536 vertices, 262 144 entries): two analyses give the same supernodes, the
+    tree is consistent, and the host solve through it matches the oracle componentwise."""
+    v, f = creation.jittered_torus(384, 192, seed=3)
+    assert v.shape[0] > 1 << 16
+    ops = hp.heat_operators(v, f)
+    pattern = ops["pattern"]
+    assert pattern["offsets"][-1] > 1 << 18
+    info, nodes = _host_analysis_nodes(pattern, v)
+    again_info, again = _host_analysis_nodes(pattern, v)
+    assert info == again_info and np.array_equal(nodes, again)
+    level, count, _, parent = nodes.T
+    assert info[0] == v.shape[0] and int(count.sum()) == v.shape[0]
+    has_parent = parent >= 0
+    assert np.all(level[parent[has_parent]] > level[has_parent])
+    assert int(level.max()) + 1 == info[2]
+    u0 = np.zeros(v.shape[0])
+    u0[17] = 1.0
+    x, _ = host_solve(pattern, ops["H"], v, False, u0)
+    ref = hp.HeatFactor(hp.csr_matrix(pattern, ops["H"])).solve(u0)
+    mask = ref > 1e-250
+    assert np.max(np.abs(x - ref)[mask] / ref[mask]) <= 1e-10

@@ -21,3 +21,25 @@ def test_packed_workload() -> None:
     again = packed_workload(3, 256)
     assert again.specs == w.specs and again.queries == w.queries
     assert 256 <= total_queries(w.queries) <= 16 * 256
+
+
+def test_mesh_bounds_match_each_mesh_alone() -> None:
+    """The union's per-mesh bounding boxes (one reduceat pass) are each mesh's own float32
+    extremes, empty meshes included."""
+    import numpy as np
+
+    from ordito_b200.packed import mesh_bounds
+
+    w = packed_workload(5, 40)
+    verts = [np.ascontiguousarray(v, dtype=np.float32).reshape(-1, 3) for v, _ in w.meshes]
+    verts.insert(7, np.zeros((0, 3), dtype=np.float32))  # an empty mesh in between
+    verts.append(np.zeros((0, 3), dtype=np.float32))     # and one at the end
+    offsets = np.zeros(len(verts) + 1, dtype=np.int32)
+    np.cumsum([v.shape[0] for v in verts], out=offsets[1:])
+    low, high, nonempty = mesh_bounds(np.concatenate(verts), offsets)
+    assert list(nonempty) == [m for m, v in enumerate(verts) if v.shape[0]]
+    for m, v in enumerate(verts):
+        if v.shape[0]:
+            assert np.array_equal(low[m], v.min(axis=0)) and np.array_equal(high[m], v.max(axis=0))
+        else:
+            assert not low[m].any() and not high[m].any()
